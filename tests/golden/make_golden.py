@@ -1,0 +1,115 @@
+"""Make the golden solve fixtures of tests/golden/*.npz.
+
+Runs the CPU oracle -- the reference's own sources compiled by oracle/Makefile
+(oracle/_ref/yuzen_oracle), with the CPU restatement of the linear-solver
+backend -- on small variants of the reference's shipped cases, with the dump
+hook on (YZO_DUMP_DIR), and stores a few of the linear systems it solved (the
+height-equation matrix I + theta dt J, the concentration matrix, their
+right-hand sides, initial guesses and the oracle's answers).
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+This script needs the reference checkout (it reads cases/*.toml there) and the
+built oracle; the fixtures it writes are self-contained.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+import tempfile
+import tomllib
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parents[1]
+sys.path.insert(0, str(HERE))
+
+import dumpio  # noqa: E402
+import tomlw  # noqa: E402
+
+ORACLE = REPO / "oracle" / "_ref" / "yuzen_oracle"
+
+QUIET_OUTPUT = {
+    "Output.FieldData.TimeInterval": 1e30,
+    "Output.FieldData.NeutralFile": False,
+    "Output.FieldData.VTKFile": False,
+    "Output.GeneralHistory.TimeInterval": 1e30,
+    "Output.CalcInfo.TimeInterval": 1e30,
+    "Output.ProbeList.TimeInterval": 1e30,
+}
+
+#  name: (reference case, overrides, which dumps to keep: the first three solves
+#  of a run are set-up solves of the boundary rows; the Newton systems follow)
+CASES = {
+    # 2-D, every term of the height equation, WM concentration; 64^2 so that
+    # the AMG has more than one level (n = 68^2 > 3000)
+    "allphys2d_64": ("allphys_2d_reg.toml", {
+        "Grid.Nx": 64, "Grid.Ny": 64,
+        "Numerics.TimeStepControl.Enable": False,
+        "Numerics.InitialDt": 1e-4, "Numerics.MaxSteps": 2,
+    }, [4, 5, 6, 8, 10]),
+    # 2-D periodic film with the disjoining pressure (no concentration solve)
+    "disjoin2d_periodic_56": ("allphys_2d_reg.toml", {
+        "Grid.Nx": 56, "Grid.Ny": 56,
+        "Boundary.XminBC.Type": "Periodic", "Boundary.XmaxBC.Type": "Periodic",
+        "Boundary.YminBC.Type": "Periodic", "Boundary.YmaxBC.Type": "Periodic",
+        "Physics.ConcField.Model": "None",
+        "Physics.SolutoCapillarity.Enable": False, "Physics.VerticalGravity.Enable": False,
+        "Physics.HorizontalGravity.Enable": False, "Physics.Centrifugal.Enable": False,
+        "Physics.Evaporation.Enable": False,
+        "Physics.DisjoiningPressure.Enable": True, "Physics.DisjoiningPressure.ContactAngle": 10.0,
+        "Physics.DisjoiningPressure.ExponentN": 3.0, "Physics.DisjoiningPressure.ExponentM": 2.0,
+        "Initial.SurfaceShape.PrecursorRatio": 0.05,
+        "Numerics.TimeStepControl.Enable": False,
+        "Numerics.InitialDt": 1e-4, "Numerics.MaxSteps": 1,
+    }, [3, 4]),
+    # 1-D capillary levelling over a substrate bump (single direct AMG level)
+    "leveling1d": ("leveling_1d_reg.toml", {
+        "Numerics.TimeStepControl.Enable": False,
+        "Numerics.InitialDt": 1e-3, "Numerics.MaxSteps": 1,
+        "Numerics.HeightEquation.LinearSolver.Backend": "amgcl",
+    }, [4, 6, 8, 10]),
+}
+
+
+def make_case(ref: Path, name: str, work: Path) -> list[dict]:
+    src, over, keep = CASES[name]
+    doc = tomllib.loads((ref / "cases" / src).read_text())
+    for k, v in {**QUIET_OUTPUT, **over}.items():
+        tomlw.setpath(doc, k, v)
+    doc["JobName"] = name
+    case = work / f"{name}.toml"
+    case.write_text(tomlw.dumps(doc))
+    dump = work / f"dump_{name}"
+    dump.mkdir()
+    env = dict(os.environ, YZO_DUMP_DIR=str(dump), YZO_DUMP_MAX="16", OMP_NUM_THREADS="4")
+    res = subprocess.run([str(ORACLE), case.name], cwd=work, env=env, capture_output=True, text=True, timeout=900)
+    if res.returncode != 0:
+        raise RuntimeError(f"{name}: oracle failed\n{res.stdout[-2000:]}\n{res.stderr[-2000:]}")
+    files = sorted(dump.glob("solve_*.bin"))
+    out = [dumpio.read_dump(files[j]) for j in keep if j < len(files)]
+    for d in out:
+        d["case"] = name
+    return out
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", default=None)
+    a = ap.parse_args()
+    if not ORACLE.exists():
+        raise SystemExit(f"{ORACLE} missing: make -C oracle ref")
+    with tempfile.TemporaryDirectory() as tmp:
+        for name in CASES:
+            if a.only and name != a.only:
+                continue
+            dumps = make_case(Path(a.ref), name, Path(tmp))
+            dumpio.save_npz(HERE / f"solve_{name}.npz", dumps)
+            print(name, [(d["n"], d["nnz"], d["conc"], d["iter"], d["ret"]) for d in dumps])
+
+
+if __name__ == "__main__":
+    main()

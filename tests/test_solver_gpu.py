@@ -1,0 +1,155 @@
+"""Parity of the CUDA linear solve with the CPU oracle.
+
+The FP64 solve is specified operation for operation by the oracle
+(oracle/solver/yzo_solver.cpp), so the bar is bit equality: the answer x, the
+iteration count, the reported residual, the return code, and the AMG
+hierarchy (every level's matrix, prolongation and aggregate map).
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import _oracle
+import _systems
+import dumpio
+import yuzen_b200 as yz
+
+pytestmark = pytest.mark.gpu
+GOLDEN = sorted(Path(__file__).parent.joinpath("golden").glob("solve_*.npz"))
+
+
+def _amg_cases():
+    for f in GOLDEN:
+        for j, d in enumerate(dumpio.load_npz(f)):
+            if int(d["flavour"]) == _oracle.YZO_AMG:
+                yield pytest.param(d, id=f"{f.stem}-{j}")
+
+
+def gpu_solve(d, backend=None, **over):
+    s = yz.LinearSolverSettings(precondition=int(over.get("precondition", d["precondition"])),
+                                scaling=bool(over.get("scaling", d["scaling"])),
+                                maxIteration=int(over.get("max_iteration", d["max_iteration"])),
+                                epsilon=float(over.get("epsilon", d["epsilon"])),
+                                conc=bool(over.get("conc", d["conc"])))
+    be = backend or yz.B200Backend()
+    pat = yz.CrsPattern(d["rowptr"], d["col"], d["sorted_col"], d["sorted_src"])
+    x = np.array(d["x0"], dtype=np.float64, copy=True)
+    ret, it, res = be.Solve(s, pat, d["values"], d["rhs"], x)
+    return ret, it, res, x, be
+
+
+def assert_same(a, b):
+    assert a[0] == b[0], ("ret", a[0], b[0])
+    assert a[1] == b[1], ("iter", a[1], b[1])
+    assert a[2] == b[2], ("resid", a[2], b[2])
+    assert np.array_equal(a[3], b[3]), np.max(np.abs(a[3] - b[3]))
+
+
+@pytest.mark.parametrize("n", [0, 1, 255, 4095, 4096, 4097, 300001, 1 << 20])
+def test_dot_bitwise(n):
+    rng = np.random.default_rng(n)
+    x, y = rng.standard_normal(n), rng.standard_normal(n) * 1e3
+    assert yz.dot(x, y) == _oracle.dot(x, y)
+
+
+@pytest.mark.parametrize("d", list(_amg_cases()))
+def test_spmv_bitwise(d):
+    x = np.random.default_rng(1).standard_normal(d["n"])
+    assert np.array_equal(yz.spmv(d["rowptr"], d["col"], d["values"], x),
+                          _oracle.spmv(d["rowptr"], d["col"], d["values"], x))
+
+
+@pytest.mark.parametrize("d", list(_amg_cases()))
+def test_golden_solve_bitwise(d):
+    g = gpu_solve(d)
+    o = _oracle.OracleSolver().solve(d)
+    assert_same(g[:4], o)
+    # and the oracle's answer inside the reference run
+    assert g[0] == d["ret"] and g[1] == d["iter"] and g[2] == d["resid"]
+    assert np.array_equal(g[3], d["x"])
+
+
+def _levels_equal(gl, ol):
+    assert len(gl) == len(ol)
+    for a, b in zip(gl, ol):
+        assert (a["rows"], a["nnz_a"], a["nnz_p"], a["direct"]) == (b["rows"], b["nnz_a"], b["nnz_p"], b["direct"])
+        assert np.array_equal(a["a_ptr"], b["a_ptr"]) and np.array_equal(a["a_col"], b["a_col"])
+        assert np.array_equal(a["a_val"], b["a_val"])
+        if not a["direct"]:
+            assert np.array_equal(a["agg"], b["agg"])
+            if a["nnz_p"]:
+                assert np.array_equal(a["p_ptr"], b["p_ptr"]) and np.array_equal(a["p_col"], b["p_col"])
+                assert np.array_equal(a["p_val"], b["p_val"])
+
+
+@pytest.mark.parametrize("d", [c for c in _amg_cases() if not c.values[0]["conc"]])
+def test_hierarchy_bitwise(d):
+    g = gpu_solve(d)
+    o = _oracle.OracleSolver()
+    o.solve(d)
+    _levels_equal(g[4].levels(), o.levels())
+
+
+@pytest.mark.parametrize("N,seed,periodic", [(96, 2, False), (200, 7, True), (384, 11, False)])
+def test_synthetic_film_bitwise(N, seed, periodic):
+    d = _systems.film_system(N, seed=seed, periodic=periodic)
+    g = gpu_solve(d)
+    o = _oracle.OracleSolver()
+    assert_same(g[:4], o.solve(d))
+    assert g[0] == 0
+    _levels_equal(g[4].levels(), o.levels())
+
+
+@pytest.mark.parametrize("pre,scaling,conc", [(0, 1, 0), (1, 1, 0), (2, 0, 0), (2, 1, 1)])
+def test_settings_variants_bitwise(pre, scaling, conc):
+    d = _systems.film_system(80, seed=4)
+    g = gpu_solve(d, precondition=pre, scaling=scaling, conc=conc)
+    o = _oracle.OracleSolver().solve(d, precondition=pre, scaling=scaling, conc=conc)
+    assert_same(g[:4], o)
+
+
+def test_backoff_sequence_matches_oracle():
+    """A SPAI0 try that fails backs off for 16 solves (TryBackoff); the GPU
+    context carries the same counters across a sequence of solves."""
+    d = _systems.film_system(48, seed=5, stiff=30.0)
+    be = yz.B200Backend()
+    o = _oracle.OracleSolver()
+    for k in range(3):
+        g = gpu_solve(d, backend=be, conc=1, max_iteration=40)
+        r = o.solve(d, conc=1, max_iteration=40)
+        assert_same(g[:4], r)
+        assert be.Memory() == o.memory()
+    be.SetMemory([0.0, 16.0])
+    assert be.Memory() == [0.0, 16.0]
+
+
+def test_poisson_analytic_through_gpu():
+    p = _systems.poisson1d(202)
+    ret, it, res, x, _ = gpu_solve(p)
+    assert ret == 0 and res < 1e-11
+    assert np.max(np.abs(x[1:-1] - p["exact"][1:-1])) < 1e-4
+
+
+def test_zero_rhs_and_untouched_inputs():
+    d = _systems.film_system(40, seed=9)
+    d["rhs"] = np.zeros(d["n"])
+    v0 = d["values"].copy()
+    ret, it, res, x, _ = gpu_solve(d)
+    assert ret == 0 and np.all(x == 0) and np.array_equal(v0, d["values"])
+
+
+def test_usage_errors_are_reported():
+    be = yz.B200Backend()
+    bad = yz.CrsPattern(np.array([0, 0], np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32))
+    with pytest.raises(yz.YzError):
+        be.SetPattern(bad)
+    x = np.zeros(1)
+    with pytest.raises(yz.YzError):
+        be.SolveDevice(yz.LinearSolverSettings(), 1, 1, 1)
+
+
+def test_kernels_actually_launch():
+    d = _systems.film_system(64, seed=1)
+    g = gpu_solve(d)
+    assert g[4].launches() > 50

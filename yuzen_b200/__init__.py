@@ -1,0 +1,275 @@
+"""yuzen_b200 -- the implicit time step of Yuzen's well-mixed film-height
+equation on one B200 (sm_100a), behind a C ABI (include/yuzen_b200.h).
+
+This module is a thin ctypes binding of that ABI.  It mirrors the reference's
+solver seam (yuzen/src/numerics/LinearSolverBackend.h:38-131):
+
+    LinearSolverSettings   -- the settings handed over on every solve
+    MakeLinearSolverBackend("b200") -> B200Backend, an ILinearSolverBackend
+        with Name / Build / Solve / Memory / SetMemory
+
+The CUDA library libyuzen_b200.so must have been built in-tree
+(python -m yuzen_b200.build); there is no CPU fallback, and every entry point
+raises when the library or a CUDA device is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+__all__ = [
+    "LinearSolverSettings", "B200Backend", "MakeLinearSolverBackend", "CrsPattern",
+    "lib", "lib_path", "YzError", "EXPORTED_SYMBOLS", "dot", "spmv",
+]
+
+_HERE = Path(__file__).resolve().parent
+_LIB = None
+
+#: every symbol include/yuzen_b200.h declares
+EXPORTED_SYMBOLS = (
+    "yz_last_error", "yz_solver_create", "yz_solver_destroy", "yz_solver_set_pattern",
+    "yz_solver_solve", "yz_solver_solve_device", "yz_solver_set_precision",
+    "yz_solver_memory", "yz_solver_set_memory", "yz_solver_levels", "yz_solver_level_info",
+    "yz_solver_level_copy", "yz_solver_last_timing", "yz_solver_launches", "yz_dot", "yz_spmv",
+)
+
+
+class YzError(RuntimeError):
+    """A non-zero status of the C ABI (-1 usage error, -2 CUDA error)."""
+
+
+def lib_path() -> Path:
+    return _HERE / "libyuzen_b200.so"
+
+
+class _Settings(ctypes.Structure):
+    _fields_ = [("precondition", ctypes.c_int), ("scaling", ctypes.c_int),
+                ("max_iteration", ctypes.c_int), ("epsilon", ctypes.c_double),
+                ("conc", ctypes.c_int)]
+
+
+_i32p = ctypes.POINTER(ctypes.c_int)
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+def lib():
+    """Load libyuzen_b200.so (built in-tree).  Raises if it was not built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    p = lib_path()
+    if not p.exists():
+        raise RuntimeError(f"{p} is not built: run `python -m yuzen_b200.build` "
+                           "(the library has no CPU fallback)")
+    L = ctypes.CDLL(str(p))
+    L.yz_last_error.restype = ctypes.c_char_p
+    L.yz_solver_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    L.yz_solver_destroy.argtypes = [ctypes.c_void_p]
+    L.yz_solver_set_pattern.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _i32p, _i32p, _i32p]
+    L.yz_solver_solve.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Settings), _f64p, _f64p, _f64p, _i32p, _f64p]
+    L.yz_solver_solve_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Settings), ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p, _i32p, _f64p]
+    L.yz_solver_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.yz_solver_memory.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_int]
+    L.yz_solver_set_memory.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_int]
+    L.yz_solver_levels.argtypes = [ctypes.c_void_p]
+    L.yz_solver_level_info.argtypes = [ctypes.c_void_p, ctypes.c_int, _i32p, _i32p, _i32p, _i32p]
+    L.yz_solver_level_copy.argtypes = [ctypes.c_void_p, ctypes.c_int, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p, _i32p]
+    L.yz_solver_last_timing.argtypes = [ctypes.c_void_p, _f64p, _f64p]
+    L.yz_solver_launches.argtypes = [ctypes.c_void_p]
+    L.yz_solver_launches.restype = ctypes.c_longlong
+    L.yz_dot.argtypes = [ctypes.c_int, _f64p, _f64p, _f64p]
+    L.yz_spmv.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
+    _LIB = L
+    return L
+
+
+def _check(status: int, what: str) -> int:
+    if status < 0:
+        msg = lib().yz_last_error().decode(errors="replace")
+        raise YzError(f"{what}: status {status}: {msg}")
+    return status
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(_i32p)
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(_f64p)
+
+
+class LinearSolverSettings:
+    """LinearSolverSettings (LinearSolverBackend.h:38-51)."""
+    tp_None, tp_Jacobi, tp_ILU = 0, 1, 2
+
+    def __init__(self, precondition: int = 2, scaling: bool = True, maxIteration: int = 100,
+                 epsilon: float = 1e-12, conc: bool = False):
+        self.precondition = precondition
+        self.scaling = scaling
+        self.maxIteration = maxIteration
+        self.epsilon = epsilon
+        self.conc = conc
+
+    def _c(self) -> _Settings:
+        return _Settings(int(self.precondition), int(bool(self.scaling)), int(self.maxIteration),
+                         float(self.epsilon), int(bool(self.conc)))
+
+
+class CrsPattern:
+    """The view of a CRS_Matrix a backend receives (CRS_Matrix.h:242-269):
+    row pointers, storage-order columns (diagonal first), the column-sorted
+    mirror and the permutation that gathers values into it."""
+
+    def __init__(self, rowptr, col, sorted_col=None, sorted_src=None):
+        self.rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+        self.col = np.ascontiguousarray(col, dtype=np.int32)
+        n = self.rowptr.size - 1
+        if sorted_col is None or sorted_src is None:
+            scol = np.empty_like(self.col)
+            ssrc = np.empty_like(self.col)
+            for i in range(n):
+                st, ed = self.rowptr[i], self.rowptr[i + 1]
+                order = np.argsort(self.col[st:ed], kind="stable")
+                scol[st:ed] = self.col[st:ed][order]
+                ssrc[st:ed] = st + order
+            sorted_col, sorted_src = scol, ssrc
+        self.sorted_col = np.ascontiguousarray(sorted_col, dtype=np.int32)
+        self.sorted_src = np.ascontiguousarray(sorted_src, dtype=np.int32)
+
+    @property
+    def n(self) -> int:
+        return self.rowptr.size - 1
+
+    @property
+    def nnz(self) -> int:
+        return int(self.rowptr[-1])
+
+
+class B200Backend:
+    """ILinearSolverBackend on the device (LinearSolverBackend.h:56-103).
+
+    Solve(settings, pattern, values, rhs, x) -> (ret, iter, resid), x updated
+    in place; ret 0 converged, 1 iteration limit, 2 breakdown / NaN."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        _check(lib().yz_solver_create(device, ctypes.byref(self._h)), "yz_solver_create")
+        self._pattern_key = None
+
+    def Name(self) -> str:
+        return "b200"
+
+    def Build(self, nRow: int, nonZero: int, nonZL: int = 0, nonZU: int = 0) -> None:
+        # storage is sized when the pattern is handed over (SetPattern)
+        self._n, self._nnz = nRow, nonZero
+
+    def SetPattern(self, pat: CrsPattern) -> None:
+        _check(lib().yz_solver_set_pattern(self._h, pat.n, pat.nnz, _ip(pat.rowptr), _ip(pat.sorted_col),
+                                           _ip(pat.sorted_src)), "yz_solver_set_pattern")
+        self._pattern_key = id(pat)
+
+    def Solve(self, s: LinearSolverSettings, pat: CrsPattern, values, rhs, x):
+        if self._pattern_key != id(pat):
+            self.SetPattern(pat)
+        values = np.ascontiguousarray(values, dtype=np.float64)
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        if x.dtype != np.float64 or not x.flags.c_contiguous:
+            raise ValueError("x must be a contiguous float64 array (it is updated in place)")
+        it = ctypes.c_int(0)
+        res = ctypes.c_double(0.0)
+        c = s._c()
+        ret = _check(lib().yz_solver_solve(self._h, ctypes.byref(c), _fp(values), _fp(rhs), _fp(x),
+                                           ctypes.byref(it), ctypes.byref(res)), "yz_solver_solve")
+        return ret, it.value, res.value
+
+    def SolveDevice(self, s: LinearSolverSettings, values_ptr: int, rhs_ptr: int, x_ptr: int):
+        it = ctypes.c_int(0)
+        res = ctypes.c_double(0.0)
+        c = s._c()
+        ret = _check(lib().yz_solver_solve_device(self._h, ctypes.byref(c), ctypes.c_void_p(values_ptr),
+                                                  ctypes.c_void_p(rhs_ptr), ctypes.c_void_p(x_ptr),
+                                                  ctypes.byref(it), ctypes.byref(res)), "yz_solver_solve_device")
+        return ret, it.value, res.value
+
+    def Memory(self) -> list:
+        buf = np.zeros(8, dtype=np.float64)
+        k = _check(lib().yz_solver_memory(self._h, _fp(buf), 8), "yz_solver_memory")
+        return buf[:k].tolist()
+
+    def SetMemory(self, m) -> None:
+        a = np.ascontiguousarray(m, dtype=np.float64)
+        _check(lib().yz_solver_set_memory(self._h, _fp(a), a.size), "yz_solver_set_memory")
+
+    def levels(self) -> list:
+        """The AMG hierarchy of the last AMG solve: one dict per level."""
+        L = lib()
+        out = []
+        nl = _check(L.yz_solver_levels(self._h), "yz_solver_levels")
+        for l in range(nl):
+            rows, nnza, nnzp, direct = (ctypes.c_int() for _ in range(4))
+            _check(L.yz_solver_level_info(self._h, l, ctypes.byref(rows), ctypes.byref(nnza),
+                                          ctypes.byref(nnzp), ctypes.byref(direct)), "level_info")
+            n, na, npn = rows.value, nnza.value, nnzp.value
+            d = {"rows": n, "nnz_a": na, "nnz_p": npn, "direct": bool(direct.value),
+                 "a_ptr": np.zeros(n + 1, np.int32), "a_col": np.zeros(max(na, 1), np.int32),
+                 "a_val": np.zeros(max(na, 1)), "p_ptr": np.zeros(n + 1, np.int32),
+                 "p_col": np.zeros(max(npn, 1), np.int32), "p_val": np.zeros(max(npn, 1)),
+                 "agg": np.full(n, -1, np.int32)}
+            _check(L.yz_solver_level_copy(self._h, l, _ip(d["a_ptr"]), _ip(d["a_col"]), _fp(d["a_val"]),
+                                          _ip(d["p_ptr"]), _ip(d["p_col"]), _fp(d["p_val"]), _ip(d["agg"])),
+                   "level_copy")
+            d["a_col"], d["a_val"] = d["a_col"][:na], d["a_val"][:na]
+            d["p_col"], d["p_val"] = d["p_col"][:npn], d["p_val"][:npn]
+            out.append(d)
+        return out
+
+    def last_timing(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(lib().yz_solver_last_timing(self._h, ctypes.byref(a), ctypes.byref(b)), "last_timing")
+        return a.value, b.value
+
+    def launches(self) -> int:
+        return int(lib().yz_solver_launches(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            lib().yz_solver_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def MakeLinearSolverBackend(name: str, inPlane: int = 2, device: int = 0) -> B200Backend:
+    """The factory entry for the name this library adds ("b200")."""
+    if name != "b200":
+        raise ValueError(f"this library provides the backend 'b200', not {name!r}")
+    return B200Backend(device)
+
+
+def dot(x, y) -> float:
+    """The deterministic dot product of the solve, on the device."""
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.ascontiguousarray(y, np.float64)
+    out = ctypes.c_double()
+    _check(lib().yz_dot(x.size, _fp(x), _fp(y), ctypes.byref(out)), "yz_dot")
+    return out.value
+
+
+def spmv(rowptr, col, val, x) -> np.ndarray:
+    """CRS_Matrix::MatVec on the device: y_i summed from 0.0 in stored order."""
+    rowptr = np.ascontiguousarray(rowptr, np.int32)
+    col = np.ascontiguousarray(col, np.int32)
+    val = np.ascontiguousarray(val, np.float64)
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.zeros(rowptr.size - 1)
+    _check(lib().yz_spmv(rowptr.size - 1, int(rowptr[-1]), _ip(rowptr), _ip(col), _fp(val), _fp(x), _fp(y)),
+           "yz_spmv")
+    return y

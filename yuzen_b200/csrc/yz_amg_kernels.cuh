@@ -1,0 +1,529 @@
+// yz_amg_kernels.cuh -- device kernels of the smoothed-aggregation AMG set-up
+// and V-cycle.  Every floating-point expression follows the oracle
+// (oracle/solver/yzo_solver.cpp) operation for operation; the file is compiled
+// with -fmad=false so that no product is fused into an addition.
+#pragma once
+
+#include "yz_common.cuh"
+
+namespace yz {
+
+enum : int { kOut = 0, kUndecided = 1, kIn = 2 };
+
+__device__ __forceinline__ uint32_t Hash32(uint32_t x)
+{
+	x ^= x >> 16; x *= 0x85ebca6bu;
+	x ^= x >> 13; x *= 0xc2b2ae35u;
+	x ^= x >> 16;
+	return x;
+}
+
+__device__ __forceinline__ unsigned long long PackKey(int state, int i)
+{
+	return ((unsigned long long)state << 62) |
+	       ((unsigned long long)(Hash32((uint32_t)i) & 0x3fffffffu) << 32) |
+	       (unsigned long long)(uint32_t)i;
+}
+
+//--------------------------------------------------------------------------
+//  ScaleRows + gather into the sorted mirror (LinearSolverBackend.cpp:227-252)
+//--------------------------------------------------------------------------
+__global__ void KScaleGather(int n, const int *__restrict__ rowptr, const int *__restrict__ ssrc,
+                             const double *__restrict__ values, const double *__restrict__ rhs, int scaling,
+                             double *__restrict__ val0, double *__restrict__ b)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		const int st = rowptr[i], ed = rowptr[i + 1];
+		const double d = scaling ? values[st] : 1.0;
+		if(!scaling || fabs(d) < 1.0e-30)
+		{
+			for(int k = st; k < ed; ++k) val0[k] = values[ssrc[k]];
+			b[i] = rhs[i];
+			continue;
+		}
+		const double inv = 1.0 / d;
+		for(int k = st; k < ed; ++k) val0[k] = values[ssrc[k]] * inv;
+		b[i] = rhs[i] * inv;
+	}
+}
+
+//--------------------------------------------------------------------------
+//  strength of connection, aggregation
+//--------------------------------------------------------------------------
+__global__ void KDiag(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                      const double *__restrict__ val, double *__restrict__ dia)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		double d = 0.0;
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k) if(col[k] == i) { d = val[k]; break; }
+		dia[i] = d;
+	}
+}
+
+__global__ void KStrength(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                          const double *__restrict__ val, const double *__restrict__ dia, double eps2,
+                          unsigned char *__restrict__ strong, int *__restrict__ icnt)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		const double e = eps2 * dia[i];
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k)
+		{
+			const int c = col[k];
+			const double v = val[k];
+			const bool s = (c != i) && (e * dia[c] < v * v);
+			strong[k] = s ? 1 : 0;
+			if(s) atomicAdd(&icnt[c], 1);
+		}
+	}
+}
+
+//  in-neighbours (rows that hold this one strongly); the order inside a list
+//  is free, every later use is a max or a min over it
+__global__ void KFillIn(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                        const unsigned char *__restrict__ strong, int *__restrict__ ifill, int *__restrict__ icol)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k)
+			if(strong[k]) icol[atomicAdd(&ifill[col[k]], 1)] = i;
+}
+
+__global__ void KMisInit(int n, const int *__restrict__ ptr, const unsigned char *__restrict__ strong,
+                         const int *__restrict__ iptr, int *__restrict__ state, unsigned char *__restrict__ iso)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		bool any = iptr[i + 1] > iptr[i];
+		for(int k = ptr[i]; k < ptr[i + 1] && !any; ++k) any = strong[k] != 0;
+		iso[i] = any ? 0 : 1;
+		state[i] = any ? kUndecided : kOut;
+	}
+}
+
+__global__ void KMisPack(int n, const int *__restrict__ state, unsigned long long *__restrict__ T0, int *__restrict__ undecided)
+{
+	int cnt = 0;
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		T0[i] = PackKey(state[i], i);
+		cnt += (state[i] == kUndecided);
+	}
+	for(int off = 16; off >= 1; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+	if((threadIdx.x & 31) == 0 && cnt) atomicAdd(undecided, cnt);
+}
+
+__global__ void KMisMax(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                        const unsigned char *__restrict__ strong, const int *__restrict__ iptr,
+                        const int *__restrict__ icol, const unsigned long long *__restrict__ Tin,
+                        unsigned long long *__restrict__ Tout, const int *__restrict__ undecided)
+{
+	if(*undecided == 0) return;
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		unsigned long long m = Tin[i];
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k) if(strong[k]) { const unsigned long long u = Tin[col[k]]; m = u > m ? u : m; }
+		for(int k = iptr[i]; k < iptr[i + 1]; ++k) { const unsigned long long u = Tin[icol[k]]; m = u > m ? u : m; }
+		Tout[i] = m;
+	}
+}
+
+__global__ void KMisUpdate(int n, int *__restrict__ state, const unsigned long long *__restrict__ T2, const int *__restrict__ undecided)
+{
+	if(*undecided == 0) return;
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		if(state[i] != kUndecided) continue;
+		const unsigned long long t = T2[i];
+		if((int)(uint32_t)(t & 0xffffffffull) == i) state[i] = kIn;
+		else if((int)(t >> 62) == kIn) state[i] = kOut;
+	}
+}
+
+__global__ void KRootFlags(int n, const int *__restrict__ state, int *__restrict__ flag)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) flag[i] = state[i] == kIn ? 1 : 0;
+}
+
+__global__ void KAssignFirst(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                             const unsigned char *__restrict__ strong, const int *__restrict__ iptr,
+                             const int *__restrict__ icol, const int *__restrict__ state,
+                             const unsigned char *__restrict__ iso, const int *__restrict__ rootId, int *__restrict__ first)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		if(state[i] == kIn) { first[i] = rootId[i]; continue; }
+		if(iso[i]) { first[i] = -1; continue; }
+		int best = -1;
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k)
+			if(strong[k]) { const int j = col[k]; if(state[j] == kIn && (best < 0 || rootId[j] < best)) best = rootId[j]; }
+		for(int k = iptr[i]; k < iptr[i + 1]; ++k)
+		{ const int j = icol[k]; if(state[j] == kIn && (best < 0 || rootId[j] < best)) best = rootId[j]; }
+		first[i] = best;
+	}
+}
+
+__global__ void KAssignSecond(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                              const unsigned char *__restrict__ strong, const int *__restrict__ iptr,
+                              const int *__restrict__ icol, const unsigned char *__restrict__ iso,
+                              const int *__restrict__ first, int *__restrict__ agg)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		if(first[i] >= 0 || iso[i]) { agg[i] = first[i]; continue; }
+		int best = -1;
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k)
+			if(strong[k]) { const int f = first[col[k]]; if(f >= 0 && (best < 0 || f < best)) best = f; }
+		for(int k = iptr[i]; k < iptr[i + 1]; ++k)
+		{ const int f = first[icol[k]]; if(f >= 0 && (best < 0 || f < best)) best = f; }
+		agg[i] = best;
+	}
+}
+
+__global__ void KSpai0(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                       const double *__restrict__ val, double *__restrict__ M)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		double num = 0.0, den = 0.0;
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k)
+		{
+			const double v = val[k];
+			den = den + v * v;
+			if(col[k] == i) num = num + v;
+		}
+		M[i] = (1.0 / den) * num;
+	}
+}
+
+//  damped Jacobi as a preconditioner: m_i = 0.72 * (1 / a_ii)
+__global__ void KDampedJacobi(int n, const double *__restrict__ dia, double *__restrict__ M)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) M[i] = 0.72 * (1.0 / dia[i]);
+}
+
+//--------------------------------------------------------------------------
+//  prolongation  P = (I - omega D_f^-1 A_f) P_tent
+//--------------------------------------------------------------------------
+constexpr int kRowCap = 256;	// distinct aggregates / columns a row may gather
+
+__global__ void KPCount(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                        const unsigned char *__restrict__ strong, const int *__restrict__ agg,
+                        int *__restrict__ cnt, int *__restrict__ overflow)
+{
+	int lc[kRowCap];
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		int m = 0;
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k)
+		{
+			const int c = col[k];
+			if(c != i && !strong[k]) continue;
+			const int cp = agg[c];
+			if(cp < 0) continue;
+			int q = 0;
+			while(q < m && lc[q] != cp) ++q;
+			if(q == m) { if(m == kRowCap) { atomicExch(overflow, 1); break; } lc[m++] = cp; }
+		}
+		cnt[i] = m;
+	}
+}
+
+__global__ void KPFill(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                       const double *__restrict__ val, const unsigned char *__restrict__ strong,
+                       const int *__restrict__ agg, const int *__restrict__ pptr,
+                       int *__restrict__ pcol, double *__restrict__ pval)
+{
+	const double omega = 2.0 / 3.0;
+	int lc[kRowCap];
+	double lv[kRowCap];
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		double dia = 0.0;
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k)
+			if(col[k] == i || !strong[k]) dia = dia + val[k];
+		const double ds = (-omega) * (1.0 / dia);
+		int m = 0;
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k)
+		{
+			const int c = col[k];
+			if(c != i && !strong[k]) continue;
+			const int cp = agg[c];
+			if(cp < 0) continue;
+			const double va = (c == i) ? (1.0 - omega) : ds * val[k];
+			int q = 0;
+			while(q < m && lc[q] != cp) ++q;
+			if(q == m) { if(m == kRowCap) break; lc[m] = cp; lv[m] = 0.0; ++m; }
+			lv[q] = lv[q] + va;
+		}
+		//  insertion sort by column (columns are distinct)
+		for(int a = 1; a < m; ++a)
+		{
+			const int kc = lc[a]; const double kv = lv[a];
+			int b = a - 1;
+			while(b >= 0 && lc[b] > kc) { lc[b + 1] = lc[b]; lv[b + 1] = lv[b]; --b; }
+			lc[b + 1] = kc; lv[b + 1] = kv;
+		}
+		const int o = pptr[i];
+		for(int q = 0; q < m; ++q) { pcol[o + q] = lc[q]; pval[o + q] = lv[q]; }
+	}
+}
+
+//  R = P^T: counts per column, atomic fill, then each row sorted by fine row
+__global__ void KColCount(int nnz, const int *__restrict__ pcol, int *__restrict__ cnt)
+{
+	for(int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += gridDim.x * blockDim.x) atomicAdd(&cnt[pcol[k]], 1);
+}
+
+__global__ void KTransposeFill(int n, const int *__restrict__ pptr, const int *__restrict__ pcol,
+                               const double *__restrict__ pval, int *__restrict__ fill,
+                               int *__restrict__ rcol, double *__restrict__ rval)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+		for(int k = pptr[i]; k < pptr[i + 1]; ++k)
+		{
+			const int d = atomicAdd(&fill[pcol[k]], 1);
+			rcol[d] = i; rval[d] = pval[k];
+		}
+}
+
+__global__ void KRowSort(int n, const int *__restrict__ ptr, int *__restrict__ col, double *__restrict__ val)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		const int st = ptr[i], ed = ptr[i + 1];
+		for(int a = st + 1; a < ed; ++a)
+		{
+			const int kc = col[a]; const double kv = val[a];
+			int b = a - 1;
+			while(b >= st && col[b] > kc) { col[b + 1] = col[b]; val[b + 1] = val[b]; --b; }
+			col[b + 1] = kc; val[b + 1] = kv;
+		}
+	}
+}
+
+//--------------------------------------------------------------------------
+//  sparse product C = X Y with the oracle's summation order: per output
+//  entry from 0.0, contributions in the order of X's row (ascending k)
+//--------------------------------------------------------------------------
+__global__ void KGemmCount(int nx, const int *__restrict__ xptr, const int *__restrict__ xcol,
+                           const int *__restrict__ yptr, const int *__restrict__ ycol,
+                           int *__restrict__ cnt, int *__restrict__ overflow)
+{
+	int lc[kRowCap];
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x)
+	{
+		int m = 0;
+		bool over = false;
+		for(int kx = xptr[i]; kx < xptr[i + 1] && !over; ++kx)
+		{
+			const int k = xcol[kx];
+			for(int ky = yptr[k]; ky < yptr[k + 1]; ++ky)
+			{
+				const int j = ycol[ky];
+				int lo = 0, hi = m;
+				while(lo < hi) { const int mid = (lo + hi) >> 1; if(lc[mid] < j) lo = mid + 1; else hi = mid; }
+				if(lo < m && lc[lo] == j) continue;
+				if(m == kRowCap) { over = true; break; }
+				for(int q = m; q > lo; --q) lc[q] = lc[q - 1];
+				lc[lo] = j; ++m;
+			}
+		}
+		if(over) atomicExch(overflow, 1);
+		cnt[i] = m;
+	}
+}
+
+__global__ void KGemmFill(int nx, const int *__restrict__ xptr, const int *__restrict__ xcol,
+                          const double *__restrict__ xval, const int *__restrict__ yptr,
+                          const int *__restrict__ ycol, const double *__restrict__ yval,
+                          const int *__restrict__ cptr, int *__restrict__ ccol, double *__restrict__ cval)
+{
+	int lc[kRowCap];
+	double lv[kRowCap];
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x)
+	{
+		int m = 0;
+		for(int kx = xptr[i]; kx < xptr[i + 1]; ++kx)
+		{
+			const int k = xcol[kx];
+			const double xv = xval[kx];
+			for(int ky = yptr[k]; ky < yptr[k + 1]; ++ky)
+			{
+				const int j = ycol[ky];
+				int lo = 0, hi = m;
+				while(lo < hi) { const int mid = (lo + hi) >> 1; if(lc[mid] < j) lo = mid + 1; else hi = mid; }
+				if(!(lo < m && lc[lo] == j))
+				{
+					if(m == kRowCap) continue;
+					for(int q = m; q > lo; --q) { lc[q] = lc[q - 1]; lv[q] = lv[q - 1]; }
+					lc[lo] = j; lv[lo] = 0.0; ++m;
+				}
+				lv[lo] = lv[lo] + xv * yval[ky];
+			}
+		}
+		const int o = cptr[i];
+		for(int q = 0; q < m; ++q) { ccol[o + q] = lc[q]; cval[o + q] = lv[q]; }
+	}
+}
+
+//--------------------------------------------------------------------------
+//  Gauss-Jordan inverse of the coarsest level on [A | I], one launch per
+//  pivot step, double-buffered (M_in -> M_out).  Every block finds the pivot
+//  of column k itself (first row of largest |a|, rows k..n-1).
+//--------------------------------------------------------------------------
+__global__ void KGjInit(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                        const double *__restrict__ val, double *__restrict__ M)
+{
+	const int w = 2 * n;
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k) M[(size_t)i * w + col[k]] = val[k];
+		M[(size_t)i * w + n + i] = 1.0;
+	}
+}
+
+__global__ void KGjStep(int n, int k, const double *__restrict__ Min, double *__restrict__ Mout)
+{
+	const int w = 2 * n;
+	__shared__ double bv[256];
+	__shared__ int bi[256];
+	__shared__ int pivRow;
+	{
+		double best = -1.0; int idx = n;
+		for(int i = k + threadIdx.x; i < n; i += blockDim.x)
+		{
+			const double a = fabs(Min[(size_t)i * w + k]);
+			if(a > best || (a == best && i < idx)) { best = a; idx = i; }
+		}
+		bv[threadIdx.x] = best; bi[threadIdx.x] = idx;
+		__syncthreads();
+		for(int off = blockDim.x / 2; off >= 1; off >>= 1)
+		{
+			if((int)threadIdx.x < off)
+			{
+				const double a = bv[threadIdx.x + off]; const int ia = bi[threadIdx.x + off];
+				if(a > bv[threadIdx.x] || (a == bv[threadIdx.x] && ia < bi[threadIdx.x])) { bv[threadIdx.x] = a; bi[threadIdx.x] = ia; }
+			}
+			__syncthreads();
+		}
+		if(threadIdx.x == 0)
+		{
+			//  the sequential rule: rows after k replace k only when strictly larger
+			const double akk = fabs(Min[(size_t)k * w + k]);
+			pivRow = (bv[0] > akk) ? bi[0] : k;
+		}
+		__syncthreads();
+	}
+	const int p = pivRow;
+	const double piv = Min[(size_t)p * w + k];
+	const int span = w - k;				// columns k .. 2n-1
+	const long long total = (long long)n * span;
+	for(long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x)
+	{
+		const int i = (int)(e / span);
+		const int j = k + (int)(e % span);
+		const double rowK = Min[(size_t)p * w + j] / piv;		// the scaled pivot row
+		double out;
+		if(i == k) out = rowK;
+		else
+		{
+			const int src = (i == p) ? k : i;
+			const double f = Min[(size_t)src * w + k];
+			const double mij = Min[(size_t)src * w + j];
+			out = (f == 0.0) ? mij : mij - f * rowK;
+		}
+		Mout[(size_t)i * w + j] = out;
+	}
+}
+
+__global__ void KGjExtract(int n, const double *__restrict__ M, double *__restrict__ invCm)
+{
+	const int w = 2 * n;
+	const long long total = (long long)n * n;
+	for(long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x)
+	{
+		const int i = (int)(e / n), j = (int)(e % n);
+		invCm[(size_t)j * n + i] = M[(size_t)i * w + n + j];
+	}
+}
+
+//--------------------------------------------------------------------------
+//  V-cycle
+//--------------------------------------------------------------------------
+//  x = m .* f, t = f - A x (x of the neighbours recomputed as m_j * f_j)
+__global__ void KPreSmoothResidual(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                                   const double *__restrict__ val, const double *__restrict__ M,
+                                   const double *__restrict__ f, double *__restrict__ x, double *__restrict__ t)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		double s = 0.0;
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k) { const int c = col[k]; s = s + val[k] * (M[c] * f[c]); }
+		x[i] = M[i] * f[i];
+		t[i] = f[i] - s;
+	}
+}
+
+__global__ void KPreSmooth(int n, const double *__restrict__ M, const double *__restrict__ f, double *__restrict__ x)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = M[i] * f[i];
+}
+
+//  y = A x (from 0.0, stored order)
+__global__ void KSpmv(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                      const double *__restrict__ val, const double *__restrict__ x, double *__restrict__ y)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		double s = 0.0;
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k) s = s + val[k] * x[col[k]];
+		y[i] = s;
+	}
+}
+
+//  xout = x + P xc
+__global__ void KProlong(int n, const int *__restrict__ pptr, const int *__restrict__ pcol,
+                         const double *__restrict__ pval, const double *__restrict__ xc,
+                         const double *__restrict__ x, double *__restrict__ xout)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		double s = 0.0;
+		for(int k = pptr[i]; k < pptr[i + 1]; ++k) s = s + pval[k] * xc[pcol[k]];
+		xout[i] = x[i] + s;
+	}
+}
+
+//  xout = x + m .* (f - A x)
+__global__ void KPostSmooth(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                            const double *__restrict__ val, const double *__restrict__ M,
+                            const double *__restrict__ f, const double *__restrict__ x, double *__restrict__ xout)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		double s = 0.0;
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k) s = s + val[k] * x[col[k]];
+		const double t = f[i] - s;
+		xout[i] = x[i] + M[i] * t;
+	}
+}
+
+//  x = inv f, inv stored column-major; summed over j from 0.0
+__global__ void KDenseMV(int n, const double *__restrict__ invCm, const double *__restrict__ f, double *__restrict__ x)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		double s = 0.0;
+		for(int j = 0; j < n; ++j) s = s + invCm[(size_t)j * n + i] * f[j];
+		x[i] = s;
+	}
+}
+
+__global__ void KDiagApply(int n, const double *__restrict__ M, const double *__restrict__ r, double *__restrict__ z)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] = M[i] * r[i];
+}
+
+} // namespace yz

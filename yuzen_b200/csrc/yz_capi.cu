@@ -1,0 +1,157 @@
+// yz_capi.cu -- the extern "C" entry points of include/yuzen_b200.h.
+// Every call catches what the C++ side throws and turns it into a status.
+#include "yz_solver_impl.h"
+
+struct yz_solver
+{
+	std::unique_ptr<yz::Solver> s;
+	int precision = YZ_PREC_FP64;
+};
+
+namespace {
+template<class F> int Guard(F &&f)
+{
+	try { return f(); }
+	catch(const yz::UsageError &e) { yz::SetLastError(e.what()); return -1; }
+	catch(const yz::CudaError &e) { yz::SetLastError(e.what()); return -2; }
+	catch(const std::exception &e) { yz::SetLastError(e.what()); return -2; }
+	catch(...) { yz::SetLastError("unknown error"); return -2; }
+}
+}
+
+extern "C" {
+
+const char *yz_last_error(void) { return yz::LastError(); }
+
+int yz_solver_create(int device, yz_solver **out)
+{
+	return Guard([&] {
+		if(!out) throw yz::UsageError("yz_solver_create: out is null");
+		int count = 0;
+		yz::Check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+		if(device < 0 || device >= count) throw yz::UsageError("yz_solver_create: no such CUDA device");
+		yz_solver *h = new yz_solver();
+		h->s.reset(new yz::Solver(device));
+		*out = h;
+		return 0;
+	});
+}
+
+int yz_solver_destroy(yz_solver *s)
+{
+	return Guard([&] { delete s; return 0; });
+}
+
+int yz_solver_set_pattern(yz_solver *s, int n, int nnz, const int *rowptr, const int *scol, const int *ssrc)
+{
+	return Guard([&] {
+		if(!s || !rowptr || !scol || !ssrc) throw yz::UsageError("yz_solver_set_pattern: null argument");
+		s->s->SetPattern(n, nnz, rowptr, scol, ssrc);
+		return 0;
+	});
+}
+
+int yz_solver_solve(yz_solver *s, const yz_settings *set, const double *values, const double *rhs, double *x,
+                    int *iter, double *resid)
+{
+	return Guard([&] {
+		if(!s || !set || !values || !rhs || !x || !iter || !resid) throw yz::UsageError("yz_solver_solve: null argument");
+		return s->s->SolveHost(*set, values, rhs, x, *iter, *resid);
+	});
+}
+
+int yz_solver_solve_device(yz_solver *s, const yz_settings *set, const double *dv, const double *dr, double *dx,
+                           int *iter, double *resid)
+{
+	return Guard([&] {
+		if(!s || !set || !dv || !dr || !dx || !iter || !resid) throw yz::UsageError("yz_solver_solve_device: null argument");
+		return s->s->Solve(*set, dv, dr, dx, *iter, *resid);
+	});
+}
+
+int yz_solver_set_precision(yz_solver *s, int precision)
+{
+	return Guard([&] {
+		if(!s) throw yz::UsageError("yz_solver_set_precision: null solver");
+		if(precision != YZ_PREC_FP64) throw yz::UsageError("yz_solver_set_precision: only YZ_PREC_FP64 is built");
+		s->precision = precision;
+		return 0;
+	});
+}
+
+int yz_solver_memory(const yz_solver *s, double *out, int cap)
+{
+	return Guard([&] {
+		if(!s || (!out && cap > 0)) throw yz::UsageError("yz_solver_memory: null argument");
+		const std::vector<double> m = s->s->Memory();
+		for(int i = 0; i < (int)m.size() && i < cap; ++i) out[i] = m[(size_t)i];
+		return (int)m.size();
+	});
+}
+
+int yz_solver_set_memory(yz_solver *s, const double *m, int len)
+{
+	return Guard([&] {
+		if(!s || (!m && len > 0)) throw yz::UsageError("yz_solver_set_memory: null argument");
+		s->s->SetMemory(m, len);
+		return 0;
+	});
+}
+
+int yz_solver_levels(const yz_solver *s)
+{
+	return Guard([&] {
+		if(!s) throw yz::UsageError("yz_solver_levels: null solver");
+		return s->s->LevelCount();
+	});
+}
+
+int yz_solver_level_info(const yz_solver *s, int level, int *rows, int *nnz_a, int *nnz_p, int *direct)
+{
+	return Guard([&] {
+		if(!s) throw yz::UsageError("yz_solver_level_info: null solver");
+		s->s->LevelInfo(level, rows, nnz_a, nnz_p, direct);
+		return 0;
+	});
+}
+
+int yz_solver_level_copy(const yz_solver *s, int level, int *a_ptr, int *a_col, double *a_val, int *p_ptr, int *p_col,
+                         double *p_val, int *agg)
+{
+	return Guard([&] {
+		if(!s) throw yz::UsageError("yz_solver_level_copy: null solver");
+		const_cast<yz_solver *>(s)->s->LevelCopy(level, a_ptr, a_col, a_val, p_ptr, p_col, p_val, agg);
+		return 0;
+	});
+}
+
+int yz_solver_last_timing(const yz_solver *s, double *setup_ms, double *iterate_ms)
+{
+	return Guard([&] {
+		if(!s) throw yz::UsageError("yz_solver_last_timing: null solver");
+		s->s->Timing(setup_ms, iterate_ms);
+		return 0;
+	});
+}
+
+long long yz_solver_launches(const yz_solver *s) { return s ? s->s->Launches() : -1; }
+
+int yz_dot(int n, const double *x, const double *y, double *out)
+{
+	return Guard([&] {
+		if(n < 0 || (n > 0 && (!x || !y)) || !out) throw yz::UsageError("yz_dot: bad argument");
+		*out = yz::DeviceDot(n, x, y);
+		return 0;
+	});
+}
+
+int yz_spmv(int n, int nnz, const int *rowptr, const int *col, const double *val, const double *x, double *y)
+{
+	return Guard([&] {
+		if(n <= 0 || nnz < 0 || !rowptr || !col || !val || !x || !y) throw yz::UsageError("yz_spmv: bad argument");
+		yz::DeviceSpmv(n, nnz, rowptr, col, val, x, y);
+		return 0;
+	});
+}
+
+} // extern "C"

@@ -1,0 +1,191 @@
+// yz_common.cuh -- shared host/device utilities of the B200 implicit-step library.
+//
+// Built for sm_100a only.  The FP64 parity kernels are compiled with
+// -fmad=false so that every a*b+c rounds twice, as the reference's host code
+// does under -ffp-contract=off (CMakeLists.txt:33-46).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace yz {
+
+//--------------------------------------------------------------------------
+//  errors and launch accounting
+//--------------------------------------------------------------------------
+struct CudaError : std::runtime_error
+{
+	explicit CudaError(const std::string &m) : std::runtime_error(m) {}
+};
+struct UsageError : std::runtime_error
+{
+	explicit UsageError(const std::string &m) : std::runtime_error(m) {}
+};
+
+inline void Check(cudaError_t e, const char *what)
+{
+	if(e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define YZ_CUDA(call) ::yz::Check((call), #call)
+
+//  Every kernel launch of the library goes through YZ_LAUNCH, which counts it.
+extern std::atomic<long long> g_launches;
+
+#define YZ_LAUNCH(kernel, grid, block, smem, stream, ...)                         \
+	do {                                                                          \
+		kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);               \
+		::yz::g_launches.fetch_add(1, std::memory_order_relaxed);                 \
+		::yz::Check(cudaGetLastError(), #kernel);                                 \
+	} while(0)
+
+void SetLastError(const std::string &m);
+
+//--------------------------------------------------------------------------
+//  device buffer (grows, never shrinks; no allocation when large enough)
+//--------------------------------------------------------------------------
+template<class T>
+struct DBuf
+{
+	T *p = nullptr;
+	size_t cap = 0;
+	DBuf() = default;
+	DBuf(const DBuf &) = delete;
+	DBuf &operator=(const DBuf &) = delete;
+	~DBuf() { if(p) cudaFree(p); }
+	T *get() const { return p; }
+	void reserve(size_t n)
+	{
+		if(n <= cap) return;
+		if(p) { cudaFree(p); p = nullptr; cap = 0; }
+		size_t want = n < 16 ? 16 : n;
+		YZ_CUDA(cudaMalloc(&p, want * sizeof(T)));
+		cap = want;
+	}
+	void upload(const T *h, size_t n, cudaStream_t st)
+	{
+		reserve(n);
+		if(n) YZ_CUDA(cudaMemcpyAsync(p, h, n * sizeof(T), cudaMemcpyHostToDevice, st));
+	}
+	void download(T *h, size_t n, cudaStream_t st) const
+	{
+		if(n) YZ_CUDA(cudaMemcpyAsync(h, p, n * sizeof(T), cudaMemcpyDeviceToHost, st));
+	}
+};
+
+//--------------------------------------------------------------------------
+//  the deterministic reduction tree (the oracle's DetSum, yzo_solver.cpp):
+//  chunk b of 4096 elements per block of 256 threads, thread t sums elements
+//  b*4096 + k*256 + t (k = 0..15) from 0.0, pairwise fold over the block,
+//  the chunk sums folded the same way by the block that finishes last.
+//--------------------------------------------------------------------------
+constexpr int kRT = 256;
+constexpr int kRK = 16;
+constexpr int kRChunk = kRT * kRK;
+
+inline int RedBlocks(int n) { const int nb = (n + kRChunk - 1) / kRChunk; return nb > 0 ? nb : 1; }
+
+//  Fold Q values per thread over a block of 256 (same order as Tree256).
+//  sh: Q*256 doubles of shared memory.  Result valid in thread 0.
+template<int Q>
+__device__ __forceinline__ void BlockTree(double (&a)[Q], double *sh)
+{
+	const int t = threadIdx.x;
+#pragma unroll
+	for(int q = 0; q < Q; ++q) sh[q * kRT + t] = a[q];
+	__syncthreads();
+#pragma unroll
+	for(int off = kRT / 2; off >= 32; off >>= 1)
+	{
+		if(t < off)
+		{
+#pragma unroll
+			for(int q = 0; q < Q; ++q) sh[q * kRT + t] = sh[q * kRT + t] + sh[q * kRT + t + off];
+		}
+		__syncthreads();
+	}
+	if(t < 32)
+	{
+#pragma unroll
+		for(int q = 0; q < Q; ++q)
+		{
+			double v = sh[q * kRT + t];
+#pragma unroll
+			for(int off = 16; off >= 1; off >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, off);
+			a[q] = v;
+		}
+	}
+}
+
+//  Reduction scratch: Q partial arrays of `blocks` doubles and a counter.
+struct RedScratch
+{
+	double *part;          // [Q][maxBlocks]
+	unsigned int *counter; // one per reduction site
+	int maxBlocks;
+};
+
+//  Called by every block after its threads hold their per-thread sums a[q]:
+//  writes the block's partials; the last block to arrive folds them all and
+//  returns true with the totals in tot[q] (valid in every thread of it).
+template<int Q>
+__device__ __forceinline__ bool GridFold(double (&a)[Q], double *sh, const RedScratch rs, double (&tot)[Q])
+{
+	__shared__ bool amLast;
+	BlockTree<Q>(a, sh);
+	const int t = threadIdx.x;
+	if(t == 0)
+	{
+#pragma unroll
+		for(int q = 0; q < Q; ++q) rs.part[q * rs.maxBlocks + blockIdx.x] = a[q];
+		__threadfence();
+		const unsigned prev = atomicAdd(rs.counter, 1u);
+		amLast = (prev == gridDim.x - 1);
+	}
+	__syncthreads();
+	if(!amLast) return false;
+	__threadfence();
+	double b[Q];
+#pragma unroll
+	for(int q = 0; q < Q; ++q)
+	{
+		double s = 0.0;
+		for(int j = t; j < (int)gridDim.x; j += kRT) s = s + __ldcg(&rs.part[q * rs.maxBlocks + j]);
+		b[q] = s;
+	}
+	__syncthreads();
+	BlockTree<Q>(b, sh);
+	__shared__ double bc[Q];
+	if(t == 0)
+	{
+#pragma unroll
+		for(int q = 0; q < Q; ++q) bc[q] = b[q];
+		*rs.counter = 0u;
+	}
+	__syncthreads();
+#pragma unroll
+	for(int q = 0; q < Q; ++q) tot[q] = bc[q];
+	return true;
+}
+
+//--------------------------------------------------------------------------
+//  exclusive scan of n ints into out[0..n] (out[n] = total); integer, so
+//  the order of the additions does not matter.  Scratch: ScanScratchSize(n).
+//--------------------------------------------------------------------------
+size_t ScanScratchSize(int n);
+void ScanExclusive(const int *in, int *out, int n, int *scratch, cudaStream_t st);
+
+//  Grid size for a grid-stride kernel over n items.
+inline int GridFor(long long n, int block, int cap = 148 * 16)
+{
+	long long g = (n + block - 1) / block;
+	if(g < 1) g = 1;
+	if(g > cap) g = cap;
+	return (int)g;
+}
+
+} // namespace yz

@@ -1,0 +1,643 @@
+// yz_solver.cu -- the linear solve of the implicit step on the device: the
+// drop-in for ILinearSolverBackend::Solve (LinearSolverBackend.h:74-88).
+//
+// The flow of one solve follows AmgclBackend::Solve
+// (LinearSolverBackend.cpp:539-728): row scaling into the sorted mirror,
+// SPAI0 tried first on a concentration solve (TryBackoff, :262-270), then
+// BiCGStab preconditioned by SA-AMG(SPAI0) rebuilt for every solve (ILU) or
+// by damped Jacobi (None, Jacobi), coarse_enough 500 above 3000 rows (:660-675),
+// a breakdown answered by the residual check of :681-713.
+#include "yz_amg_kernels.cuh"
+#include "yz_solver_impl.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace yz {
+
+//==========================================================================
+//  Krylov kernels: element-wise updates fused with the dot products they
+//  feed, all on the chunk mapping of the reduction tree (block b, thread t:
+//  elements b*4096 + k*256 + t).  Scalars live in device memory (Scal).
+//==========================================================================
+#define YZ_CHUNK_LOOP(i)                                                          \
+	for(int kk_ = 0, i = blockIdx.x * kRChunk + threadIdx.x; kk_ < kRK; ++kk_, i += kRT)
+
+//  r = b - A x;  bb = b.b, rr = r.r, rho0 = r.r (rh = r)
+__global__ void KBInit(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                       const double *__restrict__ val, const double *__restrict__ b,
+                       const double *__restrict__ x, double *__restrict__ r, double *__restrict__ rh,
+                       RedScratch rs, Scal *sc)
+{
+	__shared__ double sh[2 * kRT];
+	double a[2] = {0.0, 0.0};
+	YZ_CHUNK_LOOP(i)
+	{
+		if(i >= n) break;
+		double s = 0.0;
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k) s = s + val[k] * x[col[k]];
+		const double ri = b[i] - s;
+		r[i] = ri; rh[i] = ri;
+		a[0] = a[0] + b[i] * b[i];
+		a[1] = a[1] + ri * ri;
+	}
+	double tot[2];
+	if(GridFold<2>(a, sh, rs, tot) && threadIdx.x == 0)
+	{
+		sc->normb = sqrt(tot[0]);
+		sc->res = sqrt(tot[1]);
+		sc->rho = tot[1];
+	}
+}
+
+//  p = r (first pass) or p = r + beta (p - omega v)
+__global__ void KPUpdate(int n, int first, const double *__restrict__ r, const double *__restrict__ v,
+                         double *__restrict__ p, const Scal *sc)
+{
+	if(first)
+	{
+		for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = r[i];
+		return;
+	}
+	const double omega = sc->omega;
+	const double beta = (sc->rho / sc->rhoPrev) * (sc->alpha / omega);
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+		p[i] = r[i] + beta * (p[i] - omega * v[i]);
+}
+
+//  v = A ph; alpha = rho / (rh . v)
+__global__ void KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                           const double *__restrict__ val, const double *__restrict__ ph,
+                           const double *__restrict__ rh, double *__restrict__ v, RedScratch rs, Scal *sc)
+{
+	__shared__ double sh[kRT];
+	double a[1] = {0.0};
+	YZ_CHUNK_LOOP(i)
+	{
+		if(i >= n) break;
+		double s = 0.0;
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k) s = s + val[k] * ph[col[k]];
+		v[i] = s;
+		a[0] = a[0] + rh[i] * s;
+	}
+	double tot[1];
+	if(GridFold<1>(a, sh, rs, tot) && threadIdx.x == 0) sc->alpha = sc->rho / tot[0];
+}
+
+//  s = r - alpha v; res = |s|
+__global__ void KSUpdate(int n, const double *__restrict__ r, const double *__restrict__ v,
+                         double *__restrict__ s, RedScratch rs, Scal *sc)
+{
+	__shared__ double sh[kRT];
+	const double alpha = sc->alpha;
+	double a[1] = {0.0};
+	YZ_CHUNK_LOOP(i)
+	{
+		if(i >= n) break;
+		const double si = r[i] - alpha * v[i];
+		s[i] = si;
+		a[0] = a[0] + si * si;
+	}
+	double tot[1];
+	if(GridFold<1>(a, sh, rs, tot) && threadIdx.x == 0) sc->res = sqrt(tot[0]);
+}
+
+//  x = x + alpha ph  (the half-step exit)
+__global__ void KXHalf(int n, const double *__restrict__ ph, double *__restrict__ x, const Scal *sc)
+{
+	const double alpha = sc->alpha;
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = x[i] + alpha * ph[i];
+}
+
+//  t = A sh; omega = (t . s) / (t . t)
+__global__ void KSpmvOmega(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                           const double *__restrict__ val, const double *__restrict__ sh_,
+                           const double *__restrict__ s, double *__restrict__ t, RedScratch rs, Scal *sc)
+{
+	__shared__ double sh[2 * kRT];
+	double a[2] = {0.0, 0.0};
+	YZ_CHUNK_LOOP(i)
+	{
+		if(i >= n) break;
+		double u = 0.0;
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k) u = u + val[k] * sh_[col[k]];
+		t[i] = u;
+		a[0] = a[0] + u * u;
+		a[1] = a[1] + u * s[i];
+	}
+	double tot[2];
+	if(GridFold<2>(a, sh, rs, tot) && threadIdx.x == 0) sc->omega = tot[1] / tot[0];
+}
+
+//  x = (x + alpha ph) + omega sh; r = s - omega t; res = |r|; next rho = rh . r
+__global__ void KXRUpdate(int n, const double *__restrict__ ph, const double *__restrict__ shat,
+                          const double *__restrict__ s, const double *__restrict__ t,
+                          const double *__restrict__ rh, double *__restrict__ x, double *__restrict__ r,
+                          RedScratch rs, Scal *sc)
+{
+	__shared__ double sh[2 * kRT];
+	const double alpha = sc->alpha, omega = sc->omega;
+	double a[2] = {0.0, 0.0};
+	YZ_CHUNK_LOOP(i)
+	{
+		if(i >= n) break;
+		x[i] = (x[i] + alpha * ph[i]) + omega * shat[i];
+		const double ri = s[i] - omega * t[i];
+		r[i] = ri;
+		a[0] = a[0] + ri * ri;
+		a[1] = a[1] + rh[i] * ri;
+	}
+	double tot[2];
+	if(GridFold<2>(a, sh, rs, tot) && threadIdx.x == 0)
+	{
+		sc->res = sqrt(tot[0]);
+		sc->rhoPrev = sc->rho;
+		sc->rho = tot[1];
+	}
+}
+
+__global__ void KFill(int n, double v, double *__restrict__ x)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = v;
+}
+
+//  the deterministic dot product on its own (for the parity tests)
+__global__ void KDot(int n, const double *__restrict__ x, const double *__restrict__ y, RedScratch rs, double *out)
+{
+	__shared__ double sh[kRT];
+	double a[1] = {0.0};
+	YZ_CHUNK_LOOP(i)
+	{
+		if(i >= n) break;
+		a[0] = a[0] + x[i] * y[i];
+	}
+	double tot[1];
+	if(GridFold<1>(a, sh, rs, tot) && threadIdx.x == 0) *out = tot[0];
+}
+
+#undef YZ_CHUNK_LOOP
+
+//==========================================================================
+//  Solver
+//==========================================================================
+static const int kB = 256;
+
+Solver::Solver(int device) : _device(device)
+{
+	YZ_CUDA(cudaSetDevice(device));
+	YZ_CUDA(cudaStreamCreateWithFlags(&_st, cudaStreamNonBlocking));
+	YZ_CUDA(cudaEventCreate(&_ev0)); YZ_CUDA(cudaEventCreate(&_ev1)); YZ_CUDA(cudaEventCreate(&_ev2));
+	YZ_CUDA(cudaMallocHost(&_hsc, sizeof(Scal)));
+	_sc.reserve(1);
+	_counters.reserve(16);
+	YZ_CUDA(cudaMemsetAsync(_counters.get(), 0, 16 * sizeof(unsigned), _st));
+	_flags.reserve(8);
+}
+
+Solver::~Solver()
+{
+	cudaSetDevice(_device);
+	cudaStreamSynchronize(_st);
+	if(_hsc) cudaFreeHost(_hsc);
+	cudaEventDestroy(_ev0); cudaEventDestroy(_ev1); cudaEventDestroy(_ev2);
+	cudaStreamDestroy(_st);
+}
+
+RedScratch Solver::Red(int site)
+{
+	RedScratch r;
+	r.part = _part.get();
+	r.counter = _counters.get() + site;
+	r.maxBlocks = _partBlocks;
+	return r;
+}
+
+void Solver::SetPattern(int n, int nnz, const int *rowptr, const int *scol, const int *ssrc)
+{
+	if(n <= 0 || nnz < n) throw UsageError("set_pattern: need n > 0 and nnz >= n");
+	YZ_CUDA(cudaSetDevice(_device));
+	_n = n; _nnz = nnz;
+	_hptr.assign(rowptr, rowptr + n + 1);
+	if(_hptr[0] != 0 || _hptr[(size_t)n] != nnz) throw UsageError("set_pattern: rowptr[0] must be 0 and rowptr[n] == nnz");
+	for(int i = 0; i < n; ++i) if(_hptr[(size_t)i + 1] <= _hptr[(size_t)i]) throw UsageError("set_pattern: every row needs its diagonal");
+	for(int k = 0; k < nnz; ++k)
+		if(scol[k] < 0 || scol[k] >= n || ssrc[k] < 0 || ssrc[k] >= nnz) throw UsageError("set_pattern: index out of range");
+	_hcol.assign(scol, scol + nnz);
+	_levels.clear();
+	_levels.emplace_back(new Level());
+	Level &L0 = *_levels[0];
+	L0.n = n; L0.nnz = nnz;
+	L0.ptr.upload(rowptr, (size_t)n + 1, _st);
+	L0.col.upload(scol, (size_t)nnz, _st);
+	L0.val.reserve((size_t)nnz);
+	_ssrc.upload(ssrc, (size_t)nnz, _st);
+	_values.reserve((size_t)nnz);
+	_rhs.reserve((size_t)n);
+	for(DBuf<double> *v : {&_b, &_x, &_x0, &_r, &_rh, &_p, &_v, &_s, &_ph, &_sh, &_t, &_m})
+		v->reserve((size_t)n);
+	_partBlocks = RedBlocks(n);
+	_part.reserve((size_t)2 * _partBlocks);
+	//  set-up scratch, sized by the finest level
+	_dia.reserve((size_t)n); _strong.reserve((size_t)nnz); _icnt.reserve((size_t)n + 1);
+	_iptr.reserve((size_t)n + 1); _icol.reserve((size_t)nnz); _ifill.reserve((size_t)n + 1);
+	_state.reserve((size_t)n); _iso.reserve((size_t)n);
+	_T0.reserve((size_t)n); _T1.reserve((size_t)n);
+	_flag.reserve((size_t)n + 1); _rootId.reserve((size_t)n + 1); _first.reserve((size_t)n);
+	_cnt.reserve((size_t)n + 1);
+	_scan.reserve(ScanScratchSize(n + 1) + 4);
+	_haveH = false;
+	YZ_CUDA(cudaStreamSynchronize(_st));
+}
+
+int Solver::ReadInt(const int *d)
+{
+	int h = 0;
+	YZ_CUDA(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, _st));
+	YZ_CUDA(cudaStreamSynchronize(_st));
+	return h;
+}
+
+void Solver::ReadScal()
+{
+	YZ_CUDA(cudaMemcpyAsync(_hsc, _sc.get(), sizeof(Scal), cudaMemcpyDeviceToHost, _st));
+	YZ_CUDA(cudaStreamSynchronize(_st));
+}
+
+//  rows -> scanned row pointer; returns the total
+int Solver::ScanCounts(const int *cnt, int *out, int n)
+{
+	ScanExclusive(cnt, out, n, _scan.get(), _st);
+	return ReadInt(out + n);
+}
+
+//--------------------------------------------------------------------------
+//  the hierarchy
+//--------------------------------------------------------------------------
+void Solver::BuildHierarchy(int coarseEnough)
+{
+	_levels.resize(1);
+	double eps = 0.08;
+	for(size_t l = 0;; ++l)
+	{
+		Level &L = *_levels[l];
+		const int n = L.n, nnz = L.nnz;
+		const int g = GridFor(n, kB), gz = GridFor(nnz, kB);
+		L.M.reserve((size_t)n); L.f.reserve((size_t)n); L.x.reserve((size_t)n);
+		L.t.reserve((size_t)n); L.xt.reserve((size_t)n); L.agg.reserve((size_t)n);
+		L.direct = false; L.nc = 0; L.pnnz = 0;
+		if(n <= coarseEnough)
+		{
+			L.direct = true;
+			const size_t w = 2 * (size_t)n;
+			_gj[0].reserve((size_t)n * w); _gj[1].reserve((size_t)n * w);
+			YZ_CUDA(cudaMemsetAsync(_gj[0].get(), 0, (size_t)n * w * sizeof(double), _st));
+			YZ_CUDA(cudaMemsetAsync(_gj[1].get(), 0, (size_t)n * w * sizeof(double), _st));
+			YZ_LAUNCH(KGjInit, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), _gj[0].get());
+			for(int k = 0; k < n; ++k)
+			{
+				const long long work = (long long)n * (long long)(w - k);
+				YZ_LAUNCH(KGjStep, GridFor(work, 256, 148 * 8), 256, 0, _st, n, k, _gj[k & 1].get(), _gj[(k + 1) & 1].get());
+			}
+			L.inv.reserve((size_t)n * n);
+			YZ_LAUNCH(KGjExtract, GridFor((long long)n * n, kB), kB, 0, _st, n, _gj[n & 1].get(), L.inv.get());
+			break;
+		}
+		//  strength
+		YZ_LAUNCH(KDiag, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), _dia.get());
+		YZ_CUDA(cudaMemsetAsync(_icnt.get(), 0, ((size_t)n + 1) * sizeof(int), _st));
+		YZ_LAUNCH(KStrength, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), _dia.get(), eps * eps,
+		          _strong.get(), _icnt.get());
+		eps *= 0.5;
+		ScanExclusive(_icnt.get(), _iptr.get(), n, _scan.get(), _st);
+		YZ_CUDA(cudaMemcpyAsync(_ifill.get(), _iptr.get(), (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice, _st));
+		YZ_LAUNCH(KFillIn, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), _strong.get(), _ifill.get(), _icol.get());
+		//  MIS-2 (at most 64 rounds, as the oracle)
+		YZ_LAUNCH(KMisInit, g, kB, 0, _st, n, L.ptr.get(), _strong.get(), _iptr.get(), _state.get(), _iso.get());
+		int *undec = _flags.get();
+		for(int round = 0; round < 64; ++round)
+		{
+			YZ_CUDA(cudaMemsetAsync(undec, 0, sizeof(int), _st));
+			YZ_LAUNCH(KMisPack, g, kB, 0, _st, n, _state.get(), _T0.get(), undec);
+			YZ_LAUNCH(KMisMax, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), _strong.get(), _iptr.get(), _icol.get(),
+			          _T0.get(), _T1.get(), undec);
+			YZ_LAUNCH(KMisMax, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), _strong.get(), _iptr.get(), _icol.get(),
+			          _T1.get(), _T0.get(), undec);
+			YZ_LAUNCH(KMisUpdate, g, kB, 0, _st, n, _state.get(), _T0.get(), undec);
+			if((round & 3) == 3 && ReadInt(undec) == 0) break;
+		}
+		//  aggregates
+		YZ_LAUNCH(KRootFlags, g, kB, 0, _st, n, _state.get(), _flag.get());
+		const int nc = ScanCounts(_flag.get(), _rootId.get(), n);
+		YZ_LAUNCH(KAssignFirst, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), _strong.get(), _iptr.get(), _icol.get(),
+		          _state.get(), _iso.get(), _rootId.get(), _first.get());
+		YZ_LAUNCH(KAssignSecond, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), _strong.get(), _iptr.get(), _icol.get(),
+		          _iso.get(), _first.get(), L.agg.get());
+		YZ_LAUNCH(KSpai0, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), L.M.get());
+		L.nc = nc;
+		if(nc == 0) break;		// nothing to coarsen: this level is smoothed only
+		//  P
+		int *overflow = _flags.get() + 1;
+		YZ_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int), _st));
+		YZ_LAUNCH(KPCount, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), _strong.get(), L.agg.get(), _cnt.get(), overflow);
+		L.pptr.reserve((size_t)n + 1);
+		L.pnnz = ScanCounts(_cnt.get(), L.pptr.get(), n);
+		L.pcol.reserve((size_t)L.pnnz); L.pval.reserve((size_t)L.pnnz);
+		YZ_LAUNCH(KPFill, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), _strong.get(), L.agg.get(),
+		          L.pptr.get(), L.pcol.get(), L.pval.get());
+		//  R = P^T
+		L.rptr.reserve((size_t)nc + 1); L.rcol.reserve((size_t)L.pnnz); L.rval.reserve((size_t)L.pnnz);
+		YZ_CUDA(cudaMemsetAsync(_cnt.get(), 0, ((size_t)nc + 1) * sizeof(int), _st));
+		YZ_LAUNCH(KColCount, GridFor(L.pnnz, kB), kB, 0, _st, L.pnnz, L.pcol.get(), _cnt.get());
+		ScanExclusive(_cnt.get(), L.rptr.get(), nc, _scan.get(), _st);
+		YZ_CUDA(cudaMemcpyAsync(_ifill.get(), L.rptr.get(), (size_t)nc * sizeof(int), cudaMemcpyDeviceToDevice, _st));
+		YZ_LAUNCH(KTransposeFill, g, kB, 0, _st, n, L.pptr.get(), L.pcol.get(), L.pval.get(), _ifill.get(),
+		          L.rcol.get(), L.rval.get());
+		YZ_LAUNCH(KRowSort, GridFor(nc, kB), kB, 0, _st, nc, L.rptr.get(), L.rcol.get(), L.rval.get());
+		//  AP, then A_c = R (AP)
+		YZ_LAUNCH(KGemmCount, g, 128, 0, _st, n, L.ptr.get(), L.col.get(), L.pptr.get(), L.pcol.get(), _cnt.get(), overflow);
+		_apPtr.reserve((size_t)n + 1);
+		const int apnnz = ScanCounts(_cnt.get(), _apPtr.get(), n);
+		_apCol.reserve((size_t)apnnz); _apVal.reserve((size_t)apnnz);
+		YZ_LAUNCH(KGemmFill, g, 128, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), L.pptr.get(), L.pcol.get(),
+		          L.pval.get(), _apPtr.get(), _apCol.get(), _apVal.get());
+		_levels.emplace_back(new Level());
+		Level &C = *_levels.back();
+		Level &F = *_levels[l];
+		C.n = nc;
+		YZ_LAUNCH(KGemmCount, GridFor(nc, 128), 128, 0, _st, nc, F.rptr.get(), F.rcol.get(), _apPtr.get(), _apCol.get(),
+		          _cnt.get(), overflow);
+		C.ptr.reserve((size_t)nc + 1);
+		C.nnz = ScanCounts(_cnt.get(), C.ptr.get(), nc);
+		C.col.reserve((size_t)C.nnz); C.val.reserve((size_t)C.nnz);
+		YZ_LAUNCH(KGemmFill, GridFor(nc, 128), 128, 0, _st, nc, F.rptr.get(), F.rcol.get(), F.rval.get(), _apPtr.get(),
+		          _apCol.get(), _apVal.get(), C.ptr.get(), C.col.get(), C.val.get());
+		if(ReadInt(overflow)) throw CudaError("AMG set-up: a row gathered more than 256 distinct columns");
+	}
+	_haveH = true;
+}
+
+//  x = V(l) f from a zero guess
+void Solver::Cycle(size_t l, const double *f, double *x)
+{
+	Level &L = *_levels[l];
+	const int n = L.n, g = GridFor(n, kB);
+	if(L.direct)
+	{
+		YZ_LAUNCH(KDenseMV, g, kB, 0, _st, n, L.inv.get(), f, x);
+		return;
+	}
+	if(l + 1 < _levels.size())
+	{
+		Level &C = *_levels[l + 1];
+		YZ_LAUNCH(KPreSmoothResidual, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), L.M.get(), f, x, L.t.get());
+		YZ_LAUNCH(KSpmv, GridFor(C.n, kB), kB, 0, _st, C.n, L.rptr.get(), L.rcol.get(), L.rval.get(), L.t.get(), C.f.get());
+		Cycle(l + 1, C.f.get(), C.x.get());
+		YZ_LAUNCH(KProlong, g, kB, 0, _st, n, L.pptr.get(), L.pcol.get(), L.pval.get(), C.x.get(), x, L.xt.get());
+		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), L.M.get(), f, L.xt.get(), x);
+	}
+	else
+	{
+		YZ_LAUNCH(KPreSmooth, g, kB, 0, _st, n, L.M.get(), f, L.xt.get());
+		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), L.M.get(), f, L.xt.get(), x);
+	}
+}
+
+void Solver::ApplyPrec(int kind, const double *r, double *z)
+{
+	const int n = _n;
+	if(kind == kPrecDiag) YZ_LAUNCH(KDiagApply, GridFor(n, kB), kB, 0, _st, n, _m.get(), r, z);
+	else Cycle(0, r, z);
+}
+
+//  BiCGStab on level 0's matrix (values in _levels[0]); the oracle's
+//  BiCGStab() step by step.  Returns false on a breakdown (rho == 0).
+bool Solver::BiCGStab(int kind, int maxIter, double tol, int &itOut, double &errOut)
+{
+	Level &A = *_levels[0];
+	const int n = _n, nb = RedBlocks(n), g = GridFor(n, kB);
+	const int *ptr = A.ptr.get(), *col = A.col.get();
+	const double *val = A.val.get();
+	double *b = _b.get(), *x = _x.get();
+	YZ_LAUNCH(KBInit, nb, kRT, 0, _st, n, ptr, col, val, b, x, _r.get(), _rh.get(), Red(0), _sc.get());
+	ReadScal();
+	const double normB = _hsc->normb;
+	if(normB < 2.0 * 2.220446049250313e-16)
+	{
+		YZ_LAUNCH(KFill, g, kB, 0, _st, n, 0.0, x);
+		itOut = 0; errOut = normB;
+		return true;
+	}
+	const double eps = tol * normB;
+	double res = _hsc->res;
+	int it = 0;
+	if(res > eps)
+	{
+		while(it < maxIter)
+		{
+			if(_hsc->rho == 0.0) return false;
+			YZ_LAUNCH(KPUpdate, g, kB, 0, _st, n, it == 0 ? 1 : 0, _r.get(), _v.get(), _p.get(), _sc.get());
+			ApplyPrec(kind, _p.get(), _ph.get());
+			YZ_LAUNCH(KSpmvAlpha, nb, kRT, 0, _st, n, ptr, col, val, _ph.get(), _rh.get(), _v.get(), Red(1), _sc.get());
+			YZ_LAUNCH(KSUpdate, nb, kRT, 0, _st, n, _r.get(), _v.get(), _s.get(), Red(2), _sc.get());
+			ReadScal();
+			res = _hsc->res;
+			if(res <= eps)
+			{
+				YZ_LAUNCH(KXHalf, g, kB, 0, _st, n, _ph.get(), x, _sc.get());
+				++it;
+				break;
+			}
+			ApplyPrec(kind, _s.get(), _sh.get());
+			YZ_LAUNCH(KSpmvOmega, nb, kRT, 0, _st, n, ptr, col, val, _sh.get(), _s.get(), _t.get(), Red(3), _sc.get());
+			YZ_LAUNCH(KXRUpdate, nb, kRT, 0, _st, n, _ph.get(), _sh.get(), _s.get(), _t.get(), _rh.get(), x, _r.get(),
+			          Red(4), _sc.get());
+			ReadScal();
+			res = _hsc->res;
+			++it;
+			if(res <= eps) break;
+			if(!(res == res)) break;
+		}
+	}
+	itOut = it;
+	errOut = res / normB;
+	return true;
+}
+
+//  LinearSolverBackend.cpp:681-713, on the host (a breakdown is rare): the
+//  residual of what x holds, summed sequentially as the reference does
+double Solver::BreakdownResidual()
+{
+	const int n = _n, nnz = _nnz;
+	std::vector<double> val((size_t)nnz), b((size_t)n), x((size_t)n);
+	_levels[0]->val.download(val.data(), (size_t)nnz, _st);
+	_b.download(b.data(), (size_t)n, _st);
+	_x.download(x.data(), (size_t)n, _st);
+	YZ_CUDA(cudaStreamSynchronize(_st));
+	double rr = 0.0, bb = 0.0;
+	for(int i = 0; i < n; ++i)
+	{
+		double ax = 0.0;
+		for(int k = _hptr[(size_t)i]; k < _hptr[(size_t)i + 1]; ++k) ax += val[(size_t)k] * x[(size_t)_hcol[(size_t)k]];
+		const double d = b[(size_t)i] - ax;
+		rr += d * d; bb += b[(size_t)i] * b[(size_t)i];
+	}
+	return (bb > 0.0) ? std::sqrt(rr / bb) : std::sqrt(rr);
+}
+
+int Solver::Solve(const yz_settings &set, const double *dValues, const double *dRhs, double *dX, int &iterOut, double &residOut)
+{
+	if(_n <= 0) throw UsageError("solve: set_pattern first");
+	if(set.max_iteration < 0) throw UsageError("solve: max_iteration must be >= 0");
+	YZ_CUDA(cudaSetDevice(_device));
+	const long long l0 = g_launches.load();
+	const int n = _n, nnz = _nnz, g = GridFor(n, kB);
+	Level &L0 = *_levels[0];
+	YZ_LAUNCH(KScaleGather, g, kB, 0, _st, n, L0.ptr.get(), _ssrc.get(), dValues, dRhs, set.scaling ? 1 : 0,
+	          L0.val.get(), _b.get());
+	(void)nnz;
+	YZ_CUDA(cudaMemcpyAsync(_x.get(), dX, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+	YZ_CUDA(cudaMemcpyAsync(_x0.get(), dX, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+	YZ_CUDA(cudaEventRecord(_ev0, _st));
+	_setupMs = 0; _iterMs = 0;
+	int it = 0, itTried = 0;
+	double err = 0.0;
+	const int tryIter = set.max_iteration < 300 ? set.max_iteration : 300;
+	bool done = false;
+	bool timedSetup = false;
+
+	if(set.conc && set.precondition == 2 && _offSpai.Try())
+	{
+		YZ_LAUNCH(KSpai0, g, kB, 0, _st, n, L0.ptr.get(), L0.col.get(), L0.val.get(), _m.get());
+		if(!BiCGStab(kPrecDiag, tryIter, set.epsilon, it, err)) err = 1e300;
+		if(err <= set.epsilon) { done = true; _offSpai.Converged(); }
+		else
+		{
+			_offSpai.Failed();
+			itTried = it;
+			YZ_CUDA(cudaMemcpyAsync(_x.get(), _x0.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+		}
+	}
+	bool broke = false;
+	if(!done)
+	{
+		if(set.precondition == 0 || set.precondition == 1)
+		{
+			YZ_LAUNCH(KDiag, g, kB, 0, _st, n, L0.ptr.get(), L0.col.get(), L0.val.get(), _dia.get());
+			YZ_LAUNCH(KDampedJacobi, g, kB, 0, _st, n, _dia.get(), _m.get());
+			broke = !BiCGStab(kPrecDiag, set.max_iteration, set.epsilon, it, err);
+		}
+		else
+		{
+			BuildHierarchy(n > 3000 ? 500 : 3000);
+			YZ_CUDA(cudaEventRecord(_ev1, _st));
+			timedSetup = true;
+			broke = !BiCGStab(kPrecAmg, set.max_iteration, set.epsilon, it, err);
+		}
+	}
+	YZ_CUDA(cudaEventRecord(_ev2, _st));
+	YZ_CUDA(cudaEventSynchronize(_ev2));
+	float ms = 0;
+	if(timedSetup)
+	{
+		YZ_CUDA(cudaEventElapsedTime(&ms, _ev0, _ev1)); _setupMs = ms;
+		YZ_CUDA(cudaEventElapsedTime(&ms, _ev1, _ev2)); _iterMs = ms;
+	}
+	else { YZ_CUDA(cudaEventElapsedTime(&ms, _ev0, _ev2)); _iterMs = ms; }
+	_launches += g_launches.load() - l0;
+	if(broke)
+	{
+		const double rel = BreakdownResidual();
+		if(rel <= set.epsilon && rel == rel) { it = 0; err = rel; }
+		else { iterOut = itTried; residOut = rel; return 2; }
+	}
+	YZ_CUDA(cudaMemcpyAsync(dX, _x.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+	YZ_CUDA(cudaStreamSynchronize(_st));
+	iterOut = it + itTried;
+	residOut = err;
+	if(err <= set.epsilon) return 0;
+	if(!(err == err)) return 2;
+	return 1;
+}
+
+int Solver::SolveHost(const yz_settings &set, const double *values, const double *rhs, double *x, int &iter, double &resid)
+{
+	if(_n <= 0) throw UsageError("solve: set_pattern first");
+	YZ_CUDA(cudaSetDevice(_device));
+	_values.upload(values, (size_t)_nnz, _st);
+	_rhs.upload(rhs, (size_t)_n, _st);
+	_xio.upload(x, (size_t)_n, _st);
+	const int ret = Solve(set, _values.get(), _rhs.get(), _xio.get(), iter, resid);
+	if(ret != 2)
+	{
+		_xio.download(x, (size_t)_n, _st);
+		YZ_CUDA(cudaStreamSynchronize(_st));
+	}
+	return ret;
+}
+
+std::vector<double> Solver::Memory() const { return {(double)_offSpai.skip, (double)_offSpai.wait}; }
+void Solver::SetMemory(const double *m, int len)
+{
+	if(len != 2) return;
+	_offSpai.skip = (int)m[0]; _offSpai.wait = (int)m[1];
+}
+
+int Solver::LevelCount() const { return _haveH ? (int)_levels.size() : 0; }
+
+void Solver::LevelInfo(int l, int *rows, int *nnzA, int *nnzP, int *direct) const
+{
+	if(!_haveH || l < 0 || l >= (int)_levels.size()) throw UsageError("level_info: no such level");
+	const Level &L = *_levels[(size_t)l];
+	if(rows) *rows = L.n;
+	if(nnzA) *nnzA = L.nnz;
+	if(nnzP) *nnzP = (L.direct || L.nc == 0) ? 0 : L.pnnz;
+	if(direct) *direct = L.direct ? 1 : 0;
+}
+
+void Solver::LevelCopy(int l, int *aptr, int *acol, double *aval, int *pptr, int *pcol, double *pval, int *agg)
+{
+	if(!_haveH || l < 0 || l >= (int)_levels.size()) throw UsageError("level_copy: no such level");
+	YZ_CUDA(cudaSetDevice(_device));
+	Level &L = *_levels[(size_t)l];
+	if(aptr) L.ptr.download(aptr, (size_t)L.n + 1, _st);
+	if(acol) L.col.download(acol, (size_t)L.nnz, _st);
+	if(aval) L.val.download(aval, (size_t)L.nnz, _st);
+	if(!L.direct && L.nc > 0)
+	{
+		if(pptr) L.pptr.download(pptr, (size_t)L.n + 1, _st);
+		if(pcol) L.pcol.download(pcol, (size_t)L.pnnz, _st);
+		if(pval) L.pval.download(pval, (size_t)L.pnnz, _st);
+	}
+	if(agg && !L.direct) L.agg.download(agg, (size_t)L.n, _st);
+	YZ_CUDA(cudaStreamSynchronize(_st));
+}
+
+//--------------------------------------------------------------------------
+//  stand-alone building blocks
+//--------------------------------------------------------------------------
+double DeviceDot(int n, const double *hx, const double *hy)
+{
+	DBuf<double> x, y, part, out;
+	DBuf<unsigned> cnt;
+	x.upload(hx, (size_t)n, 0); y.upload(hy, (size_t)n, 0);
+	const int nb = RedBlocks(n);
+	part.reserve((size_t)nb); out.reserve(1); cnt.reserve(1);
+	YZ_CUDA(cudaMemset(cnt.get(), 0, sizeof(unsigned)));
+	RedScratch rs{part.get(), cnt.get(), nb};
+	YZ_LAUNCH(KDot, nb, kRT, 0, 0, n, x.get(), y.get(), rs, out.get());
+	double h = 0;
+	YZ_CUDA(cudaMemcpy(&h, out.get(), sizeof(double), cudaMemcpyDeviceToHost));
+	return h;
+}
+
+void DeviceSpmv(int n, int nnz, const int *rowptr, const int *col, const double *val, const double *hx, double *hy)
+{
+	DBuf<int> p, c; DBuf<double> v, x, y;
+	p.upload(rowptr, (size_t)n + 1, 0); c.upload(col, (size_t)nnz, 0); v.upload(val, (size_t)nnz, 0);
+	x.upload(hx, (size_t)n, 0); y.reserve((size_t)n);
+	YZ_LAUNCH(KSpmv, GridFor(n, kB), kB, 0, 0, n, p.get(), c.get(), v.get(), x.get(), y.get());
+	YZ_CUDA(cudaMemcpy(hy, y.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+}
+
+} // namespace yz

@@ -1,0 +1,108 @@
+// yz_solver_impl.h -- the device solver context behind yz_solver_* (C ABI).
+#pragma once
+
+#include "yz_common.cuh"
+#include "../../include/yuzen_b200.h"
+
+#include <memory>
+#include <vector>
+
+namespace yz {
+
+//  Scalars of one BiCGStab run, in device memory (written by the block that
+//  folds a reduction, read by the element-wise kernels and by the host).
+struct Scal
+{
+	double normb, res, rho, rhoPrev, alpha, omega;
+};
+
+//  TryBackoff, LinearSolverBackend.cpp:262-270
+struct TryBackoff
+{
+	int skip = 0, wait = 16;
+	bool Try() { if(skip > 0) { --skip; return false; } return true; }
+	void Failed() { skip = wait; wait = (wait < 1024) ? 2 * wait : 1024; }
+	void Converged() { wait = 16; }
+};
+
+struct Level
+{
+	int n = 0, nnz = 0;
+	DBuf<int> ptr, col;
+	DBuf<double> val;
+	DBuf<double> M, f, x, t, xt;
+	DBuf<int> agg;
+	int nc = 0, pnnz = 0;
+	DBuf<int> pptr, pcol, rptr, rcol;
+	DBuf<double> pval, rval;
+	bool direct = false;
+	DBuf<double> inv;		// column-major dense inverse of the direct level
+};
+
+class Solver
+{
+public:
+	explicit Solver(int device);
+	~Solver();
+
+	void SetPattern(int n, int nnz, const int *rowptr, const int *scol, const int *ssrc);
+	int Solve(const yz_settings &set, const double *dValues, const double *dRhs, double *dX, int &iter, double &resid);
+	int SolveHost(const yz_settings &set, const double *values, const double *rhs, double *x, int &iter, double &resid);
+
+	std::vector<double> Memory() const;
+	void SetMemory(const double *m, int len);
+	int LevelCount() const;
+	void LevelInfo(int l, int *rows, int *nnzA, int *nnzP, int *direct) const;
+	void LevelCopy(int l, int *aptr, int *acol, double *aval, int *pptr, int *pcol, double *pval, int *agg);
+	void Timing(double *setupMs, double *iterMs) const { if(setupMs) *setupMs = _setupMs; if(iterMs) *iterMs = _iterMs; }
+	long long Launches() const { return _launches; }
+	cudaStream_t Stream() const { return _st; }
+	int Rows() const { return _n; }
+
+private:
+	enum { kPrecDiag = 0, kPrecAmg = 1 };
+	void BuildHierarchy(int coarseEnough);
+	void Cycle(size_t l, const double *f, double *x);
+	void ApplyPrec(int kind, const double *r, double *z);
+	bool BiCGStab(int kind, int maxIter, double tol, int &itOut, double &errOut);
+	double BreakdownResidual();
+	int ReadInt(const int *d);
+	void ReadScal();
+	int ScanCounts(const int *cnt, int *out, int n);
+	RedScratch Red(int site);
+
+	int _device;
+	cudaStream_t _st = nullptr;
+	cudaEvent_t _ev0 = nullptr, _ev1 = nullptr, _ev2 = nullptr;
+	int _n = 0, _nnz = 0;
+	std::vector<int> _hptr, _hcol;
+	DBuf<int> _ssrc;
+	DBuf<double> _values, _rhs, _xio;
+	std::vector<std::unique_ptr<Level>> _levels;
+	bool _haveH = false;
+	//  Krylov vectors
+	DBuf<double> _b, _x, _x0, _r, _rh, _p, _v, _s, _ph, _sh, _t, _m;
+	DBuf<double> _part;
+	int _partBlocks = 1;
+	DBuf<unsigned> _counters;
+	DBuf<Scal> _sc;
+	Scal *_hsc = nullptr;
+	DBuf<int> _flags;
+	//  set-up scratch
+	DBuf<double> _dia;
+	DBuf<unsigned char> _strong, _iso;
+	DBuf<int> _icnt, _iptr, _icol, _ifill, _state, _flag, _rootId, _first, _cnt, _scan;
+	DBuf<unsigned long long> _T0, _T1;
+	DBuf<int> _apPtr, _apCol;
+	DBuf<double> _apVal;
+	DBuf<double> _gj[2];
+	TryBackoff _offSpai;
+	double _setupMs = 0, _iterMs = 0;
+	long long _launches = 0;
+};
+
+double DeviceDot(int n, const double *hx, const double *hy);
+void DeviceSpmv(int n, int nnz, const int *rowptr, const int *col, const double *val, const double *hx, double *hy);
+const char *LastError();
+
+} // namespace yz
