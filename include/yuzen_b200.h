@@ -104,6 +104,90 @@ int yz_dot(int n, const double* x, const double* y, double* out);
 int yz_spmv(int n, int nnz, const int* rowptr, const int* col, const double* val,
             const double* x, double* y);
 
+/*
+ * ---------------------------------------------------------------------
+ * Seam 2: the whole implicit step of the well-mixed film-height equation.
+ * Replaces C_NewtonKantorovich::TimeAdvance (NewtonKantorovich.cpp:424-486)
+ * with the hooks of WellMixed_HeightEquationBase (HeightEquationBase.h:
+ * SetMatrixA :670-788, ApplyA :804-827, SetMatrixJacobi :1062-1091,
+ * BeforeNKLoop / EveryNKLoop / AfterNKLoop :1314-) and the clock advance of
+ * the model loop (WellMixedModelBase.h:1334, TimeSteps.cpp:121-160), on a 2-D
+ * grid with two ghost layers (nx = Nx+4, row of cell (ix,iy) = iy*nx + ix,
+ * Grids.h:256).  Everything is non-dimensional, as the reference's model
+ * holds it after NonDimensionalNumbers::Build (NonDimensionalNumbers.cpp:43).
+ * ---------------------------------------------------------------------
+ */
+typedef struct yz_step yz_step;
+
+/* BoundaryCondition::tBoundaryCondition (BoundaryCondition.h:56-63); the
+ * step supports Symmetry and Periodic edges. */
+enum { YZ_BC_SYMMETRY = 0, YZ_BC_PERIODIC = 1 };
+
+typedef struct yz_step_params
+{
+	int    nx, ny;                /* points including the ghost layers */
+	int    bc[4];                 /* Xmin, Xmax, Ymin, Ymax */
+	double dx, dy;                /* C_Grid2D spacing */
+	double x0, y0;                /* coordinate of cell (0,0) */
+	double theta;                 /* 0.5: Crank-Nicolson */
+	/* physics terms (HeightEquationBase.h:565-577) */
+	int    on_laplace, on_vgrav, on_pgrav, on_marangoni, on_centrifugal, on_disjoining;
+	int    on_evap, conc_field;   /* conc_field 0: c carried unchanged (Physics.ConcField = None) */
+	double Bo, Dp, hstar, disj_n, disj_m, lambda_slip, Ev;
+	/* property laws (FluidProperty.h:100-181) */
+	double visc_c0, visc_base, visc_exp;
+	double sig_c0, sig_base, sig_coef;
+	/* evaporation (Evaporation.cpp), non-dimensional with Coef = 1 */
+	int    ev_conc_func;          /* 0 Raoult, 1 PowerN */
+	int    ev_spatial;            /* 0 uniform, 1 negPow */
+	int    ev_hast_modify;
+	double ev_m_resin, ev_m_solvent, ev_power_n, ev_conc_r, ev_negpow_exp, ev_negpow_rmax, ev_h_ast;
+	/* Newton-Kantorovich (NewtonKantorovich.h:56-70) */
+	int    nk_max, nk_min;
+	double nk_eps, nk_eps_rel;
+	/* the linear solve of the height equation */
+	yz_settings lin;
+	/* time-step control (ImplicitSolver.cpp:144-190, 271-307) */
+	int    dt_control, dt_keep_steps;
+	double dt, dt_max, dt_min, dt_change_factor, dt_criterion, dt_scale_floor;
+	double t_start;
+} yz_step_params;
+
+typedef struct yz_step_stats
+{
+	int    steps;              /* steps taken by this call */
+	int    newton_iterations;  /* Newton passes, summed */
+	int    linear_iterations;  /* BiCGStab iterations, summed */
+	int    retries;            /* attempts cut and repeated (dt control) */
+	double time;               /* the clock after the call */
+	double dt;                 /* DT().now after the call */
+	double last_resid;         /* Newton correction of the last pass */
+	double setup_ms, solve_ms, assemble_ms;  /* device time of the call */
+} yz_step_stats;
+
+/* Build the step: fields h, c, s on all nx*ny points (host arrays). */
+int yz_step_create(int device, const yz_step_params* p, const double* h, const double* c,
+                   const double* s, yz_step** out);
+int yz_step_destroy(yz_step* st);
+/* Advance nsteps time steps (TimeAdvance + the clock advance each). */
+int yz_step_advance(yz_step* st, int nsteps, yz_step_stats* stats);
+/* Fields after the last step (host arrays of nx*ny; null pointers skipped). */
+int yz_step_get_fields(yz_step* st, double* h, double* c);
+/* The fixed CRS pattern of A / I + theta dt J, storage order (diagonal
+ * first): rowptr n+1, col nnz, boundary flags n.  nnz is returned. */
+int yz_step_pattern(yz_step* st, int* rowptr, int* col, int* bc);
+/* One Newton pass's system at the film h (as SetMatrixA, SetMatrixJacobi,
+ * MakeMatrix_IA, ApplyA and MakeRHS build it with phi_old, phi_guess = h and
+ * the explicit half A(h_old) h_old, evaporation at h_old): values of
+ * I + theta dt J (nnz, storage order) and the right-hand side (n). */
+int yz_step_system(yz_step* st, const double* h_old, const double* h, double dt,
+                   double* ia_values, double* rhs);
+/* The same pattern built on the host alone, without a device (the structure
+ * C_ImplicitSolver::Alloc fixes, ImplicitSolver.cpp:60-81, with the ghost rows
+ * of BoundaryCondition2D::Apply, BoundaryCondition.cpp:376-517); arrays may be
+ * null to query nnz (the return value). */
+int yz_pattern_2d(const yz_step_params* p, int* rowptr, int* col, int* bc);
+
 #ifdef __cplusplus
 }
 #endif

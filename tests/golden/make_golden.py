@@ -27,9 +27,11 @@ REPO = HERE.parents[1]
 sys.path.insert(0, str(HERE))
 
 import dumpio  # noqa: E402
+import stateio  # noqa: E402
 import tomlw  # noqa: E402
 
 ORACLE = REPO / "oracle" / "_ref" / "yuzen_oracle"
+PROBE = REPO / "oracle" / "_ref" / "yz_probe"
 
 QUIET_OUTPUT = {
     "Output.FieldData.TimeInterval": 1e30,
@@ -74,6 +76,73 @@ CASES = {
 }
 
 
+#  Whole-step cases for the probe: name: (reference case, overrides, steps,
+#  index of the first Newton solve among the dumps)
+_NO_UPWIND = {
+    "Physics.SolutoCapillarity.Enable": False, "Physics.HorizontalGravity.Enable": False,
+    "Physics.Centrifugal.Enable": False, "Physics.ConcField.Model": "None",
+}
+STEP_CASES = {
+    # capillary + disjoining pressure, periodic edges, fixed dt
+    "step_disjoin_periodic_56": ("allphys_2d_reg.toml", {
+        **_NO_UPWIND, "Grid.Nx": 56, "Grid.Ny": 56,
+        "Boundary.XminBC.Type": "Periodic", "Boundary.XmaxBC.Type": "Periodic",
+        "Boundary.YminBC.Type": "Periodic", "Boundary.YmaxBC.Type": "Periodic",
+        "Physics.VerticalGravity.Enable": False, "Physics.Evaporation.Enable": False,
+        "Physics.DisjoiningPressure.Enable": True, "Physics.DisjoiningPressure.ContactAngle": 10.0,
+        "Physics.DisjoiningPressure.ExponentN": 3.0, "Physics.DisjoiningPressure.ExponentM": 2.0,
+        "Initial.SurfaceShape.PrecursorRatio": 0.05,
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-4,
+    }, 3, 3),
+    # capillary over a substrate bump + vertical gravity + evaporation +
+    # Navier slip, mirror edges, c carried unchanged, fixed dt
+    "step_capgrav_slip_48": ("allphys_2d_reg.toml", {
+        **_NO_UPWIND, "Grid.Nx": 48, "Grid.Ny": 44,
+        "Physics.VerticalGravity.Enable": True, "Physics.Evaporation.Enable": True,
+        "Physics.Slip.Enable": True, "Physics.Slip.Length": 5e-7,
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 2e-4,
+    }, 4, 3),
+    # capillary + disjoining with the time-step control on
+    "step_adaptive_40": ("allphys_2d_reg.toml", {
+        **_NO_UPWIND, "Grid.Nx": 40, "Grid.Ny": 40,
+        "Physics.VerticalGravity.Enable": False, "Physics.Evaporation.Enable": False,
+        "Physics.DisjoiningPressure.Enable": True, "Physics.DisjoiningPressure.ContactAngle": 15.0,
+        "Physics.DisjoiningPressure.ExponentN": 3.0, "Physics.DisjoiningPressure.ExponentM": 2.0,
+        "Initial.SurfaceShape.PrecursorRatio": 0.1,
+        "Numerics.TimeStepControl.Enable": True, "Numerics.TimeStepControl.KeepSteps": 2,
+        "Numerics.TimeStepControl.ChangeFactor": 0.75, "Numerics.InitialDt": 1e-3,
+    }, 10, 3),
+}
+
+
+def write_case(ref: Path, src: str, over: dict, name: str, work: Path) -> Path:
+    doc = tomllib.loads((ref / "cases" / src).read_text())
+    for k, v in {**QUIET_OUTPUT, **over}.items():
+        tomlw.setpath(doc, k, v)
+    doc["JobName"] = name
+    case = work / f"{name}.toml"
+    case.write_text(tomlw.dumps(doc))
+    return case
+
+
+def make_step_case(ref: Path, name: str, work: Path) -> dict:
+    src, over, steps, first = STEP_CASES[name]
+    case = write_case(ref, src, {**over, "Numerics.MaxSteps": steps}, name, work)
+    dump = work / f"dump_{name}"
+    dump.mkdir()
+    env = dict(os.environ, YZO_DUMP_DIR=str(dump), YZO_DUMP_MAX="8", OMP_NUM_THREADS="4")
+    res = subprocess.run([str(PROBE), case.name, f"{name}.bin"], cwd=work, env=env, capture_output=True,
+                         text=True, timeout=900)
+    if res.returncode != 0:
+        raise RuntimeError(f"{name}: probe failed\n{res.stdout[-2000:]}\n{res.stderr[-2000:]}")
+    d = stateio.read_state(work / f"{name}.bin")
+    sys_ = dumpio.read_dump(sorted(dump.glob("solve_*.bin"))[first])
+    d["sys_values"] = sys_["values"]
+    d["sys_rhs"] = sys_["rhs"]
+    d["case"] = name
+    return d
+
+
 def make_case(ref: Path, name: str, work: Path) -> list[dict]:
     src, over, keep = CASES[name]
     doc = tomllib.loads((ref / "cases" / src).read_text())
@@ -103,6 +172,12 @@ def main() -> None:
     if not ORACLE.exists():
         raise SystemExit(f"{ORACLE} missing: make -C oracle ref")
     with tempfile.TemporaryDirectory() as tmp:
+        for name in STEP_CASES:
+            if a.only and name != a.only:
+                continue
+            d = make_step_case(Path(a.ref), name, Path(tmp))
+            stateio.save_npz(HERE / f"{name}.npz", d)
+            print(name, d["nx"], d["ny"], "steps", d["steps_done"], "t_end", d["t_end"])
         for name in CASES:
             if a.only and name != a.only:
                 continue

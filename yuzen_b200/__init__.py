@@ -34,6 +34,8 @@ EXPORTED_SYMBOLS = (
     "yz_solver_solve", "yz_solver_solve_device", "yz_solver_set_precision",
     "yz_solver_memory", "yz_solver_set_memory", "yz_solver_levels", "yz_solver_level_info",
     "yz_solver_level_copy", "yz_solver_last_timing", "yz_solver_launches", "yz_dot", "yz_spmv",
+    "yz_step_create", "yz_step_destroy", "yz_step_advance", "yz_step_get_fields", "yz_step_pattern",
+    "yz_step_system", "yz_pattern_2d",
 )
 
 

@@ -1,11 +1,19 @@
 // yz_capi.cu -- the extern "C" entry points of include/yuzen_b200.h.
 // Every call catches what the C++ side throws and turns it into a status.
 #include "yz_solver_impl.h"
+#include "yz_step_impl.h"
+
+#include <cstring>
 
 struct yz_solver
 {
 	std::unique_ptr<yz::Solver> s;
 	int precision = YZ_PREC_FP64;
+};
+
+struct yz_step
+{
+	std::unique_ptr<yz::Step> s;
 };
 
 namespace {
@@ -151,6 +159,81 @@ int yz_spmv(int n, int nnz, const int *rowptr, const int *col, const double *val
 		if(n <= 0 || nnz < 0 || !rowptr || !col || !val || !x || !y) throw yz::UsageError("yz_spmv: bad argument");
 		yz::DeviceSpmv(n, nnz, rowptr, col, val, x, y);
 		return 0;
+	});
+}
+
+//--------------------------------------------------------------------------
+//  the whole step
+//--------------------------------------------------------------------------
+int yz_step_create(int device, const yz_step_params *p, const double *h, const double *c, const double *s, yz_step **out)
+{
+	return Guard([&] {
+		if(!p || !h || !c || !s || !out) throw yz::UsageError("yz_step_create: null argument");
+		int count = 0;
+		yz::Check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+		if(device < 0 || device >= count) throw yz::UsageError("yz_step_create: no such CUDA device");
+		yz_step *st = new yz_step();
+		try { st->s.reset(new yz::Step(device, *p, h, c, s)); }
+		catch(...) { delete st; throw; }
+		*out = st;
+		return 0;
+	});
+}
+
+int yz_step_destroy(yz_step *st)
+{
+	return Guard([&] { delete st; return 0; });
+}
+
+int yz_step_advance(yz_step *st, int nsteps, yz_step_stats *stats)
+{
+	return Guard([&] {
+		if(!st || nsteps < 0) throw yz::UsageError("yz_step_advance: bad argument");
+		yz_step_stats local;
+		std::memset(&local, 0, sizeof local);
+		st->s->Advance(nsteps, local);
+		if(stats) *stats = local;
+		return 0;
+	});
+}
+
+int yz_step_get_fields(yz_step *st, double *h, double *c)
+{
+	return Guard([&] {
+		if(!st) throw yz::UsageError("yz_step_get_fields: null step");
+		st->s->GetFields(h, c);
+		return 0;
+	});
+}
+
+int yz_step_pattern(yz_step *st, int *rowptr, int *col, int *bc)
+{
+	return Guard([&] {
+		if(!st) throw yz::UsageError("yz_step_pattern: null step");
+		return st->s->Pattern(rowptr, col, bc);
+	});
+}
+
+int yz_step_system(yz_step *st, const double *h_old, const double *h, double dt, double *ia, double *rhs)
+{
+	return Guard([&] {
+		if(!st || !h_old || !h || !ia || !rhs) throw yz::UsageError("yz_step_system: null argument");
+		st->s->System(h_old, h, dt, ia, rhs);
+		return 0;
+	});
+}
+
+int yz_pattern_2d(const yz_step_params *p, int *rowptr, int *col, int *bc)
+{
+	return Guard([&] {
+		if(!p) throw yz::UsageError("yz_pattern_2d: null params");
+		yz::CheckParams(*p);
+		std::vector<int> rp, cl, isbc, ghost, partner;
+		yz::BuildPattern2D(*p, rp, cl, isbc, ghost, partner);
+		if(rowptr) std::copy(rp.begin(), rp.end(), rowptr);
+		if(col) std::copy(cl.begin(), cl.end(), col);
+		if(bc) std::copy(isbc.begin(), isbc.end(), bc);
+		return (int)cl.size();
 	});
 }
 

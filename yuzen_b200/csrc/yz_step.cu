@@ -1,0 +1,882 @@
+// yz_step.cu -- the implicit step of the well-mixed film-height equation on
+// the device: assembly of A, J, I + theta dt J and the right-hand side for
+// every enabled term, the Newton-Kantorovich loop (NewtonKantorovich.cpp:
+// 157-486) and the time-step control (ImplicitSolver.cpp:144-190, 271-307),
+// around the device linear solve of yz_solver.cu.
+#include "yz_physics.cuh"
+#include "yz_step_impl.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+namespace yz {
+
+using namespace phys;
+
+namespace {
+
+__device__ __forceinline__ int Offset(int s, int nx)
+{
+	switch(s)
+	{
+	case oM: return -2 * nx;
+	case mm: return -nx - 1;
+	case om: return -nx;
+	case pm: return -nx + 1;
+	case Mo: return -2;
+	case mo: return -1;
+	case oo: return 0;
+	case po: return 1;
+	case Po: return 2;
+	case mp: return nx - 1;
+	case op: return nx;
+	case pp: return nx + 1;
+	default: return 2 * nx;
+	}
+}
+
+//  non-negative doubles order as their bit patterns
+__device__ __forceinline__ void AtomicMaxAbs(unsigned long long *slot, double v)
+{
+	const double a = fabs(v);
+	atomicMax(slot, (unsigned long long)__double_as_longlong(a));
+}
+
+__device__ __forceinline__ void WarpMaxAbs(unsigned long long *slot, double v)
+{
+	unsigned long long u = (unsigned long long)__double_as_longlong(fabs(v));
+	for(int off = 16; off >= 1; off >>= 1)
+	{
+		const unsigned long long w = __shfl_down_sync(0xffffffffu, u, off);
+		u = w > u ? w : u;
+	}
+	if((threadIdx.x & 31) == 0 && u) atomicMax(slot, u);
+}
+
+//--------------------------------------------------------------------------
+//  One interior row: the A entries of every term, then what the caller
+//  asks for: mode 0 -> A(h) h only (the explicit half and evapOld);
+//  mode 1 -> I + theta dt J, A(h) h, B and the right-hand side.
+//--------------------------------------------------------------------------
+struct RowOut
+{
+	double *ia;        // values of I + theta dt J (storage order)
+	double *ax;        // A(h) h
+	double *evapOld;   // mode 0: written; mode 1: read
+	double *evapB;     // mode 1: the evaporation B took
+	double *rhs;       // mode 1
+	const double *hOld, *axOld;
+	unsigned long long *rhsMax;
+};
+
+__global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ rowptr,
+                          const double *__restrict__ H, const double *__restrict__ C,
+                          const double *__restrict__ S, RowOut o)
+{
+	const int nx = k.nx, ny = k.ny;
+	const int nIn = (nx - 4) * (ny - 4);
+	double rmax = 0.0;
+	for(int t = blockIdx.x * blockDim.x + threadIdx.x; t < nIn; t += gridDim.x * blockDim.x)
+	{
+		const int ix = 2 + t % (nx - 4), iy = 2 + t / (nx - 4);
+		const int i = iy * nx + ix;
+		double h[13], c[13], s[13];
+#pragma unroll
+		for(int q = 0; q < 13; ++q)
+		{
+			const int j = i + Offset(q, nx);
+			h[q] = H[j]; c[q] = C[j]; s[q] = S[j];
+		}
+		const double hoo = h[oo], coo = c[oo];
+		//  face properties
+		double vis[4], sig[4], DL[4], FM[4], Haj[4];
+#pragma unroll
+		for(int d = 0; d < 4; ++d)
+		{
+			const int a = AdjIdx(d);
+			Haj[d] = h[a];
+			const double cfc = 0.5 * (coo + c[a]);
+			vis[d] = Viscosity(k, cfc);
+			sig[d] = SurfaceTension(k, cfc);
+			const double denom = hoo + Haj[d];
+			const double val = k.slip ? FaceDK(k, hoo, Haj[d]) : 2.0 * (hoo * hoo) * (Haj[d] * Haj[d]) / denom;
+			DL[d] = val * sig[d] / vis[d];
+			FM[d] = Face(k, hoo, Haj[d]);
+		}
+		double aA[13], aR[13];
+#pragma unroll
+		for(int q = 0; q < 13; ++q) { aA[q] = 0.0; aR[q] = 0.0; }
+		//  --- LaplacePressureKernel::SetMatrixA (LaplacePressureKernel.h:354-433)
+		if(k.onL)
+		{
+			double Tf[4];
+#pragma unroll
+			for(int d = 0; d < 4; ++d) Tf[d] = DL[d] / hoo;
+			double topo = 0;
+			for(int q = 0; q < 13; ++q)
+			{
+				double cc = 0;
+#pragma unroll
+				for(int d = 0; d < 4; ++d) cc += k.cL[d][q] * Tf[d];
+				topo += cc * s[q];
+			}
+			for(int q = 0; q < 13; ++q)
+			{
+				double val = 0;
+#pragma unroll
+				for(int d = 0; d < 4; ++d) val += k.cL[d][q] * DL[d];
+				if(q == oo) val += topo;
+				aA[q] += k.coefL * val;
+			}
+		}
+		//  --- VerticalGravityKernel::SetMatrixA (VerticalGravityKernel.h)
+		double G[4], Tface[4];
+#pragma unroll
+		for(int d = 0; d < 4; ++d)
+		{
+			G[d] = FM[d] / vis[d];
+			Tface[d] = (FM[d] == 0) ? 0.0 : FM[d] / (hoo + Haj[d]) / vis[d];
+		}
+		if(k.onV)
+		{
+			double Tsum[4], Too = 0;
+#pragma unroll
+			for(int d = 0; d < 4; ++d)
+			{
+				Tsum[d] = 0;
+				for(int q = 0; q < 13; ++q) Tsum[d] += k.cG[d][q] * s[q];
+			}
+#pragma unroll
+			for(int kk = 0; kk < 4; ++kk) { const int dd = StencilDir(kk); Too += Tsum[dd] * Tface[dd]; }
+#pragma unroll
+			for(int d = 0; d < 4; ++d) Tsum[d] *= Tface[d];
+#pragma unroll
+			for(int kk = 0; kk < 5; ++kk)
+			{
+				const int idx = NarrowIdx(kk);
+				double val = 0;
+#pragma unroll
+				for(int d = 0; d < 4; ++d) val += k.cG[d][idx] * G[d];
+				if(idx == oo) val += Too;
+				else val += Tsum[DirOfAdj(idx)];
+				aA[idx] += k.coefV * val;
+			}
+		}
+		//  --- DisjoiningPressureKernel::SetMatrixA (DisjoiningPressureKernel.h:306-349)
+		double piN[13];
+		if(k.onD)
+		{
+#pragma unroll
+			for(int kk = 0; kk < 5; ++kk)
+			{
+				const int idx = NarrowIdx(kk);
+				const double php = PiPerH(k, h[idx]);
+				double val = 0;
+#pragma unroll
+				for(int d = 0; d < 4; ++d) val += k.cG[d][idx] * G[d];
+				val *= php;
+				aR[idx] += k.coefD * val;
+			}
+		}
+		//  A = A + A_rest (HeightEquationBase.h:749-759)
+		double A[13];
+#pragma unroll
+		for(int q = 0; q < 13; ++q) A[q] = aA[q] + aR[q];
+
+		//  --- ApplyA (HeightEquationBase.h:804-827): A_rest h in storage
+		//  order, then the conservative fluxes of the capillary and the
+		//  vertical gravity terms
+		double y = 0.0;
+		y = y + aR[oo] * h[oo];
+		for(int q = 0; q < 13; ++q) if(q != oo) y = y + aR[q] * h[q];
+		if(k.onL)
+		{
+			double r = 0;
+#pragma unroll
+			for(int d = 0; d < 4; ++d)
+			{
+				const double f = k.coefL * (DL[d] * (FaceGradient(k, h, d) + FaceGradient(k, s, d)));
+				r += (d % 2 == 0) ? -f : f;
+			}
+			y += r;
+		}
+		if(k.onV)
+		{
+			double r = 0;
+#pragma unroll
+			for(int d = 0; d < 4; ++d)
+			{
+				const int a = AdjIdx(d);
+				const double hl = (d % 2 == 0) ? h[a] : hoo, hh = (d % 2 == 0) ? hoo : h[a];
+				const double sl = (d % 2 == 0) ? s[a] : s[oo], sh = (d % 2 == 0) ? s[oo] : s[a];
+				const double dn = (d < 2) ? k.dxx : k.dyy;
+				const double mu = vis[d];
+				double gf = Face(k, hl, hh);
+				const double tk = (gf == 0) ? 0.0 : gf / (hl + hh) / mu;
+				gf /= mu;
+				const double f = k.coefV * ((gf * (hh - hl) + (sh - sl) * (tk * (hl + hh))) / (dn * dn));
+				r += (d % 2 == 0) ? -f : f;
+			}
+			y += r;
+		}
+		o.ax[i] = y;
+
+		const double xx = k.x0 + ix * k.dx, yy = k.y0 + iy * k.dy;
+		if(mode == 0)
+		{
+			if(k.onEvap) o.evapOld[i] = EvapAt(k, hoo, coo, xx, yy, dt);
+			continue;
+		}
+
+		//  --- SetMatrixJacobi (HeightEquationBase.h:1062-1091): J = A, then
+		//  every term's Jacobian
+		double J[13];
+#pragma unroll
+		for(int q = 0; q < 13; ++q) J[q] = A[q];
+		if(k.onL)
+		{
+			double a[4], b[4], gAdj[4], gCen[4], sAdj[4], sCen[4];
+#pragma unroll
+			for(int d = 0; d < 4; ++d)
+			{
+				a[d] = 0; b[d] = 0;
+				for(int q = 0; q < 13; ++q) { a[d] += k.cL[d][q] * h[q]; b[d] += k.cL[d][q] * s[q]; }
+				//  NonlinearJacobiProps (LaplacePressureKernel.h:160-175)
+				const double ha = Haj[d];
+				{
+					const double H1 = ha, H2 = hoo;
+					const double den = (H1 + H2) * (H1 + H2);
+					const double val = k.slip ? FaceDK_d1(k, H1, H2) : 2.0 * (H1 * H2 * H2) * (H1 + H2 + H2) / den;
+					gAdj[d] = val * sig[d] / vis[d];
+				}
+				{
+					const double H1 = hoo, H2 = ha;
+					const double den = (H1 + H2) * (H1 + H2);
+					const double val = k.slip ? FaceDK_d1(k, H1, H2) : 2.0 * (H1 * H2 * H2) * (H1 + H2 + H2) / den;
+					gCen[d] = val * sig[d] / vis[d];
+				}
+				sAdj[d] = gAdj[d] / hoo;
+				sCen[d] = gCen[d] / hoo - DL[d] / (hoo * hoo);
+			}
+			double gaSum = 0, sbSum = 0;
+#pragma unroll
+			for(int kk = 0; kk < 4; ++kk) { const int dd = StencilDir(kk); gaSum += gCen[dd] * a[dd]; }
+#pragma unroll
+			for(int d = 0; d < 4; ++d) sbSum += sCen[d] * b[d];
+#pragma unroll
+			for(int kk = 0; kk < 5; ++kk)
+			{
+				const int idx = NarrowIdx(kk);
+				if(idx == oo) J[oo] += k.coefL * (gaSum + sbSum * hoo);
+				else
+				{
+					const int dd = DirOfAdj(idx);
+					J[idx] += k.coefL * (gAdj[dd] * a[dd] + sAdj[dd] * b[dd] * hoo);
+				}
+			}
+		}
+		if(k.onV)
+		{
+			double a[4], b[4], gAdj[4], gCen[4];
+#pragma unroll
+			for(int d = 0; d < 4; ++d)
+			{
+				a[d] = 0; b[d] = 0;
+				for(int q = 0; q < 13; ++q) { a[d] += k.cG[d][q] * h[q]; b[d] += k.cG[d][q] * s[q]; }
+				gAdj[d] = Face_d1(k, Haj[d], hoo) / vis[d];
+				gCen[d] = Face_d1(k, hoo, Haj[d]) / vis[d];
+			}
+			double gaSum = 0;
+#pragma unroll
+			for(int kk = 0; kk < 4; ++kk)
+			{
+				const int dd = StencilDir(kk);
+				gaSum += gCen[dd] * (a[dd] + b[dd]) - Tface[dd] * b[dd];
+			}
+#pragma unroll
+			for(int kk = 0; kk < 5; ++kk)
+			{
+				const int idx = NarrowIdx(kk);
+				if(idx == oo) J[oo] += k.coefV * gaSum;
+				else
+				{
+					const int dd = DirOfAdj(idx);
+					J[idx] += k.coefV * (gAdj[dd] * (a[dd] + b[dd]) - Tface[dd] * b[dd]);
+				}
+			}
+		}
+		if(k.onD)
+		{
+			double Ad[4], gAdj[4], gCen[4];
+#pragma unroll
+			for(int kk = 0; kk < 5; ++kk) { const int idx = NarrowIdx(kk); piN[idx] = Pi(k, h[idx]); }
+#pragma unroll
+			for(int d = 0; d < 4; ++d)
+			{
+				//  only the two non-zero coefficients, in stencil-point order
+				const int a = AdjIdx(d);
+				const int lo = a < oo ? a : oo, hi = a < oo ? oo : a;
+				double acc = 0;
+				acc += k.cG[d][lo] * piN[lo];
+				acc += k.cG[d][hi] * piN[hi];
+				Ad[d] = acc;
+				gAdj[d] = Face_d1(k, Haj[d], hoo) / vis[d];
+				gCen[d] = Face_d1(k, hoo, Haj[d]) / vis[d];
+			}
+			double gaSum = 0, gcSum = 0;
+#pragma unroll
+			for(int kk = 0; kk < 4; ++kk)
+			{
+				const int dd = StencilDir(kk);
+				gaSum += gCen[dd] * Ad[dd];
+				gcSum += G[dd] * k.cG[dd][oo];
+			}
+#pragma unroll
+			for(int kk = 0; kk < 5; ++kk)
+			{
+				const int idx = NarrowIdx(kk);
+				const double hj = h[idx];
+				const double dpi = dPi(k, hj) - PiPerH(k, hj);
+				if(idx == oo) J[oo] += k.coefD * (gaSum + gcSum * dpi);
+				else
+				{
+					const int dd = DirOfAdj(idx);
+					J[idx] += k.coefD * (gAdj[dd] * Ad[dd] + G[dd] * k.cG[dd][idx] * dpi);
+				}
+			}
+		}
+		//  --- MakeMatrix_IA (NewtonKantorovich.cpp:488-510)
+		const int base = rowptr[i];
+		const double td = k.theta * dt;
+		o.ia[base] = 1.0 + td * J[oo];
+#pragma unroll
+		for(int q = 0; q < 13; ++q) if(q != oo) o.ia[base + Pos(q)] = td * J[q];
+		//  --- B (HeightEquationBase.h:771-787) and MakeRHS (:512-523)
+		double evp = 0.0;
+		if(k.onEvap) evp = (1.0 - k.theta) * o.evapOld[i] + k.theta * EvapAt(k, hoo, coo, xx, yy, dt);
+		o.evapB[i] = evp;
+		const double B = evp - 0.0;
+		const double r = o.hOld[i] - hoo - (dt * k.theta * y) - (dt * (1.0 - k.theta) * o.axOld[i]) - dt * B;
+		o.rhs[i] = r;
+		rmax = fmax(rmax, fabs(r));
+	}
+	if(mode == 1) WarpMaxAbs(o.rhsMax, rmax);
+}
+
+//  ghost rows of x satisfied exactly (CRS_Matrix::SatisfyBCRows for rows
+//  [1, -1] with right-hand side 0: x_ghost = x_partner)
+__global__ void KGhostCopy(int nGhost, const int *__restrict__ ghost, const int *__restrict__ partner,
+                           double *__restrict__ x)
+{
+	for(int g = blockIdx.x * blockDim.x + threadIdx.x; g < nGhost; g += gridDim.x * blockDim.x)
+		x[ghost[g]] = x[partner[g]];
+}
+
+__global__ void KAbsMax(int n, const double *__restrict__ x, unsigned long long *out)
+{
+	double m = 0.0;
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = fmax(m, fabs(x[i]));
+	WarpMaxAbs(out, m);
+}
+
+//  phi += delta * alpha (Vector operator+= with Vector * scalar)
+__global__ void KAxpyAlpha(int n, const double *__restrict__ d, double alpha, double *__restrict__ phi)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) phi[i] += d[i] * alpha;
+}
+
+//  opt extrap (NewtonKantorovich.cpp:179-198): g = phi + r (phi - phi2);
+//  ok stays 1 unless a non-ghost cell with liquid would lose it; move = |g - phi|max
+__global__ void KExtrapCheck(int n, const double *__restrict__ phi, const double *__restrict__ phi2,
+                             const unsigned char *__restrict__ isbc, double r, int *notOk, unsigned long long *move)
+{
+	double m = 0.0;
+	int bad = 0;
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		const double g = phi[i] + r * (phi[i] - phi2[i]);
+		if(!isbc[i] && phi[i] > 0 && !(g > 0)) bad = 1;
+		m = fmax(m, fabs(g - phi[i]));
+	}
+	if(bad) atomicExch(notOk, 1);
+	WarpMaxAbs(move, m);
+}
+
+__global__ void KExtrapApply(int n, const double *__restrict__ phi, const double *__restrict__ phi2, double r,
+                             double *__restrict__ guess)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+		guess[i] = phi[i] + r * (phi[i] - phi2[i]);
+}
+
+//  LocalTruncationCriterion (ImplicitSolver.cpp:271-307): max |E_k|
+__global__ void KLte(int n, const double *__restrict__ hp, const double *__restrict__ ho, const double *__restrict__ hm,
+                     double dt0, double dt, double wfloor, unsigned long long *out)
+{
+	double m = 0.0;
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		double w = fabs(ho[i]);
+		if(w < wfloor) w = wfloor;
+		const double denom = (dt0 + dt) * w;
+		const double e = (fabs(denom) <= 2.2250738585072014e-308)   // Math::IsZero
+		    ? 0.0 : 2.0 * (dt / dt0) * (dt0 * hp[i] + dt * hm[i] - (dt0 + dt) * ho[i]) / denom;
+		m = fmax(m, fabs(e));
+	}
+	WarpMaxAbs(out, m);
+}
+
+__global__ void KSetGhostRows(int nGhost, const int *__restrict__ ghost, const int *__restrict__ rowptr,
+                              double *__restrict__ ia, double *__restrict__ rhs)
+{
+	for(int g = blockIdx.x * blockDim.x + threadIdx.x; g < nGhost; g += gridDim.x * blockDim.x)
+	{
+		const int i = ghost[g];
+		ia[rowptr[i]] = 1.0;
+		ia[rowptr[i] + 1] = -1.0;
+		rhs[i] = 0.0;
+	}
+}
+
+int PartnerOf(int a, int n, int bcLo, int bcHi)
+{
+	//  BoundaryCondition::ApplyEdge (BoundaryCondition.cpp:104-187):
+	//  Symmetry mirrors the first two layers, Periodic copies the opposite side
+	if(a < 2) return bcLo == YZ_BC_PERIODIC ? a + (n - 4) : 3 - a;
+	if(a >= n - 2) return bcHi == YZ_BC_PERIODIC ? a - (n - 4) : 2 * (n - 2) - 1 - a;
+	return a;
+}
+
+} // namespace
+
+namespace {
+inline double Bits(unsigned long long u) { double d; std::memcpy(&d, &u, sizeof d); return d; }
+
+} // namespace
+
+//==========================================================================
+//  Step
+//==========================================================================
+Step::Step(int device, const yz_step_params &p, const double *h, const double *c, const double *s)
+    : _device(device), _p(p)
+{
+	CheckParams(p);
+	if(p.on_pgrav || p.on_marangoni || p.on_centrifugal)
+		throw UsageError("step: the upwinded terms (HorizontalGravity, SolutoCapillarity, Centrifugal) are not built");
+	if(p.conc_field != 0) throw UsageError("step: the concentration equation (ConcField = WM) is not built");
+	if(p.theta <= 0.0) throw UsageError("step: theta must be > 0 (the implicit scheme)");
+	YZ_CUDA(cudaSetDevice(device));
+	_solver.reset(new Solver(device));
+	_st = _solver->Stream();
+	YZ_CUDA(cudaEventCreate(&_e0)); YZ_CUDA(cudaEventCreate(&_e1));
+	const int nx = p.nx, ny = p.ny;
+	_n = nx * ny;
+	BuildPattern();
+	BuildCoef();
+	const size_t n = (size_t)_n;
+	for(DBuf<double> *v : {&_h, &_c, &_s, &_hOld, &_hOld2, &_hNew, &_guess, &_axOld, &_axGuess, &_rhs, &_delta,
+	                       &_evapOld, &_evapB})
+	{
+		v->reserve(n);
+		YZ_CUDA(cudaMemsetAsync(v->get(), 0, n * sizeof(double), _st));
+	}
+	_ia.reserve((size_t)_nnz);
+	YZ_CUDA(cudaMemsetAsync(_ia.get(), 0, (size_t)_nnz * sizeof(double), _st));
+	_h.upload(h, n, _st); _c.upload(c, n, _st); _s.upload(s, n, _st);
+	//  C_ImplicitSolver::SetX: phi_old = phi_old2 = phi_new = h
+	YZ_CUDA(cudaMemcpyAsync(_hOld.get(), h, n * sizeof(double), cudaMemcpyHostToDevice, _st));
+	YZ_CUDA(cudaMemcpyAsync(_hOld2.get(), h, n * sizeof(double), cudaMemcpyHostToDevice, _st));
+	YZ_CUDA(cudaMemcpyAsync(_hNew.get(), h, n * sizeof(double), cudaMemcpyHostToDevice, _st));
+	_red.reserve(8);
+	_dt = p.dt; _dtOld = p.dt; _time = p.t_start;
+	YZ_LAUNCH(KSetGhostRows, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
+	          _dRowptr.get(), _ia.get(), _rhs.get());
+	YZ_CUDA(cudaStreamSynchronize(_st));
+}
+
+Step::~Step()
+{
+	cudaSetDevice(_device);
+	if(_st) cudaStreamSynchronize(_st);
+	cudaEventDestroy(_e0); cudaEventDestroy(_e1);
+}
+
+//  The pattern the reference fixes in C_ImplicitSolver::Alloc
+//  (ImplicitSolver.cpp:60-81): ghost rows [diag, partner] (EqualVal,
+//  BoundaryCondition.cpp:81-86), interior rows the capillary term's 13 points
+//  in FullIdx order with the diagonal first.
+void BuildPattern2D(const yz_step_params &p, std::vector<int> &rowptr, std::vector<int> &col,
+                    std::vector<int> &isbc, std::vector<int> &ghost, std::vector<int> &partner)
+{
+	const int nx = p.nx, ny = p.ny, n = nx * ny;
+	rowptr.assign((size_t)n + 1, 0);
+	col.clear(); isbc.assign((size_t)n, 0);
+	ghost.clear(); partner.clear();
+	static const int off[13][2] = {{0, -2}, {-1, -1}, {0, -1}, {1, -1}, {-2, 0}, {-1, 0}, {0, 0}, {1, 0}, {2, 0},
+	                               {-1, 1}, {0, 1}, {1, 1}, {0, 2}};
+	for(int iy = 0; iy < ny; ++iy)
+		for(int ix = 0; ix < nx; ++ix)
+		{
+			const int i = iy * nx + ix;
+			const bool inside = ix >= 2 && ix < nx - 2 && iy >= 2 && iy < ny - 2;
+			if(inside)
+			{
+				col.push_back(i);
+				for(int q = 0; q < 13; ++q)
+					if(q != oo) col.push_back((iy + off[q][1]) * nx + ix + off[q][0]);
+			}
+			else
+			{
+				isbc[(size_t)i] = 1;
+				const int px = PartnerOf(ix, nx, p.bc[0], p.bc[1]);
+				const int py = PartnerOf(iy, ny, p.bc[2], p.bc[3]);
+				const int j = py * nx + px;
+				col.push_back(i);
+				col.push_back(j);
+				ghost.push_back(i);
+				partner.push_back(j);
+			}
+			rowptr[(size_t)i + 1] = (int)col.size();
+		}
+}
+
+void CheckParams(const yz_step_params &p)
+{
+	if(p.nx < 8 || p.ny < 8) throw UsageError("step: the grid needs at least 4 x 4 cells");
+	for(int e = 0; e < 4; ++e)
+		if(p.bc[e] != YZ_BC_SYMMETRY && p.bc[e] != YZ_BC_PERIODIC)
+			throw UsageError("step: only Symmetry and Periodic edges are supported");
+	if((p.bc[0] == YZ_BC_PERIODIC) != (p.bc[1] == YZ_BC_PERIODIC) || (p.bc[2] == YZ_BC_PERIODIC) != (p.bc[3] == YZ_BC_PERIODIC))
+		throw UsageError("step: a Periodic edge needs a Periodic opposite edge");
+	if(!p.on_laplace) throw UsageError("step: the capillary term (Physics.LaplacePressure) must be enabled");
+}
+
+void Step::BuildPattern()
+{
+	BuildPattern2D(_p, _rowptr, _col, _isbc, _ghost, _partner);
+	_nnz = (int)_col.size();
+	//  the sorted mirror (CRS_Matrix::BuildSortPermutation, CRS_Matrix.cpp:360-384)
+	std::vector<int> scol((size_t)_nnz), ssrc((size_t)_nnz);
+	std::vector<std::pair<int, int>> tmp;
+	for(int i = 0; i < _n; ++i)
+	{
+		const int st = _rowptr[(size_t)i], ed = _rowptr[(size_t)i + 1];
+		tmp.clear();
+		for(int q = st; q < ed; ++q) tmp.push_back({_col[(size_t)q], q});
+		std::sort(tmp.begin(), tmp.end());
+		for(int q = st; q < ed; ++q) { scol[(size_t)q] = tmp[(size_t)(q - st)].first; ssrc[(size_t)q] = tmp[(size_t)(q - st)].second; }
+	}
+	_solver->SetPattern(_n, _nnz, _rowptr.data(), scol.data(), ssrc.data());
+	_dRowptr.upload(_rowptr.data(), _rowptr.size(), _st);
+	std::vector<unsigned char> bc8(_isbc.begin(), _isbc.end());
+	_dIsbc.upload(bc8.data(), bc8.size(), _st);
+	_dGhost.upload(_ghost.data(), _ghost.size(), _st);
+	_dPartner.upload(_partner.data(), _partner.size(), _st);
+}
+
+//  The coefficient tables, computed as the reference's SetLinearCoef does
+void Step::BuildCoef()
+{
+	Coef &k = _k;
+	std::memset(&k, 0, sizeof k);
+	const yz_step_params &p = _p;
+	k.nx = p.nx; k.ny = p.ny;
+	k.onL = p.on_laplace; k.onV = p.on_vgrav; k.onD = p.on_disjoining; k.onEvap = p.on_evap;
+	k.theta = p.theta;
+	const double dx = p.dx, dy = p.dy;
+	const double dx2 = dx * dx, dy2 = dy * dy, dx4 = dx2 * dx2, dy4 = dy2 * dy2, dx2dy2 = dx2 * dy2;
+	double (*C)[13] = k.cL;
+	C[0][mm] = +1.0 / dx2dy2; C[0][om] = -1.0 / dx2dy2; C[0][Mo] = +1.0 / dx4;
+	C[0][mo] = 1.0 * (-3.0 / dx4 - 2.0 / dx2dy2); C[0][oo] = 1.0 * (+3.0 / dx4 + 2.0 / dx2dy2);
+	C[0][po] = -1.0 / dx4; C[0][mp] = +1.0 / dx2dy2; C[0][op] = -1.0 / dx2dy2;
+	C[1][om] = -1.0 / dx2dy2; C[1][pm] = +1.0 / dx2dy2; C[1][mo] = -1.0 / dx4;
+	C[1][oo] = 1.0 * (+3.0 / dx4 + 2.0 / dx2dy2); C[1][po] = 1.0 * (-3.0 / dx4 - 2.0 / dx2dy2);
+	C[1][Po] = +1.0 / dx4; C[1][op] = -1.0 / dx2dy2; C[1][pp] = +1.0 / dx2dy2;
+	C[2][oM] = +1.0 / dy4; C[2][mm] = +1.0 / dx2dy2; C[2][om] = 1.0 * (-3.0 / dy4 - 2.0 / dx2dy2);
+	C[2][pm] = +1.0 / dx2dy2; C[2][mo] = -1.0 / dx2dy2; C[2][oo] = 1.0 * (+3.0 / dy4 + 2.0 / dx2dy2);
+	C[2][po] = -1.0 / dx2dy2; C[2][op] = -1.0 / dy4;
+	C[3][om] = -1.0 / dy4; C[3][mo] = -1.0 / dx2dy2; C[3][oo] = 1.0 * (+3.0 / dy4 + 2.0 / dx2dy2);
+	C[3][po] = -1.0 / dx2dy2; C[3][mp] = +1.0 / dx2dy2; C[3][op] = 1.0 * (-3.0 / dy4 - 2.0 / dx2dy2);
+	C[3][pp] = +1.0 / dx2dy2; C[3][oP] = +1.0 / dy4;
+	static const int adj[4] = {mo, po, om, op};
+	for(int d = 0; d < 4; ++d)
+	{
+		const double hs = (d / 2 == 0) ? dx : dy;
+		const double h2 = hs * hs;
+		k.cG[d][adj[d]] = +1.0 / h2;
+		k.cG[d][oo] = -1.0 / h2;
+	}
+	k.coefL = 1.0 / 3.0;
+	k.coefV = -1.0 * p.Bo / 3.0;
+	k.coefD = p.Dp / 3.0;
+	k.dx2 = dx2; k.dy2 = dy2; k.dx4 = dx4; k.dy4 = dy4; k.dx2dy2 = dx2dy2; k.dxx = dx; k.dyy = dy;
+	k.hstar = p.hstar; k.pn = p.disj_n; k.pm = p.disj_m;
+	k.slip = p.lambda_slip > 0;
+	k.lam = p.lambda_slip > 0 ? p.lambda_slip : 0.0;
+	k.a3 = 3.0 * k.lam;
+	k.viscC0 = p.visc_c0; k.viscBase = p.visc_base; k.viscExp = p.visc_exp;
+	k.sigC0 = p.sig_c0; k.sigBase = p.sig_base; k.sigCoef = p.sig_coef;
+	k.Ev = p.Ev;
+	k.evConc = p.ev_conc_func; k.evSpatial = p.ev_spatial; k.evHast = p.ev_hast_modify;
+	k.evMr = p.ev_m_resin; k.evMs = p.ev_m_solvent; k.evPowN = p.ev_power_n; k.evConcR = p.ev_conc_r;
+	k.evNegExp = p.ev_negpow_exp; k.evNegRmax = p.ev_negpow_rmax; k.evHast_h = p.ev_h_ast;
+	k.evDr = dx < dy ? dx : dy;
+	k.x0 = p.x0; k.y0 = p.y0; k.dx = dx; k.dy = dy;
+}
+
+double Step::ReadMax(int slot)
+{
+	unsigned long long u = 0;
+	YZ_CUDA(cudaMemcpyAsync(&u, _red.get() + slot, sizeof(u), cudaMemcpyDeviceToHost, _st));
+	YZ_CUDA(cudaStreamSynchronize(_st));
+	return Bits(u);
+}
+
+void Step::ZeroMax(int slot) { YZ_CUDA(cudaMemsetAsync(_red.get() + slot, 0, sizeof(unsigned long long), _st)); }
+
+void Step::Assemble(int mode, const double *hField, double dt)
+{
+	RowOut o;
+	o.ia = _ia.get(); o.ax = mode == 0 ? _axOld.get() : _axGuess.get();
+	o.evapOld = _evapOld.get(); o.evapB = _evapB.get(); o.rhs = _rhs.get();
+	o.hOld = _hOld.get(); o.axOld = _axOld.get(); o.rhsMax = _red.get() + kSlotRhs;
+	const int nIn = (_p.nx - 4) * (_p.ny - 4);
+	YZ_LAUNCH(KAssemble, GridFor(nIn, 128, 148 * 32), 128, 0, _st, _k, mode, dt, _dRowptr.get(), hField, _c.get(),
+	          _s.get(), o);
+}
+
+//  one Newton-Kantorovich attempt at the present dt (NKLoop)
+bool Step::NKLoop(int &iter, double &resid, yz_step_stats &stats)
+{
+	const int n = _n, g = GridFor(n, 256);
+	const double dt = _dt;
+	_nkIter = 0;
+	YZ_CUDA(cudaMemcpyAsync(_guess.get(), _hOld.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+	//  opt extrap
+	_extrapMove = 0;
+	if(!_extrapBlocked)
+	{
+		const double r = (_dtOld > 0) ? dt / _dtOld : 0.0;
+		if(r > 0)
+		{
+			ZeroMax(kSlotMove);
+			int *bad = reinterpret_cast<int *>(_red.get() + kSlotBad);
+			YZ_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), _st));
+			YZ_LAUNCH(KExtrapCheck, g, 256, 0, _st, n, _hOld.get(), _hOld2.get(), _dIsbc.get(), r, bad, _red.get() + kSlotMove);
+			const double move = ReadMax(kSlotMove);
+			int hbad = 0;
+			YZ_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, _st));
+			YZ_CUDA(cudaStreamSynchronize(_st));
+			if(!hbad && move > 0)
+			{
+				YZ_LAUNCH(KExtrapApply, g, 256, 0, _st, n, _hOld.get(), _hOld2.get(), r, _guess.get());
+				_extrapMove = move;
+			}
+		}
+	}
+	//  BeforeNKLoop: the working field is the committed one; SetMatrixA and
+	//  A(h^n) h^n with evapOld at h^n
+	Assemble(0, _hOld.get(), dt);
+
+	double residEqOld = 1e40, residFirst = 0, residBest = 1e40;
+	int stall = 0;
+	const int stallLimit = 5;
+	bool done = false;
+	int outer;
+	for(outer = 0; outer < _p.nk_max; ++outer)
+	{
+		//  EveryNKLoop: the working field's h is phi_guess (no concentration
+		//  equation here); Solve(): assembly at it
+		ZeroMax(kSlotRhs);
+		YZ_CUDA(cudaEventRecord(_e0, _st));
+		Assemble(1, _guess.get(), dt);
+		YZ_CUDA(cudaEventRecord(_e1, _st));
+		++_nkIter;
+		//  opt ew (NewtonKantorovich.cpp:108-126)
+		double eps = _p.lin.epsilon;
+		{
+			const double kEtaMax = 1.0e-4;
+			const double rn = ReadMax(kSlotRhs);
+			float ams = 0; YZ_CUDA(cudaEventElapsedTime(&ams, _e0, _e1)); stats.assemble_ms += ams;
+			double eta = kEtaMax;
+			if(_nkIter > 1 && _ewRhsPrev > 0)
+			{
+				const double ratio = rn / _ewRhsPrev;
+				eta = 0.9 * ratio * ratio;
+				const double safe = 0.9 * _ewEta * _ewEta;
+				if(safe > 0.1 && safe > eta) eta = safe;
+			}
+			if(eta > kEtaMax) eta = kEtaMax;
+			if(eta < _p.lin.epsilon) eta = _p.lin.epsilon;
+			_ewEta = eta;
+			_ewRhsPrev = rn;
+			eps = eta;
+		}
+		yz_settings ls = _p.lin;
+		ls.epsilon = eps;
+		ls.conc = 0;
+		int it = 0; double res = 0;
+		const int ch = _solver->Solve(ls, _ia.get(), _rhs.get(), _delta.get(), it, res);
+		double su = 0, sit = 0; _solver->Timing(&su, &sit);
+		stats.setup_ms += su; stats.solve_ms += sit;
+		stats.linear_iterations += it;
+		ZeroMax(kSlotDelta);
+		if(ch == 0)
+		{
+			YZ_LAUNCH(KGhostCopy, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
+			          _dPartner.get(), _delta.get());
+		}
+		else YZ_CUDA(cudaMemsetAsync(_delta.get(), 0, (size_t)n * sizeof(double), _st));
+		YZ_LAUNCH(KAbsMax, g, 256, 0, _st, n, _delta.get(), _red.get() + kSlotDelta);
+		double residEq = ReadMax(kSlotDelta);
+		_lastResid = residEq;
+		if(ch != 0) { done = false; break; }
+		if(outer == 0) residFirst = residEq;
+		if(residEq < residBest * 0.9) { residBest = residEq; stall = 0; }
+		else ++stall;
+		if(stall > stallLimit)
+		{
+			ZeroMax(kSlotPhi);
+			YZ_LAUNCH(KAbsMax, g, 256, 0, _st, n, _guess.get(), _red.get() + kSlotPhi);
+			const double floorPhi = 1000.0 * std::numeric_limits<double>::epsilon() * ReadMax(kSlotPhi);
+			const bool solved = (residEq < _p.nk_eps) || (residFirst > 0 && residEq < residFirst * 1.0e-4) || (residEq <= floorPhi);
+			done = solved;
+			break;
+		}
+		const double alpha = (residEq > residEqOld) ? 0.5 : 1.0;
+		YZ_LAUNCH(KAxpyAlpha, g, 256, 0, _st, n, _delta.get(), alpha, _guess.get());
+		if(outer >= _p.nk_min - 1)
+		{
+			if(residEq < _p.nk_eps) { done = true; break; }
+			if(_p.nk_eps_rel > 0 && residFirst > 0 && residEq < residFirst * _p.nk_eps_rel) { done = true; break; }
+		}
+		residEqOld = residEq;
+	}
+	iter = outer + 1;
+	resid = _lastResid;
+	return done;
+}
+
+//  TimeAdvance (NewtonKantorovich.cpp:424-486) and the clock (TimeSteps.cpp:121-160)
+void Step::Advance(int nsteps, yz_step_stats &stats)
+{
+	YZ_CUDA(cudaSetDevice(_device));
+	const size_t bytes = (size_t)_n * sizeof(double);
+	const int g = GridFor(_n, 256);
+	for(int step = 0; step < nsteps; ++step)
+	{
+		YZ_CUDA(cudaMemcpyAsync(_hOld2.get(), _hOld.get(), bytes, cudaMemcpyDeviceToDevice, _st));
+		YZ_CUDA(cudaMemcpyAsync(_hOld.get(), _hNew.get(), bytes, cudaMemcpyDeviceToDevice, _st));
+		bool timeStepDone = false;
+		int iter = 0;
+		double resid = 0;
+		do
+		{
+			bool ch = NKLoop(iter, resid, stats);
+			stats.newton_iterations += iter;
+			if(!ch && _extrapMove > 0)
+			{
+				_extrapBlocked = true;
+				ch = NKLoop(iter, resid, stats);
+				stats.newton_iterations += iter;
+				_extrapBlocked = false;
+			}
+			if(_p.dt_control)
+			{
+				double criterion = -1;
+				if(ch)
+				{
+					//  LocalTruncationCriterion(phi_guess)
+					double th = _p.dt_criterion;
+					if(std::fabs(th) <= std::numeric_limits<double>::min()) th = 1.0e-2;
+					if(std::fabs(_dtOld) <= std::numeric_limits<double>::min()) criterion = 1.0;
+					else
+					{
+						ZeroMax(kSlotPhi);
+						YZ_LAUNCH(KAbsMax, g, 256, 0, _st, _n, _hOld.get(), _red.get() + kSlotPhi);
+						const double wfloor = _p.dt_scale_floor * ReadMax(kSlotPhi);
+						ZeroMax(kSlotLte);
+						YZ_LAUNCH(KLte, g, 256, 0, _st, _n, _guess.get(), _hOld.get(), _hOld2.get(), _dtOld, _dt, wfloor,
+						          _red.get() + kSlotLte);
+						criterion = 1.0 - ReadMax(kSlotLte) / th;
+					}
+				}
+				//  TimeStepAdjustment (ImplicitSolver.cpp:144-190)
+				double dtNext = _dt;
+				if(criterion > 0.0)
+				{
+					timeStepDone = true;
+					if(criterion > 0.90 && dtNext < _p.dt_max)
+					{
+						if(++_adjustCount >= _p.dt_keep_steps)
+						{
+							_adjustCount = 0;
+							dtNext /= _p.dt_change_factor;
+							if(dtNext > _p.dt_max) dtNext = _p.dt_max;
+							if(!(dtNext < _p.dt_min || _p.dt_max < dtNext)) _pendingDt = dtNext;
+						}
+					}
+				}
+				else
+				{
+					dtNext *= _p.dt_change_factor;
+					if(dtNext < _p.dt_min) throw CudaError("step: dt fell below Numerics.TimeStepControl.MinDt");
+					if(!(dtNext < _p.dt_min || _p.dt_max < dtNext)) _dt = dtNext;
+					++stats.retries;
+				}
+			}
+			else
+			{
+				if(!ch) throw CudaError("step: the Newton iteration did not converge at the fixed step");
+				timeStepDone = true;
+			}
+		} while(!timeStepDone);
+		YZ_CUDA(cudaMemcpyAsync(_hNew.get(), _guess.get(), bytes, cudaMemcpyDeviceToDevice, _st));
+		//  AfterNKLoop without the concentration: the field takes the film
+		YZ_CUDA(cudaMemcpyAsync(_h.get(), _guess.get(), bytes, cudaMemcpyDeviceToDevice, _st));
+		//  the clock: ++ (TimeSteps.cpp:121-160)
+		_time += _dt;
+		_dtOld = _dt;
+		if(_pendingDt > 0) { _dt = _pendingDt; _pendingDt = 0; }
+		stats.steps += 1;
+		stats.last_resid = resid;
+	}
+	stats.time = _time;
+	stats.dt = _dt;
+	YZ_CUDA(cudaStreamSynchronize(_st));
+}
+
+void Step::GetFields(double *h, double *c)
+{
+	YZ_CUDA(cudaSetDevice(_device));
+	if(h) _h.download(h, (size_t)_n, _st);
+	if(c) _c.download(c, (size_t)_n, _st);
+	YZ_CUDA(cudaStreamSynchronize(_st));
+}
+
+int Step::Pattern(int *rowptr, int *col, int *bc) const
+{
+	if(rowptr) std::copy(_rowptr.begin(), _rowptr.end(), rowptr);
+	if(col) std::copy(_col.begin(), _col.end(), col);
+	if(bc) for(int i = 0; i < _n; ++i) bc[i] = _isbc[(size_t)i];
+	return _nnz;
+}
+
+void Step::System(const double *hOld, const double *h, double dt, double *ia, double *rhs)
+{
+	YZ_CUDA(cudaSetDevice(_device));
+	const size_t bytes = (size_t)_n * sizeof(double);
+	YZ_CUDA(cudaMemcpyAsync(_hOld.get(), hOld, bytes, cudaMemcpyHostToDevice, _st));
+	YZ_CUDA(cudaMemcpyAsync(_guess.get(), h, bytes, cudaMemcpyHostToDevice, _st));
+	Assemble(0, _hOld.get(), dt);
+	ZeroMax(kSlotRhs);
+	Assemble(1, _guess.get(), dt);
+	_ia.download(ia, (size_t)_nnz, _st);
+	_rhs.download(rhs, (size_t)_n, _st);
+	YZ_CUDA(cudaStreamSynchronize(_st));
+}
+
+} // namespace yz

@@ -1,0 +1,59 @@
+// yz_step_impl.h -- the device step context behind yz_step_* (C ABI).
+#pragma once
+
+#include "yz_physics.cuh"
+#include "yz_solver_impl.h"
+
+#include <memory>
+#include <vector>
+
+namespace yz {
+
+void BuildPattern2D(const yz_step_params &p, std::vector<int> &rowptr, std::vector<int> &col,
+                    std::vector<int> &isbc, std::vector<int> &ghost, std::vector<int> &partner);
+void CheckParams(const yz_step_params &p);
+
+class Step
+{
+public:
+	Step(int device, const yz_step_params &p, const double *h, const double *c, const double *s);
+	~Step();
+	void Advance(int nsteps, yz_step_stats &stats);
+	void GetFields(double *h, double *c);
+	int Pattern(int *rowptr, int *col, int *bc) const;
+	void System(const double *hOld, const double *h, double dt, double *ia, double *rhs);
+	long long Launches() const { return _solver->Launches(); }
+	int Rows() const { return _n; }
+	int Nnz() const { return _nnz; }
+
+private:
+	enum { kSlotRhs = 0, kSlotDelta = 1, kSlotPhi = 2, kSlotMove = 3, kSlotLte = 4, kSlotBad = 5 };
+	void BuildPattern();
+	void BuildCoef();
+	void Assemble(int mode, const double *hField, double dt);
+	bool NKLoop(int &iter, double &resid, yz_step_stats &stats);
+	double ReadMax(int slot);
+	void ZeroMax(int slot);
+
+	int _device;
+	yz_step_params _p;
+	phys::Coef _k;
+	std::unique_ptr<Solver> _solver;
+	cudaStream_t _st = nullptr;
+	cudaEvent_t _e0 = nullptr, _e1 = nullptr;
+	int _n = 0, _nnz = 0;
+	std::vector<int> _rowptr, _col, _isbc, _ghost, _partner;
+	DBuf<int> _dRowptr, _dGhost, _dPartner;
+	DBuf<unsigned char> _dIsbc;
+	//  fields: the committed film h (field), c, s; phi_old, phi_old2, phi_new,
+	//  phi_guess; A h at phi_old and at the guess; the system
+	DBuf<double> _h, _c, _s, _hOld, _hOld2, _hNew, _guess, _axOld, _axGuess, _rhs, _delta, _evapOld, _evapB, _ia;
+	DBuf<unsigned long long> _red;
+	//  the clock (C_TimeSteps) and the Newton state
+	double _dt = 0, _dtOld = 0, _time = 0, _pendingDt = 0;
+	int _adjustCount = 0, _nkIter = 0;
+	double _ewEta = 0, _ewRhsPrev = 0, _extrapMove = 0, _lastResid = 0;
+	bool _extrapBlocked = false;
+};
+
+} // namespace yz

@@ -1,0 +1,170 @@
+"""ctypes binding of the whole-step seam of include/yuzen_b200.h (yz_step_*):
+the implicit time step of the well-mixed film-height equation on the device,
+C_NewtonKantorovich::TimeAdvance (NewtonKantorovich.cpp:424-486) with the
+hooks of WellMixed_HeightEquationBase, in the reference's non-dimensional
+variables."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _Settings, _check, _fp, _ip, lib
+
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+class StepParams(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("bc", ctypes.c_int * 4),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("x0", ctypes.c_double), ("y0", ctypes.c_double),
+        ("theta", ctypes.c_double),
+        ("on_laplace", ctypes.c_int), ("on_vgrav", ctypes.c_int), ("on_pgrav", ctypes.c_int),
+        ("on_marangoni", ctypes.c_int), ("on_centrifugal", ctypes.c_int), ("on_disjoining", ctypes.c_int),
+        ("on_evap", ctypes.c_int), ("conc_field", ctypes.c_int),
+        ("Bo", ctypes.c_double), ("Dp", ctypes.c_double), ("hstar", ctypes.c_double), ("disj_n", ctypes.c_double),
+        ("disj_m", ctypes.c_double), ("lambda_slip", ctypes.c_double), ("Ev", ctypes.c_double),
+        ("visc_c0", ctypes.c_double), ("visc_base", ctypes.c_double), ("visc_exp", ctypes.c_double),
+        ("sig_c0", ctypes.c_double), ("sig_base", ctypes.c_double), ("sig_coef", ctypes.c_double),
+        ("ev_conc_func", ctypes.c_int), ("ev_spatial", ctypes.c_int), ("ev_hast_modify", ctypes.c_int),
+        ("ev_m_resin", ctypes.c_double), ("ev_m_solvent", ctypes.c_double), ("ev_power_n", ctypes.c_double),
+        ("ev_conc_r", ctypes.c_double), ("ev_negpow_exp", ctypes.c_double), ("ev_negpow_rmax", ctypes.c_double),
+        ("ev_h_ast", ctypes.c_double),
+        ("nk_max", ctypes.c_int), ("nk_min", ctypes.c_int), ("nk_eps", ctypes.c_double), ("nk_eps_rel", ctypes.c_double),
+        ("lin", _Settings),
+        ("dt_control", ctypes.c_int), ("dt_keep_steps", ctypes.c_int),
+        ("dt", ctypes.c_double), ("dt_max", ctypes.c_double), ("dt_min", ctypes.c_double),
+        ("dt_change_factor", ctypes.c_double), ("dt_criterion", ctypes.c_double), ("dt_scale_floor", ctypes.c_double),
+        ("t_start", ctypes.c_double),
+    ]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [
+        ("steps", ctypes.c_int), ("newton_iterations", ctypes.c_int), ("linear_iterations", ctypes.c_int),
+        ("retries", ctypes.c_int), ("time", ctypes.c_double), ("dt", ctypes.c_double),
+        ("last_resid", ctypes.c_double), ("setup_ms", ctypes.c_double), ("solve_ms", ctypes.c_double),
+        ("assemble_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def params_from_state(d: dict) -> StepParams:
+    """The step parameters of a case as the reference's model holds them
+    (the dict of the whole-step probe, tests/golden/stateio.py, or of
+    yuzen_b200.cases)."""
+    p = StepParams()
+    p.nx, p.ny = d["nx"], d["ny"]
+    for e, k in enumerate(("bc_xmin", "bc_xmax", "bc_ymin", "bc_ymax")):
+        p.bc[e] = d[k]
+    p.dx, p.dy, p.x0, p.y0, p.theta = d["dx"], d["dy"], d["x0"], d["y0"], d["theta"]
+    p.on_laplace, p.on_vgrav, p.on_pgrav = d["on_laplace"], d["on_vgrav"], d["on_pgrav"]
+    p.on_marangoni, p.on_centrifugal, p.on_disjoining = d["on_marangoni"], d["on_centrifugal"], d["on_disjoining"]
+    p.on_evap, p.conc_field = d["on_evap"], d["conc_field"]
+    p.Bo, p.Dp, p.hstar = d["Bo"], d["Dp"], d["disj_hstar"]
+    p.disj_n, p.disj_m, p.lambda_slip, p.Ev = d["disj_n"], d["disj_m"], d["lambda"], d["Ev"]
+    p.visc_c0, p.visc_base, p.visc_exp = d["visc_c0"], d["visc_base"], d["visc_exp"]
+    p.sig_c0, p.sig_base, p.sig_coef = d["sig_c0"], d["sig_base"], d["sig_coef"]
+    p.ev_conc_func, p.ev_spatial, p.ev_hast_modify = d["evap_conc_func"], d["evap_spatial"], d["evap_hast_modify"]
+    p.ev_m_resin, p.ev_m_solvent, p.ev_power_n = d["ev_m_resin"], d["ev_m_solvent"], d["ev_power_n"]
+    p.ev_conc_r, p.ev_negpow_exp, p.ev_negpow_rmax = d["ev_conc_r"], d["ev_negpow_exp"], d["ev_negpow_rmax"]
+    p.ev_h_ast = d["ev_h_ast"]
+    p.nk_max, p.nk_min, p.nk_eps, p.nk_eps_rel = d["nk_max"], d["nk_min"], d["nk_eps"], d["nk_eps_rel"]
+    p.lin = _Settings(d["lin_precond"], d["lin_scaling"], d["lin_maxit"], d["lin_eps"], 0)
+    p.dt_control, p.dt_keep_steps = d["dt_control"], d["dt_keep_steps"]
+    p.dt, p.dt_max, p.dt_min = d["dt"], d["dt_max"], d["dt_min"]
+    p.dt_change_factor, p.dt_criterion, p.dt_scale_floor = d["dt_change_factor"], d["dt_criterion"], d["dt_scale_floor"]
+    p.t_start = d["t_start"]
+    return p
+
+
+_BOUND = False
+
+
+def _bind():
+    global _BOUND
+    if _BOUND:
+        return lib()
+    L = lib()
+    L.yz_step_create.argtypes = [ctypes.c_int, ctypes.POINTER(StepParams), _f64p, _f64p, _f64p,
+                                 ctypes.POINTER(ctypes.c_void_p)]
+    L.yz_step_destroy.argtypes = [ctypes.c_void_p]
+    L.yz_step_advance.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(StepStats)]
+    L.yz_step_get_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
+    L.yz_step_pattern.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_int)]
+    L.yz_step_system.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_double, _f64p, _f64p]
+    L.yz_pattern_2d.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(ctypes.c_int),
+                                ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    _BOUND = True
+    return L
+
+
+class Step:
+    """The device step of one case: Step(params, h, c, s); advance(n)."""
+
+    def __init__(self, params: StepParams, h, c, s, device: int = 0):
+        L = _bind()
+        self.params = params
+        self.n = params.nx * params.ny
+        h, c, s = (np.ascontiguousarray(a, np.float64) for a in (h, c, s))
+        if not (h.size == c.size == s.size == self.n):
+            raise ValueError("h, c and s need nx*ny values each")
+        self._h = ctypes.c_void_p()
+        _check(L.yz_step_create(device, ctypes.byref(params), _fp(h), _fp(c), _fp(s), ctypes.byref(self._h)),
+               "yz_step_create")
+
+    def advance(self, nsteps: int = 1) -> dict:
+        st = StepStats()
+        _check(lib().yz_step_advance(self._h, nsteps, ctypes.byref(st)), "yz_step_advance")
+        return st.as_dict()
+
+    def fields(self):
+        h = np.zeros(self.n)
+        c = np.zeros(self.n)
+        _check(lib().yz_step_get_fields(self._h, _fp(h), _fp(c)), "yz_step_get_fields")
+        return h, c
+
+    def pattern(self):
+        L = lib()
+        nnz = _check(L.yz_step_pattern(self._h, None, None, None), "yz_step_pattern")
+        rowptr = np.zeros(self.n + 1, np.int32)
+        col = np.zeros(nnz, np.int32)
+        bc = np.zeros(self.n, np.int32)
+        _check(L.yz_step_pattern(self._h, _ip(rowptr), _ip(col), _ip(bc)), "yz_step_pattern")
+        return rowptr, col, bc
+
+    def system(self, h_old, h, dt: float):
+        h_old = np.ascontiguousarray(h_old, np.float64)
+        h = np.ascontiguousarray(h, np.float64)
+        rowptr, col, bc = self.pattern()
+        ia = np.zeros(col.size)
+        rhs = np.zeros(self.n)
+        _check(lib().yz_step_system(self._h, _fp(h_old), _fp(h), float(dt), _fp(ia), _fp(rhs)), "yz_step_system")
+        return ia, rhs
+
+    def close(self) -> None:
+        if self._h:
+            lib().yz_step_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pattern_2d(params: StepParams):
+    """The CRS pattern of the step, built on the host (no device needed):
+    (rowptr, col, bc)."""
+    L = _bind()
+    nnz = _check(L.yz_pattern_2d(ctypes.byref(params), None, None, None), "yz_pattern_2d")
+    n = params.nx * params.ny
+    rowptr = np.zeros(n + 1, np.int32)
+    col = np.zeros(nnz, np.int32)
+    bc = np.zeros(n, np.int32)
+    _check(L.yz_pattern_2d(ctypes.byref(params), _ip(rowptr), _ip(col), _ip(bc)), "yz_pattern_2d")
+    return rowptr, col, bc
