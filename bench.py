@@ -1,0 +1,297 @@
+#!/usr/bin/env python
+"""bench.py -- time steps per second of the implicit step of the well-mixed
+film-height equation on B200, next to the reference's CPU solver.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME]
+    python bench.py --impl reference ...      # the reference's CPU solver
+
+A step is one time step of the case (C_NewtonKantorovich::TimeAdvance and
+the clock, NewtonKantorovich.cpp:424-486): assembly, Newton passes, one
+BiCGStab + SA-AMG(SPAI0) solve per pass, all on the device.  The case is a
+seeded synthetic input built by yuzen_b200.cases (the reference reads the same
+film through its ASCII restart).  Timing: W untimed steps, then K steps, each
+timed with CUDA events on the library's stream, the L2 cache (126 MB) flushed
+by writing a 256 MiB buffer between steps (outside the timed region); under
+torchrun every rank runs an independent replica and the time is the maximum
+over ranks.  One JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "steps/s at 512² all-physics: learned-precond FP32 vs plain FP64 GPU, equal h-error"
+UNIT = "steps/s"
+
+#  The kernel whose roofline is reported (the largest share of device time in
+#  profiles/launches_spinodal_224.md) and its algorithmic bytes per launch:
+#  v = A p with alpha = rho / (rh . v): matrix values and columns (12 B per
+#  entry), row pointers (4 B per row), p read once, rh read, v written
+#  (8 B each per row).
+ROOFLINE_KERNEL = "KSpmvAlpha"
+
+
+def spmv_alpha_bytes(n: int, nnz: int) -> int:
+    return 12 * nnz + 4 * (n + 1) + 3 * 8 * n
+
+
+def measured_peaks() -> dict:
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class Clocks:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.TemporaryFile(mode="w+")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self) -> dict:
+        self.out.seek(0)
+        rows = [r for r in csv.reader(io.StringIO(self.out.read())) if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in rows]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(k)
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": float(rows[0][2]),
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def make_case(name: str, steps: int):
+    from yuzen_b200 import cases
+    return cases.CONFIGS[name](steps=steps)
+
+
+# ----------------------------------------------------------------------
+#  the reference's CPU solver (the reference's sources compiled by
+#  oracle/Makefile with the CPU restatement of its AMGCL backend)
+# ----------------------------------------------------------------------
+def reference_run(name: str, steps: int, threads: int) -> dict:
+    exe = REPO / "oracle" / "_ref" / "yuzen_oracle"
+    if not exe.exists():
+        return {"unavailable": f"{exe.relative_to(REPO)} is not built (make -C oracle ref)"}
+    cfg = make_case(name, steps)
+    with tempfile.TemporaryDirectory() as tmp:
+        cfg.write_reference(tmp)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), YUZEN_THREAD_CAP="0", OMP_PROC_BIND="close")
+        r = subprocess.run([str(exe), "case.toml"], cwd=tmp, env=env, capture_output=True, text=True, timeout=3600)
+        info = Path(tmp) / cfg.name / "JobInfo.txt"
+        if r.returncode != 0 or not info.exists():
+            return {"unavailable": f"reference run failed (exit {r.returncode})"}
+        text = info.read_text()
+    loop = float(re.search(r"Time loop \[s\]\s*:\s*([0-9.eE+-]+)", text).group(1))
+    nsteps = int(re.search(r"Time steps\s*:\s*([0-9]+)", text).group(1))
+    newton = int(re.search(r"Newton iterations\s*:\s*([0-9]+)", text).group(1))
+    linear = int(re.search(r"Linear iterations\s*:\s*([0-9]+)", text).group(1))
+    return {"value": nsteps / loop, "loop_s": loop, "steps": nsteps, "newton": newton, "linear": linear,
+            "threads": threads}
+
+
+def run_reference_arm(a) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    r = reference_run(a.config, a.steps, threads)
+    if "unavailable" in r:
+        print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
+        return
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 / r["value"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": a.config, "newton_iterations": r["newton"], "linear_iterations": r["linear"]},
+        "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{r['steps']} steps of {a.config} (the reference's sources with the CPU "
+                                   f"restatement of its AMGCL backend, {threads} OpenMP threads)"},
+        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ----------------------------------------------------------------------
+#  the device arm
+# ----------------------------------------------------------------------
+def run_device_arm(a) -> None:
+    import numpy as np
+    import torch
+
+    import yuzen_b200 as yz
+    from yuzen_b200 import step as ys
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local)
+
+    cfg = make_case(a.config, a.steps)
+    state = cfg.state()
+    params = ys.params_from_state(state)
+    st = ys.Step(params, state["field_h0"], state["field_c0"], state["field_s0"], device=local)
+    n = params.nx * params.ny
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    warm = st.advance(a.warmup) if a.warmup > 0 else None
+    yz.time_kernel(ROOFLINE_KERNEL)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    total_ms, newton, linear, launches = 0.0, 0, 0, 0
+    parts = {"setup_ms": 0.0, "solve_ms": 0.0, "assemble_ms": 0.0}
+    with Clocks(local) as clk:
+        for _ in range(a.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            r = st.advance(1)
+            total_ms += r["device_ms"]
+            newton += r["newton_iterations"]
+            linear += r["linear_iterations"]
+            launches += r["launches"]
+            for k in parts:
+                parts[k] += r[k]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    kern_ms, kern_n = yz.kernel_time()
+    yz.time_kernel(None)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * a.steps / (max_ms / 1e3)
+
+    # end to end through the C ABI with host buffers: every step uploads its
+    # film from pinned host memory and reads the result back
+    hpin = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    cpin = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    h_np, c_np = hpin.numpy(), cpin.numpy()
+    st.fields_into(h_np, c_np)
+    e2e_steps = max(1, min(a.steps, 6))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        st.set_fields(h_np, c_np)
+        st.advance(1)
+        st.fields_into(h_np, c_np)
+    e2e_s = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+    if dist:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    e2e_value = world * e2e_steps / float(e2e_t.item())
+    finite = bool(np.isfinite(h_np).all())
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    nnz = int(ys.pattern_2d(params)[1].size)
+    peaks = measured_peaks()
+    roof = None
+    if kern_n > 0:
+        bytes_ = spmv_alpha_bytes(n, nnz)
+        achieved = bytes_ / (kern_ms / kern_n / 1e3) / 1e9
+        roof = {"kernel": ROOFLINE_KERNEL, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                "peak_source": peaks["source"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                "traffic": None, "bytes_per_launch": bytes_, "launches": kern_n,
+                "avg_launch_us": kern_ms / kern_n * 1e3}
+    cpu = None
+    if world == 1 and not a.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        r = reference_run(a.config, a.cpu_steps, threads)
+        if "unavailable" not in r:
+            cpu = {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"{r['steps']} steps of {a.config}: the reference's sources with the CPU "
+                             f"restatement of its AMGCL backend, {threads} OpenMP threads"}
+        else:
+            cpu = {"unavailable": r["unavailable"]}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": max_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded, yuzen_b200.cases)",
+        "config": {"workload": a.config, "grid": [cfg.Nx, cfg.Ny], "rows": n, "nnz": nnz,
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "flushed between steps (256 MiB write)",
+                   "newton_iterations": newton, "linear_iterations": linear,
+                   "device_ms": {k: round(v, 3) for k, v in parts.items()},
+                   "finite": finite},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 2 * 8 * n,
+                "steps": e2e_steps},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=12)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="spinodal_224")
+    ap.add_argument("--cpu-steps", type=int, default=6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    if a.warmup < 3 and a.impl == "b200":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if a.impl == "reference":
+        run_reference_arm(a)
+    else:
+        run_device_arm(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -96,6 +96,14 @@ int yz_solver_last_timing(const yz_solver* s, double* setup_ms, double* iterate_
 /* Kernels this context launched since creation (a launch counter kept by the
  * host side of the library). */
 long long yz_solver_launches(const yz_solver* s);
+/* Kernels the library launched in this process, all contexts. */
+long long yz_launch_count(void);
+/* Time every later launch of the kernel with this name (its function name in
+ * the library, e.g. "KSpmvAlpha"; null or "" stops) with CUDA events on the
+ * stream it is launched on, and clear what was collected. */
+int yz_time_kernel(const char* name);
+/* Device time summed over the timed launches, and their count. */
+int yz_kernel_time(double* total_ms, long long* launches);
 
 /* Building blocks exposed for the parity tests: the deterministic dot
  * product every reduction of the solve uses, and CRS_Matrix::MatVec
@@ -162,7 +170,9 @@ typedef struct yz_step_stats
 	double time;               /* the clock after the call */
 	double dt;                 /* DT().now after the call */
 	double last_resid;         /* Newton correction of the last pass */
-	double setup_ms, solve_ms, assemble_ms;  /* device time of the call */
+	double setup_ms, solve_ms, assemble_ms;  /* device time in AMG set-up, Krylov iterations, assembly */
+	double device_ms;          /* the whole call on the step's stream (CUDA events) */
+	long long launches;        /* kernels the call launched */
 } yz_step_stats;
 
 /* Build the step: fields h, c, s on all nx*ny points (host arrays). */
@@ -173,6 +183,10 @@ int yz_step_destroy(yz_step* st);
 int yz_step_advance(yz_step* st, int nsteps, yz_step_stats* stats);
 /* Fields after the last step (host arrays of nx*ny; null pointers skipped). */
 int yz_step_get_fields(yz_step* st, double* h, double* c);
+/* Replace the committed fields (host arrays of nx*ny; null pointers skipped):
+ * the film the next step starts from, as C_ImplicitSolver::SetX takes it
+ * (phi_old = phi_new = h, ImplicitSolver.cpp:94-101). */
+int yz_step_set_fields(yz_step* st, const double* h, const double* c);
 /* The fixed CRS pattern of A / I + theta dt J, storage order (diagonal
  * first): rowptr n+1, col nnz, boundary flags n.  nnz is returned. */
 int yz_step_pattern(yz_step* st, int* rowptr, int* col, int* bc);

@@ -92,6 +92,20 @@ int main(int argc, char **argv)
 	if(!m) { std::fprintf(stderr, "yz_probe: only the 2-D well-mixed model is probed\n"); return 3; }
 	Input &inp = *m->_inputParam;
 	NonDimensionalNumbers &nd = m->_NonDim;
+	//  The prologue of WellMixed_ModelBase::Run (WellMixedModelBase.h:1235-1257),
+	//  repeated by Run itself: the step capped by the output intervals, and a
+	//  restart read (its ghosts set by the boundary conditions)
+	{
+		double max_dt = m->_timeStep.MaxDT(), val;
+		const double T0 = nd.TimeScale();
+		if(!inp.Output.FieldData.Listed()) { val = inp.Output.FieldData.TimeInterval / T0; if(val < max_dt) max_dt = val; }
+		val = inp.Output.ProbeList.TimeInterval / T0;		if(val < max_dt) max_dt = val;
+		val = inp.Output.GeneralHistory.TimeInterval / T0;	if(val < max_dt) max_dt = val;
+		val = inp.Output.CalcInfo.TimeInterval / T0;		if(val < max_dt) max_dt = val;
+		m->_timeStep.SetMaxDT(max_dt);
+		if(m->_timeStep.MaxDT() < m->_timeStep.DT().initial) m->_timeStep.ChangeDT(m->_timeStep.MaxDT());
+		if(inp.Restart.Enable) m->BuildRestart();
+	}
 	C_Grid2D *G = m->_field.GetGridPtr();
 	auto &he = m->_heightEq;
 	const BoundaryCondition2D &bc = m->_boundary;

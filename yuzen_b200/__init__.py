@@ -35,7 +35,8 @@ EXPORTED_SYMBOLS = (
     "yz_solver_memory", "yz_solver_set_memory", "yz_solver_levels", "yz_solver_level_info",
     "yz_solver_level_copy", "yz_solver_last_timing", "yz_solver_launches", "yz_dot", "yz_spmv",
     "yz_step_create", "yz_step_destroy", "yz_step_advance", "yz_step_get_fields", "yz_step_pattern",
-    "yz_step_system", "yz_pattern_2d",
+    "yz_step_system", "yz_pattern_2d", "yz_step_set_fields", "yz_launch_count",
+    "yz_time_kernel", "yz_kernel_time",
 )
 
 
@@ -85,6 +86,8 @@ def lib():
     L.yz_solver_launches.restype = ctypes.c_longlong
     L.yz_dot.argtypes = [ctypes.c_int, _f64p, _f64p, _f64p]
     L.yz_spmv.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
+    L.yz_time_kernel.argtypes = [ctypes.c_char_p]
+    L.yz_kernel_time.argtypes = [_f64p, ctypes.POINTER(ctypes.c_longlong)]
     _LIB = L
     return L
 
@@ -275,3 +278,16 @@ def spmv(rowptr, col, val, x) -> np.ndarray:
     _check(lib().yz_spmv(rowptr.size - 1, int(rowptr[-1]), _ip(rowptr), _ip(col), _fp(val), _fp(x), _fp(y)),
            "yz_spmv")
     return y
+
+
+def time_kernel(name: str | None) -> None:
+    """Bracket every later launch of the named kernel with CUDA events."""
+    _check(lib().yz_time_kernel(name.encode() if name else None), "yz_time_kernel")
+
+
+def kernel_time():
+    """(total device ms, launches) of the kernel selected by time_kernel()."""
+    ms = ctypes.c_double()
+    cnt = ctypes.c_longlong()
+    _check(lib().yz_kernel_time(ctypes.byref(ms), ctypes.byref(cnt)), "yz_kernel_time")
+    return ms.value, cnt.value

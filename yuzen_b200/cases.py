@@ -1,0 +1,351 @@
+"""Seeded synthetic cases of the implicit step, in the reference's own case
+format (TOML + an ASCII field restart) and as the non-dimensional state the
+device step starts from.
+
+The reference builds its non-dimensional state in
+NonDimensionalNumbers::Build (model/NonDimensionalNumbers.cpp:43-140), the
+grid in C_Grid2D::Build / RectGrid::SetExtentX (model/Grids.cpp:95-109,
+grid/RectGrid.h:459-465), the time-step limits in WellMixed_ModelBase::Build
+and ::Run (WellMixedModelBase.h:440-467, 1235-1250), and reads a seeded
+initial film through C_Restart::ReadAscii_WM2D (IO/Restart.cpp:280-316),
+after which BoundaryCondition2D::ApplyToField makes every ghost an exact copy
+of its partner (BoundaryCondition.cpp:309-372).  This module restates those
+steps with the same floating-point operations (Python floats are IEEE
+doubles, math.pow/sqrt/atan are the C library's), so the state it hands the
+device is the reference's own to the bit; tests/test_cases.py checks that
+against the whole-step probe.
+
+    cfg = spinodal_224()
+    state = cfg.state()               # dict: params + fields (nx*ny each)
+    cfg.write_reference(workdir)      # case.toml + init.dat for the reference
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+GG = 9.80665
+PI = 4.0 * math.atan(1.0)   # Math::pi(), MyMath.h:110
+
+#  BoundaryCondition::tBoundaryCondition
+BC = {"Symmetry": 0, "Periodic": 1}
+
+
+def _toml_value(v) -> str:
+    if isinstance(v, bool):
+        return "true" if v else "false"
+    if isinstance(v, int):
+        return str(v)
+    if isinstance(v, float):
+        return repr(v)
+    if isinstance(v, str):
+        return '"' + v + '"'
+    if isinstance(v, (list, tuple)):
+        return "[" + ", ".join(_toml_value(x) for x in v) + "]"
+    raise TypeError(type(v))
+
+
+def toml_dumps(doc: dict) -> str:
+    out: list[str] = []
+
+    def emit(t: dict, prefix: str) -> None:
+        sc = [(k, v) for k, v in t.items() if not isinstance(v, dict)]
+        sub = [(k, v) for k, v in t.items() if isinstance(v, dict)]
+        if prefix:
+            out.append(f"[{prefix}]")
+        out.extend(f"{k} = {_toml_value(v)}" for k, v in sc)
+        out.append("")
+        for k, v in sub:
+            emit(v, f"{prefix}.{k}" if prefix else k)
+
+    emit(doc, "")
+    return "\n".join(out) + "\n"
+
+
+@dataclass
+class Case:
+    """A well-mixed 2-D case: fluid, physics switches, grid, numerics and a
+    seeded initial film (interior cells, non-dimensional)."""
+    name: str
+    Nx: int
+    Ny: int
+    xlim: tuple            # dimensional [m]
+    ylim: tuple
+    h0: float              # TotalHeight [m]
+    precursor: float       # PrecursorRatio
+    bc: tuple              # Xmin, Xmax, Ymin, Ymax names
+    dt: float              # InitialDt [s]
+    steps: int = 12
+    end_time: float = 1e30
+    dt_control: bool = False
+    fluid: dict = field(default_factory=lambda: {
+        "rho": 1000.0, "sigma": 30.0e-3, "sigma_c0": 0.5, "sigma_coef": 10e-3,
+        "mu": 100.0e-3, "mu_c0": 0.5, "mu_exp": 10.0, "D": 1.0e-9, "D_c0": 0.5, "D_exp": -7.0,
+        "M_solvent": 100.0, "M_resin": 2000.0})
+    length_scale: float | None = None   # custom L0 [m], else the capillary length
+    laplace: bool = True
+    vgrav: float | None = None          # Acceleration [m/s^2], None: off
+    hgrav: tuple | None = None          # [gx, gy]
+    centrifugal: tuple | None = None    # (omega [rad/s], [x, y] axis)
+    marangoni: bool = False
+    disjoining: tuple | None = None     # (theta_e [deg], n, m)
+    evaporation: dict | None = None     # {"Coef":..., "ConcFunc":..., "SpatialFunc":...}
+    slip: float | None = None           # slip length [m]
+    conc_model: str = "None"            # "None" | "WM"
+    conc0: float = 0.5
+    h_init: np.ndarray | None = None    # (Ny, Nx) interior film, non-dimensional
+    s_init: np.ndarray | None = None
+    c_init: np.ndarray | None = None
+    newton: dict = field(default_factory=lambda: {"max": 50, "min": 1, "eps": 1e-12, "eps_rel": 1e-6})
+    linear: dict = field(default_factory=lambda: {"maxit": 8000, "eps": 1e-13, "precond": "ILU", "scaling": True})
+    dtc: dict = field(default_factory=lambda: {"MaxDtFactor": 1.0e10, "MinDt": 1.0e-15, "Criterion": 1e-3,
+                                               "KeepSteps": 50, "ChangeFactor": 0.75, "ScaleFloor": 0.0})
+
+    # ------------------------------------------------------------------
+    def toml(self, restart_file: str = "init.dat") -> dict:
+        f = self.fluid
+        doc = {
+            "SolverName": "Yuzen-1.0", "InputFormatVersion": "1.0", "JobName": self.name,
+            "Grid": {"Dimension": "xyh", "Xmin": self.xlim[0], "Xmax": self.xlim[1], "Ymin": self.ylim[0],
+                     "Ymax": self.ylim[1], "Nx": self.Nx, "Ny": self.Ny, "Nz": 1},
+            "Initial": {"Concentration": {"Type": "uniform", "Value": self.conc0},
+                        "SurfaceShape": {"TotalHeight": self.h0, "PrecursorRatio": self.precursor}},
+            "Substrate": {"TotalHeight": 0.0},
+            "Fluid": {"Name": "synthetic", "Density": {"Value": f["rho"]},
+                      "SurfaceTension": {"BaseValue": f["sigma"], "BaseConc": f["sigma_c0"], "Coef": f["sigma_coef"]},
+                      "Viscosity": {"BaseValue": f["mu"], "BaseConc": f["mu_c0"], "Exponent": f["mu_exp"]},
+                      "Diffusivity": {"BaseValue": f["D"], "BaseConc": f["D_c0"], "Exponent": f["D_exp"]},
+                      "MolarMass": {"Solvent": f["M_solvent"], "Resin": f["M_resin"]}},
+            "Physics": {
+                "ConcField": {"Model": self.conc_model, "EnableConvection": True, "EnableDiffusion": True},
+                "LaplacePressure": {"Enable": self.laplace},
+                "SolutoCapillarity": {"Enable": self.marangoni},
+                "VerticalGravity": {"Enable": self.vgrav is not None,
+                                    "Acceleration": self.vgrav if self.vgrav is not None else 9.80665},
+                "HorizontalGravity": {"Enable": self.hgrav is not None,
+                                      "Acceleration": list(self.hgrav) if self.hgrav else [0.0, 0.0]},
+                "Centrifugal": {"Enable": self.centrifugal is not None,
+                                "RotationRate": self.centrifugal[0] if self.centrifugal else 0.0,
+                                "RotationAxis": list(self.centrifugal[1]) if self.centrifugal else [0.0, 0.0]},
+                "Evaporation": {"Enable": self.evaporation is not None,
+                                **({"Coef": 1e-7, "ConcFunc": "Raoult", "SpatialFunc": "uniform",
+                                    "NegPowExponent": 0.25, "NegPowRmax": 75e-3} | (self.evaporation or {}))},
+                "DisjoiningPressure": {"Enable": self.disjoining is not None,
+                                       "ContactAngle": self.disjoining[0] if self.disjoining else 10.0,
+                                       "ExponentN": self.disjoining[1] if self.disjoining else 3.0,
+                                       "ExponentM": self.disjoining[2] if self.disjoining else 2.0},
+                "Slip": {"Enable": self.slip is not None, "Length": self.slip if self.slip else 0.0},
+                "Source": {"Enable": False},
+            },
+            "Boundary": {"XminBC": {"Type": self.bc[0]}, "XmaxBC": {"Type": self.bc[1]},
+                         "YminBC": {"Type": self.bc[2]}, "YmaxBC": {"Type": self.bc[3]}},
+            "Output": {"Dimensioned": False, "Overwrite": True,
+                       "FieldData": {"TimeInterval": 1e30, "NeutralFile": False, "VTKFile": False},
+                       "GeneralHistory": {"TimeInterval": 1e30}, "CalcInfo": {"TimeInterval": 1e30},
+                       "ProbeList": {"TimeInterval": 1e30}},
+            "Numerics": {
+                "InitialDt": self.dt, "MaxSteps": self.steps, "EndTime": self.end_time,
+                "TimeStepControl": {"Enable": self.dt_control, **self.dtc},
+                "HeightEquation": {"NewtonMaxIterations": self.newton["max"],
+                                   "NewtonMinIterations": self.newton["min"],
+                                   "NewtonEpsilon": self.newton["eps"], "NewtonEpsilonRel": self.newton["eps_rel"],
+                                   "LinearSolver": {"Backend": "amgcl", "MaxIterations": self.linear["maxit"],
+                                                    "Epsilon": self.linear["eps"], "RowScaling": self.linear["scaling"],
+                                                    "PreconditionType": self.linear["precond"]}},
+                "ConcEquation": {"LinearSolver": {"Backend": "amgcl", "MaxIterations": 5000, "Epsilon": 1e-13,
+                                                  "RowScaling": True, "PreconditionType": "ILU"}},
+            },
+            "Restart": {"Enable": True, "ASCII": True, "FileName": restart_file, "RestartTime": 0.0, "FileIndex": 0},
+        }
+        if self.length_scale is not None:
+            doc["LengthScaleType"] = "custom"
+            doc["LengthScale"] = self.length_scale
+        return doc
+
+    # ------------------------------------------------------------------
+    def scales(self) -> dict:
+        """NonDimensionalNumbers::Build (NonDimensionalNumbers.cpp:43-140)."""
+        f = self.fluid
+        sig0, rho = f["sigma"], f["rho"]
+        L0 = math.sqrt(sig0 / (rho * GG))
+        if self.length_scale is not None:
+            L0 = self.length_scale
+        h0 = self.h0
+        eps = h0 / L0
+        mu0, sigC = f["mu"], f["sigma_coef"]
+        Gz = self.vgrav if self.vgrav is not None else 9.80665
+        Gx, Gy = self.hgrav if self.hgrav else (0.0, 0.0)
+        omega = self.centrifugal[0] if self.centrifugal else 0.0
+        D0 = f["D"]
+        E0 = (self.evaporation or {}).get("Coef", 1e-7)
+        T0 = mu0 * math.pow(L0, 4.0) / (sig0 * math.pow(h0, 3.0))
+        s = {"L0": L0, "h0": h0, "T0": T0, "U0": L0 / T0}
+        s["As"] = math.pow(eps, -2.0)
+        s["Ma"] = sigC / sig0
+        s["Bo"] = rho * Gz * math.pow(L0, 2.0) / sig0
+        s["Pgx"] = rho * Gx * math.pow(L0, 2.0) / sig0 / eps
+        s["Pgy"] = rho * Gy * math.pow(L0, 2.0) / sig0 / eps
+        s["Sp"] = rho * math.pow(omega, 2.0) * math.pow(L0, 4.0) / (sig0 * h0)
+        s["HStar"] = self.precursor
+        s["Dp"] = 0.0
+        if self.disjoining is not None:
+            th_deg, nn, mm = self.disjoining
+            th = th_deg * PI / 180.0
+            s["Dp"] = s["As"] * (nn - 1.0) * (mm - 1.0) / (2.0 * s["HStar"] * (nn - mm)) * th * th
+        s["Pe"] = E0 * h0 / D0
+        s["Mr"] = f["M_resin"] / f["M_solvent"]
+        s["Ev"] = E0 * T0 / h0
+        s["Df"] = D0 * T0 / math.pow(L0, 2.0)
+        if self.vgrav is None:
+            s["Bo"] = 0.0
+        if self.hgrav is None:
+            s["Pgx"] = s["Pgy"] = 0.0
+        if self.centrifugal is None:
+            s["Sp"] = 0.0
+        if not self.marangoni:
+            s["Ma"] = 0.0
+        s["lambda"] = self.slip / h0 if self.slip else 0.0
+        return s
+
+    def grid(self, L0: float) -> dict:
+        """C_Grid2D::Build + RectGrid::SetExtentX on the non-dimensional extent."""
+        out = {}
+        for ax, lim, N in (("x", self.xlim, self.Nx), ("y", self.ylim, self.Ny)):
+            lo, hi = lim[0] / L0, lim[1] / L0
+            d0 = (hi - lo) / float(N)
+            gmin, gmax = lo - 2 * d0, hi + 2 * d0
+            n = N + 4
+            d = (gmax - gmin) / n
+            out["d" + ax] = d
+            out[ax + "min"] = gmin
+            out[ax + "0"] = gmin + 0 * d + d * 0.5
+            out["n" + ax] = n
+        return out
+
+    # ------------------------------------------------------------------
+    def fields(self):
+        """h, c, s on the whole grid (nx*ny, row iy*nx + ix), ghosts copied
+        from their partners as BoundaryCondition2D::ApplyToField leaves them."""
+        nx, ny = self.Nx + 4, self.Ny + 4
+        H = np.zeros((ny, nx))
+        S = np.zeros((ny, nx))
+        C = np.full((ny, nx), float(self.conc0))
+        H[2:-2, 2:-2] = self.h_init
+        if self.s_init is not None:
+            S[2:-2, 2:-2] = self.s_init
+        if self.c_init is not None:
+            C[2:-2, 2:-2] = self.c_init
+        bx = [BC[self.bc[0]], BC[self.bc[1]]]
+        by = [BC[self.bc[2]], BC[self.bc[3]]]
+
+        def partner(a, n, lo, hi):
+            if a < 2:
+                return a + (n - 4) if lo == 1 else 3 - a
+            if a >= n - 2:
+                return a - (n - 4) if hi == 1 else 2 * (n - 2) - 1 - a
+            return a
+
+        px = np.array([partner(a, nx, *bx) for a in range(nx)])
+        py = np.array([partner(a, ny, *by) for a in range(ny)])
+        for A in (H, S, C):
+            A[:, :] = A[np.ix_(py, px)]
+        return H.ravel(), C.ravel(), S.ravel()
+
+    def state(self) -> dict:
+        """The non-dimensional state of the step (the keys of the whole-step
+        probe, tests/golden/stateio.py)."""
+        sc = self.scales()
+        g = self.grid(sc["L0"])
+        ev = self.evaporation or {}
+        f = self.fluid
+        dt = self.dt / sc["T0"]
+        dxmin = min(g["dx"], g["dy"])
+        dt_max = self.dtc["MaxDtFactor"] * math.pow(dxmin, 4.0)
+        cap = 1e30 / sc["T0"]
+        if cap < dt_max:
+            dt_max = cap
+        if dt_max < dt:
+            dt = dt_max
+        h, c, s = self.fields()
+        return {
+            "nx": g["nx"], "ny": g["ny"], "bc_xmin": BC[self.bc[0]], "bc_xmax": BC[self.bc[1]],
+            "bc_ymin": BC[self.bc[2]], "bc_ymax": BC[self.bc[3]],
+            "on_laplace": int(self.laplace), "on_vgrav": int(self.vgrav is not None),
+            "on_pgrav": int(self.hgrav is not None), "on_marangoni": int(self.marangoni),
+            "on_centrifugal": int(self.centrifugal is not None), "on_disjoining": int(self.disjoining is not None),
+            "on_evap": int(self.evaporation is not None), "conc_field": int(self.conc_model == "WM"),
+            "slip": int(bool(self.slip)), "dt_control": int(self.dt_control),
+            "evap_conc_func": 1 if ev.get("ConcFunc") == "PowerN" else 0,
+            "evap_spatial": 1 if ev.get("SpatialFunc") == "negPow" else 0,
+            "nk_max": self.newton["max"], "nk_min": self.newton["min"], "jacobi_interval": 1,
+            "lin_precond": {"None": 0, "Jacobi": 1, "ILU": 2}[self.linear["precond"]],
+            "lin_scaling": int(self.linear["scaling"]), "lin_maxit": self.linear["maxit"],
+            "dt_keep_steps": self.dtc["KeepSteps"], "max_steps": self.steps, "on_source": 0,
+            "dx": g["dx"], "dy": g["dy"], "theta": 0.5, "dt": dt, "dt_max": dt_max, "dt_min": self.dtc["MinDt"],
+            "As": sc["As"], "Ma": sc["Ma"], "Bo": sc["Bo"], "Pgx": sc["Pgx"], "Pgy": sc["Pgy"], "Sp": sc["Sp"],
+            "Dp": sc["Dp"], "HStar": sc["HStar"], "Pe": sc["Pe"], "Mr": sc["Mr"], "Df": sc["Df"], "Ev": sc["Ev"],
+            "L0": sc["L0"], "h0": sc["h0"], "T0": sc["T0"], "lambda": sc["lambda"],
+            "disj_n": self.disjoining[1] if self.disjoining else 3.0,
+            "disj_m": self.disjoining[2] if self.disjoining else 2.0, "disj_hstar": sc["HStar"],
+            "visc_c0": f["mu_c0"], "visc_base": 1.0, "visc_exp": f["mu_exp"],
+            "sig_c0": f["sigma_c0"], "sig_base": 1.0, "sig_coef": sc["Ma"],
+            "diff_c0": f["D_c0"], "diff_base": 1.0, "diff_exp": f["D_exp"],
+            **self._evap_params(sc),
+            "nk_eps": self.newton["eps"], "nk_eps_rel": self.newton["eps_rel"], "lin_eps": self.linear["eps"],
+            "dt_change_factor": self.dtc["ChangeFactor"], "dt_criterion": self.dtc["Criterion"],
+            "dt_scale_floor": self.dtc["ScaleFloor"], "x0": g["x0"], "y0": g["y0"], "t_start": 0.0,
+            "field_h0": h, "field_c0": c, "field_s0": s,
+        }
+
+    def _evap_params(self, sc: dict) -> dict:
+        """C_Evaporation as NonDimensionalNumbers builds it (Coef 1, resin
+        molar mass Mr, solvent 1); left at its constructor's values when the
+        term is off (Evaporation.cpp:20-34)."""
+        ev = self.evaporation
+        if ev is None:
+            return {"ev_m_resin": 1.0, "ev_m_solvent": 1.0, "ev_e0": 1.0, "ev_power_n": 1.0,
+                    "ev_negpow_exp": 0.25, "ev_negpow_rmax": 1.0, "ev_conc_r": 0.0, "ev_h_ast": 0.0,
+                    "evap_hast_modify": 0}
+        return {"ev_m_resin": sc["Mr"], "ev_m_solvent": 1.0, "ev_e0": 1.0, "ev_power_n": ev.get("PowerN", 0.5),
+                "ev_negpow_exp": ev.get("NegPowExponent", 0.25),
+                "ev_negpow_rmax": ev.get("NegPowRmax", 75e-3) / sc["L0"], "ev_conc_r": ev.get("ConcR", 0.0),
+                "ev_h_ast": self.precursor, "evap_hast_modify": int(self.precursor != 0.0)}
+
+    # ------------------------------------------------------------------
+    def write_reference(self, workdir) -> Path:
+        """case.toml and the ASCII restart init.dat (columns x y h+s u v c h s,
+        rows of grid points 1..nx-2 x 1..ny-2, iy outer; non-dimensional,
+        read with coefficient 1 as Output.Dimensioned = false makes it)."""
+        w = Path(workdir)
+        w.mkdir(parents=True, exist_ok=True)
+        h, c, s = self.fields()
+        nx, ny = self.Nx + 4, self.Ny + 4
+        lines = ["# x y h+s u v c h s (synthetic initial film)"]
+        for iy in range(1, ny - 1):
+            for ix in range(1, nx - 1):
+                i = iy * nx + ix
+                hi, ci, si = float(h[i]), float(c[i]), float(s[i])
+                lines.append(f"{float(ix)!r} {float(iy)!r} {hi + si!r} 0.0 0.0 {ci!r} {hi!r} {si!r}")
+        (w / "init.dat").write_text("\n".join(lines) + "\n")
+        (w / "case.toml").write_text(toml_dumps(self.toml("init.dat")))
+        return w / "case.toml"
+
+
+# ----------------------------------------------------------------------
+#  the BASELINE configurations (seeded synthetic inputs)
+# ----------------------------------------------------------------------
+def spinodal_224(N: int = 224, seed: int = 20261203, steps: int = 12, end_time: float = 0.8) -> Case:
+    """Config 2: spinodal dewetting of a periodic film, capillary + disjoining
+    pressure, theta_e = 10 deg, h* = 0.01 h0, h = 1 + 1e-3 U(-1, 1), adaptive dt."""
+    rng = np.random.default_rng(seed)
+    h = 1.0 + 1e-3 * rng.uniform(-1.0, 1.0, size=(N, N))
+    side = 0.64e-3
+    return Case(name=f"spinodal_{N}", Nx=N, Ny=N, xlim=(-side / 2, side / 2), ylim=(-side / 2, side / 2),
+                h0=1e-6, precursor=0.01, bc=("Periodic",) * 4, dt=1e-4, steps=steps, end_time=end_time,
+                dt_control=True, disjoining=(10.0, 3.0, 2.0), h_init=h, conc0=0.5)
+
+
+CONFIGS = {"spinodal_224": spinodal_224}

@@ -144,6 +144,18 @@ int yz_solver_last_timing(const yz_solver *s, double *setup_ms, double *iterate_
 
 long long yz_solver_launches(const yz_solver *s) { return s ? s->s->Launches() : -1; }
 
+long long yz_launch_count(void) { return yz::g_launches.load(); }
+
+int yz_time_kernel(const char *name)
+{
+	return Guard([&] { yz::TimeSelect(name); return 0; });
+}
+
+int yz_kernel_time(double *total_ms, long long *launches)
+{
+	return Guard([&] { yz::TimeRead(total_ms, launches); return 0; });
+}
+
 int yz_dot(int n, const double *x, const double *y, double *out)
 {
 	return Guard([&] {
@@ -202,6 +214,15 @@ int yz_step_get_fields(yz_step *st, double *h, double *c)
 	return Guard([&] {
 		if(!st) throw yz::UsageError("yz_step_get_fields: null step");
 		st->s->GetFields(h, c);
+		return 0;
+	});
+}
+
+int yz_step_set_fields(yz_step *st, const double *h, const double *c)
+{
+	return Guard([&] {
+		if(!st) throw yz::UsageError("yz_step_set_fields: null step");
+		st->s->SetFields(h, c);
 		return 0;
 	});
 }

@@ -7,6 +7,62 @@ namespace yz {
 
 std::atomic<long long> g_launches{0};
 
+//  per-launch timing of one kernel (yz_time_kernel)
+namespace {
+std::mutex g_timeMutex;
+std::string g_timeName;
+std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_timePairs;
+cudaEvent_t g_timeOpen = nullptr;
+}
+
+bool TimedKernel(const char *name)
+{
+	if(g_timeName.empty()) return false;
+	return g_timeName == name;
+}
+
+void TimeBegin(cudaStream_t st)
+{
+	std::lock_guard<std::mutex> lk(g_timeMutex);
+	cudaEvent_t e;
+	Check(cudaEventCreate(&e), "cudaEventCreate");
+	Check(cudaEventRecord(e, st), "cudaEventRecord");
+	g_timeOpen = e;
+}
+
+void TimeEnd(cudaStream_t st)
+{
+	std::lock_guard<std::mutex> lk(g_timeMutex);
+	cudaEvent_t e;
+	Check(cudaEventCreate(&e), "cudaEventCreate");
+	Check(cudaEventRecord(e, st), "cudaEventRecord");
+	g_timePairs.push_back({g_timeOpen, e});
+	g_timeOpen = nullptr;
+}
+
+void TimeSelect(const char *name)
+{
+	std::lock_guard<std::mutex> lk(g_timeMutex);
+	for(auto &p : g_timePairs) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
+	g_timePairs.clear();
+	g_timeName = name ? name : "";
+}
+
+void TimeRead(double *ms, long long *count)
+{
+	std::lock_guard<std::mutex> lk(g_timeMutex);
+	double total = 0;
+	for(auto &p : g_timePairs)
+	{
+		Check(cudaEventSynchronize(p.second), "cudaEventSynchronize");
+		float t = 0;
+		Check(cudaEventElapsedTime(&t, p.first, p.second), "cudaEventElapsedTime");
+		total += t;
+	}
+	if(ms) *ms = total;
+	if(count) *count = (long long)g_timePairs.size();
+}
+
 namespace {
 thread_local std::string t_lastError;
 constexpr int kScanBlock = 1024;

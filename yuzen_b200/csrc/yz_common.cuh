@@ -33,12 +33,20 @@ inline void Check(cudaError_t e, const char *what)
 }
 #define YZ_CUDA(call) ::yz::Check((call), #call)
 
-//  Every kernel launch of the library goes through YZ_LAUNCH, which counts it.
+//  Every kernel launch of the library goes through YZ_LAUNCH, which counts it,
+//  and, for the one kernel named by yz_time_kernel(), brackets it with CUDA
+//  events on its own stream (the per-launch device time of that kernel).
 extern std::atomic<long long> g_launches;
+bool TimedKernel(const char *name);
+void TimeBegin(cudaStream_t st);
+void TimeEnd(cudaStream_t st);
 
 #define YZ_LAUNCH(kernel, grid, block, smem, stream, ...)                         \
 	do {                                                                          \
+		const bool yzTimed_ = ::yz::TimedKernel(#kernel);                         \
+		if(yzTimed_) ::yz::TimeBegin(stream);                                     \
 		kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);               \
+		if(yzTimed_) ::yz::TimeEnd(stream);                                       \
 		::yz::g_launches.fetch_add(1, std::memory_order_relaxed);                 \
 		::yz::Check(cudaGetLastError(), #kernel);                                 \
 	} while(0)

@@ -104,5 +104,7 @@ private:
 double DeviceDot(int n, const double *hx, const double *hy);
 void DeviceSpmv(int n, int nnz, const int *rowptr, const int *col, const double *val, const double *hx, double *hy);
 const char *LastError();
+void TimeSelect(const char *name);
+void TimeRead(double *ms, long long *count);
 
 } // namespace yz

@@ -472,6 +472,7 @@ Step::Step(int device, const yz_step_params &p, const double *h, const double *c
 	_solver.reset(new Solver(device));
 	_st = _solver->Stream();
 	YZ_CUDA(cudaEventCreate(&_e0)); YZ_CUDA(cudaEventCreate(&_e1));
+	YZ_CUDA(cudaEventCreate(&_eA)); YZ_CUDA(cudaEventCreate(&_eB));
 	const int nx = p.nx, ny = p.ny;
 	_n = nx * ny;
 	BuildPattern();
@@ -501,7 +502,7 @@ Step::~Step()
 {
 	cudaSetDevice(_device);
 	if(_st) cudaStreamSynchronize(_st);
-	cudaEventDestroy(_e0); cudaEventDestroy(_e1);
+	cudaEventDestroy(_e0); cudaEventDestroy(_e1); cudaEventDestroy(_eA); cudaEventDestroy(_eB);
 }
 
 //  The pattern the reference fixes in C_ImplicitSolver::Alloc
@@ -766,6 +767,8 @@ void Step::Advance(int nsteps, yz_step_stats &stats)
 	YZ_CUDA(cudaSetDevice(_device));
 	const size_t bytes = (size_t)_n * sizeof(double);
 	const int g = GridFor(_n, 256);
+	const long long l0 = g_launches.load();
+	YZ_CUDA(cudaEventRecord(_eA, _st));
 	for(int step = 0; step < nsteps; ++step)
 	{
 		YZ_CUDA(cudaMemcpyAsync(_hOld2.get(), _hOld.get(), bytes, cudaMemcpyDeviceToDevice, _st));
@@ -846,7 +849,24 @@ void Step::Advance(int nsteps, yz_step_stats &stats)
 	}
 	stats.time = _time;
 	stats.dt = _dt;
-	YZ_CUDA(cudaStreamSynchronize(_st));
+	YZ_CUDA(cudaEventRecord(_eB, _st));
+	YZ_CUDA(cudaEventSynchronize(_eB));
+	float ms = 0;
+	YZ_CUDA(cudaEventElapsedTime(&ms, _eA, _eB));
+	stats.device_ms = ms;
+	stats.launches = g_launches.load() - l0;
+}
+
+void Step::SetFields(const double *h, const double *c)
+{
+	YZ_CUDA(cudaSetDevice(_device));
+	const size_t bytes = (size_t)_n * sizeof(double);
+	if(h)
+	{
+		YZ_CUDA(cudaMemcpyAsync(_h.get(), h, bytes, cudaMemcpyHostToDevice, _st));
+		YZ_CUDA(cudaMemcpyAsync(_hNew.get(), _h.get(), bytes, cudaMemcpyDeviceToDevice, _st));
+	}
+	if(c) YZ_CUDA(cudaMemcpyAsync(_c.get(), c, bytes, cudaMemcpyHostToDevice, _st));
 }
 
 void Step::GetFields(double *h, double *c)

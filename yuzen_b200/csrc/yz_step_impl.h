@@ -20,6 +20,7 @@ public:
 	~Step();
 	void Advance(int nsteps, yz_step_stats &stats);
 	void GetFields(double *h, double *c);
+	void SetFields(const double *h, const double *c);
 	int Pattern(int *rowptr, int *col, int *bc) const;
 	void System(const double *hOld, const double *h, double dt, double *ia, double *rhs);
 	long long Launches() const { return _solver->Launches(); }
@@ -40,7 +41,7 @@ private:
 	phys::Coef _k;
 	std::unique_ptr<Solver> _solver;
 	cudaStream_t _st = nullptr;
-	cudaEvent_t _e0 = nullptr, _e1 = nullptr;
+	cudaEvent_t _e0 = nullptr, _e1 = nullptr, _eA = nullptr, _eB = nullptr;
 	int _n = 0, _nnz = 0;
 	std::vector<int> _rowptr, _col, _isbc, _ghost, _partner;
 	DBuf<int> _dRowptr, _dGhost, _dPartner;

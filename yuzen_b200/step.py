@@ -44,7 +44,7 @@ class StepStats(ctypes.Structure):
         ("steps", ctypes.c_int), ("newton_iterations", ctypes.c_int), ("linear_iterations", ctypes.c_int),
         ("retries", ctypes.c_int), ("time", ctypes.c_double), ("dt", ctypes.c_double),
         ("last_resid", ctypes.c_double), ("setup_ms", ctypes.c_double), ("solve_ms", ctypes.c_double),
-        ("assemble_ms", ctypes.c_double),
+        ("assemble_ms", ctypes.c_double), ("device_ms", ctypes.c_double), ("launches", ctypes.c_longlong),
     ]
 
     def as_dict(self) -> dict:
@@ -93,6 +93,8 @@ def _bind():
     L.yz_step_destroy.argtypes = [ctypes.c_void_p]
     L.yz_step_advance.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(StepStats)]
     L.yz_step_get_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
+    L.yz_step_set_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
+    L.yz_launch_count.restype = ctypes.c_longlong
     L.yz_step_pattern.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                   ctypes.POINTER(ctypes.c_int)]
     L.yz_step_system.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_double, _f64p, _f64p]
@@ -126,6 +128,14 @@ class Step:
         c = np.zeros(self.n)
         _check(lib().yz_step_get_fields(self._h, _fp(h), _fp(c)), "yz_step_get_fields")
         return h, c
+
+    def fields_into(self, h: np.ndarray, c: np.ndarray | None = None) -> None:
+        """Download the fields into caller-owned (e.g. pinned) float64 arrays."""
+        _check(lib().yz_step_get_fields(self._h, _fp(h), _fp(c) if c is not None else None), "yz_step_get_fields")
+
+    def set_fields(self, h: np.ndarray, c: np.ndarray | None = None) -> None:
+        """Upload the fields the next step starts from (host arrays)."""
+        _check(lib().yz_step_set_fields(self._h, _fp(h), _fp(c) if c is not None else None), "yz_step_set_fields")
 
     def pattern(self):
         L = lib()
@@ -168,3 +178,8 @@ def pattern_2d(params: StepParams):
     bc = np.zeros(n, np.int32)
     _check(L.yz_pattern_2d(ctypes.byref(params), _ip(rowptr), _ip(col), _ip(bc)), "yz_pattern_2d")
     return rowptr, col, bc
+
+
+def launch_count() -> int:
+    """Kernels the library launched in this process."""
+    return int(_bind().yz_launch_count())
