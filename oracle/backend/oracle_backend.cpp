@@ -11,7 +11,10 @@
  *   "auto"             -> amgcl in 2-D, eigen in 1-D (factory, :759-804)
  *   anything else      -> eigen (the reference's rule)
  * With the b200 adapter linked in (YZ_WITH_B200), "b200" creates the GPU
- * backend of yuzen_b200/host/yz_backend_adapter.cpp.
+ * backend of yuzen_b200/host/yz_backend_adapter.cpp; since the reference's
+ * input reader (compiled unchanged) accepts only auto / eigen / amgcl,
+ * YZ_BACKEND=b200 in the environment makes every request for the 2-D AMG
+ * backend (amgcl, or auto in 2-D) return it.
  *
  * Dump hook: with YZO_DUMP_DIR set, every solve writes its matrix (storage
  * order and sorted mirror), boundary flags, right-hand side, initial guess and
@@ -120,6 +123,9 @@ ILinearSolverBackend* MakeLinearSolverBackend(const std::string &name, int inPla
 {
 #ifdef YZ_WITH_B200
 	if(name == "b200") return MakeB200LinearSolverBackend();
+	if(const char *e = std::getenv("YZ_BACKEND"))
+		if(std::string(e) == "b200" && (name == "amgcl" || (name == "auto" && inPlane >= 2)))
+			return MakeB200LinearSolverBackend();
 #endif
 	if(name == "auto")
 	{

@@ -115,6 +115,27 @@ STEP_CASES = {
 }
 
 
+#  Cases the reference's driver runs with either backend (the drop-in test):
+#  written as TOML files under tests/golden/cases/
+DROPIN_CASES = {
+    # every term of the height equation and the WM concentration equation
+    "dropin_allphys_48": ("allphys_2d_reg.toml", {
+        "Grid.Nx": 48, "Grid.Ny": 40,
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-4, "Numerics.MaxSteps": 3,
+    }),
+    "dropin_disjoin_periodic_40": ("allphys_2d_reg.toml", {
+        **_NO_UPWIND, "Grid.Nx": 40, "Grid.Ny": 40,
+        "Boundary.XminBC.Type": "Periodic", "Boundary.XmaxBC.Type": "Periodic",
+        "Boundary.YminBC.Type": "Periodic", "Boundary.YmaxBC.Type": "Periodic",
+        "Physics.VerticalGravity.Enable": False, "Physics.Evaporation.Enable": False,
+        "Physics.DisjoiningPressure.Enable": True, "Physics.DisjoiningPressure.ContactAngle": 10.0,
+        "Physics.DisjoiningPressure.ExponentN": 3.0, "Physics.DisjoiningPressure.ExponentM": 2.0,
+        "Initial.SurfaceShape.PrecursorRatio": 0.05,
+        "Numerics.TimeStepControl.Enable": True, "Numerics.InitialDt": 1e-4, "Numerics.MaxSteps": 4,
+    }),
+}
+
+
 def write_case(ref: Path, src: str, over: dict, name: str, work: Path) -> Path:
     doc = tomllib.loads((ref / "cases" / src).read_text())
     for k, v in {**QUIET_OUTPUT, **over}.items():
@@ -172,6 +193,11 @@ def main() -> None:
     if not ORACLE.exists():
         raise SystemExit(f"{ORACLE} missing: make -C oracle ref")
     with tempfile.TemporaryDirectory() as tmp:
+        cases_dir = HERE / "cases"
+        cases_dir.mkdir(exist_ok=True)
+        for name, (src, over) in DROPIN_CASES.items():
+            write_case(Path(a.ref), src, over, name, cases_dir)
+            print("case", name)
         for name in STEP_CASES:
             if a.only and name != a.only:
                 continue
