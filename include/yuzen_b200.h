@@ -112,6 +112,20 @@ int yz_dot(int n, const double* x, const double* y, double* out);
 int yz_spmv(int n, int nnz, const int* rowptr, const int* col, const double* val,
             const double* x, double* y);
 
+/* The dot product of yz_dot for callers that cannot allocate device memory
+ * (a host code that owns all device memory itself, or a path that must not
+ * take cudaMalloc's device-wide synchronisation).  This entry point has no
+ * counterpart in the reference.  d_x, d_y (n each) and d_out (one double) are
+ * the caller's device arrays on the current device; the call is queued on
+ * `stream` (a cudaStream_t, null: the default stream) and allocates nothing:
+ * its scratch is a static array of the library, at most
+ * yz_dot_noalloc_max() elements (16,777,216); larger n returns -1.  The
+ * array is shared by every call, so calls that overlap on the GPU race; the
+ * first call on a device takes the array's address (cudaGetSymbolAddress)
+ * and should come before any stream capture. */
+int yz_dot_noalloc(int n, const double* d_x, const double* d_y, double* d_out, void* stream);
+long long yz_dot_noalloc_max(void);
+
 /*
  * ---------------------------------------------------------------------
  * Seam 2: the whole implicit step of the well-mixed film-height equation.

@@ -36,7 +36,7 @@ EXPORTED_SYMBOLS = (
     "yz_solver_level_copy", "yz_solver_last_timing", "yz_solver_launches", "yz_dot", "yz_spmv",
     "yz_step_create", "yz_step_destroy", "yz_step_advance", "yz_step_get_fields", "yz_step_pattern",
     "yz_step_system", "yz_pattern_2d", "yz_step_set_fields", "yz_launch_count",
-    "yz_time_kernel", "yz_kernel_time",
+    "yz_time_kernel", "yz_kernel_time", "yz_dot_noalloc", "yz_dot_noalloc_max",
 )
 
 
@@ -86,6 +86,8 @@ def lib():
     L.yz_solver_launches.restype = ctypes.c_longlong
     L.yz_dot.argtypes = [ctypes.c_int, _f64p, _f64p, _f64p]
     L.yz_spmv.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
+    L.yz_dot_noalloc.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.yz_dot_noalloc_max.restype = ctypes.c_longlong
     L.yz_time_kernel.argtypes = [ctypes.c_char_p]
     L.yz_kernel_time.argtypes = [_f64p, ctypes.POINTER(ctypes.c_longlong)]
     _LIB = L
@@ -291,3 +293,9 @@ def kernel_time():
     cnt = ctypes.c_longlong()
     _check(lib().yz_kernel_time(ctypes.byref(ms), ctypes.byref(cnt)), "yz_kernel_time")
     return ms.value, cnt.value
+
+
+def dot_noalloc(n: int, x_ptr: int, y_ptr: int, out_ptr: int, stream: int = 0) -> None:
+    """yz_dot_noalloc on device pointers (the caller owns every buffer)."""
+    _check(lib().yz_dot_noalloc(int(n), ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), ctypes.c_void_p(out_ptr),
+                                ctypes.c_void_p(stream) if stream else None), "yz_dot_noalloc")

@@ -146,6 +146,16 @@ long long yz_solver_launches(const yz_solver *s) { return s ? s->s->Launches() :
 
 long long yz_launch_count(void) { return yz::g_launches.load(); }
 
+int yz_dot_noalloc(int n, const double *d_x, const double *d_y, double *d_out, void *stream)
+{
+	return Guard([&] {
+		yz::DotNoAlloc(n, d_x, d_y, d_out, static_cast<cudaStream_t>(stream));
+		return 0;
+	});
+}
+
+long long yz_dot_noalloc_max(void) { return yz::NoAllocMaxElements(); }
+
 int yz_time_kernel(const char *name)
 {
 	return Guard([&] { yz::TimeSelect(name); return 0; });

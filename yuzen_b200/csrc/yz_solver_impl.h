@@ -105,6 +105,8 @@ double DeviceDot(int n, const double *hx, const double *hy);
 void DeviceSpmv(int n, int nnz, const int *rowptr, const int *col, const double *val, const double *hx, double *hy);
 const char *LastError();
 void TimeSelect(const char *name);
+void DotNoAlloc(int n, const double *dx, const double *dy, double *dout, cudaStream_t st);
+long long NoAllocMaxElements();
 void TimeRead(double *ms, long long *count);
 
 } // namespace yz
