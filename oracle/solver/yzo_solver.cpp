@@ -63,7 +63,7 @@ namespace {
 //--------------------------------------------------------------------------
 //  deterministic reduction
 //--------------------------------------------------------------------------
-const int kRT = 256, kRK = 16, kRChunk = kRT * kRK;
+const int kRT = 256, kRK = 1, kRChunk = kRT * kRK;
 
 double Tree256(double *s)
 {
@@ -446,12 +446,21 @@ struct Hierarchy
 		const int n = L.A.n;
 		if(L.direct)
 		{
+			//  row i of the inverse times f as 32 strided partial sums
+			//  (lane l: j = l, l+32, ... from 0.0) folded pairwise
 			for(int i = 0; i < n; ++i)
 			{
-				double s = 0.0;
+				double s[32];
 				const double *row = &L.inv[(size_t)i * n];
-				for(int j = 0; j < n; ++j) s = s + row[j] * f[j];
-				x[i] = s;
+				for(int l = 0; l < 32; ++l)
+				{
+					double a = 0.0;
+					for(int j = l; j < n; j += 32) a = a + row[j] * f[j];
+					s[l] = a;
+				}
+				for(int off = 16; off >= 1; off >>= 1)
+					for(int l = 0; l < off; ++l) s[l] = s[l] + s[l + off];
+				x[i] = s[0];
 			}
 			return;
 		}

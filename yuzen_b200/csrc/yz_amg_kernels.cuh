@@ -307,11 +307,15 @@ __global__ void KRowSort(int n, const int *__restrict__ ptr, int *__restrict__ c
 //  sparse product C = X Y with the oracle's summation order: per output
 //  entry from 0.0, contributions in the order of X's row (ascending k)
 //--------------------------------------------------------------------------
+//  CAP bounds the distinct columns of one output row held in registers /
+//  local memory; a row beyond it sets *overflow (the caller then runs the
+//  product again with the larger capacity).
+template<int CAP>
 __global__ void KGemmCount(int nx, const int *__restrict__ xptr, const int *__restrict__ xcol,
                            const int *__restrict__ yptr, const int *__restrict__ ycol,
                            int *__restrict__ cnt, int *__restrict__ overflow)
 {
-	int lc[kRowCap];
+	int lc[CAP];
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x)
 	{
 		int m = 0;
@@ -325,7 +329,7 @@ __global__ void KGemmCount(int nx, const int *__restrict__ xptr, const int *__re
 				int lo = 0, hi = m;
 				while(lo < hi) { const int mid = (lo + hi) >> 1; if(lc[mid] < j) lo = mid + 1; else hi = mid; }
 				if(lo < m && lc[lo] == j) continue;
-				if(m == kRowCap) { over = true; break; }
+				if(m == CAP) { over = true; break; }
 				for(int q = m; q > lo; --q) lc[q] = lc[q - 1];
 				lc[lo] = j; ++m;
 			}
@@ -335,13 +339,14 @@ __global__ void KGemmCount(int nx, const int *__restrict__ xptr, const int *__re
 	}
 }
 
+template<int CAP>
 __global__ void KGemmFill(int nx, const int *__restrict__ xptr, const int *__restrict__ xcol,
                           const double *__restrict__ xval, const int *__restrict__ yptr,
                           const int *__restrict__ ycol, const double *__restrict__ yval,
                           const int *__restrict__ cptr, int *__restrict__ ccol, double *__restrict__ cval)
 {
-	int lc[kRowCap];
-	double lv[kRowCap];
+	int lc[CAP];
+	double lv[CAP];
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x)
 	{
 		int m = 0;
@@ -356,7 +361,7 @@ __global__ void KGemmFill(int nx, const int *__restrict__ xptr, const int *__res
 				while(lo < hi) { const int mid = (lo + hi) >> 1; if(lc[mid] < j) lo = mid + 1; else hi = mid; }
 				if(!(lo < m && lc[lo] == j))
 				{
-					if(m == kRowCap) continue;
+					if(m == CAP) continue;
 					for(int q = m; q > lo; --q) { lc[q] = lc[q - 1]; lv[q] = lv[q - 1]; }
 					lc[lo] = j; lv[lo] = 0.0; ++m;
 				}
@@ -438,14 +443,15 @@ __global__ void KGjStep(int n, int k, const double *__restrict__ Min, double *__
 	}
 }
 
-__global__ void KGjExtract(int n, const double *__restrict__ M, double *__restrict__ invCm)
+//  the right half of [I | A^-1], row-major
+__global__ void KGjExtract(int n, const double *__restrict__ M, double *__restrict__ inv)
 {
 	const int w = 2 * n;
 	const long long total = (long long)n * n;
 	for(long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x)
 	{
 		const int i = (int)(e / n), j = (int)(e % n);
-		invCm[(size_t)j * n + i] = M[(size_t)i * w + n + j];
+		inv[(size_t)i * n + j] = M[(size_t)i * w + n + j];
 	}
 }
 
@@ -510,14 +516,20 @@ __global__ void KPostSmooth(int n, const int *__restrict__ ptr, const int *__res
 	}
 }
 
-//  x = inv f, inv stored column-major; summed over j from 0.0
-__global__ void KDenseMV(int n, const double *__restrict__ invCm, const double *__restrict__ f, double *__restrict__ x)
+//  x = inv f, inv row-major: one warp per row, lane l sums j = l, l+32, ...
+//  from 0.0 (coalesced reads of the row), then a pairwise shuffle fold
+__global__ void KDenseMV(int n, const double *__restrict__ inv, const double *__restrict__ f, double *__restrict__ x)
 {
-	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	const int lane = threadIdx.x & 31;
+	const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+	for(long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps)
 	{
+		const double *row = inv + (size_t)i * n;
 		double s = 0.0;
-		for(int j = 0; j < n; ++j) s = s + invCm[(size_t)j * n + i] * f[j];
-		x[i] = s;
+		for(int j = lane; j < n; j += 32) s = s + row[j] * f[j];
+#pragma unroll
+		for(int off = 16; off >= 1; off >>= 1) s = s + __shfl_down_sync(0xffffffffu, s, off);
+		if(lane == 0) x[i] = s;
 	}
 }
 

@@ -87,12 +87,14 @@ struct DBuf
 
 //--------------------------------------------------------------------------
 //  the deterministic reduction tree (the oracle's DetSum, yzo_solver.cpp):
-//  chunk b of 4096 elements per block of 256 threads, thread t sums elements
-//  b*4096 + k*256 + t (k = 0..15) from 0.0, pairwise fold over the block,
-//  the chunk sums folded the same way by the block that finishes last.
+//  chunk b of 256 elements per block of 256 threads, thread t holds element
+//  b*256 + t, pairwise fold over the block; the chunk sums are summed
+//  strided by 256 threads (thread t: chunks t, t+256, ... from 0.0) and
+//  folded the same way by the block that finishes last.  One element per
+//  thread keeps every SM busy at the sizes of a film (n / 256 blocks).
 //--------------------------------------------------------------------------
 constexpr int kRT = 256;
-constexpr int kRK = 16;
+constexpr int kRK = 1;
 constexpr int kRChunk = kRT * kRK;
 
 inline int RedBlocks(int n) { const int nb = (n + kRChunk - 1) / kRChunk; return nb > 0 ? nb : 1; }

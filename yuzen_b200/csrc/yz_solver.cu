@@ -271,6 +271,32 @@ int Solver::ScanCounts(const int *cnt, int *out, int n)
 	return ReadInt(out + n);
 }
 
+//  C = X Y (KGemmCount / KGemmFill): first with room for 64 distinct
+//  columns per row in registers, again with kRowCap if a row needs more;
+//  returns nnz(C)
+int Solver::Gemm(int nx, const int *xptr, const int *xcol, const double *xval, const int *yptr, const int *ycol,
+                 const double *yval, DBuf<int> &cptr, DBuf<int> &ccol, DBuf<double> &cval)
+{
+	int *overflow = _flags.get() + 1;
+	const int g = GridFor(nx, 128);
+	YZ_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int), _st));
+	YZ_LAUNCH(KGemmCount<64>, g, 128, 0, _st, nx, xptr, xcol, yptr, ycol, _cnt.get(), overflow);
+	cptr.reserve((size_t)nx + 1);
+	int nnz = ScanCounts(_cnt.get(), cptr.get(), nx);
+	const bool wide = ReadInt(overflow) != 0;
+	if(wide)
+	{
+		YZ_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int), _st));
+		YZ_LAUNCH(KGemmCount<kRowCap>, g, 128, 0, _st, nx, xptr, xcol, yptr, ycol, _cnt.get(), overflow);
+		nnz = ScanCounts(_cnt.get(), cptr.get(), nx);
+		if(ReadInt(overflow)) throw CudaError("AMG set-up: a row of a product gathered more than 256 distinct columns");
+	}
+	ccol.reserve((size_t)nnz); cval.reserve((size_t)nnz);
+	if(wide) YZ_LAUNCH(KGemmFill<kRowCap>, g, 128, 0, _st, nx, xptr, xcol, xval, yptr, ycol, yval, cptr.get(), ccol.get(), cval.get());
+	else YZ_LAUNCH(KGemmFill<64>, g, 128, 0, _st, nx, xptr, xcol, xval, yptr, ycol, yval, cptr.get(), ccol.get(), cval.get());
+	return nnz;
+}
+
 //--------------------------------------------------------------------------
 //  the hierarchy
 //--------------------------------------------------------------------------
@@ -342,6 +368,7 @@ void Solver::BuildHierarchy(int coarseEnough)
 		YZ_LAUNCH(KPCount, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), _strong.get(), L.agg.get(), _cnt.get(), overflow);
 		L.pptr.reserve((size_t)n + 1);
 		L.pnnz = ScanCounts(_cnt.get(), L.pptr.get(), n);
+		if(ReadInt(overflow)) throw CudaError("AMG set-up: a row of P gathered more than 256 distinct aggregates");
 		L.pcol.reserve((size_t)L.pnnz); L.pval.reserve((size_t)L.pnnz);
 		YZ_LAUNCH(KPFill, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), _strong.get(), L.agg.get(),
 		          L.pptr.get(), L.pcol.get(), L.pval.get());
@@ -355,24 +382,13 @@ void Solver::BuildHierarchy(int coarseEnough)
 		          L.rcol.get(), L.rval.get());
 		YZ_LAUNCH(KRowSort, GridFor(nc, kB), kB, 0, _st, nc, L.rptr.get(), L.rcol.get(), L.rval.get());
 		//  AP, then A_c = R (AP)
-		YZ_LAUNCH(KGemmCount, g, 128, 0, _st, n, L.ptr.get(), L.col.get(), L.pptr.get(), L.pcol.get(), _cnt.get(), overflow);
-		_apPtr.reserve((size_t)n + 1);
-		const int apnnz = ScanCounts(_cnt.get(), _apPtr.get(), n);
-		_apCol.reserve((size_t)apnnz); _apVal.reserve((size_t)apnnz);
-		YZ_LAUNCH(KGemmFill, g, 128, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), L.pptr.get(), L.pcol.get(),
-		          L.pval.get(), _apPtr.get(), _apCol.get(), _apVal.get());
+		Gemm(n, L.ptr.get(), L.col.get(), L.val.get(), L.pptr.get(), L.pcol.get(), L.pval.get(), _apPtr, _apCol, _apVal);
 		_levels.emplace_back(new Level());
 		Level &C = *_levels.back();
 		Level &F = *_levels[l];
 		C.n = nc;
-		YZ_LAUNCH(KGemmCount, GridFor(nc, 128), 128, 0, _st, nc, F.rptr.get(), F.rcol.get(), _apPtr.get(), _apCol.get(),
-		          _cnt.get(), overflow);
-		C.ptr.reserve((size_t)nc + 1);
-		C.nnz = ScanCounts(_cnt.get(), C.ptr.get(), nc);
-		C.col.reserve((size_t)C.nnz); C.val.reserve((size_t)C.nnz);
-		YZ_LAUNCH(KGemmFill, GridFor(nc, 128), 128, 0, _st, nc, F.rptr.get(), F.rcol.get(), F.rval.get(), _apPtr.get(),
-		          _apCol.get(), _apVal.get(), C.ptr.get(), C.col.get(), C.val.get());
-		if(ReadInt(overflow)) throw CudaError("AMG set-up: a row gathered more than 256 distinct columns");
+		C.nnz = Gemm(nc, F.rptr.get(), F.rcol.get(), F.rval.get(), _apPtr.get(), _apCol.get(), _apVal.get(), C.ptr, C.col,
+		             C.val);
 	}
 	_haveH = true;
 }
@@ -384,7 +400,7 @@ void Solver::Cycle(size_t l, const double *f, double *x)
 	const int n = L.n, g = GridFor(n, kB);
 	if(L.direct)
 	{
-		YZ_LAUNCH(KDenseMV, g, kB, 0, _st, n, L.inv.get(), f, x);
+		YZ_LAUNCH(KDenseMV, GridFor((long long)n * 32, kB), kB, 0, _st, n, L.inv.get(), f, x);
 		return;
 	}
 	if(l + 1 < _levels.size())

@@ -69,6 +69,8 @@ private:
 	int ReadInt(const int *d);
 	void ReadScal();
 	int ScanCounts(const int *cnt, int *out, int n);
+	int Gemm(int nx, const int *xptr, const int *xcol, const double *xval, const int *yptr, const int *ycol,
+	         const double *yval, DBuf<int> &cptr, DBuf<int> &ccol, DBuf<double> &cval);
 	RedScratch Red(int site);
 
 	int _device;
