@@ -145,12 +145,20 @@ typedef struct yz_step yz_step;
  * step supports Symmetry and Periodic edges. */
 enum { YZ_BC_SYMMETRY = 0, YZ_BC_PERIODIC = 1 };
 
+/* C_Interpolation_base4::t_Scheme (FiniteDifferences.h:42-53), the face
+ * interpolation of Numerics.Convection.Height / .Concentration.  The
+ * upwinded height terms take the limited ones (Koren, the default, and
+ * VanLeer); the concentration takes every scheme. */
+enum { YZ_SCHEME_UPWIND1 = 0, YZ_SCHEME_UPWIND2 = 1, YZ_SCHEME_CENTRAL2 = 2, YZ_SCHEME_UTOPIA = 3,
+       YZ_SCHEME_QUICK = 4, YZ_SCHEME_KK = 5, YZ_SCHEME_CENTRAL4 = 6, YZ_SCHEME_KOREN = 7,
+       YZ_SCHEME_VANLEER = 8 };
+
 typedef struct yz_step_params
 {
 	int    nx, ny;                /* points including the ghost layers */
 	int    bc[4];                 /* Xmin, Xmax, Ymin, Ymax */
 	double dx, dy;                /* C_Grid2D spacing */
-	double x0, y0;                /* coordinate of cell (0,0) */
+	double xmin, ymin;            /* the grid's lower corner: X / Y of the low faces of cell (0,0) (RectGrid.h:375-383) */
 	double theta;                 /* 0.5: Crank-Nicolson */
 	/* physics terms (HeightEquationBase.h:565-577) */
 	int    on_laplace, on_vgrav, on_pgrav, on_marangoni, on_centrifugal, on_disjoining;
@@ -173,6 +181,19 @@ typedef struct yz_step_params
 	int    dt_control, dt_keep_steps;
 	double dt, dt_max, dt_min, dt_change_factor, dt_criterion, dt_scale_floor;
 	double t_start;
+	/* the upwinded terms (BodyForceKernel.h, ParallelGravityKernel.h,
+	 * CentrifugalKernel.h, SolutoCapillarityKernel.h) */
+	int    conv_height;           /* YZ_SCHEME_KOREN or YZ_SCHEME_VANLEER */
+	double Pgx, Pgy;              /* in-plane gravity groups (coefficients Pg/3) */
+	double Sp, rot_x, rot_y;      /* rotation group and the axis (non-dimensional) */
+	double As, Ma;                /* Marangoni coefficient As*Ma/2 */
+	/* the well-mixed concentration equation (ConcEquationBase.h), solved in
+	 * every Newton pass when conc_field = 1 */
+	int    conv_conc;             /* any YZ_SCHEME_* (UTOPIA is the reference's default) */
+	int    conc_convection, conc_diffusion;
+	double theta_c;               /* 0.5 (Crank-Nicolson) */
+	double Df, diff_c0, diff_base, diff_exp;   /* Df and the diffusivity law D(c) = base exp(exp (c - c0)) */
+	yz_settings lin_conc;         /* its linear solve (conc = 1: the SPAI0-first role) */
 } yz_step_params;
 
 typedef struct yz_step_stats
@@ -187,6 +208,8 @@ typedef struct yz_step_stats
 	double setup_ms, solve_ms, assemble_ms;  /* device time in AMG set-up, Krylov iterations, assembly */
 	double device_ms;          /* the whole call on the step's stream (CUDA events) */
 	long long launches;        /* kernels the call launched */
+	int    conc_iterations;    /* BiCGStab iterations of the concentration solves, summed */
+	int    conc_solves;        /* concentration solves */
 } yz_step_stats;
 
 /* Build the step: fields h, c, s on all nx*ny points (host arrays). */
@@ -210,6 +233,17 @@ int yz_step_pattern(yz_step* st, int* rowptr, int* col, int* bc);
  * I + theta dt J (nnz, storage order) and the right-hand side (n). */
 int yz_step_system(yz_step* st, const double* h_old, const double* h, double dt,
                    double* ia_values, double* rhs);
+/* The concentration equation's pattern (conc_field = 1): rowptr n+1 and col
+ * (storage order, diagonal first, ConcEquationBase.h:243-259); nnz is
+ * returned, 0 without the concentration equation. */
+int yz_step_conc_pattern(yz_step* st, int* rowptr, int* col);
+/* The concentration system of the first Newton pass of a step that starts
+ * from the committed film h and concentration c (ConcEquationBase.h:271-396
+ * with h1 = h0 = h, the face fluxes F1 = F0 at that film, the limiter at c):
+ * the matrix values (storage order) and the right-hand side of the
+ * correction d = c1 - c0. */
+int yz_step_conc_system(yz_step* st, const double* h, const double* c, double dt,
+                        double* values, double* rhs);
 /* The same pattern built on the host alone, without a device (the structure
  * C_ImplicitSolver::Alloc fixes, ImplicitSolver.cpp:60-81, with the ghost rows
  * of BoundaryCondition2D::Apply, BoundaryCondition.cpp:376-517); arrays may be

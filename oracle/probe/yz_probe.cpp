@@ -13,7 +13,9 @@
  * integer header, the integers; int32 count of the real header, the doubles;
  * then float64 arrays of nx*ny each (row = IL(ix,iy) = iy*nx + ix):
  * HH0, CC0, SS0 (after Build), HH1, CC1 (after the run); int32 rowptr[n+1],
- * col[nnz] of A's fixed pattern (storage order) and bc[n].
+ * col[nnz] of A's fixed pattern (storage order) and bc[n]; int32 n_c, nnz_c,
+ * rowptr_c[n_c+1], col_c[nnz_c] of the concentration equation's pattern
+ * (n_c = 0 without the WM concentration).
  * The header keys are listed in tests/golden/stateio.py.
  *
  * Private members are reached by compiling the reference headers with their
@@ -141,6 +143,18 @@ int main(int argc, char **argv)
 	put(D, he._adjustTimeChangeFactor); put(D, he._adjustTimeCriterion); put(D, he._adjustTimeScaleFloor);
 	put(D, G->X(G->At<Zface>(0, 0))); put(D, G->Y(G->At<Zface>(0, 0)));
 	put(D, m->_timeStep.NowTime());
+	//  the upwinded terms and the concentration equation
+	{
+		Zface z0 = G->At<Zface>(0, 0);
+		const auto &ce = m->_concEq;
+		put(I, (int)he._ParallelGravity._scheme.Scheme()); put(I, (int)ce._scheme.Scheme());
+		put(I, ce._swConvection ? 1 : 0); put(I, ce._swDiffusion ? 1 : 0);
+		put(I, (int)ce._bcg._set.precondition); put(I, ce._bcg._set.scaling ? 1 : 0); put(I, ce._bcg._set.maxIteration);
+		put(I, ce._bcg._set.conc ? 1 : 0);
+		put(D, G->X(G->HalfXm(z0))); put(D, G->Y(G->HalfYm(z0)));
+		put(D, he._Centrifugal._Cnt[0]); put(D, he._Centrifugal._Cnt[1]);
+		put(D, ce._bcg._set.epsilon); put(D, ce._theta);
+	}
 
 	std::vector<double> h0, c0, s0;
 	Fields(m, h0, c0, s0);
@@ -148,6 +162,14 @@ int main(int argc, char **argv)
 	const int n = A.RowSize(), nnz = A.NonZero();
 	std::vector<int> rowptr(A.RowPtrData(), A.RowPtrData() + n + 1), col(A.ColIndData(), A.ColIndData() + nnz), flag(n);
 	for(int i = 0; i < n; ++i) flag[(size_t)i] = A.IsBC(i) ? 1 : 0;
+	//  the concentration equation's pattern (none without ConcField = WM)
+	std::vector<int> crow, ccol;
+	if(he._swConcField)
+	{
+		const CRS_Matrix &Ac = m->_concEq._crsA;
+		crow.assign(Ac.RowPtrData(), Ac.RowPtrData() + Ac.RowSize() + 1);
+		ccol.assign(Ac.ColIndData(), Ac.ColIndData() + Ac.NonZero());
+	}
 
 	auto t0 = std::chrono::steady_clock::now();
 	m->Run();
@@ -171,6 +193,10 @@ int main(int argc, char **argv)
 	std::fwrite(rowptr.data(), sizeof(int), rowptr.size(), f);
 	std::fwrite(col.data(), sizeof(int), col.size(), f);
 	std::fwrite(flag.data(), sizeof(int), flag.size(), f);
+	const int cn = crow.empty() ? 0 : (int)crow.size() - 1, cnnz = (int)ccol.size();
+	std::fwrite(&cn, sizeof(int), 1, f); std::fwrite(&cnnz, sizeof(int), 1, f);
+	std::fwrite(crow.data(), sizeof(int), crow.size(), f);
+	std::fwrite(ccol.data(), sizeof(int), ccol.size(), f);
 	std::fclose(f);
 	return 0;
 }

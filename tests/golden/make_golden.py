@@ -102,6 +102,26 @@ STEP_CASES = {
         "Physics.Slip.Enable": True, "Physics.Slip.Length": 5e-7,
         "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 2e-4,
     }, 4, 3),
+    # every height term with the upwinded ones (in-plane gravity, rotation,
+    # Marangoni) on the Koren-limited path, c carried unchanged, fixed dt
+    "step_upwind_48": ("allphys_2d_reg.toml", {
+        "Physics.ConcField.Model": "None", "Grid.Nx": 48, "Grid.Ny": 44,
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-3,
+    }, 3, 3),
+    # every term and the well-mixed concentration solved in every Newton pass
+    "step_wm_allphys_48": ("allphys_2d_reg.toml", {
+        "Grid.Nx": 48, "Grid.Ny": 40,
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-2,
+    }, 3, -1),
+    # the same with Navier slip, the VanLeer limiter, a Koren-limited
+    # concentration and the time-step control on
+    "step_wm_slip_adaptive_40": ("allphys_2d_reg.toml", {
+        "Grid.Nx": 40, "Grid.Ny": 40,
+        "Physics.Slip.Enable": True, "Physics.Slip.Length": 5e-7,
+        "Numerics.Convection.Height": "VanLeer", "Numerics.Convection.Concentration": "Koren",
+        "Numerics.TimeStepControl.Enable": True, "Numerics.TimeStepControl.KeepSteps": 2,
+        "Numerics.TimeStepControl.ChangeFactor": 0.75, "Numerics.InitialDt": 1e-2,
+    }, 6, -1),
     # capillary + disjoining with the time-step control on
     "step_adaptive_40": ("allphys_2d_reg.toml", {
         **_NO_UPWIND, "Grid.Nx": 40, "Grid.Ny": 40,
@@ -112,6 +132,14 @@ STEP_CASES = {
         "Numerics.TimeStepControl.Enable": True, "Numerics.TimeStepControl.KeepSteps": 2,
         "Numerics.TimeStepControl.ChangeFactor": 0.75, "Numerics.InitialDt": 1e-3,
     }, 10, 3),
+}
+
+
+#  Whole-step cases from the seeded case builder (yuzen_b200/cases.py): name:
+#  (builder name, keyword arguments)
+BUILT_STEP_CASES = {
+    # the all-physics film of the 512^2 workload on 64^2 cells, 3 steps
+    "step_allphys_64": ("allphys", {"N": 64, "steps": 3}),
 }
 
 
@@ -157,9 +185,48 @@ def make_step_case(ref: Path, name: str, work: Path) -> dict:
     if res.returncode != 0:
         raise RuntimeError(f"{name}: probe failed\n{res.stdout[-2000:]}\n{res.stderr[-2000:]}")
     d = stateio.read_state(work / f"{name}.bin")
-    sys_ = dumpio.read_dump(sorted(dump.glob("solve_*.bin"))[first])
-    d["sys_values"] = sys_["values"]
-    d["sys_rhs"] = sys_["rhs"]
+    dumps = sorted(dump.glob("solve_*.bin"))
+    if first >= 0:
+        sys_ = dumpio.read_dump(dumps[first])
+        d["sys_values"] = sys_["values"]
+        d["sys_rhs"] = sys_["rhs"]
+    else:
+        # the first Newton pass solves the concentration first (EveryNKLoop):
+        # the first dump after the set-up solves with the concentration flag
+        for f in dumps:
+            sys_ = dumpio.read_dump(f)
+            if sys_["conc"]:
+                d["csys_values"] = sys_["values"]
+                d["csys_rhs"] = sys_["rhs"]
+                d["csys_x"] = sys_["x"]
+                break
+    d["case"] = name
+    return d
+
+
+def make_built_step_case(name: str, work: Path) -> dict:
+    sys.path.insert(0, str(REPO))
+    from yuzen_b200 import cases
+    builder, kw = BUILT_STEP_CASES[name]
+    case = getattr(cases, builder)(**kw)
+    w = work / name
+    case.write_reference(w)
+    dump = (w / "dump").resolve()
+    dump.mkdir()
+    #  the restart's set-up solves of the boundary rows come first
+    env = dict(os.environ, YZO_DUMP_DIR=str(dump), YZO_DUMP_MAX="64", OMP_NUM_THREADS="4")
+    res = subprocess.run([str(PROBE), "case.toml", f"{name}.bin"], cwd=w, env=env, capture_output=True, text=True,
+                         timeout=900)
+    if res.returncode != 0:
+        raise RuntimeError(f"{name}: probe failed\n{res.stdout[-2000:]}\n{res.stderr[-2000:]}")
+    d = stateio.read_state(w / f"{name}.bin")
+    for f in sorted(dump.glob("solve_*.bin")):
+        sys_ = dumpio.read_dump(f)
+        if sys_["conc"]:
+            d["csys_values"] = sys_["values"]
+            d["csys_rhs"] = sys_["rhs"]
+            d["csys_x"] = sys_["x"]
+            break
     d["case"] = name
     return d
 
@@ -202,6 +269,12 @@ def main() -> None:
             if a.only and name != a.only:
                 continue
             d = make_step_case(Path(a.ref), name, Path(tmp))
+            stateio.save_npz(HERE / f"{name}.npz", d)
+            print(name, d["nx"], d["ny"], "steps", d["steps_done"], "t_end", d["t_end"])
+        for name in BUILT_STEP_CASES:
+            if a.only and name != a.only:
+                continue
+            d = make_built_step_case(name, Path(tmp))
             stateio.save_npz(HERE / f"{name}.npz", d)
             print(name, d["nx"], d["ny"], "steps", d["steps_done"], "t_end", d["t_end"])
         for name in CASES:

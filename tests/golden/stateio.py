@@ -12,6 +12,8 @@ INT_KEYS = (
     "on_evap", "conc_field", "slip", "dt_control", "evap_conc_func", "evap_spatial", "evap_hast_modify",
     "nk_max", "nk_min", "jacobi_interval", "lin_precond", "lin_scaling", "lin_maxit", "dt_keep_steps",
     "max_steps", "on_source",
+    "conv_height", "conv_conc", "conc_conv", "conc_diff", "lin_c_precond", "lin_c_scaling", "lin_c_maxit",
+    "lin_c_conc",
     # appended after the run
     "steps_done", "diverged",
 )
@@ -23,6 +25,7 @@ REAL_KEYS = (
     "ev_m_resin", "ev_m_solvent", "ev_e0", "ev_power_n", "ev_negpow_exp", "ev_negpow_rmax", "ev_conc_r", "ev_h_ast",
     "nk_eps", "nk_eps_rel", "lin_eps", "dt_change_factor", "dt_criterion", "dt_scale_floor",
     "x0", "y0", "t_start",
+    "xmin", "ymin", "rot_x", "rot_y", "lin_c_eps", "theta_c",
     # appended after the run
     "run_seconds", "t_end",
 )
@@ -51,6 +54,10 @@ def read_state(path) -> dict:
     d["rowptr"] = np.frombuffer(raw, "<i4", n + 1, off).copy(); off += 4 * (n + 1)
     d["col"] = np.frombuffer(raw, "<i4", nnz, off).copy(); off += 4 * nnz
     d["bc"] = np.frombuffer(raw, "<i4", n, off).copy(); off += 4 * n
+    cn = int(np.frombuffer(raw, "<i4", 1, off)[0]); off += 4
+    cnnz = int(np.frombuffer(raw, "<i4", 1, off)[0]); off += 4
+    d["rowptr_c"] = np.frombuffer(raw, "<i4", cn + 1 if cn else 0, off).copy(); off += 4 * (cn + 1 if cn else 0)
+    d["col_c"] = np.frombuffer(raw, "<i4", cnnz, off).copy(); off += 4 * cnnz
     return d
 
 

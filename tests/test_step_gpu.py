@@ -8,7 +8,10 @@ Bars: the CRS pattern bit for bit; the first pass's I + theta dt J entry by
 entry within 1e-12 of its row's largest entry and the right-hand side within
 1e-9 of its largest entry (the device's exp/pow/log1p may differ from the
 host's in the last place, and A h is a difference of terms ~1/dx^4 larger);
-h after N steps within 1e-10 relative L2, and the clock to 1e-12.
+h after N steps within 1e-10 relative L2, and the clock to 1e-12.  With
+the well-mixed concentration solved in every Newton pass: its pattern bit for
+bit, its first system as the film's, c after N steps within 1e-10 relative L2
+and its change over the steps within 1e-6.
 """
 from pathlib import Path
 
@@ -30,13 +33,20 @@ def make(d):
 @pytest.mark.parametrize("f", STEPS, ids=IDS)
 def test_pattern_bitwise(f):
     d = stateio.load_npz(f)
-    rowptr, col, bc = make(d).pattern()
+    st = make(d)
+    rowptr, col, bc = st.pattern()
     assert np.array_equal(rowptr, d["rowptr"]) and np.array_equal(col, d["col"]) and np.array_equal(bc, d["bc"])
+    #  the concentration equation's pattern (ConcField = WM only)
+    crow, ccol = st.conc_pattern()
+    assert np.array_equal(crow, d.get("rowptr_c", np.zeros(0, np.int32)))
+    assert np.array_equal(ccol, d.get("col_c", np.zeros(0, np.int32)))
 
 
 @pytest.mark.parametrize("f", STEPS, ids=IDS)
 def test_first_newton_system(f):
     d = stateio.load_npz(f)
+    if "sys_values" not in d:
+        pytest.skip("the first Newton pass solves the concentration first (test_first_conc_system)")
     st = make(d)
     ia, rhs = st.system(d["field_h0"], d["field_h0"], d["dt"])
     ref_ia, ref_rhs = d["sys_values"], d["sys_rhs"]
@@ -51,6 +61,27 @@ def test_first_newton_system(f):
 
 
 @pytest.mark.parametrize("f", STEPS, ids=IDS)
+def test_first_conc_system(f):
+    """The concentration system of the first Newton pass (ConcEquationBase.h:
+    302-369) entry by entry within 1e-12 of its row's largest entry, the
+    right-hand side within 1e-10 of its largest entry."""
+    d = stateio.load_npz(f)
+    if "csys_values" not in d:
+        pytest.skip("no concentration equation in this case")
+    st = make(d)
+    val, rhs = st.conc_system(d["field_h0"], d["field_c0"], d["dt"])
+    ref_val, ref_rhs = d["csys_values"], d["csys_rhs"]
+    rp = d["rowptr_c"]
+    rows = np.repeat(np.arange(rp.size - 1), np.diff(rp))
+    rowmax = np.zeros(rp.size - 1)
+    np.maximum.at(rowmax, rows, np.abs(ref_val))
+    err = np.abs(val - ref_val) / rowmax[rows]
+    assert err.max() <= 1e-12, err.max()
+    scale = np.abs(ref_rhs).max()
+    assert np.abs(rhs - ref_rhs).max() <= 1e-10 * scale + 1e-300, (np.abs(rhs - ref_rhs).max(), scale)
+
+
+@pytest.mark.parametrize("f", STEPS, ids=IDS)
 def test_fields_after_steps(f):
     d = stateio.load_npz(f)
     st = make(d)
@@ -60,4 +91,13 @@ def test_fields_after_steps(f):
     rel = np.linalg.norm(h - ref) / np.linalg.norm(ref)
     assert rel <= 1e-10, rel
     assert abs(stats["time"] - d["t_end"]) <= 1e-12 * abs(d["t_end"]), (stats["time"], d["t_end"])
-    assert np.array_equal(c, d["field_c1"])
+    if not d["conc_field"]:
+        assert np.array_equal(c, d["field_c1"])
+        return
+    #  the concentration: within 1e-10 relative L2, and its change over the
+    #  steps (small next to c itself) within 1e-6 of the reference's change
+    cref = d["field_c1"]
+    assert np.linalg.norm(c - cref) / np.linalg.norm(cref) <= 1e-10
+    dref = cref - d["field_c0"]
+    assert np.linalg.norm((c - d["field_c0"]) - dref) <= 1e-6 * np.linalg.norm(dref), \
+        (np.linalg.norm((c - d["field_c0"]) - dref), np.linalg.norm(dref))

@@ -37,6 +37,7 @@ EXPORTED_SYMBOLS = (
     "yz_step_create", "yz_step_destroy", "yz_step_advance", "yz_step_get_fields", "yz_step_pattern",
     "yz_step_system", "yz_pattern_2d", "yz_step_set_fields", "yz_launch_count",
     "yz_time_kernel", "yz_kernel_time", "yz_dot_noalloc", "yz_dot_noalloc_max",
+    "yz_step_conc_pattern", "yz_step_conc_system",
 )
 
 

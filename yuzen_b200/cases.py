@@ -32,6 +32,9 @@ PI = 4.0 * math.atan(1.0)   # Math::pi(), MyMath.h:110
 
 #  BoundaryCondition::tBoundaryCondition
 BC = {"Symmetry": 0, "Periodic": 1}
+#  C_Interpolation_base4::t_Scheme by its Numerics.Convection key (FiniteDifferences.cpp:216-226)
+SCHEMES = {"Upwind1": 0, "Upwind2": 1, "Central2": 2, "UTOPIA": 3, "QUICK": 4, "KK": 5, "Central4": 6,
+           "Koren": 7, "VanLeer": 8}
 
 
 def _toml_value(v) -> str:
@@ -99,6 +102,8 @@ class Case:
     h_init: np.ndarray | None = None    # (Ny, Nx) interior film, non-dimensional
     s_init: np.ndarray | None = None
     c_init: np.ndarray | None = None
+    conv_height: str = "Koren"          # Numerics.Convection.Height
+    conv_conc: str = "UTOPIA"           # Numerics.Convection.Concentration
     newton: dict = field(default_factory=lambda: {"max": 50, "min": 1, "eps": 1e-12, "eps_rel": 1e-6})
     linear: dict = field(default_factory=lambda: {"maxit": 8000, "eps": 1e-13, "precond": "ILU", "scaling": True})
     dtc: dict = field(default_factory=lambda: {"MaxDtFactor": 1.0e10, "MinDt": 1.0e-15, "Criterion": 1e-3,
@@ -148,6 +153,7 @@ class Case:
                        "ProbeList": {"TimeInterval": 1e30}},
             "Numerics": {
                 "InitialDt": self.dt, "MaxSteps": self.steps, "EndTime": self.end_time,
+                "Convection": {"Height": self.conv_height, "Concentration": self.conv_conc},
                 "TimeStepControl": {"Enable": self.dt_control, **self.dtc},
                 "HeightEquation": {"NewtonMaxIterations": self.newton["max"],
                                    "NewtonMinIterations": self.newton["min"],
@@ -297,8 +303,25 @@ class Case:
             "nk_eps": self.newton["eps"], "nk_eps_rel": self.newton["eps_rel"], "lin_eps": self.linear["eps"],
             "dt_change_factor": self.dtc["ChangeFactor"], "dt_criterion": self.dtc["Criterion"],
             "dt_scale_floor": self.dtc["ScaleFloor"], "x0": g["x0"], "y0": g["y0"], "t_start": 0.0,
+            "xmin": g["xmin"], "ymin": g["ymin"],
+            "rot_x": (self.centrifugal[1][0] if self.centrifugal else 0.0) / sc["L0"],
+            "rot_y": (self.centrifugal[1][1] if self.centrifugal else 0.0) / sc["L0"],
+            "conv_height": SCHEMES[self.conv_height], "conv_conc": SCHEMES[self.conv_conc],
+            "conc_conv": 1, "conc_diff": 1,
+            **self._conc_solver(),
             "field_h0": h, "field_c0": c, "field_s0": s,
         }
+
+    def _conc_solver(self) -> dict:
+        """The concentration equation's linear solver as the model holds it:
+        Numerics.ConcEquation.LinearSolver with the concentration role when
+        ConcField = WM; the LinearSolver defaults otherwise (the equation is
+        not built, LinearSolverBackend.h:48-50)."""
+        if self.conc_model == "WM":
+            return {"lin_c_precond": 2, "lin_c_scaling": 1, "lin_c_maxit": 5000, "lin_c_eps": 1e-13,
+                    "lin_c_conc": 1, "theta_c": 0.5}
+        return {"lin_c_precond": 2, "lin_c_scaling": 1, "lin_c_maxit": 100, "lin_c_eps": 1e-12,
+                "lin_c_conc": 0, "theta_c": 0.5}
 
     def _evap_params(self, sc: dict) -> dict:
         """C_Evaporation as NonDimensionalNumbers builds it (Coef 1, resin
@@ -348,4 +371,42 @@ def spinodal_224(N: int = 224, seed: int = 20261203, steps: int = 12, end_time: 
                 dt_control=True, disjoining=(10.0, 3.0, 2.0), h_init=h, conc0=0.5)
 
 
-CONFIGS = {"spinodal_224": spinodal_224}
+def allphys(N: int = 512, steps: int = 12, dt: float = 1e-5) -> Case:
+    """Config 3: every term of the well-mixed model on an N x N film with
+    Symmetry edges.  A film edge along a 30 degree oblique tanh front
+    (h = 1 behind it, the precursor 0.01 ahead, the front 8 cells wide),
+    Bo = 0.5, Pg = (0.2, 0.1), Sp = 0.3 about the centre, As Ma = 0.05,
+    Ev = 1e-3, Navier slip lambda = 0.05, the disjoining pressure with
+    theta_e = 10 deg, and the concentration solved (WM) from c0 = 0.2 with
+    mu(c) = exp(4c).  The dimensional inputs are chosen so that the reference's
+    NonDimensionalNumbers::Build gives those groups (to rounding), with the
+    custom length scale L0 = 100 um, h0 = 1 um; the cell is 5/512 L0 at every
+    N (the domain grows with N), so that smaller N are the same film on fewer
+    cells.  dt is fixed (seconds): at 1e-5 s the Newton iteration takes 4-5
+    passes per step, the fewest this film takes at any dt (4.5 per step from
+    1e-7 s to 1e-5 s, more above)."""
+    L0, h0, sig0, rho, mu0 = 1e-4, 1e-6, 30.0e-3, 1000.0, 100.0e-3
+    eps = h0 / L0
+    As = (L0 / h0) ** 2
+    T0 = mu0 * L0 ** 4 / (sig0 * h0 ** 3)
+    g_z = 0.5 * sig0 / (rho * L0 ** 2)
+    g_xy = (0.2 * sig0 * eps / (rho * L0 ** 2), 0.1 * sig0 * eps / (rho * L0 ** 2))
+    omega = math.sqrt(0.3 * sig0 * h0 / (rho * L0 ** 4))
+    dx = 5.0 / 512.0
+    half = 0.5 * N * dx * L0
+    xs = (np.arange(N) + 0.5) * dx - 0.5 * N * dx
+    X, Y = np.meshgrid(xs, xs)
+    s = X * math.cos(math.pi / 6.0) + Y * math.sin(math.pi / 6.0)
+    prec = 0.01
+    h = prec + (1.0 - prec) * 0.5 * (1.0 - np.tanh(s / (4.0 * dx)))
+    fluid = {"rho": rho, "sigma": sig0, "sigma_c0": 0.2, "sigma_coef": 0.05 / As * sig0,
+             "mu": mu0, "mu_c0": 0.0, "mu_exp": 4.0, "D": 1e-11, "D_c0": 0.2, "D_exp": 0.0,
+             "M_solvent": 100.0, "M_resin": 2000.0}
+    return Case(name=f"allphys_{N}", Nx=N, Ny=N, xlim=(-half, half), ylim=(-half, half), h0=h0, precursor=prec,
+                bc=("Symmetry",) * 4, dt=dt, steps=steps, dt_control=False, fluid=fluid, length_scale=L0,
+                vgrav=g_z, hgrav=g_xy, centrifugal=(omega, (0.0, 0.0)), marangoni=True,
+                disjoining=(10.0, 3.0, 2.0), evaporation={"Coef": 1e-3 * h0 / T0}, slip=0.05 * h0,
+                conc_model="WM", conc0=0.2, h_init=h)
+
+
+CONFIGS = {"spinodal_224": spinodal_224, "allphys_512": allphys}

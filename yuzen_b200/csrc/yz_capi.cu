@@ -254,6 +254,23 @@ int yz_step_system(yz_step *st, const double *h_old, const double *h, double dt,
 	});
 }
 
+int yz_step_conc_pattern(yz_step *st, int *rowptr, int *col)
+{
+	return Guard([&] {
+		if(!st) throw yz::UsageError("yz_step_conc_pattern: null step");
+		return st->s->ConcPattern(rowptr, col);
+	});
+}
+
+int yz_step_conc_system(yz_step *st, const double *h, const double *c, double dt, double *values, double *rhs)
+{
+	return Guard([&] {
+		if(!st || !h || !c || !values || !rhs) throw yz::UsageError("yz_step_conc_system: null argument");
+		st->s->ConcSystem(h, c, dt, values, rhs);
+		return 0;
+	});
+}
+
 int yz_pattern_2d(const yz_step_params *p, int *rowptr, int *col, int *bc)
 {
 	return Guard([&] {

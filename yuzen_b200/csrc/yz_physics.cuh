@@ -27,6 +27,49 @@ __device__ __forceinline__ int StencilDir(int k) { return k == 0 ? 2 : (k == 1 ?
 __device__ __forceinline__ int DirOfAdj(int idx) { return idx == mo ? 0 : (idx == po ? 1 : (idx == om ? 2 : (idx == op ? 3 : -1))); }
 __device__ __forceinline__ int NarrowIdx(int k) { return k == 0 ? om : (k == 1 ? mo : (k == 2 ? oo : (k == 3 ? po : op))); }
 
+//--------------------------------------------------------------------------
+//  stencil sets of the 2-D grid (GridTraits.h WM2D_Grid)
+//--------------------------------------------------------------------------
+//  FaceStencil(d, q): LL, L, R, RR of face d
+__host__ __device__ constexpr int FS(int d, int q)
+{
+	return d == 0 ? (q == 0 ? Mo : q == 1 ? mo : q == 2 ? oo : po)
+	     : d == 1 ? (q == 0 ? mo : q == 1 ? oo : q == 2 ? po : Po)
+	     : d == 2 ? (q == 0 ? oM : q == 1 ? om : q == 2 ? oo : op)
+	              : (q == 0 ? om : q == 1 ? oo : q == 2 ? op : oP);
+}
+//  AxisStencil(a, q), q = 0..4
+__host__ __device__ constexpr int AS(int a, int q)
+{
+	return a == 0 ? (q == 0 ? Mo : q == 1 ? mo : q == 2 ? oo : q == 3 ? po : Po)
+	              : (q == 0 ? oM : q == 1 ? om : q == 2 ? oo : q == 3 ? op : oP);
+}
+//  WideIdx(k), k = 0..8
+__host__ __device__ constexpr int WI(int k)
+{
+	return k == 0 ? oM : k == 1 ? om : k == 2 ? Mo : k == 3 ? mo : k == 4 ? oo : k == 5 ? po : k == 6 ? Po
+	     : k == 7 ? op : oP;
+}
+__host__ __device__ constexpr bool InFace(int d, int idx)
+{
+	return FS(d, 0) == idx || FS(d, 1) == idx || FS(d, 2) == idx || FS(d, 3) == idx;
+}
+__host__ __device__ constexpr int DirOfAdjC(int idx) { return idx == mo ? 0 : idx == po ? 1 : idx == om ? 2 : idx == op ? 3 : -1; }
+__host__ __device__ constexpr int StencilDirC(int k) { return k == 0 ? 2 : k == 1 ? 0 : k == 2 ? 1 : 3; }
+
+__host__ __device__ __forceinline__ double MSign(double x) { return x >= 0 ? 1.0 : -1.0; }   // Math::Sign
+
+//--------------------------------------------------------------------------
+//  C_Interpolation_base4 (FiniteDifferences.cpp:22-213): the four-point face
+//  interpolation; positions LL = 0, L = 1, R = 2, RR = 3
+//--------------------------------------------------------------------------
+struct Interp
+{
+	int kind;                 // YZ_SCHEME_*
+	int limited;              // Koren or VanLeer
+	double c1[4], c2[4];      // SetCoef (divided by the sum of c1)
+};
+
 //  what the assembly needs, passed by value to the kernels
 struct Coef
 {
@@ -44,14 +87,171 @@ struct Coef
 	double Ev;
 	int evConc, evSpatial, evHast;
 	double evMr, evMs, evPowN, evConcR, evNegExp, evNegRmax, evHast_h, evDr;
-	double x0, y0, dx, dy;
+	double xmin, ymin, dx, dy, dx2h, dy2h;   // grid corner, spacing, half spacing (RectGrid.h:459-465)
+	//  the upwinded terms (limited path, UpwindKernelBase.h / BodyForceKernel.h:527-691 /
+	//  SolutoCapillarityKernel.h:411-516)
+	int onPG, onSC, onCF;
+	int wall[4];                // IsWall of the Xmin, Xmax, Ymin, Ymax edges (Symmetry, Pinning)
+	Interp hI;                  // Numerics.Convection.Height (a limited scheme)
+	double pgMag[2], pgSign[2]; // Pg/3 per axis and Math::Sign(Pg)
+	double cfMag, cnt[2];       // Sp/3 and the rotation axis
+	double scMag;               // As*Ma/2
 };
+
+//  what the concentration equation's kernels need (ConcEquationBase.h)
+struct ConcCoef
+{
+	int nx, ny;
+	int conv, diff;
+	double th;                   // theta of the concentration equation (0.5)
+	double Df, dC0, dBase, dExp; // Df and the diffusivity law
+	double dxx, dyy;
+	Interp cI;                   // Numerics.Convection.Concentration
+};
+
+//  WallFace (GridTraits.h:524-538) for face d of the interior cell (ix, iy)
+__device__ __forceinline__ bool WallFace(const Coef &k, int d, int ix, int iy)
+{
+	switch(d)
+	{
+	case 0:  return ix == 2 && k.wall[0];
+	case 1:  return ix == k.nx - 3 && k.wall[1];
+	case 2:  return iy == 2 && k.wall[2];
+	default: return iy == k.ny - 3 && k.wall[3];
+	}
+}
+
+__device__ __forceinline__ double Limiter(int kind, double a, double b, double &pa, double &pb)
+{
+	double phi = 0;
+	pa = 0; pb = 0;
+	const bool same = (a > 0 && b > 0) || (a < 0 && b < 0);
+	if(same)
+	{
+		if(kind == 7)
+		{
+			const double s = (b > 0) ? 1.0 : -1.0;
+			const double aa = fabs(a), ab = fabs(b);
+			const double t1 = 2.0 * aa, t2 = (2.0 * ab + aa) / 3.0, t3 = 2.0 * ab;
+			if(t1 <= t2 && t1 <= t3) { phi = s * t1; pa = 2.0; pb = 0.0; }
+			else if(t2 <= t3) { phi = s * t2; pa = 1.0 / 3.0; pb = 2.0 / 3.0; }
+			else { phi = s * t3; pa = 0.0; pb = 2.0; }
+		}
+		else if(kind == 8)
+		{
+			const double sum = a + b;
+			const double ra = a / sum, rb = b / sum;
+			phi = 2.0 * a * rb;
+			pa = 2.0 * rb * rb;
+			pb = 2.0 * ra * ra;
+		}
+	}
+	return phi;
+}
+
+//  The upwind side (UpwindPositions, FiniteDifferences.cpp:146-150): sign >= 0
+//  takes (UU, U, D) = (LL, L, R), otherwise (RR, R, L).  Written with selects
+//  so that the four values stay in registers.
+__device__ __forceinline__ double FaceValue(const Interp &I, const double f[4], double sign)
+{
+	if(!I.limited)
+	{
+		double v = 0;
+#pragma unroll
+		for(int j = 0; j < 4; ++j) v += (I.c1[j] + MSign(sign) * I.c2[j]) * f[j];
+		return v;
+	}
+	const bool pos = sign >= 0;
+	const double fuu = pos ? f[0] : f[3], fu = pos ? f[1] : f[2], fd = pos ? f[2] : f[1];
+	double pa, pb;
+	return fu + 0.5 * Limiter(I.kind, fu - fuu, fd - fu, pa, pb);
+}
+
+//  rowPos: the position of the row's own cell (1 = L or 2 = R), or -1 for the
+//  downwind form
+__device__ __forceinline__ void FaceWeights(const Interp &I, const double f[4], double sign, int rowPos, double w[4])
+{
+	if(!I.limited)
+	{
+#pragma unroll
+		for(int j = 0; j < 4; ++j) w[j] = I.c1[j] + MSign(sign) * I.c2[j];
+		return;
+	}
+	const bool pos = sign >= 0;
+	const double fuu = pos ? f[0] : f[3], fu = pos ? f[1] : f[2], fd = pos ? f[2] : f[1];
+	const double a = fu - fuu, b = fd - fu;
+	double pa, pb;
+	const double phi = Limiter(I.kind, a, b, pa, pb);
+	w[0] = 0; w[1] = 0; w[2] = 0; w[3] = 0;
+	if(rowPos == (pos ? 1 : 2))
+	{
+		//  upwind form: f_U + chi/2 (f_U - f_UU)
+		const double chi = (a != 0) ? phi / a : 0.0;
+		const double wu = 1.0 + 0.5 * chi, wuu = -0.5 * chi;
+		if(pos) { w[1] = wu; w[0] = wuu; }
+		else { w[2] = wu; w[3] = wuu; }
+	}
+	else
+	{
+		//  downwind form: f_U + psi/2 (f_D - f_U)
+		const double psi = (b != 0) ? phi / b : 0.0;
+		const double wu = 1.0 - 0.5 * psi, wd = 0.5 * psi;
+		if(pos) { w[1] = wu; w[2] = wd; }
+		else { w[2] = wu; w[1] = wd; }
+	}
+}
+
+__device__ __forceinline__ double FaceDerivative(const Interp &I, const double f[4], double sign, double g[4])
+{
+	if(!I.limited)
+	{
+#pragma unroll
+		for(int j = 0; j < 4; ++j) g[j] = I.c1[j] + MSign(sign) * I.c2[j];
+		return FaceValue(I, f, sign);
+	}
+	const bool pos = sign >= 0;
+	const double fuu = pos ? f[0] : f[3], fu = pos ? f[1] : f[2], fd = pos ? f[2] : f[1];
+	double pa, pb;
+	const double phi = Limiter(I.kind, fu - fuu, fd - fu, pa, pb);
+	const double guu = -0.5 * pa, gu = 1.0 + 0.5 * (pa - pb), gd = 0.5 * pb;
+	if(pos) { g[0] = guu; g[1] = gu; g[2] = gd; g[3] = 0; }
+	else { g[3] = guu; g[2] = gu; g[1] = gd; g[0] = 0; }
+	return fu + 0.5 * phi;
+}
+
+//  the scheme's coefficients (FiniteDifferences.cpp:22-76)
+inline Interp MakeInterp(int kind)
+{
+	Interp I;
+	I.kind = kind;
+	I.limited = (kind == 7 || kind == 8);
+	double c1[4] = {0, 0, 0, 0}, c2[4] = {0, 0, 0, 0};
+	switch(kind)
+	{
+	case 0: c1[1] = 1; c1[2] = 1; c2[1] = 1; c2[2] = -1; break;
+	case 2: c1[1] = 1; c1[2] = 1; break;
+	case 6: c1[0] = -1; c1[1] = 9; c1[2] = 9; c1[3] = -1; break;
+	case 1: c1[0] = -1; c1[1] = 3; c1[2] = 3; c1[3] = -1; c2[0] = -1; c2[1] = 3; c2[2] = -3; c2[3] = 1; break;
+	case 3: case 7: c1[0] = -1; c1[1] = 7; c1[2] = 7; c1[3] = -1; c2[0] = -1; c2[1] = 3; c2[2] = -3; c2[3] = 1; break;
+	case 4: c1[0] = -1; c1[1] = 9; c1[2] = 9; c1[3] = -1; c2[0] = -1; c2[1] = 3; c2[2] = -3; c2[3] = 1; break;
+	case 5: c1[0] = -1; c1[1] = 7; c1[2] = 7; c1[3] = -1; c2[0] = -1; c2[1] = 3; c2[2] = -3; c2[3] = 1; break;
+	case 8: c1[0] = -1; c1[1] = 5; c1[2] = 5; c1[3] = -1; c2[0] = -1; c2[1] = 3; c2[2] = -3; c2[3] = 1; break;
+	default: break;
+	}
+	double denom = 0;
+	for(int j = 0; j < 4; ++j) denom += c1[j];
+	if(kind == 5) for(int j = 0; j < 4; ++j) c2[j] *= 3.0;
+	for(int j = 0; j < 4; ++j) { I.c1[j] = c1[j] / denom; I.c2[j] = c2[j] / denom; }
+	return I;
+}
 
 //--------------------------------------------------------------------------
 //  Mobility (model/Mobility.h)
 //--------------------------------------------------------------------------
 __device__ __forceinline__ double MobD(const Coef &k, double h) { const double u = fabs(h); return h * u * (u + k.a3); }
 __device__ __forceinline__ double MobdD(const Coef &k, double h) { const double u = fabs(h); return u * (3.0 * u + 2.0 * k.a3); }
+//  Mobility::DperH = Upwind (the slip mobility over h of an upwinded face)
+__device__ __forceinline__ double MobDperH(const Coef &k, double h) { const double u = fabs(h); return u * (u + k.a3); }
 
 __device__ inline double MobG(const Coef &k, double h)
 {

@@ -183,10 +183,11 @@ __global__ void KDot(int n, const double *__restrict__ x, const double *__restri
 //==========================================================================
 static const int kB = 256;
 
-Solver::Solver(int device) : _device(device)
+Solver::Solver(int device, cudaStream_t stream) : _device(device)
 {
 	YZ_CUDA(cudaSetDevice(device));
-	YZ_CUDA(cudaStreamCreateWithFlags(&_st, cudaStreamNonBlocking));
+	if(stream) { _st = stream; _ownStream = false; }
+	else YZ_CUDA(cudaStreamCreateWithFlags(&_st, cudaStreamNonBlocking));
 	YZ_CUDA(cudaEventCreate(&_ev0)); YZ_CUDA(cudaEventCreate(&_ev1)); YZ_CUDA(cudaEventCreate(&_ev2));
 	YZ_CUDA(cudaMallocHost(&_hsc, sizeof(Scal)));
 	_sc.reserve(1);
@@ -201,7 +202,7 @@ Solver::~Solver()
 	cudaStreamSynchronize(_st);
 	if(_hsc) cudaFreeHost(_hsc);
 	cudaEventDestroy(_ev0); cudaEventDestroy(_ev1); cudaEventDestroy(_ev2);
-	cudaStreamDestroy(_st);
+	if(_ownStream) cudaStreamDestroy(_st);
 }
 
 RedScratch Solver::Red(int site)

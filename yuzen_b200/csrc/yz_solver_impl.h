@@ -36,13 +36,15 @@ struct Level
 	DBuf<int> pptr, pcol, rptr, rcol;
 	DBuf<double> pval, rval;
 	bool direct = false;
-	DBuf<double> inv;		// column-major dense inverse of the direct level
+	DBuf<double> inv;		// row-major dense inverse of the direct level
 };
 
 class Solver
 {
 public:
-	explicit Solver(int device);
+	//  stream null: the solver makes (and owns) a stream of its own;
+	//  otherwise it runs on the caller's stream
+	explicit Solver(int device, cudaStream_t stream = nullptr);
 	~Solver();
 
 	void SetPattern(int n, int nnz, const int *rowptr, const int *scol, const int *ssrc);
@@ -75,6 +77,7 @@ private:
 
 	int _device;
 	cudaStream_t _st = nullptr;
+	bool _ownStream = true;
 	cudaEvent_t _ev0 = nullptr, _ev1 = nullptr, _ev2 = nullptr;
 	int _n = 0, _nnz = 0;
 	std::vector<int> _hptr, _hcol;

@@ -4,6 +4,8 @@
 // 157-486) and the time-step control (ImplicitSolver.cpp:144-190, 271-307),
 // around the device linear solve of yz_solver.cu.
 #include "yz_physics.cuh"
+#include "yz_upwind.cuh"
+#include "yz_conc.cuh"
 #include "yz_step_impl.h"
 
 #include <algorithm>
@@ -165,6 +167,11 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 				aA[idx] += k.coefV * val;
 			}
 		}
+		//  --- the upwinded terms into A_rest, in the order of the physics list
+		//  (HeightEquationBase.h:565-577): in-plane gravity, Marangoni, rotation
+		if(k.onPG) BodyForceA<kPG>(k, h, vis, ix, iy, aR);
+		if(k.onSC) MarangoniA(k, h, c, vis, ix, iy, aR);
+		if(k.onCF) BodyForceA<kCF>(k, h, vis, ix, iy, aR);
 		//  --- DisjoiningPressureKernel::SetMatrixA (DisjoiningPressureKernel.h:306-349)
 		double piN[13];
 		if(k.onD)
@@ -224,7 +231,8 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 		}
 		o.ax[i] = y;
 
-		const double xx = k.x0 + ix * k.dx, yy = k.y0 + iy * k.dy;
+		//  the cell centre (RectGrid::X of a cell site, RectGrid.h:375-383)
+		const double xx = k.xmin + ix * k.dx + k.dx2h, yy = k.ymin + iy * k.dy + k.dy2h;
 		if(mode == 0)
 		{
 			if(k.onEvap) o.evapOld[i] = EvapAt(k, hoo, coo, xx, yy, dt);
@@ -308,6 +316,9 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 				}
 			}
 		}
+		if(k.onPG) BodyForceJ<kPG>(k, h, vis, ix, iy, J);
+		if(k.onSC) MarangoniJ(k, h, c, vis, ix, iy, J);
+		if(k.onCF) BodyForceJ<kCF>(k, h, vis, ix, iy, J);
 		if(k.onD)
 		{
 			double Ad[4], gAdj[4], gCen[4];
@@ -464,9 +475,6 @@ Step::Step(int device, const yz_step_params &p, const double *h, const double *c
     : _device(device), _p(p)
 {
 	CheckParams(p);
-	if(p.on_pgrav || p.on_marangoni || p.on_centrifugal)
-		throw UsageError("step: the upwinded terms (HorizontalGravity, SolutoCapillarity, Centrifugal) are not built");
-	if(p.conc_field != 0) throw UsageError("step: the concentration equation (ConcField = WM) is not built");
 	if(p.theta <= 0.0) throw UsageError("step: theta must be > 0 (the implicit scheme)");
 	YZ_CUDA(cudaSetDevice(device));
 	_solver.reset(new Solver(device));
@@ -495,6 +503,10 @@ Step::Step(int device, const yz_step_params &p, const double *h, const double *c
 	_dt = p.dt; _dtOld = p.dt; _time = p.t_start;
 	YZ_LAUNCH(KSetGhostRows, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
 	          _dRowptr.get(), _ia.get(), _rhs.get());
+	_cw.reserve(n);
+	YZ_CUDA(cudaMemcpyAsync(_cw.get(), _c.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+	_conc = (p.conc_field != 0);
+	if(_conc) BuildConc();
 	YZ_CUDA(cudaStreamSynchronize(_st));
 }
 
@@ -553,6 +565,16 @@ void CheckParams(const yz_step_params &p)
 	if((p.bc[0] == YZ_BC_PERIODIC) != (p.bc[1] == YZ_BC_PERIODIC) || (p.bc[2] == YZ_BC_PERIODIC) != (p.bc[3] == YZ_BC_PERIODIC))
 		throw UsageError("step: a Periodic edge needs a Periodic opposite edge");
 	if(!p.on_laplace) throw UsageError("step: the capillary term (Physics.LaplacePressure) must be enabled");
+	if((p.on_pgrav || p.on_marangoni || p.on_centrifugal) && p.conv_height != YZ_SCHEME_KOREN &&
+	   p.conv_height != YZ_SCHEME_VANLEER)
+		throw UsageError("step: the upwinded terms are built on the limited path (Numerics.Convection.Height = "
+		                 "Koren or VanLeer)");
+	if(p.conc_field != 0)
+	{
+		if(p.conv_conc < YZ_SCHEME_UPWIND1 || p.conv_conc > YZ_SCHEME_VANLEER)
+			throw UsageError("step: unknown Numerics.Convection.Concentration scheme");
+		if(!(p.theta_c > 0.0)) throw UsageError("step: theta_c must be > 0");
+	}
 }
 
 void Step::BuildPattern()
@@ -625,7 +647,25 @@ void Step::BuildCoef()
 	k.evMr = p.ev_m_resin; k.evMs = p.ev_m_solvent; k.evPowN = p.ev_power_n; k.evConcR = p.ev_conc_r;
 	k.evNegExp = p.ev_negpow_exp; k.evNegRmax = p.ev_negpow_rmax; k.evHast_h = p.ev_h_ast;
 	k.evDr = dx < dy ? dx : dy;
-	k.x0 = p.x0; k.y0 = p.y0; k.dx = dx; k.dy = dy;
+	k.xmin = p.xmin; k.ymin = p.ymin; k.dx = dx; k.dy = dy; k.dx2h = dx * 0.5; k.dy2h = dy * 0.5;
+	//  the upwinded terms
+	k.onPG = p.on_pgrav; k.onSC = p.on_marangoni; k.onCF = p.on_centrifugal;
+	for(int e = 0; e < 4; ++e) k.wall[e] = (p.bc[e] == YZ_BC_SYMMETRY);   // BoundaryCondition::IsWall
+	k.hI = MakeInterp(p.conv_height);
+	const double pg[2] = {p.Pgx, p.Pgy};
+	for(int a = 0; a < 2; ++a) { k.pgMag[a] = pg[a] / 3.0; k.pgSign[a] = pg[a] >= 0 ? 1.0 : -1.0; }
+	k.cfMag = p.Sp / 3.0;
+	k.cnt[0] = p.rot_x; k.cnt[1] = p.rot_y;
+	k.scMag = p.As * p.Ma / 2.0;
+	//  the concentration equation
+	ConcCoef &q = _kc;
+	std::memset(&q, 0, sizeof q);
+	q.nx = p.nx; q.ny = p.ny;
+	q.conv = p.conc_convection; q.diff = p.conc_diffusion;
+	q.th = p.theta_c;
+	q.Df = p.Df; q.dC0 = p.diff_c0; q.dBase = p.diff_base; q.dExp = p.diff_exp;
+	q.dxx = dx; q.dyy = dy;
+	q.cI = MakeInterp(p.conv_conc);
 }
 
 double Step::ReadMax(int slot)
@@ -638,14 +678,14 @@ double Step::ReadMax(int slot)
 
 void Step::ZeroMax(int slot) { YZ_CUDA(cudaMemsetAsync(_red.get() + slot, 0, sizeof(unsigned long long), _st)); }
 
-void Step::Assemble(int mode, const double *hField, double dt)
+void Step::Assemble(int mode, const double *hField, const double *cField, double dt)
 {
 	RowOut o;
 	o.ia = _ia.get(); o.ax = mode == 0 ? _axOld.get() : _axGuess.get();
 	o.evapOld = _evapOld.get(); o.evapB = _evapB.get(); o.rhs = _rhs.get();
 	o.hOld = _hOld.get(); o.axOld = _axOld.get(); o.rhsMax = _red.get() + kSlotRhs;
 	const int nIn = (_p.nx - 4) * (_p.ny - 4);
-	YZ_LAUNCH(KAssemble, GridFor(nIn, 128, 148 * 32), 128, 0, _st, _k, mode, dt, _dRowptr.get(), hField, _c.get(),
+	YZ_LAUNCH(KAssemble, GridFor(nIn, 128, 148 * 32), 128, 0, _st, _k, mode, dt, _dRowptr.get(), hField, cField,
 	          _s.get(), o);
 }
 
@@ -678,9 +718,21 @@ bool Step::NKLoop(int &iter, double &resid, yz_step_stats &stats)
 			}
 		}
 	}
-	//  BeforeNKLoop: the working field is the committed one; SetMatrixA and
-	//  A(h^n) h^n with evapOld at h^n
-	Assemble(0, _hOld.get(), dt);
+	//  BeforeNKLoop (HeightEquationBase.h:1314-1387): the working field is the
+	//  committed one; with the concentration, the limiter and the reference
+	//  of the coupled correction at the step's start, the face fluxes there
+	//  (F0) and the solves of the step from d = 0.  Then SetMatrixA and
+	//  A(h^n) h^n with evapOld at h^n.
+	_coupled = 0;
+	YZ_CUDA(cudaMemcpyAsync(_cw.get(), _c.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+	if(_conc)
+	{
+		YZ_CUDA(cudaMemcpyAsync(_cLim.get(), _c.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+		YZ_CUDA(cudaMemcpyAsync(_cPrev.get(), _c.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+		FaceFluxes(_h.get(), _c.get(), _F0x.get(), _F0y.get(), dt, false);
+		YZ_CUDA(cudaMemsetAsync(_dC.get(), 0, (size_t)n * sizeof(double), _st));
+	}
+	Assemble(0, _hOld.get(), _c.get(), dt);
 
 	double residEqOld = 1e40, residFirst = 0, residBest = 1e40;
 	int stall = 0;
@@ -689,11 +741,14 @@ bool Step::NKLoop(int &iter, double &resid, yz_step_stats &stats)
 	int outer;
 	for(outer = 0; outer < _p.nk_max; ++outer)
 	{
-		//  EveryNKLoop: the working field's h is phi_guess (no concentration
-		//  equation here); Solve(): assembly at it
+		//  EveryNKLoop: the working field's h is phi_guess; with the
+		//  concentration, its solve at this film first (a failed one fails
+		//  the pass and with it the attempt).  Solve(): assembly at the film
+		//  and the working field's c.
+		if(_conc && !ConcPass(dt, stats)) { done = false; break; }
 		ZeroMax(kSlotRhs);
 		YZ_CUDA(cudaEventRecord(_e0, _st));
-		Assemble(1, _guess.get(), dt);
+		Assemble(1, _guess.get(), _cw.get(), dt);
 		YZ_CUDA(cudaEventRecord(_e1, _st));
 		++_nkIter;
 		//  opt ew (NewtonKantorovich.cpp:108-126)
@@ -733,6 +788,9 @@ bool Step::NKLoop(int &iter, double &resid, yz_step_stats &stats)
 		else YZ_CUDA(cudaMemsetAsync(_delta.get(), 0, (size_t)n * sizeof(double), _st));
 		YZ_LAUNCH(KAbsMax, g, 256, 0, _st, n, _delta.get(), _red.get() + kSlotDelta);
 		double residEq = ReadMax(kSlotDelta);
+		//  the convergence test takes the larger of the film's correction and
+		//  the concentration's (NewtonKantorovich.cpp:323)
+		if(_coupled > residEq) residEq = _coupled;
 		_lastResid = residEq;
 		if(ch != 0) { done = false; break; }
 		if(outer == 0) residFirst = residEq;
@@ -838,7 +896,9 @@ void Step::Advance(int nsteps, yz_step_stats &stats)
 			}
 		} while(!timeStepDone);
 		YZ_CUDA(cudaMemcpyAsync(_hNew.get(), _guess.get(), bytes, cudaMemcpyDeviceToDevice, _st));
-		//  AfterNKLoop without the concentration: the field takes the film
+		//  AfterNKLoop: with the concentration, the step of h c completed
+		//  (ConcCommit); the field takes the film
+		if(_conc) ConcCommit(_dt, stats);
 		YZ_CUDA(cudaMemcpyAsync(_h.get(), _guess.get(), bytes, cudaMemcpyDeviceToDevice, _st));
 		//  the clock: ++ (TimeSteps.cpp:121-160)
 		_time += _dt;
@@ -866,7 +926,13 @@ void Step::SetFields(const double *h, const double *c)
 		YZ_CUDA(cudaMemcpyAsync(_h.get(), h, bytes, cudaMemcpyHostToDevice, _st));
 		YZ_CUDA(cudaMemcpyAsync(_hNew.get(), _h.get(), bytes, cudaMemcpyDeviceToDevice, _st));
 	}
-	if(c) YZ_CUDA(cudaMemcpyAsync(_c.get(), c, bytes, cudaMemcpyHostToDevice, _st));
+	if(c)
+	{
+		YZ_CUDA(cudaMemcpyAsync(_c.get(), c, bytes, cudaMemcpyHostToDevice, _st));
+		YZ_CUDA(cudaMemcpyAsync(_cw.get(), _c.get(), bytes, cudaMemcpyDeviceToDevice, _st));
+		//  C_ImplicitSolver::SetX of the concentration equation
+		if(_conc) YZ_CUDA(cudaMemcpyAsync(_c0.get(), _c.get(), bytes, cudaMemcpyDeviceToDevice, _st));
+	}
 }
 
 void Step::GetFields(double *h, double *c)
@@ -891,11 +957,283 @@ void Step::System(const double *hOld, const double *h, double dt, double *ia, do
 	const size_t bytes = (size_t)_n * sizeof(double);
 	YZ_CUDA(cudaMemcpyAsync(_hOld.get(), hOld, bytes, cudaMemcpyHostToDevice, _st));
 	YZ_CUDA(cudaMemcpyAsync(_guess.get(), h, bytes, cudaMemcpyHostToDevice, _st));
-	Assemble(0, _hOld.get(), dt);
+	Assemble(0, _hOld.get(), _c.get(), dt);
 	ZeroMax(kSlotRhs);
-	Assemble(1, _guess.get(), dt);
+	Assemble(1, _guess.get(), _c.get(), dt);
 	_ia.download(ia, (size_t)_nnz, _st);
 	_rhs.download(rhs, (size_t)_n, _st);
+	YZ_CUDA(cudaStreamSynchronize(_st));
+}
+
+//==========================================================================
+//  The well-mixed concentration equation
+//==========================================================================
+//  Its pattern (C_ImplicitSolver::Alloc with ConcEquationBase::SetMatrixA,
+//  ConcEquationBase.h:243-259): the boundary rows of BoundaryCondition2D::
+//  Apply for the concentration (EqualVal [diag, partner] on Symmetry and
+//  Periodic edges, as for the film), interior rows the diagonal and the wide
+//  set in WideIdx order.
+void BuildConcPattern2D(const yz_step_params &p, std::vector<int> &rowptr, std::vector<int> &col)
+{
+	const int nx = p.nx, ny = p.ny, n = nx * ny;
+	rowptr.assign((size_t)n + 1, 0);
+	col.clear();
+	static const int wide[8][2] = {{0, -2}, {0, -1}, {-2, 0}, {-1, 0}, {1, 0}, {2, 0}, {0, 1}, {0, 2}};
+	for(int iy = 0; iy < ny; ++iy)
+		for(int ix = 0; ix < nx; ++ix)
+		{
+			const int i = iy * nx + ix;
+			col.push_back(i);
+			const bool inside = ix >= 2 && ix < nx - 2 && iy >= 2 && iy < ny - 2;
+			if(inside)
+				for(int q = 0; q < 8; ++q) col.push_back((iy + wide[q][1]) * nx + ix + wide[q][0]);
+			else
+			{
+				const int px = PartnerOf(ix, nx, p.bc[0], p.bc[1]);
+				const int py = PartnerOf(iy, ny, p.bc[2], p.bc[3]);
+				col.push_back(py * nx + px);
+			}
+			rowptr[(size_t)i + 1] = (int)col.size();
+		}
+}
+
+void Step::BuildConc()
+{
+	const size_t n = (size_t)_n;
+	BuildConcPattern2D(_p, _rowptrC, _colC);
+	_nnzC = (int)_colC.size();
+	std::vector<int> scol((size_t)_nnzC), ssrc((size_t)_nnzC);
+	std::vector<std::pair<int, int>> tmp;
+	for(int i = 0; i < _n; ++i)
+	{
+		const int st = _rowptrC[(size_t)i], ed = _rowptrC[(size_t)i + 1];
+		tmp.clear();
+		for(int q = st; q < ed; ++q) tmp.push_back({_colC[(size_t)q], q});
+		std::sort(tmp.begin(), tmp.end());
+		for(int q = st; q < ed; ++q) { scol[(size_t)q] = tmp[(size_t)(q - st)].first; ssrc[(size_t)q] = tmp[(size_t)(q - st)].second; }
+	}
+	_solverC.reset(new Solver(_device, _st));
+	_solverC->SetPattern(_n, _nnzC, _rowptrC.data(), scol.data(), ssrc.data());
+	_dRowptrC.upload(_rowptrC.data(), _rowptrC.size(), _st);
+	std::vector<int> pall(n);
+	for(int i = 0; i < _n; ++i) pall[(size_t)i] = i;
+	for(size_t g = 0; g < _ghost.size(); ++g) pall[(size_t)_ghost[g]] = _partner[g];
+	_dPartnerAll.upload(pall.data(), n, _st);
+	for(DBuf<double> *v : {&_c0, &_cLim, &_cPrev, &_cx, &_cxLast, &_dC, &_rhsC, &_F0x, &_F0y, &_F1x, &_F1y, &_evpStep,
+	                       &_rho, &_room, &_give})
+	{
+		v->reserve(n);
+		YZ_CUDA(cudaMemsetAsync(v->get(), 0, n * sizeof(double), _st));
+	}
+	for(DBuf<double> *v : {&_rowSum, &_accY})
+	{
+		v->reserve((size_t)_p.ny);
+		YZ_CUDA(cudaMemsetAsync(v->get(), 0, (size_t)_p.ny * sizeof(double), _st));
+	}
+	_sums.reserve(4);
+	_partStep.reserve((size_t)2 * RedBlocks(_n));
+	_cntStep.reserve(4);
+	YZ_CUDA(cudaMemsetAsync(_cntStep.get(), 0, 4 * sizeof(unsigned int), _st));
+	_iflags.reserve(4);
+	//  the matrix: the boundary rows [1, -1] once, the interior rows every solve
+	std::vector<double> vals((size_t)_nnzC, 0.0);
+	for(size_t g = 0; g < _ghost.size(); ++g)
+	{
+		const int i = _ghost[g];
+		vals[(size_t)_rowptrC[(size_t)i]] = 1.0;
+		vals[(size_t)_rowptrC[(size_t)i] + 1] = -1.0;
+	}
+	_iaC.upload(vals.data(), vals.size(), _st);
+	//  C_ImplicitSolver::SetX: c0 = c
+	YZ_CUDA(cudaMemcpyAsync(_c0.get(), _c.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+}
+
+RedScratch Step::StepRed(int site)
+{
+	RedScratch r;
+	r.part = _partStep.get();
+	r.counter = _cntStep.get() + site;
+	r.maxBlocks = RedBlocks(_n);
+	return r;
+}
+
+//  FaceVolumeFluxes of the film (H, C) into Fx / Fy; with withEvap, the
+//  evaporation of the step (StepSources); returns FilmNotPositive
+int Step::FaceFluxes(const double *H, const double *C, double *Fx, double *Fy, double dt, bool withEvap)
+{
+	const int nIn = (_p.nx - 4) * (_p.ny - 4);
+	int *bad = _iflags.get();
+	YZ_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), _st));
+	YZ_LAUNCH(KFaceFlux, GridFor(nIn, 128, 148 * 32), 128, 0, _st, _k, H, C, _s.get(), Fx, Fy, _evapOld.get(), dt,
+	          withEvap ? _evpStep.get() : nullptr, bad);
+	int h = 0;
+	YZ_CUDA(cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, _st));
+	YZ_CUDA(cudaStreamSynchronize(_st));
+	return h;
+}
+
+void Step::ConcAssemble(double dt)
+{
+	const int nIn = (_p.nx - 4) * (_p.ny - 4);
+	ConcIn in;
+	in.c0 = _c0.get(); in.cLim = _cLim.get(); in.h0 = _hOld.get(); in.h1 = _guess.get(); in.cw = _cw.get();
+	in.F0x = _F0x.get(); in.F0y = _F0y.get(); in.F1x = _F1x.get(); in.F1y = _F1y.get(); in.evp = _evpStep.get();
+	YZ_LAUNCH(KConcAssemble, GridFor(nIn, 128, 148 * 32), 128, 0, _st, _kc, dt, in, _dRowptrC.get(), _iaC.get(),
+	          _rhsC.get());
+	YZ_LAUNCH(KConcGhostRhs, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
+	          _dPartner.get(), _c0.get(), _rhsC.get());
+}
+
+//  _bcg.Solve of the concentration (ConcEquationBase.h:371): d in/out
+int Step::ConcSolve(yz_step_stats &stats)
+{
+	int it = 0; double res = 0;
+	const int ch = _solverC->Solve(_p.lin_conc, _iaC.get(), _rhsC.get(), _dC.get(), it, res);
+	double su = 0, sit = 0; _solverC->Timing(&su, &sit);
+	stats.setup_ms += su; stats.solve_ms += sit;
+	stats.conc_iterations += it;
+	stats.conc_solves += 1;
+	return ch;
+}
+
+//  The concentration part of EveryNKLoop (HeightEquationBase.h:1391-1444)
+bool Step::ConcPass(double dt, yz_step_stats &stats)
+{
+	const int n = _n, g = GridFor(n, 256);
+	//  the fluxes and the sources of this pass's film, and whether it has a
+	//  cell without liquid (then the concentration is left as it is)
+	if(FaceFluxes(_guess.get(), _cw.get(), _F1x.get(), _F1y.get(), dt, true)) { _coupled = 0; return true; }
+	ConcAssemble(dt);
+	const int ch = ConcSolve(stats);
+	if(ch != 0) return false;
+	ZeroMax(kSlotCorr);
+	YZ_LAUNCH(KConcUpdate, g, 256, 0, _st, n, 0, _dPartnerAll.get(), _c0.get(), _dC.get(), _rhsC.get(), _cx.get(),
+	          _cLim.get(), _cw.get(), _cPrev.get(), _red.get() + kSlotCorr);
+	_coupled = ReadMax(kSlotCorr);
+	return true;
+}
+
+//  The concentration part of AfterNKLoop (HeightEquationBase.h:1447-1576)
+void Step::ConcCommit(double dt, yz_step_stats &stats)
+{
+	const int n = _n, g = GridFor(n, 256);
+	const size_t bytes = (size_t)n * sizeof(double);
+	const int nx = _p.nx, ny = _p.ny;
+	//  the fluxes at the film the iteration ended on, with the last pass's c;
+	//  the evaporation as the last pass's B took it
+	const bool noFilm = FaceFluxes(_guess.get(), _cw.get(), _F1x.get(), _F1y.get(), dt, false) != 0;
+	YZ_CUDA(cudaMemcpyAsync(_evpStep.get(), _evapB.get(), bytes, cudaMemcpyDeviceToDevice, _st));
+	//  ConsistentFluxes: the fluxes of the step the film took
+	{
+		const int nIn = (nx - 4) * (ny - 4);
+		const double w = 1.0 / _p.theta;
+		YZ_LAUNCH(KRho, RedBlocks(nIn), kRT, 0, _st, nx, ny, _p.theta, dt, _hOld.get(), _guess.get(), _F1x.get(),
+		          _F1y.get(), _F0x.get(), _F0y.get(), _evpStep.get(), _rho.get(), StepRed(0), _sums.get());
+		YZ_LAUNCH(KRowPass, GridFor(ny - 4, 64), 64, 0, _st, nx, ny, w, _rho.get(), _sums.get(), _rowSum.get(),
+		          _F1x.get());
+		YZ_LAUNCH(KAccY, 1, 32, 0, _st, nx, ny, _rowSum.get(), _accY.get());
+		YZ_LAUNCH(KFyFix, GridFor((long long)(nx - 4) * (ny - 5), 256), 256, 0, _st, nx, ny, w, _accY.get(), _F1y.get());
+	}
+	//  the solve repeated with a limited scheme's limiter frozen at its own
+	//  answer until that settles
+	YZ_CUDA(cudaMemcpyAsync(_cxLast.get(), _cx.get(), bytes, cudaMemcpyDeviceToDevice, _st));
+	const bool limited = _kc.conv && _kc.cI.limited;
+	bool solved = true;
+	for(int k = 0; k < (limited ? 8 : 1) && !noFilm; ++k)
+	{
+		ConcAssemble(dt);
+		if(ConcSolve(stats) != 0) { solved = false; break; }
+		ZeroMax(kSlotCorr);
+		YZ_LAUNCH(KConcUpdate, g, 256, 0, _st, n, 1, _dPartnerAll.get(), _c0.get(), _dC.get(), _rhsC.get(), _cx.get(),
+		          _cLim.get(), _cw.get(), _cPrev.get(), _red.get() + kSlotCorr);
+		if(!limited) break;
+		if(ReadMax(kSlotCorr) <= 1e-12) break;
+	}
+	if(!solved) YZ_CUDA(cudaMemcpyAsync(_cx.get(), _cxLast.get(), bytes, cudaMemcpyDeviceToDevice, _st));
+	//  0 <= c <= 1 without taking solute away or making any
+	Redistribute();
+	//  CommitStep; the working field and the field take c1 capped at 1
+	YZ_LAUNCH(KConcCommit, g, 256, 0, _st, n, _cx.get(), _c0.get(), _cw.get(), _cLim.get(), _c.get());
+}
+
+//  RedistributeExcess (HeightEquationBase.h:1130-1170) on c1, with the film
+//  the step ended on
+void Step::Redistribute()
+{
+	const int n = _n, g = GridFor(n, 256);
+	int *flags = _iflags.get() + 1;
+	YZ_CUDA(cudaMemsetAsync(flags, 0, sizeof(int), _st));
+	YZ_LAUNCH(KExcessFlags, g, 256, 0, _st, n, _dIsbc.get(), _cx.get(), flags);
+	int f = 0;
+	YZ_CUDA(cudaMemcpyAsync(&f, flags, sizeof(int), cudaMemcpyDeviceToHost, _st));
+	YZ_CUDA(cudaStreamSynchronize(_st));
+	const bool over = (f & 1) != 0, under = (f & 2) != 0;
+	if(over) MoveExcess(false);
+	if(under) MoveExcess(true);
+	if(over || under)
+		YZ_LAUNCH(KGhostCopy, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
+		          _dPartner.get(), _cx.get());
+	YZ_LAUNCH(KBoundRows, g, 256, 0, _st, n, under ? 1 : 0, _cx.get());
+}
+
+void Step::MoveExcess(bool lower)
+{
+	const int n = _n, g = GridFor(n, 256), nx = _p.nx;
+	const int lw = lower ? 1 : 0;
+	int *flags = _iflags.get() + 2;
+	bool any = true;
+	for(int pass = 0; pass < 4 && any; ++pass)
+	{
+		YZ_LAUNCH(KRoom, g, 256, 0, _st, n, lw, _dIsbc.get(), _guess.get(), _cx.get(), _room.get());
+		YZ_CUDA(cudaMemsetAsync(flags, 0, sizeof(int), _st));
+		YZ_LAUNCH(KOutside, g, 256, 0, _st, nx, n, lw, pass, _dIsbc.get(), _guess.get(), _cx.get(), _room.get(),
+		          _give.get(), flags);
+		YZ_LAUNCH(KGain, g, 256, 0, _st, nx, n, lw, _dIsbc.get(), _guess.get(), _cx.get(), _room.get(), _give.get(),
+		          flags);
+		int h = 0;
+		YZ_CUDA(cudaMemcpyAsync(&h, flags, sizeof(int), cudaMemcpyDeviceToHost, _st));
+		YZ_CUDA(cudaStreamSynchronize(_st));
+		any = (h != 0);
+	}
+	if(!any) return;
+	//  what is left: spread over every real cell with room, in proportion
+	YZ_LAUNCH(KSpreadSums, RedBlocks(n), kRT, 0, _st, n, lw, _dIsbc.get(), _guess.get(), _cx.get(), StepRed(1),
+	          _sums.get() + 2);
+	double sums[2] = {0, 0};
+	YZ_CUDA(cudaMemcpyAsync(sums, _sums.get() + 2, sizeof sums, cudaMemcpyDeviceToHost, _st));
+	YZ_CUDA(cudaStreamSynchronize(_st));
+	const double left = sums[0], total = sums[1];
+	const double f = (total > 0.0) ? std::min(1.0, left / total) : 0.0;
+	if(f > 0.0) YZ_LAUNCH(KSpreadApply, g, 256, 0, _st, n, lw, _dIsbc.get(), _guess.get(), _cx.get(), f);
+}
+
+int Step::ConcPattern(int *rowptr, int *col) const
+{
+	if(!_conc) return 0;
+	if(rowptr) std::copy(_rowptrC.begin(), _rowptrC.end(), rowptr);
+	if(col) std::copy(_colC.begin(), _colC.end(), col);
+	return _nnzC;
+}
+
+//  The first pass's concentration system of a step from (h, c): h1 = h0 = h,
+//  F1 = F0, the limiter and the working field's c at c
+void Step::ConcSystem(const double *h, const double *c, double dt, double *val, double *rhs)
+{
+	if(!_conc) throw UsageError("step: the case has no concentration equation (conc_field = 0)");
+	YZ_CUDA(cudaSetDevice(_device));
+	const size_t bytes = (size_t)_n * sizeof(double);
+	YZ_CUDA(cudaMemcpyAsync(_hOld.get(), h, bytes, cudaMemcpyHostToDevice, _st));
+	YZ_CUDA(cudaMemcpyAsync(_guess.get(), h, bytes, cudaMemcpyHostToDevice, _st));
+	YZ_CUDA(cudaMemcpyAsync(_c0.get(), c, bytes, cudaMemcpyHostToDevice, _st));
+	YZ_CUDA(cudaMemcpyAsync(_cw.get(), c, bytes, cudaMemcpyHostToDevice, _st));
+	YZ_CUDA(cudaMemcpyAsync(_cLim.get(), c, bytes, cudaMemcpyHostToDevice, _st));
+	//  evapOld at h (mode 0 of the assembly), then the pass's fluxes and sources
+	Assemble(0, _hOld.get(), _cw.get(), dt);
+	FaceFluxes(_hOld.get(), _cw.get(), _F0x.get(), _F0y.get(), dt, false);
+	FaceFluxes(_guess.get(), _cw.get(), _F1x.get(), _F1y.get(), dt, true);
+	ConcAssemble(dt);
+	_iaC.download(val, (size_t)_nnzC, _st);
+	_rhsC.download(rhs, (size_t)_n, _st);
 	YZ_CUDA(cudaStreamSynchronize(_st));
 }
 

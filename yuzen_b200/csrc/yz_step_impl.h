@@ -23,16 +23,29 @@ public:
 	void SetFields(const double *h, const double *c);
 	int Pattern(int *rowptr, int *col, int *bc) const;
 	void System(const double *hOld, const double *h, double dt, double *ia, double *rhs);
+	int ConcPattern(int *rowptr, int *col) const;
+	void ConcSystem(const double *h, const double *c, double dt, double *val, double *rhs);
 	long long Launches() const { return _solver->Launches(); }
 	int Rows() const { return _n; }
 	int Nnz() const { return _nnz; }
 
 private:
-	enum { kSlotRhs = 0, kSlotDelta = 1, kSlotPhi = 2, kSlotMove = 3, kSlotLte = 4, kSlotBad = 5 };
+	enum { kSlotRhs = 0, kSlotDelta = 1, kSlotPhi = 2, kSlotMove = 3, kSlotLte = 4, kSlotBad = 5, kSlotCorr = 6,
+	       kSlotFlags = 7 };
 	void BuildPattern();
 	void BuildCoef();
-	void Assemble(int mode, const double *hField, double dt);
+	void Assemble(int mode, const double *hField, const double *cField, double dt);
 	bool NKLoop(int &iter, double &resid, yz_step_stats &stats);
+	//  the concentration equation
+	void BuildConc();
+	int FaceFluxes(const double *H, const double *C, double *Fx, double *Fy, double dt, bool withEvap);
+	void ConcAssemble(double dt);
+	int ConcSolve(yz_step_stats &stats);
+	bool ConcPass(double dt, yz_step_stats &stats);
+	void ConcCommit(double dt, yz_step_stats &stats);
+	void Redistribute();
+	void MoveExcess(bool lower);
+	RedScratch StepRed(int site);
 	double ReadMax(int slot);
 	void ZeroMax(int slot);
 
@@ -50,6 +63,23 @@ private:
 	//  phi_guess; A h at phi_old and at the guess; the system
 	DBuf<double> _h, _c, _s, _hOld, _hOld2, _hNew, _guess, _axOld, _axGuess, _rhs, _delta, _evapOld, _evapB, _ia;
 	DBuf<unsigned long long> _red;
+	//  the concentration equation: its pattern and solver; c0 (its phi_old),
+	//  the working field's c, the limiter state, the c of the last pass,
+	//  the solution c1 and the one before the solves that complete the step,
+	//  the correction d (and the next solve's guess), its system; the face
+	//  volume fluxes at the start of the step (F0) and at the pass's film (F1),
+	//  the evaporation of the step, ConsistentFluxes' and MoveExcess' scratch
+	bool _conc = false;
+	phys::ConcCoef _kc;
+	std::unique_ptr<Solver> _solverC;
+	int _nnzC = 0;
+	std::vector<int> _rowptrC, _colC;
+	DBuf<int> _dRowptrC, _dPartnerAll;
+	DBuf<double> _cw, _c0, _cLim, _cPrev, _cx, _cxLast, _dC, _rhsC, _iaC, _F0x, _F0y, _F1x, _F1y, _evpStep;
+	DBuf<double> _rho, _rowSum, _accY, _room, _give, _sums, _partStep;
+	DBuf<unsigned int> _cntStep;
+	DBuf<int> _iflags;
+	double _coupled = 0;
 	//  the clock (C_TimeSteps) and the Newton state
 	double _dt = 0, _dtOld = 0, _time = 0, _pendingDt = 0;
 	int _adjustCount = 0, _nkIter = 0;

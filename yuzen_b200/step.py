@@ -17,7 +17,7 @@ _f64p = ctypes.POINTER(ctypes.c_double)
 class StepParams(ctypes.Structure):
     _fields_ = [
         ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("bc", ctypes.c_int * 4),
-        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("x0", ctypes.c_double), ("y0", ctypes.c_double),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("xmin", ctypes.c_double), ("ymin", ctypes.c_double),
         ("theta", ctypes.c_double),
         ("on_laplace", ctypes.c_int), ("on_vgrav", ctypes.c_int), ("on_pgrav", ctypes.c_int),
         ("on_marangoni", ctypes.c_int), ("on_centrifugal", ctypes.c_int), ("on_disjoining", ctypes.c_int),
@@ -36,6 +36,15 @@ class StepParams(ctypes.Structure):
         ("dt", ctypes.c_double), ("dt_max", ctypes.c_double), ("dt_min", ctypes.c_double),
         ("dt_change_factor", ctypes.c_double), ("dt_criterion", ctypes.c_double), ("dt_scale_floor", ctypes.c_double),
         ("t_start", ctypes.c_double),
+        ("conv_height", ctypes.c_int),
+        ("Pgx", ctypes.c_double), ("Pgy", ctypes.c_double),
+        ("Sp", ctypes.c_double), ("rot_x", ctypes.c_double), ("rot_y", ctypes.c_double),
+        ("As", ctypes.c_double), ("Ma", ctypes.c_double),
+        ("conv_conc", ctypes.c_int), ("conc_convection", ctypes.c_int), ("conc_diffusion", ctypes.c_int),
+        ("theta_c", ctypes.c_double),
+        ("Df", ctypes.c_double), ("diff_c0", ctypes.c_double), ("diff_base", ctypes.c_double),
+        ("diff_exp", ctypes.c_double),
+        ("lin_conc", _Settings),
     ]
 
 
@@ -45,6 +54,7 @@ class StepStats(ctypes.Structure):
         ("retries", ctypes.c_int), ("time", ctypes.c_double), ("dt", ctypes.c_double),
         ("last_resid", ctypes.c_double), ("setup_ms", ctypes.c_double), ("solve_ms", ctypes.c_double),
         ("assemble_ms", ctypes.c_double), ("device_ms", ctypes.c_double), ("launches", ctypes.c_longlong),
+        ("conc_iterations", ctypes.c_int), ("conc_solves", ctypes.c_int),
     ]
 
     def as_dict(self) -> dict:
@@ -59,7 +69,7 @@ def params_from_state(d: dict) -> StepParams:
     p.nx, p.ny = d["nx"], d["ny"]
     for e, k in enumerate(("bc_xmin", "bc_xmax", "bc_ymin", "bc_ymax")):
         p.bc[e] = d[k]
-    p.dx, p.dy, p.x0, p.y0, p.theta = d["dx"], d["dy"], d["x0"], d["y0"], d["theta"]
+    p.dx, p.dy, p.xmin, p.ymin, p.theta = d["dx"], d["dy"], d["xmin"], d["ymin"], d["theta"]
     p.on_laplace, p.on_vgrav, p.on_pgrav = d["on_laplace"], d["on_vgrav"], d["on_pgrav"]
     p.on_marangoni, p.on_centrifugal, p.on_disjoining = d["on_marangoni"], d["on_centrifugal"], d["on_disjoining"]
     p.on_evap, p.conc_field = d["on_evap"], d["conc_field"]
@@ -77,6 +87,13 @@ def params_from_state(d: dict) -> StepParams:
     p.dt, p.dt_max, p.dt_min = d["dt"], d["dt_max"], d["dt_min"]
     p.dt_change_factor, p.dt_criterion, p.dt_scale_floor = d["dt_change_factor"], d["dt_criterion"], d["dt_scale_floor"]
     p.t_start = d["t_start"]
+    p.conv_height = d["conv_height"]
+    p.Pgx, p.Pgy, p.Sp, p.rot_x, p.rot_y = d["Pgx"], d["Pgy"], d["Sp"], d["rot_x"], d["rot_y"]
+    p.As, p.Ma = d["As"], d["Ma"]
+    p.conv_conc, p.conc_convection, p.conc_diffusion = d["conv_conc"], d["conc_conv"], d["conc_diff"]
+    p.theta_c = d["theta_c"]
+    p.Df, p.diff_c0, p.diff_base, p.diff_exp = d["Df"], d["diff_c0"], d["diff_base"], d["diff_exp"]
+    p.lin_conc = _Settings(d["lin_c_precond"], d["lin_c_scaling"], d["lin_c_maxit"], d["lin_c_eps"], d["lin_c_conc"])
     return p
 
 
@@ -98,6 +115,8 @@ def _bind():
     L.yz_step_pattern.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                   ctypes.POINTER(ctypes.c_int)]
     L.yz_step_system.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_double, _f64p, _f64p]
+    L.yz_step_conc_pattern.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    L.yz_step_conc_system.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_double, _f64p, _f64p]
     L.yz_pattern_2d.argtypes = [ctypes.POINTER(StepParams), ctypes.POINTER(ctypes.c_int),
                                 ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     _BOUND = True
@@ -154,6 +173,30 @@ class Step:
         rhs = np.zeros(self.n)
         _check(lib().yz_step_system(self._h, _fp(h_old), _fp(h), float(dt), _fp(ia), _fp(rhs)), "yz_step_system")
         return ia, rhs
+
+    def conc_pattern(self):
+        """The concentration equation's CRS pattern (rowptr, col); empty
+        arrays without the concentration equation."""
+        L = lib()
+        nnz = _check(L.yz_step_conc_pattern(self._h, None, None), "yz_step_conc_pattern")
+        if nnz == 0:
+            return np.zeros(0, np.int32), np.zeros(0, np.int32)
+        rowptr = np.zeros(self.n + 1, np.int32)
+        col = np.zeros(nnz, np.int32)
+        _check(L.yz_step_conc_pattern(self._h, _ip(rowptr), _ip(col)), "yz_step_conc_pattern")
+        return rowptr, col
+
+    def conc_system(self, h, c, dt: float):
+        """The first Newton pass's concentration system of a step from the
+        committed (h, c): (values in storage order, right-hand side)."""
+        h = np.ascontiguousarray(h, np.float64)
+        c = np.ascontiguousarray(c, np.float64)
+        rowptr, col = self.conc_pattern()
+        val = np.zeros(col.size)
+        rhs = np.zeros(self.n)
+        _check(lib().yz_step_conc_system(self._h, _fp(h), _fp(c), float(dt), _fp(val), _fp(rhs)),
+               "yz_step_conc_system")
+        return val, rhs
 
     def close(self) -> None:
         if self._h:
