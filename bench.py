@@ -7,9 +7,13 @@ film-height equation on B200, next to the reference's CPU solver.
 
 A step is one time step of the case (C_NewtonKantorovich::TimeAdvance and
 the clock, NewtonKantorovich.cpp:424-486): assembly, Newton passes, one
-BiCGStab + SA-AMG(SPAI0) solve per pass, all on the device.  The case is a
-seeded synthetic input built by yuzen_b200.cases (the reference reads the same
-film through its ASCII restart).  Timing: W untimed steps, then K steps, each
+BiCGStab + SA-AMG(SPAI0) solve of the film and one of the well-mixed
+concentration per pass, all on the device.  The default workload is the
+512 x 512 all-physics film (yuzen_b200.cases.allphys: capillary, disjoining,
+vertical and in-plane gravity, rotation, Marangoni, evaporation, slip, the
+concentration solved), on the plain FP64 path; the case is a seeded synthetic
+input built by yuzen_b200.cases (the reference reads the same film through
+its ASCII restart).  Timing: W untimed steps, then K steps, each
 timed with CUDA events on the library's stream, the L2 cache (126 MB) flushed
 by writing a 256 MiB buffer between steps (outside the timed region); under
 torchrun every rank runs an independent replica and the time is the maximum
@@ -185,7 +189,7 @@ def run_device_arm(a) -> None:
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    total_ms, newton, linear, launches = 0.0, 0, 0, 0
+    total_ms, newton, linear, launches, conc_solves, conc_iters = 0.0, 0, 0, 0, 0, 0
     parts = {"setup_ms": 0.0, "solve_ms": 0.0, "assemble_ms": 0.0}
     with Clocks(local) as clk:
         for _ in range(a.steps):
@@ -196,6 +200,8 @@ def run_device_arm(a) -> None:
             newton += r["newton_iterations"]
             linear += r["linear_iterations"]
             launches += r["launches"]
+            conc_solves += r["conc_solves"]
+            conc_iters += r["conc_iterations"]
             for k in parts:
                 parts[k] += r[k]
     if dist:
@@ -260,6 +266,8 @@ def run_device_arm(a) -> None:
         "config": {"workload": a.config, "grid": [cfg.Nx, cfg.Ny], "rows": n, "nnz": nnz,
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                    "l2": "flushed between steps (256 MiB write)",
+                   "path": "plain FP64 (the FP32 inner solve and the learned preconditioner are not built)",
+                   "conc_solves": conc_solves, "conc_iterations": conc_iters,
                    "newton_iterations": newton, "linear_iterations": linear,
                    "device_ms": {k: round(v, 3) for k, v in parts.items()},
                    "finite": finite},
@@ -281,8 +289,8 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=12)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="spinodal_224")
-    ap.add_argument("--cpu-steps", type=int, default=6)
+    ap.add_argument("--config", default="allphys_512")
+    ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     a = ap.parse_args()
     if a.warmup < 3 and a.impl == "b200":
