@@ -374,95 +374,249 @@ __global__ void KGemmFill(int nx, const int *__restrict__ xptr, const int *__res
 }
 
 //--------------------------------------------------------------------------
-//  Gauss-Jordan inverse of the coarsest level on [A | I], one launch per
-//  pivot step, double-buffered (M_in -> M_out).  Every block finds the pivot
-//  of column k itself (first row of largest |a|, rows k..n-1).
+//  The same product with one warp per output row: the row's distinct columns
+//  and sums in shared memory (at most CAP), X's row taken entry by entry and
+//  each Y row 32 entries at a time (a Y row holds a column once, so the
+//  lanes of one step never add into the same sum); every sum gets its
+//  contributions in X's row order from 0.0, as the thread-per-row kernels
+//  and the oracle give them.  FILL false: the count of every row (a row
+//  beyond CAP sets *overflow and is done again by KGemmCount<kRowCap>);
+//  FILL true: the row sorted by column into cptr[i]...
 //--------------------------------------------------------------------------
-__global__ void KGjInit(int n, const int *__restrict__ ptr, const int *__restrict__ col,
-                        const double *__restrict__ val, double *__restrict__ M)
+template<int CAP, bool FILL>
+__global__ void __launch_bounds__(256) KGemmWarp(int nx, const int *__restrict__ xptr, const int *__restrict__ xcol,
+                                                 const double *__restrict__ xval, const int *__restrict__ yptr,
+                                                 const int *__restrict__ ycol, const double *__restrict__ yval,
+                                                 int *__restrict__ cnt, const int *__restrict__ cptr,
+                                                 int *__restrict__ ccol, double *__restrict__ cval,
+                                                 int *__restrict__ overflow)
 {
-	const int w = 2 * n;
-	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	constexpr int W = 8;
+	__shared__ int scol[W][CAP];
+	__shared__ double sval[W][FILL ? CAP : 1];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	const unsigned lt = (1u << lane) - 1u;
+	const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+	for(long long row = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nx; row += warps)
 	{
-		for(int k = ptr[i]; k < ptr[i + 1]; ++k) M[(size_t)i * w + col[k]] = val[k];
-		M[(size_t)i * w + n + i] = 1.0;
+		const int i = (int)row;
+		int m = 0;
+		bool over = false;
+		for(int kx = xptr[i]; kx < xptr[i + 1] && !over; ++kx)
+		{
+			const int k = xcol[kx];
+			const double xv = FILL ? xval[kx] : 0.0;
+			const int y1 = yptr[k + 1];
+			for(int base = yptr[k]; base < y1 && !over; base += 32)
+			{
+				const int ky = base + lane;
+				const bool active = ky < y1;
+				const int j = active ? ycol[ky] : -1;
+				int slot = -1;
+				if(active)
+					for(int q = 0; q < m; ++q) if(scol[w][q] == j) { slot = q; break; }
+				const bool need = active && slot < 0;
+				const unsigned mask = __ballot_sync(0xffffffffu, need);
+				const int add = __popc(mask);
+				if(m + add > CAP) { over = true; break; }
+				if(need)
+				{
+					slot = m + __popc(mask & lt);
+					scol[w][slot] = j;
+					if(FILL) sval[w][slot] = 0.0;
+				}
+				m += add;
+				__syncwarp();
+				if(FILL && active) sval[w][slot] = sval[w][slot] + xv * yval[ky];
+				__syncwarp();
+			}
+		}
+		if(!FILL)
+		{
+			if(lane == 0)
+			{
+				if(over) { atomicExch(overflow, 1); cnt[i] = 0; }
+				else cnt[i] = m;
+			}
+		}
+		else
+		{
+			const int o = cptr[i];
+			for(int q = lane; q < m; q += 32)
+			{
+				const int c = scol[w][q];
+				int r = 0;
+				for(int t = 0; t < m; ++t) r += (scol[w][t] < c);
+				ccol[o + r] = c;
+				cval[o + r] = sval[w][q];
+			}
+		}
+		__syncwarp();
 	}
 }
 
-__global__ void KGjStep(int n, int k, const double *__restrict__ Min, double *__restrict__ Mout)
+//--------------------------------------------------------------------------
+//  Gauss-Jordan inverse of the coarsest level on [A | I] with partial
+//  pivoting (the oracle's GaussJordanInverse, yzo_solver.cpp), blocked.
+//  Step k of the unblocked algorithm changes every column j >= k by the same
+//  rule, in which only the column's own values, the pivot row p_k, the pivot
+//  piv_k and the multipliers f_k(i) = M[src_i][k] (column k before the step,
+//  src_i = k for i = p_k, else i) appear:
+//      row k:    M[k][j] = M[p][j] / piv
+//      row i:    M[i][j] = f == 0 ? M[src_i][j] : M[src_i][j] - f M[k][j]
+//  so a panel of B consecutive columns is run through its B steps by one
+//  block (recording p, piv and f of each), and every later column then
+//  replays those B steps on its own.  Each element sees exactly the
+//  operations of the unblocked algorithm, in the same order: the result is
+//  the oracle's to the bit, in 2 n / B launches instead of n.
+//  M is held column-major (column j at Mc + j n), n <= 3000.
+//--------------------------------------------------------------------------
+__global__ void KGjInit(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                        const double *__restrict__ val, double *__restrict__ Mc)
 {
-	const int w = 2 * n;
-	__shared__ double bv[256];
-	__shared__ int bi[256];
-	__shared__ int pivRow;
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
-		double best = -1.0; int idx = n;
-		for(int i = k + threadIdx.x; i < n; i += blockDim.x)
+		for(int k = ptr[i]; k < ptr[i + 1]; ++k) Mc[(size_t)col[k] * n + i] = val[k];
+		Mc[(size_t)(n + i) * n + i] = 1.0;
+	}
+}
+
+//  the pivot of column c of the panel among rows k..n-1: the first row of
+//  the largest |a|, taken only when larger than |a_kk| (the sequential rule)
+__device__ __forceinline__ int GjPivot(const double *colc, int n, int k, double *rv, int *ri)
+{
+	const int t = threadIdx.x, nt = blockDim.x;
+	double best = -1.0; int idx = n;
+	for(int i = k + t; i < n; i += nt)
+	{
+		const double a = fabs(colc[i]);
+		if(a > best || (a == best && i < idx)) { best = a; idx = i; }
+	}
+	rv[t] = best; ri[t] = idx;
+	__syncthreads();
+	for(int off = nt / 2; off >= 1; off >>= 1)
+	{
+		if(t < off)
 		{
-			const double a = fabs(Min[(size_t)i * w + k]);
-			if(a > best || (a == best && i < idx)) { best = a; idx = i; }
+			const double a = rv[t + off]; const int ia = ri[t + off];
+			if(a > rv[t] || (a == rv[t] && ia < ri[t])) { rv[t] = a; ri[t] = ia; }
 		}
-		bv[threadIdx.x] = best; bi[threadIdx.x] = idx;
 		__syncthreads();
-		for(int off = blockDim.x / 2; off >= 1; off >>= 1)
+	}
+	const int p = (rv[0] > fabs(colc[k])) ? ri[0] : k;
+	__syncthreads();
+	return p;
+}
+
+//  one block of 512 threads: the B columns k0..k0+B-1, their steps; records
+//  pivRow, pivVal and F (B x n) for the columns after them
+__global__ void __launch_bounds__(512) KGjPanel(int n, int k0, int B, const double *__restrict__ Mc,
+                                                double *__restrict__ F, int *__restrict__ pivRow,
+                                                double *__restrict__ pivVal)
+{
+	extern __shared__ double smem[];
+	double *P = smem;                                  // B columns of n
+	double *rv = smem + (size_t)B * n;                 // 512 reduction values
+	int *ri = reinterpret_cast<int *>(rv + 512);       // 512 reduction indices
+	__shared__ int sp;
+	__shared__ double spiv;
+	const int t = threadIdx.x, nt = blockDim.x;
+	for(int e = t; e < B * n; e += nt) P[e] = Mc[(size_t)k0 * n + e];
+	__syncthreads();
+	const int lane = t & 31, warp = t >> 5, nw = nt >> 5;
+	for(int c = 0; c < B; ++c)
+	{
+		const int k = k0 + c;
+		double *colc = P + (size_t)c * n;
+		const int p = GjPivot(colc, n, k, rv, ri);
+		if(t == 0) { sp = p; spiv = colc[p]; pivRow[c] = p; pivVal[c] = colc[p]; }
+		//  the multipliers, column c before the step
+		for(int i = t; i < n; i += nt) F[(size_t)c * n + i] = colc[(i == p) ? k : i];
+		__syncthreads();
+		const double piv = spiv;
+		//  the step on the panel's columns c..B-1, one warp per column
+		for(int cc = c + warp; cc < B; cc += nw)
 		{
-			if((int)threadIdx.x < off)
+			double *cl = P + (size_t)cc * n;
+			const double colp = cl[p], colk = cl[k];
+			__syncwarp();
+			const double rowK = colp / piv;
+			for(int i = lane; i < n; i += 32)
 			{
-				const double a = bv[threadIdx.x + off]; const int ia = bi[threadIdx.x + off];
-				if(a > bv[threadIdx.x] || (a == bv[threadIdx.x] && ia < bi[threadIdx.x])) { bv[threadIdx.x] = a; bi[threadIdx.x] = ia; }
+				double out;
+				if(i == k) out = rowK;
+				else
+				{
+					const int src = (i == p) ? k : i;
+					const double f = F[(size_t)c * n + i];
+					const double mij = (src == k) ? colk : cl[i];
+					out = (f == 0.0) ? mij : mij - f * rowK;
+				}
+				cl[i] = out;
 			}
-			__syncthreads();
-		}
-		if(threadIdx.x == 0)
-		{
-			//  the sequential rule: rows after k replace k only when strictly larger
-			const double akk = fabs(Min[(size_t)k * w + k]);
-			pivRow = (bv[0] > akk) ? bi[0] : k;
+			__syncwarp();
 		}
 		__syncthreads();
 	}
-	const int p = pivRow;
-	const double piv = Min[(size_t)p * w + k];
-	const int span = w - k;				// columns k .. 2n-1
-	const long long total = (long long)n * span;
-	for(long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x)
+}
+
+//  every column j >= jStart replays the panel's B steps; one block per column
+__global__ void KGjUpdate(int n, int k0, int B, int jStart, double *__restrict__ Mc, const double *__restrict__ F,
+                          const int *__restrict__ pivRow, const double *__restrict__ pivVal)
+{
+	extern __shared__ double colv[];
+	__shared__ double sColp, sColk;
+	const int j = jStart + blockIdx.x;
+	const int t = threadIdx.x, nt = blockDim.x;
+	double *g = Mc + (size_t)j * n;
+	for(int i = t; i < n; i += nt) colv[i] = g[i];
+	__syncthreads();
+	for(int c = 0; c < B; ++c)
 	{
-		const int i = (int)(e / span);
-		const int j = k + (int)(e % span);
-		const double rowK = Min[(size_t)p * w + j] / piv;		// the scaled pivot row
-		double out;
-		if(i == k) out = rowK;
-		else
+		const int k = k0 + c, p = pivRow[c];
+		if(t == 0) { sColp = colv[p]; sColk = colv[k]; }
+		__syncthreads();
+		const double rowK = sColp / pivVal[c], colk = sColk;
+		for(int i = t; i < n; i += nt)
 		{
-			const int src = (i == p) ? k : i;
-			const double f = Min[(size_t)src * w + k];
-			const double mij = Min[(size_t)src * w + j];
-			out = (f == 0.0) ? mij : mij - f * rowK;
+			double out;
+			if(i == k) out = rowK;
+			else
+			{
+				const int src = (i == p) ? k : i;
+				const double f = F[(size_t)c * n + i];
+				const double mij = (src == k) ? colk : colv[i];
+				out = (f == 0.0) ? mij : mij - f * rowK;
+			}
+			colv[i] = out;
 		}
-		Mout[(size_t)i * w + j] = out;
+		__syncthreads();
 	}
+	for(int i = t; i < n; i += nt) g[i] = colv[i];
 }
 
 //  the right half of [I | A^-1], row-major
-__global__ void KGjExtract(int n, const double *__restrict__ M, double *__restrict__ inv)
+__global__ void KGjExtract(int n, const double *__restrict__ Mc, double *__restrict__ inv)
 {
-	const int w = 2 * n;
 	const long long total = (long long)n * n;
 	for(long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x)
 	{
 		const int i = (int)(e / n), j = (int)(e % n);
-		inv[(size_t)i * n + j] = M[(size_t)i * w + n + j];
+		inv[(size_t)i * n + j] = Mc[(size_t)(n + j) * n + i];
 	}
 }
 
 //--------------------------------------------------------------------------
-//  V-cycle
+//  V-cycle.  Every kernel of the solve's iteration takes halt, the state
+//  word of its BiCGStab run (non-zero once it has stopped), and does nothing
+//  when it is set: the iterations are queued ahead of the host's check.
 //--------------------------------------------------------------------------
 //  x = m .* f, t = f - A x (x of the neighbours recomputed as m_j * f_j)
-__global__ void KPreSmoothResidual(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+__global__ void KPreSmoothResidual(const int *__restrict__ halt, int n, const int *__restrict__ ptr, const int *__restrict__ col,
                                    const double *__restrict__ val, const double *__restrict__ M,
                                    const double *__restrict__ f, double *__restrict__ x, double *__restrict__ t)
 {
+	if(halt && *halt) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		double s = 0.0;
@@ -472,15 +626,17 @@ __global__ void KPreSmoothResidual(int n, const int *__restrict__ ptr, const int
 	}
 }
 
-__global__ void KPreSmooth(int n, const double *__restrict__ M, const double *__restrict__ f, double *__restrict__ x)
+__global__ void KPreSmooth(const int *__restrict__ halt, int n, const double *__restrict__ M, const double *__restrict__ f, double *__restrict__ x)
 {
+	if(halt && *halt) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = M[i] * f[i];
 }
 
 //  y = A x (from 0.0, stored order)
-__global__ void KSpmv(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+__global__ void KSpmv(const int *__restrict__ halt, int n, const int *__restrict__ ptr, const int *__restrict__ col,
                       const double *__restrict__ val, const double *__restrict__ x, double *__restrict__ y)
 {
+	if(halt && *halt) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		double s = 0.0;
@@ -490,10 +646,11 @@ __global__ void KSpmv(int n, const int *__restrict__ ptr, const int *__restrict_
 }
 
 //  xout = x + P xc
-__global__ void KProlong(int n, const int *__restrict__ pptr, const int *__restrict__ pcol,
+__global__ void KProlong(const int *__restrict__ halt, int n, const int *__restrict__ pptr, const int *__restrict__ pcol,
                          const double *__restrict__ pval, const double *__restrict__ xc,
                          const double *__restrict__ x, double *__restrict__ xout)
 {
+	if(halt && *halt) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		double s = 0.0;
@@ -503,10 +660,11 @@ __global__ void KProlong(int n, const int *__restrict__ pptr, const int *__restr
 }
 
 //  xout = x + m .* (f - A x)
-__global__ void KPostSmooth(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+__global__ void KPostSmooth(const int *__restrict__ halt, int n, const int *__restrict__ ptr, const int *__restrict__ col,
                             const double *__restrict__ val, const double *__restrict__ M,
                             const double *__restrict__ f, const double *__restrict__ x, double *__restrict__ xout)
 {
+	if(halt && *halt) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		double s = 0.0;
@@ -518,8 +676,9 @@ __global__ void KPostSmooth(int n, const int *__restrict__ ptr, const int *__res
 
 //  x = inv f, inv row-major: one warp per row, lane l sums j = l, l+32, ...
 //  from 0.0 (coalesced reads of the row), then a pairwise shuffle fold
-__global__ void KDenseMV(int n, const double *__restrict__ inv, const double *__restrict__ f, double *__restrict__ x)
+__global__ void KDenseMV(const int *__restrict__ halt, int n, const double *__restrict__ inv, const double *__restrict__ f, double *__restrict__ x)
 {
+	if(halt && *halt) return;
 	const int lane = threadIdx.x & 31;
 	const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
 	for(long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps)
@@ -533,8 +692,9 @@ __global__ void KDenseMV(int n, const double *__restrict__ inv, const double *__
 	}
 }
 
-__global__ void KDiagApply(int n, const double *__restrict__ M, const double *__restrict__ r, double *__restrict__ z)
+__global__ void KDiagApply(const int *__restrict__ halt, int n, const double *__restrict__ M, const double *__restrict__ r, double *__restrict__ z)
 {
+	if(halt && *halt) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] = M[i] * r[i];
 }
 

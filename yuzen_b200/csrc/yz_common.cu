@@ -21,6 +21,8 @@ bool TimedKernel(const char *name)
 	return g_timeName == name;
 }
 
+bool TimingActive() { return !g_timeName.empty(); }
+
 void TimeBegin(cudaStream_t st)
 {
 	std::lock_guard<std::mutex> lk(g_timeMutex);

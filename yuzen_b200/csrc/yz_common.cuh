@@ -38,6 +38,7 @@ inline void Check(cudaError_t e, const char *what)
 //  events on its own stream (the per-launch device time of that kernel).
 extern std::atomic<long long> g_launches;
 bool TimedKernel(const char *name);
+bool TimingActive();   // a kernel is selected for per-launch timing
 void TimeBegin(cudaStream_t st);
 void TimeEnd(cudaStream_t st);
 

@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 namespace yz {
@@ -51,10 +52,16 @@ __global__ void KBInit(int n, const int *__restrict__ ptr, const int *__restrict
 	}
 }
 
-//  p = r (first pass) or p = r + beta (p - omega v)
-__global__ void KPUpdate(int n, int first, const double *__restrict__ r, const double *__restrict__ v,
-                         double *__restrict__ p, const Scal *sc)
+//  The top of an iteration (the oracle's `while(it < maxIter)` and its
+//  breakdown test), then p = r (first pass) or p = r + beta (p - omega v)
+__global__ void KPUpdate(int n, const double *__restrict__ r, const double *__restrict__ v,
+                         double *__restrict__ p, Scal *sc)
 {
+	if(sc->state != kRun) return;
+	const bool lead = (blockIdx.x == 0 && threadIdx.x == 0);
+	if(sc->it >= sc->maxIter) { if(lead) sc->state = kCap; return; }
+	if(sc->rho == 0.0) { if(lead) sc->state = kBreak; return; }
+	const int first = (sc->it == 0);
 	if(first)
 	{
 		for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = r[i];
@@ -71,6 +78,7 @@ __global__ void KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__rest
                            const double *__restrict__ val, const double *__restrict__ ph,
                            const double *__restrict__ rh, double *__restrict__ v, RedScratch rs, Scal *sc)
 {
+	if(sc->state != kRun) return;
 	__shared__ double sh[kRT];
 	double a[1] = {0.0};
 	YZ_CHUNK_LOOP(i)
@@ -89,6 +97,7 @@ __global__ void KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__rest
 __global__ void KSUpdate(int n, const double *__restrict__ r, const double *__restrict__ v,
                          double *__restrict__ s, RedScratch rs, Scal *sc)
 {
+	if(sc->state != kRun) return;
 	__shared__ double sh[kRT];
 	const double alpha = sc->alpha;
 	double a[1] = {0.0};
@@ -100,12 +109,20 @@ __global__ void KSUpdate(int n, const double *__restrict__ r, const double *__re
 		a[0] = a[0] + si * si;
 	}
 	double tot[1];
-	if(GridFold<1>(a, sh, rs, tot) && threadIdx.x == 0) sc->res = sqrt(tot[0]);
+	if(GridFold<1>(a, sh, rs, tot) && threadIdx.x == 0)
+	{
+		const double res = sqrt(tot[0]);
+		sc->res = res;
+		//  converged at the half step: x takes alpha ph (KXHalf) and the
+		//  iteration counts
+		if(res <= sc->eps) { sc->state = kConvHalf; sc->it += 1; }
+	}
 }
 
 //  x = x + alpha ph  (the half-step exit)
 __global__ void KXHalf(int n, const double *__restrict__ ph, double *__restrict__ x, const Scal *sc)
 {
+	if(sc->state != kConvHalf) return;
 	const double alpha = sc->alpha;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = x[i] + alpha * ph[i];
 }
@@ -115,6 +132,7 @@ __global__ void KSpmvOmega(int n, const int *__restrict__ ptr, const int *__rest
                            const double *__restrict__ val, const double *__restrict__ sh_,
                            const double *__restrict__ s, double *__restrict__ t, RedScratch rs, Scal *sc)
 {
+	if(sc->state != kRun) return;
 	__shared__ double sh[2 * kRT];
 	double a[2] = {0.0, 0.0};
 	YZ_CHUNK_LOOP(i)
@@ -136,6 +154,7 @@ __global__ void KXRUpdate(int n, const double *__restrict__ ph, const double *__
                           const double *__restrict__ rh, double *__restrict__ x, double *__restrict__ r,
                           RedScratch rs, Scal *sc)
 {
+	if(sc->state != kRun) return;
 	__shared__ double sh[2 * kRT];
 	const double alpha = sc->alpha, omega = sc->omega;
 	double a[2] = {0.0, 0.0};
@@ -151,11 +170,31 @@ __global__ void KXRUpdate(int n, const double *__restrict__ ph, const double *__
 	double tot[2];
 	if(GridFold<2>(a, sh, rs, tot) && threadIdx.x == 0)
 	{
-		sc->res = sqrt(tot[0]);
+		const double res = sqrt(tot[0]);
+		sc->res = res;
 		sc->rhoPrev = sc->rho;
 		sc->rho = tot[1];
+		sc->it += 1;
+		if(res <= sc->eps) sc->state = kConv;
+		else if(!(res == res)) sc->state = kNaN;
 	}
 }
+
+//  the start of the iterations: the tolerance, the cap, the counters
+__global__ void KCtlInit(Scal *sc, double eps, int maxIter)
+{
+	sc->eps = eps; sc->maxIter = maxIter; sc->it = 0; sc->state = kRun; sc->bodies = 0;
+}
+
+//  the loop's condition: another iteration while the run goes on
+__global__ void KLoopCond(cudaGraphConditionalHandle h, Scal *sc)
+{
+	sc->bodies += 1;
+	cudaGraphSetConditional(h, sc->state == kRun ? 1u : 0u);
+}
+
+//  the same count where the iterations are queued one by one
+__global__ void KLoopCount(Scal *sc) { sc->bodies += 1; }
 
 __global__ void KFill(int n, double v, double *__restrict__ x)
 {
@@ -227,6 +266,7 @@ void Solver::SetPattern(int n, int nnz, const int *rowptr, const int *scol, cons
 	_hcol.assign(scol, scol + nnz);
 	_levels.clear();
 	_levels.emplace_back(new Level());
+	_nlev = 1;
 	Level &L0 = *_levels[0];
 	L0.n = n; L0.nnz = nnz;
 	L0.ptr.upload(rowptr, (size_t)n + 1, _st);
@@ -272,16 +312,18 @@ int Solver::ScanCounts(const int *cnt, int *out, int n)
 	return ReadInt(out + n);
 }
 
-//  C = X Y (KGemmCount / KGemmFill): first with room for 64 distinct
-//  columns per row in registers, again with kRowCap if a row needs more;
+//  C = X Y: one warp per row with room for 64 distinct columns (KGemmWarp),
+//  the thread-per-row kernels with kRowCap where a row needs more;
 //  returns nnz(C)
 int Solver::Gemm(int nx, const int *xptr, const int *xcol, const double *xval, const int *yptr, const int *ycol,
                  const double *yval, DBuf<int> &cptr, DBuf<int> &ccol, DBuf<double> &cval)
 {
 	int *overflow = _flags.get() + 1;
 	const int g = GridFor(nx, 128);
+	const int gw = GridFor((long long)nx * 32, 256, 148 * 64);
 	YZ_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int), _st));
-	YZ_LAUNCH(KGemmCount<64>, g, 128, 0, _st, nx, xptr, xcol, yptr, ycol, _cnt.get(), overflow);
+	YZ_LAUNCH((KGemmWarp<64, false>), gw, 256, 0, _st, nx, xptr, xcol, xval, yptr, ycol, yval, _cnt.get(), nullptr,
+	          nullptr, nullptr, overflow);
 	cptr.reserve((size_t)nx + 1);
 	int nnz = ScanCounts(_cnt.get(), cptr.get(), nx);
 	const bool wide = ReadInt(overflow) != 0;
@@ -294,8 +336,48 @@ int Solver::Gemm(int nx, const int *xptr, const int *xcol, const double *xval, c
 	}
 	ccol.reserve((size_t)nnz); cval.reserve((size_t)nnz);
 	if(wide) YZ_LAUNCH(KGemmFill<kRowCap>, g, 128, 0, _st, nx, xptr, xcol, xval, yptr, ycol, yval, cptr.get(), ccol.get(), cval.get());
-	else YZ_LAUNCH(KGemmFill<64>, g, 128, 0, _st, nx, xptr, xcol, xval, yptr, ycol, yval, cptr.get(), ccol.get(), cval.get());
+	else YZ_LAUNCH((KGemmWarp<64, true>), gw, 256, 0, _st, nx, xptr, xcol, xval, yptr, ycol, yval, nullptr, cptr.get(),
+	               ccol.get(), cval.get(), overflow);
 	return nnz;
+}
+
+//  The dense inverse of the direct level (KGjPanel / KGjUpdate): panels of B
+//  columns, B as large as fits the panel block's shared memory (32 below
+//  ~770 rows)
+void Solver::DirectInverse(Level &L)
+{
+	const int n = L.n;
+	if(n > 3000) throw UsageError("AMG set-up: the direct level has more than 3000 rows");
+	const size_t w = 2 * (size_t)n;
+	_gj[0].reserve((size_t)n * w);
+	_gj[1].reserve((size_t)32 * n);
+	_gjPiv.reserve(32);
+	_gjRow.reserve(32);
+	double *Mc = _gj[0].get(), *F = _gj[1].get();
+	YZ_CUDA(cudaMemsetAsync(Mc, 0, (size_t)n * w * sizeof(double), _st));
+	YZ_LAUNCH(KGjInit, GridFor(n, kB), kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), Mc);
+	const size_t maxSmem = 200 * 1024;
+	int B = (int)std::min<size_t>(32, (maxSmem - 512 * 12) / ((size_t)n * sizeof(double)));
+	if(B < 1) B = 1;
+	static bool attrSet = false;
+	if(!attrSet)
+	{
+		YZ_CUDA(cudaFuncSetAttribute(KGjPanel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxSmem));
+		YZ_CUDA(cudaFuncSetAttribute(KGjUpdate, cudaFuncAttributeMaxDynamicSharedMemorySize, 3000 * 8));
+		attrSet = true;
+	}
+	for(int k0 = 0; k0 < n; k0 += B)
+	{
+		const int b = std::min(B, n - k0);
+		const size_t smem = (size_t)b * n * sizeof(double) + 512 * (sizeof(double) + sizeof(int));
+		YZ_LAUNCH(KGjPanel, 1, 512, smem, _st, n, k0, b, Mc, F, _gjRow.get(), _gjPiv.get());
+		const int jStart = k0 + b, cols = (int)w - jStart;
+		if(cols > 0)
+			YZ_LAUNCH(KGjUpdate, cols, 128, (size_t)n * sizeof(double), _st, n, k0, b, jStart, Mc, F, _gjRow.get(),
+			          _gjPiv.get());
+	}
+	L.inv.reserve((size_t)n * n);
+	YZ_LAUNCH(KGjExtract, GridFor((long long)n * n, kB), kB, 0, _st, n, Mc, L.inv.get());
 }
 
 //--------------------------------------------------------------------------
@@ -303,7 +385,9 @@ int Solver::Gemm(int nx, const int *xptr, const int *xcol, const double *xval, c
 //--------------------------------------------------------------------------
 void Solver::BuildHierarchy(int coarseEnough)
 {
-	_levels.resize(1);
+	//  the levels of the last set-up are reused with their buffers (which
+	//  only grow): no device allocation or free once the sizes have settled
+	_nlev = 1;
 	double eps = 0.08;
 	for(size_t l = 0;; ++l)
 	{
@@ -316,18 +400,7 @@ void Solver::BuildHierarchy(int coarseEnough)
 		if(n <= coarseEnough)
 		{
 			L.direct = true;
-			const size_t w = 2 * (size_t)n;
-			_gj[0].reserve((size_t)n * w); _gj[1].reserve((size_t)n * w);
-			YZ_CUDA(cudaMemsetAsync(_gj[0].get(), 0, (size_t)n * w * sizeof(double), _st));
-			YZ_CUDA(cudaMemsetAsync(_gj[1].get(), 0, (size_t)n * w * sizeof(double), _st));
-			YZ_LAUNCH(KGjInit, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), _gj[0].get());
-			for(int k = 0; k < n; ++k)
-			{
-				const long long work = (long long)n * (long long)(w - k);
-				YZ_LAUNCH(KGjStep, GridFor(work, 256, 148 * 8), 256, 0, _st, n, k, _gj[k & 1].get(), _gj[(k + 1) & 1].get());
-			}
-			L.inv.reserve((size_t)n * n);
-			YZ_LAUNCH(KGjExtract, GridFor((long long)n * n, kB), kB, 0, _st, n, _gj[n & 1].get(), L.inv.get());
+			DirectInverse(L);
 			break;
 		}
 		//  strength
@@ -384,8 +457,9 @@ void Solver::BuildHierarchy(int coarseEnough)
 		YZ_LAUNCH(KRowSort, GridFor(nc, kB), kB, 0, _st, nc, L.rptr.get(), L.rcol.get(), L.rval.get());
 		//  AP, then A_c = R (AP)
 		Gemm(n, L.ptr.get(), L.col.get(), L.val.get(), L.pptr.get(), L.pcol.get(), L.pval.get(), _apPtr, _apCol, _apVal);
-		_levels.emplace_back(new Level());
-		Level &C = *_levels.back();
+		if(_levels.size() <= l + 1) _levels.emplace_back(new Level());
+		_nlev = l + 2;
+		Level &C = *_levels[l + 1];
 		Level &F = *_levels[l];
 		C.n = nc;
 		C.nnz = Gemm(nc, F.rptr.get(), F.rcol.get(), F.rval.get(), _apPtr.get(), _apCol.get(), _apVal.get(), C.ptr, C.col,
@@ -401,30 +475,127 @@ void Solver::Cycle(size_t l, const double *f, double *x)
 	const int n = L.n, g = GridFor(n, kB);
 	if(L.direct)
 	{
-		YZ_LAUNCH(KDenseMV, GridFor((long long)n * 32, kB), kB, 0, _st, n, L.inv.get(), f, x);
+		YZ_LAUNCH(KDenseMV, GridFor((long long)n * 32, kB), kB, 0, _st, Halt(), n, L.inv.get(), f, x);
 		return;
 	}
-	if(l + 1 < _levels.size())
+	if(l + 1 < _nlev)
 	{
 		Level &C = *_levels[l + 1];
-		YZ_LAUNCH(KPreSmoothResidual, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), L.M.get(), f, x, L.t.get());
-		YZ_LAUNCH(KSpmv, GridFor(C.n, kB), kB, 0, _st, C.n, L.rptr.get(), L.rcol.get(), L.rval.get(), L.t.get(), C.f.get());
+		YZ_LAUNCH(KPreSmoothResidual, g, kB, 0, _st, Halt(), n, L.ptr.get(), L.col.get(), L.val.get(), L.M.get(), f, x,
+		          L.t.get());
+		YZ_LAUNCH(KSpmv, GridFor(C.n, kB), kB, 0, _st, Halt(), C.n, L.rptr.get(), L.rcol.get(), L.rval.get(), L.t.get(),
+		          C.f.get());
 		Cycle(l + 1, C.f.get(), C.x.get());
-		YZ_LAUNCH(KProlong, g, kB, 0, _st, n, L.pptr.get(), L.pcol.get(), L.pval.get(), C.x.get(), x, L.xt.get());
-		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), L.M.get(), f, L.xt.get(), x);
+		YZ_LAUNCH(KProlong, g, kB, 0, _st, Halt(), n, L.pptr.get(), L.pcol.get(), L.pval.get(), C.x.get(), x, L.xt.get());
+		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, Halt(), n, L.ptr.get(), L.col.get(), L.val.get(), L.M.get(), f, L.xt.get(),
+		          x);
 	}
 	else
 	{
-		YZ_LAUNCH(KPreSmooth, g, kB, 0, _st, n, L.M.get(), f, L.xt.get());
-		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), L.M.get(), f, L.xt.get(), x);
+		YZ_LAUNCH(KPreSmooth, g, kB, 0, _st, Halt(), n, L.M.get(), f, L.xt.get());
+		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, Halt(), n, L.ptr.get(), L.col.get(), L.val.get(), L.M.get(), f, L.xt.get(),
+		          x);
 	}
 }
 
 void Solver::ApplyPrec(int kind, const double *r, double *z)
 {
 	const int n = _n;
-	if(kind == kPrecDiag) YZ_LAUNCH(KDiagApply, GridFor(n, kB), kB, 0, _st, n, _m.get(), r, z);
+	if(kind == kPrecDiag) YZ_LAUNCH(KDiagApply, GridFor(n, kB), kB, 0, _st, Halt(), n, _m.get(), r, z);
 	else Cycle(0, r, z);
+}
+
+//  One BiCGStab iteration queued on the stream: every kernel reads the run's
+//  state word and does nothing once it is set (KState), so iterations may be
+//  queued ahead of the test the host would make between them.
+void Solver::EnqueueIteration(int kind)
+{
+	Level &A = *_levels[0];
+	const int n = _n, nb = RedBlocks(n), g = GridFor(n, kB);
+	const int *ptr = A.ptr.get(), *col = A.col.get();
+	const double *val = A.val.get();
+	Scal *sc = _sc.get();
+	double *x = _x.get();
+	YZ_LAUNCH(KPUpdate, g, kB, 0, _st, n, _r.get(), _v.get(), _p.get(), sc);
+	ApplyPrec(kind, _p.get(), _ph.get());
+	YZ_LAUNCH(KSpmvAlpha, nb, kRT, 0, _st, n, ptr, col, val, _ph.get(), _rh.get(), _v.get(), Red(1), sc);
+	YZ_LAUNCH(KSUpdate, nb, kRT, 0, _st, n, _r.get(), _v.get(), _s.get(), Red(2), sc);
+	YZ_LAUNCH(KXHalf, g, kB, 0, _st, n, _ph.get(), x, sc);
+	ApplyPrec(kind, _s.get(), _sh.get());
+	YZ_LAUNCH(KSpmvOmega, nb, kRT, 0, _st, n, ptr, col, val, _sh.get(), _s.get(), _t.get(), Red(3), sc);
+	YZ_LAUNCH(KXRUpdate, nb, kRT, 0, _st, n, _ph.get(), _sh.get(), _s.get(), _t.get(), _rh.get(), x, _r.get(),
+	          Red(4), sc);
+}
+
+//  The iterations of one run until its state is set: queued one at a time
+//  with one read of the state after each (the host's test between two
+//  iterations of the oracle is on the device).  With YZ_GRAPH set, one CUDA
+//  graph holds them instead: a while node whose body is one iteration and
+//  whose condition the body's last kernel sets from the state, so the run is
+//  one launch and one read.  Its capture, instantiation and destruction
+//  (0.3-0.5 ms a solve on B200, the hierarchy changing every solve) cost
+//  more than the reads it saves at the iteration counts of the implicit step,
+//  so it is not the default.  A kernel selected for per-launch timing (whose
+//  events a graph cannot carry) always takes the queued path.
+void Solver::RunIterations(int kind)
+{
+	static const bool useGraph = std::getenv("YZ_GRAPH") != nullptr;
+	Scal *sc = _sc.get();
+	if(!useGraph || TimingActive())
+	{
+		for(;;)
+		{
+			EnqueueIteration(kind);
+			YZ_LAUNCH(KLoopCount, 1, 1, 0, _st, sc);
+			ReadScal();
+			if(_hsc->state != kRun || _hsc->it >= _hsc->maxIter) break;
+		}
+		return;
+	}
+	cudaGraph_t graph = nullptr, body = nullptr;
+	cudaGraphExec_t exec = nullptr;
+	YZ_CUDA(cudaGraphCreate(&graph, 0));
+	try
+	{
+		cudaGraphConditionalHandle h;
+		YZ_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault));
+		cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+		cp.conditional.handle = h;
+		cp.conditional.type = cudaGraphCondTypeWhile;
+		cp.conditional.size = 1;
+		cudaGraphNode_t node;
+		YZ_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+		body = cp.conditional.phGraph_out[0];
+		const long long l0 = g_launches.load();
+		YZ_CUDA(cudaStreamBeginCaptureToGraph(_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+		try
+		{
+			EnqueueIteration(kind);
+			YZ_LAUNCH(KLoopCond, 1, 1, 0, _st, h, sc);
+		}
+		catch(...)
+		{
+			cudaGraph_t dummy = nullptr;
+			cudaStreamEndCapture(_st, &dummy);
+			throw;
+		}
+		YZ_CUDA(cudaStreamEndCapture(_st, &body));
+		const long long perBody = g_launches.load() - l0;
+		g_launches.fetch_sub(perBody);
+		YZ_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+		YZ_CUDA(cudaGraphLaunch(exec, _st));
+		ReadScal();
+		//  the kernels the loop ran
+		g_launches.fetch_add(perBody * (long long)_hsc->bodies);
+	}
+	catch(...)
+	{
+		if(exec) cudaGraphExecDestroy(exec);
+		cudaGraphDestroy(graph);
+		throw;
+	}
+	YZ_CUDA(cudaGraphExecDestroy(exec));
+	YZ_CUDA(cudaGraphDestroy(graph));
 }
 
 //  BiCGStab on level 0's matrix (values in _levels[0]); the oracle's
@@ -433,10 +604,9 @@ bool Solver::BiCGStab(int kind, int maxIter, double tol, int &itOut, double &err
 {
 	Level &A = *_levels[0];
 	const int n = _n, nb = RedBlocks(n), g = GridFor(n, kB);
-	const int *ptr = A.ptr.get(), *col = A.col.get();
-	const double *val = A.val.get();
 	double *b = _b.get(), *x = _x.get();
-	YZ_LAUNCH(KBInit, nb, kRT, 0, _st, n, ptr, col, val, b, x, _r.get(), _rh.get(), Red(0), _sc.get());
+	YZ_LAUNCH(KBInit, nb, kRT, 0, _st, n, A.ptr.get(), A.col.get(), A.val.get(), b, x, _r.get(), _rh.get(), Red(0),
+	          _sc.get());
 	ReadScal();
 	const double normB = _hsc->normb;
 	if(normB < 2.0 * 2.220446049250313e-16)
@@ -448,33 +618,13 @@ bool Solver::BiCGStab(int kind, int maxIter, double tol, int &itOut, double &err
 	const double eps = tol * normB;
 	double res = _hsc->res;
 	int it = 0;
-	if(res > eps)
+	if(res > eps && maxIter > 0)
 	{
-		while(it < maxIter)
-		{
-			if(_hsc->rho == 0.0) return false;
-			YZ_LAUNCH(KPUpdate, g, kB, 0, _st, n, it == 0 ? 1 : 0, _r.get(), _v.get(), _p.get(), _sc.get());
-			ApplyPrec(kind, _p.get(), _ph.get());
-			YZ_LAUNCH(KSpmvAlpha, nb, kRT, 0, _st, n, ptr, col, val, _ph.get(), _rh.get(), _v.get(), Red(1), _sc.get());
-			YZ_LAUNCH(KSUpdate, nb, kRT, 0, _st, n, _r.get(), _v.get(), _s.get(), Red(2), _sc.get());
-			ReadScal();
-			res = _hsc->res;
-			if(res <= eps)
-			{
-				YZ_LAUNCH(KXHalf, g, kB, 0, _st, n, _ph.get(), x, _sc.get());
-				++it;
-				break;
-			}
-			ApplyPrec(kind, _s.get(), _sh.get());
-			YZ_LAUNCH(KSpmvOmega, nb, kRT, 0, _st, n, ptr, col, val, _sh.get(), _s.get(), _t.get(), Red(3), _sc.get());
-			YZ_LAUNCH(KXRUpdate, nb, kRT, 0, _st, n, _ph.get(), _sh.get(), _s.get(), _t.get(), _rh.get(), x, _r.get(),
-			          Red(4), _sc.get());
-			ReadScal();
-			res = _hsc->res;
-			++it;
-			if(res <= eps) break;
-			if(!(res == res)) break;
-		}
+		YZ_LAUNCH(KCtlInit, 1, 1, 0, _st, _sc.get(), eps, maxIter);
+		RunIterations(kind);
+		if(_hsc->state == kBreak) return false;
+		it = _hsc->it;
+		res = _hsc->res;
 	}
 	itOut = it;
 	errOut = res / normB;
@@ -600,11 +750,11 @@ void Solver::SetMemory(const double *m, int len)
 	_offSpai.skip = (int)m[0]; _offSpai.wait = (int)m[1];
 }
 
-int Solver::LevelCount() const { return _haveH ? (int)_levels.size() : 0; }
+int Solver::LevelCount() const { return _haveH ? (int)_nlev : 0; }
 
 void Solver::LevelInfo(int l, int *rows, int *nnzA, int *nnzP, int *direct) const
 {
-	if(!_haveH || l < 0 || l >= (int)_levels.size()) throw UsageError("level_info: no such level");
+	if(!_haveH || l < 0 || l >= (int)_nlev) throw UsageError("level_info: no such level");
 	const Level &L = *_levels[(size_t)l];
 	if(rows) *rows = L.n;
 	if(nnzA) *nnzA = L.nnz;
@@ -614,7 +764,7 @@ void Solver::LevelInfo(int l, int *rows, int *nnzA, int *nnzP, int *direct) cons
 
 void Solver::LevelCopy(int l, int *aptr, int *acol, double *aval, int *pptr, int *pcol, double *pval, int *agg)
 {
-	if(!_haveH || l < 0 || l >= (int)_levels.size()) throw UsageError("level_copy: no such level");
+	if(!_haveH || l < 0 || l >= (int)_nlev) throw UsageError("level_copy: no such level");
 	YZ_CUDA(cudaSetDevice(_device));
 	Level &L = *_levels[(size_t)l];
 	if(aptr) L.ptr.download(aptr, (size_t)L.n + 1, _st);
@@ -653,7 +803,7 @@ void DeviceSpmv(int n, int nnz, const int *rowptr, const int *col, const double 
 	DBuf<int> p, c; DBuf<double> v, x, y;
 	p.upload(rowptr, (size_t)n + 1, 0); c.upload(col, (size_t)nnz, 0); v.upload(val, (size_t)nnz, 0);
 	x.upload(hx, (size_t)n, 0); y.reserve((size_t)n);
-	YZ_LAUNCH(KSpmv, GridFor(n, kB), kB, 0, 0, n, p.get(), c.get(), v.get(), x.get(), y.get());
+	YZ_LAUNCH(KSpmv, GridFor(n, kB), kB, 0, 0, nullptr, n, p.get(), c.get(), v.get(), x.get(), y.get());
 	YZ_CUDA(cudaMemcpy(hy, y.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
 }
 

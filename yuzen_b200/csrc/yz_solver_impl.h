@@ -14,7 +14,14 @@ namespace yz {
 struct Scal
 {
 	double normb, res, rho, rhoPrev, alpha, omega;
+	double eps;              // tol * |b|
+	int it, maxIter;         // iterations done, the cap
+	int state;               // 0 running; see KState
+	int bodies;              // iterations queued and run (the graph's loop count)
 };
+
+//  the state word of a BiCGStab run on the device
+enum KState { kRun = 0, kConv = 1, kConvHalf = 2, kBreak = 3, kNaN = 4, kCap = 5 };
 
 //  TryBackoff, LinearSolverBackend.cpp:262-270
 struct TryBackoff
@@ -64,8 +71,12 @@ public:
 private:
 	enum { kPrecDiag = 0, kPrecAmg = 1 };
 	void BuildHierarchy(int coarseEnough);
+	void DirectInverse(Level &L);
 	void Cycle(size_t l, const double *f, double *x);
+	const int *Halt() const { return &_sc.get()->state; }
 	void ApplyPrec(int kind, const double *r, double *z);
+	void EnqueueIteration(int kind);
+	void RunIterations(int kind);
 	bool BiCGStab(int kind, int maxIter, double tol, int &itOut, double &errOut);
 	double BreakdownResidual();
 	int ReadInt(const int *d);
@@ -83,7 +94,8 @@ private:
 	std::vector<int> _hptr, _hcol;
 	DBuf<int> _ssrc;
 	DBuf<double> _values, _rhs, _xio;
-	std::vector<std::unique_ptr<Level>> _levels;
+	std::vector<std::unique_ptr<Level>> _levels;   // grows, never shrinks
+	size_t _nlev = 0;                              // the levels of the present hierarchy
 	bool _haveH = false;
 	//  Krylov vectors
 	DBuf<double> _b, _x, _x0, _r, _rh, _p, _v, _s, _ph, _sh, _t, _m;
@@ -100,7 +112,9 @@ private:
 	DBuf<unsigned long long> _T0, _T1;
 	DBuf<int> _apPtr, _apCol;
 	DBuf<double> _apVal;
-	DBuf<double> _gj[2];
+	DBuf<double> _gj[2];          // [A | I] column-major, the panel multipliers
+	DBuf<double> _gjPiv;
+	DBuf<int> _gjRow;
 	TryBackoff _offSpai;
 	double _setupMs = 0, _iterMs = 0;
 	long long _launches = 0;

@@ -104,9 +104,11 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 			vis[d] = Viscosity(k, cfc);
 			sig[d] = SurfaceTension(k, cfc);
 			const double denom = hoo + Haj[d];
-			const double val = k.slip ? FaceDK(k, hoo, Haj[d]) : 2.0 * (hoo * hoo) * (Haj[d] * Haj[d]) / denom;
-			DL[d] = val * sig[d] / vis[d];
+			//  with slip the capillary face mobility is Mobility::FaceDK,
+			//  which Face also is: evaluated once
 			FM[d] = Face(k, hoo, Haj[d]);
+			const double val = k.slip ? FM[d] : 2.0 * (hoo * hoo) * (Haj[d] * Haj[d]) / denom;
+			DL[d] = val * sig[d] / vis[d];
 		}
 		double aA[13], aR[13];
 #pragma unroll
@@ -118,6 +120,7 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 #pragma unroll
 			for(int d = 0; d < 4; ++d) Tf[d] = DL[d] / hoo;
 			double topo = 0;
+#pragma unroll
 			for(int q = 0; q < 13; ++q)
 			{
 				double cc = 0;
@@ -125,6 +128,7 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 				for(int d = 0; d < 4; ++d) cc += k.cL[d][q] * Tf[d];
 				topo += cc * s[q];
 			}
+#pragma unroll
 			for(int q = 0; q < 13; ++q)
 			{
 				double val = 0;
@@ -149,6 +153,7 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 			for(int d = 0; d < 4; ++d)
 			{
 				Tsum[d] = 0;
+#pragma unroll
 				for(int q = 0; q < 13; ++q) Tsum[d] += k.cG[d][q] * s[q];
 			}
 #pragma unroll
@@ -172,15 +177,29 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 		if(k.onPG) BodyForceA<kPG>(k, h, vis, ix, iy, aR);
 		if(k.onSC) MarangoniA(k, h, c, vis, ix, iy, aR);
 		if(k.onCF) BodyForceA<kCF>(k, h, vis, ix, iy, aR);
-		//  --- DisjoiningPressureKernel::SetMatrixA (DisjoiningPressureKernel.h:306-349)
-		double piN[13];
+		//  --- DisjoiningPressureKernel::SetMatrixA (DisjoiningPressureKernel.h:306-349).
+		//  Pi, Pi/h and dPi of the five narrow points from one pair of pow
+		//  calls each: the same values the reference's three functions give
+		double piN[13], phN[13], dpN[13];
 		if(k.onD)
 		{
 #pragma unroll
 			for(int kk = 0; kk < 5; ++kk)
 			{
 				const int idx = NarrowIdx(kk);
-				const double php = PiPerH(k, h[idx]);
+				const double hj = h[idx];
+				if(hj <= 0) { piN[idx] = 0; phN[idx] = 0; dpN[idx] = 0; continue; }
+				const double r = k.hstar / hj;
+				const double rn = pow(r, k.pn), rm = pow(r, k.pm);
+				piN[idx] = rn - rm;
+				phN[idx] = piN[idx] / hj;
+				dpN[idx] = -(k.pn * rn - k.pm * rm) / hj;
+			}
+#pragma unroll
+			for(int kk = 0; kk < 5; ++kk)
+			{
+				const int idx = NarrowIdx(kk);
+				const double php = phN[idx];
 				double val = 0;
 #pragma unroll
 				for(int d = 0; d < 4; ++d) val += k.cG[d][idx] * G[d];
@@ -244,6 +263,16 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 		double J[13];
 #pragma unroll
 		for(int q = 0; q < 13; ++q) J[q] = A[q];
+		//  the face mobility's derivatives by the neighbour (A) and by this
+		//  cell (C): Mobility::Face_d1, which with slip is also the capillary
+		//  term's FaceDK_d1; evaluated once for every term
+		double fdA[4], fdC[4];
+#pragma unroll
+		for(int d = 0; d < 4; ++d)
+		{
+			fdA[d] = (k.onV || k.onD || k.slip) ? Face_d1(k, Haj[d], hoo) : 0.0;
+			fdC[d] = (k.onV || k.onD || k.slip) ? Face_d1(k, hoo, Haj[d]) : 0.0;
+		}
 		if(k.onL)
 		{
 			double a[4], b[4], gAdj[4], gCen[4], sAdj[4], sCen[4];
@@ -251,19 +280,20 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 			for(int d = 0; d < 4; ++d)
 			{
 				a[d] = 0; b[d] = 0;
+#pragma unroll
 				for(int q = 0; q < 13; ++q) { a[d] += k.cL[d][q] * h[q]; b[d] += k.cL[d][q] * s[q]; }
 				//  NonlinearJacobiProps (LaplacePressureKernel.h:160-175)
 				const double ha = Haj[d];
 				{
 					const double H1 = ha, H2 = hoo;
 					const double den = (H1 + H2) * (H1 + H2);
-					const double val = k.slip ? FaceDK_d1(k, H1, H2) : 2.0 * (H1 * H2 * H2) * (H1 + H2 + H2) / den;
+					const double val = k.slip ? fdA[d] : 2.0 * (H1 * H2 * H2) * (H1 + H2 + H2) / den;
 					gAdj[d] = val * sig[d] / vis[d];
 				}
 				{
 					const double H1 = hoo, H2 = ha;
 					const double den = (H1 + H2) * (H1 + H2);
-					const double val = k.slip ? FaceDK_d1(k, H1, H2) : 2.0 * (H1 * H2 * H2) * (H1 + H2 + H2) / den;
+					const double val = k.slip ? fdC[d] : 2.0 * (H1 * H2 * H2) * (H1 + H2 + H2) / den;
 					gCen[d] = val * sig[d] / vis[d];
 				}
 				sAdj[d] = gAdj[d] / hoo;
@@ -293,9 +323,10 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 			for(int d = 0; d < 4; ++d)
 			{
 				a[d] = 0; b[d] = 0;
+#pragma unroll
 				for(int q = 0; q < 13; ++q) { a[d] += k.cG[d][q] * h[q]; b[d] += k.cG[d][q] * s[q]; }
-				gAdj[d] = Face_d1(k, Haj[d], hoo) / vis[d];
-				gCen[d] = Face_d1(k, hoo, Haj[d]) / vis[d];
+				gAdj[d] = fdA[d] / vis[d];
+				gCen[d] = fdC[d] / vis[d];
 			}
 			double gaSum = 0;
 #pragma unroll
@@ -323,8 +354,6 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 		{
 			double Ad[4], gAdj[4], gCen[4];
 #pragma unroll
-			for(int kk = 0; kk < 5; ++kk) { const int idx = NarrowIdx(kk); piN[idx] = Pi(k, h[idx]); }
-#pragma unroll
 			for(int d = 0; d < 4; ++d)
 			{
 				//  only the two non-zero coefficients, in stencil-point order
@@ -334,8 +363,8 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 				acc += k.cG[d][lo] * piN[lo];
 				acc += k.cG[d][hi] * piN[hi];
 				Ad[d] = acc;
-				gAdj[d] = Face_d1(k, Haj[d], hoo) / vis[d];
-				gCen[d] = Face_d1(k, hoo, Haj[d]) / vis[d];
+				gAdj[d] = fdA[d] / vis[d];
+				gCen[d] = fdC[d] / vis[d];
 			}
 			double gaSum = 0, gcSum = 0;
 #pragma unroll
@@ -349,8 +378,7 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 			for(int kk = 0; kk < 5; ++kk)
 			{
 				const int idx = NarrowIdx(kk);
-				const double hj = h[idx];
-				const double dpi = dPi(k, hj) - PiPerH(k, hj);
+				const double dpi = dpN[idx] - phN[idx];
 				if(idx == oo) J[oo] += k.coefD * (gaSum + gcSum * dpi);
 				else
 				{
