@@ -26,24 +26,48 @@ __device__ __forceinline__ unsigned long long PackKey(int state, int i)
 }
 
 //--------------------------------------------------------------------------
-//  ScaleRows + gather into the sorted mirror (LinearSolverBackend.cpp:227-252)
+//  Row access of the finest level.  Its matrix is held twice: CSR for the
+//  set-up, and sliced ELLPACK (slices of 32 rows, entry k of every row of a
+//  slice side by side, SELL-32) for the kernels of the iterations, whose
+//  loads a warp then makes as whole lines.  A row's entries are taken in
+//  the same order either way (ascending column), so every sum is the same.
+//  sellOff null: CSR.
+//--------------------------------------------------------------------------
+__device__ __forceinline__ void RowRange(const int *__restrict__ ptr, const int *__restrict__ sellOff, int i, int &start,
+                                         int &len, int &stride)
+{
+	len = ptr[i + 1] - ptr[i];
+	if(sellOff) { start = sellOff[i >> 5] + (i & 31); stride = 32; }
+	else { start = ptr[i]; stride = 1; }
+}
+
+//--------------------------------------------------------------------------
+//  ScaleRows + gather into the sorted mirror (LinearSolverBackend.cpp:227-252),
+//  into both layouts of the finest level
 //--------------------------------------------------------------------------
 __global__ void KScaleGather(int n, const int *__restrict__ rowptr, const int *__restrict__ ssrc,
                              const double *__restrict__ values, const double *__restrict__ rhs, int scaling,
-                             double *__restrict__ val0, double *__restrict__ b)
+                             double *__restrict__ val0, double *__restrict__ b, const int *__restrict__ sellOff,
+                             double *__restrict__ sellVal)
 {
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		const int st = rowptr[i], ed = rowptr[i + 1];
+		const int so = sellOff[i >> 5] + (i & 31);
 		const double d = scaling ? values[st] : 1.0;
 		if(!scaling || fabs(d) < 1.0e-30)
 		{
-			for(int k = st; k < ed; ++k) val0[k] = values[ssrc[k]];
+			for(int k = st; k < ed; ++k) { const double v = values[ssrc[k]]; val0[k] = v; sellVal[so + 32 * (k - st)] = v; }
 			b[i] = rhs[i];
 			continue;
 		}
 		const double inv = 1.0 / d;
-		for(int k = st; k < ed; ++k) val0[k] = values[ssrc[k]] * inv;
+		for(int k = st; k < ed; ++k)
+		{
+			const double v = values[ssrc[k]] * inv;
+			val0[k] = v;
+			sellVal[so + 32 * (k - st)] = v;
+		}
 		b[i] = rhs[i] * inv;
 	}
 }
@@ -102,6 +126,12 @@ __global__ void KMisInit(int n, const int *__restrict__ ptr, const unsigned char
 	}
 }
 
+//  The rounds of the distance-2 independent set.  Round r reads the count of
+//  undecided rows u[r & 1] (0: the set is complete, the round does nothing),
+//  takes the largest key within distance 2 (KMisMax twice), and KMisUpdate
+//  decides the rows, writes the keys of the next round over the maxima it
+//  has read and counts the rows still undecided into u[(r + 1) & 1], which
+//  the round's first KMisMax has zeroed.
 __global__ void KMisPack(int n, const int *__restrict__ state, unsigned long long *__restrict__ T0, int *__restrict__ undecided)
 {
 	int cnt = 0;
@@ -117,8 +147,9 @@ __global__ void KMisPack(int n, const int *__restrict__ state, unsigned long lon
 __global__ void KMisMax(int n, const int *__restrict__ ptr, const int *__restrict__ col,
                         const unsigned char *__restrict__ strong, const int *__restrict__ iptr,
                         const int *__restrict__ icol, const unsigned long long *__restrict__ Tin,
-                        unsigned long long *__restrict__ Tout, const int *__restrict__ undecided)
+                        unsigned long long *__restrict__ Tout, const int *__restrict__ undecided, int *zero)
 {
+	if(zero && blockIdx.x == 0 && threadIdx.x == 0) *zero = 0;
 	if(*undecided == 0) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
@@ -129,16 +160,26 @@ __global__ void KMisMax(int n, const int *__restrict__ ptr, const int *__restric
 	}
 }
 
-__global__ void KMisUpdate(int n, int *__restrict__ state, const unsigned long long *__restrict__ T2, const int *__restrict__ undecided)
+__global__ void KMisUpdate(int n, int *__restrict__ state, unsigned long long *__restrict__ T2, const int *__restrict__ undecided,
+                           int *__restrict__ nextUndecided)
 {
 	if(*undecided == 0) return;
+	int cnt = 0;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
-		if(state[i] != kUndecided) continue;
-		const unsigned long long t = T2[i];
-		if((int)(uint32_t)(t & 0xffffffffull) == i) state[i] = kIn;
-		else if((int)(t >> 62) == kIn) state[i] = kOut;
+		int st = state[i];
+		if(st == kUndecided)
+		{
+			const unsigned long long t = T2[i];
+			if((int)(uint32_t)(t & 0xffffffffull) == i) st = kIn;
+			else if((int)(t >> 62) == kIn) st = kOut;
+			state[i] = st;
+		}
+		T2[i] = PackKey(st, i);
+		cnt += (st == kUndecided);
 	}
+	for(int off = 16; off >= 1; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+	if((threadIdx.x & 31) == 0 && cnt) atomicAdd(nextUndecided, cnt);
 }
 
 __global__ void KRootFlags(int n, const int *__restrict__ state, int *__restrict__ flag)
@@ -208,11 +249,15 @@ __global__ void KDampedJacobi(int n, const double *__restrict__ dia, double *__r
 //--------------------------------------------------------------------------
 constexpr int kRowCap = 256;	// distinct aggregates / columns a row may gather
 
+//  CAP: the distinct aggregates a row may gather in this launch (a row of A
+//  with more entries than CAP sets *overflow; the caller then launches the
+//  kRowCap instance)
+template<int CAP>
 __global__ void KPCount(int n, const int *__restrict__ ptr, const int *__restrict__ col,
                         const unsigned char *__restrict__ strong, const int *__restrict__ agg,
                         int *__restrict__ cnt, int *__restrict__ overflow)
 {
-	int lc[kRowCap];
+	int lc[CAP];
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		int m = 0;
@@ -224,20 +269,21 @@ __global__ void KPCount(int n, const int *__restrict__ ptr, const int *__restric
 			if(cp < 0) continue;
 			int q = 0;
 			while(q < m && lc[q] != cp) ++q;
-			if(q == m) { if(m == kRowCap) { atomicExch(overflow, 1); break; } lc[m++] = cp; }
+			if(q == m) { if(m == CAP) { atomicExch(overflow, 1); break; } lc[m++] = cp; }
 		}
 		cnt[i] = m;
 	}
 }
 
+template<int CAP>
 __global__ void KPFill(int n, const int *__restrict__ ptr, const int *__restrict__ col,
                        const double *__restrict__ val, const unsigned char *__restrict__ strong,
                        const int *__restrict__ agg, const int *__restrict__ pptr,
                        int *__restrict__ pcol, double *__restrict__ pval)
 {
 	const double omega = 2.0 / 3.0;
-	int lc[kRowCap];
-	double lv[kRowCap];
+	int lc[CAP];
+	double lv[CAP];
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		double dia = 0.0;
@@ -254,7 +300,7 @@ __global__ void KPFill(int n, const int *__restrict__ ptr, const int *__restrict
 			const double va = (c == i) ? (1.0 - omega) : ds * val[k];
 			int q = 0;
 			while(q < m && lc[q] != cp) ++q;
-			if(q == m) { if(m == kRowCap) break; lc[m] = cp; lv[m] = 0.0; ++m; }
+			if(q == m) { if(m == CAP) break; lc[m] = cp; lv[m] = 0.0; ++m; }
 			lv[q] = lv[q] + va;
 		}
 		//  insertion sort by column (columns are distinct)
@@ -288,11 +334,29 @@ __global__ void KTransposeFill(int n, const int *__restrict__ pptr, const int *_
 		}
 }
 
+//  each row sorted by column (the columns of a row are distinct); a row of
+//  up to 48 entries is sorted in the thread's own memory and written once
 __global__ void KRowSort(int n, const int *__restrict__ ptr, int *__restrict__ col, double *__restrict__ val)
 {
+	constexpr int L = 48;
+	int lc[L];
+	double lv[L];
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		const int st = ptr[i], ed = ptr[i + 1];
+		if(ed - st <= L)
+		{
+			const int m = ed - st;
+			for(int a = 0; a < m; ++a)
+			{
+				const int kc = col[st + a]; const double kv = val[st + a];
+				int b = a - 1;
+				while(b >= 0 && lc[b] > kc) { lc[b + 1] = lc[b]; lv[b + 1] = lv[b]; --b; }
+				lc[b + 1] = kc; lv[b + 1] = kv;
+			}
+			for(int a = 0; a < m; ++a) { col[st + a] = lc[a]; val[st + a] = lv[a]; }
+			continue;
+		}
 		for(int a = st + 1; a < ed; ++a)
 		{
 			const int kc = col[a]; const double kv = val[a];
@@ -612,7 +676,8 @@ __global__ void KGjExtract(int n, const double *__restrict__ Mc, double *__restr
 //  when it is set: the iterations are queued ahead of the host's check.
 //--------------------------------------------------------------------------
 //  x = m .* f, t = f - A x (x of the neighbours recomputed as m_j * f_j)
-__global__ void KPreSmoothResidual(const int *__restrict__ halt, int n, const int *__restrict__ ptr, const int *__restrict__ col,
+__global__ void KPreSmoothResidual(const int *__restrict__ halt, int n, const int *__restrict__ ptr,
+                                   const int *__restrict__ sellOff, const int *__restrict__ col,
                                    const double *__restrict__ val, const double *__restrict__ M,
                                    const double *__restrict__ f, double *__restrict__ x, double *__restrict__ t)
 {
@@ -620,7 +685,9 @@ __global__ void KPreSmoothResidual(const int *__restrict__ halt, int n, const in
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		double s = 0.0;
-		for(int k = ptr[i]; k < ptr[i + 1]; ++k) { const int c = col[k]; s = s + val[k] * (M[c] * f[c]); }
+		int st, len, sd;
+		RowRange(ptr, sellOff, i, st, len, sd);
+		for(int k = 0, e = st; k < len; ++k, e += sd) { const int c = col[e]; s = s + val[e] * (M[c] * f[c]); }
 		x[i] = M[i] * f[i];
 		t[i] = f[i] - s;
 	}
@@ -660,7 +727,8 @@ __global__ void KProlong(const int *__restrict__ halt, int n, const int *__restr
 }
 
 //  xout = x + m .* (f - A x)
-__global__ void KPostSmooth(const int *__restrict__ halt, int n, const int *__restrict__ ptr, const int *__restrict__ col,
+__global__ void KPostSmooth(const int *__restrict__ halt, int n, const int *__restrict__ ptr,
+                            const int *__restrict__ sellOff, const int *__restrict__ col,
                             const double *__restrict__ val, const double *__restrict__ M,
                             const double *__restrict__ f, const double *__restrict__ x, double *__restrict__ xout)
 {
@@ -668,7 +736,9 @@ __global__ void KPostSmooth(const int *__restrict__ halt, int n, const int *__re
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		double s = 0.0;
-		for(int k = ptr[i]; k < ptr[i + 1]; ++k) s = s + val[k] * x[col[k]];
+		int st, len, sd;
+		RowRange(ptr, sellOff, i, st, len, sd);
+		for(int k = 0, e = st; k < len; ++k, e += sd) s = s + val[e] * x[col[e]];
 		const double t = f[i] - s;
 		xout[i] = x[i] + M[i] * t;
 	}

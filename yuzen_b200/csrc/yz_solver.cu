@@ -26,7 +26,7 @@ namespace yz {
 	for(int kk_ = 0, i = blockIdx.x * kRChunk + threadIdx.x; kk_ < kRK; ++kk_, i += kRT)
 
 //  r = b - A x;  bb = b.b, rr = r.r, rho0 = r.r (rh = r)
-__global__ void KBInit(int n, const int *__restrict__ ptr, const int *__restrict__ col,
+__global__ void KBInit(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, const int *__restrict__ col,
                        const double *__restrict__ val, const double *__restrict__ b,
                        const double *__restrict__ x, double *__restrict__ r, double *__restrict__ rh,
                        RedScratch rs, Scal *sc)
@@ -37,7 +37,9 @@ __global__ void KBInit(int n, const int *__restrict__ ptr, const int *__restrict
 	{
 		if(i >= n) break;
 		double s = 0.0;
-		for(int k = ptr[i]; k < ptr[i + 1]; ++k) s = s + val[k] * x[col[k]];
+		int st, len, sd;
+		RowRange(ptr, sellOff, i, st, len, sd);
+		for(int k = 0, e = st; k < len; ++k, e += sd) s = s + val[e] * x[col[e]];
 		const double ri = b[i] - s;
 		r[i] = ri; rh[i] = ri;
 		a[0] = a[0] + b[i] * b[i];
@@ -74,8 +76,8 @@ __global__ void KPUpdate(int n, const double *__restrict__ r, const double *__re
 }
 
 //  v = A ph; alpha = rho / (rh . v)
-__global__ void KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__restrict__ col,
-                           const double *__restrict__ val, const double *__restrict__ ph,
+__global__ void KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff,
+                           const int *__restrict__ col, const double *__restrict__ val, const double *__restrict__ ph,
                            const double *__restrict__ rh, double *__restrict__ v, RedScratch rs, Scal *sc)
 {
 	if(sc->state != kRun) return;
@@ -85,7 +87,9 @@ __global__ void KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__rest
 	{
 		if(i >= n) break;
 		double s = 0.0;
-		for(int k = ptr[i]; k < ptr[i + 1]; ++k) s = s + val[k] * ph[col[k]];
+		int st, len, sd;
+		RowRange(ptr, sellOff, i, st, len, sd);
+		for(int k = 0, e = st; k < len; ++k, e += sd) s = s + val[e] * ph[col[e]];
 		v[i] = s;
 		a[0] = a[0] + rh[i] * s;
 	}
@@ -128,8 +132,8 @@ __global__ void KXHalf(int n, const double *__restrict__ ph, double *__restrict_
 }
 
 //  t = A sh; omega = (t . s) / (t . t)
-__global__ void KSpmvOmega(int n, const int *__restrict__ ptr, const int *__restrict__ col,
-                           const double *__restrict__ val, const double *__restrict__ sh_,
+__global__ void KSpmvOmega(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff,
+                           const int *__restrict__ col, const double *__restrict__ val, const double *__restrict__ sh_,
                            const double *__restrict__ s, double *__restrict__ t, RedScratch rs, Scal *sc)
 {
 	if(sc->state != kRun) return;
@@ -139,7 +143,9 @@ __global__ void KSpmvOmega(int n, const int *__restrict__ ptr, const int *__rest
 	{
 		if(i >= n) break;
 		double u = 0.0;
-		for(int k = ptr[i]; k < ptr[i + 1]; ++k) u = u + val[k] * sh_[col[k]];
+		int st, len, sd;
+		RowRange(ptr, sellOff, i, st, len, sd);
+		for(int k = 0, e = st; k < len; ++k, e += sd) u = u + val[e] * sh_[col[e]];
 		t[i] = u;
 		a[0] = a[0] + u * u;
 		a[1] = a[1] + u * s[i];
@@ -186,15 +192,23 @@ __global__ void KCtlInit(Scal *sc, double eps, int maxIter)
 	sc->eps = eps; sc->maxIter = maxIter; sc->it = 0; sc->state = kRun; sc->bodies = 0;
 }
 
-//  the loop's condition: another iteration while the run goes on
+//  The end of an iteration: a half-step exit, whose x update KXHalf has just
+//  made, becomes a plain exit, so that an iteration queued after it makes
+//  no second one; then the loop's condition (another iteration while the
+//  run goes on)
 __global__ void KLoopCond(cudaGraphConditionalHandle h, Scal *sc)
 {
 	sc->bodies += 1;
+	if(sc->state == kConvHalf) sc->state = kConv;
 	cudaGraphSetConditional(h, sc->state == kRun ? 1u : 0u);
 }
 
-//  the same count where the iterations are queued one by one
-__global__ void KLoopCount(Scal *sc) { sc->bodies += 1; }
+//  the same where the iterations are queued one by one
+__global__ void KLoopCount(Scal *sc)
+{
+	sc->bodies += 1;
+	if(sc->state == kConvHalf) sc->state = kConv;
+}
 
 __global__ void KFill(int n, double v, double *__restrict__ x)
 {
@@ -229,6 +243,10 @@ Solver::Solver(int device, cudaStream_t stream) : _device(device)
 	else YZ_CUDA(cudaStreamCreateWithFlags(&_st, cudaStreamNonBlocking));
 	YZ_CUDA(cudaEventCreate(&_ev0)); YZ_CUDA(cudaEventCreate(&_ev1)); YZ_CUDA(cudaEventCreate(&_ev2));
 	YZ_CUDA(cudaMallocHost(&_hsc, sizeof(Scal)));
+	YZ_CUDA(cudaMallocHost(&_hint, 4 * sizeof(int)));
+	YZ_CUDA(cudaMallocHost(&_hring, 2 * sizeof(Scal)));
+	YZ_CUDA(cudaEventCreateWithFlags(&_evRing[0], cudaEventDisableTiming));
+	YZ_CUDA(cudaEventCreateWithFlags(&_evRing[1], cudaEventDisableTiming));
 	_sc.reserve(1);
 	_counters.reserve(16);
 	YZ_CUDA(cudaMemsetAsync(_counters.get(), 0, 16 * sizeof(unsigned), _st));
@@ -240,6 +258,9 @@ Solver::~Solver()
 	cudaSetDevice(_device);
 	cudaStreamSynchronize(_st);
 	if(_hsc) cudaFreeHost(_hsc);
+	if(_hint) cudaFreeHost(_hint);
+	if(_hring) cudaFreeHost(_hring);
+	cudaEventDestroy(_evRing[0]); cudaEventDestroy(_evRing[1]);
 	cudaEventDestroy(_ev0); cudaEventDestroy(_ev1); cudaEventDestroy(_ev2);
 	if(_ownStream) cudaStreamDestroy(_st);
 }
@@ -264,6 +285,30 @@ void Solver::SetPattern(int n, int nnz, const int *rowptr, const int *scol, cons
 	for(int k = 0; k < nnz; ++k)
 		if(scol[k] < 0 || scol[k] >= n || ssrc[k] < 0 || ssrc[k] >= nnz) throw UsageError("set_pattern: index out of range");
 	_hcol.assign(scol, scol + nnz);
+	//  the SELL-32 copy of the finest level: slice offsets and columns (the
+	//  padding of a short row is never read)
+	{
+		const int S = (n + 31) / 32;
+		std::vector<int> off((size_t)S + 1, 0);
+		for(int sl = 0; sl < S; ++sl)
+		{
+			int w = 0;
+			for(int r = 32 * sl; r < std::min(n, 32 * sl + 32); ++r) w = std::max(w, _hptr[(size_t)r + 1] - _hptr[(size_t)r]);
+			off[(size_t)sl + 1] = off[(size_t)sl] + 32 * w;
+		}
+		std::vector<int> scl((size_t)off[(size_t)S], 0);
+		for(int i = 0; i < n; ++i)
+		{
+			const int base = off[(size_t)(i >> 5)] + (i & 31);
+			for(int k = _hptr[(size_t)i], e = 0; k < _hptr[(size_t)i + 1]; ++k, ++e) scl[(size_t)base + 32 * e] = scol[k];
+			for(int e = _hptr[(size_t)i + 1] - _hptr[(size_t)i]; 32 * e + base < off[(size_t)(i >> 5) + 1]; ++e)
+				scl[(size_t)base + 32 * e] = i;
+		}
+		_sellOff.upload(off.data(), off.size(), _st);
+		_sellCol.upload(scl.data(), scl.size(), _st);
+		_sellVal.reserve(scl.size());
+		YZ_CUDA(cudaMemsetAsync(_sellVal.get(), 0, scl.size() * sizeof(double), _st));
+	}
 	_levels.clear();
 	_levels.emplace_back(new Level());
 	_nlev = 1;
@@ -306,10 +351,16 @@ void Solver::ReadScal()
 }
 
 //  rows -> scanned row pointer; returns the total
-int Solver::ScanCounts(const int *cnt, int *out, int n)
+int Solver::ScanCounts(const int *cnt, int *out, int n, const int *flag, int *flagOut)
 {
 	ScanExclusive(cnt, out, n, _scan.get(), _st);
-	return ReadInt(out + n);
+	if(!flag) return ReadInt(out + n);
+	//  the total and a flag in one round trip
+	YZ_CUDA(cudaMemcpyAsync(_hint, out + n, sizeof(int), cudaMemcpyDeviceToHost, _st));
+	YZ_CUDA(cudaMemcpyAsync(_hint + 1, flag, sizeof(int), cudaMemcpyDeviceToHost, _st));
+	YZ_CUDA(cudaStreamSynchronize(_st));
+	*flagOut = _hint[1];
+	return _hint[0];
 }
 
 //  C = X Y: one warp per row with room for 64 distinct columns (KGemmWarp),
@@ -325,8 +376,9 @@ int Solver::Gemm(int nx, const int *xptr, const int *xcol, const double *xval, c
 	YZ_LAUNCH((KGemmWarp<64, false>), gw, 256, 0, _st, nx, xptr, xcol, xval, yptr, ycol, yval, _cnt.get(), nullptr,
 	          nullptr, nullptr, overflow);
 	cptr.reserve((size_t)nx + 1);
-	int nnz = ScanCounts(_cnt.get(), cptr.get(), nx);
-	const bool wide = ReadInt(overflow) != 0;
+	int ovf = 0;
+	int nnz = ScanCounts(_cnt.get(), cptr.get(), nx, overflow, &ovf);
+	const bool wide = ovf != 0;
 	if(wide)
 	{
 		YZ_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int), _st));
@@ -414,17 +466,18 @@ void Solver::BuildHierarchy(int coarseEnough)
 		YZ_LAUNCH(KFillIn, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), _strong.get(), _ifill.get(), _icol.get());
 		//  MIS-2 (at most 64 rounds, as the oracle)
 		YZ_LAUNCH(KMisInit, g, kB, 0, _st, n, L.ptr.get(), _strong.get(), _iptr.get(), _state.get(), _iso.get());
-		int *undec = _flags.get();
+		int *undec = _flags.get() + 4;		// two counters, by round parity
+		YZ_CUDA(cudaMemsetAsync(undec, 0, 2 * sizeof(int), _st));
+		YZ_LAUNCH(KMisPack, g, kB, 0, _st, n, _state.get(), _T0.get(), undec);
 		for(int round = 0; round < 64; ++round)
 		{
-			YZ_CUDA(cudaMemsetAsync(undec, 0, sizeof(int), _st));
-			YZ_LAUNCH(KMisPack, g, kB, 0, _st, n, _state.get(), _T0.get(), undec);
+			int *u = undec + (round & 1), *un = undec + ((round + 1) & 1);
 			YZ_LAUNCH(KMisMax, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), _strong.get(), _iptr.get(), _icol.get(),
-			          _T0.get(), _T1.get(), undec);
+			          _T0.get(), _T1.get(), u, un);
 			YZ_LAUNCH(KMisMax, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), _strong.get(), _iptr.get(), _icol.get(),
-			          _T1.get(), _T0.get(), undec);
-			YZ_LAUNCH(KMisUpdate, g, kB, 0, _st, n, _state.get(), _T0.get(), undec);
-			if((round & 3) == 3 && ReadInt(undec) == 0) break;
+			          _T1.get(), _T0.get(), u, nullptr);
+			YZ_LAUNCH(KMisUpdate, g, kB, 0, _st, n, _state.get(), _T0.get(), u, un);
+			if((round & 3) == 3 && ReadInt(un) == 0) break;
 		}
 		//  aggregates
 		YZ_LAUNCH(KRootFlags, g, kB, 0, _st, n, _state.get(), _flag.get());
@@ -439,13 +492,27 @@ void Solver::BuildHierarchy(int coarseEnough)
 		//  P
 		int *overflow = _flags.get() + 1;
 		YZ_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int), _st));
-		YZ_LAUNCH(KPCount, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), _strong.get(), L.agg.get(), _cnt.get(), overflow);
+		YZ_LAUNCH(KPCount<32>, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), _strong.get(), L.agg.get(), _cnt.get(),
+		          overflow);
 		L.pptr.reserve((size_t)n + 1);
-		L.pnnz = ScanCounts(_cnt.get(), L.pptr.get(), n);
-		if(ReadInt(overflow)) throw CudaError("AMG set-up: a row of P gathered more than 256 distinct aggregates");
+		int ovfP = 0;
+		L.pnnz = ScanCounts(_cnt.get(), L.pptr.get(), n, overflow, &ovfP);
+		const bool wideP = ovfP != 0;
+		if(wideP)
+		{
+			YZ_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int), _st));
+			YZ_LAUNCH(KPCount<kRowCap>, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), _strong.get(), L.agg.get(),
+			          _cnt.get(), overflow);
+			L.pnnz = ScanCounts(_cnt.get(), L.pptr.get(), n);
+			if(ReadInt(overflow)) throw CudaError("AMG set-up: a row of P gathered more than 256 distinct aggregates");
+		}
 		L.pcol.reserve((size_t)L.pnnz); L.pval.reserve((size_t)L.pnnz);
-		YZ_LAUNCH(KPFill, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), _strong.get(), L.agg.get(),
-		          L.pptr.get(), L.pcol.get(), L.pval.get());
+		if(wideP)
+			YZ_LAUNCH(KPFill<kRowCap>, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), _strong.get(), L.agg.get(),
+			          L.pptr.get(), L.pcol.get(), L.pval.get());
+		else
+			YZ_LAUNCH(KPFill<32>, g, kB, 0, _st, n, L.ptr.get(), L.col.get(), L.val.get(), _strong.get(), L.agg.get(),
+			          L.pptr.get(), L.pcol.get(), L.pval.get());
 		//  R = P^T
 		L.rptr.reserve((size_t)nc + 1); L.rcol.reserve((size_t)L.pnnz); L.rval.reserve((size_t)L.pnnz);
 		YZ_CUDA(cudaMemsetAsync(_cnt.get(), 0, ((size_t)nc + 1) * sizeof(int), _st));
@@ -481,20 +548,20 @@ void Solver::Cycle(size_t l, const double *f, double *x)
 	if(l + 1 < _nlev)
 	{
 		Level &C = *_levels[l + 1];
-		YZ_LAUNCH(KPreSmoothResidual, g, kB, 0, _st, Halt(), n, L.ptr.get(), L.col.get(), L.val.get(), L.M.get(), f, x,
-		          L.t.get());
+		YZ_LAUNCH(KPreSmoothResidual, g, kB, 0, _st, Halt(), n, L.ptr.get(), l == 0 ? _sellOff.get() : nullptr,
+		          l == 0 ? _sellCol.get() : L.col.get(), l == 0 ? _sellVal.get() : L.val.get(), L.M.get(), f, x, L.t.get());
 		YZ_LAUNCH(KSpmv, GridFor(C.n, kB), kB, 0, _st, Halt(), C.n, L.rptr.get(), L.rcol.get(), L.rval.get(), L.t.get(),
 		          C.f.get());
 		Cycle(l + 1, C.f.get(), C.x.get());
 		YZ_LAUNCH(KProlong, g, kB, 0, _st, Halt(), n, L.pptr.get(), L.pcol.get(), L.pval.get(), C.x.get(), x, L.xt.get());
-		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, Halt(), n, L.ptr.get(), L.col.get(), L.val.get(), L.M.get(), f, L.xt.get(),
-		          x);
+		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, Halt(), n, L.ptr.get(), l == 0 ? _sellOff.get() : nullptr,
+		          l == 0 ? _sellCol.get() : L.col.get(), l == 0 ? _sellVal.get() : L.val.get(), L.M.get(), f, L.xt.get(), x);
 	}
 	else
 	{
 		YZ_LAUNCH(KPreSmooth, g, kB, 0, _st, Halt(), n, L.M.get(), f, L.xt.get());
-		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, Halt(), n, L.ptr.get(), L.col.get(), L.val.get(), L.M.get(), f, L.xt.get(),
-		          x);
+		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, Halt(), n, L.ptr.get(), l == 0 ? _sellOff.get() : nullptr,
+		          l == 0 ? _sellCol.get() : L.col.get(), l == 0 ? _sellVal.get() : L.val.get(), L.M.get(), f, L.xt.get(), x);
 	}
 }
 
@@ -512,17 +579,17 @@ void Solver::EnqueueIteration(int kind)
 {
 	Level &A = *_levels[0];
 	const int n = _n, nb = RedBlocks(n), g = GridFor(n, kB);
-	const int *ptr = A.ptr.get(), *col = A.col.get();
-	const double *val = A.val.get();
+	const int *ptr = A.ptr.get(), *so = _sellOff.get(), *col = _sellCol.get();
+	const double *val = _sellVal.get();
 	Scal *sc = _sc.get();
 	double *x = _x.get();
 	YZ_LAUNCH(KPUpdate, g, kB, 0, _st, n, _r.get(), _v.get(), _p.get(), sc);
 	ApplyPrec(kind, _p.get(), _ph.get());
-	YZ_LAUNCH(KSpmvAlpha, nb, kRT, 0, _st, n, ptr, col, val, _ph.get(), _rh.get(), _v.get(), Red(1), sc);
+	YZ_LAUNCH(KSpmvAlpha, nb, kRT, 0, _st, n, ptr, so, col, val, _ph.get(), _rh.get(), _v.get(), Red(1), sc);
 	YZ_LAUNCH(KSUpdate, nb, kRT, 0, _st, n, _r.get(), _v.get(), _s.get(), Red(2), sc);
 	YZ_LAUNCH(KXHalf, g, kB, 0, _st, n, _ph.get(), x, sc);
 	ApplyPrec(kind, _s.get(), _sh.get());
-	YZ_LAUNCH(KSpmvOmega, nb, kRT, 0, _st, n, ptr, col, val, _sh.get(), _s.get(), _t.get(), Red(3), sc);
+	YZ_LAUNCH(KSpmvOmega, nb, kRT, 0, _st, n, ptr, so, col, val, _sh.get(), _s.get(), _t.get(), Red(3), sc);
 	YZ_LAUNCH(KXRUpdate, nb, kRT, 0, _st, n, _ph.get(), _sh.get(), _s.get(), _t.get(), _rh.get(), x, _r.get(),
 	          Red(4), sc);
 }
@@ -541,8 +608,10 @@ void Solver::RunIterations(int kind)
 {
 	static const bool useGraph = std::getenv("YZ_GRAPH") != nullptr;
 	Scal *sc = _sc.get();
-	if(!useGraph || TimingActive())
+	if(TimingActive())
 	{
+		//  one iteration at a time: no launch of the timed kernel is a
+		//  halted one
 		for(;;)
 		{
 			EnqueueIteration(kind);
@@ -551,6 +620,35 @@ void Solver::RunIterations(int kind)
 			if(_hsc->state != kRun || _hsc->it >= _hsc->maxIter) break;
 		}
 		return;
+	}
+	if(!useGraph)
+	{
+		//  one iteration kept in flight: the state after iteration k is
+		//  copied to pinned memory and read while iteration k+1 runs; the
+		//  iteration queued after the last one finds the state set and does
+		//  nothing
+		int slot = 0;
+		EnqueueIteration(kind);
+		YZ_LAUNCH(KLoopCount, 1, 1, 0, _st, sc);
+		YZ_CUDA(cudaMemcpyAsync(_hring + slot, sc, sizeof(Scal), cudaMemcpyDeviceToHost, _st));
+		YZ_CUDA(cudaEventRecord(_evRing[slot], _st));
+		for(;;)
+		{
+			EnqueueIteration(kind);
+			YZ_LAUNCH(KLoopCount, 1, 1, 0, _st, sc);
+			const int next = slot ^ 1;
+			YZ_CUDA(cudaMemcpyAsync(_hring + next, sc, sizeof(Scal), cudaMemcpyDeviceToHost, _st));
+			YZ_CUDA(cudaEventRecord(_evRing[next], _st));
+			YZ_CUDA(cudaEventSynchronize(_evRing[slot]));
+			const Scal &h = _hring[slot];
+			if(h.state != kRun || h.it >= h.maxIter)
+			{
+				YZ_CUDA(cudaStreamSynchronize(_st));
+				*_hsc = h;
+				return;
+			}
+			slot = next;
+		}
 	}
 	cudaGraph_t graph = nullptr, body = nullptr;
 	cudaGraphExec_t exec = nullptr;
@@ -605,8 +703,8 @@ bool Solver::BiCGStab(int kind, int maxIter, double tol, int &itOut, double &err
 	Level &A = *_levels[0];
 	const int n = _n, nb = RedBlocks(n), g = GridFor(n, kB);
 	double *b = _b.get(), *x = _x.get();
-	YZ_LAUNCH(KBInit, nb, kRT, 0, _st, n, A.ptr.get(), A.col.get(), A.val.get(), b, x, _r.get(), _rh.get(), Red(0),
-	          _sc.get());
+	YZ_LAUNCH(KBInit, nb, kRT, 0, _st, n, A.ptr.get(), _sellOff.get(), _sellCol.get(), _sellVal.get(), b, x, _r.get(),
+	          _rh.get(), Red(0), _sc.get());
 	ReadScal();
 	const double normB = _hsc->normb;
 	if(normB < 2.0 * 2.220446049250313e-16)
@@ -661,7 +759,7 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 	const int n = _n, nnz = _nnz, g = GridFor(n, kB);
 	Level &L0 = *_levels[0];
 	YZ_LAUNCH(KScaleGather, g, kB, 0, _st, n, L0.ptr.get(), _ssrc.get(), dValues, dRhs, set.scaling ? 1 : 0,
-	          L0.val.get(), _b.get());
+	          L0.val.get(), _b.get(), _sellOff.get(), _sellVal.get());
 	(void)nnz;
 	YZ_CUDA(cudaMemcpyAsync(_x.get(), dX, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
 	YZ_CUDA(cudaMemcpyAsync(_x0.get(), dX, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));

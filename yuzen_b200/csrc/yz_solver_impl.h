@@ -81,7 +81,7 @@ private:
 	double BreakdownResidual();
 	int ReadInt(const int *d);
 	void ReadScal();
-	int ScanCounts(const int *cnt, int *out, int n);
+	int ScanCounts(const int *cnt, int *out, int n, const int *flag = nullptr, int *flagOut = nullptr);
 	int Gemm(int nx, const int *xptr, const int *xcol, const double *xval, const int *yptr, const int *ycol,
 	         const double *yval, DBuf<int> &cptr, DBuf<int> &ccol, DBuf<double> &cval);
 	RedScratch Red(int site);
@@ -93,6 +93,8 @@ private:
 	int _n = 0, _nnz = 0;
 	std::vector<int> _hptr, _hcol;
 	DBuf<int> _ssrc;
+	DBuf<int> _sellOff, _sellCol;     // the finest level in SELL-32 (slice offsets, columns)
+	DBuf<double> _sellVal;
 	DBuf<double> _values, _rhs, _xio;
 	std::vector<std::unique_ptr<Level>> _levels;   // grows, never shrinks
 	size_t _nlev = 0;                              // the levels of the present hierarchy
@@ -104,6 +106,9 @@ private:
 	DBuf<unsigned> _counters;
 	DBuf<Scal> _sc;
 	Scal *_hsc = nullptr;
+	int *_hint = nullptr;      // pinned: totals and flags read back together
+	Scal *_hring = nullptr;    // pinned: the state after the last two iterations
+	cudaEvent_t _evRing[2] = {nullptr, nullptr};
 	DBuf<int> _flags;
 	//  set-up scratch
 	DBuf<double> _dia;
