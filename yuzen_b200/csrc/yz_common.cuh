@@ -67,11 +67,16 @@ struct DBuf
 	DBuf &operator=(const DBuf &) = delete;
 	~DBuf() { if(p) cudaFree(p); }
 	T *get() const { return p; }
+	//  a buffer that must grow takes half as much again, so that sizes that
+	//  creep up from solve to solve (the coarse levels of the hierarchy) do
+	//  not free and allocate (each a device-wide synchronisation) every time
 	void reserve(size_t n)
 	{
 		if(n <= cap) return;
+		const size_t grown = cap ? cap + cap / 2 : 0;
 		if(p) { cudaFree(p); p = nullptr; cap = 0; }
 		size_t want = n < 16 ? 16 : n;
+		if(grown > want) want = grown;
 		YZ_CUDA(cudaMalloc(&p, want * sizeof(T)));
 		cap = want;
 	}

@@ -59,7 +59,8 @@ __device__ __forceinline__ double KFace(const ConcCoef &q, double ha, double hb,
 //  whether the film has a cell without liquid (FilmNotPositive).
 //--------------------------------------------------------------------------
 __device__ __forceinline__ double FaceFluxSum(const Coef &k, const double *h, const double *c, const double *s,
-                                              const double *vis, const double *DL, int d, int ix, int iy)
+                                              const double *vis, const double *DL, const double *FM, const double *pi,
+                                              int d, int ix, int iy)
 {
 	double sum = 0;
 	const int a = AdjIdx(d);
@@ -70,7 +71,7 @@ __device__ __forceinline__ double FaceFluxSum(const Coef &k, const double *h, co
 		const double sl = (d % 2 == 0) ? s[a] : s[oo], sh = (d % 2 == 0) ? s[oo] : s[a];
 		const double dn = (d < 2) ? k.dxx : k.dyy;
 		const double mu = vis[d];
-		double gf = Face(k, hl, hh);
+		double gf = FM[d];
 		const double tk = (gf == 0) ? 0.0 : gf / (hl + hh) / mu;
 		gf /= mu;
 		sum += k.coefV * ((gf * (hh - hl) + (sh - sl) * (tk * (hl + hh))) / (dn * dn));
@@ -80,8 +81,8 @@ __device__ __forceinline__ double FaceFluxSum(const Coef &k, const double *h, co
 	if(k.onCF) sum += BodyForceFlux<kCF>(k, h, vis[d], d, ix, iy);
 	if(k.onD)
 	{
-		const double G = Face(k, h[oo], h[a]) / vis[d];
-		const double v = k.cG[d][a] * Pi(k, h[a]) + k.cG[d][oo] * Pi(k, h[oo]);
+		const double G = FM[d] / vis[d];
+		const double v = k.cG[d][a] * pi[a] + k.cG[d][oo] * pi[oo];
 		const double f = k.coefD * (G * v);
 		sum += (d % 2 == 0) ? -f : f;
 	}
@@ -90,7 +91,8 @@ __device__ __forceinline__ double FaceFluxSum(const Coef &k, const double *h, co
 
 __global__ void KFaceFlux(Coef k, const double *__restrict__ H, const double *__restrict__ C,
                           const double *__restrict__ S, double *__restrict__ Fx, double *__restrict__ Fy,
-                          const double *__restrict__ evapOld, double dt, double *__restrict__ evp, int *filmBad)
+                          const double *__restrict__ evapOld, double dt, double *__restrict__ evp, int *filmBad,
+                          FaceBuf fb)
 {
 	const int nx = k.nx, ny = k.ny;
 	const int nIn = (nx - 4) * (ny - 4);
@@ -106,20 +108,23 @@ __global__ void KFaceFlux(Coef k, const double *__restrict__ H, const double *__
 			const int j = i + OffsetOf(q, nx);
 			h[q] = H[j]; c[q] = C[j]; s[q] = S[j];
 		}
-		double vis[4], DL[4];
+		double vis[4], DL[4], FM[4], pi[13];
 #pragma unroll
 		for(int d = 0; d < 4; ++d)
 		{
-			const int a = AdjIdx(d);
-			const double cfc = 0.5 * (c[oo] + c[a]);
-			vis[d] = Viscosity(k, cfc);
-			const double val = k.slip ? FaceDK(k, h[oo], h[a]) : 2.0 * (h[oo] * h[oo]) * (h[a] * h[a]) / (h[oo] + h[a]);
-			DL[d] = val * SurfaceTension(k, cfc) / vis[d];
+			const FaceSet f = (d < 2) ? fb.x : fb.y;
+			const int fi = (d == 0) ? i - 1 : (d == 2) ? i - nx : i;
+			vis[d] = f.vis[fi]; DL[d] = f.DL[fi]; FM[d] = f.FM[fi];
 		}
-		Fx[i] = FaceFluxSum(k, h, c, s, vis, DL, 1, ix, iy);
-		Fy[i] = FaceFluxSum(k, h, c, s, vis, DL, 3, ix, iy);
-		if(ix == 2) Fx[i - 1] = FaceFluxSum(k, h, c, s, vis, DL, 0, ix, iy);
-		if(iy == 2) Fy[i - nx] = FaceFluxSum(k, h, c, s, vis, DL, 2, ix, iy);
+		if(k.onD)
+		{
+#pragma unroll
+			for(int kk = 0; kk < 5; ++kk) { const int idx = NarrowIdx(kk); pi[idx] = fb.piN[i + OffsetOf(idx, nx)]; }
+		}
+		Fx[i] = FaceFluxSum(k, h, c, s, vis, DL, FM, pi, 1, ix, iy);
+		Fy[i] = FaceFluxSum(k, h, c, s, vis, DL, FM, pi, 3, ix, iy);
+		if(ix == 2) Fx[i - 1] = FaceFluxSum(k, h, c, s, vis, DL, FM, pi, 0, ix, iy);
+		if(iy == 2) Fy[i - nx] = FaceFluxSum(k, h, c, s, vis, DL, FM, pi, 2, ix, iy);
 		if(evp)
 		{
 			const double xx = k.xmin + ix * k.dx + k.dx2h, yy = k.ymin + iy * k.dy + k.dy2h;

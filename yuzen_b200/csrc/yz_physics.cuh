@@ -98,6 +98,24 @@ struct Coef
 	double scMag;               // As*Ma/2
 };
 
+//  The face properties of a film (H, C), once per face: face f of axis a is
+//  held at the index of its low cell.  vis, sig: the viscosity and surface
+//  tension at the face's mean concentration; FM: Mobility::Face; DL: the
+//  capillary face mobility times sig / vis; fdLH, fdHL: Face_d1 by the low /
+//  the high cell; gLH, gHL: the capillary term's NonlinearJacobiProps by the
+//  low / the high cell.  Every value is the one each of the two rows of the
+//  face would compute (the expressions are symmetric in the two cells to
+//  the bit).  piN, phN, dpN: Pi, Pi / h and dPi of every cell.
+struct FaceSet
+{
+	double *vis, *sig, *FM, *DL, *fdLH, *fdHL, *gLH, *gHL;
+};
+struct FaceBuf
+{
+	FaceSet x, y;
+	double *piN, *phN, *dpN;
+};
+
 //  what the concentration equation's kernels need (ConcEquationBase.h)
 struct ConcCoef
 {

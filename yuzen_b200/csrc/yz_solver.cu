@@ -36,10 +36,9 @@ __global__ void KBInit(int n, const int *__restrict__ ptr, const int *__restrict
 	YZ_CHUNK_LOOP(i)
 	{
 		if(i >= n) break;
-		double s = 0.0;
 		int st, len, sd;
 		RowRange(ptr, sellOff, i, st, len, sd);
-		for(int k = 0, e = st; k < len; ++k, e += sd) s = s + val[e] * x[col[e]];
+		const double s = RowSum(st, len, sd, col, val, [&](int c) { return x[c]; });
 		const double ri = b[i] - s;
 		r[i] = ri; rh[i] = ri;
 		a[0] = a[0] + b[i] * b[i];
@@ -86,10 +85,9 @@ __global__ void KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__rest
 	YZ_CHUNK_LOOP(i)
 	{
 		if(i >= n) break;
-		double s = 0.0;
 		int st, len, sd;
 		RowRange(ptr, sellOff, i, st, len, sd);
-		for(int k = 0, e = st; k < len; ++k, e += sd) s = s + val[e] * ph[col[e]];
+		const double s = RowSum(st, len, sd, col, val, [&](int c) { return ph[c]; });
 		v[i] = s;
 		a[0] = a[0] + rh[i] * s;
 	}
@@ -142,10 +140,9 @@ __global__ void KSpmvOmega(int n, const int *__restrict__ ptr, const int *__rest
 	YZ_CHUNK_LOOP(i)
 	{
 		if(i >= n) break;
-		double u = 0.0;
 		int st, len, sd;
 		RowRange(ptr, sellOff, i, st, len, sd);
-		for(int k = 0, e = st; k < len; ++k, e += sd) u = u + val[e] * sh_[col[e]];
+		const double u = RowSum(st, len, sd, col, val, [&](int c) { return sh_[c]; });
 		t[i] = u;
 		a[0] = a[0] + u * u;
 		a[1] = a[1] + u * s[i];

@@ -59,6 +59,85 @@ __device__ __forceinline__ void WarpMaxAbs(unsigned long long *slot, double v)
 }
 
 //--------------------------------------------------------------------------
+//  Face properties (FaceBuf): one thread per face; with J, also the
+//  derivatives the Jacobian takes.  Faces of axis x: low cells ix 1..nx-3,
+//  iy 2..ny-3; of axis y: ix 2..nx-3, iy 1..ny-3.
+//--------------------------------------------------------------------------
+template<bool J>
+__global__ void KFaceProps(Coef k, const double *__restrict__ H, const double *__restrict__ C, FaceBuf fb)
+{
+	const int nx = k.nx, ny = k.ny;
+	const int nxF = (nx - 3) * (ny - 4), nyF = (nx - 4) * (ny - 3);
+	for(int t = blockIdx.x * blockDim.x + threadIdx.x; t < nxF + nyF; t += gridDim.x * blockDim.x)
+	{
+		int lo, hi;
+		FaceSet f;
+		if(t < nxF)
+		{
+			const int ix = 1 + t % (nx - 3), iy = 2 + t / (nx - 3);
+			lo = iy * nx + ix; hi = lo + 1; f = fb.x;
+		}
+		else
+		{
+			const int u = t - nxF;
+			const int ix = 2 + u % (nx - 4), iy = 1 + u / (nx - 4);
+			lo = iy * nx + ix; hi = lo + nx; f = fb.y;
+		}
+		const double hl = H[lo], hh = H[hi];
+		const double cfc = 0.5 * (C[lo] + C[hi]);
+		const double vis = Viscosity(k, cfc), sig = SurfaceTension(k, cfc);
+		const double FM = Face(k, hl, hh);
+		const double val = k.slip ? FM : 2.0 * (hl * hl) * (hh * hh) / (hl + hh);
+		f.vis[lo] = vis; f.sig[lo] = sig; f.FM[lo] = FM;
+		f.DL[lo] = val * sig / vis;
+		if(!J) continue;
+		const double dLH = (k.onV || k.onD || k.slip) ? Face_d1(k, hl, hh) : 0.0;
+		const double dHL = (k.onV || k.onD || k.slip) ? Face_d1(k, hh, hl) : 0.0;
+		f.fdLH[lo] = dLH; f.fdHL[lo] = dHL;
+		if(k.onL)
+		{
+			//  NonlinearJacobiProps (LaplacePressureKernel.h:160-175)
+			const double den = (hl + hh) * (hl + hh);
+			const double vLH = k.slip ? dLH : 2.0 * (hl * hh * hh) * (hl + hh + hh) / den;
+			const double den2 = (hh + hl) * (hh + hl);
+			const double vHL = k.slip ? dHL : 2.0 * (hh * hl * hl) * (hh + hl + hl) / den2;
+			f.gLH[lo] = vLH * sig / vis;
+			f.gHL[lo] = vHL * sig / vis;
+		}
+	}
+}
+
+//  Pi, Pi / h and dPi of every cell (DisjoiningPressureKernel.h:191-218),
+//  from one pair of pow calls
+__global__ void KCellPi(Coef k, int n, const double *__restrict__ H, FaceBuf fb)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		const double hj = H[i];
+		if(hj <= 0) { fb.piN[i] = 0; fb.phN[i] = 0; fb.dpN[i] = 0; continue; }
+		const double r = k.hstar / hj;
+		const double rn = pow(r, k.pn), rm = pow(r, k.pm);
+		const double p = rn - rm;
+		fb.piN[i] = p;
+		fb.phN[i] = p / hj;
+		fb.dpN[i] = -(k.pn * rn - k.pm * rm) / hj;
+	}
+}
+
+//  face d of the interior row i: its index in the face arrays and whether
+//  the row is the face's low cell
+__device__ __forceinline__ void FaceOf(int d, int i, int nx, const FaceBuf &fb, FaceSet &f, int &idx, bool &low)
+{
+	switch(d)
+	{
+	case 0:  f = fb.x; idx = i - 1; low = false; break;
+	case 1:  f = fb.x; idx = i; low = true; break;
+	case 2:  f = fb.y; idx = i - nx; low = false; break;
+	default: f = fb.y; idx = i; low = true; break;
+	}
+}
+
+//--------------------------------------------------------------------------
 //  One interior row: the A entries of every term, then what the caller
 //  asks for: mode 0 -> A(h) h only (the explicit half and evapOld);
 //  mode 1 -> I + theta dt J, A(h) h, B and the right-hand side.
@@ -76,7 +155,7 @@ struct RowOut
 
 __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ rowptr,
                           const double *__restrict__ H, const double *__restrict__ C,
-                          const double *__restrict__ S, RowOut o)
+                          const double *__restrict__ S, RowOut o, FaceBuf fb)
 {
 	const int nx = k.nx, ny = k.ny;
 	const int nIn = (nx - 4) * (ny - 4);
@@ -94,21 +173,20 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 		}
 		const double hoo = h[oo], coo = c[oo];
 		//  face properties
+		(void)coo;
 		double vis[4], sig[4], DL[4], FM[4], Haj[4];
+		int fIdx[4];
+		bool fLow[4];
+		FaceSet fs[4];
 #pragma unroll
 		for(int d = 0; d < 4; ++d)
 		{
-			const int a = AdjIdx(d);
-			Haj[d] = h[a];
-			const double cfc = 0.5 * (coo + c[a]);
-			vis[d] = Viscosity(k, cfc);
-			sig[d] = SurfaceTension(k, cfc);
-			const double denom = hoo + Haj[d];
-			//  with slip the capillary face mobility is Mobility::FaceDK,
-			//  which Face also is: evaluated once
-			FM[d] = Face(k, hoo, Haj[d]);
-			const double val = k.slip ? FM[d] : 2.0 * (hoo * hoo) * (Haj[d] * Haj[d]) / denom;
-			DL[d] = val * sig[d] / vis[d];
+			Haj[d] = h[AdjIdx(d)];
+			FaceOf(d, i, nx, fb, fs[d], fIdx[d], fLow[d]);
+			vis[d] = fs[d].vis[fIdx[d]];
+			sig[d] = fs[d].sig[fIdx[d]];
+			FM[d] = fs[d].FM[fIdx[d]];
+			DL[d] = fs[d].DL[fIdx[d]];
 		}
 		double aA[13], aR[13];
 #pragma unroll
@@ -187,13 +265,8 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 			for(int kk = 0; kk < 5; ++kk)
 			{
 				const int idx = NarrowIdx(kk);
-				const double hj = h[idx];
-				if(hj <= 0) { piN[idx] = 0; phN[idx] = 0; dpN[idx] = 0; continue; }
-				const double r = k.hstar / hj;
-				const double rn = pow(r, k.pn), rm = pow(r, k.pm);
-				piN[idx] = rn - rm;
-				phN[idx] = piN[idx] / hj;
-				dpN[idx] = -(k.pn * rn - k.pm * rm) / hj;
+				const int j = i + Offset(idx, nx);
+				piN[idx] = fb.piN[j]; phN[idx] = fb.phN[j]; dpN[idx] = fb.dpN[j];
 			}
 #pragma unroll
 			for(int kk = 0; kk < 5; ++kk)
@@ -270,8 +343,9 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 #pragma unroll
 		for(int d = 0; d < 4; ++d)
 		{
-			fdA[d] = (k.onV || k.onD || k.slip) ? Face_d1(k, Haj[d], hoo) : 0.0;
-			fdC[d] = (k.onV || k.onD || k.slip) ? Face_d1(k, hoo, Haj[d]) : 0.0;
+			const double LH = fs[d].fdLH[fIdx[d]], HL = fs[d].fdHL[fIdx[d]];
+			fdA[d] = fLow[d] ? HL : LH;
+			fdC[d] = fLow[d] ? LH : HL;
 		}
 		if(k.onL)
 		{
@@ -282,19 +356,12 @@ __global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ r
 				a[d] = 0; b[d] = 0;
 #pragma unroll
 				for(int q = 0; q < 13; ++q) { a[d] += k.cL[d][q] * h[q]; b[d] += k.cL[d][q] * s[q]; }
-				//  NonlinearJacobiProps (LaplacePressureKernel.h:160-175)
-				const double ha = Haj[d];
+				//  NonlinearJacobiProps (LaplacePressureKernel.h:160-175), by
+				//  the neighbour and by this cell
 				{
-					const double H1 = ha, H2 = hoo;
-					const double den = (H1 + H2) * (H1 + H2);
-					const double val = k.slip ? fdA[d] : 2.0 * (H1 * H2 * H2) * (H1 + H2 + H2) / den;
-					gAdj[d] = val * sig[d] / vis[d];
-				}
-				{
-					const double H1 = hoo, H2 = ha;
-					const double den = (H1 + H2) * (H1 + H2);
-					const double val = k.slip ? fdC[d] : 2.0 * (H1 * H2 * H2) * (H1 + H2 + H2) / den;
-					gCen[d] = val * sig[d] / vis[d];
+					const double LH = fs[d].gLH[fIdx[d]], HL = fs[d].gHL[fIdx[d]];
+					gAdj[d] = fLow[d] ? HL : LH;
+					gCen[d] = fLow[d] ? LH : HL;
 				}
 				sAdj[d] = gAdj[d] / hoo;
 				sCen[d] = gCen[d] / hoo - DL[d] / (hoo * hoo);
@@ -528,6 +595,16 @@ Step::Step(int device, const yz_step_params &p, const double *h, const double *c
 	YZ_CUDA(cudaMemcpyAsync(_hOld2.get(), h, n * sizeof(double), cudaMemcpyHostToDevice, _st));
 	YZ_CUDA(cudaMemcpyAsync(_hNew.get(), h, n * sizeof(double), cudaMemcpyHostToDevice, _st));
 	_red.reserve(8);
+	//  the face properties (16 arrays of n, indexed by a face's low cell) and Pi
+	_faceMem.reserve(19 * n);
+	YZ_CUDA(cudaMemsetAsync(_faceMem.get(), 0, 19 * n * sizeof(double), _st));
+	{
+		double *m = _faceMem.get();
+		double **slots[19] = {&_fb.x.vis, &_fb.x.sig, &_fb.x.FM, &_fb.x.DL, &_fb.x.fdLH, &_fb.x.fdHL, &_fb.x.gLH,
+		                      &_fb.x.gHL, &_fb.y.vis, &_fb.y.sig, &_fb.y.FM, &_fb.y.DL, &_fb.y.fdLH, &_fb.y.fdHL,
+		                      &_fb.y.gLH, &_fb.y.gHL, &_fb.piN, &_fb.phN, &_fb.dpN};
+		for(int q = 0; q < 19; ++q) *slots[q] = m + (size_t)q * n;
+	}
 	_dt = p.dt; _dtOld = p.dt; _time = p.t_start;
 	YZ_LAUNCH(KSetGhostRows, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
 	          _dRowptr.get(), _ia.get(), _rhs.get());
@@ -706,15 +783,26 @@ double Step::ReadMax(int slot)
 
 void Step::ZeroMax(int slot) { YZ_CUDA(cudaMemsetAsync(_red.get() + slot, 0, sizeof(unsigned long long), _st)); }
 
+//  the face properties of the film (H, C) into _fb (with the Jacobian's
+//  derivatives when J), and Pi of every cell
+void Step::FaceProps(const double *H, const double *C, bool J)
+{
+	const int nF = (_p.nx - 3) * (_p.ny - 4) + (_p.nx - 4) * (_p.ny - 3);
+	if(J) YZ_LAUNCH(KFaceProps<true>, GridFor(nF, 128, 148 * 32), 128, 0, _st, _k, H, C, _fb);
+	else YZ_LAUNCH(KFaceProps<false>, GridFor(nF, 128, 148 * 32), 128, 0, _st, _k, H, C, _fb);
+	if(_k.onD) YZ_LAUNCH(KCellPi, GridFor(_n, 256), 256, 0, _st, _k, _n, H, _fb);
+}
+
 void Step::Assemble(int mode, const double *hField, const double *cField, double dt)
 {
+	FaceProps(hField, cField, mode == 1);
 	RowOut o;
 	o.ia = _ia.get(); o.ax = mode == 0 ? _axOld.get() : _axGuess.get();
 	o.evapOld = _evapOld.get(); o.evapB = _evapB.get(); o.rhs = _rhs.get();
 	o.hOld = _hOld.get(); o.axOld = _axOld.get(); o.rhsMax = _red.get() + kSlotRhs;
 	const int nIn = (_p.nx - 4) * (_p.ny - 4);
 	YZ_LAUNCH(KAssemble, GridFor(nIn, 128, 148 * 32), 128, 0, _st, _k, mode, dt, _dRowptr.get(), hField, cField,
-	          _s.get(), o);
+	          _s.get(), o, _fb);
 }
 
 //  one Newton-Kantorovich attempt at the present dt (NKLoop)
@@ -1092,8 +1180,9 @@ int Step::FaceFluxes(const double *H, const double *C, double *Fx, double *Fy, d
 	const int nIn = (_p.nx - 4) * (_p.ny - 4);
 	int *bad = _iflags.get();
 	YZ_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), _st));
+	FaceProps(H, C, false);
 	YZ_LAUNCH(KFaceFlux, GridFor(nIn, 128, 148 * 32), 128, 0, _st, _k, H, C, _s.get(), Fx, Fy, _evapOld.get(), dt,
-	          withEvap ? _evpStep.get() : nullptr, bad);
+	          withEvap ? _evpStep.get() : nullptr, bad, _fb);
 	int h = 0;
 	YZ_CUDA(cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, _st));
 	YZ_CUDA(cudaStreamSynchronize(_st));

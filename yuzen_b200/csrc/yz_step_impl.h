@@ -34,6 +34,7 @@ private:
 	       kSlotFlags = 7 };
 	void BuildPattern();
 	void BuildCoef();
+	void FaceProps(const double *H, const double *C, bool J);
 	void Assemble(int mode, const double *hField, const double *cField, double dt);
 	bool NKLoop(int &iter, double &resid, yz_step_stats &stats);
 	//  the concentration equation
@@ -63,6 +64,8 @@ private:
 	//  phi_guess; A h at phi_old and at the guess; the system
 	DBuf<double> _h, _c, _s, _hOld, _hOld2, _hNew, _guess, _axOld, _axGuess, _rhs, _delta, _evapOld, _evapB, _ia;
 	DBuf<unsigned long long> _red;
+	DBuf<double> _faceMem;
+	phys::FaceBuf _fb;
 	//  the concentration equation: its pattern and solver; c0 (its phi_old),
 	//  the working field's c, the limiter state, the c of the last pass,
 	//  the solution c1 and the one before the solves that complete the step,
