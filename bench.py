@@ -190,6 +190,7 @@ def run_device_arm(a) -> None:
         dist.barrier()
     torch.cuda.synchronize()
     total_ms, newton, linear, launches, conc_solves, conc_iters = 0.0, 0, 0, 0, 0, 0
+    per_step, per_setup = [], []
     parts = {"setup_ms": 0.0, "solve_ms": 0.0, "assemble_ms": 0.0}
     with Clocks(local) as clk:
         for _ in range(a.steps):
@@ -197,6 +198,8 @@ def run_device_arm(a) -> None:
             torch.cuda.synchronize()
             r = st.advance(1)
             total_ms += r["device_ms"]
+            per_step.append(round(r["device_ms"], 2))
+            per_setup.append(round(r["setup_ms"], 2))
             newton += r["newton_iterations"]
             linear += r["linear_iterations"]
             launches += r["launches"]
@@ -270,6 +273,7 @@ def run_device_arm(a) -> None:
                    "conc_solves": conc_solves, "conc_iterations": conc_iters,
                    "newton_iterations": newton, "linear_iterations": linear,
                    "device_ms": {k: round(v, 3) for k, v in parts.items()},
+                   "step_ms": per_step, "setup_ms_per_step": per_setup,
                    "finite": finite},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 2 * 8 * n,
                 "steps": e2e_steps},
