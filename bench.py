@@ -41,8 +41,9 @@ sys.path.insert(0, str(REPO))
 METRIC = "steps/s at 512² all-physics: learned-precond FP32 vs plain FP64 GPU, equal h-error"
 UNIT = "steps/s"
 
-#  The kernel whose roofline is reported (the largest share of device time in
-#  profiles/launches_spinodal_224.md) and its algorithmic bytes per launch:
+#  The kernel whose roofline is reported (the finest level's SpMV of the
+#  BiCGStab iteration, profiles/KSpmvAlpha_allphys_512.md) and its algorithmic
+#  bytes per launch:
 #  v = A p with alpha = rho / (rh . v): matrix values and columns (12 B per
 #  entry), row pointers (4 B per row), p read once, rh read, v written
 #  (8 B each per row).
@@ -51,6 +52,17 @@ ROOFLINE_KERNEL = "KSpmvAlpha"
 
 def spmv_alpha_bytes(n: int, nnz: int) -> int:
     return 12 * nnz + 4 * (n + 1) + 3 * 8 * n
+
+
+def profiled_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of the kernel (dram__bytes_read.sum +
+    dram__bytes_write.sum) from the committed ncu summary of that kernel on
+    that workload, profiles/<kernel>_<workload>.md, or None."""
+    p = REPO / "profiles" / f"{kernel}_{workload}.md"
+    if not p.exists():
+        return None
+    m = re.search(r"dram bytes per launch:\s*([0-9]+)", p.read_text())
+    return int(m.group(1)) if m else None
 
 
 def measured_peaks() -> dict:
@@ -250,7 +262,7 @@ def run_device_arm(a) -> None:
         achieved = bytes_ / (kern_ms / kern_n / 1e3) / 1e9
         roof = {"kernel": ROOFLINE_KERNEL, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
                 "peak_source": peaks["source"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                "traffic": None, "bytes_per_launch": bytes_, "launches": kern_n,
+                "traffic": profiled_traffic(ROOFLINE_KERNEL, a.config), "bytes_per_launch": bytes_, "launches": kern_n,
                 "avg_launch_us": kern_ms / kern_n * 1e3}
     cpu = None
     if world == 1 and not a.no_cpu_baseline:

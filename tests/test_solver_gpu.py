@@ -153,3 +153,36 @@ def test_kernels_actually_launch():
     d = _systems.film_system(64, seed=1)
     g = gpu_solve(d)
     assert g[4].launches() > 50
+
+
+_GRAPH_CHILD = r"""
+import sys
+sys.path[:0] = [sys.argv[1], sys.argv[1] + '/tests', sys.argv[1] + '/tests/golden']
+import numpy as np
+import _oracle, _systems
+import yuzen_b200 as yz
+d = _systems.film_system(200, seed=7, periodic=True)
+s = yz.LinearSolverSettings(int(d['precondition']), bool(d['scaling']), int(d['max_iteration']),
+                            float(d['epsilon']), bool(d['conc']))
+be = yz.B200Backend()
+pat = yz.CrsPattern(d['rowptr'], d['col'], d['sorted_col'], d['sorted_src'])
+x = np.array(d['x0'], copy=True)
+ret, it, res = be.Solve(s, pat, d['values'], d['rhs'], x)
+o = _oracle.OracleSolver().solve(d)
+assert (ret, it, res) == tuple(o[:3]), ((ret, it, res), o[:3])
+assert np.array_equal(x, o[3])
+print('ok', it)
+"""
+
+
+def test_graph_loop_bitwise():
+    """The CUDA-graph form of the iterations (YZ_GRAPH=1: a conditional while
+    node whose body is one BiCGStab iteration) gives the oracle's answer to
+    the bit, as the default queued form does."""
+    import os
+    import subprocess
+    import sys
+    repo = str(Path(__file__).resolve().parents[1])
+    r = subprocess.run([sys.executable, "-c", _GRAPH_CHILD, repo], env=dict(os.environ, YZ_GRAPH="1"),
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout[-2000:] + r.stderr[-2000:]

@@ -358,35 +358,42 @@ __global__ void KTransposeFill(int n, const int *__restrict__ pptr, const int *_
 		}
 }
 
-//  each row sorted by column (the columns of a row are distinct); a row of
-//  up to 48 entries is sorted in the thread's own memory and written once
-__global__ void KRowSort(int n, const int *__restrict__ ptr, int *__restrict__ col, double *__restrict__ val)
+//  each row sorted by column (the columns of a row are distinct): one warp
+//  per row, every entry placed at its rank among the row's columns (rows of
+//  up to 64 entries), longer rows by insertion in place
+__global__ void __launch_bounds__(256) KRowSort(int n, const int *__restrict__ ptr, int *__restrict__ col,
+                                                double *__restrict__ val)
 {
-	constexpr int L = 48;
-	int lc[L];
-	double lv[L];
-	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	constexpr int L = 64, W = 8;
+	__shared__ int sc[W][L];
+	__shared__ double sv[W][L];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+	for(long long row = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += warps)
 	{
-		const int st = ptr[i], ed = ptr[i + 1];
-		if(ed - st <= L)
+		const int i = (int)row;
+		const int st = ptr[i], ed = ptr[i + 1], m = ed - st;
+		if(m <= L)
 		{
-			const int m = ed - st;
-			for(int a = 0; a < m; ++a)
+			for(int a2 = lane; a2 < m; a2 += 32) { sc[w][a2] = col[st + a2]; sv[w][a2] = val[st + a2]; }
+			__syncwarp();
+			for(int a2 = lane; a2 < m; a2 += 32)
 			{
-				const int kc = col[st + a]; const double kv = val[st + a];
-				int b = a - 1;
-				while(b >= 0 && lc[b] > kc) { lc[b + 1] = lc[b]; lv[b + 1] = lv[b]; --b; }
-				lc[b + 1] = kc; lv[b + 1] = kv;
+				const int cc = sc[w][a2];
+				int r = 0;
+				for(int b2 = 0; b2 < m; ++b2) r += (sc[w][b2] < cc);
+				col[st + r] = cc; val[st + r] = sv[w][a2];
 			}
-			for(int a = 0; a < m; ++a) { col[st + a] = lc[a]; val[st + a] = lv[a]; }
+			__syncwarp();
 			continue;
 		}
-		for(int a = st + 1; a < ed; ++a)
+		if(lane != 0) continue;
+		for(int a2 = st + 1; a2 < ed; ++a2)
 		{
-			const int kc = col[a]; const double kv = val[a];
-			int b = a - 1;
-			while(b >= st && col[b] > kc) { col[b + 1] = col[b]; val[b + 1] = val[b]; --b; }
-			col[b + 1] = kc; val[b + 1] = kv;
+			const int kc = col[a2]; const double kv = val[a2];
+			int b2 = a2 - 1;
+			while(b2 >= st && col[b2] > kc) { col[b2 + 1] = col[b2]; val[b2 + 1] = val[b2]; --b2; }
+			col[b2 + 1] = kc; val[b2 + 1] = kv;
 		}
 	}
 }
@@ -490,12 +497,23 @@ __global__ void __launch_bounds__(256) KGemmWarp(int nx, const int *__restrict__
 		const int i = (int)row;
 		int m = 0;
 		bool over = false;
-		for(int kx = xptr[i]; kx < xptr[i + 1] && !over; ++kx)
+		const int xe = xptr[i + 1];
+		//  X's row 32 entries at a time: each lane loads one entry and its Y
+		//  row's bounds, which the warp then takes in order by shuffles
+		for(int xb = xptr[i]; xb < xe && !over; xb += 32)
 		{
-			const int k = xcol[kx];
-			const double xv = FILL ? xval[kx] : 0.0;
-			const int y1 = yptr[k + 1];
-			for(int base = yptr[k]; base < y1 && !over; base += 32)
+			const int xk = xb + lane;
+			const bool av = xk < xe;
+			const int kk = av ? xcol[xk] : 0;
+			const double xvv = (FILL && av) ? xval[xk] : 0.0;
+			const int ys = av ? yptr[kk] : 0, ye = av ? yptr[kk + 1] : 0;
+			const int cntx = (xe - xb < 32) ? xe - xb : 32;
+		for(int jx = 0; jx < cntx && !over; ++jx)
+		{
+			const int y0 = __shfl_sync(0xffffffffu, ys, jx);
+			const int y1 = __shfl_sync(0xffffffffu, ye, jx);
+			const double xv = __shfl_sync(0xffffffffu, xvv, jx);
+			for(int base = y0; base < y1 && !over; base += 32)
 			{
 				const int ky = base + lane;
 				const bool active = ky < y1;
@@ -519,6 +537,7 @@ __global__ void __launch_bounds__(256) KGemmWarp(int nx, const int *__restrict__
 				__syncwarp();
 			}
 		}
+		}
 		if(!FILL)
 		{
 			if(lane == 0)
@@ -529,8 +548,15 @@ __global__ void __launch_bounds__(256) KGemmWarp(int nx, const int *__restrict__
 		}
 		else
 		{
-			const int o = cptr[i];
-			for(int q = lane; q < m; q += 32)
+			//  cptr given: the row at its place; else staged at i * CAP with
+			//  its count (KGemmCompact moves it once the counts are scanned)
+			if(!cptr && lane == 0)
+			{
+				if(over) { atomicExch(overflow, 1); cnt[i] = 0; }
+				else cnt[i] = m;
+			}
+			const long long o = cptr ? (long long)cptr[i] : (long long)i * CAP;
+			for(int q = lane; q < m && !over; q += 32)
 			{
 				const int c = scol[w][q];
 				int r = 0;
@@ -540,6 +566,20 @@ __global__ void __launch_bounds__(256) KGemmWarp(int nx, const int *__restrict__
 			}
 		}
 		__syncwarp();
+	}
+}
+
+//  the staged rows (stride CAP) to their places
+template<int CAP>
+__global__ void KGemmCompact(int nx, const int *__restrict__ cptr, const int *__restrict__ tcol,
+                             const double *__restrict__ tval, int *__restrict__ ccol, double *__restrict__ cval)
+{
+	for(long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < (long long)nx * CAP;
+	    e += (long long)gridDim.x * blockDim.x)
+	{
+		const int i = (int)(e / CAP), r = (int)(e % CAP);
+		const int o = cptr[i];
+		if(r < cptr[i + 1] - o) { ccol[o + r] = tcol[e]; cval[o + r] = tval[e]; }
 	}
 }
 
@@ -569,29 +609,43 @@ __global__ void KGjInit(int n, const int *__restrict__ ptr, const int *__restric
 	}
 }
 
+__device__ __forceinline__ void GjBetter(double &best, int &idx, double a, int ia)
+{
+	if(a > best || (a == best && ia < idx)) { best = a; idx = ia; }
+}
+
 //  the pivot of column c of the panel among rows k..n-1: the first row of
-//  the largest |a|, taken only when larger than |a_kk| (the sequential rule)
+//  the largest |a|, taken only when larger than |a_kk| (the sequential
+//  rule); the largest |a| (first row among equals) over each warp by
+//  shuffles, then over the warps' results -- the same choice as any order of
+//  comparison (a NaN is never taken, as in the sequential scan)
 __device__ __forceinline__ int GjPivot(const double *colc, int n, int k, double *rv, int *ri)
 {
-	const int t = threadIdx.x, nt = blockDim.x;
+	const int t = threadIdx.x, nt = blockDim.x, lane = t & 31, w = t >> 5;
 	double best = -1.0; int idx = n;
-	for(int i = k + t; i < n; i += nt)
+	for(int i = k + t; i < n; i += nt) GjBetter(best, idx, fabs(colc[i]), i);
+	for(int off = 16; off >= 1; off >>= 1)
 	{
-		const double a = fabs(colc[i]);
-		if(a > best || (a == best && i < idx)) { best = a; idx = i; }
+		const double a = __shfl_down_sync(0xffffffffu, best, off);
+		const int ia = __shfl_down_sync(0xffffffffu, idx, off);
+		GjBetter(best, idx, a, ia);
 	}
-	rv[t] = best; ri[t] = idx;
+	if(lane == 0) { rv[w] = best; ri[w] = idx; }
 	__syncthreads();
-	for(int off = nt / 2; off >= 1; off >>= 1)
+	if(w == 0)
 	{
-		if(t < off)
+		const int nw = nt >> 5;
+		best = (lane < nw) ? rv[lane] : -1.0; idx = (lane < nw) ? ri[lane] : n;
+		for(int off = 16; off >= 1; off >>= 1)
 		{
-			const double a = rv[t + off]; const int ia = ri[t + off];
-			if(a > rv[t] || (a == rv[t] && ia < ri[t])) { rv[t] = a; ri[t] = ia; }
+			const double a = __shfl_down_sync(0xffffffffu, best, off);
+			const int ia = __shfl_down_sync(0xffffffffu, idx, off);
+			GjBetter(best, idx, a, ia);
 		}
-		__syncthreads();
+		if(lane == 0) { rv[32] = best; ri[32] = idx; }
 	}
-	const int p = (rv[0] > fabs(colc[k])) ? ri[0] : k;
+	__syncthreads();
+	const int p = (rv[32] > fabs(colc[k])) ? ri[32] : k;
 	__syncthreads();
 	return p;
 }

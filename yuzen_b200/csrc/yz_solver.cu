@@ -361,8 +361,9 @@ int Solver::ScanCounts(const int *cnt, int *out, int n, const int *flag, int *fl
 }
 
 //  C = X Y: one warp per row with room for 64 distinct columns (KGemmWarp),
-//  the thread-per-row kernels with kRowCap where a row needs more;
-//  returns nnz(C)
+//  each row computed once into a staging slot and moved to its place after
+//  the counts are scanned; the thread-per-row kernels with kRowCap where a
+//  row needs more; returns nnz(C)
 int Solver::Gemm(int nx, const int *xptr, const int *xcol, const double *xval, const int *yptr, const int *ycol,
                  const double *yval, DBuf<int> &cptr, DBuf<int> &ccol, DBuf<double> &cval)
 {
@@ -370,8 +371,10 @@ int Solver::Gemm(int nx, const int *xptr, const int *xcol, const double *xval, c
 	const int g = GridFor(nx, 128);
 	const int gw = GridFor((long long)nx * 32, 256, 148 * 64);
 	YZ_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int), _st));
-	YZ_LAUNCH((KGemmWarp<64, false>), gw, 256, 0, _st, nx, xptr, xcol, xval, yptr, ycol, yval, _cnt.get(), nullptr,
-	          nullptr, nullptr, overflow);
+	//  one pass: every row into a staging slot of 64, with its count
+	_gtCol.reserve((size_t)nx * 64); _gtVal.reserve((size_t)nx * 64);
+	YZ_LAUNCH((KGemmWarp<64, true>), gw, 256, 0, _st, nx, xptr, xcol, xval, yptr, ycol, yval, _cnt.get(), nullptr,
+	          _gtCol.get(), _gtVal.get(), overflow);
 	cptr.reserve((size_t)nx + 1);
 	int ovf = 0;
 	int nnz = ScanCounts(_cnt.get(), cptr.get(), nx, overflow, &ovf);
@@ -385,8 +388,8 @@ int Solver::Gemm(int nx, const int *xptr, const int *xcol, const double *xval, c
 	}
 	ccol.reserve((size_t)nnz); cval.reserve((size_t)nnz);
 	if(wide) YZ_LAUNCH(KGemmFill<kRowCap>, g, 128, 0, _st, nx, xptr, xcol, xval, yptr, ycol, yval, cptr.get(), ccol.get(), cval.get());
-	else YZ_LAUNCH((KGemmWarp<64, true>), gw, 256, 0, _st, nx, xptr, xcol, xval, yptr, ycol, yval, nullptr, cptr.get(),
-	               ccol.get(), cval.get(), overflow);
+	else YZ_LAUNCH(KGemmCompact<64>, GridFor((long long)nx * 64, 256, 148 * 64), 256, 0, _st, nx, cptr.get(),
+	               _gtCol.get(), _gtVal.get(), ccol.get(), cval.get());
 	return nnz;
 }
 
@@ -518,7 +521,8 @@ void Solver::BuildHierarchy(int coarseEnough)
 		YZ_CUDA(cudaMemcpyAsync(_ifill.get(), L.rptr.get(), (size_t)nc * sizeof(int), cudaMemcpyDeviceToDevice, _st));
 		YZ_LAUNCH(KTransposeFill, g, kB, 0, _st, n, L.pptr.get(), L.pcol.get(), L.pval.get(), _ifill.get(),
 		          L.rcol.get(), L.rval.get());
-		YZ_LAUNCH(KRowSort, GridFor(nc, kB), kB, 0, _st, nc, L.rptr.get(), L.rcol.get(), L.rval.get());
+		YZ_LAUNCH(KRowSort, GridFor((long long)nc * 32, 256, 148 * 64), 256, 0, _st, nc, L.rptr.get(), L.rcol.get(),
+		          L.rval.get());
 		//  AP, then A_c = R (AP)
 		Gemm(n, L.ptr.get(), L.col.get(), L.val.get(), L.pptr.get(), L.pcol.get(), L.pval.get(), _apPtr, _apCol, _apVal);
 		if(_levels.size() <= l + 1) _levels.emplace_back(new Level());

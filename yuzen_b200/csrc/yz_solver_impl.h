@@ -115,6 +115,8 @@ private:
 	DBuf<unsigned char> _strong, _iso;
 	DBuf<int> _icnt, _iptr, _icol, _ifill, _state, _flag, _rootId, _first, _cnt, _scan;
 	DBuf<unsigned long long> _T0, _T1;
+	DBuf<int> _gtCol;             // staged rows of a product (64 a row)
+	DBuf<double> _gtVal;
 	DBuf<int> _apPtr, _apCol;
 	DBuf<double> _apVal;
 	DBuf<double> _gj[2];          // [A | I] column-major, the panel multipliers
