@@ -41,8 +41,13 @@ typedef struct yz_settings
 	int    conc;
 } yz_settings;
 
-/* Which arithmetic the inner solve runs in. */
-enum { YZ_PREC_FP64 = 0, YZ_PREC_FP32_REFINED = 1 };
+/* Which arithmetic the AMG preconditioner runs in.  YZ_PREC_FP64: all of it
+ * (the drop-in parity path).  YZ_PREC_FP32_CYCLE: the set-up in FP64 as
+ * always, then every level's A, SPAI0 diagonal, P, R and the coarsest
+ * inverse rounded to float, and the V-cycle run in float; the BiCGStab
+ * around it (its SpMVs, dot products, residuals, convergence test and the
+ * solution) stays FP64, so a converged solve meets the same tolerance. */
+enum { YZ_PREC_FP64 = 0, YZ_PREC_FP32_CYCLE = 1 };
 
 const char* yz_last_error(void);
 
@@ -71,8 +76,19 @@ int yz_solver_solve(yz_solver* s, const yz_settings* set, const double* values,
 int yz_solver_solve_device(yz_solver* s, const yz_settings* set, const double* d_values,
                            const double* d_rhs, double* d_x, int* iter, double* resid);
 
-/* Inner-solve arithmetic (YZ_PREC_*).  FP64 is the drop-in parity path. */
+/* Preconditioner arithmetic (YZ_PREC_*), from the next solve on. */
 int yz_solver_set_precision(yz_solver* s, int precision);
+
+/* AMG hierarchy reuse.  0 (the default, the reference's way): a new SA-AMG
+ * set-up for every solve.  k > 0: a set-up serves up to k further solves of
+ * the same pattern -- the finest level's SPAI0 is recomputed from each new
+ * matrix and the cycle's finest level is the new matrix, the coarser levels
+ * are the set-up's -- and the BiCGStab loop is replayed as one cached CUDA
+ * graph.  A solve on a reused hierarchy that fails is repeated on a new
+ * set-up; one that takes clearly more iterations than the set-up's first
+ * solve (more than max(4, half) again) makes the next solve set up afresh.
+ * The Krylov solve stays FP64 to the same tolerance. */
+int yz_solver_set_amg_reuse(yz_solver* s, int max_solves);
 
 /* ILinearSolverBackend::Memory / SetMemory (LinearSolverBackend.h:89-102):
  * the TryBackoff counters.  yz_solver_memory returns the count written. */
@@ -216,6 +232,11 @@ typedef struct yz_step_stats
 int yz_step_create(int device, const yz_step_params* p, const double* h, const double* c,
                    const double* s, yz_step** out);
 int yz_step_destroy(yz_step* st);
+/* Preconditioner arithmetic (YZ_PREC_*) of the step's height and
+ * concentration solves, from the next solve on; FP64 unless set. */
+int yz_step_set_precision(yz_step* st, int precision);
+/* AMG hierarchy reuse (yz_solver_set_amg_reuse) for the step's solves. */
+int yz_step_set_amg_reuse(yz_step* st, int max_solves);
 /* Advance nsteps time steps (TimeAdvance + the clock advance each). */
 int yz_step_advance(yz_step* st, int nsteps, yz_step_stats* stats);
 /* Fields after the last step (host arrays of nx*ny; null pointers skipped). */

@@ -126,6 +126,20 @@ void Spmv(const Csr &A, const double *x, double *y)
 	}
 }
 
+//  the restriction R t: each row as four strided partial sums (entries q,
+//  q+4, ... of the row into partial q, from 0.0) folded (p0 + p1) + (p2 + p3),
+//  the order the device's four lanes per row take
+void Restrict(const Csr &R, const double *t, double *y)
+{
+	for(int i = 0; i < R.n; ++i)
+	{
+		double p[4] = {0.0, 0.0, 0.0, 0.0};
+		const int st = R.ptr[(size_t)i], ed = R.ptr[(size_t)i + 1];
+		for(int k = st; k < ed; ++k) p[(k - st) & 3] = p[(k - st) & 3] + R.val[(size_t)k] * t[R.col[(size_t)k]];
+		y[i] = (p[0] + p[1]) + (p[2] + p[3]);
+	}
+}
+
 void Residual(const Csr &A, const double *f, const double *x, double *r)
 {
 	for(int i = 0; i < A.n; ++i)
@@ -469,7 +483,7 @@ struct Hierarchy
 		if(l + 1 < lv.size())
 		{
 			Level &C = lv[l + 1];
-			Spmv(L.R, L.t.data(), C.f.data());
+			Restrict(L.R, L.t.data(), C.f.data());
 			Cycle(l + 1, C.f.data(), C.x.data());
 			for(int i = 0; i < n; ++i)
 			{

@@ -120,7 +120,7 @@ STEP_CASES = {
         "Physics.Slip.Enable": True, "Physics.Slip.Length": 5e-7,
         "Numerics.Convection.Height": "VanLeer", "Numerics.Convection.Concentration": "Koren",
         "Numerics.TimeStepControl.Enable": True, "Numerics.TimeStepControl.KeepSteps": 2,
-        "Numerics.TimeStepControl.ChangeFactor": 0.75, "Numerics.InitialDt": 1e-2,
+        "Numerics.TimeStepControl.ChangeFactor": 0.75, "Numerics.InitialDt": 1e-3,
     }, 6, -1),
     # capillary + disjoining with the time-step control on
     "step_adaptive_40": ("allphys_2d_reg.toml", {

@@ -186,3 +186,98 @@ def test_graph_loop_bitwise():
     r = subprocess.run([sys.executable, "-c", _GRAPH_CHILD, repo], env=dict(os.environ, YZ_GRAPH="1"),
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout[-2000:] + r.stderr[-2000:]
+
+
+def _true_residual(d, x):
+    """|b - A x| / |b| of the row-scaled system (the one the solve's
+    tolerance is on), in numpy FP64"""
+    n, rp, col, val = d["n"], d["rowptr"], d["col"], d["values"]
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    r = np.asarray(d["rhs"], np.float64) - np.bincount(rows, weights=val * x[col], minlength=n)
+    b = np.asarray(d["rhs"], np.float64).copy()
+    if int(d["scaling"]):
+        dia = val[rp[:-1]]              # the diagonal is stored first
+        ok = np.abs(dia) >= 1e-30
+        r[ok] /= dia[ok]
+        b[ok] /= dia[ok]
+    return np.linalg.norm(r) / np.linalg.norm(b)
+
+
+_FP32_CASES = [c for c in _amg_cases() if not c.values[0]["conc"]] + [
+    pytest.param(_systems.film_system(200, seed=7, periodic=True), id="film200-periodic"),
+    pytest.param(_systems.film_system(384, seed=11), id="film384")]
+
+
+@pytest.mark.parametrize("d", _FP32_CASES)
+def test_fp32_cycle_meets_the_tolerance(d):
+    """The V-cycle in float (PREC_FP32_CYCLE) changes the preconditioner only:
+    the hierarchy is the FP64 set-up's (the oracle's to the bit), and the
+    FP64 BiCGStab around the cycle converges to the same tolerance in about
+    as many iterations.  Its x has the true residual of the oracle's x (the
+    recurrence's residual drifts from the true one by about the same amount
+    in both, far above the tolerance where the start was far off) and lies
+    within what that residual allows of the oracle's x."""
+    be = yz.B200Backend()
+    be.SetPrecision(yz.PREC_FP32_CYCLE)
+    g = gpu_solve(d, backend=be)
+    o = _oracle.OracleSolver()
+    r = o.solve(d)
+    _levels_equal(be.levels(), o.levels())
+    assert g[0] == r[0] == 0, (g[:3], r[:3])
+    eps = float(d["epsilon"])
+    assert g[2] <= eps
+    tg, to = _true_residual(d, g[3]), _true_residual(d, r[3])
+    assert tg <= max(2.0 * eps, 4.0 * to), (tg, to, eps)
+    assert g[1] <= r[1] + max(2, r[1] // 4), (g[1], r[1])
+    assert np.linalg.norm(g[3] - r[3]) <= 1e4 * max(eps, to) * np.linalg.norm(r[3]) + 1e-300, \
+        (np.linalg.norm(g[3] - r[3]) / np.linalg.norm(r[3]), eps, to)
+
+
+def test_precision_usage_errors():
+    be = yz.B200Backend()
+    with pytest.raises(yz.YzError):
+        be.SetPrecision(7)
+    be.SetPrecision(yz.PREC_FP32_CYCLE)
+    be.SetPrecision(yz.PREC_FP64)
+
+
+def _height_sequences():
+    """the film's solves of each golden run, in the order the reference made
+    them (one pattern per run)"""
+    for f in GOLDEN:
+        seq = [d for d in dumpio.load_npz(f) if int(d["flavour"]) == _oracle.YZO_AMG and not d["conc"]]
+        if len(seq) >= 2:
+            yield pytest.param(seq, id=f.stem)
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32cycle"])
+@pytest.mark.parametrize("seq", list(_height_sequences()))
+def test_amg_reuse_meets_the_tolerance(seq, precision):
+    """With hierarchy reuse on, the solves after the first run on the first
+    solve's hierarchy (fewer launches: no set-up) and the FP64 BiCGStab still
+    meets each solve's tolerance, with the true residual of the oracle's own
+    answer."""
+    fresh, reused = yz.B200Backend(), yz.B200Backend()
+    for be in (fresh, reused):
+        be.SetPrecision(precision)
+    reused.SetAmgReuse(8)
+    n_fresh, n_reused = [], []
+    for d in seq:
+        for be, counts in ((fresh, n_fresh), (reused, n_reused)):
+            l0 = be.launches()
+            g = gpu_solve(d, backend=be)
+            counts.append(be.launches() - l0)
+            r = _oracle.OracleSolver().solve(d)
+            assert g[0] == 0, g[:3]
+            tg, to = _true_residual(d, g[3]), _true_residual(d, r[3])
+            assert tg <= max(2.0 * float(d["epsilon"]), 4.0 * to), (tg, to, d["epsilon"])
+    #  the second and later solves skipped the set-up (while the iteration
+    #  counts stayed near the first solve's)
+    assert any(b < a for a, b in zip(n_fresh[1:], n_reused[1:])), (n_fresh, n_reused)
+
+
+def test_amg_reuse_usage_errors():
+    be = yz.B200Backend()
+    with pytest.raises(yz.YzError):
+        be.SetAmgReuse(-1)
+    be.SetAmgReuse(0)

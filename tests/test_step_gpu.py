@@ -101,3 +101,44 @@ def test_fields_after_steps(f):
     dref = cref - d["field_c0"]
     assert np.linalg.norm((c - d["field_c0"]) - dref) <= 1e-6 * np.linalg.norm(dref), \
         (np.linalg.norm((c - d["field_c0"]) - dref), np.linalg.norm(dref))
+
+
+@pytest.mark.parametrize("f", STEPS, ids=IDS)
+def test_fields_after_steps_fp32_cycle(f):
+    """The step with its solves' V-cycles in float (PREC_FP32_CYCLE): the
+    FP64 BiCGStab meets the same tolerances, so h after N steps stays within
+    1e-8 relative L2 of the reference's FP64 run (the error bar the FP32 arm
+    is held to) and the clock is the same."""
+    d = stateio.load_npz(f)
+    st = make(d)
+    st.set_precision(1)
+    stats = st.advance(d["steps_done"])
+    h, c = st.fields()
+    ref = d["field_h1"]
+    rel = np.linalg.norm(h - ref) / np.linalg.norm(ref)
+    assert rel <= 1e-8, rel
+    assert abs(stats["time"] - d["t_end"]) <= 1e-12 * abs(d["t_end"]), (stats["time"], d["t_end"])
+    if d["conc_field"]:
+        cref = d["field_c1"]
+        assert np.linalg.norm(c - cref) / np.linalg.norm(cref) <= 1e-8
+
+
+@pytest.mark.parametrize("f", STEPS, ids=IDS)
+def test_fields_after_steps_fp32_cycle_amg_reuse(f):
+    """The fast form of the step: V-cycles in float and each AMG set-up
+    serving several solves.  The FP64 Newton iteration and BiCGStab meet the
+    same tolerances, so h stays within 1e-8 relative L2 of the reference's
+    FP64 run."""
+    d = stateio.load_npz(f)
+    st = make(d)
+    st.set_precision(1)
+    st.set_amg_reuse(8)
+    stats = st.advance(d["steps_done"])
+    h, c = st.fields()
+    ref = d["field_h1"]
+    rel = np.linalg.norm(h - ref) / np.linalg.norm(ref)
+    assert rel <= 1e-8, rel
+    assert abs(stats["time"] - d["t_end"]) <= 1e-12 * abs(d["t_end"]), (stats["time"], d["t_end"])
+    if d["conc_field"]:
+        cref = d["field_c1"]
+        assert np.linalg.norm(c - cref) / np.linalg.norm(cref) <= 1e-8

@@ -22,7 +22,7 @@ import numpy as np
 
 __all__ = [
     "LinearSolverSettings", "B200Backend", "MakeLinearSolverBackend", "CrsPattern",
-    "lib", "lib_path", "YzError", "EXPORTED_SYMBOLS", "dot", "spmv",
+    "lib", "lib_path", "YzError", "EXPORTED_SYMBOLS", "dot", "spmv", "PREC_FP64", "PREC_FP32_CYCLE",
 ]
 
 _HERE = Path(__file__).resolve().parent
@@ -37,8 +37,13 @@ EXPORTED_SYMBOLS = (
     "yz_step_create", "yz_step_destroy", "yz_step_advance", "yz_step_get_fields", "yz_step_pattern",
     "yz_step_system", "yz_pattern_2d", "yz_step_set_fields", "yz_launch_count",
     "yz_time_kernel", "yz_kernel_time", "yz_dot_noalloc", "yz_dot_noalloc_max",
-    "yz_step_conc_pattern", "yz_step_conc_system",
+    "yz_step_conc_pattern", "yz_step_conc_system", "yz_step_set_precision", "yz_solver_set_amg_reuse",
+    "yz_step_set_amg_reuse",
 )
+
+#: the preconditioner's arithmetic (YZ_PREC_* of include/yuzen_b200.h)
+PREC_FP64 = 0
+PREC_FP32_CYCLE = 1
 
 
 class YzError(RuntimeError):
@@ -77,6 +82,7 @@ def lib():
     L.yz_solver_solve_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Settings), ctypes.c_void_p,
                                          ctypes.c_void_p, ctypes.c_void_p, _i32p, _f64p]
     L.yz_solver_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.yz_solver_set_amg_reuse.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_solver_memory.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_int]
     L.yz_solver_set_memory.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_int]
     L.yz_solver_levels.argtypes = [ctypes.c_void_p]
@@ -202,6 +208,16 @@ class B200Backend:
                                                   ctypes.c_void_p(rhs_ptr), ctypes.c_void_p(x_ptr),
                                                   ctypes.byref(it), ctypes.byref(res)), "yz_solver_solve_device")
         return ret, it.value, res.value
+
+    def SetPrecision(self, precision: int) -> None:
+        """PREC_FP64 (the drop-in path) or PREC_FP32_CYCLE (the V-cycle in
+        float inside the FP64 BiCGStab), from the next solve on."""
+        _check(lib().yz_solver_set_precision(self._h, precision), "yz_solver_set_precision")
+
+    def SetAmgReuse(self, max_solves: int) -> None:
+        """0: a new AMG set-up every solve (the reference's way); k > 0: a
+        set-up serves up to k further solves (yz_solver_set_amg_reuse)."""
+        _check(lib().yz_solver_set_amg_reuse(self._h, max_solves), "yz_solver_set_amg_reuse")
 
     def Memory(self) -> list:
         buf = np.zeros(8, dtype=np.float64)

@@ -41,21 +41,22 @@ __device__ __forceinline__ void RowRange(const int *__restrict__ ptr, const int 
 	else { start = ptr[i]; stride = 1; }
 }
 
-//  sum_k val[e_k] * X(col[e_k]) over a row (e_k = st + k stride), from 0.0 in
+//  sum_k val[e_k] * X(col[e_k]) over a row (e_k = st + k stride), from 0 in
 //  the row's order: the loads of four entries are issued together and the
 //  products then added one after the other, so the sum is the sequential
-//  one with four loads in flight instead of one
-template<class XF>
-__device__ __forceinline__ double RowSum(int st, int len, int sd, const int *__restrict__ col,
-                                         const double *__restrict__ val, XF xf)
+//  one with four loads in flight instead of one.  T is the arithmetic (the
+//  type of the values): double everywhere but in the FP32 V-cycle.
+template<class T, class XF>
+__device__ __forceinline__ T RowSum(int st, int len, int sd, const int *__restrict__ col, const T *__restrict__ val,
+                                    XF xf)
 {
-	double s = 0.0;
+	T s = T(0);
 	int k = 0, e = st;
 	for(; k + 4 <= len; k += 4, e += 4 * sd)
 	{
 		const int c0 = col[e], c1 = col[e + sd], c2 = col[e + 2 * sd], c3 = col[e + 3 * sd];
-		const double v0 = val[e], v1 = val[e + sd], v2 = val[e + 2 * sd], v3 = val[e + 3 * sd];
-		const double x0 = xf(c0), x1 = xf(c1), x2 = xf(c2), x3 = xf(c3);
+		const T v0 = val[e], v1 = val[e + sd], v2 = val[e + 2 * sd], v3 = val[e + 3 * sd];
+		const T x0 = xf(c0), x1 = xf(c1), x2 = xf(c2), x3 = xf(c3);
 		s = s + v0 * x0;
 		s = s + v1 * x1;
 		s = s + v2 * x2;
@@ -72,7 +73,7 @@ __device__ __forceinline__ double RowSum(int st, int len, int sd, const int *__r
 __global__ void KScaleGather(int n, const int *__restrict__ rowptr, const int *__restrict__ ssrc,
                              const double *__restrict__ values, const double *__restrict__ rhs, int scaling,
                              double *__restrict__ val0, double *__restrict__ b, const int *__restrict__ sellOff,
-                             double *__restrict__ sellVal)
+                             double *__restrict__ sellVal, float *__restrict__ sellVal32)
 {
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
@@ -81,7 +82,13 @@ __global__ void KScaleGather(int n, const int *__restrict__ rowptr, const int *_
 		const double d = scaling ? values[st] : 1.0;
 		if(!scaling || fabs(d) < 1.0e-30)
 		{
-			for(int k = st; k < ed; ++k) { const double v = values[ssrc[k]]; val0[k] = v; sellVal[so + 32 * (k - st)] = v; }
+			for(int k = st; k < ed; ++k)
+			{
+				const double v = values[ssrc[k]];
+				val0[k] = v;
+				sellVal[so + 32 * (k - st)] = v;
+				if(sellVal32) sellVal32[so + 32 * (k - st)] = (float)v;
+			}
 			b[i] = rhs[i];
 			continue;
 		}
@@ -91,6 +98,7 @@ __global__ void KScaleGather(int n, const int *__restrict__ rowptr, const int *_
 			const double v = values[ssrc[k]] * inv;
 			val0[k] = v;
 			sellVal[so + 32 * (k - st)] = v;
+			if(sellVal32) sellVal32[so + 32 * (k - st)] = (float)v;
 		}
 		b[i] = rhs[i] * inv;
 	}
@@ -753,27 +761,39 @@ __global__ void KGjExtract(int n, const double *__restrict__ Mc, double *__restr
 //  word of its BiCGStab run (non-zero once it has stopped), and does nothing
 //  when it is set: the iterations are queued ahead of the host's check.
 //--------------------------------------------------------------------------
+//  The kernels of the cycle are written for the arithmetic T of the cycle's
+//  matrices and vectors (double; float in the FP32 V-cycle, whose matrices
+//  are the FP64 set-up's rounded to float).  The right-hand side f of the
+//  finest level and the result x written there are the Krylov vectors, of
+//  type TF and TX: each value is converted to T where it is read and the
+//  result to TX where it is written.  With T = TF = TX = double every
+//  conversion is the identity and the arithmetic the oracle's.
+//--------------------------------------------------------------------------
 //  x = m .* f, t = f - A x (x of the neighbours recomputed as m_j * f_j)
+template<class T, class TF, class TX>
 __global__ void KPreSmoothResidual(const int *__restrict__ halt, int n, const int *__restrict__ ptr,
                                    const int *__restrict__ sellOff, const int *__restrict__ col,
-                                   const double *__restrict__ val, const double *__restrict__ M,
-                                   const double *__restrict__ f, double *__restrict__ x, double *__restrict__ t)
+                                   const T *__restrict__ val, const T *__restrict__ M, const TF *__restrict__ f,
+                                   TX *__restrict__ x, T *__restrict__ t)
 {
 	if(halt && *halt) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		int st, len, sd;
 		RowRange(ptr, sellOff, i, st, len, sd);
-		const double s = RowSum(st, len, sd, col, val, [&](int c) { return M[c] * f[c]; });
-		x[i] = M[i] * f[i];
-		t[i] = f[i] - s;
+		const T s = RowSum(st, len, sd, col, val, [&](int c) { return M[c] * (T)f[c]; });
+		const T fi = (T)f[i];
+		x[i] = (TX)(M[i] * fi);
+		t[i] = fi - s;
 	}
 }
 
-__global__ void KPreSmooth(const int *__restrict__ halt, int n, const double *__restrict__ M, const double *__restrict__ f, double *__restrict__ x)
+template<class T, class TF, class TX>
+__global__ void KPreSmooth(const int *__restrict__ halt, int n, const T *__restrict__ M, const TF *__restrict__ f,
+                           TX *__restrict__ x)
 {
 	if(halt && *halt) return;
-	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = M[i] * f[i];
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = (TX)(M[i] * (T)f[i]);
 }
 
 //  y = A x (from 0.0, stored order)
@@ -785,51 +805,105 @@ __global__ void KSpmv(const int *__restrict__ halt, int n, const int *__restrict
 		y[i] = RowSum(ptr[i], ptr[i + 1] - ptr[i], 1, col, val, [&](int c) { return x[c]; });
 }
 
+//  f_c = R t with four lanes per row: lane q sums the row's entries q, q+4,
+//  ... from 0.0 and the four partials are folded (p0 + p1) + (p2 + p3) --
+//  the oracle's Restrict -- so that the long rows of R (an aggregate and its
+//  neighbours) are taken four entries at a time; eight rows a warp, the
+//  loop alike for all its lanes
+template<class T>
+__global__ void KRestrict(const int *__restrict__ halt, int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                          const T *__restrict__ val, const T *__restrict__ t, T *__restrict__ y)
+{
+	if(halt && *halt) return;
+	const int lane = threadIdx.x & 31, q = lane & 3;
+	const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+	for(long long base = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 8; base < n; base += warps * 8)
+	{
+		const long long row = base + (lane >> 2);
+		const bool active = row < n;
+		T p = T(0);
+		if(active)
+		{
+			const int st = ptr[row], len = ptr[row + 1] - st;
+			for(int k = q; k < len; k += 4) p = p + val[st + k] * t[col[st + k]];
+		}
+		p = p + __shfl_down_sync(0xffffffffu, p, 1);
+		p = p + __shfl_down_sync(0xffffffffu, p, 2);
+		if(active && q == 0) y[row] = p;
+	}
+}
+
 //  xout = x + P xc
+template<class T>
 __global__ void KProlong(const int *__restrict__ halt, int n, const int *__restrict__ pptr, const int *__restrict__ pcol,
-                         const double *__restrict__ pval, const double *__restrict__ xc,
-                         const double *__restrict__ x, double *__restrict__ xout)
+                         const T *__restrict__ pval, const T *__restrict__ xc, const T *__restrict__ x,
+                         T *__restrict__ xout)
 {
 	if(halt && *halt) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
-		const double s = RowSum(pptr[i], pptr[i + 1] - pptr[i], 1, pcol, pval, [&](int c) { return xc[c]; });
+		const T s = RowSum(pptr[i], pptr[i + 1] - pptr[i], 1, pcol, pval, [&](int c) { return xc[c]; });
 		xout[i] = x[i] + s;
 	}
 }
 
 //  xout = x + m .* (f - A x)
+template<class T, class TF, class TX>
 __global__ void KPostSmooth(const int *__restrict__ halt, int n, const int *__restrict__ ptr,
-                            const int *__restrict__ sellOff, const int *__restrict__ col,
-                            const double *__restrict__ val, const double *__restrict__ M,
-                            const double *__restrict__ f, const double *__restrict__ x, double *__restrict__ xout)
+                            const int *__restrict__ sellOff, const int *__restrict__ col, const T *__restrict__ val,
+                            const T *__restrict__ M, const TF *__restrict__ f, const T *__restrict__ x,
+                            TX *__restrict__ xout)
 {
 	if(halt && *halt) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		int st, len, sd;
 		RowRange(ptr, sellOff, i, st, len, sd);
-		const double s = RowSum(st, len, sd, col, val, [&](int c) { return x[c]; });
-		const double t = f[i] - s;
-		xout[i] = x[i] + M[i] * t;
+		const T s = RowSum(st, len, sd, col, val, [&](int c) { return x[c]; });
+		const T t = (T)f[i] - s;
+		xout[i] = (TX)(x[i] + M[i] * t);
 	}
 }
 
 //  x = inv f, inv row-major: one warp per row, lane l sums j = l, l+32, ...
 //  from 0.0 (coalesced reads of the row), then a pairwise shuffle fold
-__global__ void KDenseMV(const int *__restrict__ halt, int n, const double *__restrict__ inv, const double *__restrict__ f, double *__restrict__ x)
+template<class T, class TF, class TX>
+__global__ void KDenseMV(const int *__restrict__ halt, int n, const T *__restrict__ inv, const TF *__restrict__ f,
+                         TX *__restrict__ x)
 {
 	if(halt && *halt) return;
 	const int lane = threadIdx.x & 31;
 	const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
 	for(long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps)
 	{
-		const double *row = inv + (size_t)i * n;
-		double s = 0.0;
-		for(int j = lane; j < n; j += 32) s = s + row[j] * f[j];
+		const T *row = inv + (size_t)i * n;
+		T s = T(0);
+		for(int j = lane; j < n; j += 32) s = s + row[j] * (T)f[j];
 #pragma unroll
 		for(int off = 16; off >= 1; off >>= 1) s = s + __shfl_down_sync(0xffffffffu, s, off);
-		if(lane == 0) x[i] = s;
+		if(lane == 0) x[i] = (TX)s;
+	}
+}
+
+//  the FP32 copies of the V-cycle's matrices: dst_k[i] = (float)src_k[i] over
+//  a list of arrays, one launch for all of them
+struct RoundList
+{
+	enum { kMax = 64 };
+	const double *src[kMax];
+	float *dst[kMax];
+	long long n[kMax];
+	int count;
+};
+
+__global__ void KRoundToFloat(RoundList L)
+{
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for(int k = 0; k < L.count; ++k)
+	{
+		const double *__restrict__ s = L.src[k];
+		float *__restrict__ d = L.dst[k];
+		for(long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < L.n[k]; i += stride) d[i] = (float)s[i];
 	}
 }
 

@@ -8,7 +8,6 @@
 struct yz_solver
 {
 	std::unique_ptr<yz::Solver> s;
-	int precision = YZ_PREC_FP64;
 };
 
 struct yz_step
@@ -81,8 +80,16 @@ int yz_solver_set_precision(yz_solver *s, int precision)
 {
 	return Guard([&] {
 		if(!s) throw yz::UsageError("yz_solver_set_precision: null solver");
-		if(precision != YZ_PREC_FP64) throw yz::UsageError("yz_solver_set_precision: only YZ_PREC_FP64 is built");
-		s->precision = precision;
+		s->s->SetPrecision(precision);
+		return 0;
+	});
+}
+
+int yz_solver_set_amg_reuse(yz_solver *s, int maxSolves)
+{
+	return Guard([&] {
+		if(!s) throw yz::UsageError("yz_solver_set_amg_reuse: null solver");
+		s->s->SetAmgReuse(maxSolves);
 		return 0;
 	});
 }
@@ -205,6 +212,24 @@ int yz_step_create(int device, const yz_step_params *p, const double *h, const d
 int yz_step_destroy(yz_step *st)
 {
 	return Guard([&] { delete st; return 0; });
+}
+
+int yz_step_set_precision(yz_step *st, int precision)
+{
+	return Guard([&] {
+		if(!st) throw yz::UsageError("yz_step_set_precision: null step");
+		st->s->SetPrecision(precision);
+		return 0;
+	});
+}
+
+int yz_step_set_amg_reuse(yz_step *st, int maxSolves)
+{
+	return Guard([&] {
+		if(!st) throw yz::UsageError("yz_step_set_amg_reuse: null step");
+		st->s->SetAmgReuse(maxSolves);
+		return 0;
+	});
 }
 
 int yz_step_advance(yz_step *st, int nsteps, yz_step_stats *stats)

@@ -42,6 +42,24 @@ void TimeEnd(cudaStream_t st)
 	g_timeOpen = nullptr;
 }
 
+long long TimeCount()
+{
+	std::lock_guard<std::mutex> lk(g_timeMutex);
+	return (long long)g_timePairs.size();
+}
+
+void TimeDropLast(long long k)
+{
+	std::lock_guard<std::mutex> lk(g_timeMutex);
+	for(; k > 0 && !g_timePairs.empty(); --k)
+	{
+		auto &p = g_timePairs.back();
+		cudaEventDestroy(p.first);
+		cudaEventDestroy(p.second);
+		g_timePairs.pop_back();
+	}
+}
+
 void TimeSelect(const char *name)
 {
 	std::lock_guard<std::mutex> lk(g_timeMutex);

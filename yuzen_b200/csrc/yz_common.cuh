@@ -41,6 +41,8 @@ bool TimedKernel(const char *name);
 bool TimingActive();   // a kernel is selected for per-launch timing
 void TimeBegin(cudaStream_t st);
 void TimeEnd(cudaStream_t st);
+long long TimeCount();            // timed launches recorded so far
+void TimeDropLast(long long k);   // forget the last k of them
 
 #define YZ_LAUNCH(kernel, grid, block, smem, stream, ...)                         \
 	do {                                                                          \

@@ -259,6 +259,7 @@ Solver::~Solver()
 	if(_hring) cudaFreeHost(_hring);
 	cudaEventDestroy(_evRing[0]); cudaEventDestroy(_evRing[1]);
 	cudaEventDestroy(_ev0); cudaEventDestroy(_ev1); cudaEventDestroy(_ev2);
+	FreeLoopGraph(_loop[0]); FreeLoopGraph(_loop[1]);
 	if(_ownStream) cudaStreamDestroy(_st);
 }
 
@@ -275,6 +276,7 @@ void Solver::SetPattern(int n, int nnz, const int *rowptr, const int *scol, cons
 {
 	if(n <= 0 || nnz < n) throw UsageError("set_pattern: need n > 0 and nnz >= n");
 	YZ_CUDA(cudaSetDevice(_device));
+	++_epoch;
 	_n = n; _nnz = nnz;
 	_hptr.assign(rowptr, rowptr + n + 1);
 	if(_hptr[0] != 0 || _hptr[(size_t)n] != nnz) throw UsageError("set_pattern: rowptr[0] must be 0 and rowptr[n] == nnz");
@@ -305,6 +307,7 @@ void Solver::SetPattern(int n, int nnz, const int *rowptr, const int *scol, cons
 		_sellCol.upload(scl.data(), scl.size(), _st);
 		_sellVal.reserve(scl.size());
 		YZ_CUDA(cudaMemsetAsync(_sellVal.get(), 0, scl.size() * sizeof(double), _st));
+		_sellSize = scl.size();
 	}
 	_levels.clear();
 	_levels.emplace_back(new Level());
@@ -439,6 +442,8 @@ void Solver::BuildHierarchy(int coarseEnough)
 {
 	//  the levels of the last set-up are reused with their buffers (which
 	//  only grow): no device allocation or free once the sizes have settled
+	++_epoch;
+	++_rebuilds;
 	_nlev = 1;
 	double eps = 0.08;
 	for(size_t l = 0;; ++l)
@@ -551,8 +556,8 @@ void Solver::Cycle(size_t l, const double *f, double *x)
 		Level &C = *_levels[l + 1];
 		YZ_LAUNCH(KPreSmoothResidual, g, kB, 0, _st, Halt(), n, L.ptr.get(), l == 0 ? _sellOff.get() : nullptr,
 		          l == 0 ? _sellCol.get() : L.col.get(), l == 0 ? _sellVal.get() : L.val.get(), L.M.get(), f, x, L.t.get());
-		YZ_LAUNCH(KSpmv, GridFor(C.n, kB), kB, 0, _st, Halt(), C.n, L.rptr.get(), L.rcol.get(), L.rval.get(), L.t.get(),
-		          C.f.get());
+		YZ_LAUNCH(KRestrict, GridFor((long long)C.n * 4, kB), kB, 0, _st, Halt(), C.n, L.rptr.get(), L.rcol.get(),
+		          L.rval.get(), L.t.get(), C.f.get());
 		Cycle(l + 1, C.f.get(), C.x.get());
 		YZ_LAUNCH(KProlong, g, kB, 0, _st, Halt(), n, L.pptr.get(), L.pcol.get(), L.pval.get(), C.x.get(), x, L.xt.get());
 		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, Halt(), n, L.ptr.get(), l == 0 ? _sellOff.get() : nullptr,
@@ -566,10 +571,108 @@ void Solver::Cycle(size_t l, const double *f, double *x)
 	}
 }
 
+//  The same cycle in float (YZ_PREC_FP32_CYCLE) on the rounded copies that
+//  RoundCycle made: f and x are the Krylov vectors (double) at the finest
+//  level, the level's own float vectors below it.  The pre-smoothed x goes
+//  to the level's x32 and the prolonged one to its xt32, so that the finest
+//  level writes only the result into the caller's x.
+template<class TF, class TX>
+void Solver::Cycle32(size_t l, const TF *f, TX *x)
+{
+	Level &L = *_levels[l];
+	const int n = L.n, g = GridFor(n, kB);
+	if(L.direct)
+	{
+		YZ_LAUNCH((KDenseMV<float, TF, TX>), GridFor((long long)n * 32, kB), kB, 0, _st, Halt(), n, L.inv32.get(), f, x);
+		return;
+	}
+	const int *so = l == 0 ? _sellOff.get() : nullptr, *col = l == 0 ? _sellCol.get() : L.col.get();
+	const float *val = l == 0 ? _sellVal32.get() : L.val32.get();
+	if(l + 1 < _nlev)
+	{
+		Level &C = *_levels[l + 1];
+		YZ_LAUNCH((KPreSmoothResidual<float, TF, float>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, col, val,
+		          L.M32.get(), f, L.x32.get(), L.t32.get());
+		YZ_LAUNCH(KRestrict<float>, GridFor((long long)C.n * 4, kB), kB, 0, _st, Halt(), C.n, L.rptr.get(), L.rcol.get(),
+		          L.rval32.get(), L.t32.get(), C.f32.get());
+		Cycle32<float, float>(l + 1, C.f32.get(), C.x32.get());
+		YZ_LAUNCH(KProlong<float>, g, kB, 0, _st, Halt(), n, L.pptr.get(), L.pcol.get(), L.pval32.get(), C.x32.get(),
+		          L.x32.get(), L.xt32.get());
+		YZ_LAUNCH((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, col, val, L.M32.get(), f,
+		          L.xt32.get(), x);
+	}
+	else
+	{
+		YZ_LAUNCH((KPreSmooth<float, TF, float>), g, kB, 0, _st, Halt(), n, L.M32.get(), f, L.xt32.get());
+		YZ_LAUNCH((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, col, val, L.M32.get(), f,
+		          L.xt32.get(), x);
+	}
+}
+
+//  After an FP64 set-up: every level's matrices rounded to float for
+//  Cycle32 (the finest level's A was rounded by KScaleGather), in one launch
+void Solver::RoundCycle()
+{
+	RoundList list;
+	list.count = 0;
+	auto add = [&](const double *src, float *dst, long long cnt) {
+		if(cnt <= 0) return;
+		if(list.count == RoundList::kMax)
+		{
+			YZ_LAUNCH(KRoundToFloat, 148 * 4, kB, 0, _st, list);
+			list.count = 0;
+		}
+		list.src[list.count] = src; list.dst[list.count] = dst; list.n[list.count] = cnt; ++list.count;
+	};
+	for(size_t l = 0; l < _nlev; ++l)
+	{
+		Level &L = *_levels[l];
+		const size_t n = (size_t)L.n;
+		L.f32.reserve(n); L.x32.reserve(n); L.t32.reserve(n); L.xt32.reserve(n);
+		if(L.direct)
+		{
+			L.inv32.reserve(n * n);
+			add(L.inv.get(), L.inv32.get(), (long long)(n * n));
+			continue;
+		}
+		L.M32.reserve(n);
+		add(L.M.get(), L.M32.get(), (long long)n);
+		if(l > 0)
+		{
+			L.val32.reserve((size_t)L.nnz);
+			add(L.val.get(), L.val32.get(), L.nnz);
+		}
+		if(l + 1 < _nlev)
+		{
+			L.pval32.reserve((size_t)L.pnnz); L.rval32.reserve((size_t)L.pnnz);
+			add(L.pval.get(), L.pval32.get(), L.pnnz);
+			add(L.rval.get(), L.rval32.get(), L.pnnz);
+		}
+	}
+	if(list.count) YZ_LAUNCH(KRoundToFloat, 148 * 4, kB, 0, _st, list);
+}
+
+void Solver::SetPrecision(int precision)
+{
+	if(precision != YZ_PREC_FP64 && precision != YZ_PREC_FP32_CYCLE)
+		throw UsageError("set_precision: precision must be YZ_PREC_FP64 or YZ_PREC_FP32_CYCLE");
+	if(precision != _precision) ++_epoch;
+	_precision = precision;
+}
+
+void Solver::SetAmgReuse(int maxSolves)
+{
+	if(maxSolves < 0) throw UsageError("set_amg_reuse: max_solves must be >= 0");
+	_amgReuse = maxSolves;
+	_sinceBuild = 0;
+	_stale = true;		// the next AMG solve sets up afresh
+}
+
 void Solver::ApplyPrec(int kind, const double *r, double *z)
 {
 	const int n = _n;
 	if(kind == kPrecDiag) YZ_LAUNCH(KDiagApply, GridFor(n, kB), kB, 0, _st, Halt(), n, _m.get(), r, z);
+	else if(_precision == YZ_PREC_FP32_CYCLE) Cycle32<double, double>(0, r, z);
 	else Cycle(0, r, z);
 }
 
@@ -609,33 +712,26 @@ void Solver::RunIterations(int kind)
 {
 	static const bool useGraph = std::getenv("YZ_GRAPH") != nullptr;
 	Scal *sc = _sc.get();
-	if(TimingActive())
-	{
-		//  one iteration at a time: no launch of the timed kernel is a
-		//  halted one
-		for(;;)
-		{
-			EnqueueIteration(kind);
-			YZ_LAUNCH(KLoopCount, 1, 1, 0, _st, sc);
-			ReadScal();
-			if(_hsc->state != kRun || _hsc->it >= _hsc->maxIter) break;
-		}
-		return;
-	}
-	if(!useGraph)
+	if((!useGraph && _amgReuse == 0) || TimingActive())
 	{
 		//  one iteration kept in flight: the state after iteration k is
 		//  copied to pinned memory and read while iteration k+1 runs; the
 		//  iteration queued after the last one finds the state set and does
-		//  nothing
+		//  nothing.  While a kernel is timed, the timed launches of the
+		//  iterations that found the run stopped are dropped: an iteration
+		//  launches the timed kernel the same number of times each, and the
+		//  iterations that did work are the run's count (exact for a kernel
+		//  that precedes the half-step test, as KSpmvAlpha).
+		const long long mark = TimeCount();
+		int queued = 0;
 		int slot = 0;
-		EnqueueIteration(kind);
+		EnqueueIteration(kind); ++queued;
 		YZ_LAUNCH(KLoopCount, 1, 1, 0, _st, sc);
 		YZ_CUDA(cudaMemcpyAsync(_hring + slot, sc, sizeof(Scal), cudaMemcpyDeviceToHost, _st));
 		YZ_CUDA(cudaEventRecord(_evRing[slot], _st));
 		for(;;)
 		{
-			EnqueueIteration(kind);
+			EnqueueIteration(kind); ++queued;
 			YZ_LAUNCH(KLoopCount, 1, 1, 0, _st, sc);
 			const int next = slot ^ 1;
 			YZ_CUDA(cudaMemcpyAsync(_hring + next, sc, sizeof(Scal), cudaMemcpyDeviceToHost, _st));
@@ -646,11 +742,40 @@ void Solver::RunIterations(int kind)
 			{
 				YZ_CUDA(cudaStreamSynchronize(_st));
 				*_hsc = h;
-				return;
+				break;
 			}
 			slot = next;
 		}
+		const long long timed = TimeCount() - mark;
+		if(timed > 0 && queued > _hsc->it) TimeDropLast(timed / queued * (queued - _hsc->it));
+		return;
 	}
+	//  the graph form: kept (and relaunched) while the hierarchy is reused,
+	//  built for this run alone otherwise
+	LoopGraph &lg = _loop[kind == kPrecAmg ? 1 : 0];
+	if(lg.exec == nullptr || lg.epoch != _epoch)
+	{
+		FreeLoopGraph(lg);
+		BuildLoopGraph(kind, lg);
+		lg.epoch = _epoch;
+	}
+	YZ_CUDA(cudaGraphLaunch(lg.exec, _st));
+	ReadScal();
+	//  the kernels the loop ran
+	g_launches.fetch_add(lg.perBody * (long long)_hsc->bodies);
+	if(_amgReuse == 0) FreeLoopGraph(lg);
+}
+
+void Solver::FreeLoopGraph(LoopGraph &g)
+{
+	if(g.exec) cudaGraphExecDestroy(g.exec);
+	if(g.graph) cudaGraphDestroy(g.graph);
+	g = LoopGraph();
+}
+
+void Solver::BuildLoopGraph(int kind, LoopGraph &lg)
+{
+	Scal *sc = _sc.get();
 	cudaGraph_t graph = nullptr, body = nullptr;
 	cudaGraphExec_t exec = nullptr;
 	YZ_CUDA(cudaGraphCreate(&graph, 0));
@@ -679,13 +804,9 @@ void Solver::RunIterations(int kind)
 			throw;
 		}
 		YZ_CUDA(cudaStreamEndCapture(_st, &body));
-		const long long perBody = g_launches.load() - l0;
-		g_launches.fetch_sub(perBody);
+		lg.perBody = g_launches.load() - l0;
+		g_launches.fetch_sub(lg.perBody);
 		YZ_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-		YZ_CUDA(cudaGraphLaunch(exec, _st));
-		ReadScal();
-		//  the kernels the loop ran
-		g_launches.fetch_add(perBody * (long long)_hsc->bodies);
 	}
 	catch(...)
 	{
@@ -693,8 +814,8 @@ void Solver::RunIterations(int kind)
 		cudaGraphDestroy(graph);
 		throw;
 	}
-	YZ_CUDA(cudaGraphExecDestroy(exec));
-	YZ_CUDA(cudaGraphDestroy(graph));
+	lg.graph = graph;
+	lg.exec = exec;
 }
 
 //  BiCGStab on level 0's matrix (values in _levels[0]); the oracle's
@@ -759,8 +880,15 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 	const long long l0 = g_launches.load();
 	const int n = _n, nnz = _nnz, g = GridFor(n, kB);
 	Level &L0 = *_levels[0];
+	const bool fp32 = _precision == YZ_PREC_FP32_CYCLE;
+	if(fp32)
+	{
+		const float *was = _sellVal32.get();
+		_sellVal32.reserve(_sellSize);
+		if(_sellVal32.get() != was) ++_epoch;
+	}
 	YZ_LAUNCH(KScaleGather, g, kB, 0, _st, n, L0.ptr.get(), _ssrc.get(), dValues, dRhs, set.scaling ? 1 : 0,
-	          L0.val.get(), _b.get(), _sellOff.get(), _sellVal.get());
+	          L0.val.get(), _b.get(), _sellOff.get(), _sellVal.get(), fp32 ? _sellVal32.get() : nullptr);
 	(void)nnz;
 	YZ_CUDA(cudaMemcpyAsync(_x.get(), dX, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
 	YZ_CUDA(cudaMemcpyAsync(_x0.get(), dX, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
@@ -795,10 +923,52 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 		}
 		else
 		{
-			BuildHierarchy(n > 3000 ? 500 : 3000);
-			YZ_CUDA(cudaEventRecord(_ev1, _st));
-			timedSetup = true;
-			broke = !BiCGStab(kPrecAmg, set.max_iteration, set.epsilon, it, err);
+			//  with reuse on, the last set-up's hierarchy serves until it has
+			//  served _amgReuse solves or a solve on it took clearly more
+			//  iterations than the first one did; only the finest level's
+			//  SPAI0 is recomputed from the new matrix (the finest level's A
+			//  in the cycle is the new matrix itself)
+			for(;;)
+			{
+				const bool reuse = _amgReuse > 0 && _haveH && !_stale && _sinceBuild < _amgReuse;
+				if(reuse)
+				{
+					Level &F = *_levels[0];
+					if(!F.direct)
+					{
+						YZ_LAUNCH(KSpai0, g, kB, 0, _st, n, F.ptr.get(), F.col.get(), F.val.get(), F.M.get());
+						if(fp32)
+						{
+							RoundList one;
+							one.count = 1; one.src[0] = F.M.get(); one.dst[0] = F.M32.get(); one.n[0] = n;
+							YZ_LAUNCH(KRoundToFloat, GridFor(n, kB), kB, 0, _st, one);
+						}
+					}
+					++_sinceBuild;
+				}
+				else
+				{
+					BuildHierarchy(n > 3000 ? 500 : 3000);
+					if(fp32) RoundCycle();
+					_sinceBuild = 0;
+					_stale = false;
+				}
+				YZ_CUDA(cudaEventRecord(_ev1, _st));
+				timedSetup = true;
+				broke = !BiCGStab(kPrecAmg, set.max_iteration, set.epsilon, it, err);
+				if(!reuse) { _freshIters = it; break; }
+				if(broke || !(err <= set.epsilon))
+				{
+					//  the old hierarchy failed where a new one may not: set up
+					//  afresh and solve again from the caller's guess
+					_stale = true;
+					itTried += broke ? 0 : it;
+					YZ_CUDA(cudaMemcpyAsync(_x.get(), _x0.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+					continue;
+				}
+				if(it > _freshIters + std::max(4, _freshIters / 2)) _stale = true;
+				break;
+			}
 		}
 	}
 	YZ_CUDA(cudaEventRecord(_ev2, _st));

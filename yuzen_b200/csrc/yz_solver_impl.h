@@ -44,6 +44,10 @@ struct Level
 	DBuf<double> pval, rval;
 	bool direct = false;
 	DBuf<double> inv;		// row-major dense inverse of the direct level
+	//  the FP32 V-cycle (YZ_PREC_FP32_CYCLE): A (levels below the finest),
+	//  SPAI0, P, R and the inverse rounded from the FP64 set-up, and the
+	//  cycle's vectors
+	DBuf<float> val32, M32, pval32, rval32, inv32, f32, x32, t32, xt32;
 };
 
 class Solver
@@ -65,6 +69,10 @@ public:
 	void LevelCopy(int l, int *aptr, int *acol, double *aval, int *pptr, int *pcol, double *pval, int *agg);
 	void Timing(double *setupMs, double *iterMs) const { if(setupMs) *setupMs = _setupMs; if(iterMs) *iterMs = _iterMs; }
 	long long Launches() const { return _launches; }
+	void SetPrecision(int precision);
+	int Precision() const { return _precision; }
+	void SetAmgReuse(int maxSolves);
+	int Rebuilds() const { return _rebuilds; }
 	cudaStream_t Stream() const { return _st; }
 	int Rows() const { return _n; }
 
@@ -73,10 +81,23 @@ private:
 	void BuildHierarchy(int coarseEnough);
 	void DirectInverse(Level &L);
 	void Cycle(size_t l, const double *f, double *x);
+	void RoundCycle();
+	template<class TF, class TX> void Cycle32(size_t l, const TF *f, TX *x);
 	const int *Halt() const { return &_sc.get()->state; }
 	void ApplyPrec(int kind, const double *r, double *z);
 	void EnqueueIteration(int kind);
 	void RunIterations(int kind);
+	//  the BiCGStab loop as a CUDA graph (a conditional while node whose body
+	//  is one iteration); kept across solves while the hierarchy is reused
+	struct LoopGraph
+	{
+		cudaGraph_t graph = nullptr;
+		cudaGraphExec_t exec = nullptr;
+		long long perBody = 0;
+		unsigned epoch = ~0u;
+	};
+	void BuildLoopGraph(int kind, LoopGraph &g);
+	static void FreeLoopGraph(LoopGraph &g);
 	bool BiCGStab(int kind, int maxIter, double tol, int &itOut, double &errOut);
 	double BreakdownResidual();
 	int ReadInt(const int *d);
@@ -95,6 +116,9 @@ private:
 	DBuf<int> _ssrc;
 	DBuf<int> _sellOff, _sellCol;     // the finest level in SELL-32 (slice offsets, columns)
 	DBuf<double> _sellVal;
+	DBuf<float> _sellVal32;           // its FP32 copy, read by the FP32 V-cycle
+	size_t _sellSize = 0;
+	int _precision = YZ_PREC_FP64;
 	DBuf<double> _values, _rhs, _xio;
 	std::vector<std::unique_ptr<Level>> _levels;   // grows, never shrinks
 	size_t _nlev = 0;                              // the levels of the present hierarchy
@@ -123,6 +147,11 @@ private:
 	DBuf<double> _gjPiv;
 	DBuf<int> _gjRow;
 	TryBackoff _offSpai;
+	//  hierarchy reuse (0: a new set-up every solve, the reference's way)
+	int _amgReuse = 0, _sinceBuild = 0, _freshIters = 0, _rebuilds = 0;
+	bool _stale = false;
+	unsigned _epoch = 0;          // bumped whenever a pointer or size a graph holds may change
+	LoopGraph _loop[2];
 	double _setupMs = 0, _iterMs = 0;
 	long long _launches = 0;
 };

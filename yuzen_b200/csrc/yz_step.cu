@@ -153,7 +153,11 @@ struct RowOut
 	unsigned long long *rhsMax;
 };
 
-__global__ void KAssemble(Coef k, int mode, double dt, const int *__restrict__ rowptr,
+#ifndef YZ_ASSEMBLE_MIN_BLOCKS
+#define YZ_ASSEMBLE_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(128, YZ_ASSEMBLE_MIN_BLOCKS)
+KAssemble(Coef k, int mode, double dt, const int *__restrict__ rowptr,
                           const double *__restrict__ H, const double *__restrict__ C,
                           const double *__restrict__ S, RowOut o, FaceBuf fb)
 {
@@ -1129,6 +1133,8 @@ void Step::BuildConc()
 		for(int q = st; q < ed; ++q) { scol[(size_t)q] = tmp[(size_t)(q - st)].first; ssrc[(size_t)q] = tmp[(size_t)(q - st)].second; }
 	}
 	_solverC.reset(new Solver(_device, _st));
+	_solverC->SetPrecision(_precision);
+	_solverC->SetAmgReuse(_amgReuse);
 	_solverC->SetPattern(_n, _nnzC, _rowptrC.data(), scol.data(), ssrc.data());
 	_dRowptrC.upload(_rowptrC.data(), _rowptrC.size(), _st);
 	std::vector<int> pall(n);

@@ -26,6 +26,18 @@ public:
 	int ConcPattern(int *rowptr, int *col) const;
 	void ConcSystem(const double *h, const double *c, double dt, double *val, double *rhs);
 	long long Launches() const { return _solver->Launches(); }
+	void SetPrecision(int precision)
+	{
+		_solver->SetPrecision(precision);
+		if(_solverC) _solverC->SetPrecision(precision);
+		_precision = precision;
+	}
+	void SetAmgReuse(int maxSolves)
+	{
+		_solver->SetAmgReuse(maxSolves);
+		if(_solverC) _solverC->SetAmgReuse(maxSolves);
+		_amgReuse = maxSolves;
+	}
 	int Rows() const { return _n; }
 	int Nnz() const { return _nnz; }
 
@@ -75,6 +87,7 @@ private:
 	bool _conc = false;
 	phys::ConcCoef _kc;
 	std::unique_ptr<Solver> _solverC;
+	int _precision = YZ_PREC_FP64, _amgReuse = 0;
 	int _nnzC = 0;
 	std::vector<int> _rowptrC, _colC;
 	DBuf<int> _dRowptrC, _dPartnerAll;

@@ -109,6 +109,8 @@ def _bind():
                                  ctypes.POINTER(ctypes.c_void_p)]
     L.yz_step_destroy.argtypes = [ctypes.c_void_p]
     L.yz_step_advance.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(StepStats)]
+    L.yz_step_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.yz_step_set_amg_reuse.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_step_get_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
     L.yz_step_set_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
     L.yz_launch_count.restype = ctypes.c_longlong
@@ -136,6 +138,17 @@ class Step:
         self._h = ctypes.c_void_p()
         _check(L.yz_step_create(device, ctypes.byref(params), _fp(h), _fp(c), _fp(s), ctypes.byref(self._h)),
                "yz_step_create")
+
+    def set_precision(self, precision: int) -> None:
+        """The preconditioner arithmetic of the step's solves (PREC_FP64, or
+        PREC_FP32_CYCLE: the V-cycle in float inside the FP64 BiCGStab)."""
+        _check(lib().yz_step_set_precision(self._h, precision), "yz_step_set_precision")
+
+    def set_amg_reuse(self, max_solves: int) -> None:
+        """AMG hierarchy reuse of the step's solves (0: a new set-up every
+        solve, the reference's way; k > 0: a set-up serves up to k further
+        solves)."""
+        _check(lib().yz_step_set_amg_reuse(self._h, max_solves), "yz_step_set_amg_reuse")
 
     def advance(self, nsteps: int = 1) -> dict:
         st = StepStats()
