@@ -175,15 +175,16 @@ print('ok', it)
 """
 
 
-def test_graph_loop_bitwise():
-    """The CUDA-graph form of the iterations (YZ_GRAPH=1: a conditional while
-    node whose body is one BiCGStab iteration) gives the oracle's answer to
-    the bit, as the default queued form does."""
+def test_stream_loop_bitwise():
+    """The iterations launched from the stream (YZ_GRAPH=0: one iteration kept
+    in flight, the form kernel timing uses) give the oracle's answer to the
+    bit, as the default CUDA-graph form (a conditional while node whose body
+    is one BiCGStab iteration) does."""
     import os
     import subprocess
     import sys
     repo = str(Path(__file__).resolve().parents[1])
-    r = subprocess.run([sys.executable, "-c", _GRAPH_CHILD, repo], env=dict(os.environ, YZ_GRAPH="1"),
+    r = subprocess.run([sys.executable, "-c", _GRAPH_CHILD, repo], env=dict(os.environ, YZ_GRAPH="0"),
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout[-2000:] + r.stderr[-2000:]
 
@@ -262,10 +263,16 @@ def test_amg_reuse_meets_the_tolerance(seq, precision):
         be.SetPrecision(precision)
     reused.SetAmgReuse(8)
     n_fresh, n_reused = [], []
+    d0 = seq[0]
+    pat = yz.CrsPattern(d0["rowptr"], d0["col"], d0["sorted_col"], d0["sorted_src"])
     for d in seq:
+        assert np.array_equal(d["rowptr"], d0["rowptr"]) and np.array_equal(d["col"], d0["col"])
+        s = yz.LinearSolverSettings(int(d["precondition"]), bool(d["scaling"]), int(d["max_iteration"]),
+                                    float(d["epsilon"]), bool(d["conc"]))
         for be, counts in ((fresh, n_fresh), (reused, n_reused)):
             l0 = be.launches()
-            g = gpu_solve(d, backend=be)
+            x = np.array(d["x0"], dtype=np.float64, copy=True)
+            g = be.Solve(s, pat, d["values"], d["rhs"], x) + (x,)
             counts.append(be.launches() - l0)
             r = _oracle.OracleSolver().solve(d)
             assert g[0] == 0, g[:3]

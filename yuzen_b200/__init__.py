@@ -172,7 +172,7 @@ class B200Backend:
     def __init__(self, device: int = 0):
         self._h = ctypes.c_void_p()
         _check(lib().yz_solver_create(device, ctypes.byref(self._h)), "yz_solver_create")
-        self._pattern_key = None
+        self._pattern = None
 
     def Name(self) -> str:
         return "b200"
@@ -184,10 +184,10 @@ class B200Backend:
     def SetPattern(self, pat: CrsPattern) -> None:
         _check(lib().yz_solver_set_pattern(self._h, pat.n, pat.nnz, _ip(pat.rowptr), _ip(pat.sorted_col),
                                            _ip(pat.sorted_src)), "yz_solver_set_pattern")
-        self._pattern_key = id(pat)
+        self._pattern = pat     # held, so that the identity test below cannot see a recycled id
 
     def Solve(self, s: LinearSolverSettings, pat: CrsPattern, values, rhs, x):
-        if self._pattern_key != id(pat):
+        if self._pattern is not pat:
             self.SetPattern(pat)
         values = np.ascontiguousarray(values, dtype=np.float64)
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)

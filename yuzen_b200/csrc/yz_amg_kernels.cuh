@@ -66,6 +66,34 @@ __device__ __forceinline__ T RowSum(int st, int len, int sd, const int *__restri
 	return s;
 }
 
+//  RowSum of row i of the finest level (SELL-32, entry k at st + 32 k).  A
+//  stencil row's loop is unrolled to the 16 entries a stencil may have, so
+//  that every offset is read from the kernel's parameters by a constant
+//  index; the sum is the same sequential one.
+template<class T, class XF>
+__device__ __forceinline__ T RowSumSten(const Sten &sn, int i, int st, int len, int sd, const int *__restrict__ col,
+                                        const T *__restrict__ val, XF xf)
+{
+	if(sn.slice && sn.slice[i >> 5])
+	{
+		T s = T(0);
+#pragma unroll
+		for(int k0 = 0; k0 < 16; k0 += 4)
+		{
+			if(k0 >= len) break;
+			T v[4], xv[4];
+#pragma unroll
+			for(int j = 0; j < 4; ++j)
+				if(k0 + j < len) { v[j] = val[st + (k0 + j) * sd]; xv[j] = xf(i + sn.off[k0 + j]); }
+#pragma unroll
+			for(int j = 0; j < 4; ++j)
+				if(k0 + j < len) s = s + v[j] * xv[j];
+		}
+		return s;
+	}
+	return RowSum(st, len, sd, col, val, xf);
+}
+
 //--------------------------------------------------------------------------
 //  ScaleRows + gather into the sorted mirror (LinearSolverBackend.cpp:227-252),
 //  into both layouts of the finest level
@@ -772,7 +800,7 @@ __global__ void KGjExtract(int n, const double *__restrict__ Mc, double *__restr
 //  x = m .* f, t = f - A x (x of the neighbours recomputed as m_j * f_j)
 template<class T, class TF, class TX>
 __global__ void KPreSmoothResidual(const int *__restrict__ halt, int n, const int *__restrict__ ptr,
-                                   const int *__restrict__ sellOff, const int *__restrict__ col,
+                                   const int *__restrict__ sellOff, Sten sn, const int *__restrict__ col,
                                    const T *__restrict__ val, const T *__restrict__ M, const TF *__restrict__ f,
                                    TX *__restrict__ x, T *__restrict__ t)
 {
@@ -781,7 +809,7 @@ __global__ void KPreSmoothResidual(const int *__restrict__ halt, int n, const in
 	{
 		int st, len, sd;
 		RowRange(ptr, sellOff, i, st, len, sd);
-		const T s = RowSum(st, len, sd, col, val, [&](int c) { return M[c] * (T)f[c]; });
+		const T s = RowSumSten(sn, i, st, len, sd, col, val, [&](int c) { return M[c] * (T)f[c]; });
 		const T fi = (T)f[i];
 		x[i] = (TX)(M[i] * fi);
 		t[i] = fi - s;
@@ -850,16 +878,16 @@ __global__ void KProlong(const int *__restrict__ halt, int n, const int *__restr
 //  xout = x + m .* (f - A x)
 template<class T, class TF, class TX>
 __global__ void KPostSmooth(const int *__restrict__ halt, int n, const int *__restrict__ ptr,
-                            const int *__restrict__ sellOff, const int *__restrict__ col, const T *__restrict__ val,
-                            const T *__restrict__ M, const TF *__restrict__ f, const T *__restrict__ x,
-                            TX *__restrict__ xout)
+                            const int *__restrict__ sellOff, Sten sn, const int *__restrict__ col,
+                            const T *__restrict__ val, const T *__restrict__ M, const TF *__restrict__ f,
+                            const T *__restrict__ x, TX *__restrict__ xout)
 {
 	if(halt && *halt) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		int st, len, sd;
 		RowRange(ptr, sellOff, i, st, len, sd);
-		const T s = RowSum(st, len, sd, col, val, [&](int c) { return x[c]; });
+		const T s = RowSumSten(sn, i, st, len, sd, col, val, [&](int c) { return x[c]; });
 		const T t = (T)f[i] - s;
 		xout[i] = (TX)(x[i] + M[i] * t);
 	}

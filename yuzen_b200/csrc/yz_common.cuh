@@ -59,6 +59,17 @@ void SetLastError(const std::string &m);
 //--------------------------------------------------------------------------
 //  device buffer (grows, never shrinks; no allocation when large enough)
 //--------------------------------------------------------------------------
+//  The finest level's stencil: the slices of 32 rows (SELL-32) whose every
+//  row has the pattern's most common column set relative to the row (the
+//  interior rows of the film: columns i + off[k], ascending) are flagged;
+//  their columns are computed, not loaded.  slice null: no flagged slices.
+struct Sten
+{
+	const unsigned char *slice;
+	int len;
+	int off[16];
+};
+
 template<class T>
 struct DBuf
 {

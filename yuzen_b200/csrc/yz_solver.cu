@@ -10,6 +10,8 @@
 #include "yz_amg_kernels.cuh"
 #include "yz_solver_impl.h"
 
+#include <map>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -26,7 +28,7 @@ namespace yz {
 	for(int kk_ = 0, i = blockIdx.x * kRChunk + threadIdx.x; kk_ < kRK; ++kk_, i += kRT)
 
 //  r = b - A x;  bb = b.b, rr = r.r, rho0 = r.r (rh = r)
-__global__ void KBInit(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, const int *__restrict__ col,
+__global__ void __launch_bounds__(kRT, 8) KBInit(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, Sten sn, const int *__restrict__ col,
                        const double *__restrict__ val, const double *__restrict__ b,
                        const double *__restrict__ x, double *__restrict__ r, double *__restrict__ rh,
                        RedScratch rs, Scal *sc)
@@ -38,7 +40,7 @@ __global__ void KBInit(int n, const int *__restrict__ ptr, const int *__restrict
 		if(i >= n) break;
 		int st, len, sd;
 		RowRange(ptr, sellOff, i, st, len, sd);
-		const double s = RowSum(st, len, sd, col, val, [&](int c) { return x[c]; });
+		const double s = RowSumSten(sn, i, st, len, sd, col, val, [&](int c) { return x[c]; });
 		const double ri = b[i] - s;
 		r[i] = ri; rh[i] = ri;
 		a[0] = a[0] + b[i] * b[i];
@@ -75,7 +77,7 @@ __global__ void KPUpdate(int n, const double *__restrict__ r, const double *__re
 }
 
 //  v = A ph; alpha = rho / (rh . v)
-__global__ void KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff,
+__global__ void __launch_bounds__(kRT, 8) KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, Sten sn,
                            const int *__restrict__ col, const double *__restrict__ val, const double *__restrict__ ph,
                            const double *__restrict__ rh, double *__restrict__ v, RedScratch rs, Scal *sc)
 {
@@ -87,7 +89,7 @@ __global__ void KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__rest
 		if(i >= n) break;
 		int st, len, sd;
 		RowRange(ptr, sellOff, i, st, len, sd);
-		const double s = RowSum(st, len, sd, col, val, [&](int c) { return ph[c]; });
+		const double s = RowSumSten(sn, i, st, len, sd, col, val, [&](int c) { return ph[c]; });
 		v[i] = s;
 		a[0] = a[0] + rh[i] * s;
 	}
@@ -130,7 +132,7 @@ __global__ void KXHalf(int n, const double *__restrict__ ph, double *__restrict_
 }
 
 //  t = A sh; omega = (t . s) / (t . t)
-__global__ void KSpmvOmega(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff,
+__global__ void __launch_bounds__(kRT, 8) KSpmvOmega(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, Sten sn,
                            const int *__restrict__ col, const double *__restrict__ val, const double *__restrict__ sh_,
                            const double *__restrict__ s, double *__restrict__ t, RedScratch rs, Scal *sc)
 {
@@ -142,7 +144,7 @@ __global__ void KSpmvOmega(int n, const int *__restrict__ ptr, const int *__rest
 		if(i >= n) break;
 		int st, len, sd;
 		RowRange(ptr, sellOff, i, st, len, sd);
-		const double u = RowSum(st, len, sd, col, val, [&](int c) { return sh_[c]; });
+		const double u = RowSumSten(sn, i, st, len, sd, col, val, [&](int c) { return sh_[c]; });
 		t[i] = u;
 		a[0] = a[0] + u * u;
 		a[1] = a[1] + u * s[i];
@@ -308,6 +310,43 @@ void Solver::SetPattern(int n, int nnz, const int *rowptr, const int *scol, cons
 		_sellVal.reserve(scl.size());
 		YZ_CUDA(cudaMemsetAsync(_sellVal.get(), 0, scl.size() * sizeof(double), _st));
 		_sellSize = scl.size();
+		//  the stencil: the most common column set relative to the row
+		//  (up to 16 entries), and the slices all of whose rows have it
+		std::map<std::vector<int>, int> seen;
+		std::vector<int> rel;
+		for(int i = 0; i < n; ++i)
+		{
+			const int a = _hptr[(size_t)i], b = _hptr[(size_t)i + 1];
+			if(b - a > 16) continue;
+			rel.clear();
+			for(int k = a; k < b; ++k) rel.push_back(scol[k] - i);
+			++seen[rel];
+		}
+		std::vector<int> best;
+		int bestCount = 0;
+		for(auto &kv : seen) if(kv.second > bestCount) { best = kv.first; bestCount = kv.second; }
+		std::vector<unsigned char> flag((size_t)S, 0);
+		int flagged = 0;
+		for(int sl = 0; sl < S && !best.empty(); ++sl)
+		{
+			bool all = true;
+			for(int i = 32 * sl; i < std::min(n, 32 * sl + 32) && all; ++i)
+			{
+				const int a = _hptr[(size_t)i], b = _hptr[(size_t)i + 1];
+				if(b - a != (int)best.size()) { all = false; break; }
+				for(int k = a; k < b; ++k) if(scol[k] - i != best[(size_t)(k - a)]) { all = false; break; }
+			}
+			flag[(size_t)sl] = all ? 1 : 0;
+			flagged += all ? 1 : 0;
+		}
+		_sten = Sten();
+		if(flagged > 0)
+		{
+			_stenSlice.upload(flag.data(), flag.size(), _st);
+			_sten.slice = _stenSlice.get();
+			_sten.len = (int)best.size();
+			for(size_t k = 0; k < best.size(); ++k) _sten.off[k] = best[k];
+		}
 	}
 	_levels.clear();
 	_levels.emplace_back(new Level());
@@ -442,7 +481,7 @@ void Solver::BuildHierarchy(int coarseEnough)
 {
 	//  the levels of the last set-up are reused with their buffers (which
 	//  only grow): no device allocation or free once the sizes have settled
-	++_epoch;
+	++_epochH;
 	++_rebuilds;
 	_nlev = 1;
 	double eps = 0.08;
@@ -542,6 +581,13 @@ void Solver::BuildHierarchy(int coarseEnough)
 }
 
 //  x = V(l) f from a zero guess
+Sten Solver::StenOf(size_t l) const
+{
+	if(l == 0) return _sten;
+	Sten none = Sten();
+	return none;
+}
+
 void Solver::Cycle(size_t l, const double *f, double *x)
 {
 	Level &L = *_levels[l];
@@ -554,19 +600,19 @@ void Solver::Cycle(size_t l, const double *f, double *x)
 	if(l + 1 < _nlev)
 	{
 		Level &C = *_levels[l + 1];
-		YZ_LAUNCH(KPreSmoothResidual, g, kB, 0, _st, Halt(), n, L.ptr.get(), l == 0 ? _sellOff.get() : nullptr,
+		YZ_LAUNCH(KPreSmoothResidual, g, kB, 0, _st, Halt(), n, L.ptr.get(), l == 0 ? _sellOff.get() : nullptr, StenOf(l),
 		          l == 0 ? _sellCol.get() : L.col.get(), l == 0 ? _sellVal.get() : L.val.get(), L.M.get(), f, x, L.t.get());
 		YZ_LAUNCH(KRestrict, GridFor((long long)C.n * 4, kB), kB, 0, _st, Halt(), C.n, L.rptr.get(), L.rcol.get(),
 		          L.rval.get(), L.t.get(), C.f.get());
 		Cycle(l + 1, C.f.get(), C.x.get());
 		YZ_LAUNCH(KProlong, g, kB, 0, _st, Halt(), n, L.pptr.get(), L.pcol.get(), L.pval.get(), C.x.get(), x, L.xt.get());
-		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, Halt(), n, L.ptr.get(), l == 0 ? _sellOff.get() : nullptr,
+		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, Halt(), n, L.ptr.get(), l == 0 ? _sellOff.get() : nullptr, StenOf(l),
 		          l == 0 ? _sellCol.get() : L.col.get(), l == 0 ? _sellVal.get() : L.val.get(), L.M.get(), f, L.xt.get(), x);
 	}
 	else
 	{
 		YZ_LAUNCH(KPreSmooth, g, kB, 0, _st, Halt(), n, L.M.get(), f, L.xt.get());
-		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, Halt(), n, L.ptr.get(), l == 0 ? _sellOff.get() : nullptr,
+		YZ_LAUNCH(KPostSmooth, g, kB, 0, _st, Halt(), n, L.ptr.get(), l == 0 ? _sellOff.get() : nullptr, StenOf(l),
 		          l == 0 ? _sellCol.get() : L.col.get(), l == 0 ? _sellVal.get() : L.val.get(), L.M.get(), f, L.xt.get(), x);
 	}
 }
@@ -591,20 +637,20 @@ void Solver::Cycle32(size_t l, const TF *f, TX *x)
 	if(l + 1 < _nlev)
 	{
 		Level &C = *_levels[l + 1];
-		YZ_LAUNCH((KPreSmoothResidual<float, TF, float>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, col, val,
+		YZ_LAUNCH((KPreSmoothResidual<float, TF, float>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val,
 		          L.M32.get(), f, L.x32.get(), L.t32.get());
 		YZ_LAUNCH(KRestrict<float>, GridFor((long long)C.n * 4, kB), kB, 0, _st, Halt(), C.n, L.rptr.get(), L.rcol.get(),
 		          L.rval32.get(), L.t32.get(), C.f32.get());
 		Cycle32<float, float>(l + 1, C.f32.get(), C.x32.get());
 		YZ_LAUNCH(KProlong<float>, g, kB, 0, _st, Halt(), n, L.pptr.get(), L.pcol.get(), L.pval32.get(), C.x32.get(),
 		          L.x32.get(), L.xt32.get());
-		YZ_LAUNCH((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, col, val, L.M32.get(), f,
+		YZ_LAUNCH((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val, L.M32.get(), f,
 		          L.xt32.get(), x);
 	}
 	else
 	{
 		YZ_LAUNCH((KPreSmooth<float, TF, float>), g, kB, 0, _st, Halt(), n, L.M32.get(), f, L.xt32.get());
-		YZ_LAUNCH((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, col, val, L.M32.get(), f,
+		YZ_LAUNCH((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val, L.M32.get(), f,
 		          L.xt32.get(), x);
 	}
 }
@@ -689,30 +735,35 @@ void Solver::EnqueueIteration(int kind)
 	double *x = _x.get();
 	YZ_LAUNCH(KPUpdate, g, kB, 0, _st, n, _r.get(), _v.get(), _p.get(), sc);
 	ApplyPrec(kind, _p.get(), _ph.get());
-	YZ_LAUNCH(KSpmvAlpha, nb, kRT, 0, _st, n, ptr, so, col, val, _ph.get(), _rh.get(), _v.get(), Red(1), sc);
+	YZ_LAUNCH(KSpmvAlpha, nb, kRT, 0, _st, n, ptr, so, _sten, col, val, _ph.get(), _rh.get(), _v.get(), Red(1), sc);
 	YZ_LAUNCH(KSUpdate, nb, kRT, 0, _st, n, _r.get(), _v.get(), _s.get(), Red(2), sc);
 	YZ_LAUNCH(KXHalf, g, kB, 0, _st, n, _ph.get(), x, sc);
 	ApplyPrec(kind, _s.get(), _sh.get());
-	YZ_LAUNCH(KSpmvOmega, nb, kRT, 0, _st, n, ptr, so, col, val, _sh.get(), _s.get(), _t.get(), Red(3), sc);
+	YZ_LAUNCH(KSpmvOmega, nb, kRT, 0, _st, n, ptr, so, _sten, col, val, _sh.get(), _s.get(), _t.get(), Red(3), sc);
 	YZ_LAUNCH(KXRUpdate, nb, kRT, 0, _st, n, _ph.get(), _sh.get(), _s.get(), _t.get(), _rh.get(), x, _r.get(),
 	          Red(4), sc);
 }
 
-//  The iterations of one run until its state is set: queued one at a time
-//  with one read of the state after each (the host's test between two
-//  iterations of the oracle is on the device).  With YZ_GRAPH set, one CUDA
-//  graph holds them instead: a while node whose body is one iteration and
-//  whose condition the body's last kernel sets from the state, so the run is
-//  one launch and one read.  Its capture, instantiation and destruction
-//  (0.3-0.5 ms a solve on B200, the hierarchy changing every solve) cost
-//  more than the reads it saves at the iteration counts of the implicit step,
-//  so it is not the default.  A kernel selected for per-launch timing (whose
-//  events a graph cannot carry) always takes the queued path.
+//  The iterations of one run until its state is set, as one CUDA graph
+//  launch and one read of the state, or from the stream with one iteration
+//  kept in flight (the host's test between two iterations of the oracle is
+//  on the device either way).
 void Solver::RunIterations(int kind)
 {
-	static const bool useGraph = std::getenv("YZ_GRAPH") != nullptr;
+	//  The loop runs as a CUDA graph: a conditional while node whose body is
+	//  one iteration, so that the device decides when it ends and the host
+	//  launches nothing per iteration.  The graph is kept while its kernels
+	//  and buffers stay those it was captured with (the same pattern and
+	//  precision and, for the AMG kind, the same hierarchy: a reused one),
+	//  and captured anew otherwise (0.2-0.5 ms, less than the host launches
+	//  it saves on the 512^2 film).  YZ_GRAPH=0, or a kernel being timed:
+	//  the iterations are launched from the stream instead.
+	static const char *env = std::getenv("YZ_GRAPH");
+	static const bool graphOff = env && env[0] == '0';
+	LoopGraph &lg = _loop[kind == kPrecAmg ? 1 : 0];
+	const unsigned long long key = ((unsigned long long)_epoch << 32) | (kind == kPrecAmg ? _epochH : 0u);
 	Scal *sc = _sc.get();
-	if((!useGraph && _amgReuse == 0) || TimingActive())
+	if(graphOff || TimingActive())
 	{
 		//  one iteration kept in flight: the state after iteration k is
 		//  copied to pinned memory and read while iteration k+1 runs; the
@@ -750,27 +801,25 @@ void Solver::RunIterations(int kind)
 		if(timed > 0 && queued > _hsc->it) TimeDropLast(timed / queued * (queued - _hsc->it));
 		return;
 	}
-	//  the graph form: kept (and relaunched) while the hierarchy is reused,
-	//  built for this run alone otherwise
-	LoopGraph &lg = _loop[kind == kPrecAmg ? 1 : 0];
-	if(lg.exec == nullptr || lg.epoch != _epoch)
+	if(lg.exec == nullptr || lg.key != key)
 	{
 		FreeLoopGraph(lg);
 		BuildLoopGraph(kind, lg);
-		lg.epoch = _epoch;
+		lg.key = key;
 	}
 	YZ_CUDA(cudaGraphLaunch(lg.exec, _st));
 	ReadScal();
 	//  the kernels the loop ran
 	g_launches.fetch_add(lg.perBody * (long long)_hsc->bodies);
-	if(_amgReuse == 0) FreeLoopGraph(lg);
 }
 
 void Solver::FreeLoopGraph(LoopGraph &g)
 {
 	if(g.exec) cudaGraphExecDestroy(g.exec);
 	if(g.graph) cudaGraphDestroy(g.graph);
-	g = LoopGraph();
+	g.exec = nullptr;
+	g.graph = nullptr;
+	g.key = ~0ull;
 }
 
 void Solver::BuildLoopGraph(int kind, LoopGraph &lg)
@@ -825,7 +874,7 @@ bool Solver::BiCGStab(int kind, int maxIter, double tol, int &itOut, double &err
 	Level &A = *_levels[0];
 	const int n = _n, nb = RedBlocks(n), g = GridFor(n, kB);
 	double *b = _b.get(), *x = _x.get();
-	YZ_LAUNCH(KBInit, nb, kRT, 0, _st, n, A.ptr.get(), _sellOff.get(), _sellCol.get(), _sellVal.get(), b, x, _r.get(),
+	YZ_LAUNCH(KBInit, nb, kRT, 0, _st, n, A.ptr.get(), _sellOff.get(), _sten, _sellCol.get(), _sellVal.get(), b, x, _r.get(),
 	          _rh.get(), Red(0), _sc.get());
 	ReadScal();
 	const double normB = _hsc->normb;

@@ -81,6 +81,7 @@ private:
 	void BuildHierarchy(int coarseEnough);
 	void DirectInverse(Level &L);
 	void Cycle(size_t l, const double *f, double *x);
+	Sten StenOf(size_t l) const;
 	void RoundCycle();
 	template<class TF, class TX> void Cycle32(size_t l, const TF *f, TX *x);
 	const int *Halt() const { return &_sc.get()->state; }
@@ -94,7 +95,7 @@ private:
 		cudaGraph_t graph = nullptr;
 		cudaGraphExec_t exec = nullptr;
 		long long perBody = 0;
-		unsigned epoch = ~0u;
+		unsigned long long key = ~0ull;       // the pattern/precision and hierarchy it was built for
 	};
 	void BuildLoopGraph(int kind, LoopGraph &g);
 	static void FreeLoopGraph(LoopGraph &g);
@@ -117,6 +118,8 @@ private:
 	DBuf<int> _sellOff, _sellCol;     // the finest level in SELL-32 (slice offsets, columns)
 	DBuf<double> _sellVal;
 	DBuf<float> _sellVal32;           // its FP32 copy, read by the FP32 V-cycle
+	DBuf<unsigned char> _stenSlice;   // the slices whose rows are the stencil's
+	Sten _sten = Sten();
 	size_t _sellSize = 0;
 	int _precision = YZ_PREC_FP64;
 	DBuf<double> _values, _rhs, _xio;
@@ -150,7 +153,9 @@ private:
 	//  hierarchy reuse (0: a new set-up every solve, the reference's way)
 	int _amgReuse = 0, _sinceBuild = 0, _freshIters = 0, _rebuilds = 0;
 	bool _stale = false;
-	unsigned _epoch = 0;          // bumped whenever a pointer or size a graph holds may change
+	//  bumped whenever a pointer or size a loop graph holds may change: the
+	//  pattern, precision or buffers (_epoch), the hierarchy (_epochH)
+	unsigned _epoch = 0, _epochH = 0;
 	LoopGraph _loop[2];
 	double _setupMs = 0, _iterMs = 0;
 	long long _launches = 0;

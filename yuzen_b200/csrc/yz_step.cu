@@ -153,8 +153,11 @@ struct RowOut
 	unsigned long long *rhsMax;
 };
 
+//  three blocks of 128 a SM (168 registers a thread, a few spills) ran the
+//  512^2 all-physics assembly 13 % faster than two (255 registers); four or
+//  five blocks spill more than the occupancy gains
 #ifndef YZ_ASSEMBLE_MIN_BLOCKS
-#define YZ_ASSEMBLE_MIN_BLOCKS 1
+#define YZ_ASSEMBLE_MIN_BLOCKS 3
 #endif
 __global__ void __launch_bounds__(128, YZ_ASSEMBLE_MIN_BLOCKS)
 KAssemble(Coef k, int mode, double dt, const int *__restrict__ rowptr,
