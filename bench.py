@@ -140,11 +140,11 @@ def make_case(name: str, steps: int):
 #  the reference's CPU solver (the reference's sources compiled by
 #  oracle/Makefile with the CPU restatement of its AMGCL backend)
 # ----------------------------------------------------------------------
-def reference_run(name: str, steps: int, threads: int) -> dict:
+def reference_run(name: str, steps: int, threads: int, case=None) -> dict:
     exe = REPO / "oracle" / "_ref" / "yuzen_oracle"
     if not exe.exists():
         return {"unavailable": f"{exe.relative_to(REPO)} is not built (make -C oracle ref)"}
-    cfg = make_case(name, steps)
+    cfg = case if case is not None else make_case(name, steps)
     with tempfile.TemporaryDirectory() as tmp:
         cfg.write_reference(tmp)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads), YUZEN_THREAD_CAP="0", OMP_PROC_BIND="close")
@@ -161,11 +161,51 @@ def reference_run(name: str, steps: int, threads: int) -> dict:
             "threads": threads}
 
 
+def ensemble_reference(a, threads: int) -> dict:
+    """The reference's CPU solver on a bounded sample of the ensemble: the
+    first a.ref_instances instances (one size each where the batch has it),
+    a.steps steps each, one after the other with all host threads."""
+    from yuzen_b200 import cases
+    batch = cases.batch(256, steps=a.steps)
+    seen, sample = set(), []
+    for c in batch:
+        if c.Nx not in seen:
+            seen.add(c.Nx)
+            sample.append(c)
+    sample = sample[:a.ref_instances]
+    loop, steps = 0.0, 0
+    for c in sample:
+        r = reference_run("", a.steps, threads, case=c)
+        if "unavailable" in r:
+            return r
+        loop += r["loop_s"]
+        steps += r["steps"]
+    cells = sum(c.Nx * c.Ny for c in sample)
+    #  instance-steps/s of the sample, scaled to the batch's mean instance
+    mean_cells = sum(c.Nx * c.Ny for c in batch) / len(batch)
+    return {"value": steps / loop * (cells / len(sample)) / mean_cells, "loop_s": loop, "steps": steps,
+            "sample": f"{len(sample)} instances ({', '.join(str(c.Nx) for c in sample)} cells a side), "
+                      f"{a.steps} steps each, scaled by cells to the batch's mean instance"}
+
+
 def run_reference_arm(a) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    if a.config == "batch_256":
+        r = ensemble_reference(a, threads)
+        if "unavailable" in r:
+            print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
+            return
+        print(json.dumps({
+            "impl": "reference", "metric": ENSEMBLE_METRIC, "value": r["value"], "unit": ENSEMBLE_UNIT,
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": {"workload": a.config},
+            "cpu_baseline": {"value": r["value"], "unit": ENSEMBLE_UNIT, "cores": threads, "kind": "reference",
+                             "sample": r["sample"]},
+            "e2e": {"value": r["value"], "unit": ENSEMBLE_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
     r = reference_run(a.config, a.steps, threads)
     if "unavailable" in r:
         print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
@@ -367,6 +407,126 @@ def run_device_arm(a) -> None:
         dist.destroy_process_group()
 
 
+ENSEMBLE_METRIC = "instance-steps/s of the 256-instance dewetting ensemble (64²-256², periodic)"
+ENSEMBLE_UNIT = "instance-steps/s"
+
+
+def run_ensemble_arm(a) -> None:
+    """The batched ensemble (yuzen_b200.ensemble): 256 seeded dewetting
+    instances partitioned over the ranks by cost, each rank advancing its
+    instances concurrently on its GPU; a step is one step of every instance.
+    Timed with CUDA events between device-wide synchronisations (the
+    instances run on streams of their own), the maximum over ranks."""
+    import numpy as np
+    import torch
+
+    import yuzen_b200 as yz
+    from yuzen_b200 import cases, ensemble
+    from yuzen_b200 import step as ys
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    batch = cases.batch(256, steps=a.steps)
+    parts = ensemble.partition([ensemble.instance_cost(c) for c in batch], world)
+    mine = parts[rank]
+    arms = {}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    for name in [x for x in a.arms.split(",") if x]:
+        prec, reuse = ARMS[name]
+        ens = ensemble.Ensemble([batch[k] for k in mine], device=local, precision=prec,
+                                amg_reuse=a.amg_reuse if reuse else 0, workers=a.workers)
+        if a.warmup > 0:
+            ens.advance(a.warmup)
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        total_ms, launches = 0.0, 0
+        for _ in range(a.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            l0 = ys.launch_count()
+            e0.record()
+            ens.advance(1)
+            torch.cuda.synchronize()
+            e1.record()
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            launches += ys.launch_count() - l0
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        max_ms = float(t.item())
+        h = {mine[j]: ensemble.checksum(ens.fields(j)[0]) for j in range(len(mine))}
+        arms[name] = {"value": len(batch) * a.steps / (max_ms / 1e3), "max_ms": max_ms, "launches": launches,
+                      "checksums": ensemble.gather_results(h, world, dist), "ens": ens}
+    names = list(arms)
+    head_name = names[-1]
+    head = arms[head_name]
+    #  end to end through the step's public calls with host buffers: every
+    #  instance's film uploaded from pinned memory, one step, read back
+    ens = head["ens"]
+    pins = []
+    for j in range(len(ens)):
+        nn = ens.steps[j].n
+        hp = torch.empty(nn, dtype=torch.float64, pin_memory=True).numpy()
+        cp = torch.empty(nn, dtype=torch.float64, pin_memory=True).numpy()
+        ens.steps[j].fields_into(hp, cp)
+        pins.append((hp, cp))
+
+    def e2e_one(j):
+        st = ens.steps[j]
+        st.set_fields(*pins[j])
+        st.advance(1)
+        st.fields_into(*pins[j])
+
+    e2e_steps = max(0, min(a.steps, a.e2e_steps))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        list(ens._pool.map(e2e_one, range(len(ens))))
+    e2e_s = max(time.perf_counter() - t0, 1e-9)
+    et = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+    if dist:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    bytes_step = sum(2 * 8 * ens.steps[j].n for j in range(len(ens)))
+    diff = None
+    if "fp64" in arms and head_name != "fp64":
+        a64, ah = arms["fp64"]["checksums"], head["checksums"]
+        diff = max(abs(ah[k] - a64[k]) / max(abs(a64[k]), 1e-300) for k in a64)
+    if rank == 0:
+        line = {
+            "metric": ENSEMBLE_METRIC, "value": head["value"], "unit": ENSEMBLE_UNIT, "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": head["max_ms"] / a.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64" if head_name == "fp64" else "f64 (V-cycle f32)", "data": "synthetic (seeded, cases.batch)",
+            "config": {"workload": a.config, "instances": len(batch), "instances_rank0": len(mine),
+                       "sizes": sorted({c.Nx for c in batch}), "path": PATHS[head_name],
+                       "parallelism": f"instances partitioned over {world} GPUs" if world > 1 else "1 GPU",
+                       "l2": "flushed between steps (256 MiB write)", "workers": ens.workers,
+                       "arms": {k: {"instance_steps_per_s": v["value"], "ms_per_step": v["max_ms"] / a.steps,
+                                    "gpu_launches": v["launches"]} for k, v in arms.items()},
+                       "checksum_rel_diff_vs_fp64": diff},
+            "e2e": {"value": len(batch) * e2e_steps / float(et.item()) if e2e_steps else None, "unit": ENSEMBLE_UNIT,
+                    "h2d_bytes_per_step": bytes_step, "d2h_bytes_per_step": bytes_step, "steps": e2e_steps},
+            "gpu_launches": head["launches"],
+            "roofline": None,
+            "cpu_baseline": None,
+        }
+        print(json.dumps(line))
+    for v in arms.values():
+        v["ens"].close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -382,11 +542,15 @@ def main() -> None:
                          "film is within 1e-8 of the FP64 arm's")
     ap.add_argument("--amg-reuse", type=int, default=16, help="solves an AMG set-up serves in the fp32_reuse arm")
     ap.add_argument("--roofline-steps", type=int, default=3, help="steps over which the roofline kernel is timed")
+    ap.add_argument("--workers", type=int, default=32, help="host threads advancing the ensemble's instances")
+    ap.add_argument("--ref-instances", type=int, default=3, help="ensemble instances the reference arm samples")
     a = ap.parse_args()
     if a.warmup < 3 and a.impl == "b200":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if a.impl == "reference":
         run_reference_arm(a)
+    elif a.config == "batch_256":
+        run_ensemble_arm(a)
     else:
         run_device_arm(a)
 

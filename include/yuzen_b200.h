@@ -90,6 +90,13 @@ int yz_solver_set_precision(yz_solver* s, int precision);
  * The Krylov solve stays FP64 to the same tolerance. */
 int yz_solver_set_amg_reuse(yz_solver* s, int max_solves);
 
+/* The BiCGStab loop as one CUDA graph launch per solve (1, the default) or
+ * launched from the stream with one iteration in flight (0).  A program that
+ * drives several contexts from several host threads while any of them may
+ * allocate device memory sets 0: a graph is captured from the context's
+ * stream, and a capture does not mix with other threads' allocations. */
+int yz_solver_set_graph_loop(yz_solver* s, int on);
+
 /* ILinearSolverBackend::Memory / SetMemory (LinearSolverBackend.h:89-102):
  * the TryBackoff counters.  yz_solver_memory returns the count written. */
 int yz_solver_memory(const yz_solver* s, double* out, int cap);
@@ -237,6 +244,8 @@ int yz_step_destroy(yz_step* st);
 int yz_step_set_precision(yz_step* st, int precision);
 /* AMG hierarchy reuse (yz_solver_set_amg_reuse) for the step's solves. */
 int yz_step_set_amg_reuse(yz_step* st, int max_solves);
+/* The graph form of the step's BiCGStab loops (yz_solver_set_graph_loop). */
+int yz_step_set_graph_loop(yz_step* st, int on);
 /* Advance nsteps time steps (TimeAdvance + the clock advance each). */
 int yz_step_advance(yz_step* st, int nsteps, yz_step_stats* stats);
 /* Fields after the last step (host arrays of nx*ny; null pointers skipped). */

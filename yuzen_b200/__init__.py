@@ -38,7 +38,7 @@ EXPORTED_SYMBOLS = (
     "yz_step_system", "yz_pattern_2d", "yz_step_set_fields", "yz_launch_count",
     "yz_time_kernel", "yz_kernel_time", "yz_dot_noalloc", "yz_dot_noalloc_max",
     "yz_step_conc_pattern", "yz_step_conc_system", "yz_step_set_precision", "yz_solver_set_amg_reuse",
-    "yz_step_set_amg_reuse",
+    "yz_step_set_amg_reuse", "yz_solver_set_graph_loop", "yz_step_set_graph_loop",
 )
 
 #: the preconditioner's arithmetic (YZ_PREC_* of include/yuzen_b200.h)
@@ -83,6 +83,7 @@ def lib():
                                          ctypes.c_void_p, ctypes.c_void_p, _i32p, _f64p]
     L.yz_solver_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_solver_set_amg_reuse.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.yz_solver_set_graph_loop.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_solver_memory.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_int]
     L.yz_solver_set_memory.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_int]
     L.yz_solver_levels.argtypes = [ctypes.c_void_p]
@@ -218,6 +219,11 @@ class B200Backend:
         """0: a new AMG set-up every solve (the reference's way); k > 0: a
         set-up serves up to k further solves (yz_solver_set_amg_reuse)."""
         _check(lib().yz_solver_set_amg_reuse(self._h, max_solves), "yz_solver_set_amg_reuse")
+
+    def SetGraphLoop(self, on: bool) -> None:
+        """The BiCGStab loop as one CUDA graph launch (default) or from the
+        stream (yz_solver_set_graph_loop)."""
+        _check(lib().yz_solver_set_graph_loop(self._h, int(bool(on))), "yz_solver_set_graph_loop")
 
     def Memory(self) -> list:
         buf = np.zeros(8, dtype=np.float64)

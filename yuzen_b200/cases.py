@@ -371,6 +371,30 @@ def spinodal_224(N: int = 224, seed: int = 20261203, steps: int = 12, end_time: 
                 dt_control=True, disjoining=(10.0, 3.0, 2.0), h_init=h, conc0=0.5)
 
 
+def dewetting(N: int, theta_e: float, amp: float, seed: int, steps: int = 12, end_time: float = 0.8) -> Case:
+    """One instance of the batched ensemble: the spinodal film of
+    spinodal_224 on N x N periodic cells of the same size (2.857 um), with
+    contact angle theta_e [deg] and noise h = 1 + amp U(-1, 1) from its seed;
+    capillary + disjoining pressure, adaptive dt."""
+    rng = np.random.default_rng(seed)
+    h = 1.0 + amp * rng.uniform(-1.0, 1.0, size=(N, N))
+    side = 0.64e-3 * N / 224.0
+    return Case(name=f"dewetting_{N}_{seed}", Nx=N, Ny=N, xlim=(-side / 2, side / 2), ylim=(-side / 2, side / 2),
+                h0=1e-6, precursor=0.01, bc=("Periodic",) * 4, dt=1e-4, steps=steps, end_time=end_time,
+                dt_control=True, disjoining=(theta_e, 3.0, 2.0), h_init=h, conc0=0.5)
+
+
+def batch(count: int = 256, seed: int = 20261204, sizes=(64, 96, 128, 192, 256), steps: int = 12) -> list:
+    """The batched ensemble: count seeded dewetting instances, N uniform in
+    sizes, theta_e uniform in [5, 20] deg, noise amplitude log-uniform in
+    [1e-4, 1e-2], periodic edges; instance k is seeded by (seed, k)."""
+    rng = np.random.default_rng(seed)
+    Ns = rng.choice(np.asarray(sizes), size=count)
+    th = rng.uniform(5.0, 20.0, size=count)
+    amp = 10.0 ** rng.uniform(-4.0, -2.0, size=count)
+    return [dewetting(int(Ns[k]), float(th[k]), float(amp[k]), seed=seed * 1000 + k, steps=steps) for k in range(count)]
+
+
 def allphys(N: int = 512, steps: int = 12, dt: float = 1e-5) -> Case:
     """Config 3: every term of the well-mixed model on an N x N film with
     Symmetry edges.  A film edge along a 30 degree oblique tanh front

@@ -94,6 +94,15 @@ int yz_solver_set_amg_reuse(yz_solver *s, int maxSolves)
 	});
 }
 
+int yz_solver_set_graph_loop(yz_solver *s, int on)
+{
+	return Guard([&] {
+		if(!s) throw yz::UsageError("yz_solver_set_graph_loop: null solver");
+		s->s->SetGraphLoop(on != 0);
+		return 0;
+	});
+}
+
 int yz_solver_memory(const yz_solver *s, double *out, int cap)
 {
 	return Guard([&] {
@@ -228,6 +237,15 @@ int yz_step_set_amg_reuse(yz_step *st, int maxSolves)
 	return Guard([&] {
 		if(!st) throw yz::UsageError("yz_step_set_amg_reuse: null step");
 		st->s->SetAmgReuse(maxSolves);
+		return 0;
+	});
+}
+
+int yz_step_set_graph_loop(yz_step *st, int on)
+{
+	return Guard([&] {
+		if(!st) throw yz::UsageError("yz_step_set_graph_loop: null step");
+		st->s->SetGraphLoop(on != 0);
 		return 0;
 	});
 }

@@ -117,18 +117,10 @@ __global__ void KSUpdate(int n, const double *__restrict__ r, const double *__re
 	{
 		const double res = sqrt(tot[0]);
 		sc->res = res;
-		//  converged at the half step: x takes alpha ph (KXHalf) and the
+		//  converged at the half step: x takes alpha ph (in KXRUpdate) and the
 		//  iteration counts
 		if(res <= sc->eps) { sc->state = kConvHalf; sc->it += 1; }
 	}
-}
-
-//  x = x + alpha ph  (the half-step exit)
-__global__ void KXHalf(int n, const double *__restrict__ ph, double *__restrict__ x, const Scal *sc)
-{
-	if(sc->state != kConvHalf) return;
-	const double alpha = sc->alpha;
-	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = x[i] + alpha * ph[i];
 }
 
 //  t = A sh; omega = (t . s) / (t . t)
@@ -153,13 +145,27 @@ __global__ void __launch_bounds__(kRT, 8) KSpmvOmega(int n, const int *__restric
 	if(GridFold<2>(a, sh, rs, tot) && threadIdx.x == 0) sc->omega = tot[1] / tot[0];
 }
 
-//  x = (x + alpha ph) + omega sh; r = s - omega t; res = |r|; next rho = rh . r
+//  x = (x + alpha ph) + omega sh; r = s - omega t; res = |r|; next rho = rh . r.
+//  After a half-step exit (KSUpdate set kConvHalf, the rest of the iteration
+//  did nothing): x = x + alpha ph instead; the iteration's end turns the
+//  state into kConv, so that no later kernel repeats it.
 __global__ void KXRUpdate(int n, const double *__restrict__ ph, const double *__restrict__ shat,
                           const double *__restrict__ s, const double *__restrict__ t,
                           const double *__restrict__ rh, double *__restrict__ x, double *__restrict__ r,
                           RedScratch rs, Scal *sc)
 {
-	if(sc->state != kRun) return;
+	const int state = sc->state;
+	if(state == kConvHalf)
+	{
+		const double alpha = sc->alpha;
+		YZ_CHUNK_LOOP(i)
+		{
+			if(i >= n) break;
+			x[i] = x[i] + alpha * ph[i];
+		}
+		return;
+	}
+	if(state != kRun) return;
 	__shared__ double sh[2 * kRT];
 	const double alpha = sc->alpha, omega = sc->omega;
 	double a[2] = {0.0, 0.0};
@@ -191,7 +197,7 @@ __global__ void KCtlInit(Scal *sc, double eps, int maxIter)
 	sc->eps = eps; sc->maxIter = maxIter; sc->it = 0; sc->state = kRun; sc->bodies = 0;
 }
 
-//  The end of an iteration: a half-step exit, whose x update KXHalf has just
+//  The end of an iteration: a half-step exit, whose x update KXRUpdate has just
 //  made, becomes a plain exit, so that an iteration queued after it makes
 //  no second one; then the loop's condition (another iteration while the
 //  run goes on)
@@ -737,7 +743,6 @@ void Solver::EnqueueIteration(int kind)
 	ApplyPrec(kind, _p.get(), _ph.get());
 	YZ_LAUNCH(KSpmvAlpha, nb, kRT, 0, _st, n, ptr, so, _sten, col, val, _ph.get(), _rh.get(), _v.get(), Red(1), sc);
 	YZ_LAUNCH(KSUpdate, nb, kRT, 0, _st, n, _r.get(), _v.get(), _s.get(), Red(2), sc);
-	YZ_LAUNCH(KXHalf, g, kB, 0, _st, n, _ph.get(), x, sc);
 	ApplyPrec(kind, _s.get(), _sh.get());
 	YZ_LAUNCH(KSpmvOmega, nb, kRT, 0, _st, n, ptr, so, _sten, col, val, _sh.get(), _s.get(), _t.get(), Red(3), sc);
 	YZ_LAUNCH(KXRUpdate, nb, kRT, 0, _st, n, _ph.get(), _sh.get(), _s.get(), _t.get(), _rh.get(), x, _r.get(),
@@ -756,14 +761,15 @@ void Solver::RunIterations(int kind)
 	//  and buffers stay those it was captured with (the same pattern and
 	//  precision and, for the AMG kind, the same hierarchy: a reused one),
 	//  and captured anew otherwise (0.2-0.5 ms, less than the host launches
-	//  it saves on the 512^2 film).  YZ_GRAPH=0, or a kernel being timed:
-	//  the iterations are launched from the stream instead.
+	//  it saves on the 512^2 film).  YZ_GRAPH=0, the context's switch off
+	//  (SetGraphLoop), or a kernel being timed: the iterations are launched
+	//  from the stream instead.
 	static const char *env = std::getenv("YZ_GRAPH");
 	static const bool graphOff = env && env[0] == '0';
 	LoopGraph &lg = _loop[kind == kPrecAmg ? 1 : 0];
 	const unsigned long long key = ((unsigned long long)_epoch << 32) | (kind == kPrecAmg ? _epochH : 0u);
 	Scal *sc = _sc.get();
-	if(graphOff || TimingActive())
+	if(graphOff || !_graphLoop || TimingActive())
 	{
 		//  one iteration kept in flight: the state after iteration k is
 		//  copied to pinned memory and read while iteration k+1 runs; the

@@ -72,6 +72,7 @@ public:
 	void SetPrecision(int precision);
 	int Precision() const { return _precision; }
 	void SetAmgReuse(int maxSolves);
+	void SetGraphLoop(bool on) { _graphLoop = on; }
 	int Rebuilds() const { return _rebuilds; }
 	cudaStream_t Stream() const { return _st; }
 	int Rows() const { return _n; }
@@ -157,6 +158,7 @@ private:
 	//  pattern, precision or buffers (_epoch), the hierarchy (_epochH)
 	unsigned _epoch = 0, _epochH = 0;
 	LoopGraph _loop[2];
+	bool _graphLoop = true;       // the loop as a CUDA graph (else from the stream)
 	double _setupMs = 0, _iterMs = 0;
 	long long _launches = 0;
 };

@@ -1138,6 +1138,7 @@ void Step::BuildConc()
 	_solverC.reset(new Solver(_device, _st));
 	_solverC->SetPrecision(_precision);
 	_solverC->SetAmgReuse(_amgReuse);
+	_solverC->SetGraphLoop(_graphLoop);
 	_solverC->SetPattern(_n, _nnzC, _rowptrC.data(), scol.data(), ssrc.data());
 	_dRowptrC.upload(_rowptrC.data(), _rowptrC.size(), _st);
 	std::vector<int> pall(n);

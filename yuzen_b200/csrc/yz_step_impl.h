@@ -32,6 +32,12 @@ public:
 		if(_solverC) _solverC->SetPrecision(precision);
 		_precision = precision;
 	}
+	void SetGraphLoop(bool on)
+	{
+		_solver->SetGraphLoop(on);
+		if(_solverC) _solverC->SetGraphLoop(on);
+		_graphLoop = on;
+	}
 	void SetAmgReuse(int maxSolves)
 	{
 		_solver->SetAmgReuse(maxSolves);
@@ -88,6 +94,7 @@ private:
 	phys::ConcCoef _kc;
 	std::unique_ptr<Solver> _solverC;
 	int _precision = YZ_PREC_FP64, _amgReuse = 0;
+	bool _graphLoop = true;
 	int _nnzC = 0;
 	std::vector<int> _rowptrC, _colC;
 	DBuf<int> _dRowptrC, _dPartnerAll;

@@ -111,6 +111,7 @@ def _bind():
     L.yz_step_advance.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(StepStats)]
     L.yz_step_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_step_set_amg_reuse.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.yz_step_set_graph_loop.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_step_get_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
     L.yz_step_set_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
     L.yz_launch_count.restype = ctypes.c_longlong
@@ -149,6 +150,11 @@ class Step:
         solve, the reference's way; k > 0: a set-up serves up to k further
         solves)."""
         _check(lib().yz_step_set_amg_reuse(self._h, max_solves), "yz_step_set_amg_reuse")
+
+    def set_graph_loop(self, on: bool) -> None:
+        """The step's BiCGStab loops as CUDA graph launches (default) or
+        from the stream (yz_step_set_graph_loop)."""
+        _check(lib().yz_step_set_graph_loop(self._h, int(bool(on))), "yz_step_set_graph_loop")
 
     def advance(self, nsteps: int = 1) -> dict:
         st = StepStats()
