@@ -540,7 +540,7 @@ def main() -> None:
     ap.add_argument("--arms", default="fp64,fp32_cycle,fp32_reuse",
                     help="the arms timed, in order (fp64, fp32_cycle, fp32_reuse); headline: the last one whose "
                          "film is within 1e-8 of the FP64 arm's")
-    ap.add_argument("--amg-reuse", type=int, default=16, help="solves an AMG set-up serves in the fp32_reuse arm")
+    ap.add_argument("--amg-reuse", type=int, default=64, help="solves an AMG set-up serves in the fp32_reuse arm")
     ap.add_argument("--roofline-steps", type=int, default=3, help="steps over which the roofline kernel is timed")
     ap.add_argument("--workers", type=int, default=32, help="host threads advancing the ensemble's instances")
     ap.add_argument("--ref-instances", type=int, default=3, help="ensemble instances the reference arm samples")

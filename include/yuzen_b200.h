@@ -246,6 +246,11 @@ int yz_step_set_precision(yz_step* st, int precision);
 int yz_step_set_amg_reuse(yz_step* st, int max_solves);
 /* The graph form of the step's BiCGStab loops (yz_solver_set_graph_loop). */
 int yz_step_set_graph_loop(yz_step* st, int on);
+/* The energy budget of the film the step holds (WellMixed_ModelBase::EnergyEval,
+ * WellMixedModelBase.h:883-893, after EnergyBudget.h): the free energy F and
+ * the flux power D (HeightEquationBase::FluxPower), both times the cell
+ * measure. */
+int yz_step_energy(yz_step* st, double* F, double* D);
 /* Advance nsteps time steps (TimeAdvance + the clock advance each). */
 int yz_step_advance(yz_step* st, int nsteps, yz_step_stats* stats);
 /* Fields after the last step (host arrays of nx*ny; null pointers skipped). */

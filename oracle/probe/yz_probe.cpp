@@ -171,14 +171,21 @@ int main(int argc, char **argv)
 		ccol.assign(Ac.ColIndData(), Ac.ColIndData() + Ac.NonZero());
 	}
 
+	//  the energy budget (WellMixed_ModelBase::EnergyEval) of the film the
+	//  step starts from and of the one it ends on
+	m->EnergyEval();
+	const double enF0 = m->_enF, enD0 = m->_enD;
 	auto t0 = std::chrono::steady_clock::now();
 	m->Run();
 	auto t1 = std::chrono::steady_clock::now();
+	m->EnergyEval();
+	const double enF1 = m->_enF, enD1 = m->_enD;
 	solver.Finalize();
 	std::vector<double> h1, c1, s1;
 	Fields(m, h1, c1, s1);
 	put(D, std::chrono::duration<double>(t1 - t0).count());
 	put(D, m->_timeStep.NowTime());
+	put(D, enF0); put(D, enD0); put(D, enF1); put(D, enD1);
 	put(I, (int)m->_timeStep.TimeStep());
 	put(I, m->Diverged() ? 1 : 0);
 

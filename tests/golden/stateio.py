@@ -28,6 +28,8 @@ REAL_KEYS = (
     "xmin", "ymin", "rot_x", "rot_y", "lin_c_eps", "theta_c",
     # appended after the run
     "run_seconds", "t_end",
+    # the energy budget (EnergyEval) of the start and the end film
+    "energy_F0", "energy_D0", "energy_F1", "energy_D1",
 )
 #  BoundaryCondition::tBoundaryCondition (model/BoundaryCondition.h)
 BC_NAMES = {0: "Symmetry", 1: "Periodic", 2: "Pinning", 3: "FreshInlet", 4: "Outlet"}

@@ -250,6 +250,15 @@ int yz_step_set_graph_loop(yz_step *st, int on)
 	});
 }
 
+int yz_step_energy(yz_step *st, double *F, double *D)
+{
+	return Guard([&] {
+		if(!st || !F || !D) throw yz::UsageError("yz_step_energy: null argument");
+		st->s->Energy(*F, *D);
+		return 0;
+	});
+}
+
 int yz_step_advance(yz_step *st, int nsteps, yz_step_stats *stats)
 {
 	return Guard([&] {

@@ -138,6 +138,36 @@ __device__ __forceinline__ void FaceOf(int d, int i, int nx, const FaceBuf &fb, 
 }
 
 //--------------------------------------------------------------------------
+//  The limited upwind terms' faces (UpwindFaces in yz_upwind.cuh): one
+//  thread a cell, its high x and y faces where a row needs them
+//--------------------------------------------------------------------------
+template<bool J>
+__global__ void KUpwindFaces(Coef k, const double *__restrict__ H, const double *__restrict__ C, FaceBuf fb,
+                             UpBuf up)
+{
+	const int nx = k.nx, ny = k.ny;
+	const long long n = (long long)nx * ny;
+	for(long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x)
+	{
+		const int ix = (int)(j % nx), iy = (int)(j / nx);
+#pragma unroll
+		for(int a = 0; a < 2; ++a)
+		{
+			const bool in = (a == 0) ? (ix >= 1 && ix <= nx - 3 && iy >= 2 && iy <= ny - 3)
+			                         : (iy >= 1 && iy <= ny - 3 && ix >= 2 && ix <= nx - 3);
+			if(!in) continue;
+			const long long s = (a == 0) ? 1 : nx;
+			const double f[4] = {H[j - s], H[j], H[j + s], H[j + 2 * s]};
+			const double vis = (a == 0) ? fb.x.vis[j] : fb.y.vis[j];
+			const bool wall = WallFaceLow(k, a, ix, iy);
+			if(k.onPG) BodyForceFace<kPG, J>(k, f, vis, a, ix, iy, wall, up, j);
+			if(k.onCF) BodyForceFace<kCF, J>(k, f, vis, a, ix, iy, wall, up, j);
+			if(k.onSC) MarangoniFace<J>(k, f, C[j], C[j + s], vis, a, wall, up, j);
+		}
+	}
+}
+
+//--------------------------------------------------------------------------
 //  One interior row: the A entries of every term, then what the caller
 //  asks for: mode 0 -> A(h) h only (the explicit half and evapOld);
 //  mode 1 -> I + theta dt J, A(h) h, B and the right-hand side.
@@ -162,7 +192,7 @@ struct RowOut
 __global__ void __launch_bounds__(128, YZ_ASSEMBLE_MIN_BLOCKS)
 KAssemble(Coef k, int mode, double dt, const int *__restrict__ rowptr,
                           const double *__restrict__ H, const double *__restrict__ C,
-                          const double *__restrict__ S, RowOut o, FaceBuf fb)
+                          const double *__restrict__ S, RowOut o, FaceBuf fb, UpBuf up)
 {
 	const int nx = k.nx, ny = k.ny;
 	const int nIn = (nx - 4) * (ny - 4);
@@ -259,9 +289,9 @@ KAssemble(Coef k, int mode, double dt, const int *__restrict__ rowptr,
 		}
 		//  --- the upwinded terms into A_rest, in the order of the physics list
 		//  (HeightEquationBase.h:565-577): in-plane gravity, Marangoni, rotation
-		if(k.onPG) BodyForceA<kPG>(k, h, vis, ix, iy, aR);
-		if(k.onSC) MarangoniA(k, h, c, vis, ix, iy, aR);
-		if(k.onCF) BodyForceA<kCF>(k, h, vis, ix, iy, aR);
+		if(k.onPG) BodyForceAF<kPG>(k, up, i, aR);
+		if(k.onSC) MarangoniAF(k, up, i, aR);
+		if(k.onCF) BodyForceAF<kCF>(k, up, i, aR);
 		//  --- DisjoiningPressureKernel::SetMatrixA (DisjoiningPressureKernel.h:306-349).
 		//  Pi, Pi/h and dPi of the five narrow points from one pair of pow
 		//  calls each: the same values the reference's three functions give
@@ -421,9 +451,9 @@ KAssemble(Coef k, int mode, double dt, const int *__restrict__ rowptr,
 				}
 			}
 		}
-		if(k.onPG) BodyForceJ<kPG>(k, h, vis, ix, iy, J);
-		if(k.onSC) MarangoniJ(k, h, c, vis, ix, iy, J);
-		if(k.onCF) BodyForceJ<kCF>(k, h, vis, ix, iy, J);
+		if(k.onPG) BodyForceJF<kPG>(k, up, i, J);
+		if(k.onSC) MarangoniJF(k, up, i, J);
+		if(k.onCF) BodyForceJF<kCF>(k, up, i, J);
 		if(k.onD)
 		{
 			double Ad[4], gAdj[4], gCen[4];
@@ -477,6 +507,88 @@ KAssemble(Coef k, int mode, double dt, const int *__restrict__ rowptr,
 		rmax = fmax(rmax, fabs(r));
 	}
 	if(mode == 1) WarpMaxAbs(o.rhsMax, rmax);
+}
+
+//--------------------------------------------------------------------------
+//  The energy budget (EnergyBudget.h; WellMixedModelBase.h:883-893): the
+//  free energy F = sum over the real cells of Bo/2 f^2 + Dp w(h) plus the
+//  capillary energy of the cell's high faces (and of its low faces on an
+//  edge that is not periodic), f = h + s, times dx dy; and the flux power
+//  D = sum over the real cells of phi (-div F) times dx dy
+//  (HeightEquationBase::FluxPower with no side rate in 2-D), phi the
+//  driving potential (LubFields.cpp:278-289) and F the face volume fluxes of
+//  the film (FaceVolumeFluxes, KFaceFlux).  One element a thread over the
+//  real cells, both sums by the fixed reduction tree.
+//--------------------------------------------------------------------------
+struct EnergyPar
+{
+	double bo, dp, hstar, pn, pm;
+	int capillary, perX, perY;
+};
+
+//  w(h) = -int_{h*}^{h} Pi(s) ds (EnergyBudget.h:59-67)
+__device__ __forceinline__ double EnergyW(const EnergyPar &e, double h)
+{
+	if(e.dp == 0 || !(h > 0)) return 0;
+	const double hs = e.hstar, n = e.pn, m = e.pm;
+	const double in = pow(hs, n) * (pow(h, 1.0 - n) - pow(hs, 1.0 - n)) / (1.0 - n);
+	const double im = pow(hs, m) * (pow(h, 1.0 - m) - pow(hs, 1.0 - m)) / (1.0 - m);
+	return -e.dp * (in - im);
+}
+
+__device__ __forceinline__ double EnergyFace(const Coef &k, const EnergyPar &e, double fi, double fj, double ci,
+                                             double cj, double dn)
+{
+	if(!e.capillary) return 0;
+	const double g = (fj - fi) / dn;
+	return 0.25 * (SurfaceTension(k, ci) + SurfaceTension(k, cj)) * g * g;
+}
+
+__global__ void KEnergy(Coef k, EnergyPar e, const double *__restrict__ H, const double *__restrict__ C,
+                        const double *__restrict__ S, const double *__restrict__ Fx, const double *__restrict__ Fy,
+                        RedScratch rs, double *__restrict__ out)
+{
+	__shared__ double sh[2 * kRT];
+	const int nx = k.nx, ny = k.ny;
+	const int nIn = (nx - 4) * (ny - 4);
+	const double dx2 = k.dx * k.dx, dy2 = k.dy * k.dy;
+	double a[2] = {0.0, 0.0};
+	for(int kk = 0, t = blockIdx.x * kRChunk + threadIdx.x; kk < kRK; ++kk, t += kRT)
+	{
+		if(t >= nIn) break;
+		const int ix = 2 + t % (nx - 4), iy = 2 + t / (nx - 4);
+		const int i = iy * nx + ix;
+		const double h = H[i], c = C[i], v = H[i] + S[i];
+		const double vxp = H[i + 1] + S[i + 1], vxm = H[i - 1] + S[i - 1];
+		const double vyp = H[i + nx] + S[i + nx], vym = H[i - nx] + S[i - nx];
+		//  FreeEnergy: the cell, its high faces, its low faces at a wall
+		double f = 0.5 * e.bo * v * v + EnergyW(e, h);
+		f = f + EnergyFace(k, e, v, vxp, c, C[i + 1], k.dx);
+		f = f + EnergyFace(k, e, v, vyp, c, C[i + nx], k.dy);
+		if(!e.perX && ix == 2) f = f + EnergyFace(k, e, vxm, v, C[i - 1], c, k.dx);
+		if(!e.perY && iy == 2) f = f + EnergyFace(k, e, vym, v, C[i - nx], c, k.dy);
+		//  Potential (PotentialAt) and FluxPower
+		const double lap = (vxp - 2.0 * v + vxm) / dx2 + (vyp - 2.0 * v + vym) / dy2;
+		double phi = 0;
+		if(e.capillary) phi += SurfaceTension(k, c) * lap;
+		if(e.dp != 0 && h > 0)
+		{
+			const double r = e.hstar / h;
+			phi += e.dp * (pow(r, e.pn) - pow(r, e.pm));
+		}
+		if(e.bo != 0) phi -= e.bo * v;
+		double div = 0;
+		div += Fx[i] - Fx[i - 1];
+		div += Fy[i] - Fy[i - nx];
+		a[0] = a[0] + f;
+		a[1] = a[1] + phi * (-div - 0.0);
+	}
+	double tot[2];
+	if(GridFold<2>(a, sh, rs, tot) && threadIdx.x == 0)
+	{
+		out[0] = tot[0] * k.dx * k.dy;
+		out[1] = tot[1] * (k.dx * k.dy);
+	}
 }
 
 //  ghost rows of x satisfied exactly (CRS_Matrix::SatisfyBCRows for rows
@@ -803,13 +915,22 @@ void Step::FaceProps(const double *H, const double *C, bool J)
 void Step::Assemble(int mode, const double *hField, const double *cField, double dt)
 {
 	FaceProps(hField, cField, mode == 1);
+	UpBuf up;
+	up.base = nullptr; up.stride = _n;
+	if(_k.onPG || _k.onCF || _k.onSC)
+	{
+		_upMem.reserve((size_t)48 * _n);
+		up.base = _upMem.get();
+		if(mode == 1) YZ_LAUNCH(KUpwindFaces<true>, GridFor(_n, 128, 148 * 32), 128, 0, _st, _k, hField, cField, _fb, up);
+		else YZ_LAUNCH(KUpwindFaces<false>, GridFor(_n, 128, 148 * 32), 128, 0, _st, _k, hField, cField, _fb, up);
+	}
 	RowOut o;
 	o.ia = _ia.get(); o.ax = mode == 0 ? _axOld.get() : _axGuess.get();
 	o.evapOld = _evapOld.get(); o.evapB = _evapB.get(); o.rhs = _rhs.get();
 	o.hOld = _hOld.get(); o.axOld = _axOld.get(); o.rhsMax = _red.get() + kSlotRhs;
 	const int nIn = (_p.nx - 4) * (_p.ny - 4);
 	YZ_LAUNCH(KAssemble, GridFor(nIn, 128, 148 * 32), 128, 0, _st, _k, mode, dt, _dRowptr.get(), hField, cField,
-	          _s.get(), o, _fb);
+	          _s.get(), o, _fb, up);
 }
 
 //  one Newton-Kantorovich attempt at the present dt (NKLoop)
@@ -1056,6 +1177,26 @@ void Step::SetFields(const double *h, const double *c)
 		//  C_ImplicitSolver::SetX of the concentration equation
 		if(_conc) YZ_CUDA(cudaMemcpyAsync(_c0.get(), _c.get(), bytes, cudaMemcpyDeviceToDevice, _st));
 	}
+}
+
+void Step::Energy(double &F, double &D)
+{
+	YZ_CUDA(cudaSetDevice(_device));
+	const int nIn = (_p.nx - 4) * (_p.ny - 4);
+	_enFx.reserve((size_t)_n); _enFy.reserve((size_t)_n); _enOut.reserve(2);
+	FaceFluxes(_h.get(), _c.get(), _enFx.get(), _enFy.get(), 0.0, false);
+	EnergyPar e;
+	e.bo = _p.Bo; e.dp = _p.Dp; e.hstar = _p.hstar; e.pn = _p.disj_n; e.pm = _p.disj_m;
+	e.capillary = _p.on_laplace ? 1 : 0;
+	e.perX = _p.bc[0] == YZ_BC_PERIODIC ? 1 : 0;
+	e.perY = _p.bc[2] == YZ_BC_PERIODIC ? 1 : 0;
+	YZ_LAUNCH(KEnergy, RedBlocks(nIn), kRT, 0, _st, _k, e, _h.get(), _c.get(), _s.get(), _enFx.get(), _enFy.get(),
+	          StepRed(2), _enOut.get());
+	double out[2];
+	YZ_CUDA(cudaMemcpyAsync(out, _enOut.get(), sizeof out, cudaMemcpyDeviceToHost, _st));
+	YZ_CUDA(cudaStreamSynchronize(_st));
+	F = out[0];
+	D = out[1];
 }
 
 void Step::GetFields(double *h, double *c)

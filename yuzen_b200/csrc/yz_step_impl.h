@@ -20,6 +20,7 @@ public:
 	~Step();
 	void Advance(int nsteps, yz_step_stats &stats);
 	void GetFields(double *h, double *c);
+	void Energy(double &F, double &D);
 	void SetFields(const double *h, const double *c);
 	int Pattern(int *rowptr, int *col, int *bc) const;
 	void System(const double *hOld, const double *h, double dt, double *ia, double *rhs);
@@ -83,6 +84,8 @@ private:
 	DBuf<double> _h, _c, _s, _hOld, _hOld2, _hNew, _guess, _axOld, _axGuess, _rhs, _delta, _evapOld, _evapB, _ia;
 	DBuf<unsigned long long> _red;
 	DBuf<double> _faceMem;
+	DBuf<double> _enFx, _enFy, _enOut;       // the energy budget's face fluxes and its two sums
+	DBuf<double> _upMem;                     // the limited upwind terms' faces (UpBuf)
 	phys::FaceBuf _fb;
 	//  the concentration equation: its pattern and solver; c0 (its phi_old),
 	//  the working field's c, the limiter state, the c of the last pass,

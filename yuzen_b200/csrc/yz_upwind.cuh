@@ -63,6 +63,26 @@ __device__ __forceinline__ double Mag(const Coef &k, int a) { return T == kPG ? 
 //  BodyForceKernel::LimitedFace: the face value hf, the weights wt / dx,
 //  D = h_f^2 / mu (slip: Upwind(h_f) / mu), 0 on a wall face; with g, also
 //  dh_f/dh_q / dx
+//  LimitedFace on the face's own values: f its four films (LL, L, R, RR),
+//  dv its drive, hs its spacing, wall whether it is a wall face
+template<bool DER>
+__device__ __forceinline__ void LimitedFaceF(const Coef &k, const double f[4], double vis, double dv, double hs,
+                                             bool wall, double &hf, double &D, double wt[4], double g[4])
+{
+	if(DER)
+	{
+		hf = FaceDerivative(k.hI, f, dv, g);
+#pragma unroll
+		for(int q = 0; q < 4; ++q) g[q] /= hs;
+	}
+	else hf = FaceValue(k.hI, f, dv);
+	FaceWeights(k.hI, f, dv, -1, wt);
+#pragma unroll
+	for(int q = 0; q < 4; ++q) wt[q] /= hs;
+	D = (k.slip ? MobDperH(k, hf) : hf * hf) / vis;
+	if(wall) D = 0;
+}
+
 template<int T, bool DER>
 __device__ __forceinline__ void LimitedFace(const Coef &k, const double *h, double vis, int d, int ix, int iy,
                                             double &hf, double &D, double wt[4], double g[4])
@@ -86,74 +106,6 @@ __device__ __forceinline__ void LimitedFace(const Coef &k, const double *h, doub
 	if(WallFace(k, d, ix, iy)) D = 0;
 }
 
-//  SetMatrixA_Limited (BodyForceKernel.h:595-633) into the row's A_rest
-template<int T>
-__device__ __forceinline__ void BodyForceA(const Coef &k, const double *h, const double *vis, int ix, int iy,
-                                           double *aR)
-{
-	double wt[4][4], D[4], w[4];
-#pragma unroll
-	for(int j = 0; j < 4; ++j)
-	{
-		double hf;
-		LimitedFace<T, false>(k, h, vis[j], j, ix, iy, hf, D[j], wt[j], nullptr);
-		w[j] = Weight<T>(k, j, ix, iy);
-	}
-#pragma unroll
-	for(int a = 0; a < 2; ++a)
-	{
-		const int dm = 2 * a, dp = 2 * a + 1;
-		const double Coef_ = Mag<T>(k, a);
-#pragma unroll
-		for(int q = 0; q < 5; ++q)
-		{
-			const int idx = AS(a, q);
-			const double Wm = (q < 4) ? wt[dm][q] : 0.0;
-			const double Wp = (q > 0) ? wt[dp][q - 1] : 0.0;
-			const double val = -w[dm] * Wm * D[dm] + w[dp] * Wp * D[dp];
-			aR[idx] += Coef_ * val;
-		}
-	}
-}
-
-//  SetJacobiMatrix_Limited (BodyForceKernel.h:635-691)
-template<int T>
-__device__ __forceinline__ void BodyForceJ(const Coef &k, const double *h, const double *vis, int ix, int iy,
-                                           double *J)
-{
-	double X[4][4];
-#pragma unroll
-	for(int j = 0; j < 4; ++j)
-	{
-		double hf, D, wt[4], g[4];
-		LimitedFace<T, true>(k, h, vis[j], j, ix, iy, hf, D, wt, g);
-		double r3 = 3.0;
-		if(k.slip)
-		{
-			const double up = MobDperH(k, hf);
-			r3 = (up != 0.0) ? MobdD(k, hf) / up : 0.0;
-		}
-		const double sg = (j % 2 == 0) ? -1.0 : +1.0;
-		const double w = Weight<T>(k, j, ix, iy);
-#pragma unroll
-		for(int q = 0; q < 4; ++q) X[j][q] = sg * w * (r3 * g[q] - wt[q]) * D;
-	}
-#pragma unroll
-	for(int a = 0; a < 2; ++a)
-	{
-		const int dm = 2 * a, dp = 2 * a + 1;
-		const double Coef_ = Mag<T>(k, a);
-#pragma unroll
-		for(int q = 0; q < 5; ++q)
-		{
-			const int idx = AS(a, q);
-			const double xm = (q < 4) ? X[dm][q] : 0.0;
-			const double xp = (q > 0) ? X[dp][q - 1] : 0.0;
-			J[idx] += Coef_ * (xm + xp);
-		}
-	}
-}
-
 //  BodyForceKernel::FaceFlux, limited: Mag w (sum_q wt_q h_q) D through face d
 template<int T>
 __device__ __forceinline__ double BodyForceFlux(const Coef &k, const double *h, double vis, int d, int ix, int iy)
@@ -174,97 +126,6 @@ __device__ __forceinline__ double FaceDc(const Coef &k, const double *c, int d)
 	return (c[FS(d, 2)] - c[FS(d, 1)]) / hsp;
 }
 
-//  SolutoCapillarityKernel::SetMatrixA_Limited into the row's A_rest
-__device__ __forceinline__ void MarangoniA(const Coef &k, const double *h, const double *c, const double *vis, int ix,
-                                           int iy, double *aR)
-{
-	double Val[13];
-#pragma unroll
-	for(int q = 0; q < 13; ++q) Val[q] = 0;
-#pragma unroll
-	for(int d = 0; d < 4; ++d)
-	{
-		const double dc = FaceDc(k, c, d);
-		double f[4], wt[4];
-#pragma unroll
-		for(int q = 0; q < 4; ++q) f[q] = h[FS(d, q)];
-		const double up = MSign(k.scMag) * MSign(dc);
-		const double hf = FaceValue(k.hI, f, up);
-		FaceWeights(k.hI, f, up, -1, wt);
-		const double S = WallFace(k, d, ix, iy) ? 0.0 : (k.slip ? dc / vis[d] * (hf + 2.0 * k.lam) : dc / vis[d] * hf);
-		const double hsp = (d < 2) ? k.dxx : k.dyy;
-		const double sg = (d % 2 == 0) ? -1.0 : +1.0;
-#pragma unroll
-		for(int q = 0; q < 4; ++q) Val[FS(d, q)] += sg * wt[q] * S / hsp;
-	}
-#pragma unroll
-	for(int kk = 0; kk < 9; ++kk) aR[WI(kk)] += k.scMag * Val[WI(kk)];
-}
-
-//  SolutoCapillarityKernel::SetJacobiMatrix_Limited with ScatterJacobiWide
-__device__ __forceinline__ void MarangoniJ(const Coef &k, const double *h, const double *c, const double *vis, int ix,
-                                           int iy, double *J)
-{
-	double a[4], g[4][4];
-#pragma unroll
-	for(int d = 0; d < 4; ++d)
-	{
-		const double dc = FaceDc(k, c, d);
-		double f[4], wt[4], gd[4];
-#pragma unroll
-		for(int q = 0; q < 4; ++q) f[q] = h[FS(d, q)];
-		const double up = MSign(k.scMag) * MSign(dc);
-		const double hf = FaceDerivative(k.hI, f, up, gd);
-		FaceWeights(k.hI, f, up, -1, wt);
-		const double r = WallFace(k, d, ix, iy) ? 0.0 : dc / vis[d];
-		const double hsp = (d < 2) ? k.dxx : k.dyy;
-		const double sg = (d % 2 == 0) ? -1.0 : +1.0;
-		if(k.slip)
-		{
-			const double L2 = 2.0 * k.lam;
-			a[d] = sg / hsp;
-#pragma unroll
-			for(int q = 0; q < 4; ++q) g[d][q] = r * ((2.0 * hf + L2) * gd[q] - (hf + L2) * wt[q]);
-		}
-		else
-		{
-			a[d] = sg * hf / hsp;
-#pragma unroll
-			for(int q = 0; q < 4; ++q) g[d][q] = r * (2.0 * gd[q] - wt[q]);
-		}
-	}
-	//  ScatterJacobiWide: the diagonal over the directions in stencil order;
-	//  another point: the direction that has it as its neighbour first, the
-	//  rest in axis order
-#pragma unroll
-	for(int kk = 0; kk < 9; ++kk)
-	{
-		const int idx = WI(kk);
-		double val = 0;
-		if(idx == oo)
-		{
-#pragma unroll
-			for(int j = 0; j < 4; ++j)
-			{
-				const int d = StencilDirC(j);
-				val += g[d][QOf(d, oo)] * a[d];
-			}
-		}
-		else
-		{
-			const int first = DirOfAdjC(idx);
-			if(first >= 0) val += g[first][QOf(first, idx)] * a[first];
-#pragma unroll
-			for(int d = 0; d < 4; ++d)
-			{
-				if(d == first || QOf(d, idx) < 0) continue;
-				val += g[d][QOf(d, idx)] * a[d];
-			}
-		}
-		J[idx] += k.scMag * val;
-	}
-}
-
 //  SolutoCapillarityKernel::FaceFlux, limited: Mag S (sum_q wt_q f_q) / dx
 __device__ __forceinline__ double MarangoniFlux(const Coef &k, const double *h, const double *c, double vis, int d,
                                                 int ix, int iy)
@@ -282,6 +143,230 @@ __device__ __forceinline__ double MarangoniFlux(const Coef &k, const double *h, 
 #pragma unroll
 	for(int q = 0; q < 4; ++q) hs += wt[q] * f[q];
 	return k.scMag * (S * hs / hsp);
+}
+
+//==========================================================================
+//  The limited upwind terms face by face.  Every quantity the rows take from
+//  a face (its limited value, weights and derivatives, D, the drive and
+//  weight, Marangoni's S and dc) depends on the face alone, and every face is
+//  shared by two rows, whose A and J both need it: UpwindFaces evaluates
+//  each face once (its high face for every cell that has one a row needs)
+//  and stores the products the rows add, up to a sign that is the row's
+//  side of the face.  The row kernels then add them in the same order as
+//  BodyForceA/J and MarangoniA/J; negating a product is exact, so the sums
+//  are those of the per-row evaluation (to the sign of a zero).
+//
+//  UpBuf: kind (0 A, 1 J) x axis x term (kPG, kCF, Marangoni) x q arrays of
+//  n doubles, indexed by the face's low cell.
+//==========================================================================
+enum { kUpSC = 2 };
+struct UpBuf
+{
+	double *base;
+	long long stride;
+	__device__ __forceinline__ double *at(int kind, int axis, int term, int q) const
+	{
+		return base + (long long)(((kind * 2 + axis) * 3 + term) * 4 + q) * stride;
+	}
+};
+
+//  WallFace of the face whose low cell is (ix, iy) on axis a: the low wall
+//  face of the first interior cell or the high one of the last
+__device__ __forceinline__ bool WallFaceLow(const Coef &k, int a, int ix, int iy)
+{
+	if(a == 0) return (ix == 1 && k.wall[0]) || (ix == k.nx - 3 && k.wall[1]);
+	return (iy == 1 && k.wall[2]) || (iy == k.ny - 3 && k.wall[3]);
+}
+
+//  one face of a body force: A's w wt_q D, J's w (r3 g_q - wt_q) D (the
+//  face seen as the high face d = 2a + 1 of its low cell)
+template<int T, bool J>
+__device__ __forceinline__ void BodyForceFace(const Coef &k, const double f[4], double vis, int a, int ix, int iy,
+                                              bool wall, const UpBuf &up, long long j)
+{
+	const int d = 2 * a + 1;
+	const double dv = DriveFace<T>(k, d, ix, iy);
+	const double hs = (d < 2) ? k.dxx : k.dyy;
+	const double w = Weight<T>(k, d, ix, iy);
+	const int term = (T == kPG) ? 0 : 1;
+	double hf, D, wt[4], g[4];
+	LimitedFaceF<false>(k, f, vis, dv, hs, wall, hf, D, wt, nullptr);
+#pragma unroll
+	for(int q = 0; q < 4; ++q) up.at(0, a, term, q)[j] = w * wt[q] * D;
+	if(J)
+	{
+		LimitedFaceF<true>(k, f, vis, dv, hs, wall, hf, D, wt, g);
+		double r3 = 3.0;
+		if(k.slip)
+		{
+			const double upd = MobDperH(k, hf);
+			r3 = (upd != 0.0) ? MobdD(k, hf) / upd : 0.0;
+		}
+#pragma unroll
+		for(int q = 0; q < 4; ++q) up.at(1, a, term, q)[j] = w * (r3 * g[q] - wt[q]) * D;
+	}
+}
+
+//  one face of the Marangoni term: A's wt_q S / hsp, J's g_q a' with
+//  a' = 1 / hsp (slip) or hf / hsp
+template<bool J>
+__device__ __forceinline__ void MarangoniFace(const Coef &k, const double f[4], double cl, double cr, double vis,
+                                              int a, bool wall, const UpBuf &up, long long j)
+{
+	const double hsp = (a == 0) ? k.dxx : k.dyy;
+	const double dc = (cr - cl) / hsp;
+	const double upw = MSign(k.scMag) * MSign(dc);
+	{
+		double wt[4];
+		const double hf = FaceValue(k.hI, f, upw);
+		FaceWeights(k.hI, f, upw, -1, wt);
+		const double S = wall ? 0.0 : (k.slip ? dc / vis * (hf + 2.0 * k.lam) : dc / vis * hf);
+#pragma unroll
+		for(int q = 0; q < 4; ++q) up.at(0, a, kUpSC, q)[j] = wt[q] * S / hsp;
+	}
+	if(J)
+	{
+		double wt[4], gd[4];
+		const double hf = FaceDerivative(k.hI, f, upw, gd);
+		FaceWeights(k.hI, f, upw, -1, wt);
+		const double r = wall ? 0.0 : dc / vis;
+		if(k.slip)
+		{
+			const double L2 = 2.0 * k.lam;
+			const double ap = 1.0 / hsp;
+#pragma unroll
+			for(int q = 0; q < 4; ++q) up.at(1, a, kUpSC, q)[j] = (r * ((2.0 * hf + L2) * gd[q] - (hf + L2) * wt[q])) * ap;
+		}
+		else
+		{
+			const double ap = hf / hsp;
+#pragma unroll
+			for(int q = 0; q < 4; ++q) up.at(1, a, kUpSC, q)[j] = (r * (2.0 * gd[q] - wt[q])) * ap;
+		}
+	}
+}
+
+//  the face of direction d of row i: its low cell, axis, and the row's sign
+__device__ __forceinline__ long long FaceLow(int d, long long i, int nx)
+{
+	return d == 0 ? i - 1 : d == 1 ? i : d == 2 ? i - nx : i;
+}
+
+//  BodyForceA from the faces: SetMatrixA_Limited (BodyForceKernel.h:595-633)
+//  into the row's A_rest, axis by axis over AxisStencil
+template<int T>
+__device__ __forceinline__ void BodyForceAF(const Coef &k, const UpBuf &up, long long i, double *aR)
+{
+	const int term = (T == kPG) ? 0 : 1;
+#pragma unroll
+	for(int a = 0; a < 2; ++a)
+	{
+		const int dm = 2 * a, dp = 2 * a + 1;
+		const long long jm = FaceLow(dm, i, k.nx), jp = FaceLow(dp, i, k.nx);
+		const double Coef_ = Mag<T>(k, a);
+#pragma unroll
+		for(int q = 0; q < 5; ++q)
+		{
+			const int idx = AS(a, q);
+			const double tm = (q < 4) ? -up.at(0, a, term, q)[jm] : 0.0;
+			const double tp = (q > 0) ? up.at(0, a, term, q - 1)[jp] : 0.0;
+			const double val = tm + tp;
+			aR[idx] += Coef_ * val;
+		}
+	}
+}
+
+//  BodyForceJ from the faces: SetJacobiMatrix_Limited (BodyForceKernel.h:635-691)
+template<int T>
+__device__ __forceinline__ void BodyForceJF(const Coef &k, const UpBuf &up, long long i, double *J)
+{
+	const int term = (T == kPG) ? 0 : 1;
+#pragma unroll
+	for(int a = 0; a < 2; ++a)
+	{
+		const int dm = 2 * a, dp = 2 * a + 1;
+		const long long jm = FaceLow(dm, i, k.nx), jp = FaceLow(dp, i, k.nx);
+		const double Coef_ = Mag<T>(k, a);
+#pragma unroll
+		for(int q = 0; q < 5; ++q)
+		{
+			const int idx = AS(a, q);
+			const double xm = (q < 4) ? -up.at(1, a, term, q)[jm] : 0.0;
+			const double xp = (q > 0) ? up.at(1, a, term, q - 1)[jp] : 0.0;
+			J[idx] += Coef_ * (xm + xp);
+		}
+	}
+}
+
+//  MarangoniA from the faces: SolutoCapillarityKernel::SetMatrixA_Limited
+//  into the row's A_rest (SolutoCapillarityKernel.h:411-516)
+__device__ __forceinline__ void MarangoniAF(const Coef &k, const UpBuf &up, long long i, double *aR)
+{
+	double Val[13];
+#pragma unroll
+	for(int q = 0; q < 13; ++q) Val[q] = 0;
+#pragma unroll
+	for(int d = 0; d < 4; ++d)
+	{
+		const long long jf = FaceLow(d, i, k.nx);
+		const bool neg = (d % 2 == 0);
+#pragma unroll
+		for(int q = 0; q < 4; ++q)
+		{
+			const double z = up.at(0, d / 2, kUpSC, q)[jf];
+			Val[FS(d, q)] += neg ? -z : z;
+		}
+	}
+#pragma unroll
+	for(int kk = 0; kk < 9; ++kk) aR[WI(kk)] += k.scMag * Val[WI(kk)];
+}
+
+//  MarangoniJ from the faces: SolutoCapillarityKernel::SetJacobiMatrix_Limited
+//  with ScatterJacobiWide (UpwindKernelBase.h:179-213): the diagonal over the
+//  directions in stencil order; another point: the direction that has it as
+//  its neighbour first, the rest in axis order
+__device__ __forceinline__ void MarangoniJF(const Coef &k, const UpBuf &up, long long i, double *J)
+{
+	double ga[4][4];
+#pragma unroll
+	for(int d = 0; d < 4; ++d)
+	{
+		const long long jf = FaceLow(d, i, k.nx);
+		const bool neg = (d % 2 == 0);
+#pragma unroll
+		for(int q = 0; q < 4; ++q)
+		{
+			const double v = up.at(1, d / 2, kUpSC, q)[jf];
+			ga[d][q] = neg ? -v : v;
+		}
+	}
+#pragma unroll
+	for(int kk = 0; kk < 9; ++kk)
+	{
+		const int idx = WI(kk);
+		double val = 0;
+		if(idx == oo)
+		{
+#pragma unroll
+			for(int j = 0; j < 4; ++j)
+			{
+				const int d = StencilDirC(j);
+				val += ga[d][QOf(d, oo)];
+			}
+		}
+		else
+		{
+			const int first = DirOfAdjC(idx);
+			if(first >= 0) val += ga[first][QOf(first, idx)];
+#pragma unroll
+			for(int d = 0; d < 4; ++d)
+			{
+				if(d == first || QOf(d, idx) < 0) continue;
+				val += ga[d][QOf(d, idx)];
+			}
+		}
+		J[idx] += k.scMag * val;
+	}
 }
 
 } // namespace phys

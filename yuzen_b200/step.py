@@ -112,6 +112,7 @@ def _bind():
     L.yz_step_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_step_set_amg_reuse.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_step_set_graph_loop.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.yz_step_energy.argtypes = [ctypes.c_void_p, _f64p, _f64p]
     L.yz_step_get_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
     L.yz_step_set_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
     L.yz_launch_count.restype = ctypes.c_longlong
@@ -155,6 +156,13 @@ class Step:
         """The step's BiCGStab loops as CUDA graph launches (default) or
         from the stream (yz_step_set_graph_loop)."""
         _check(lib().yz_step_set_graph_loop(self._h, int(bool(on))), "yz_step_set_graph_loop")
+
+    def energy(self):
+        """(F, D): the free energy of the film the step holds and the flux
+        power of the potential (the reference's EnergyEval)."""
+        F, D = ctypes.c_double(), ctypes.c_double()
+        _check(lib().yz_step_energy(self._h, ctypes.byref(F), ctypes.byref(D)), "yz_step_energy")
+        return F.value, D.value
 
     def advance(self, nsteps: int = 1) -> dict:
         st = StepStats()
