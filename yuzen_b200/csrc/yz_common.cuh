@@ -29,7 +29,13 @@ struct UsageError : std::runtime_error
 
 inline void Check(cudaError_t e, const char *what)
 {
-	if(e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+	if(e != cudaSuccess)
+	{
+		//  a failed call also leaves its error as the thread's last error:
+		//  take it, so that the next launch's check does not report it again
+		(void)cudaGetLastError();
+		throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+	}
 }
 #define YZ_CUDA(call) ::yz::Check((call), #call)
 

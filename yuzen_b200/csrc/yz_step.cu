@@ -1184,6 +1184,15 @@ void Step::Energy(double &F, double &D)
 	YZ_CUDA(cudaSetDevice(_device));
 	const int nIn = (_p.nx - 4) * (_p.ny - 4);
 	_enFx.reserve((size_t)_n); _enFy.reserve((size_t)_n); _enOut.reserve(2);
+	//  FaceFluxes' film flag and the reduction scratch, which the
+	//  concentration equation holds when it is on
+	_iflags.reserve(4);
+	_partStep.reserve((size_t)2 * RedBlocks(_n));
+	if(_cntStep.get() == nullptr)
+	{
+		_cntStep.reserve(4);
+		YZ_CUDA(cudaMemsetAsync(_cntStep.get(), 0, 4 * sizeof(unsigned int), _st));
+	}
 	FaceFluxes(_h.get(), _c.get(), _enFx.get(), _enFy.get(), 0.0, false);
 	EnergyPar e;
 	e.bo = _p.Bo; e.dp = _p.Dp; e.hstar = _p.hstar; e.pn = _p.disj_n; e.pm = _p.disj_m;
