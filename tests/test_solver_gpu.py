@@ -288,3 +288,29 @@ def test_amg_reuse_usage_errors():
     with pytest.raises(yz.YzError):
         be.SetAmgReuse(-1)
     be.SetAmgReuse(0)
+
+
+def test_amg_reuse_failure_sets_up_afresh():
+    """A solve on a reused hierarchy that fails is repeated from the caller's
+    guess on a new set-up.  The second system is far from the first (another
+    mobility field, 30 times stiffer) and its cap is the iteration count the
+    oracle needs with a new set-up: when the stale hierarchy misses the cap,
+    the repeat is the oracle's solve to the bit (its iterations come on top
+    of the failed ones); when it does not, the answer meets the tolerance."""
+    a = _systems.film_system(96, seed=2)
+    b = _systems.film_system(96, seed=9, stiff=30.0)
+    o = _oracle.OracleSolver().solve(b)
+    assert o[0] == 0
+    be = yz.B200Backend()
+    be.SetAmgReuse(8)
+    pat = yz.CrsPattern(a["rowptr"], a["col"], a["sorted_col"], a["sorted_src"])
+    for d, cap in ((a, int(a["max_iteration"])), (b, int(o[1]))):
+        s = yz.LinearSolverSettings(int(d["precondition"]), bool(d["scaling"]), cap, float(d["epsilon"]),
+                                    bool(d["conc"]))
+        x = np.array(d["x0"], dtype=np.float64, copy=True)
+        ret, it, res = be.Solve(s, pat, d["values"], d["rhs"], x)
+        assert ret == 0, (ret, it, res)
+    if it > o[1]:
+        assert res == o[2] and np.array_equal(x, o[3])
+    else:
+        assert res <= float(b["epsilon"])
