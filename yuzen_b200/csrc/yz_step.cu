@@ -139,31 +139,30 @@ __device__ __forceinline__ void FaceOf(int d, int i, int nx, const FaceBuf &fb, 
 
 //--------------------------------------------------------------------------
 //  The limited upwind terms' faces (UpwindFaces in yz_upwind.cuh): one
-//  thread a cell, its high x and y faces where a row needs them
+//  thread a cell and (grid y) an axis and a term, the cell's high face on
+//  that axis where a row needs it
 //--------------------------------------------------------------------------
 template<bool J>
 __global__ void KUpwindFaces(Coef k, const double *__restrict__ H, const double *__restrict__ C, FaceBuf fb,
                              UpBuf up)
 {
+	const int a = blockIdx.y / 3, term = blockIdx.y % 3;
+	if(!(term == 0 ? k.onPG : term == 1 ? k.onCF : k.onSC)) return;
 	const int nx = k.nx, ny = k.ny;
 	const long long n = (long long)nx * ny;
+	const long long s = (a == 0) ? 1 : nx;
 	for(long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x)
 	{
 		const int ix = (int)(j % nx), iy = (int)(j / nx);
-#pragma unroll
-		for(int a = 0; a < 2; ++a)
-		{
-			const bool in = (a == 0) ? (ix >= 1 && ix <= nx - 3 && iy >= 2 && iy <= ny - 3)
-			                         : (iy >= 1 && iy <= ny - 3 && ix >= 2 && ix <= nx - 3);
-			if(!in) continue;
-			const long long s = (a == 0) ? 1 : nx;
-			const double f[4] = {H[j - s], H[j], H[j + s], H[j + 2 * s]};
-			const double vis = (a == 0) ? fb.x.vis[j] : fb.y.vis[j];
-			const bool wall = WallFaceLow(k, a, ix, iy);
-			if(k.onPG) BodyForceFace<kPG, J>(k, f, vis, a, ix, iy, wall, up, j);
-			if(k.onCF) BodyForceFace<kCF, J>(k, f, vis, a, ix, iy, wall, up, j);
-			if(k.onSC) MarangoniFace<J>(k, f, C[j], C[j + s], vis, a, wall, up, j);
-		}
+		const bool in = (a == 0) ? (ix >= 1 && ix <= nx - 3 && iy >= 2 && iy <= ny - 3)
+		                         : (iy >= 1 && iy <= ny - 3 && ix >= 2 && ix <= nx - 3);
+		if(!in) continue;
+		const double f[4] = {H[j - s], H[j], H[j + s], H[j + 2 * s]};
+		const double vis = (a == 0) ? fb.x.vis[j] : fb.y.vis[j];
+		const bool wall = WallFaceLow(k, a, ix, iy);
+		if(term == 0) BodyForceFace<kPG, J>(k, f, vis, a, ix, iy, wall, up, j);
+		else if(term == 1) BodyForceFace<kCF, J>(k, f, vis, a, ix, iy, wall, up, j);
+		else MarangoniFace<J>(k, f, C[j], C[j + s], vis, a, wall, up, j);
 	}
 }
 
@@ -921,8 +920,9 @@ void Step::Assemble(int mode, const double *hField, const double *cField, double
 	{
 		_upMem.reserve((size_t)48 * _n);
 		up.base = _upMem.get();
-		if(mode == 1) YZ_LAUNCH(KUpwindFaces<true>, GridFor(_n, 128, 148 * 32), 128, 0, _st, _k, hField, cField, _fb, up);
-		else YZ_LAUNCH(KUpwindFaces<false>, GridFor(_n, 128, 148 * 32), 128, 0, _st, _k, hField, cField, _fb, up);
+		const dim3 grid(GridFor(_n, 128, 148 * 16), 6);
+		if(mode == 1) YZ_LAUNCH(KUpwindFaces<true>, grid, 128, 0, _st, _k, hField, cField, _fb, up);
+		else YZ_LAUNCH(KUpwindFaces<false>, grid, 128, 0, _st, _k, hField, cField, _fb, up);
 	}
 	RowOut o;
 	o.ia = _ia.get(); o.ax = mode == 0 ? _axOld.get() : _axGuess.get();
