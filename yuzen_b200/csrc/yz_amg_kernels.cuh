@@ -913,6 +913,89 @@ __global__ void KDenseMV(const int *__restrict__ halt, int n, const T *__restric
 	}
 }
 
+//--------------------------------------------------------------------------
+//  The coarse levels of the FP32 cycle with L lanes per row (L = 2, 4, 8):
+//  lane q sums the row's entries q, q + L, ... and the group folds its L
+//  partials by shuffles.  The coarse rows (an aggregate's Galerkin row, 10
+//  to 30 entries) are few, so one thread a row leaves most of the GPU idle;
+//  the FP32 cycle's sums are not the oracle's to begin with, so their order
+//  is free.  32 / L rows a warp, the loop alike for all its lanes.
+//--------------------------------------------------------------------------
+template<int L, class T, class XF>
+__device__ __forceinline__ T RowSumLanes(const int *__restrict__ ptr, const int *__restrict__ col,
+                                         const T *__restrict__ val, long long row, bool active, int q, XF xf)
+{
+	T p = T(0);
+	if(active)
+	{
+		const int st = ptr[row], len = ptr[row + 1] - st;
+		for(int k = q; k < len; k += L) p = p + val[st + k] * xf(col[st + k]);
+	}
+#pragma unroll
+	for(int off = L / 2; off >= 1; off >>= 1) p = p + __shfl_down_sync(0xffffffffu, p, off);
+	return p;
+}
+
+#define YZ_LANE_LOOP(L)                                                                              \
+	const int lane_ = threadIdx.x & 31, q = lane_ % (L);                                             \
+	const long long warps_ = ((long long)gridDim.x * blockDim.x) >> 5;                              \
+	for(long long base_ = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 / (L));   \
+	    base_ < n; base_ += warps_ * (32 / (L)))
+
+//  x = m .* f, t = f - A x
+template<int L, class T>
+__global__ void KPreSmoothResidualL(const int *__restrict__ halt, int n, const int *__restrict__ ptr,
+                                    const int *__restrict__ col, const T *__restrict__ val, const T *__restrict__ M,
+                                    const T *__restrict__ f, T *__restrict__ x, T *__restrict__ t)
+{
+	if(halt && *halt) return;
+	YZ_LANE_LOOP(L)
+	{
+		const long long row = base_ + lane_ / L;
+		const bool active = row < n;
+		const T s = RowSumLanes<L>(ptr, col, val, row, active, q, [&](int c) { return M[c] * f[c]; });
+		if(active && q == 0)
+		{
+			const T fi = f[row];
+			x[row] = M[row] * fi;
+			t[row] = fi - s;
+		}
+	}
+}
+
+//  xout = x + m .* (f - A x)
+template<int L, class T>
+__global__ void KPostSmoothL(const int *__restrict__ halt, int n, const int *__restrict__ ptr,
+                             const int *__restrict__ col, const T *__restrict__ val, const T *__restrict__ M,
+                             const T *__restrict__ f, const T *__restrict__ x, T *__restrict__ xout)
+{
+	if(halt && *halt) return;
+	YZ_LANE_LOOP(L)
+	{
+		const long long row = base_ + lane_ / L;
+		const bool active = row < n;
+		const T s = RowSumLanes<L>(ptr, col, val, row, active, q, [&](int c) { return x[c]; });
+		if(active && q == 0) xout[row] = x[row] + M[row] * (f[row] - s);
+	}
+}
+
+//  xout = x + P xc
+template<int L, class T>
+__global__ void KProlongL(const int *__restrict__ halt, int n, const int *__restrict__ pptr, const int *__restrict__ pcol,
+                          const T *__restrict__ pval, const T *__restrict__ xc, const T *__restrict__ x,
+                          T *__restrict__ xout)
+{
+	if(halt && *halt) return;
+	YZ_LANE_LOOP(L)
+	{
+		const long long row = base_ + lane_ / L;
+		const bool active = row < n;
+		const T s = RowSumLanes<L>(pptr, pcol, pval, row, active, q, [&](int c) { return xc[c]; });
+		if(active && q == 0) xout[row] = x[row] + s;
+	}
+}
+#undef YZ_LANE_LOOP
+
 //  the FP32 copies of the V-cycle's matrices: dst_k[i] = (float)src_k[i] over
 //  a list of arrays, one launch for all of them
 struct RoundList

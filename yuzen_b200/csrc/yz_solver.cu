@@ -643,15 +643,26 @@ void Solver::Cycle32(size_t l, const TF *f, TX *x)
 	if(l + 1 < _nlev)
 	{
 		Level &C = *_levels[l + 1];
-		YZ_LAUNCH((KPreSmoothResidual<float, TF, float>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val,
-		          L.M32.get(), f, L.x32.get(), L.t32.get());
+		//  the coarse levels (CSR, float throughout) with several lanes a row
+		const int la = l == 0 ? 1 : LanesFor(L.nnz, n), lp = l == 0 ? 1 : LanesFor(L.pnnz, n);
+		if(la > 1)
+			CoarsePreSmooth(la, n, L.ptr.get(), col, val, L.M32.get(), (const float *)f, L.x32.get(), L.t32.get());
+		else
+			YZ_LAUNCH((KPreSmoothResidual<float, TF, float>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col,
+			          val, L.M32.get(), f, L.x32.get(), L.t32.get());
 		YZ_LAUNCH(KRestrict<float>, GridFor((long long)C.n * 4, kB), kB, 0, _st, Halt(), C.n, L.rptr.get(), L.rcol.get(),
 		          L.rval32.get(), L.t32.get(), C.f32.get());
 		Cycle32<float, float>(l + 1, C.f32.get(), C.x32.get());
-		YZ_LAUNCH(KProlong<float>, g, kB, 0, _st, Halt(), n, L.pptr.get(), L.pcol.get(), L.pval32.get(), C.x32.get(),
-		          L.x32.get(), L.xt32.get());
-		YZ_LAUNCH((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val, L.M32.get(), f,
-		          L.xt32.get(), x);
+		if(lp > 1)
+			CoarseProlong(lp, n, L.pptr.get(), L.pcol.get(), L.pval32.get(), C.x32.get(), L.x32.get(), L.xt32.get());
+		else
+			YZ_LAUNCH(KProlong<float>, g, kB, 0, _st, Halt(), n, L.pptr.get(), L.pcol.get(), L.pval32.get(), C.x32.get(),
+			          L.x32.get(), L.xt32.get());
+		if(la > 1)
+			CoarsePostSmooth(la, n, L.ptr.get(), col, val, L.M32.get(), (const float *)f, L.xt32.get(), (float *)x);
+		else
+			YZ_LAUNCH((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val,
+			          L.M32.get(), f, L.xt32.get(), x);
 	}
 	else
 	{
@@ -660,6 +671,42 @@ void Solver::Cycle32(size_t l, const TF *f, TX *x)
 		          L.xt32.get(), x);
 	}
 }
+
+//  lanes a row for a coarse level of the FP32 cycle, by its mean row length
+int Solver::LanesFor(long long nnz, int n)
+{
+	const long long avg = n > 0 ? nnz / n : 0;
+	return avg >= 24 ? 8 : avg >= 10 ? 4 : avg >= 4 ? 2 : 1;
+}
+
+#define YZ_BY_LANES(lanes, K, n, ...)                                                                   \
+	do {                                                                                                \
+		switch(lanes)                                                                                   \
+		{                                                                                               \
+		case 8:  YZ_LAUNCH((K<8, float>), GridFor((long long)(n) * 8, kB), kB, 0, _st, __VA_ARGS__); break;  \
+		case 4:  YZ_LAUNCH((K<4, float>), GridFor((long long)(n) * 4, kB), kB, 0, _st, __VA_ARGS__); break;  \
+		default: YZ_LAUNCH((K<2, float>), GridFor((long long)(n) * 2, kB), kB, 0, _st, __VA_ARGS__); break;  \
+		}                                                                                               \
+	} while(0)
+
+void Solver::CoarsePreSmooth(int lanes, int n, const int *ptr, const int *col, const float *val, const float *M,
+                             const float *f, float *x, float *t)
+{
+	YZ_BY_LANES(lanes, KPreSmoothResidualL, n, Halt(), n, ptr, col, val, M, f, x, t);
+}
+
+void Solver::CoarsePostSmooth(int lanes, int n, const int *ptr, const int *col, const float *val, const float *M,
+                              const float *f, const float *x, float *xout)
+{
+	YZ_BY_LANES(lanes, KPostSmoothL, n, Halt(), n, ptr, col, val, M, f, x, xout);
+}
+
+void Solver::CoarseProlong(int lanes, int n, const int *pptr, const int *pcol, const float *pval, const float *xc,
+                           const float *x, float *xout)
+{
+	YZ_BY_LANES(lanes, KProlongL, n, Halt(), n, pptr, pcol, pval, xc, x, xout);
+}
+#undef YZ_BY_LANES
 
 //  After an FP64 set-up: every level's matrices rounded to float for
 //  Cycle32 (the finest level's A was rounded by KScaleGather), in one launch

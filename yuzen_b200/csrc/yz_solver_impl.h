@@ -85,6 +85,13 @@ private:
 	Sten StenOf(size_t l) const;
 	void RoundCycle();
 	template<class TF, class TX> void Cycle32(size_t l, const TF *f, TX *x);
+	static int LanesFor(long long nnz, int n);
+	void CoarsePreSmooth(int lanes, int n, const int *ptr, const int *col, const float *val, const float *M,
+	                     const float *f, float *x, float *t);
+	void CoarsePostSmooth(int lanes, int n, const int *ptr, const int *col, const float *val, const float *M,
+	                      const float *f, const float *x, float *xout);
+	void CoarseProlong(int lanes, int n, const int *pptr, const int *pcol, const float *pval, const float *xc,
+	                   const float *x, float *xout);
 	const int *Halt() const { return &_sc.get()->state; }
 	void ApplyPrec(int kind, const double *r, double *z);
 	void EnqueueIteration(int kind);
