@@ -60,9 +60,14 @@ PATHS = {
     "fp32_cycle": "FP32 V-cycle inside the FP64 BiCGStab (AMG set-up, Krylov vectors, SpMVs and tests FP64)",
     "fp32_reuse": "FP32 V-cycle inside the FP64 BiCGStab, each AMG set-up serving several solves, the "
                   "BiCGStab loop replayed as a cached CUDA graph",
+    "fp32m_reuse": "FP32 V-cycle and FP32 matrix values in the BiCGStab's SpMVs (vectors, dot products and "
+                   "recurrences FP64; the Newton residual FP64), each AMG set-up serving several solves, the "
+                   "BiCGStab loop replayed as a cached CUDA graph",
 }
-#  arm -> (preconditioner arithmetic, AMG hierarchy reuse on)
-ARMS = {"fp64": (0, False), "fp32_cycle": (1, False), "fp32_reuse": (1, True)}
+DTYPES = {"fp64": "f64", "fp32_cycle": "f64 (V-cycle f32)", "fp32_reuse": "f64 (V-cycle f32)",
+          "fp32m_reuse": "f64 Newton / f32 matrix and V-cycle in an f64 Krylov"}
+#  arm -> (arithmetic of the solve, AMG hierarchy reuse on)
+ARMS = {"fp64": (0, False), "fp32_cycle": (1, False), "fp32_reuse": (1, True), "fp32m_reuse": (2, True)}
 
 
 def spmv_alpha_bytes(n: int, nnz: int) -> int:
@@ -379,7 +384,7 @@ def run_device_arm(a) -> None:
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": max_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if head_name == "fp64" else "f64 (V-cycle f32)",
+        "dtype": DTYPES[head_name],
         "data": "synthetic (seeded, yuzen_b200.cases)",
         "config": {"workload": a.config, "grid": [cfg.Nx, cfg.Ny], "rows": n, "nnz": nnz,
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
@@ -505,7 +510,7 @@ def run_ensemble_arm(a) -> None:
             "metric": ENSEMBLE_METRIC, "value": head["value"], "unit": ENSEMBLE_UNIT, "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": head["max_ms"] / a.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None,
-            "dtype": "f64" if head_name == "fp64" else "f64 (V-cycle f32)", "data": "synthetic (seeded, cases.batch)",
+            "dtype": DTYPES[head_name], "data": "synthetic (seeded, cases.batch)",
             "config": {"workload": a.config, "instances": len(batch), "instances_rank0": len(mine),
                        "sizes": sorted({c.Nx for c in batch}), "path": PATHS[head_name],
                        "parallelism": f"instances partitioned over {world} GPUs" if world > 1 else "1 GPU",
@@ -537,9 +542,9 @@ def main() -> None:
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=6, help="steps of the end-to-end (host buffers) measurement")
-    ap.add_argument("--arms", default="fp64,fp32_cycle,fp32_reuse",
-                    help="the arms timed, in order (fp64, fp32_cycle, fp32_reuse); headline: the last one whose "
-                         "film is within 1e-8 of the FP64 arm's")
+    ap.add_argument("--arms", default="fp64,fp32_cycle,fp32_reuse,fp32m_reuse",
+                    help="the arms timed, in order (fp64, fp32_cycle, fp32_reuse, fp32m_reuse); headline: the last "
+                         "one whose film is within 1e-8 of the FP64 arm's")
     ap.add_argument("--amg-reuse", type=int, default=64, help="solves an AMG set-up serves in the fp32_reuse arm")
     ap.add_argument("--roofline-steps", type=int, default=3, help="steps over which the roofline kernel is timed")
     ap.add_argument("--workers", type=int, default=32, help="host threads advancing the ensemble's instances")

@@ -46,8 +46,13 @@ typedef struct yz_settings
  * always, then every level's A, SPAI0 diagonal, P, R and the coarsest
  * inverse rounded to float, and the V-cycle run in float; the BiCGStab
  * around it (its SpMVs, dot products, residuals, convergence test and the
- * solution) stays FP64, so a converged solve meets the same tolerance. */
-enum { YZ_PREC_FP64 = 0, YZ_PREC_FP32_CYCLE = 1 };
+ * solution) stays FP64, so a converged solve meets the same tolerance.
+ * YZ_PREC_FP32_MATRIX: the same cycle, and the BiCGStab's SpMVs read the
+ * matrix rounded to float (vectors, dot products, recurrences and the test
+ * FP64): the solve meets its tolerance on the rounded matrix, a relative
+ * change of the system of about 6e-8, which the Newton iteration's FP64
+ * residual corrects in the step. */
+enum { YZ_PREC_FP64 = 0, YZ_PREC_FP32_CYCLE = 1, YZ_PREC_FP32_MATRIX = 2 };
 
 const char* yz_last_error(void);
 

@@ -315,3 +315,22 @@ def test_amg_reuse_failure_sets_up_afresh():
         assert res == o[2] and np.array_equal(x, o[3])
     else:
         assert res <= float(b["epsilon"])
+
+
+@pytest.mark.parametrize("d", _FP32_CASES)
+def test_fp32_matrix_solves_the_rounded_system(d):
+    """PREC_FP32_MATRIX: the BiCGStab's SpMVs read the matrix rounded to
+    float.  The solve converges to its tolerance on that system; measured on
+    the FP64 system its residual is within the matrix's rounding (1e-6
+    relative, against the 6e-8 of a float's last place times the row's
+    growth), and the hierarchy is still the FP64 set-up's."""
+    be = yz.B200Backend()
+    be.SetPrecision(yz.PREC_FP32_MATRIX)
+    g = gpu_solve(d, backend=be)
+    o = _oracle.OracleSolver()
+    r = o.solve(d)
+    _levels_equal(be.levels(), o.levels())
+    assert g[0] == 0, g[:3]
+    assert g[2] <= float(d["epsilon"])
+    tg, to = _true_residual(d, g[3]), _true_residual(d, r[3])
+    assert tg <= max(1e-6, 4.0 * to), (tg, to)

@@ -22,7 +22,7 @@ import numpy as np
 
 __all__ = [
     "LinearSolverSettings", "B200Backend", "MakeLinearSolverBackend", "CrsPattern",
-    "lib", "lib_path", "YzError", "EXPORTED_SYMBOLS", "dot", "spmv", "PREC_FP64", "PREC_FP32_CYCLE",
+    "lib", "lib_path", "YzError", "EXPORTED_SYMBOLS", "dot", "spmv", "PREC_FP64", "PREC_FP32_CYCLE", "PREC_FP32_MATRIX",
 ]
 
 _HERE = Path(__file__).resolve().parent
@@ -44,6 +44,7 @@ EXPORTED_SYMBOLS = (
 #: the preconditioner's arithmetic (YZ_PREC_* of include/yuzen_b200.h)
 PREC_FP64 = 0
 PREC_FP32_CYCLE = 1
+PREC_FP32_MATRIX = 2
 
 
 class YzError(RuntimeError):
@@ -211,8 +212,10 @@ class B200Backend:
         return ret, it.value, res.value
 
     def SetPrecision(self, precision: int) -> None:
-        """PREC_FP64 (the drop-in path) or PREC_FP32_CYCLE (the V-cycle in
-        float inside the FP64 BiCGStab), from the next solve on."""
+        """PREC_FP64 (the drop-in path), PREC_FP32_CYCLE (the V-cycle in float
+        inside the FP64 BiCGStab) or PREC_FP32_MATRIX (that, and the
+        BiCGStab's SpMVs on the matrix rounded to float), from the next solve
+        on."""
         _check(lib().yz_solver_set_precision(self._h, precision), "yz_solver_set_precision")
 
     def SetAmgReuse(self, max_solves: int) -> None:

@@ -46,23 +46,26 @@ __device__ __forceinline__ void RowRange(const int *__restrict__ ptr, const int 
 //  products then added one after the other, so the sum is the sequential
 //  one with four loads in flight instead of one.  T is the arithmetic (the
 //  type of the values): double everywhere but in the FP32 V-cycle.
-template<class T, class XF>
-__device__ __forceinline__ T RowSum(int st, int len, int sd, const int *__restrict__ col, const T *__restrict__ val,
-                                    XF xf)
+//  The values may be stored narrower than the arithmetic (float values in a
+//  double sum: the FP32-matrix SpMV); the arithmetic is that of X.
+template<class V, class XF>
+__device__ __forceinline__ auto RowSum(int st, int len, int sd, const int *__restrict__ col, const V *__restrict__ val,
+                                       XF xf) -> decltype(xf(0))
 {
+	using T = decltype(xf(0));
 	T s = T(0);
 	int k = 0, e = st;
 	for(; k + 4 <= len; k += 4, e += 4 * sd)
 	{
 		const int c0 = col[e], c1 = col[e + sd], c2 = col[e + 2 * sd], c3 = col[e + 3 * sd];
-		const T v0 = val[e], v1 = val[e + sd], v2 = val[e + 2 * sd], v3 = val[e + 3 * sd];
+		const T v0 = (T)val[e], v1 = (T)val[e + sd], v2 = (T)val[e + 2 * sd], v3 = (T)val[e + 3 * sd];
 		const T x0 = xf(c0), x1 = xf(c1), x2 = xf(c2), x3 = xf(c3);
 		s = s + v0 * x0;
 		s = s + v1 * x1;
 		s = s + v2 * x2;
 		s = s + v3 * x3;
 	}
-	for(; k < len; ++k, e += sd) s = s + val[e] * xf(col[e]);
+	for(; k < len; ++k, e += sd) s = s + (T)val[e] * xf(col[e]);
 	return s;
 }
 
@@ -70,10 +73,11 @@ __device__ __forceinline__ T RowSum(int st, int len, int sd, const int *__restri
 //  stencil row's loop is unrolled to the 16 entries a stencil may have, so
 //  that every offset is read from the kernel's parameters by a constant
 //  index; the sum is the same sequential one.
-template<class T, class XF>
-__device__ __forceinline__ T RowSumSten(const Sten &sn, int i, int st, int len, int sd, const int *__restrict__ col,
-                                        const T *__restrict__ val, XF xf)
+template<class V, class XF>
+__device__ __forceinline__ auto RowSumSten(const Sten &sn, int i, int st, int len, int sd, const int *__restrict__ col,
+                                           const V *__restrict__ val, XF xf) -> decltype(xf(0))
 {
+	using T = decltype(xf(0));
 	if(sn.slice && sn.slice[i >> 5])
 	{
 		T s = T(0);
@@ -84,7 +88,7 @@ __device__ __forceinline__ T RowSumSten(const Sten &sn, int i, int st, int len, 
 			T v[4], xv[4];
 #pragma unroll
 			for(int j = 0; j < 4; ++j)
-				if(k0 + j < len) { v[j] = val[st + (k0 + j) * sd]; xv[j] = xf(i + sn.off[k0 + j]); }
+				if(k0 + j < len) { v[j] = (T)val[st + (k0 + j) * sd]; xv[j] = xf(i + sn.off[k0 + j]); }
 #pragma unroll
 			for(int j = 0; j < 4; ++j)
 				if(k0 + j < len) s = s + v[j] * xv[j];

@@ -28,8 +28,9 @@ namespace yz {
 	for(int kk_ = 0, i = blockIdx.x * kRChunk + threadIdx.x; kk_ < kRK; ++kk_, i += kRT)
 
 //  r = b - A x;  bb = b.b, rr = r.r, rho0 = r.r (rh = r)
+template<class V>
 __global__ void __launch_bounds__(kRT, 8) KBInit(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, Sten sn, const int *__restrict__ col,
-                       const double *__restrict__ val, const double *__restrict__ b,
+                       const V *__restrict__ val, const double *__restrict__ b,
                        const double *__restrict__ x, double *__restrict__ r, double *__restrict__ rh,
                        RedScratch rs, Scal *sc)
 {
@@ -77,8 +78,9 @@ __global__ void KPUpdate(int n, const double *__restrict__ r, const double *__re
 }
 
 //  v = A ph; alpha = rho / (rh . v)
+template<class V>
 __global__ void __launch_bounds__(kRT, 8) KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, Sten sn,
-                           const int *__restrict__ col, const double *__restrict__ val, const double *__restrict__ ph,
+                           const int *__restrict__ col, const V *__restrict__ val, const double *__restrict__ ph,
                            const double *__restrict__ rh, double *__restrict__ v, RedScratch rs, Scal *sc)
 {
 	if(sc->state != kRun) return;
@@ -124,8 +126,9 @@ __global__ void KSUpdate(int n, const double *__restrict__ r, const double *__re
 }
 
 //  t = A sh; omega = (t . s) / (t . t)
+template<class V>
 __global__ void __launch_bounds__(kRT, 8) KSpmvOmega(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, Sten sn,
-                           const int *__restrict__ col, const double *__restrict__ val, const double *__restrict__ sh_,
+                           const int *__restrict__ col, const V *__restrict__ val, const double *__restrict__ sh_,
                            const double *__restrict__ s, double *__restrict__ t, RedScratch rs, Scal *sc)
 {
 	if(sc->state != kRun) return;
@@ -753,8 +756,8 @@ void Solver::RoundCycle()
 
 void Solver::SetPrecision(int precision)
 {
-	if(precision != YZ_PREC_FP64 && precision != YZ_PREC_FP32_CYCLE)
-		throw UsageError("set_precision: precision must be YZ_PREC_FP64 or YZ_PREC_FP32_CYCLE");
+	if(precision != YZ_PREC_FP64 && precision != YZ_PREC_FP32_CYCLE && precision != YZ_PREC_FP32_MATRIX)
+		throw UsageError("set_precision: precision must be YZ_PREC_FP64, YZ_PREC_FP32_CYCLE or YZ_PREC_FP32_MATRIX");
 	if(precision != _precision) ++_epoch;
 	_precision = precision;
 }
@@ -771,7 +774,7 @@ void Solver::ApplyPrec(int kind, const double *r, double *z)
 {
 	const int n = _n;
 	if(kind == kPrecDiag) YZ_LAUNCH(KDiagApply, GridFor(n, kB), kB, 0, _st, Halt(), n, _m.get(), r, z);
-	else if(_precision == YZ_PREC_FP32_CYCLE) Cycle32<double, double>(0, r, z);
+	else if(_precision != YZ_PREC_FP64) Cycle32<double, double>(0, r, z);
 	else Cycle(0, r, z);
 }
 
@@ -784,14 +787,22 @@ void Solver::EnqueueIteration(int kind)
 	const int n = _n, nb = RedBlocks(n), g = GridFor(n, kB);
 	const int *ptr = A.ptr.get(), *so = _sellOff.get(), *col = _sellCol.get();
 	const double *val = _sellVal.get();
+	//  YZ_PREC_FP32_MATRIX: the SpMVs read the float copy of the values
+	const float *val32 = _precision == YZ_PREC_FP32_MATRIX ? _sellVal32.get() : nullptr;
 	Scal *sc = _sc.get();
 	double *x = _x.get();
 	YZ_LAUNCH(KPUpdate, g, kB, 0, _st, n, _r.get(), _v.get(), _p.get(), sc);
 	ApplyPrec(kind, _p.get(), _ph.get());
-	YZ_LAUNCH(KSpmvAlpha, nb, kRT, 0, _st, n, ptr, so, _sten, col, val, _ph.get(), _rh.get(), _v.get(), Red(1), sc);
+	if(val32)
+		YZ_LAUNCH(KSpmvAlpha, nb, kRT, 0, _st, n, ptr, so, _sten, col, val32, _ph.get(), _rh.get(), _v.get(), Red(1), sc);
+	else
+		YZ_LAUNCH(KSpmvAlpha, nb, kRT, 0, _st, n, ptr, so, _sten, col, val, _ph.get(), _rh.get(), _v.get(), Red(1), sc);
 	YZ_LAUNCH(KSUpdate, nb, kRT, 0, _st, n, _r.get(), _v.get(), _s.get(), Red(2), sc);
 	ApplyPrec(kind, _s.get(), _sh.get());
-	YZ_LAUNCH(KSpmvOmega, nb, kRT, 0, _st, n, ptr, so, _sten, col, val, _sh.get(), _s.get(), _t.get(), Red(3), sc);
+	if(val32)
+		YZ_LAUNCH(KSpmvOmega, nb, kRT, 0, _st, n, ptr, so, _sten, col, val32, _sh.get(), _s.get(), _t.get(), Red(3), sc);
+	else
+		YZ_LAUNCH(KSpmvOmega, nb, kRT, 0, _st, n, ptr, so, _sten, col, val, _sh.get(), _s.get(), _t.get(), Red(3), sc);
 	YZ_LAUNCH(KXRUpdate, nb, kRT, 0, _st, n, _ph.get(), _sh.get(), _s.get(), _t.get(), _rh.get(), x, _r.get(),
 	          Red(4), sc);
 }
@@ -927,8 +938,12 @@ bool Solver::BiCGStab(int kind, int maxIter, double tol, int &itOut, double &err
 	Level &A = *_levels[0];
 	const int n = _n, nb = RedBlocks(n), g = GridFor(n, kB);
 	double *b = _b.get(), *x = _x.get();
-	YZ_LAUNCH(KBInit, nb, kRT, 0, _st, n, A.ptr.get(), _sellOff.get(), _sten, _sellCol.get(), _sellVal.get(), b, x, _r.get(),
-	          _rh.get(), Red(0), _sc.get());
+	if(_precision == YZ_PREC_FP32_MATRIX)
+		YZ_LAUNCH(KBInit, nb, kRT, 0, _st, n, A.ptr.get(), _sellOff.get(), _sten, _sellCol.get(),
+		          (const float *)_sellVal32.get(), b, x, _r.get(), _rh.get(), Red(0), _sc.get());
+	else
+		YZ_LAUNCH(KBInit, nb, kRT, 0, _st, n, A.ptr.get(), _sellOff.get(), _sten, _sellCol.get(), _sellVal.get(), b, x,
+		          _r.get(), _rh.get(), Red(0), _sc.get());
 	ReadScal();
 	const double normB = _hsc->normb;
 	if(normB < 2.0 * 2.220446049250313e-16)
@@ -982,7 +997,7 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 	const long long l0 = g_launches.load();
 	const int n = _n, nnz = _nnz, g = GridFor(n, kB);
 	Level &L0 = *_levels[0];
-	const bool fp32 = _precision == YZ_PREC_FP32_CYCLE;
+	const bool fp32 = _precision != YZ_PREC_FP64;
 	if(fp32)
 	{
 		const float *was = _sellVal32.get();
