@@ -13,12 +13,13 @@ concentration per pass, all on the device.  The default workload is the
 vertical and in-plane gravity, rotation, Marangoni, evaporation, slip, the
 concentration solved); the case is a seeded synthetic input built by
 yuzen_b200.cases (the reference reads the same film through its ASCII
-restart).  Three arms run from the same start: the plain FP64 path (the
+restart).  Four arms run from the same start: the plain FP64 path (the
 drop-in), the FP32 V-cycle (the AMG preconditioner in float inside the FP64
-BiCGStab), and the FP32 V-cycle with each AMG set-up serving several solves
-and the BiCGStab loop replayed as a cached CUDA graph; the headline is the
-last arm whose film after the timed steps is within 1e-8 (relative L2) of the
-FP64 arm's.  Timing: per arm W untimed steps, then K steps, each
+BiCGStab), the FP32 V-cycle with each AMG set-up serving several solves
+and the BiCGStab loop replayed as a cached CUDA graph, and that with the
+BiCGStab's SpMVs on the float copy of the matrix; the headline is the fastest
+arm whose film after the timed steps is within 1e-8 (relative L2) of the FP64
+arm's.  Timing: per arm W untimed steps, then K steps, each
 timed with CUDA events on the library's stream, the L2 cache (126 MB) flushed
 by writing a 256 MiB buffer between steps (outside the timed region); under
 torchrun every rank runs an independent replica and the time is the maximum
@@ -296,8 +297,8 @@ def run_device_arm(a) -> None:
         return out
 
     #  the arms from the same start, the plain FP64 one first; the headline
-    #  is the last arm named whose film after the timed steps is within 1e-8
-    #  (relative L2) of the FP64 arm's (the FP64 arm itself if none is)
+    #  is the fastest arm whose film after the timed steps is within 1e-8
+    #  (relative L2) of the FP64 arm's (the FP64 arm itself qualifies)
     names = [x for x in a.arms.split(",") if x]
     for x in names:
         if x not in ARMS:
@@ -312,10 +313,8 @@ def run_device_arm(a) -> None:
         for x in arms:
             if x != "fp64":
                 h_err[x] = float(np.linalg.norm(arms[x]["h"] - h64) / np.linalg.norm(h64))
-    head_name = names[0]
-    for x in names:
-        if x == "fp64" or h_err.get(x, 0.0) <= 1e-8:
-            head_name = x
+    qualified = [x for x in names if x == "fp64" or h_err.get(x, 0.0) <= 1e-8]
+    head_name = max(qualified or names[:1], key=lambda x: arms[x]["value"])
     head = arms[head_name]
     total_ms, max_ms, value = head["total_ms"], head["max_ms"], head["value"]
     launches = head["launches"]
@@ -543,8 +542,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=6, help="steps of the end-to-end (host buffers) measurement")
     ap.add_argument("--arms", default="fp64,fp32_cycle,fp32_reuse,fp32m_reuse",
-                    help="the arms timed, in order (fp64, fp32_cycle, fp32_reuse, fp32m_reuse); headline: the last "
-                         "one whose film is within 1e-8 of the FP64 arm's")
+                    help="the arms timed, in order (fp64, fp32_cycle, fp32_reuse, fp32m_reuse); headline: the "
+                         "fastest one whose film is within 1e-8 of the FP64 arm's")
     ap.add_argument("--amg-reuse", type=int, default=64, help="solves an AMG set-up serves in the fp32_reuse arm")
     ap.add_argument("--roofline-steps", type=int, default=3, help="steps over which the roofline kernel is timed")
     ap.add_argument("--workers", type=int, default=32, help="host threads advancing the ensemble's instances")

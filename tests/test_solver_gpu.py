@@ -204,6 +204,21 @@ def _true_residual(d, x):
     return np.linalg.norm(r) / np.linalg.norm(b)
 
 
+def _abs_product(d, x):
+    """| |A| |x| | / |b| of the row-scaled system: the size of the change
+    that rounding the matrix's entries by a relative 1 can make in A x"""
+    n, rp, col, val = d["n"], d["rowptr"], d["col"], d["values"]
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    ax = np.bincount(rows, weights=np.abs(val) * np.abs(x[col]), minlength=n)
+    b = np.asarray(d["rhs"], np.float64).copy()
+    if int(d["scaling"]):
+        dia = np.abs(val[rp[:-1]])
+        ok = dia >= 1e-30
+        ax[ok] /= dia[ok]
+        b[ok] /= dia[ok]
+    return np.linalg.norm(ax) / np.linalg.norm(b)
+
+
 _FP32_CASES = [c for c in _amg_cases() if not c.values[0]["conc"]] + [
     pytest.param(_systems.film_system(200, seed=7, periodic=True), id="film200-periodic"),
     pytest.param(_systems.film_system(384, seed=11), id="film384")]
@@ -321,9 +336,10 @@ def test_amg_reuse_failure_sets_up_afresh():
 def test_fp32_matrix_solves_the_rounded_system(d):
     """PREC_FP32_MATRIX: the BiCGStab's SpMVs read the matrix rounded to
     float.  The solve converges to its tolerance on that system; measured on
-    the FP64 system its residual is within the matrix's rounding (1e-6
-    relative, against the 6e-8 of a float's last place times the row's
-    growth), and the hierarchy is still the FP64 set-up's."""
+    the FP64 system its residual is within what rounding the matrix to float
+    can change it by, 2^-24 |A| |x| (a few times that, against the norm of
+    b; large on the ill-conditioned 1-D fourth-order systems), and the
+    hierarchy is still the FP64 set-up's."""
     be = yz.B200Backend()
     be.SetPrecision(yz.PREC_FP32_MATRIX)
     g = gpu_solve(d, backend=be)
@@ -333,4 +349,5 @@ def test_fp32_matrix_solves_the_rounded_system(d):
     assert g[0] == 0, g[:3]
     assert g[2] <= float(d["epsilon"])
     tg, to = _true_residual(d, g[3]), _true_residual(d, r[3])
-    assert tg <= max(1e-6, 4.0 * to), (tg, to)
+    rounding = 4.0 * 2.0 ** -24 * _abs_product(d, g[3])
+    assert tg <= max(2.0 * float(d["epsilon"]), 4.0 * to) + rounding, (tg, to, rounding)
