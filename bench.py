@@ -445,7 +445,8 @@ def run_ensemble_arm(a) -> None:
     for name in [x for x in a.arms.split(",") if x]:
         prec, reuse = ARMS[name]
         ens = ensemble.Ensemble([batch[k] for k in mine], device=local, precision=prec,
-                                amg_reuse=a.amg_reuse if reuse else 0, workers=a.workers)
+                                amg_reuse=a.amg_reuse if reuse else 0, workers=a.workers,
+                                graph_loop=bool(a.ensemble_graph))
         if a.warmup > 0:
             ens.advance(a.warmup)
         if dist:
@@ -514,6 +515,7 @@ def run_ensemble_arm(a) -> None:
                        "sizes": sorted({c.Nx for c in batch}), "path": PATHS[head_name],
                        "parallelism": f"instances partitioned over {world} GPUs" if world > 1 else "1 GPU",
                        "l2": "flushed between steps (256 MiB write)", "workers": ens.workers,
+                       "graph_loop": bool(a.ensemble_graph),
                        "arms": {k: {"instance_steps_per_s": v["value"], "ms_per_step": v["max_ms"] / a.steps,
                                     "gpu_launches": v["launches"]} for k, v in arms.items()},
                        "checksum_rel_diff_vs_fp64": diff},
@@ -548,6 +550,8 @@ def main() -> None:
     ap.add_argument("--roofline-steps", type=int, default=3, help="steps over which the roofline kernel is timed")
     ap.add_argument("--workers", type=int, default=32, help="host threads advancing the ensemble's instances")
     ap.add_argument("--ref-instances", type=int, default=3, help="ensemble instances the reference arm samples")
+    ap.add_argument("--ensemble-graph", type=int, default=0,
+                    help="1: the ensemble's BiCGStab loops as CUDA graphs (captured from the instances' threads)")
     a = ap.parse_args()
     if a.warmup < 3 and a.impl == "b200":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
