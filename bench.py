@@ -548,10 +548,10 @@ def main() -> None:
                          "fastest one whose film is within 1e-8 of the FP64 arm's")
     ap.add_argument("--amg-reuse", type=int, default=64, help="solves an AMG set-up serves in the fp32_reuse arm")
     ap.add_argument("--roofline-steps", type=int, default=3, help="steps over which the roofline kernel is timed")
-    ap.add_argument("--workers", type=int, default=32, help="host threads advancing the ensemble's instances")
+    ap.add_argument("--workers", type=int, default=64, help="host threads advancing the ensemble's instances")
     ap.add_argument("--ref-instances", type=int, default=3, help="ensemble instances the reference arm samples")
-    ap.add_argument("--ensemble-graph", type=int, default=0,
-                    help="1: the ensemble's BiCGStab loops as CUDA graphs (captured from the instances' threads)")
+    ap.add_argument("--ensemble-graph", type=int, default=1,
+                    help="0: the ensemble's BiCGStab loops launched from the streams instead of as CUDA graphs")
     a = ap.parse_args()
     if a.warmup < 3 and a.impl == "b200":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

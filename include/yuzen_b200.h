@@ -96,10 +96,9 @@ int yz_solver_set_precision(yz_solver* s, int precision);
 int yz_solver_set_amg_reuse(yz_solver* s, int max_solves);
 
 /* The BiCGStab loop as one CUDA graph launch per solve (1, the default) or
- * launched from the stream with one iteration in flight (0).  A program that
- * drives several contexts from several host threads while any of them may
- * allocate device memory sets 0: a graph is captured from the context's
- * stream, and a capture does not mix with other threads' allocations. */
+ * launched from the stream with one iteration in flight (0).  The graph is
+ * captured from the context's stream in thread-local capture mode, so other
+ * host threads may drive their own contexts (and allocate) meanwhile. */
 int yz_solver_set_graph_loop(yz_solver* s, int on);
 
 /* ILinearSolverBackend::Memory / SetMemory (LinearSolverBackend.h:89-102):

@@ -50,7 +50,7 @@ class Ensemble:
     case; advance(n) advances every instance n steps concurrently."""
 
     def __init__(self, cases, device: int = 0, precision: int = PREC_FP64, amg_reuse: int = 0,
-                 workers: int | None = None, graph_loop: bool = False):
+                 workers: int | None = None, graph_loop: bool = True):
         self.cases = list(cases)
         self.steps = []
         for c in self.cases:
@@ -58,12 +58,11 @@ class Ensemble:
             st = ys.Step(ys.params_from_state(st0), st0["field_h0"], st0["field_c0"], st0["field_s0"], device=device)
             st.set_precision(precision)
             st.set_amg_reuse(amg_reuse)
-            #  several contexts driven from several threads: the loops run
-            #  from their streams unless asked otherwise (a graph capture
-            #  does not mix with other threads' allocations)
+            #  each context captures its loop graph from its own thread in
+            #  thread-local mode; graph_loop False launches from the stream
             st.set_graph_loop(graph_loop)
             self.steps.append(st)
-        self.workers = workers or min(len(self.steps), max(1, (os.cpu_count() or 1)))
+        self.workers = workers or min(len(self.steps), max(1, 2 * (os.cpu_count() or 1)))
         self._pool = concurrent.futures.ThreadPoolExecutor(max_workers=self.workers) if self.steps else None
 
     def __len__(self) -> int:
