@@ -11,6 +11,7 @@
 #include "yz_solver_impl.h"
 
 #include <map>
+#include <type_traits>
 
 #include <algorithm>
 #include <cmath>
@@ -647,10 +648,13 @@ void Solver::Cycle32(size_t l, const TF *f, TX *x)
 	{
 		Level &C = *_levels[l + 1];
 		//  the coarse levels (CSR, float throughout) with several lanes a row
-		const int la = l == 0 ? 1 : LanesFor(L.nnz, n), lp = l == 0 ? 1 : LanesFor(L.pnnz, n);
-		if(la > 1)
-			CoarsePreSmooth(la, n, L.ptr.get(), col, val, L.M32.get(), (const float *)f, L.x32.get(), L.t32.get());
-		else
+		constexpr bool coarse = std::is_same<TF, float>::value && std::is_same<TX, float>::value;
+		const int la = coarse ? LanesFor(L.nnz, n) : 1, lp = coarse ? LanesFor(L.pnnz, n) : 1;
+		if constexpr(coarse)
+		{
+			if(la > 1) CoarsePreSmooth(la, n, L.ptr.get(), col, val, L.M32.get(), f, L.x32.get(), L.t32.get());
+		}
+		if(la == 1)
 			YZ_LAUNCH((KPreSmoothResidual<float, TF, float>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col,
 			          val, L.M32.get(), f, L.x32.get(), L.t32.get());
 		YZ_LAUNCH(KRestrict<float>, GridFor((long long)C.n * 4, kB), kB, 0, _st, Halt(), C.n, L.rptr.get(), L.rcol.get(),
@@ -661,9 +665,11 @@ void Solver::Cycle32(size_t l, const TF *f, TX *x)
 		else
 			YZ_LAUNCH(KProlong<float>, g, kB, 0, _st, Halt(), n, L.pptr.get(), L.pcol.get(), L.pval32.get(), C.x32.get(),
 			          L.x32.get(), L.xt32.get());
-		if(la > 1)
-			CoarsePostSmooth(la, n, L.ptr.get(), col, val, L.M32.get(), (const float *)f, L.xt32.get(), (float *)x);
-		else
+		if constexpr(coarse)
+		{
+			if(la > 1) CoarsePostSmooth(la, n, L.ptr.get(), col, val, L.M32.get(), f, L.xt32.get(), x);
+		}
+		if(la == 1)
 			YZ_LAUNCH((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val,
 			          L.M32.get(), f, L.xt32.get(), x);
 	}
