@@ -122,6 +122,16 @@ STEP_CASES = {
         "Numerics.TimeStepControl.Enable": True, "Numerics.TimeStepControl.KeepSteps": 2,
         "Numerics.TimeStepControl.ChangeFactor": 0.75, "Numerics.InitialDt": 1e-3,
     }, 6, -1),
+    # every term, the well-mixed concentration solved, and the other
+    # evaporation laws: PowerN in c, the negPow spatial profile, a rate ten
+    # times the case's so that the caps (half the film per step, the solvent
+    # there is) take part
+    "step_evap_powern_negpow_40": ("allphys_2d_reg.toml", {
+        "Grid.Nx": 40, "Grid.Ny": 40,
+        "Physics.Evaporation.ConcFunc": "PowerN", "Physics.Evaporation.PowerN": 2.0,
+        "Physics.Evaporation.SpatialFunc": "negPow", "Physics.Evaporation.Coef": 1e-6,
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-2,
+    }, 3, -1),
     # capillary + disjoining with the time-step control on
     "step_adaptive_40": ("allphys_2d_reg.toml", {
         **_NO_UPWIND, "Grid.Nx": 40, "Grid.Ny": 40,
