@@ -446,7 +446,7 @@ def run_ensemble_arm(a) -> None:
         prec, reuse = ARMS[name]
         ens = ensemble.Ensemble([batch[k] for k in mine], device=local, precision=prec,
                                 amg_reuse=a.amg_reuse if reuse else 0, workers=a.workers,
-                                graph_loop=bool(a.ensemble_graph))
+                                graph_loop=None if a.ensemble_graph < 0 else bool(a.ensemble_graph))
         if a.warmup > 0:
             ens.advance(a.warmup)
         if dist:
@@ -515,7 +515,7 @@ def run_ensemble_arm(a) -> None:
                        "sizes": sorted({c.Nx for c in batch}), "path": PATHS[head_name],
                        "parallelism": f"instances partitioned over {world} GPUs" if world > 1 else "1 GPU",
                        "l2": "flushed between steps (256 MiB write)", "workers": ens.workers,
-                       "graph_loop": bool(a.ensemble_graph),
+                       "graph_loop": "with hierarchy reuse" if a.ensemble_graph < 0 else bool(a.ensemble_graph),
                        "arms": {k: {"instance_steps_per_s": v["value"], "ms_per_step": v["max_ms"] / a.steps,
                                     "gpu_launches": v["launches"]} for k, v in arms.items()},
                        "checksum_rel_diff_vs_fp64": diff},
@@ -550,8 +550,9 @@ def main() -> None:
     ap.add_argument("--roofline-steps", type=int, default=3, help="steps over which the roofline kernel is timed")
     ap.add_argument("--workers", type=int, default=64, help="host threads advancing the ensemble's instances")
     ap.add_argument("--ref-instances", type=int, default=3, help="ensemble instances the reference arm samples")
-    ap.add_argument("--ensemble-graph", type=int, default=1,
-                    help="0: the ensemble's BiCGStab loops launched from the streams instead of as CUDA graphs")
+    ap.add_argument("--ensemble-graph", type=int, default=-1,
+                    help="the ensemble's BiCGStab loops as CUDA graphs (1) or from the streams (0); -1: graphs "
+                         "where the AMG hierarchy is reused")
     a = ap.parse_args()
     if a.warmup < 3 and a.impl == "b200":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

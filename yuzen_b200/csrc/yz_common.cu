@@ -6,6 +6,7 @@
 namespace yz {
 
 std::atomic<long long> g_launches{0};
+thread_local long long t_launches = 0;
 
 //  per-launch timing of one kernel (yz_time_kernel)
 namespace {

@@ -42,7 +42,14 @@ inline void Check(cudaError_t e, const char *what)
 //  Every kernel launch of the library goes through YZ_LAUNCH, which counts it,
 //  and, for the one kernel named by yz_time_kernel(), brackets it with CUDA
 //  events on its own stream (the per-launch device time of that kernel).
-extern std::atomic<long long> g_launches;
+extern std::atomic<long long> g_launches;     // every launch of the process (yz_launch_count)
+extern thread_local long long t_launches;     // this thread's: a context's counts are taken from it
+//  count n launches (negative: take back launches that were captured, not run)
+inline void CountLaunches(long long n)
+{
+	g_launches.fetch_add(n, std::memory_order_relaxed);
+	t_launches += n;
+}
 bool TimedKernel(const char *name);
 bool TimingActive();   // a kernel is selected for per-launch timing
 void TimeBegin(cudaStream_t st);
@@ -56,7 +63,7 @@ void TimeDropLast(long long k);   // forget the last k of them
 		if(yzTimed_) ::yz::TimeBegin(stream);                                     \
 		kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);               \
 		if(yzTimed_) ::yz::TimeEnd(stream);                                       \
-		::yz::g_launches.fetch_add(1, std::memory_order_relaxed);                 \
+		::yz::CountLaunches(1);                                                   \
 		::yz::Check(cudaGetLastError(), #kernel);                                 \
 	} while(0)
 

@@ -880,7 +880,7 @@ void Solver::RunIterations(int kind)
 	YZ_CUDA(cudaGraphLaunch(lg.exec, _st));
 	ReadScal();
 	//  the kernels the loop ran
-	g_launches.fetch_add(lg.perBody * (long long)_hsc->bodies);
+	CountLaunches(lg.perBody * (long long)_hsc->bodies);
 }
 
 void Solver::FreeLoopGraph(LoopGraph &g)
@@ -909,7 +909,7 @@ void Solver::BuildLoopGraph(int kind, LoopGraph &lg)
 		cudaGraphNode_t node;
 		YZ_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
 		body = cp.conditional.phGraph_out[0];
-		const long long l0 = g_launches.load();
+		const long long l0 = t_launches;
 		YZ_CUDA(cudaStreamBeginCaptureToGraph(_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
 		try
 		{
@@ -923,8 +923,8 @@ void Solver::BuildLoopGraph(int kind, LoopGraph &lg)
 			throw;
 		}
 		YZ_CUDA(cudaStreamEndCapture(_st, &body));
-		lg.perBody = g_launches.load() - l0;
-		g_launches.fetch_sub(lg.perBody);
+		lg.perBody = t_launches - l0;
+		CountLaunches(-lg.perBody);
 		YZ_CUDA(cudaGraphInstantiate(&exec, graph, 0));
 	}
 	catch(...)
@@ -1000,7 +1000,7 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 	if(_n <= 0) throw UsageError("solve: set_pattern first");
 	if(set.max_iteration < 0) throw UsageError("solve: max_iteration must be >= 0");
 	YZ_CUDA(cudaSetDevice(_device));
-	const long long l0 = g_launches.load();
+	const long long l0 = t_launches;
 	const int n = _n, nnz = _nnz, g = GridFor(n, kB);
 	Level &L0 = *_levels[0];
 	const bool fp32 = _precision != YZ_PREC_FP64;
@@ -1103,7 +1103,7 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 		YZ_CUDA(cudaEventElapsedTime(&ms, _ev1, _ev2)); _iterMs = ms;
 	}
 	else { YZ_CUDA(cudaEventElapsedTime(&ms, _ev0, _ev2)); _iterMs = ms; }
-	_launches += g_launches.load() - l0;
+	_launches += t_launches - l0;
 	if(broke)
 	{
 		const double rel = BreakdownResidual();

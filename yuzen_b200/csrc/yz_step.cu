@@ -1069,7 +1069,7 @@ void Step::Advance(int nsteps, yz_step_stats &stats)
 	YZ_CUDA(cudaSetDevice(_device));
 	const size_t bytes = (size_t)_n * sizeof(double);
 	const int g = GridFor(_n, 256);
-	const long long l0 = g_launches.load();
+	const long long l0 = t_launches;
 	YZ_CUDA(cudaEventRecord(_eA, _st));
 	for(int step = 0; step < nsteps; ++step)
 	{
@@ -1158,7 +1158,7 @@ void Step::Advance(int nsteps, yz_step_stats &stats)
 	float ms = 0;
 	YZ_CUDA(cudaEventElapsedTime(&ms, _eA, _eB));
 	stats.device_ms = ms;
-	stats.launches = g_launches.load() - l0;
+	stats.launches = t_launches - l0;
 }
 
 void Step::SetFields(const double *h, const double *c)

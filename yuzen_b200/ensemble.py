@@ -50,9 +50,14 @@ class Ensemble:
     case; advance(n) advances every instance n steps concurrently."""
 
     def __init__(self, cases, device: int = 0, precision: int = PREC_FP64, amg_reuse: int = 0,
-                 workers: int | None = None, graph_loop: bool = True):
+                 workers: int | None = None, graph_loop: bool | None = None):
         self.cases = list(cases)
         self.steps = []
+        #  the loop graphs pay when a hierarchy serves several solves (a
+        #  graph kept for them); with a new set-up every solve each solve
+        #  would capture anew, from many threads at once
+        if graph_loop is None:
+            graph_loop = amg_reuse > 0
         for c in self.cases:
             st0 = c.state()
             st = ys.Step(ys.params_from_state(st0), st0["field_h0"], st0["field_c0"], st0["field_s0"], device=device)
@@ -60,7 +65,7 @@ class Ensemble:
             st.set_amg_reuse(amg_reuse)
             #  each context captures its loop graph from its own thread in
             #  thread-local mode; graph_loop False launches from the stream
-            st.set_graph_loop(graph_loop)
+            st.set_graph_loop(bool(graph_loop))
             self.steps.append(st)
         self.workers = workers or min(len(self.steps), max(1, 2 * (os.cpu_count() or 1)))
         self._pool = concurrent.futures.ThreadPoolExecutor(max_workers=self.workers) if self.steps else None
