@@ -201,6 +201,26 @@ __global__ void KCtlInit(Scal *sc, double eps, int maxIter)
 	sc->eps = eps; sc->maxIter = maxIter; sc->it = 0; sc->state = kRun; sc->bodies = 0;
 }
 
+//  The start of a run from KBInit's norms, on the device (the oracle's tests
+//  before its loop): |b| < 2 eps_machine gives x = 0 and no iteration; else
+//  eps = tol |b|, and the loop runs while the start residual is above it and
+//  an iteration is allowed
+__global__ void KCtlStart(Scal *sc, double tol, int maxIter)
+{
+	sc->maxIter = maxIter; sc->it = 0; sc->bodies = 0;
+	const double normB = sc->normb;
+	if(normB < 2.0 * 2.220446049250313e-16) { sc->state = kTiny; return; }
+	const double eps = tol * normB;
+	sc->eps = eps;
+	sc->state = (sc->res > eps && maxIter > 0) ? kRun : kSkip;
+}
+
+__global__ void KZeroIfTiny(int n, const Scal *sc, double *__restrict__ x)
+{
+	if(sc->state != kTiny) return;
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = 0.0;
+}
+
 //  The end of an iteration: a half-step exit, whose x update KXRUpdate has just
 //  made, becomes a plain exit, so that an iteration queued after it makes
 //  no second one; then the loop's condition (another iteration while the
@@ -844,6 +864,7 @@ void Solver::RunIterations(int kind)
 		//  iterations that did work are the run's count (exact for a kernel
 		//  that precedes the half-step test, as KSpmvAlpha).
 		const long long mark = TimeCount();
+		_tailDone = false;		// Solve copies the answer after this run
 		int queued = 0;
 		int slot = 0;
 		EnqueueIteration(kind); ++queued;
@@ -878,6 +899,14 @@ void Solver::RunIterations(int kind)
 		lg.key = key;
 	}
 	YZ_CUDA(cudaGraphLaunch(lg.exec, _st));
+	//  the end of the run queued behind the loop -- its time, the answer
+	//  into the caller's x (Solve's tail) -- so that one wait covers all
+	YZ_CUDA(cudaEventRecord(_ev2, _st));
+	if(_tailDst)
+	{
+		YZ_CUDA(cudaMemcpyAsync(_tailDst, _tailSrc, _tailBytes, cudaMemcpyDeviceToDevice, _st));
+		_tailDone = true;
+	}
 	ReadScal();
 	//  the kernels the loop ran
 	CountLaunches(lg.perBody * (long long)_hsc->bodies);
@@ -938,7 +967,9 @@ void Solver::BuildLoopGraph(int kind, LoopGraph &lg)
 }
 
 //  BiCGStab on level 0's matrix (values in _levels[0]); the oracle's
-//  BiCGStab() step by step.  Returns false on a breakdown (rho == 0).
+//  BiCGStab() step by step.  The start tests run on the device (KCtlStart),
+//  so the host waits once, after the run (RunIterations leaves the state in
+//  _hsc).  Returns false on a breakdown (rho == 0).
 bool Solver::BiCGStab(int kind, int maxIter, double tol, int &itOut, double &errOut)
 {
 	Level &A = *_levels[0];
@@ -950,27 +981,14 @@ bool Solver::BiCGStab(int kind, int maxIter, double tol, int &itOut, double &err
 	else
 		YZ_LAUNCH(KBInit, nb, kRT, 0, _st, n, A.ptr.get(), _sellOff.get(), _sten, _sellCol.get(), _sellVal.get(), b, x,
 		          _r.get(), _rh.get(), Red(0), _sc.get());
-	ReadScal();
-	const double normB = _hsc->normb;
-	if(normB < 2.0 * 2.220446049250313e-16)
-	{
-		YZ_LAUNCH(KFill, g, kB, 0, _st, n, 0.0, x);
-		itOut = 0; errOut = normB;
-		return true;
-	}
-	const double eps = tol * normB;
-	double res = _hsc->res;
-	int it = 0;
-	if(res > eps && maxIter > 0)
-	{
-		YZ_LAUNCH(KCtlInit, 1, 1, 0, _st, _sc.get(), eps, maxIter);
-		RunIterations(kind);
-		if(_hsc->state == kBreak) return false;
-		it = _hsc->it;
-		res = _hsc->res;
-	}
-	itOut = it;
-	errOut = res / normB;
+	YZ_LAUNCH(KCtlStart, 1, 1, 0, _st, _sc.get(), tol, maxIter);
+	YZ_LAUNCH(KZeroIfTiny, g, kB, 0, _st, n, _sc.get(), x);
+	RunIterations(kind);
+	const Scal &h = *_hsc;
+	if(h.state == kTiny) { itOut = 0; errOut = h.normb; return true; }
+	if(h.state == kBreak) return false;
+	itOut = (h.state == kSkip) ? 0 : h.it;
+	errOut = h.res / h.normb;
 	return true;
 }
 
@@ -1016,6 +1034,9 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 	YZ_CUDA(cudaMemcpyAsync(_x.get(), dX, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
 	YZ_CUDA(cudaMemcpyAsync(_x0.get(), dX, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
 	YZ_CUDA(cudaEventRecord(_ev0, _st));
+	//  a run in graph form copies its answer to dX behind the loop (the
+	//  last run's copy is the one that stays)
+	_tailDst = dX; _tailSrc = _x.get(); _tailBytes = (size_t)n * sizeof(double); _tailDone = false;
 	_setupMs = 0; _iterMs = 0;
 	int it = 0, itTried = 0;
 	double err = 0.0;
@@ -1094,7 +1115,8 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 			}
 		}
 	}
-	YZ_CUDA(cudaEventRecord(_ev2, _st));
+	_tailDst = nullptr;
+	if(!_tailDone) YZ_CUDA(cudaEventRecord(_ev2, _st));	// else recorded behind the loop
 	YZ_CUDA(cudaEventSynchronize(_ev2));
 	float ms = 0;
 	if(timedSetup)
@@ -1108,10 +1130,22 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 	{
 		const double rel = BreakdownResidual();
 		if(rel <= set.epsilon && rel == rel) { it = 0; err = rel; }
-		else { iterOut = itTried; residOut = rel; return 2; }
+		else
+		{
+			//  x is left as the caller gave it
+			if(_tailDone)
+			{
+				YZ_CUDA(cudaMemcpyAsync(dX, _x0.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+				YZ_CUDA(cudaStreamSynchronize(_st));
+			}
+			iterOut = itTried; residOut = rel; return 2;
+		}
 	}
-	YZ_CUDA(cudaMemcpyAsync(dX, _x.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
-	YZ_CUDA(cudaStreamSynchronize(_st));
+	if(!_tailDone)
+	{
+		YZ_CUDA(cudaMemcpyAsync(dX, _x.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+		YZ_CUDA(cudaStreamSynchronize(_st));
+	}
 	iterOut = it + itTried;
 	residOut = err;
 	if(err <= set.epsilon) return 0;

@@ -21,7 +21,9 @@ struct Scal
 };
 
 //  the state word of a BiCGStab run on the device
-enum KState { kRun = 0, kConv = 1, kConvHalf = 2, kBreak = 3, kNaN = 4, kCap = 5 };
+//  kTiny: |b| below twice the machine epsilon (x = 0, no iteration); kSkip:
+//  the start residual already meets the tolerance, or no iteration allowed
+enum KState { kRun = 0, kConv = 1, kConvHalf = 2, kBreak = 3, kNaN = 4, kCap = 5, kTiny = 6, kSkip = 7 };
 
 //  TryBackoff, LinearSolverBackend.cpp:262-270
 struct TryBackoff
@@ -166,6 +168,11 @@ private:
 	unsigned _epoch = 0, _epochH = 0;
 	LoopGraph _loop[2];
 	bool _graphLoop = true;       // the loop as a CUDA graph (else from the stream)
+	//  Solve's tail, queued behind a graph run: x into the caller's dX
+	double *_tailDst = nullptr;
+	const double *_tailSrc = nullptr;
+	size_t _tailBytes = 0;
+	bool _tailDone = false;
 	double _setupMs = 0, _iterMs = 0;
 	long long _launches = 0;
 };
