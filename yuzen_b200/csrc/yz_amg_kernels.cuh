@@ -700,7 +700,6 @@ __global__ void __launch_bounds__(512) KGjPanel(int n, int k0, int B, const doub
 	double *P = smem;                                  // B columns of n
 	double *rv = smem + (size_t)B * n;                 // 512 reduction values
 	int *ri = reinterpret_cast<int *>(rv + 512);       // 512 reduction indices
-	__shared__ int sp;
 	__shared__ double spiv;
 	const int t = threadIdx.x, nt = blockDim.x;
 	for(int e = t; e < B * n; e += nt) P[e] = Mc[(size_t)k0 * n + e];
@@ -711,7 +710,7 @@ __global__ void __launch_bounds__(512) KGjPanel(int n, int k0, int B, const doub
 		const int k = k0 + c;
 		double *colc = P + (size_t)c * n;
 		const int p = GjPivot(colc, n, k, rv, ri);
-		if(t == 0) { sp = p; spiv = colc[p]; pivRow[c] = p; pivVal[c] = colc[p]; }
+		if(t == 0) { spiv = colc[p]; pivRow[c] = p; pivVal[c] = colc[p]; }
 		//  the multipliers, column c before the step
 		for(int i = t; i < n; i += nt) F[(size_t)c * n + i] = colc[(i == p) ? k : i];
 		__syncthreads();

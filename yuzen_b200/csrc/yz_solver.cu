@@ -931,6 +931,7 @@ void Solver::BuildLoopGraph(int kind, LoopGraph &lg)
 	{
 		cudaGraphConditionalHandle h;
 		YZ_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault));
+		//  the other members are value-initialised (zero), as the API asks
 		cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
 		cp.conditional.handle = h;
 		cp.conditional.type = cudaGraphCondTypeWhile;

@@ -40,13 +40,8 @@ __device__ __forceinline__ int Offset(int s, int nx)
 	}
 }
 
-//  non-negative doubles order as their bit patterns
-__device__ __forceinline__ void AtomicMaxAbs(unsigned long long *slot, double v)
-{
-	const double a = fabs(v);
-	atomicMax(slot, (unsigned long long)__double_as_longlong(a));
-}
-
+//  |v| into a running maximum: non-negative doubles order as their bit
+//  patterns, so the warp's maximum goes in with one integer atomicMax
 __device__ __forceinline__ void WarpMaxAbs(unsigned long long *slot, double v)
 {
 	unsigned long long u = (unsigned long long)__double_as_longlong(fabs(v));
@@ -210,7 +205,7 @@ KAssemble(Coef k, int mode, double dt, const int *__restrict__ rowptr,
 		const double hoo = h[oo], coo = c[oo];
 		//  face properties
 		(void)coo;
-		double vis[4], sig[4], DL[4], FM[4], Haj[4];
+		double vis[4], DL[4], FM[4], Haj[4];
 		int fIdx[4];
 		bool fLow[4];
 		FaceSet fs[4];
@@ -220,7 +215,6 @@ KAssemble(Coef k, int mode, double dt, const int *__restrict__ rowptr,
 			Haj[d] = h[AdjIdx(d)];
 			FaceOf(d, i, nx, fb, fs[d], fIdx[d], fLow[d]);
 			vis[d] = fs[d].vis[fIdx[d]];
-			sig[d] = fs[d].sig[fIdx[d]];
 			FM[d] = fs[d].FM[fIdx[d]];
 			DL[d] = fs[d].DL[fIdx[d]];
 		}
