@@ -121,10 +121,18 @@ __global__ void KFaceFlux(Coef k, const double *__restrict__ H, const double *__
 #pragma unroll
 			for(int kk = 0; kk < 5; ++kk) { const int idx = NarrowIdx(kk); pi[idx] = fb.piN[i + OffsetOf(idx, nx)]; }
 		}
-		Fx[i] = FaceFluxSum(k, h, c, s, vis, DL, FM, pi, 1, ix, iy);
-		Fy[i] = FaceFluxSum(k, h, c, s, vis, DL, FM, pi, 3, ix, iy);
-		if(ix == 2) Fx[i - 1] = FaceFluxSum(k, h, c, s, vis, DL, FM, pi, 0, ix, iy);
-		if(iy == 2) Fy[i - nx] = FaceFluxSum(k, h, c, s, vis, DL, FM, pi, 2, ix, iy);
+		//  grid y: the cell's x faces (0) or its y faces (1)
+		if(blockIdx.y == 0)
+		{
+			Fx[i] = FaceFluxSum(k, h, c, s, vis, DL, FM, pi, 1, ix, iy);
+			if(ix == 2) Fx[i - 1] = FaceFluxSum(k, h, c, s, vis, DL, FM, pi, 0, ix, iy);
+		}
+		else
+		{
+			Fy[i] = FaceFluxSum(k, h, c, s, vis, DL, FM, pi, 3, ix, iy);
+			if(iy == 2) Fy[i - nx] = FaceFluxSum(k, h, c, s, vis, DL, FM, pi, 2, ix, iy);
+			continue;
+		}
 		if(evp)
 		{
 			const double xx = k.xmin + ix * k.dx + k.dx2h, yy = k.ymin + iy * k.dy + k.dy2h;

@@ -1335,7 +1335,7 @@ int Step::FaceFluxes(const double *H, const double *C, double *Fx, double *Fy, d
 	int *bad = _iflags.get();
 	YZ_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), _st));
 	FaceProps(H, C, false);
-	YZ_LAUNCH(KFaceFlux, GridFor(nIn, 128, 148 * 32), 128, 0, _st, _k, H, C, _s.get(), Fx, Fy, _evapOld.get(), dt,
+	YZ_LAUNCH(KFaceFlux, dim3(GridFor(nIn, 128, 148 * 16), 2), 128, 0, _st, _k, H, C, _s.get(), Fx, Fy, _evapOld.get(), dt,
 	          withEvap ? _evpStep.get() : nullptr, bad, _fb);
 	int h = 0;
 	YZ_CUDA(cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, _st));
