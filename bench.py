@@ -206,7 +206,7 @@ def run_reference_arm(a) -> None:
             return
         print(json.dumps({
             "impl": "reference", "metric": ENSEMBLE_METRIC, "value": r["value"], "unit": ENSEMBLE_UNIT,
-            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": {"workload": a.config},
             "cpu_baseline": {"value": r["value"], "unit": ENSEMBLE_UNIT, "cores": threads, "kind": "reference",
                              "sample": r["sample"]},
