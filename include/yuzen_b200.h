@@ -237,6 +237,11 @@ typedef struct yz_step_stats
 	long long launches;        /* kernels the call launched */
 	int    conc_iterations;    /* BiCGStab iterations of the concentration solves, summed */
 	int    conc_solves;        /* concentration solves */
+	/* with the energy history on (yz_step_set_energy): after the call, the
+	 * free energy and flux power of the film, the energy dissipated since
+	 * the history started and the balance of the last step
+	 * (WellMixedModelBase.h:1405-1411); 0 otherwise */
+	double energy_F, energy_D, energy_dissipated, energy_balance;
 } yz_step_stats;
 
 /* Build the step: fields h, c, s on all nx*ny points (host arrays). */
@@ -246,6 +251,11 @@ int yz_step_destroy(yz_step* st);
 /* Preconditioner arithmetic (YZ_PREC_*) of the step's height and
  * concentration solves, from the next solve on; FP64 unless set. */
 int yz_step_set_precision(yz_step* st, int precision);
+/* The energy history (Output.Energy): on = 1 evaluates the budget of the
+ * present film (yz_step_energy) and starts the dissipated energy at 0; every
+ * later step evaluates it at the film it ends on and adds the step's
+ * Crank-Nicolson share of the flux power (WellMixedModelBase.h:1405-1411). */
+int yz_step_set_energy(yz_step* st, int on);
 /* AMG hierarchy reuse (yz_solver_set_amg_reuse) for the step's solves. */
 int yz_step_set_amg_reuse(yz_step* st, int max_solves);
 /* The graph form of the step's BiCGStab loops (yz_solver_set_graph_loop). */

@@ -186,6 +186,9 @@ int main(int argc, char **argv)
 	put(D, std::chrono::duration<double>(t1 - t0).count());
 	put(D, m->_timeStep.NowTime());
 	put(D, enF0); put(D, enD0); put(D, enF1); put(D, enD1);
+	//  with Output.Energy, the energy dissipated over the run and the balance
+	//  of its last step (WellMixedModelBase.h:1405-1411)
+	put(D, m->_enDiss); put(D, m->_enBal);
 	put(I, (int)m->_timeStep.TimeStep());
 	put(I, m->Diverged() ? 1 : 0);
 

@@ -186,7 +186,7 @@ def write_case(ref: Path, src: str, over: dict, name: str, work: Path) -> Path:
 
 def make_step_case(ref: Path, name: str, work: Path) -> dict:
     src, over, steps, first = STEP_CASES[name]
-    case = write_case(ref, src, {**over, "Numerics.MaxSteps": steps}, name, work)
+    case = write_case(ref, src, {**over, "Numerics.MaxSteps": steps, "Output.Energy.Enable": True}, name, work)
     dump = work / f"dump_{name}"
     dump.mkdir()
     env = dict(os.environ, YZO_DUMP_DIR=str(dump), YZO_DUMP_MAX="8", OMP_NUM_THREADS="4")
@@ -220,7 +220,11 @@ def make_built_step_case(name: str, work: Path) -> dict:
     builder, kw = BUILT_STEP_CASES[name]
     case = getattr(cases, builder)(**kw)
     w = work / name
-    case.write_reference(w)
+    toml_path = case.write_reference(w)
+    #  the reference keeps its energy history (Output.Energy)
+    doc = tomllib.loads(Path(toml_path).read_text())
+    tomlw.setpath(doc, "Output.Energy.Enable", True)
+    Path(toml_path).write_text(tomlw.dumps(doc))
     dump = (w / "dump").resolve()
     dump.mkdir()
     #  the restart's set-up solves of the boundary rows come first

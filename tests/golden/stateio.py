@@ -30,6 +30,8 @@ REAL_KEYS = (
     "run_seconds", "t_end",
     # the energy budget (EnergyEval) of the start and the end film
     "energy_F0", "energy_D0", "energy_F1", "energy_D1",
+    # with Output.Energy: the energy dissipated over the run, the last step's balance
+    "energy_dissipated", "energy_balance",
 )
 #  BoundaryCondition::tBoundaryCondition (model/BoundaryCondition.h)
 BC_NAMES = {0: "Symmetry", 1: "Periodic", 2: "Pinning", 3: "FreshInlet", 4: "Outlet"}

@@ -185,3 +185,23 @@ def test_fields_after_steps_fp32_matrix_amg_reuse(f):
     if d["conc_field"]:
         cref = d["field_c1"]
         assert np.linalg.norm(c - cref) / np.linalg.norm(cref) <= 1e-8
+
+
+@pytest.mark.parametrize("f", STEPS, ids=IDS)
+def test_energy_history(f):
+    """The energy history (Output.Energy) over the fixture's steps against
+    the reference's own: the budget of the film the run ends on, the energy
+    dissipated over the run (the trapezoid of the flux power over every
+    step's dt) to 1e-12 relative, and the balance of the last step, a
+    difference of energies over dt that is near 0 when the scheme is
+    consistent, to 1e-9 of the flux power."""
+    d = stateio.load_npz(f)
+    st = make(d)
+    st.set_energy(True)
+    s = st.advance(d["steps_done"])
+    scale_d = max(abs(d["energy_D0"]), abs(d["energy_D1"]), 1e-300)
+    assert abs(s["energy_F"] - d["energy_F1"]) <= 1e-12 * abs(d["energy_F1"]), (s["energy_F"], d["energy_F1"])
+    assert abs(s["energy_D"] - d["energy_D1"]) <= 1e-12 * scale_d, (s["energy_D"], d["energy_D1"])
+    assert abs(s["energy_dissipated"] - d["energy_dissipated"]) <= 1e-12 * abs(d["energy_dissipated"]) + 1e-300, \
+        (s["energy_dissipated"], d["energy_dissipated"])
+    assert abs(s["energy_balance"] - d["energy_balance"]) <= 1e-9 * scale_d, (s["energy_balance"], d["energy_balance"])

@@ -39,6 +39,7 @@ EXPORTED_SYMBOLS = (
     "yz_time_kernel", "yz_kernel_time", "yz_dot_noalloc", "yz_dot_noalloc_max",
     "yz_step_conc_pattern", "yz_step_conc_system", "yz_step_set_precision", "yz_solver_set_amg_reuse",
     "yz_step_set_amg_reuse", "yz_solver_set_graph_loop", "yz_step_set_graph_loop", "yz_step_energy",
+    "yz_step_set_energy",
 )
 
 #: the preconditioner's arithmetic (YZ_PREC_* of include/yuzen_b200.h)

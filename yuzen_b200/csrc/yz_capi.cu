@@ -250,6 +250,15 @@ int yz_step_set_graph_loop(yz_step *st, int on)
 	});
 }
 
+int yz_step_set_energy(yz_step *st, int on)
+{
+	return Guard([&] {
+		if(!st) throw yz::UsageError("yz_step_set_energy: null step");
+		st->s->SetEnergy(on != 0);
+		return 0;
+	});
+}
+
 int yz_step_energy(yz_step *st, double *F, double *D)
 {
 	return Guard([&] {

@@ -1138,6 +1138,16 @@ void Step::Advance(int nsteps, yz_step_stats &stats)
 		//  (ConcCommit); the field takes the film
 		if(_conc) ConcCommit(_dt, stats);
 		YZ_CUDA(cudaMemcpyAsync(_h.get(), _guess.get(), bytes, cudaMemcpyDeviceToDevice, _st));
+		//  the energy budget of the film the step reached, the energy
+		//  dissipated over the step at its Crank-Nicolson weighting, and
+		//  the balance (WellMixedModelBase.h:1405-1411)
+		if(_energyOn)
+		{
+			const double f0 = _enF, d0 = _enD;
+			Energy(_enF, _enD);
+			_enDiss += 0.5 * (d0 + _enD) * _dt;
+			_enBal = (_enF - f0) / _dt + 0.5 * (d0 + _enD);
+		}
 		//  the clock: ++ (TimeSteps.cpp:121-160)
 		_time += _dt;
 		_dtOld = _dt;
@@ -1147,6 +1157,11 @@ void Step::Advance(int nsteps, yz_step_stats &stats)
 	}
 	stats.time = _time;
 	stats.dt = _dt;
+	if(_energyOn)
+	{
+		stats.energy_F = _enF; stats.energy_D = _enD;
+		stats.energy_dissipated = _enDiss; stats.energy_balance = _enBal;
+	}
 	YZ_CUDA(cudaEventRecord(_eB, _st));
 	YZ_CUDA(cudaEventSynchronize(_eB));
 	float ms = 0;
@@ -1200,6 +1215,13 @@ void Step::Energy(double &F, double &D)
 	YZ_CUDA(cudaStreamSynchronize(_st));
 	F = out[0];
 	D = out[1];
+}
+
+void Step::SetEnergy(bool on)
+{
+	_energyOn = on;
+	_enDiss = 0; _enBal = 0;
+	if(on) Energy(_enF, _enD);
 }
 
 void Step::GetFields(double *h, double *c)

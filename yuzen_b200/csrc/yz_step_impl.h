@@ -21,6 +21,7 @@ public:
 	void Advance(int nsteps, yz_step_stats &stats);
 	void GetFields(double *h, double *c);
 	void Energy(double &F, double &D);
+	void SetEnergy(bool on);
 	void SetFields(const double *h, const double *c);
 	int Pattern(int *rowptr, int *col, int *bc) const;
 	void System(const double *hOld, const double *h, double dt, double *ia, double *rhs);
@@ -86,6 +87,9 @@ private:
 	DBuf<double> _faceMem;
 	DBuf<double> _enFx, _enFy, _enOut;       // the energy budget's face fluxes and its two sums
 	DBuf<double> _upMem;                     // the limited upwind terms' faces (UpBuf)
+	//  the energy history (Output.Energy)
+	bool _energyOn = false;
+	double _enF = 0, _enD = 0, _enDiss = 0, _enBal = 0;
 	phys::FaceBuf _fb;
 	//  the concentration equation: its pattern and solver; c0 (its phi_old),
 	//  the working field's c, the limiter state, the c of the last pass,

@@ -55,6 +55,8 @@ class StepStats(ctypes.Structure):
         ("last_resid", ctypes.c_double), ("setup_ms", ctypes.c_double), ("solve_ms", ctypes.c_double),
         ("assemble_ms", ctypes.c_double), ("device_ms", ctypes.c_double), ("launches", ctypes.c_longlong),
         ("conc_iterations", ctypes.c_int), ("conc_solves", ctypes.c_int),
+        ("energy_F", ctypes.c_double), ("energy_D", ctypes.c_double),
+        ("energy_dissipated", ctypes.c_double), ("energy_balance", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -113,6 +115,7 @@ def _bind():
     L.yz_step_set_amg_reuse.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_step_set_graph_loop.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_step_energy.argtypes = [ctypes.c_void_p, _f64p, _f64p]
+    L.yz_step_set_energy.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_step_get_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
     L.yz_step_set_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
     L.yz_launch_count.restype = ctypes.c_longlong
@@ -163,6 +166,12 @@ class Step:
         F, D = ctypes.c_double(), ctypes.c_double()
         _check(lib().yz_step_energy(self._h, ctypes.byref(F), ctypes.byref(D)), "yz_step_energy")
         return F.value, D.value
+
+    def set_energy(self, on: bool) -> None:
+        """The energy history (Output.Energy): the budget of the present film,
+        then every step's, with the energy dissipated and the last step's
+        balance in advance()'s stats (yz_step_set_energy)."""
+        _check(lib().yz_step_set_energy(self._h, int(bool(on))), "yz_step_set_energy")
 
     def advance(self, nsteps: int = 1) -> dict:
         st = StepStats()
