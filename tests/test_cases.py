@@ -1,5 +1,6 @@
-"""The seeded case builder (yuzen_b200/cases.py) against the reference's own
-set-up: the case is written in the reference's format, the whole-step probe
+"""The seeded case builders (yuzen_b200/cases.py: the spinodal film, the
+all-physics film, an instance of the batched ensemble) against the
+reference's own set-up: the case is written in the reference's format, the whole-step probe
 (the reference's C_Yuzen driver, oracle/probe/yz_probe.cpp) builds it, and
 the non-dimensional state it hands the step -- every header value and the
 fields h, c, s -- must equal the builder's to the bit.  Needs the probe
@@ -36,7 +37,9 @@ def _probe(case: cases.Case, work: Path) -> dict:
 
 
 @pytest.mark.parametrize("make", [lambda: cases.spinodal_224(N=24, steps=1),
-                                  lambda: cases.allphys(N=24, steps=1)], ids=["spinodal_24", "allphys_24"])
+                                  lambda: cases.allphys(N=24, steps=1),
+                                  lambda: cases.dewetting(24, theta_e=13.7, amp=3e-3, seed=5, steps=1)],
+                         ids=["spinodal_24", "allphys_24", "dewetting_24"])
 def test_state_bitwise(make, tmp_path):
     case = make()
     ref = _probe(case, tmp_path)
