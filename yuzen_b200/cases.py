@@ -15,7 +15,7 @@ doubles, math.pow/sqrt/atan are the C library's), so the state it hands the
 device is the reference's own to the bit; tests/test_cases.py checks that
 against the whole-step probe.
 
-    cfg = spinodal_224()
+    cfg = spinodal_224()              # the 224^2 spinodal film
     state = cfg.state()               # dict: params + fields (nx*ny each)
     cfg.write_reference(workdir)      # case.toml + init.dat for the reference
 """
@@ -358,10 +358,10 @@ class Case:
 
 
 # ----------------------------------------------------------------------
-#  the BASELINE configurations (seeded synthetic inputs)
+#  the benchmark workloads (seeded synthetic inputs)
 # ----------------------------------------------------------------------
 def spinodal_224(N: int = 224, seed: int = 20261203, steps: int = 12, end_time: float = 0.8) -> Case:
-    """Config 2: spinodal dewetting of a periodic film, capillary + disjoining
+    """Spinodal dewetting of a periodic 224^2 film, capillary + disjoining
     pressure, theta_e = 10 deg, h* = 0.01 h0, h = 1 + 1e-3 U(-1, 1), adaptive dt."""
     rng = np.random.default_rng(seed)
     h = 1.0 + 1e-3 * rng.uniform(-1.0, 1.0, size=(N, N))
@@ -396,7 +396,7 @@ def batch(count: int = 256, seed: int = 20261204, sizes=(64, 96, 128, 192, 256),
 
 
 def allphys(N: int = 512, steps: int = 12, dt: float = 1e-5) -> Case:
-    """Config 3: every term of the well-mixed model on an N x N film with
+    """The all-physics film: every term of the well-mixed model on an N x N film with
     Symmetry edges.  A film edge along a 30 degree oblique tanh front
     (h = 1 behind it, the precursor 0.01 ahead, the front 8 cells wide),
     Bo = 0.5, Pg = (0.2, 0.1), Sp = 0.3 about the centre, As Ma = 0.05,
