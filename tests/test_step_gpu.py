@@ -205,3 +205,24 @@ def test_energy_history(f):
     assert abs(s["energy_dissipated"] - d["energy_dissipated"]) <= 1e-12 * abs(d["energy_dissipated"]) + 1e-300, \
         (s["energy_dissipated"], d["energy_dissipated"])
     assert abs(s["energy_balance"] - d["energy_balance"]) <= 1e-9 * scale_d, (s["energy_balance"], d["energy_balance"])
+
+
+def test_precision_switch_mid_run():
+    """The arithmetic of the solves switched between steps, with hierarchy
+    reuse on: the hierarchy set up in FP64 is not reused by the FP32 cycle
+    (a change of precision sets up afresh), and the run still ends within
+    the 1e-8 bar of the reference's."""
+    f = [p for p in STEPS if p.stem == "step_allphys_64"][0]
+    d = stateio.load_npz(f)
+    st = make(d)
+    st.set_amg_reuse(8)
+    n = int(d["steps_done"])
+    st.advance(1)
+    st.set_precision(1)
+    st.advance(n - 2)
+    st.set_precision(0)
+    stats = st.advance(1)
+    h, _ = st.fields()
+    ref = d["field_h1"]
+    assert np.linalg.norm(h - ref) / np.linalg.norm(ref) <= 1e-8
+    assert abs(stats["time"] - d["t_end"]) <= 1e-12 * abs(d["t_end"])

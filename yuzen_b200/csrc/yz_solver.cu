@@ -784,7 +784,13 @@ void Solver::SetPrecision(int precision)
 {
 	if(precision != YZ_PREC_FP64 && precision != YZ_PREC_FP32_CYCLE && precision != YZ_PREC_FP32_MATRIX)
 		throw UsageError("set_precision: precision must be YZ_PREC_FP64, YZ_PREC_FP32_CYCLE or YZ_PREC_FP32_MATRIX");
-	if(precision != _precision) ++_epoch;
+	if(precision != _precision)
+	{
+		++_epoch;
+		//  a hierarchy set up in the other precision has no (or stale)
+		//  float copies: the next AMG solve sets up afresh
+		_stale = true;
+	}
 	_precision = precision;
 }
 
