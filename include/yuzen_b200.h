@@ -7,6 +7,13 @@
  *    2  a solve broke down or produced NaN
  *   -1  usage error (bad argument, wrong order of calls)
  *   -2  CUDA error
+ *   -3  the time step failed numerically (yz_step_advance only): dt fell
+ *       below MinDt, or the Newton iteration did not converge at a fixed
+ *       step -- the cases where the reference aborts with FatalError
+ *       (ImplicitSolver.cpp:180-184, :192-201); the message is the
+ *       reference's.  The step context is then left mid-step (its dt and
+ *       Newton guess changed): restore it with yz_step_set_fields (or
+ *       yz_step_set_state) before advancing it again.
  * yz_last_error() describes the last non-zero status of the calling thread.
  * No exception crosses this boundary.  A context is used from one host
  * thread at a time and owns one CUDA stream and all its device buffers.
@@ -149,7 +156,11 @@ int yz_spmv(int n, int nnz, const int* rowptr, const int* col, const double* val
  * yz_dot_noalloc_max() elements (16,777,216); larger n returns -1.  The
  * array is shared by every call, so calls that overlap on the GPU race; the
  * first call on a device takes the array's address (cudaGetSymbolAddress)
- * and should come before any stream capture. */
+ * and should come before any stream capture.  That address is kept per
+ * device index for the life of the process and belongs to the device's
+ * primary context: after cudaDeviceReset, or from a thread whose current
+ * context is a non-primary driver context, the kept address is stale and
+ * the call must not be used. */
 int yz_dot_noalloc(int n, const double* d_x, const double* d_y, double* d_out, void* stream);
 long long yz_dot_noalloc_max(void);
 
@@ -242,6 +253,7 @@ typedef struct yz_step_stats
 	 * the history started and the balance of the last step
 	 * (WellMixedModelBase.h:1405-1411); 0 otherwise */
 	double energy_F, energy_D, energy_dissipated, energy_balance;
+	int    amg_setups;         /* SA-AMG hierarchies set up (height and concentration solves) */
 } yz_step_stats;
 
 /* Build the step: fields h, c, s on all nx*ny points (host arrays). */

@@ -217,11 +217,18 @@ def test_precision_switch_mid_run():
     st = make(d)
     st.set_amg_reuse(8)
     n = int(d["steps_done"])
-    st.advance(1)
+    assert n >= 3
+    first = st.advance(1)
+    assert first["amg_setups"] >= 1
     st.set_precision(1)
-    st.advance(n - 2)
+    # the first step after the switch sets up afresh, a later one reuses
+    assert st.advance(1)["amg_setups"] >= 1
+    if n > 3:
+        later = st.advance(n - 3)
+        assert later["amg_setups"] < later["newton_iterations"], later
     st.set_precision(0)
     stats = st.advance(1)
+    assert stats["amg_setups"] >= 1
     h, _ = st.fields()
     ref = d["field_h1"]
     assert np.linalg.norm(h - ref) / np.linalg.norm(ref) <= 1e-8

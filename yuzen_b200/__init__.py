@@ -49,7 +49,17 @@ PREC_FP32_MATRIX = 2
 
 
 class YzError(RuntimeError):
-    """A non-zero status of the C ABI (-1 usage error, -2 CUDA error)."""
+    """A negative status of the C ABI (-1 usage error, -2 CUDA error, -3 a
+    failed time step); `status` holds it."""
+
+    def __init__(self, msg: str, status: int = -2):
+        super().__init__(msg)
+        self.status = status
+
+
+class StepFailedError(YzError):
+    """Status -3: the time step failed numerically where the reference aborts
+    with its FatalError (dt below MinDt; no convergence at a fixed step)."""
 
 
 def lib_path() -> Path:
@@ -107,7 +117,8 @@ def lib():
 def _check(status: int, what: str) -> int:
     if status < 0:
         msg = lib().yz_last_error().decode(errors="replace")
-        raise YzError(f"{what}: status {status}: {msg}")
+        cls = StepFailedError if status == -3 else YzError
+        raise cls(f"{what}: status {status}: {msg}", status)
     return status
 
 

@@ -20,6 +20,7 @@ template<class F> int Guard(F &&f)
 {
 	try { return f(); }
 	catch(const yz::UsageError &e) { yz::SetLastError(e.what()); return -1; }
+	catch(const yz::StepFailed &e) { yz::SetLastError(e.what()); return -3; }
 	catch(const yz::CudaError &e) { yz::SetLastError(e.what()); return -2; }
 	catch(const std::exception &e) { yz::SetLastError(e.what()); return -2; }
 	catch(...) { yz::SetLastError("unknown error"); return -2; }

@@ -11,18 +11,22 @@ thread_local long long t_launches = 0;
 //  per-launch timing of one kernel (yz_time_kernel)
 namespace {
 std::mutex g_timeMutex;
-std::string g_timeName;
+std::string g_timeName;                       // read and written under g_timeMutex
+std::atomic<bool> g_timeOn{false};            // a name is selected (the launch path's fast test)
 std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_timePairs;
-cudaEvent_t g_timeOpen = nullptr;
+//  the event that opens a timed launch, per host thread: contexts driven
+//  from several threads at once each pair their own events
+thread_local cudaEvent_t t_timeOpen = nullptr;
 }
 
 bool TimedKernel(const char *name)
 {
-	if(g_timeName.empty()) return false;
-	return g_timeName == name;
+	if(!g_timeOn.load(std::memory_order_acquire)) return false;
+	std::lock_guard<std::mutex> lk(g_timeMutex);
+	return !g_timeName.empty() && g_timeName == name;
 }
 
-bool TimingActive() { return !g_timeName.empty(); }
+bool TimingActive() { return g_timeOn.load(std::memory_order_acquire); }
 
 void TimeBegin(cudaStream_t st)
 {
@@ -30,7 +34,7 @@ void TimeBegin(cudaStream_t st)
 	cudaEvent_t e;
 	Check(cudaEventCreate(&e), "cudaEventCreate");
 	Check(cudaEventRecord(e, st), "cudaEventRecord");
-	g_timeOpen = e;
+	t_timeOpen = e;
 }
 
 void TimeEnd(cudaStream_t st)
@@ -39,8 +43,8 @@ void TimeEnd(cudaStream_t st)
 	cudaEvent_t e;
 	Check(cudaEventCreate(&e), "cudaEventCreate");
 	Check(cudaEventRecord(e, st), "cudaEventRecord");
-	g_timePairs.push_back({g_timeOpen, e});
-	g_timeOpen = nullptr;
+	g_timePairs.push_back({t_timeOpen, e});
+	t_timeOpen = nullptr;
 }
 
 long long TimeCount()
@@ -67,6 +71,7 @@ void TimeSelect(const char *name)
 	for(auto &p : g_timePairs) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
 	g_timePairs.clear();
 	g_timeName = name ? name : "";
+	g_timeOn.store(!g_timeName.empty(), std::memory_order_release);
 }
 
 void TimeRead(double *ms, long long *count)

@@ -26,6 +26,13 @@ struct UsageError : std::runtime_error
 {
 	explicit UsageError(const std::string &m) : std::runtime_error(m) {}
 };
+//  a numerical failure of the time step (the reference's FatalError at the
+//  step: dt below MinDt, ImplicitSolver.cpp:180-184; no convergence at a
+//  fixed step, FailedFixedStep, ImplicitSolver.cpp:192-201)
+struct StepFailed : std::runtime_error
+{
+	explicit StepFailed(const std::string &m) : std::runtime_error(m) {}
+};
 
 inline void Check(cudaError_t e, const char *what)
 {

@@ -16,7 +16,9 @@
 // zero is cleared by each call before its kernel.  The device address of the
 // array is taken once per device, on the first call made with that device
 // current, by cudaGetSymbolAddress; that first call should come before any
-// stream capture.
+// stream capture.  The address is kept per device index for the life of the
+// process and belongs to the device's primary context: after cudaDeviceReset,
+// or under a non-primary driver context, it is stale.
 #include "yz_common.cuh"
 
 #include <array>

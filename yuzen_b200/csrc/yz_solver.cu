@@ -1081,7 +1081,10 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 			//  in the cycle is the new matrix itself)
 			for(;;)
 			{
-				const bool reuse = _amgReuse > 0 && _haveH && !_stale && _sinceBuild < _amgReuse;
+				//  a float cycle runs only on a hierarchy that has its float
+				//  copies (one set up, or rounded, in a float precision)
+				const bool reuse = _amgReuse > 0 && _haveH && !_stale && _sinceBuild < _amgReuse &&
+				                   (!fp32 || _hPrec != YZ_PREC_FP64);
 				if(reuse)
 				{
 					Level &F = *_levels[0];
@@ -1101,6 +1104,7 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 				{
 					BuildHierarchy(n > 3000 ? 500 : 3000);
 					if(fp32) RoundCycle();
+					_hPrec = _precision;
 					_sinceBuild = 0;
 					_stale = false;
 				}

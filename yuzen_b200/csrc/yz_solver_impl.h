@@ -163,6 +163,7 @@ private:
 	//  hierarchy reuse (0: a new set-up every solve, the reference's way)
 	int _amgReuse = 0, _sinceBuild = 0, _freshIters = 0, _rebuilds = 0;
 	bool _stale = false;
+	int _hPrec = YZ_PREC_FP64;    // the precision the present hierarchy was set up in
 	//  bumped whenever a pointer or size a loop graph holds may change: the
 	//  pattern, precision or buffers (_epoch), the hierarchy (_epochH)
 	unsigned _epoch = 0, _epochH = 0;

@@ -1013,9 +1013,11 @@ bool Step::NKLoop(int &iter, double &resid, yz_step_stats &stats)
 		ls.epsilon = eps;
 		ls.conc = 0;
 		int it = 0; double res = 0;
+		const int r0 = _solver->Rebuilds();
 		const int ch = _solver->Solve(ls, _ia.get(), _rhs.get(), _delta.get(), it, res);
 		double su = 0, sit = 0; _solver->Timing(&su, &sit);
 		stats.setup_ms += su; stats.solve_ms += sit;
+		stats.amg_setups += _solver->Rebuilds() - r0;
 		stats.linear_iterations += it;
 		ZeroMax(kSlotDelta);
 		if(ch == 0)
@@ -1122,14 +1124,19 @@ void Step::Advance(int nsteps, yz_step_stats &stats)
 				else
 				{
 					dtNext *= _p.dt_change_factor;
-					if(dtNext < _p.dt_min) throw CudaError("step: dt fell below Numerics.TimeStepControl.MinDt");
+					if(dtNext < _p.dt_min)
+						throw StepFailed("TimeStepAdjustment(). Under flow: the requested step fell below "
+						                 "Numerics.TimeStepControl.MinDt.");
 					if(!(dtNext < _p.dt_min || _p.dt_max < dtNext)) _dt = dtNext;
 					++stats.retries;
 				}
 			}
 			else
 			{
-				if(!ch) throw CudaError("step: the Newton iteration did not converge at the fixed step");
+				if(!ch)
+					throw StepFailed("Newton-Kantorovich: the step did not converge at the fixed step, and with "
+					                 "Numerics.TimeStepControl.Enable = false it cannot be retried at a shorter "
+					                 "one. Shorten Numerics.InitialDt or enable the time-step control.");
 				timeStepDone = true;
 			}
 		} while(!timeStepDone);
@@ -1381,9 +1388,11 @@ void Step::ConcAssemble(double dt)
 int Step::ConcSolve(yz_step_stats &stats)
 {
 	int it = 0; double res = 0;
+	const int r0 = _solverC->Rebuilds();
 	const int ch = _solverC->Solve(_p.lin_conc, _iaC.get(), _rhsC.get(), _dC.get(), it, res);
 	double su = 0, sit = 0; _solverC->Timing(&su, &sit);
 	stats.setup_ms += su; stats.solve_ms += sit;
+	stats.amg_setups += _solverC->Rebuilds() - r0;
 	stats.conc_iterations += it;
 	stats.conc_solves += 1;
 	return ch;

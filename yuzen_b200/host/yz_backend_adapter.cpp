@@ -12,7 +12,7 @@
  *     if(name == "b200") return MakeB200LinearSolverBackend();
  *
  * oracle/Makefile builds the reference's driver with it (target b200) for
- * the drop-in test; INTEGRATION.md shows the same lines for a maintainer.
+ * the drop-in test.
  */
 #include "LinearSolverBackend.h"
 #include "CRS_Matrix.h"

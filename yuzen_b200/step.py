@@ -57,6 +57,7 @@ class StepStats(ctypes.Structure):
         ("conc_iterations", ctypes.c_int), ("conc_solves", ctypes.c_int),
         ("energy_F", ctypes.c_double), ("energy_D", ctypes.c_double),
         ("energy_dissipated", ctypes.c_double), ("energy_balance", ctypes.c_double),
+        ("amg_setups", ctypes.c_int),
     ]
 
     def as_dict(self) -> dict:
