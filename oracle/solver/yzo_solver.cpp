@@ -77,8 +77,11 @@ template<class F> double DetSum(int n, F f)
 	const int nb = (n + kRChunk - 1) / kRChunk;
 	std::vector<double> part((size_t)(nb > 0 ? nb : 1), 0.0);
 	double s[kRT];
+	//  the chunks' sums are independent, each its own fixed tree
+#pragma omp parallel for schedule(static) if(nb > 16)
 	for(int b = 0; b < nb; ++b)
 	{
+		double s[kRT];
 		for(int t = 0; t < kRT; ++t)
 		{
 			double a = 0.0;
@@ -91,6 +94,7 @@ template<class F> double DetSum(int n, F f)
 		}
 		part[(size_t)b] = Tree256(s);
 	}
+#pragma omp parallel for schedule(static) if(nb > 4096)
 	for(int t = 0; t < kRT; ++t)
 	{
 		double a = 0.0;
@@ -118,6 +122,7 @@ struct Csr
 
 void Spmv(const Csr &A, const double *x, double *y)
 {
+#pragma omp parallel for schedule(static)
 	for(int i = 0; i < A.n; ++i)
 	{
 		double s = 0.0;
@@ -131,6 +136,7 @@ void Spmv(const Csr &A, const double *x, double *y)
 //  the order the device's four lanes per row take
 void Restrict(const Csr &R, const double *t, double *y)
 {
+#pragma omp parallel for schedule(static)
 	for(int i = 0; i < R.n; ++i)
 	{
 		double p[4] = {0.0, 0.0, 0.0, 0.0};
@@ -142,6 +148,7 @@ void Restrict(const Csr &R, const double *t, double *y)
 
 void Residual(const Csr &A, const double *f, const double *x, double *r)
 {
+#pragma omp parallel for schedule(static)
 	for(int i = 0; i < A.n; ++i)
 	{
 		double s = 0.0;
@@ -160,6 +167,7 @@ double DiagOf(const Csr &A, int i)
 void Spai0(const Csr &A, std::vector<double> &M)
 {
 	M.assign((size_t)A.n, 0.0);
+#pragma omp parallel for schedule(static)
 	for(int i = 0; i < A.n; ++i)
 	{
 		double num = 0.0, den = 0.0;
@@ -179,26 +187,44 @@ void Multiply(const Csr &X, const Csr &Y, Csr &C)
 	C.n = X.n; C.m = Y.m;
 	C.ptr.assign((size_t)C.n + 1, 0);
 	C.col.clear(); C.val.clear();
-	std::vector<int> marker((size_t)Y.m, -1);
-	std::vector<double> acc((size_t)Y.m, 0.0);
-	std::vector<int> cols;
+	//  every row on its own (rows in parallel, each with its own marker and
+	//  accumulator), then the rows laid end to end
+	std::vector<std::vector<int>> rc((size_t)X.n);
+	std::vector<std::vector<double>> rv((size_t)X.n);
+#pragma omp parallel
+	{
+		std::vector<int> marker((size_t)Y.m, -1);
+		std::vector<double> acc((size_t)Y.m, 0.0);
+		std::vector<int> cols;
+#pragma omp for schedule(static)
+		for(int i = 0; i < X.n; ++i)
+		{
+			cols.clear();
+			for(int kx = X.ptr[(size_t)i]; kx < X.ptr[(size_t)i + 1]; ++kx)
+			{
+				const int k = X.col[(size_t)kx];
+				const double xv = X.val[(size_t)kx];
+				for(int ky = Y.ptr[(size_t)k]; ky < Y.ptr[(size_t)k + 1]; ++ky)
+				{
+					const int j = Y.col[(size_t)ky];
+					if(marker[(size_t)j] != i) { marker[(size_t)j] = i; acc[(size_t)j] = 0.0; cols.push_back(j); }
+					acc[(size_t)j] = acc[(size_t)j] + xv * Y.val[(size_t)ky];
+				}
+			}
+			std::sort(cols.begin(), cols.end());
+			rc[(size_t)i] = cols;
+			rv[(size_t)i].resize(cols.size());
+			for(size_t q = 0; q < cols.size(); ++q) rv[(size_t)i][q] = acc[(size_t)cols[q]];
+		}
+	}
+	for(int i = 0; i < X.n; ++i) C.ptr[(size_t)i + 1] = C.ptr[(size_t)i] + (int)rc[(size_t)i].size();
+	C.col.resize((size_t)C.ptr[(size_t)X.n]);
+	C.val.resize((size_t)C.ptr[(size_t)X.n]);
+#pragma omp parallel for schedule(static)
 	for(int i = 0; i < X.n; ++i)
 	{
-		cols.clear();
-		for(int kx = X.ptr[(size_t)i]; kx < X.ptr[(size_t)i + 1]; ++kx)
-		{
-			const int k = X.col[(size_t)kx];
-			const double xv = X.val[(size_t)kx];
-			for(int ky = Y.ptr[(size_t)k]; ky < Y.ptr[(size_t)k + 1]; ++ky)
-			{
-				const int j = Y.col[(size_t)ky];
-				if(marker[(size_t)j] != i) { marker[(size_t)j] = i; acc[(size_t)j] = 0.0; cols.push_back(j); }
-				acc[(size_t)j] = acc[(size_t)j] + xv * Y.val[(size_t)ky];
-			}
-		}
-		std::sort(cols.begin(), cols.end());
-		for(int j : cols) { C.col.push_back(j); C.val.push_back(acc[(size_t)j]); }
-		C.ptr[(size_t)i + 1] = (int)C.col.size();
+		std::copy(rc[(size_t)i].begin(), rc[(size_t)i].end(), C.col.begin() + C.ptr[(size_t)i]);
+		std::copy(rv[(size_t)i].begin(), rv[(size_t)i].end(), C.val.begin() + C.ptr[(size_t)i]);
 	}
 }
 
@@ -245,9 +271,11 @@ uint64_t Pack(int state, int i)
 void Strength(const Csr &A, double eps, std::vector<char> &strong, std::vector<double> &dia)
 {
 	dia.assign((size_t)A.n, 0.0);
+#pragma omp parallel for schedule(static)
 	for(int i = 0; i < A.n; ++i) dia[(size_t)i] = DiagOf(A, i);
 	strong.assign((size_t)A.nnz(), 0);
 	const double eps2 = eps * eps;
+#pragma omp parallel for schedule(static)
 	for(int i = 0; i < A.n; ++i)
 	{
 		const double e = eps2 * dia[(size_t)i];
@@ -294,9 +322,13 @@ int Aggregate(const Csr &A, const std::vector<char> &strong, std::vector<int> &a
 		bool undecided = false;
 		for(int i = 0; i < n; ++i) if(state[(size_t)i] == kUndecided) { undecided = true; break; }
 		if(!undecided) break;
+#pragma omp parallel for schedule(static)
 		for(int i = 0; i < n; ++i) T0[(size_t)i] = Pack(state[(size_t)i], i);
+#pragma omp parallel for schedule(static)
 		for(int i = 0; i < n; ++i) { uint64_t m = T0[(size_t)i]; forNbr(i, [&](int j) { m = std::max(m, T0[(size_t)j]); }); T1[(size_t)i] = m; }
+#pragma omp parallel for schedule(static)
 		for(int i = 0; i < n; ++i) { uint64_t m = T1[(size_t)i]; forNbr(i, [&](int j) { m = std::max(m, T1[(size_t)j]); }); T2[(size_t)i] = m; }
+#pragma omp parallel for schedule(static)
 		for(int i = 0; i < n; ++i)
 		{
 			if(state[(size_t)i] != kUndecided) continue;
@@ -310,6 +342,7 @@ int Aggregate(const Csr &A, const std::vector<char> &strong, std::vector<int> &a
 	for(int i = 0; i < n; ++i) if(state[(size_t)i] == kIn) agg[(size_t)i] = nc++;
 	//  first pass: the adjacent root
 	std::vector<int> first(agg);
+#pragma omp parallel for schedule(static)
 	for(int i = 0; i < n; ++i)
 	{
 		if(state[(size_t)i] == kIn || isolated[(size_t)i]) continue;
@@ -319,6 +352,7 @@ int Aggregate(const Csr &A, const std::vector<char> &strong, std::vector<int> &a
 	}
 	//  second pass: a neighbour placed by the first
 	std::vector<int> second(first);
+#pragma omp parallel for schedule(static)
 	for(int i = 0; i < n; ++i)
 	{
 		if(first[(size_t)i] >= 0 || isolated[(size_t)i]) continue;
@@ -337,8 +371,14 @@ void SmoothedP(const Csr &A, const std::vector<char> &strong, const std::vector<
 	P.n = A.n; P.m = nc;
 	P.ptr.assign((size_t)A.n + 1, 0);
 	P.col.clear(); P.val.clear();
+	//  every row on its own (rows in parallel), then laid end to end
+	std::vector<std::vector<int>> rc((size_t)A.n);
+	std::vector<std::vector<double>> rv((size_t)A.n);
+#pragma omp parallel
+	{
 	std::vector<int> lc; std::vector<double> lv;
 	std::vector<int> order;
+#pragma omp for schedule(static)
 	for(int i = 0; i < A.n; ++i)
 	{
 		double dia = 0.0;
@@ -361,8 +401,17 @@ void SmoothedP(const Csr &A, const std::vector<char> &strong, const std::vector<
 		order.resize(lc.size());
 		for(size_t q = 0; q < lc.size(); ++q) order[q] = (int)q;
 		std::sort(order.begin(), order.end(), [&](int a, int b) { return lc[(size_t)a] < lc[(size_t)b]; });
-		for(int q : order) { P.col.push_back(lc[(size_t)q]); P.val.push_back(lv[(size_t)q]); }
-		P.ptr[(size_t)i + 1] = (int)P.col.size();
+		for(int q : order) { rc[(size_t)i].push_back(lc[(size_t)q]); rv[(size_t)i].push_back(lv[(size_t)q]); }
+	}
+	}
+	for(int i = 0; i < A.n; ++i) P.ptr[(size_t)i + 1] = P.ptr[(size_t)i] + (int)rc[(size_t)i].size();
+	P.col.resize((size_t)P.ptr[(size_t)A.n]);
+	P.val.resize((size_t)P.ptr[(size_t)A.n]);
+#pragma omp parallel for schedule(static)
+	for(int i = 0; i < A.n; ++i)
+	{
+		std::copy(rc[(size_t)i].begin(), rc[(size_t)i].end(), P.col.begin() + P.ptr[(size_t)i]);
+		std::copy(rv[(size_t)i].begin(), rv[(size_t)i].end(), P.val.begin() + P.ptr[(size_t)i]);
 	}
 }
 
@@ -388,6 +437,7 @@ void GaussJordanInverse(const Csr &A, std::vector<double> &inv)
 			for(int j = 0; j < w; ++j) std::swap(M[(size_t)k * w + j], M[(size_t)p * w + j]);
 		const double piv = M[(size_t)k * w + k];
 		for(int j = 0; j < w; ++j) M[(size_t)k * w + j] = M[(size_t)k * w + j] / piv;
+#pragma omp parallel for schedule(static) if(n > 64)
 		for(int i = 0; i < n; ++i)
 		{
 			if(i == k) continue;
@@ -462,6 +512,7 @@ struct Hierarchy
 		{
 			//  row i of the inverse times f as 32 strided partial sums
 			//  (lane l: j = l, l+32, ... from 0.0) folded pairwise
+#pragma omp parallel for schedule(static) if(n > 64)
 			for(int i = 0; i < n; ++i)
 			{
 				double s[32];
@@ -478,6 +529,7 @@ struct Hierarchy
 			}
 			return;
 		}
+#pragma omp parallel for schedule(static)
 		for(int i = 0; i < n; ++i) x[i] = L.M[(size_t)i] * f[i];
 		Residual(L.A, f, x, L.t.data());
 		if(l + 1 < lv.size())
@@ -485,6 +537,7 @@ struct Hierarchy
 			Level &C = lv[l + 1];
 			Restrict(L.R, L.t.data(), C.f.data());
 			Cycle(l + 1, C.f.data(), C.x.data());
+#pragma omp parallel for schedule(static)
 			for(int i = 0; i < n; ++i)
 			{
 				double s = 0.0;
@@ -493,6 +546,7 @@ struct Hierarchy
 			}
 			Residual(L.A, f, x, L.t.data());
 		}
+#pragma omp parallel for schedule(static)
 		for(int i = 0; i < n; ++i) x[i] = x[i] + L.M[(size_t)i] * L.t[(size_t)i];
 	}
 };
@@ -586,11 +640,13 @@ void BiCGStab(const Csr &A, Prec &&prec, const double *b, double *x, int maxIter
 			else
 			{
 				const double beta = (rho / rhoPrev) * (alpha / omega);
+#pragma omp parallel for schedule(static)
 				for(int i = 0; i < n; ++i) p[(size_t)i] = r[(size_t)i] + beta * (p[(size_t)i] - omega * v[(size_t)i]);
 			}
 			prec(p.data(), ph.data());
 			Spmv(A, ph.data(), v.data());
 			alpha = rho / Dot(n, rh.data(), v.data());
+#pragma omp parallel for schedule(static)
 			for(int i = 0; i < n; ++i) s[(size_t)i] = r[(size_t)i] - alpha * v[(size_t)i];
 			res = std::sqrt(Dot(n, s.data(), s.data()));
 			if(res <= eps)
@@ -604,7 +660,9 @@ void BiCGStab(const Csr &A, Prec &&prec, const double *b, double *x, int maxIter
 			const double tt = Dot(n, t.data(), t.data());
 			const double ts = Dot(n, t.data(), s.data());
 			omega = ts / tt;
+#pragma omp parallel for schedule(static)
 			for(int i = 0; i < n; ++i) x[i] = (x[i] + alpha * ph[(size_t)i]) + omega * sh[(size_t)i];
+#pragma omp parallel for schedule(static)
 			for(int i = 0; i < n; ++i) r[(size_t)i] = s[(size_t)i] - omega * t[(size_t)i];
 			rhoPrev = rho;
 			res = std::sqrt(Dot(n, r.data(), r.data()));
@@ -675,6 +733,7 @@ int yzo_solve(yzo_solver *S, const yzo_settings *set, int n,
 	S->b.assign((size_t)n, 0.0);
 	S->xx.assign(x, x + n);
 	//  ScaleRows, LinearSolverBackend.cpp:227-252
+#pragma omp parallel for schedule(static)
 	for(int i = 0; i < n; ++i)
 	{
 		const int st = rowptr[i], ed = rowptr[i + 1];

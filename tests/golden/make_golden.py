@@ -20,6 +20,8 @@ import subprocess
 import sys
 import tempfile
 import tomllib
+
+import numpy as np
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
@@ -153,6 +155,53 @@ BUILT_STEP_CASES = {
 }
 
 
+#  Whole-step cases at the measured workloads' sizes (yuzen_b200.cases: the
+#  224^2 spinodal film, the 512^2 all-physics film): name: (builder name,
+#  keyword arguments).  Their fixtures are compact (big_<name>.npz): the start
+#  state is rebuilt by the builder, so the fixture keeps the probe's header
+#  values, hashes of its start fields and patterns, and the fields after the
+#  reference's steps.
+BIG_STEP_CASES = {
+    # the 224^2 spinodal film: periodic, adaptive dt, 5 steps
+    "spinodal_224": ("spinodal_224", {"N": 224, "steps": 5}),
+    # the 512^2 all-physics film at dt = 1e-5 s, 2 steps
+    "allphys_512": ("allphys", {"N": 512, "steps": 2}),
+}
+
+
+def field_hash(a) -> str:
+    """sha256 of an array's little-endian bytes (the fixtures' check of a
+    start field or pattern they do not store)."""
+    import hashlib
+    a = np.ascontiguousarray(a)
+    return hashlib.sha256(a.astype(a.dtype.newbyteorder("<"), copy=False).tobytes()).hexdigest()
+
+
+def make_big_step_case(name: str, work: Path, threads: int) -> dict:
+    sys.path.insert(0, str(REPO))
+    from yuzen_b200 import cases
+    builder, kw = BIG_STEP_CASES[name]
+    case = getattr(cases, builder)(**kw)
+    w = work / name
+    case.write_reference(w)
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    res = subprocess.run([str(PROBE), "case.toml", f"{name}.bin"], cwd=w, env=env, capture_output=True, text=True,
+                         timeout=7200)
+    if res.returncode != 0:
+        raise RuntimeError(f"{name}: probe failed\n{res.stdout[-2000:]}\n{res.stderr[-2000:]}")
+    d = stateio.read_state(w / f"{name}.bin")
+    out = {k: d[k] for k in stateio.INT_KEYS + stateio.REAL_KEYS}
+    out["builder"] = builder
+    out["builder_kw"] = repr(kw)
+    for k in ("field_h0", "field_c0", "field_s0", "rowptr", "col", "bc", "rowptr_c", "col_c"):
+        out["sha_" + k] = field_hash(d[k])
+    out["field_h1"] = d["field_h1"]
+    if d["conc_field"]:
+        out["field_c1"] = d["field_c1"]
+    out["case"] = name
+    return out
+
+
 #  Cases the reference's driver runs with either backend (the drop-in test):
 #  written as TOML files under tests/golden/cases/
 DROPIN_CASES = {
@@ -270,6 +319,8 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--only", default=None)
+    ap.add_argument("--big", action="store_true", help="also the compact fixtures at the workloads' sizes")
+    ap.add_argument("--threads", type=int, default=os.cpu_count() or 1, help="OpenMP threads of the big runs")
     a = ap.parse_args()
     if not ORACLE.exists():
         raise SystemExit(f"{ORACLE} missing: make -C oracle ref")
@@ -290,6 +341,14 @@ def main() -> None:
                 continue
             d = make_built_step_case(name, Path(tmp))
             stateio.save_npz(HERE / f"{name}.npz", d)
+            print(name, d["nx"], d["ny"], "steps", d["steps_done"], "t_end", d["t_end"])
+        for name in BIG_STEP_CASES:
+            if a.only and name != a.only:
+                continue
+            if not a.big and a.only != name:
+                continue
+            d = make_big_step_case(name, Path(tmp), a.threads)
+            stateio.save_npz(HERE / f"big_{name}.npz", d)
             print(name, d["nx"], d["ny"], "steps", d["steps_done"], "t_end", d["t_end"])
         for name in CASES:
             if a.only and name != a.only:
