@@ -17,13 +17,17 @@ restart).  Four arms run from the same start: the plain FP64 path (the
 drop-in), the FP32 V-cycle (the AMG preconditioner in float inside the FP64
 BiCGStab), the FP32 V-cycle with each AMG set-up serving several solves
 and the BiCGStab loop replayed as a cached CUDA graph, and that with the
-BiCGStab's SpMVs on the float copy of the matrix; the headline is the fastest
-arm whose film after the timed steps is within 1e-8 (relative L2) of the FP64
-arm's.  Timing: per arm W untimed steps, then K steps, each
-timed with CUDA events on the library's stream, the L2 cache (126 MB) flushed
-by writing a 256 MiB buffer between steps (outside the timed region); under
-torchrun every rank runs an independent replica and the time is the maximum
-over ranks.  One JSON line on rank 0.
+BiCGStab's SpMVs on the float copy of the matrix.  Every arm's first steps
+are checked against the reference's own run of the same case (the fixture
+tests/golden/big_<workload>.npz: h and c after its steps); the headline is
+the fastest arm whose film there is within 1e-8 (relative L2) of the
+reference's.  Timing: per arm W untimed steps (the checked ones among them),
+then K steps, each timed with CUDA events on the library's stream, the L2
+cache (126 MB) flushed by writing a 256 MiB buffer between steps (outside the
+timed region).  The same K steps are also timed end to end on the host clock
+around the public calls (the film uploaded from pinned host memory, the step,
+the film read back).  Under torchrun every rank runs an independent replica
+and the time is the maximum over ranks.  One JSON line on rank 0.
 """
 from __future__ import annotations
 
@@ -48,12 +52,20 @@ METRIC = "steps/s at 512² all-physics: learned-precond FP32 vs plain FP64 GPU, 
 UNIT = "steps/s"
 
 #  The kernel whose roofline is reported (the finest level's SpMV of the
-#  BiCGStab iteration, profiles/KSpmvAlpha_allphys_512.md) and its algorithmic
-#  bytes per launch:
+#  BiCGStab iteration) and its algorithmic bytes per launch:
 #  v = A p with alpha = rho / (rh . v): matrix values and columns (12 B per
 #  entry), row pointers (4 B per row), p read once, rh read, v written
 #  (8 B each per row).
 ROOFLINE_KERNEL = "KSpmvAlpha"
+
+#  DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
+#  the reported kernels, from one ncu capture of each on its workload (a
+#  single-kernel capture, cold L2, --clock-control none), by kernel and
+#  workload: what roofline.traffic reports.  A kernel or workload without a
+#  capture reports null.
+NCU_TRAFFIC = {
+    ("KSpmvAlpha", "allphys_512"): 33880064,
+}
 
 
 PATHS = {
@@ -75,15 +87,24 @@ def spmv_alpha_bytes(n: int, nnz: int) -> int:
     return 12 * nnz + 4 * (n + 1) + 3 * 8 * n
 
 
-def profiled_traffic(kernel: str, workload: str):
-    """DRAM bytes per launch of the kernel (dram__bytes_read.sum +
-    dram__bytes_write.sum) from the committed ncu summary of that kernel on
-    that workload, profiles/<kernel>_<workload>.md, or None."""
-    p = REPO / "profiles" / f"{kernel}_{workload}.md"
+def assembly_bytes(n: int, nnz: int) -> int:
+    """Algorithmic bytes of one Newton pass's assembly (A, J, I + theta dt J
+    and the right-hand side in one pass): read h, c, s, h^n and A(h^n) h^n
+    (8 B each per row), write the I + theta dt J values and the A values kept
+    for the explicit half (8 B per entry each) and the right-hand side."""
+    return 5 * 8 * n + 2 * 8 * nnz + 8 * n
+
+
+def oracle_fixture(workload: str):
+    """The reference's own run of the workload's first steps (h and c after
+    them), the fixture the parity tests hold the device to, or None."""
+    p = REPO / "tests" / "golden" / f"big_{workload}.npz"
     if not p.exists():
         return None
-    m = re.search(r"dram bytes per launch:\s*([0-9]+)", p.read_text())
-    return int(m.group(1)) if m else None
+    import numpy as np
+    z = np.load(p)
+    return {"steps": int(z["steps_done"]), "h": z["field_h1"], "c": z["field_c1"] if "field_c1" in z.files else None,
+            "t_end": float(z["t_end"])}
 
 
 def measured_peaks() -> dict:
@@ -255,25 +276,50 @@ def run_device_arm(a) -> None:
     params = ys.params_from_state(state)
     n = params.nx * params.ny
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    fx = oracle_fixture(a.config)
+    hpin = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    cpin = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
 
-    def timed_arm(precision: int, reuse: int) -> dict:
-        """W untimed steps, then K steps each timed on the device, on a fresh
-        step of the case with the solves' V-cycles in the given arithmetic
-        and the given AMG hierarchy reuse"""
+    def rel(x, y) -> float:
+        return float(np.linalg.norm(x - y) / np.linalg.norm(y))
+
+    def timed_arm(name: str) -> dict:
+        """On a fresh step of the case: the fixture's steps (checked against
+        the reference's run), the rest of the W untimed steps, then K steps
+        each timed on the device (CUDA events inside the step) and, around the
+        same calls, end to end on the host clock: the film uploaded from
+        pinned host memory, the step, the film read back"""
+        precision, reuse = ARMS[name]
         st = ys.Step(params, state["field_h0"], state["field_c0"], state["field_s0"], device=local)
         st.set_precision(precision)
-        st.set_amg_reuse(reuse)
-        if a.warmup > 0:
-            st.advance(a.warmup)
+        st.set_amg_reuse(a.amg_reuse if reuse else 0)
+        out = {"total_ms": 0.0, "wall_s": 0.0, "newton": 0, "linear": 0, "launches": 0, "conc_solves": 0,
+               "conc_iters": 0, "per_step": [], "per_setup": [], "warmup": 0,
+               "parts": {"setup_ms": 0.0, "solve_ms": 0.0, "assemble_ms": 0.0}}
+        done = 0
+        if fx is not None:
+            r = st.advance(fx["steps"])
+            done = fx["steps"]
+            h, c = st.fields()
+            out["h_err_vs_oracle"] = rel(h, fx["h"])
+            out["c_err_vs_oracle"] = rel(c, fx["c"]) if fx["c"] is not None else None
+            out["t_err_vs_oracle"] = abs(r["time"] - fx["t_end"]) / abs(fx["t_end"])
+        if a.warmup > done:
+            st.advance(a.warmup - done)
+            done = a.warmup
+        out["warmup"] = done
+        st.fields_into(hpin, cpin)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        out = {"total_ms": 0.0, "newton": 0, "linear": 0, "launches": 0, "conc_solves": 0, "conc_iters": 0,
-               "per_step": [], "per_setup": [], "parts": {"setup_ms": 0.0, "solve_ms": 0.0, "assemble_ms": 0.0}}
         for _ in range(a.steps):
             flush.zero_()
             torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st.set_fields(hpin, cpin)
             r = st.advance(1)
+            st.fields_into(hpin, cpin)
+            out["wall_s"] += time.perf_counter() - t0
             out["total_ms"] += r["device_ms"]
             out["per_step"].append(round(r["device_ms"], 2))
             out["per_setup"].append(round(r["setup_ms"], 2))
@@ -287,18 +333,17 @@ def run_device_arm(a) -> None:
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        t = torch.tensor([out["total_ms"]], dtype=torch.float64, device=f"cuda:{local}")
+        t = torch.tensor([out["total_ms"], out["wall_s"]], dtype=torch.float64, device=f"cuda:{local}")
         if dist:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        out["max_ms"] = float(t.item())
+        out["max_ms"] = float(t[0].item())
+        out["max_wall_s"] = float(t[1].item())
         out["value"] = world * a.steps / (out["max_ms"] / 1e3)
-        out["h"] = st.fields()[0]
+        out["e2e"] = world * a.steps / max(out["max_wall_s"], 1e-9)
+        out["finite"] = bool(np.isfinite(hpin).all())
         out["step"] = st
         return out
 
-    #  the arms from the same start, the plain FP64 one first; the headline
-    #  is the fastest arm whose film after the timed steps is within 1e-8
-    #  (relative L2) of the FP64 arm's (the FP64 arm itself qualifies)
     names = [x for x in a.arms.split(",") if x]
     for x in names:
         if x not in ARMS:
@@ -306,18 +351,19 @@ def run_device_arm(a) -> None:
     arms = {}
     with Clocks(local) as clk:
         for x in names:
-            arms[x] = timed_arm(ARMS[x][0], a.amg_reuse if ARMS[x][1] else 0)
-    h_err = {}
-    if "fp64" in arms:
-        h64 = arms["fp64"]["h"]
-        for x in arms:
-            if x != "fp64":
-                h_err[x] = float(np.linalg.norm(arms[x]["h"] - h64) / np.linalg.norm(h64))
-    qualified = [x for x in names if x == "fp64" or h_err.get(x, 0.0) <= 1e-8]
+            arms[x] = timed_arm(x)
+    #  the headline: the fastest arm within 1e-8 of the reference's run (of
+    #  its h, and c where the case solves it); without a fixture, of the FP64
+    #  arm's h after the timed steps
+    def qualifies(x) -> bool:
+        v = arms[x]
+        if fx is not None:
+            return v["h_err_vs_oracle"] <= 1e-8 and (v["c_err_vs_oracle"] is None or v["c_err_vs_oracle"] <= 1e-8)
+        return x == "fp64"
+    qualified = [x for x in names if qualifies(x)]
     head_name = max(qualified or names[:1], key=lambda x: arms[x]["value"])
     head = arms[head_name]
-    total_ms, max_ms, value = head["total_ms"], head["max_ms"], head["value"]
-    launches = head["launches"]
+    max_ms, value = head["max_ms"], head["value"]
 
     #  the roofline kernel (the finest level's FP64 SpMV + dot, the same
     #  kernel in every arm), every launch bracketed by CUDA events on the
@@ -333,27 +379,6 @@ def run_device_arm(a) -> None:
     torch.cuda.synchronize()
     kern_ms, kern_n = yz.kernel_time()
     yz.time_kernel(None)
-    st = head["step"]
-
-    # end to end through the C ABI with host buffers: every step uploads its
-    # film from pinned host memory and reads the result back
-    hpin = torch.empty(n, dtype=torch.float64, pin_memory=True)
-    cpin = torch.empty(n, dtype=torch.float64, pin_memory=True)
-    h_np, c_np = hpin.numpy(), cpin.numpy()
-    st.fields_into(h_np, c_np)
-    e2e_steps = max(0, min(a.steps, a.e2e_steps))
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        st.set_fields(h_np, c_np)
-        st.advance(1)
-        st.fields_into(h_np, c_np)
-    e2e_s = max(time.perf_counter() - t0, 1e-9)
-    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-    if dist:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-        dist.barrier()
-    e2e_value = world * e2e_steps / float(e2e_t.item()) if e2e_steps else None
-    finite = bool(np.isfinite(h_np).all())
 
     if rank != 0:
         if dist:
@@ -367,9 +392,22 @@ def run_device_arm(a) -> None:
         achieved = bytes_ / (kern_ms / kern_n / 1e3) / 1e9
         roof = {"kernel": ROOFLINE_KERNEL, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
                 "peak_source": peaks["source"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                "traffic": profiled_traffic(ROOFLINE_KERNEL, a.config), "bytes_per_launch": bytes_, "launches": kern_n,
+                "traffic": NCU_TRAFFIC.get((ROOFLINE_KERNEL, a.config)), "bytes_per_launch": bytes_,
+                "launches": kern_n,
                 "timed_over": f"{a.roofline_steps} further steps of the {names[0]} arm, L2 flushed between steps",
                 "avg_launch_us": kern_ms / kern_n * 1e3}
+    #  the assembly of a Newton pass (every term's A and J, I + theta dt J and
+    #  the right-hand side), timed with CUDA events around it in every pass
+    #  of the headline arm's timed steps
+    asm = None
+    if head["newton"] > 0 and head["parts"]["assemble_ms"] > 0:
+        ab = assembly_bytes(n, nnz)
+        per_pass_ms = head["parts"]["assemble_ms"] / head["newton"]
+        ach = ab / (per_pass_ms / 1e3) / 1e9
+        asm = {"kernel": "assembly of a Newton pass", "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"],
+               "peak_source": peaks["source"], "unit": "GB/s", "frac": ach / peaks["hbm_gbs"],
+               "traffic": NCU_TRAFFIC.get(("assembly", a.config)), "bytes_per_launch": ab, "passes": head["newton"],
+               "avg_pass_us": per_pass_ms * 1e3}
     cpu = None
     if world == 1 and not a.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -377,32 +415,46 @@ def run_device_arm(a) -> None:
         if "unavailable" not in r:
             cpu = {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "reference",
                    "sample": f"{r['steps']} steps of {a.config}: the reference's sources with the CPU "
-                             f"restatement of its AMGCL backend, {threads} OpenMP threads"}
+                             f"restatement of its AMGCL backend (linear solve and assembly on {threads} "
+                             f"OpenMP threads)"}
         else:
             cpu = {"unavailable": r["unavailable"]}
+    cfg_line = {"workload": a.config, "grid": [cfg.Nx, cfg.Ny], "rows": n, "nnz": nnz,
+                "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                "l2": "flushed between steps (256 MiB write)",
+                "path": PATHS[head_name], "arm": head_name,
+                "amg_reuse": a.amg_reuse if ARMS[head_name][1] else 0,
+                "warmup_steps": head["warmup"]}
+    if fx is not None:
+        cfg_line.update({
+            "oracle_steps": fx["steps"],
+            "h_err_vs_oracle": head["h_err_vs_oracle"], "c_err_vs_oracle": head["c_err_vs_oracle"],
+            "h_err_vs_oracle_fp64": arms["fp64"]["h_err_vs_oracle"] if "fp64" in arms else None,
+            "c_err_vs_oracle_fp64": arms["fp64"]["c_err_vs_oracle"] if "fp64" in arms else None})
+    if "fp64" in arms:
+        cfg_line["fp64_steps_per_s"] = arms["fp64"]["value"]
+        cfg_line["speedup_vs_fp64"] = value / arms["fp64"]["value"]
+    cfg_line["arms"] = {k: {"steps_per_s": v["value"], "e2e_steps_per_s": v["e2e"],
+                            "ms_per_step": v["max_ms"] / a.steps,
+                            "h_err_vs_oracle": v.get("h_err_vs_oracle"), "c_err_vs_oracle": v.get("c_err_vs_oracle"),
+                            "newton_iterations": v["newton"], "linear_iterations": v["linear"],
+                            "conc_solves": v["conc_solves"], "conc_iterations": v["conc_iters"],
+                            "device_ms": {q: round(w, 3) for q, w in v["parts"].items()},
+                            "step_ms": v["per_step"], "setup_ms_per_step": v["per_setup"],
+                            "gpu_launches": v["launches"]} for k, v in arms.items()}
+    cfg_line["finite"] = all(v["finite"] for v in arms.values())
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": max_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": DTYPES[head_name],
         "data": "synthetic (seeded, yuzen_b200.cases)",
-        "config": {"workload": a.config, "grid": [cfg.Nx, cfg.Ny], "rows": n, "nnz": nnz,
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                   "l2": "flushed between steps (256 MiB write)",
-                   "path": PATHS[head_name],
-                   "h_error_vs_fp64": h_err,
-                   "amg_reuse": a.amg_reuse if ARMS[head_name][1] else 0,
-                   "arms": {k: {"steps_per_s": v["value"], "ms_per_step": v["max_ms"] / a.steps,
-                                "newton_iterations": v["newton"], "linear_iterations": v["linear"],
-                                "conc_solves": v["conc_solves"], "conc_iterations": v["conc_iters"],
-                                "device_ms": {q: round(w, 3) for q, w in v["parts"].items()},
-                                "step_ms": v["per_step"], "setup_ms_per_step": v["per_setup"],
-                                "gpu_launches": v["launches"]} for k, v in arms.items()},
-                   "learned_preconditioner": "not built: the reference has none and no trained weights exist",
-                   "finite": finite},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 2 * 8 * n,
-                "steps": e2e_steps},
-        "gpu_launches": launches,
+        "config": cfg_line,
+        "e2e": {"value": head["e2e"], "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 2 * 8 * n,
+                "steps": a.steps, "timed": "the same K steps as value, host clock around set_fields + advance + "
+                                          "fields_into, L2 flushed between steps"},
+        "gpu_launches": head["launches"],
         "roofline": roof,
+        "roofline_assembly": asm,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
     }
@@ -542,7 +594,7 @@ def main() -> None:
     ap.add_argument("--config", default="allphys_512")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=6, help="steps of the end-to-end (host buffers) measurement")
+    ap.add_argument("--e2e-steps", type=int, default=6, help="steps of the ensemble's end-to-end measurement")
     ap.add_argument("--arms", default="fp64,fp32_cycle,fp32_reuse,fp32m_reuse",
                     help="the arms timed, in order (fp64, fp32_cycle, fp32_reuse, fp32m_reuse); headline: the "
                          "fastest one whose film is within 1e-8 of the FP64 arm's")

@@ -166,7 +166,42 @@ BIG_STEP_CASES = {
     "spinodal_224": ("spinodal_224", {"N": 224, "steps": 5}),
     # the 512^2 all-physics film at dt = 1e-5 s, 2 steps
     "allphys_512": ("allphys", {"N": 512, "steps": 2}),
+    # the reference's own 512^2 scaling case (cases/scaling/bench2d_n0512.toml), 2 steps
+    "bench2d_512": ("bench2d_512", {"N": 512, "steps": 2}),
 }
+
+
+#  The reference's own benchmark cases restated by the seeded builder:
+#  name: (reference case file, builder name, keyword arguments).  The fixture
+#  (ref_<name>.npz) keeps the start state the reference's set-up builds from
+#  its own TOML (the probe, one step): header values, hashes of h and c, and
+#  the substrate s, which the builder restates to rounding.
+REF_CASES = {
+    "bench2d_512": ("scaling/bench2d_n0512.toml", "bench2d_512", {"N": 512}),
+}
+
+
+def make_ref_case(ref: Path, name: str, work: Path, threads: int) -> dict:
+    src, builder, kw = REF_CASES[name]
+    doc = tomllib.loads((ref / "cases" / src).read_text())
+    tomlw.setpath(doc, "Numerics.MaxSteps", 1)
+    w = work / name
+    w.mkdir()
+    (w / "case.toml").write_text(tomlw.dumps(doc))
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    res = subprocess.run([str(PROBE), "case.toml", f"{name}.bin"], cwd=w, env=env, capture_output=True, text=True,
+                         timeout=3600)
+    if res.returncode != 0:
+        raise RuntimeError(f"{name}: probe failed\n{res.stdout[-2000:]}\n{res.stderr[-2000:]}")
+    d = stateio.read_state(w / f"{name}.bin")
+    out = {k: d[k] for k in stateio.INT_KEYS + stateio.REAL_KEYS}
+    out["builder"] = builder
+    out["builder_kw"] = repr(kw)
+    out["sha_field_h0"] = field_hash(d["field_h0"])
+    out["sha_field_c0"] = field_hash(d["field_c0"])
+    out["field_s0"] = d["field_s0"]
+    out["case"] = name
+    return out
 
 
 def field_hash(a) -> str:
@@ -342,6 +377,12 @@ def main() -> None:
             d = make_built_step_case(name, Path(tmp))
             stateio.save_npz(HERE / f"{name}.npz", d)
             print(name, d["nx"], d["ny"], "steps", d["steps_done"], "t_end", d["t_end"])
+        for name in REF_CASES:
+            if (a.only and name != a.only) or (not a.big and a.only != name):
+                continue
+            d = make_ref_case(Path(a.ref), name, Path(tmp), a.threads)
+            stateio.save_npz(HERE / f"ref_{name}.npz", d)
+            print(name, d["nx"], d["ny"])
         for name in BIG_STEP_CASES:
             if a.only and name != a.only:
                 continue

@@ -433,4 +433,52 @@ def allphys(N: int = 512, steps: int = 12, dt: float = 1e-5) -> Case:
                 conc_model="WM", conc0=0.2, h_init=h)
 
 
-CONFIGS = {"spinodal_224": spinodal_224, "allphys_512": allphys}
+def _ellipse_bump(x, y, center, width, slope):
+    """C_EllipseBump of height 1 (ShapeFunctions.cpp:61-66): the profile
+    RectProfile_base(rr, 0, 1, slope) (:19-22) of the elliptic radius rr,
+    with Math::Sigmoid (MyMath_I.h:109-112)."""
+    rr = np.sqrt(np.power((x - center[0]) / width[0], 2.0) + np.power((y - center[1]) / width[1], 2.0))
+
+    def sig(v, v0, eps):
+        return 1.0 / (1.0 + np.exp(-(v - v0) / eps))
+
+    return sig(rr, -0.5, slope * 0.1) * (1.0 - sig(rr, 0.5, slope * 0.1))
+
+
+def bench2d_512(N: int = 512, steps: int = 12) -> Case:
+    """The reference's own 2-D scaling benchmark at 512^2 (cases/scaling/
+    bench2d_n0512.toml, the case of its published CPU timings): a 10 um film
+    of the default resist (mu(c) = exp(10 (c - 0.5)), sigma(c), D(c)) on a
+    1 mm square with Symmetry edges, over a substrate step -- an elliptic bump
+    of half the film's height centred at x = 0.5 mm, width 1 x 0.5 mm, edge
+    0.1 mm, added to both the substrate and the free surface (stacked on a
+    precursor of half the height) -- with capillary pressure, Marangoni
+    stress, Raoult evaporation (1e-7 m/s) and the well-mixed concentration
+    solved from c = 0.5; fixed dt = 1.25e-5 s, 12 steps.  The film and
+    substrate are the reference's C_InitialSurface / C_Substrate profiles
+    (InitialCondition.cpp:93-120, Substrate.cpp:48-62) restated here and
+    handed to both the reference and the device through the same ASCII
+    restart, so both solve the same case."""
+    side = 1.0e-3
+    h0 = 10e-6
+    prec = 0.5
+    probe = Case(name="probe", Nx=N, Ny=N, xlim=(-side / 2, side / 2), ylim=(-side / 2, side / 2), h0=h0,
+                 precursor=prec, bc=("Symmetry",) * 4, dt=1.25e-5)
+    L0 = probe.scales()["L0"]
+    g = probe.grid(L0)
+    xs = (g["xmin"] + (np.arange(N) + 2) * g["dx"] + g["dx"] * 0.5) * L0
+    ys = (g["ymin"] + (np.arange(N) + 2) * g["dy"] + g["dy"] * 0.5) * L0
+    X, Y = np.meshgrid(xs, ys)
+    prof = _ellipse_bump(X, Y, (0.5, 0.0), (1.0, 0.5), 0.1e-3)
+    #  the free surface: the bump stacked (Height 0.5, Base 0) on the
+    #  precursor; the substrate: the same bump added (TotalHeight 10 um)
+    hs = h0 * ((0.5 * prof) * (1.0 - prec) + prec)
+    ss = h0 * np.maximum(0.0, 0.5 * prof)
+    hh = np.maximum(hs - ss, prec * h0)
+    return Case(name=f"bench2d_{N}", Nx=N, Ny=N, xlim=(-side / 2, side / 2), ylim=(-side / 2, side / 2), h0=h0,
+                precursor=prec, bc=("Symmetry",) * 4, dt=1.25e-5, steps=steps, dt_control=False, marangoni=True,
+                evaporation={"Coef": 1e-7, "ConcFunc": "Raoult", "SpatialFunc": "uniform"}, conc_model="WM",
+                conc0=0.5, h_init=hh / h0, s_init=ss / h0)
+
+
+CONFIGS = {"spinodal_224": spinodal_224, "allphys_512": allphys, "bench2d_512": bench2d_512}
