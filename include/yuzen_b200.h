@@ -254,6 +254,13 @@ typedef struct yz_step_stats
 	 * (WellMixedModelBase.h:1405-1411); 0 otherwise */
 	double energy_F, energy_D, energy_dissipated, energy_balance;
 	int    amg_setups;         /* SA-AMG hierarchies set up (height and concentration solves) */
+	/* the learned preconditioner (yz_step_set_learned), for this call: film
+	 * solves it converged, solves it handed back to SA-AMG, its BiCGStab
+	 * iterations, the samples held, the device time spent training, and the
+	 * network's held-out error against the V-cycle and last training loss
+	 * (-1 before it is trained) */
+	int    learned_solves, learned_fallbacks, learned_iterations, learned_samples;
+	double learned_train_ms, learned_val_err, learned_loss;
 } yz_step_stats;
 
 /* Build the step: fields h, c, s on all nx*ny points (host arrays). */
@@ -310,6 +317,100 @@ int yz_step_conc_system(yz_step* st, const double* h, const double* c, double dt
  * of BoundaryCondition2D::Apply, BoundaryCondition.cpp:376-517); arrays may be
  * null to query nnz (the return value). */
 int yz_pattern_2d(const yz_step_params* p, int* rowptr, int* col, int* bc);
+
+/*
+ * ---------------------------------------------------------------------
+ * The learned preconditioner.  The reference has no counterpart: these
+ * entry points add a preconditioner beside its SA-AMG one, for the film's
+ * solve (LinearSolverBackend.cpp:660-679 is the AMG it sits beside and falls
+ * back to).  A small U-Net on the film's grid (levels of 16, 32, 64 and 64
+ * channels, 3x3 convolutions in BF16 on the tensor cores with FP32
+ * accumulation) maps a residual r -- with the matrix diagonal and the film
+ * height as two more input maps -- to z ~ V r, the SA-AMG V-cycle's answer;
+ * it is trained on the device, by its own forward and backward kernels, on
+ * (r, V r) pairs the solver collects from its own AMG-preconditioned solves,
+ * and used in a flexible BiCGStab (the right-preconditioned iteration with a
+ * preconditioner that may change between applications).  SA-AMG stays the
+ * judge and the fallback: a learned solve that needs more than cap_factor
+ * times the iterations of the last SA-AMG solve is repeated on the AMG path,
+ * and the network then sits out a growing number of solves.
+ * ---------------------------------------------------------------------
+ */
+typedef struct yz_unet yz_unet;
+
+/* A network for a grid of nx x ny points (rows iy*nx + ix, ghost layers
+ * included), holding up to `capacity` training pairs; weights initialised
+ * from `seed`. */
+int yz_unet_create(int device, int nx, int ny, int capacity, unsigned seed, yz_unet** out);
+int yz_unet_destroy(yz_unet* u);
+long long yz_unet_param_count(const yz_unet* u);
+/* The FP32 master weights (yz_unet_param_count floats). */
+int yz_unet_get_params(yz_unet* u, float* out);
+int yz_unet_set_params(yz_unet* u, const float* in);
+/* The network's output for normalised input maps feat3 = [r/rms; diagonal
+ * feature; height feature] (3 x n floats), in normalised units (n floats). */
+int yz_unet_forward(yz_unet* u, const float* feat3, float* out);
+/* One pair's loss, sum over the n rows of (out - target)^2 / n, and its
+ * gradient w.r.t. every weight (yz_unet_param_count floats). */
+int yz_unet_loss_grad(yz_unet* u, const float* feat3, const float* target, double* loss, float* grad);
+/* A training pair from host arrays: the residual r, the V-cycle's answer z,
+ * the matrix diagonal and the film height (null: none), n each. */
+int yz_unet_add_sample(yz_unet* u, const double* r, const double* z, const double* diag, const double* h);
+int yz_unet_samples(const yz_unet* u);
+/* Adam over the pairs held, the last `holdout` kept out: iters steps of
+ * `batch` pairs at learning rate lr; the last step's mean loss, and the
+ * held-out relative error ||N r - V r|| / ||V r|| (-1 without held-out pairs). */
+int yz_unet_train(yz_unet* u, int iters, int batch, float lr, int holdout, double* loss, double* val_err);
+/* The network applied to a device vector r (n doubles) as the preconditioner
+ * applies it: z = N(r) rms(r), with the diagonal of d_values (storage order,
+ * diagonal first in each row of d_rowptr) and the height d_h as features.
+ * Queued on `stream` (a cudaStream_t, null: the default stream). */
+int yz_unet_apply(yz_unet* u, const double* d_values, const int* d_rowptr, const double* d_h,
+                  const double* d_r, double* d_z, void* stream);
+
+/* The seam-1 solver with the network: mode 0 off; 1 collect (the next
+ * `collect_solves` SA-AMG solves each add up to `per_solve` (r, V r) pairs to
+ * the network's ring); 2 use (the flexible BiCGStab with the network first,
+ * SA-AMG the fallback).  The network must be trained before mode 2 uses it
+ * and must outlive its use by the solver. */
+int yz_solver_set_learned(yz_solver* s, yz_unet* u, int mode, int collect_solves, int per_solve,
+                          double cap_factor);
+/* The film height (device vector of n) the network reads as a feature, for
+ * the next solves; null: none. */
+int yz_solver_set_aux(yz_solver* s, const double* d_h);
+/* Counters of the learned path: solves it converged, fallbacks to SA-AMG,
+ * its iterations, solves it sat out. */
+int yz_solver_learned_stats(const yz_solver* s, int* solves, int* fallbacks, int* iterations, int* skipped);
+
+/* The step's film solves with a learned preconditioner of its own: the
+ * first `collect_solves` SA-AMG solves collect up to `samples_per_solve`
+ * pairs each; the film solve after them trains the network (train_iters Adam
+ * steps of `batch` pairs at rate lr, `holdout` pairs kept out to measure it
+ * against the V-cycle); from then on every film solve tries the network
+ * first, within cap_factor x the last SA-AMG solve's iterations.  The
+ * concentration's solves keep their SPAI0 / SA-AMG path.  Null: off. */
+typedef struct yz_learned_cfg
+{
+	int      collect_solves;
+	int      samples_per_solve;
+	int      capacity;
+	int      train_iters;
+	int      batch;
+	float    lr;
+	int      holdout;
+	double   cap_factor;
+	unsigned seed;
+} yz_learned_cfg;
+int yz_step_set_learned(yz_step* st, const yz_learned_cfg* cfg);
+
+/* One 3x3 convolution of the network's tensor-core kernel on host arrays
+ * (its parity test): x is H x W pixels of cin channels (pixel-major,
+ * channels innermost), w[n][9][cin] (tap = (dy+1)*3 + dx+1), bias[n] or
+ * null; y[p][n] = act(bias + sum w x[p + dy W + dx]) in BF16 arithmetic with
+ * FP32 accumulation, 0 outside the real_w x real_h corner; relu 0 or 1.
+ * cin and n multiples of 16 (cin <= 128, n <= 256). */
+int yz_conv3x3(int H, int W, int cin, int n, int real_w, int real_h, int relu, const float* x,
+               const float* w, const float* bias, float* y);
 
 #ifdef __cplusplus
 }

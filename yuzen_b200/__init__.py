@@ -40,6 +40,11 @@ EXPORTED_SYMBOLS = (
     "yz_step_conc_pattern", "yz_step_conc_system", "yz_step_set_precision", "yz_solver_set_amg_reuse",
     "yz_step_set_amg_reuse", "yz_solver_set_graph_loop", "yz_step_set_graph_loop", "yz_step_energy",
     "yz_step_set_energy",
+    # the learned preconditioner
+    "yz_unet_create", "yz_unet_destroy", "yz_unet_param_count", "yz_unet_get_params", "yz_unet_set_params",
+    "yz_unet_forward", "yz_unet_loss_grad", "yz_unet_add_sample", "yz_unet_samples", "yz_unet_train",
+    "yz_unet_apply", "yz_solver_set_learned", "yz_solver_set_aux", "yz_solver_learned_stats",
+    "yz_step_set_learned", "yz_conv3x3",
 )
 
 #: the preconditioner's arithmetic (YZ_PREC_* of include/yuzen_b200.h)
@@ -279,6 +284,29 @@ class B200Backend:
 
     def launches(self) -> int:
         return int(lib().yz_solver_launches(self._h))
+
+    def SetLearned(self, net, mode: int, collect_solves: int = 0, per_solve: int = 0, cap_factor: float = 1.0):
+        """The learned preconditioner (yuzen_b200.learned.UNet) of the film's
+        solves: mode 0 off, 1 collect (AMG solves feed its sample ring), 2 use
+        (flexible BiCGStab with the network first, SA-AMG the fallback)."""
+        from . import learned
+        L = learned._bind()
+        self._net = net
+        _check(L.yz_solver_set_learned(self._h, net.handle if net is not None else None, mode, collect_solves,
+                                       per_solve, cap_factor), "yz_solver_set_learned")
+
+    def SetAux(self, h_ptr: int | None) -> None:
+        """The film height on the device (a pointer to n doubles) the network
+        reads as a feature; None: none."""
+        from . import learned
+        _check(learned._bind().yz_solver_set_aux(self._h, ctypes.c_void_p(h_ptr) if h_ptr else None),
+               "yz_solver_set_aux")
+
+    def learned_stats(self) -> dict:
+        from . import learned
+        v = [ctypes.c_int() for _ in range(4)]
+        _check(learned._bind().yz_solver_learned_stats(self._h, *[ctypes.byref(x) for x in v]), "learned_stats")
+        return dict(zip(("solves", "fallbacks", "iterations", "skipped"), (x.value for x in v)))
 
     def close(self) -> None:
         if self._h:

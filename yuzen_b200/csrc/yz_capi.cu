@@ -15,6 +15,16 @@ struct yz_step
 	std::unique_ptr<yz::Step> s;
 };
 
+struct yz_unet
+{
+	std::unique_ptr<yz::Learned> u;
+};
+
+namespace yz {
+void Conv3x3Host(int H, int W, int cin, int n, int realW, int realH, int relu, const float *x, const float *w,
+                 const float *bias, float *y);
+}
+
 namespace {
 template<class F> int Guard(F &&f)
 {
@@ -344,6 +354,156 @@ int yz_pattern_2d(const yz_step_params *p, int *rowptr, int *col, int *bc)
 		if(col) std::copy(cl.begin(), cl.end(), col);
 		if(bc) std::copy(isbc.begin(), isbc.end(), bc);
 		return (int)cl.size();
+	});
+}
+
+//--------------------------------------------------------------------------
+//  the learned preconditioner
+//--------------------------------------------------------------------------
+int yz_unet_create(int device, int nx, int ny, int capacity, unsigned seed, yz_unet **out)
+{
+	return Guard([&] {
+		if(!out) throw yz::UsageError("yz_unet_create: out is null");
+		int count = 0;
+		yz::Check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+		if(device < 0 || device >= count) throw yz::UsageError("yz_unet_create: no such CUDA device");
+		yz_unet *h = new yz_unet();
+		try { h->u.reset(new yz::Learned(device, nx, ny, capacity, seed)); }
+		catch(...) { delete h; throw; }
+		*out = h;
+		return 0;
+	});
+}
+
+int yz_unet_destroy(yz_unet *u)
+{
+	return Guard([&] { delete u; return 0; });
+}
+
+long long yz_unet_param_count(const yz_unet *u) { return u ? (long long)u->u->ParamCount() : -1; }
+
+int yz_unet_get_params(yz_unet *u, float *out)
+{
+	return Guard([&] {
+		if(!u || !out) throw yz::UsageError("yz_unet_get_params: null argument");
+		u->u->GetParams(out, 0);
+		return 0;
+	});
+}
+
+int yz_unet_set_params(yz_unet *u, const float *in)
+{
+	return Guard([&] {
+		if(!u || !in) throw yz::UsageError("yz_unet_set_params: null argument");
+		u->u->SetParams(in, 0);
+		return 0;
+	});
+}
+
+int yz_unet_forward(yz_unet *u, const float *feat3, float *out)
+{
+	return Guard([&] {
+		if(!u || !feat3 || !out) throw yz::UsageError("yz_unet_forward: null argument");
+		u->u->Forward(feat3, out, 0);
+		return 0;
+	});
+}
+
+int yz_unet_loss_grad(yz_unet *u, const float *feat3, const float *target, double *loss, float *grad)
+{
+	return Guard([&] {
+		if(!u || !feat3 || !target || !grad) throw yz::UsageError("yz_unet_loss_grad: null argument");
+		const double l = u->u->LossGrad(feat3, target, grad, 0);
+		if(loss) *loss = l;
+		return 0;
+	});
+}
+
+int yz_unet_add_sample(yz_unet *u, const double *r, const double *z, const double *diag, const double *h)
+{
+	return Guard([&] {
+		if(!u || !r || !z || !diag) throw yz::UsageError("yz_unet_add_sample: null argument");
+		u->u->AddSampleHost(r, z, diag, h, 0);
+		return 0;
+	});
+}
+
+int yz_unet_samples(const yz_unet *u) { return u ? u->u->Samples() : -1; }
+
+int yz_unet_train(yz_unet *u, int iters, int batch, float lr, int holdout, double *loss, double *val_err)
+{
+	return Guard([&] {
+		if(!u) throw yz::UsageError("yz_unet_train: null network");
+		if(iters < 0 || batch < 1 || !(lr > 0) || holdout < 0)
+			throw yz::UsageError("yz_unet_train: iters >= 0, batch >= 1, lr > 0, holdout >= 0");
+		double v = -1.0;
+		const double l = u->u->Train(iters, batch, lr, holdout, &v, 0);
+		if(loss) *loss = l;
+		if(val_err) *val_err = v;
+		return 0;
+	});
+}
+
+int yz_unet_apply(yz_unet *u, const double *d_values, const int *d_rowptr, const double *d_h, const double *d_r,
+                  double *d_z, void *stream)
+{
+	return Guard([&] {
+		if(!u || !d_values || !d_rowptr || !d_r || !d_z) throw yz::UsageError("yz_unet_apply: null argument");
+		cudaStream_t st = static_cast<cudaStream_t>(stream);
+		u->u->SetAux(d_values, d_rowptr, d_h, st);
+		u->u->Apply(d_r, d_z, st, nullptr);
+		return 0;
+	});
+}
+
+int yz_solver_set_learned(yz_solver *s, yz_unet *u, int mode, int collect_solves, int per_solve, double cap_factor)
+{
+	return Guard([&] {
+		if(!s) throw yz::UsageError("yz_solver_set_learned: null solver");
+		if(mode == 2 && u && !u->u->Trained()) throw yz::UsageError("yz_solver_set_learned: the network is not trained");
+		s->s->SetLearned(u ? u->u.get() : nullptr, mode, collect_solves, per_solve, cap_factor);
+		return 0;
+	});
+}
+
+int yz_solver_set_aux(yz_solver *s, const double *d_h)
+{
+	return Guard([&] {
+		if(!s) throw yz::UsageError("yz_solver_set_aux: null solver");
+		s->s->SetAux(d_h);
+		return 0;
+	});
+}
+
+int yz_solver_learned_stats(const yz_solver *s, int *solves, int *fallbacks, int *iterations, int *skipped)
+{
+	return Guard([&] {
+		if(!s) throw yz::UsageError("yz_solver_learned_stats: null solver");
+		const yz::Solver::LearnedStats &l = s->s->LStats();
+		if(solves) *solves = l.solves;
+		if(fallbacks) *fallbacks = l.fallbacks;
+		if(iterations) *iterations = l.iterations;
+		if(skipped) *skipped = l.skipped;
+		return 0;
+	});
+}
+
+int yz_step_set_learned(yz_step *st, const yz_learned_cfg *cfg)
+{
+	return Guard([&] {
+		if(!st) throw yz::UsageError("yz_step_set_learned: null step");
+		st->s->SetLearned(cfg);
+		return 0;
+	});
+}
+
+int yz_conv3x3(int H, int W, int cin, int n, int real_w, int real_h, int relu, const float *x, const float *w,
+               const float *bias, float *y)
+{
+	return Guard([&] {
+		if(!x || !w || !y) throw yz::UsageError("yz_conv3x3: null argument");
+		yz::Conv3x3Host(H, W, cin, n, real_w, real_h, relu, x, w, bias, y);
+		return 0;
 	});
 }
 

@@ -8,6 +8,7 @@
 // by damped Jacobi (None, Jacobi), coarse_enough 500 above 3000 rows (:660-675),
 // a breakdown answered by the residual check of :681-713.
 #include "yz_amg_kernels.cuh"
+#include "yz_learned.h"
 #include "yz_solver_impl.h"
 
 #include <map>
@@ -291,7 +292,7 @@ Solver::~Solver()
 	if(_hring) cudaFreeHost(_hring);
 	cudaEventDestroy(_evRing[0]); cudaEventDestroy(_evRing[1]);
 	cudaEventDestroy(_ev0); cudaEventDestroy(_ev1); cudaEventDestroy(_ev2);
-	FreeLoopGraph(_loop[0]); FreeLoopGraph(_loop[1]);
+	FreeLoopGraph(_loop[0]); FreeLoopGraph(_loop[1]); FreeLoopGraph(_loop[2]);
 	if(_ownStream) cudaStreamDestroy(_st);
 }
 
@@ -802,9 +803,25 @@ void Solver::SetAmgReuse(int maxSolves)
 	_stale = true;		// the next AMG solve sets up afresh
 }
 
+void Solver::SetLearned(Learned *L, int mode, int collectSolves, int perSolve, double capFactor)
+{
+	if(mode < 0 || mode > 2) throw UsageError("set_learned: mode must be 0 (off), 1 (collect) or 2 (use)");
+	if(mode && !L) throw UsageError("set_learned: no network given");
+	if(L && _n > 0 && L->Rows() != _n) throw UsageError("set_learned: the network's grid does not have the pattern's rows");
+	if(capFactor <= 0) throw UsageError("set_learned: cap_factor must be > 0");
+	if(L != _learned) ++_epoch;
+	_learned = L;
+	_learnedMode = mode;
+	_collectLeft = (mode >= 1) ? collectSolves : 0;
+	_perSolve = perSolve;
+	_capFactor = capFactor;
+	_offLearned = TryBackoff();
+}
+
 void Solver::ApplyPrec(int kind, const double *r, double *z)
 {
 	const int n = _n;
+	if(kind == kPrecLearned) { _learned->Apply(r, z, _st, Halt()); return; }
 	if(kind == kPrecDiag) YZ_LAUNCH(KDiagApply, GridFor(n, kB), kB, 0, _st, Halt(), n, _m.get(), r, z);
 	else if(_precision != YZ_PREC_FP64) Cycle32<double, double>(0, r, z);
 	else Cycle(0, r, z);
@@ -856,10 +873,21 @@ void Solver::RunIterations(int kind)
 	//  from the stream instead.
 	static const char *env = std::getenv("YZ_GRAPH");
 	static const bool graphOff = env && env[0] == '0';
-	LoopGraph &lg = _loop[kind == kPrecAmg ? 1 : 0];
+	LoopGraph &lg = _loop[kind];
 	const unsigned long long key = ((unsigned long long)_epoch << 32) | (kind == kPrecAmg ? _epochH : 0u);
 	Scal *sc = _sc.get();
-	if(graphOff || !_graphLoop || TimingActive())
+	//  an AMG run that feeds the network's sample ring: after each of its
+	//  first iterations, the residual r and the V-cycle's answer to it
+	const bool collect = kind == kPrecAmg && _learned && _collectLeft > 0 && _perSolve > 0;
+	int hooks = 0;
+	auto hook = [&]() {
+		if(!collect || hooks >= _perSolve) return;
+		ApplyPrec(kPrecAmg, _r.get(), _zs.get());
+		_learned->AddSample(_r.get(), _zs.get(), _st, Halt());
+		++hooks;
+	};
+	if(collect) _zs.reserve((size_t)_n);
+	if(graphOff || !_graphLoop || TimingActive() || collect)
 	{
 		//  one iteration kept in flight: the state after iteration k is
 		//  copied to pinned memory and read while iteration k+1 runs; the
@@ -875,12 +903,14 @@ void Solver::RunIterations(int kind)
 		int slot = 0;
 		EnqueueIteration(kind); ++queued;
 		YZ_LAUNCH(KLoopCount, 1, 1, 0, _st, sc);
+		hook();
 		YZ_CUDA(cudaMemcpyAsync(_hring + slot, sc, sizeof(Scal), cudaMemcpyDeviceToHost, _st));
 		YZ_CUDA(cudaEventRecord(_evRing[slot], _st));
 		for(;;)
 		{
 			EnqueueIteration(kind); ++queued;
 			YZ_LAUNCH(KLoopCount, 1, 1, 0, _st, sc);
+			hook();
 			const int next = slot ^ 1;
 			YZ_CUDA(cudaMemcpyAsync(_hring + next, sc, sizeof(Scal), cudaMemcpyDeviceToHost, _st));
 			YZ_CUDA(cudaEventRecord(_evRing[next], _st));
@@ -896,6 +926,7 @@ void Solver::RunIterations(int kind)
 		}
 		const long long timed = TimeCount() - mark;
 		if(timed > 0 && queued > _hsc->it) TimeDropLast(timed / queued * (queued - _hsc->it));
+		if(collect) { --_collectLeft; _collected += hooks; }
 		return;
 	}
 	if(lg.exec == nullptr || lg.key != key)
@@ -1063,6 +1094,43 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 			YZ_CUDA(cudaMemcpyAsync(_x.get(), _x0.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
 		}
 	}
+	//  The learned preconditioner first, on a solve of the film (SA-AMG
+	//  preconditioning asked for, not the concentration's role): a flexible
+	//  BiCGStab (the right-preconditioned iteration with the network as its
+	//  preconditioner, which may change from one application to the next;
+	//  x and the residual recurrence stay those of the true matrix) allowed
+	//  cap_factor times the last SA-AMG solve's iterations.  One that does not
+	//  converge within them is repeated from the caller's guess on the AMG
+	//  path, and the network sits out the next solves (TryBackoff, as the
+	//  SPAI0 try does).
+	if(!done && _learnedMode == 2 && _learned && _learned->Trained() && !set.conc && set.precondition == 2)
+	{
+		if(_offLearned.Try())
+		{
+			_learned->SetAux(dValues, L0.ptr.get(), _aux, _st);
+			//  the plain path's count: the last SA-AMG solve's, else the cap
+			const double plain = _amgIters > 0 ? (double)_amgIters : (double)set.max_iteration;
+			const int cap = (int)std::max(1.0, std::min((double)set.max_iteration, std::ceil(_capFactor * plain)));
+			int itL = 0;
+			double errL = 0;
+			const bool okL = BiCGStab(kPrecLearned, cap, set.epsilon, itL, errL);
+			if(okL && errL <= set.epsilon)
+			{
+				done = true; it = itL; err = errL;
+				++_lstats.solves; _lstats.iterations += itL;
+				_offLearned.Converged();
+			}
+			else
+			{
+				++_lstats.fallbacks;
+				itTried += okL ? itL : 0;
+				_offLearned.Failed();
+				YZ_CUDA(cudaMemcpyAsync(_x.get(), _x0.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+			}
+		}
+		else
+			++_lstats.skipped;
+	}
 	bool broke = false;
 	if(!done)
 	{
@@ -1111,6 +1179,7 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 				YZ_CUDA(cudaEventRecord(_ev1, _st));
 				timedSetup = true;
 				broke = !BiCGStab(kPrecAmg, set.max_iteration, set.epsilon, it, err);
+				if(!broke && !set.conc && err <= set.epsilon) _amgIters = it;
 				if(!reuse) { _freshIters = it; break; }
 				if(broke || !(err <= set.epsilon))
 				{

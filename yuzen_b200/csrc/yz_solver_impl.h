@@ -9,6 +9,8 @@
 
 namespace yz {
 
+class Learned;
+
 //  Scalars of one BiCGStab run, in device memory (written by the block that
 //  folds a reduction, read by the element-wise kernels and by the host).
 struct Scal
@@ -76,11 +78,22 @@ public:
 	void SetAmgReuse(int maxSolves);
 	void SetGraphLoop(bool on) { _graphLoop = on; }
 	int Rebuilds() const { return _rebuilds; }
+	//  the learned preconditioner (not owned): mode 0 off, 1 collect (the
+	//  next `collectSolves` AMG solves feed the network's sample ring with up
+	//  to `perSolve` (residual, V-cycle) pairs each), 2 use (the network in a
+	//  flexible BiCGStab first, SA-AMG as the fallback)
+	void SetLearned(Learned *L, int mode, int collectSolves, int perSolve, double capFactor);
+	//  the film height for the network's features (a device vector of n; null: none)
+	void SetAux(const double *dH) { _aux = dH; }
+	int CollectLeft() const { return _collectLeft; }
+	struct LearnedStats { int solves = 0, fallbacks = 0, iterations = 0, skipped = 0; };
+	const LearnedStats &LStats() const { return _lstats; }
+	int AmgIters() const { return _amgIters; }
 	cudaStream_t Stream() const { return _st; }
 	int Rows() const { return _n; }
 
 private:
-	enum { kPrecDiag = 0, kPrecAmg = 1 };
+	enum { kPrecDiag = 0, kPrecAmg = 1, kPrecLearned = 2 };
 	void BuildHierarchy(int coarseEnough);
 	void DirectInverse(Level &L);
 	void Cycle(size_t l, const double *f, double *x);
@@ -167,13 +180,22 @@ private:
 	//  bumped whenever a pointer or size a loop graph holds may change: the
 	//  pattern, precision or buffers (_epoch), the hierarchy (_epochH)
 	unsigned _epoch = 0, _epochH = 0;
-	LoopGraph _loop[2];
+	LoopGraph _loop[3];
 	bool _graphLoop = true;       // the loop as a CUDA graph (else from the stream)
 	//  Solve's tail, queued behind a graph run: x into the caller's dX
 	double *_tailDst = nullptr;
 	const double *_tailSrc = nullptr;
 	size_t _tailBytes = 0;
 	bool _tailDone = false;
+	//  the learned preconditioner
+	Learned *_learned = nullptr;
+	int _learnedMode = 0, _collectLeft = 0, _perSolve = 0, _collected = 0;
+	double _capFactor = 1.0;
+	const double *_aux = nullptr;
+	int _amgIters = 0;              // iterations of the last SA-AMG solve (the plain path's count)
+	TryBackoff _offLearned;
+	LearnedStats _lstats;
+	DBuf<double> _zs;               // a collected pair's V-cycle output
 	double _setupMs = 0, _iterMs = 0;
 	long long _launches = 0;
 };

@@ -1013,6 +1013,13 @@ bool Step::NKLoop(int &iter, double &resid, yz_step_stats &stats)
 		ls.epsilon = eps;
 		ls.conc = 0;
 		int it = 0; double res = 0;
+		//  the learned preconditioner reads the pass's film as a feature, and
+		//  is trained once the solves that collect its pairs are done
+		if(_learned)
+		{
+			_solver->SetAux(_guess.get());
+			if(!_learned->Trained() && _solver->CollectLeft() == 0) TrainLearned(stats);
+		}
 		const int r0 = _solver->Rebuilds();
 		const int ch = _solver->Solve(ls, _ia.get(), _rhs.get(), _delta.get(), it, res);
 		double su = 0, sit = 0; _solver->Timing(&su, &sit);
@@ -1060,12 +1067,56 @@ bool Step::NKLoop(int &iter, double &resid, yz_step_stats &stats)
 }
 
 //  TimeAdvance (NewtonKantorovich.cpp:424-486) and the clock (TimeSteps.cpp:121-160)
+void Step::SetLearned(const yz_learned_cfg *cfg)
+{
+	YZ_CUDA(cudaSetDevice(_device));
+	if(!cfg)
+	{
+		_solver->SetLearned(nullptr, 0, 0, 0, 1.0);
+		_learned.reset();
+		return;
+	}
+	if(cfg->collect_solves < 1 || cfg->samples_per_solve < 1 || cfg->capacity < 2 || cfg->train_iters < 0 ||
+	   cfg->batch < 1 || !(cfg->lr > 0) || cfg->holdout < 0 || !(cfg->cap_factor > 0))
+		throw UsageError("set_learned: collect_solves, samples_per_solve, batch >= 1, capacity >= 2, lr and "
+		                 "cap_factor > 0, train_iters and holdout >= 0");
+	_lcfg = *cfg;
+	_solver->SetLearned(nullptr, 0, 0, 0, 1.0);
+	_learned.reset(new Learned(_device, _p.nx, _p.ny, cfg->capacity, cfg->seed));
+	_solver->SetLearned(_learned.get(), 1, cfg->collect_solves, cfg->samples_per_solve, cfg->cap_factor);
+	_lValErr = -1.0;
+	_lLoss = -1.0;
+}
+
+//  Adam on the pairs the film's solves collected; then the film's solves try
+//  the network first
+void Step::TrainLearned(yz_step_stats &stats)
+{
+	cudaEvent_t e0, e1;
+	YZ_CUDA(cudaEventCreate(&e0));
+	YZ_CUDA(cudaEventCreate(&e1));
+	YZ_CUDA(cudaEventRecord(e0, _st));
+	const int hold = std::min(_lcfg.holdout, std::max(0, _learned->Samples() - 1));
+	double val = -1.0;
+	_lLoss = _learned->Train(_lcfg.train_iters, _lcfg.batch, _lcfg.lr, hold, &val, _st);
+	_lValErr = val;
+	YZ_CUDA(cudaEventRecord(e1, _st));
+	YZ_CUDA(cudaEventSynchronize(e1));
+	float ms = 0;
+	YZ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	stats.learned_train_ms += ms;
+	_solver->SetLearned(_learned.get(), 2, 0, 0, _lcfg.cap_factor);
+}
+
 void Step::Advance(int nsteps, yz_step_stats &stats)
 {
 	YZ_CUDA(cudaSetDevice(_device));
 	const size_t bytes = (size_t)_n * sizeof(double);
 	const int g = GridFor(_n, 256);
 	const long long l0 = t_launches;
+	const Solver::LearnedStats ls0 = _solver->LStats();
 	YZ_CUDA(cudaEventRecord(_eA, _st));
 	for(int step = 0; step < nsteps; ++step)
 	{
@@ -1164,6 +1215,15 @@ void Step::Advance(int nsteps, yz_step_stats &stats)
 	}
 	stats.time = _time;
 	stats.dt = _dt;
+	{
+		const Solver::LearnedStats &ls1 = _solver->LStats();
+		stats.learned_solves += ls1.solves - ls0.solves;
+		stats.learned_fallbacks += ls1.fallbacks - ls0.fallbacks;
+		stats.learned_iterations += ls1.iterations - ls0.iterations;
+		stats.learned_samples = _learned ? _learned->Samples() : 0;
+		stats.learned_val_err = _lValErr;
+		stats.learned_loss = _lLoss;
+	}
 	if(_energyOn)
 	{
 		stats.energy_F = _enF; stats.energy_D = _enD;

@@ -1,6 +1,7 @@
 // yz_step_impl.h -- the device step context behind yz_step_* (C ABI).
 #pragma once
 
+#include "yz_learned.h"
 #include "yz_physics.cuh"
 #include "yz_solver_impl.h"
 
@@ -48,6 +49,9 @@ public:
 	}
 	int Rows() const { return _n; }
 	int Nnz() const { return _nnz; }
+	//  the learned preconditioner of the film's solves (null: off)
+	void SetLearned(const yz_learned_cfg *cfg);
+	Learned *GetLearned() const { return _learned.get(); }
 
 private:
 	enum { kSlotRhs = 0, kSlotDelta = 1, kSlotPhi = 2, kSlotMove = 3, kSlotLte = 4, kSlotBad = 5, kSlotCorr = 6,
@@ -115,6 +119,12 @@ private:
 	int _adjustCount = 0, _nkIter = 0;
 	double _ewEta = 0, _ewRhsPrev = 0, _extrapMove = 0, _lastResid = 0;
 	bool _extrapBlocked = false;
+	//  the learned preconditioner: the network (its weights and sample
+	//  ring), its settings and what its training reported
+	std::unique_ptr<Learned> _learned;
+	yz_learned_cfg _lcfg{};
+	double _lValErr = -1.0, _lLoss = -1.0;
+	void TrainLearned(yz_step_stats &stats);
 };
 
 } // namespace yz

@@ -58,6 +58,9 @@ class StepStats(ctypes.Structure):
         ("energy_F", ctypes.c_double), ("energy_D", ctypes.c_double),
         ("energy_dissipated", ctypes.c_double), ("energy_balance", ctypes.c_double),
         ("amg_setups", ctypes.c_int),
+        ("learned_solves", ctypes.c_int), ("learned_fallbacks", ctypes.c_int), ("learned_iterations", ctypes.c_int),
+        ("learned_samples", ctypes.c_int), ("learned_train_ms", ctypes.c_double), ("learned_val_err", ctypes.c_double),
+        ("learned_loss", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -160,6 +163,13 @@ class Step:
         """The step's BiCGStab loops as CUDA graph launches (default) or
         from the stream (yz_step_set_graph_loop)."""
         _check(lib().yz_step_set_graph_loop(self._h, int(bool(on))), "yz_step_set_graph_loop")
+
+    def set_learned(self, cfg=None) -> None:
+        """The learned preconditioner of the film's solves
+        (yuzen_b200.learned.LearnedConfig, or default_config(); None: off)."""
+        from . import learned
+        L = learned._bind()
+        _check(L.yz_step_set_learned(self._h, ctypes.byref(cfg) if cfg is not None else None), "yz_step_set_learned")
 
     def energy(self):
         """(F, D): the free energy of the film the step holds and the flux
