@@ -325,8 +325,11 @@ int yz_pattern_2d(const yz_step_params* p, int* rowptr, int* col, int* bc);
  * solve (LinearSolverBackend.cpp:660-679 is the AMG it sits beside and falls
  * back to).  A small U-Net on the film's grid (levels of 16, 32, 64 and 64
  * channels, 3x3 convolutions in BF16 on the tensor cores with FP32
- * accumulation) maps a residual r -- with the matrix diagonal and the film
- * height as two more input maps -- to z ~ V r, the SA-AMG V-cycle's answer;
+ * accumulation) maps a residual r -- its input channels are r and r times
+ * two feature maps, the matrix diagonal's and the film height's, and their
+ * squares and product -- to z ~ V r, the SA-AMG V-cycle's answer; without
+ * activation (activation 0, the preconditioner's form: no bias, no ReLU) it
+ * is a linear operator on r whose coefficients follow the system;
  * it is trained on the device, by its own forward and backward kernels, on
  * (r, V r) pairs the solver collects from its own AMG-preconditioned solves,
  * and used in a flexible BiCGStab (the right-preconditioned iteration with a
@@ -340,15 +343,15 @@ typedef struct yz_unet yz_unet;
 
 /* A network for a grid of nx x ny points (rows iy*nx + ix, ghost layers
  * included), holding up to `capacity` training pairs; weights initialised
- * from `seed`. */
-int yz_unet_create(int device, int nx, int ny, int capacity, unsigned seed, yz_unet** out);
+ * from `seed`; activation 0 linear (no bias, no ReLU), 1 bias and ReLU. */
+int yz_unet_create(int device, int nx, int ny, int capacity, unsigned seed, int activation, yz_unet** out);
 int yz_unet_destroy(yz_unet* u);
 long long yz_unet_param_count(const yz_unet* u);
 /* The FP32 master weights (yz_unet_param_count floats). */
 int yz_unet_get_params(yz_unet* u, float* out);
 int yz_unet_set_params(yz_unet* u, const float* in);
 /* The network's output for normalised input maps feat3 = [r/rms; diagonal
- * feature; height feature] (3 x n floats), in normalised units (n floats). */
+ * feature; height feature] (3 x n floats), in units of z / rms(r) (n floats). */
 int yz_unet_forward(yz_unet* u, const float* feat3, float* out);
 /* One pair's loss, sum over the n rows of (out - target)^2 / n, and its
  * gradient w.r.t. every weight (yz_unet_param_count floats). */
@@ -362,7 +365,7 @@ int yz_unet_samples(const yz_unet* u);
  * held-out relative error ||N r - V r|| / ||V r|| (-1 without held-out pairs). */
 int yz_unet_train(yz_unet* u, int iters, int batch, float lr, int holdout, double* loss, double* val_err);
 /* The network applied to a device vector r (n doubles) as the preconditioner
- * applies it: z = N(r) rms(r), with the diagonal of d_values (storage order,
+ * applies it: z = N(r), with the diagonal of d_values (storage order,
  * diagonal first in each row of d_rowptr) and the height d_h as features.
  * Queued on `stream` (a cudaStream_t, null: the default stream). */
 int yz_unet_apply(yz_unet* u, const double* d_values, const int* d_rowptr, const double* d_h,
@@ -400,6 +403,7 @@ typedef struct yz_learned_cfg
 	int      holdout;
 	double   cap_factor;
 	unsigned seed;
+	int      activation;   /* 0 linear (the default), 1 ReLU */
 } yz_learned_cfg;
 int yz_step_set_learned(yz_step* st, const yz_learned_cfg* cfg);
 

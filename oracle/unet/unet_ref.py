@@ -3,11 +3,15 @@
 This is the checker the device network (yuzen_b200/csrc/yz_unet.cu) is
 compared against; nothing of the product path imports it.  The reference has
 no learned preconditioner, so this module restates the device network's own
-definition (yuzen_b200/csrc/yz_learned.h): the image geometry, the U-Net
-(levels of 16, 32, 64, 64 channels; 3x3 convolutions with bias and ReLU;
-2x2 average pooling; nearest upsampling with the encoder's output concatenated
-in front; a 1x1 output layer), the loss sum (out - t)^2 / n over the real
-pixels, and the analytic gradient of that loss w.r.t. every weight.
+definition (yuzen_b200/csrc/yz_learned.h): the image geometry, the input
+channels (r and its products with the two feature maps f1, f2: r, r f1,
+r f2, r f1^2, r f2^2, r f1 f2), the U-Net (levels of 16, 32, 64, 64
+channels; 3x3 convolutions, with bias and ReLU when act = 1, neither when
+act = 0; 2x2 average pooling; nearest upsampling with the encoder's output
+concatenated in front; a 1x1 output layer), the loss sum (out - t)^2 / n
+over the real pixels, and the analytic gradient of that loss w.r.t. every
+weight (the biases' gradients are 0 when act = 0: the device keeps them
+at 0).
 
 Numbers are float64.  With bf16=True every tensor the device stores in BF16
 (activations, the gradients of activations, the network's inputs and packed
@@ -68,10 +72,11 @@ def unpack(params: np.ndarray):
 
 
 class Net:
-    def __init__(self, nx: int, ny: int, bf16: bool = True):
+    def __init__(self, nx: int, ny: int, bf16: bool = True, act: int = 1):
         self.nx, self.ny, self.n = nx, ny, nx * ny
         self.lv = geometry(nx, ny)
         self.bf16 = bf16
+        self.act = act
 
     def r(self, x):
         return to_bf16(x) if self.bf16 else np.asarray(x, dtype=np.float64)
@@ -158,12 +163,17 @@ class Net:
 
     # ------------------------------------------------------------------
     def image(self, feat3):
-        """the input image (H0 W0, 16): channels 0..2 the features, bf16"""
+        """the input image (H0 W0, 16): channels r, r f1, r f2, r f1^2,
+        r f2^2, r f1 f2 of the maps feat3 = (r, f1, f2), products in float32
+        as the device forms them, bf16"""
         H, W, _, _ = self.lv[0]
         F = np.zeros((H * W, 16))
         idx = self.rows_to_pixels()
-        for c in range(3):
-            F[idx, c] = feat3[c]
+        r, f1, f2 = (np.asarray(feat3[c], dtype=np.float32) for c in range(3))
+        if not self.bf16:
+            r, f1, f2 = (np.asarray(feat3[c], dtype=np.float64) for c in range(3))
+        for c, v in enumerate((r, r * f1, r * f2, (r * f1) * f1, (r * f2) * f2, (r * f1) * f2)):
+            F[idx, c] = v
         return self.r(F)
 
     def rows_to_pixels(self):
@@ -177,19 +187,20 @@ class Net:
         a = {}
         F = self.image(feat3)
         a["F"] = F
-        E0 = self.conv(F, Ws[ENC0], bs[ENC0], 0, True)
+        A = self.act == 1
+        E0 = self.conv(F, Ws[ENC0], bs[ENC0], 0, A)
         P1 = self.pool(E0, 0)
-        E1 = self.conv(P1, Ws[ENC1], bs[ENC1], 1, True)
+        E1 = self.conv(P1, Ws[ENC1], bs[ENC1], 1, A)
         P2 = self.pool(E1, 1)
-        E2 = self.conv(P2, Ws[ENC2], bs[ENC2], 2, True)
+        E2 = self.conv(P2, Ws[ENC2], bs[ENC2], 2, A)
         P3 = self.pool(E2, 2)
-        B3 = self.conv(P3, Ws[BOTT], bs[BOTT], 3, True)
+        B3 = self.conv(P3, Ws[BOTT], bs[BOTT], 3, A)
         U2 = np.concatenate([E2, self.up(B3, 2)], axis=1)
-        D2 = self.conv(U2, Ws[DEC2], bs[DEC2], 2, True)
+        D2 = self.conv(U2, Ws[DEC2], bs[DEC2], 2, A)
         U1 = np.concatenate([E1, self.up(D2, 1)], axis=1)
-        D1 = self.conv(U1, Ws[DEC1], bs[DEC1], 1, True)
+        D1 = self.conv(U1, Ws[DEC1], bs[DEC1], 1, A)
         U0 = np.concatenate([E0, self.up(D1, 0)], axis=1)
-        D0 = self.conv(U0, Ws[DEC0], bs[DEC0], 0, True)
+        D0 = self.conv(U0, Ws[DEC0], bs[DEC0], 0, A)
         a.update(E0=E0, P1=P1, E1=E1, P2=P2, E2=E2, P3=P3, B3=B3, U2=U2, D2=D2, U1=U1, D1=D1, U0=U0, D0=D0, W=Ws,
                  wo=wo, bo=bo)
         out = D0[self.rows_to_pixels()] @ wo + bo
@@ -208,28 +219,32 @@ class Net:
         pix = self.rows_to_pixels()
         D0 = a["D0"]
         grad[ow:ow + 16] = g @ D0[pix]
-        grad[ob] = g.sum()
+        grad[ob] = g.sum() if self.act else 0.0
         gD0 = np.zeros_like(D0)
-        gD0[pix] = np.outer(g, wo) * (D0[pix] > 0)
+        gD0[pix] = np.outer(g, wo) * ((D0[pix] > 0) if self.act else 1.0)
         gD0 = self.r(gD0)
 
         def put(k, dW, db):
             wo_, bo_ = lay[k]
             grad[wo_:bo_] += dW.reshape(-1)
-            grad[bo_:bo_ + CONVS[k][1]] += db
+            if self.act:
+                grad[bo_:bo_ + CONVS[k][1]] += db
+
+        def mask(x):
+            return (x > 0) if self.act else 1.0
 
         # dec0
         gU0 = self.conv_t(gD0, Ws[DEC0], 0)
         put(DEC0, *self.wgrad(a["U0"], gD0, 0))
-        gD1 = self.r(self.up_back(gU0[:, 16:48], 0) * (a["D1"] > 0))
+        gD1 = self.r(self.up_back(gU0[:, 16:48], 0) * mask(a["D1"]))
         # dec1
         gU1 = self.conv_t(gD1, Ws[DEC1], 1)
         put(DEC1, *self.wgrad(a["U1"], gD1, 1))
-        gD2 = self.r(self.up_back(gU1[:, 32:96], 1) * (a["D2"] > 0))
+        gD2 = self.r(self.up_back(gU1[:, 32:96], 1) * mask(a["D2"]))
         # dec2
         gU2 = self.conv_t(gD2, Ws[DEC2], 2)
         put(DEC2, *self.wgrad(a["U2"], gD2, 2))
-        gB3 = self.r(self.up_back(gU2[:, 64:128], 2) * (a["B3"] > 0))
+        gB3 = self.r(self.up_back(gU2[:, 64:128], 2) * mask(a["B3"]))
         # bottleneck
         gP3 = self.conv_t(gB3, Ws[BOTT], 3)
         put(BOTT, *self.wgrad(a["P3"], gB3, 3))
@@ -247,20 +262,23 @@ class Net:
     def skip_back(self, gU, gP, E, l):
         H, W, _, _ = self.lv[l]
         par = self.up(gP, l)
-        o = (gU + 0.25 * par) * (E > 0)
+        o = (gU + 0.25 * par) * ((E > 0) if self.act else 1.0)
         o[~self.real(l)] = 0.0
         return o
 
 
-def init_params(seed: int = 0) -> np.ndarray:
-    """A He-normal draw in the device's parameter order (for CPU-only tests;
-    the device draws its own from its generator)."""
+def init_params(seed: int = 0, act: int = 1) -> np.ndarray:
+    """A random draw in the device's parameter order (for the tests; the
+    device draws its own from its generator): He-normal weights, small
+    biases with act = 1; weights of variance 1/fan-in and zero biases with
+    act = 0."""
     rng = np.random.default_rng(seed)
     lay, ow, ob = param_layout()
     p = np.zeros(param_count())
     for (wo, bo), (cin, cout, _) in zip(lay, CONVS):
-        p[wo:bo] = rng.normal(0.0, np.sqrt(2.0 / (9 * cin)), bo - wo)
-        p[bo:bo + cout] = rng.normal(0.0, 0.05, cout)
+        p[wo:bo] = rng.normal(0.0, np.sqrt((2.0 if act else 1.0) / (9 * cin)), bo - wo)
+        if act:
+            p[bo:bo + cout] = rng.normal(0.0, 0.05, cout)
     p[ow:ow + 16] = rng.normal(0.0, 0.25, 16)
-    p[ob] = 0.01
+    p[ob] = 0.01 if act else 0.0
     return p

@@ -37,16 +37,21 @@ def test_bf16_rounding():
     assert np.all(np.abs(r - x) <= np.abs(x) * 2 ** -8)
 
 
-def test_gradient_matches_finite_differences():
+@pytest.mark.parametrize("act", [0, 1])
+def test_gradient_matches_finite_differences(act):
     nx = ny = 10
-    net = unet_ref.Net(nx, ny, bf16=False)
+    net = unet_ref.Net(nx, ny, bf16=False, act=act)
     rng = np.random.default_rng(3)
-    p = unet_ref.init_params(5)
+    p = unet_ref.init_params(5, act)
     feat = rng.standard_normal((3, nx * ny))
     t = rng.standard_normal(nx * ny)
     loss, g = net.loss_grad(p, feat, t)
-    idx = rng.choice(p.size, 60, replace=False)
-    idx = np.concatenate([idx, [p.size - 1, p.size - 2]])      # the output layer too
+    lay, ow, ob = unet_ref.param_layout()
+    weights = np.concatenate([np.arange(a, b) for a, b in lay] + [np.arange(ow, ow + 16)])
+    # without activation the biases are held at 0 (their gradient is not computed)
+    pool = np.arange(p.size) if act else weights
+    idx = rng.choice(pool, 60, replace=False)
+    idx = np.concatenate([idx, [p.size - 2] + ([p.size - 1] if act else [])])      # the output layer too
     eps = 1e-6
     worst = 0.0
     for k in idx:
@@ -57,3 +62,18 @@ def test_gradient_matches_finite_differences():
         fd = (lp - lm) / (2 * eps)
         worst = max(worst, abs(fd - g[k]) / max(1e-6, abs(fd) + abs(g[k])))
     assert worst < 1e-4, worst
+
+
+def test_linear_network_is_linear_in_r():
+    """Without activation the network is a linear operator on r (the input
+    channels are r times functions of the features)."""
+    nx = ny = 12
+    net = unet_ref.Net(nx, ny, bf16=False, act=0)
+    rng = np.random.default_rng(4)
+    p = unet_ref.init_params(2, 0)
+    f = rng.standard_normal((3, nx * ny))
+    r1, r2 = rng.standard_normal(nx * ny), rng.standard_normal(nx * ny)
+    out = lambda r: net.forward(p, np.stack([r, f[1], f[2]]))[0]
+    a, b = 0.7, -2.3
+    lhs = out(a * r1 + b * r2)
+    assert np.allclose(lhs, a * out(r1) + b * out(r2), rtol=1e-10, atol=1e-12 * np.abs(lhs).max())

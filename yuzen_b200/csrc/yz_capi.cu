@@ -360,7 +360,7 @@ int yz_pattern_2d(const yz_step_params *p, int *rowptr, int *col, int *bc)
 //--------------------------------------------------------------------------
 //  the learned preconditioner
 //--------------------------------------------------------------------------
-int yz_unet_create(int device, int nx, int ny, int capacity, unsigned seed, yz_unet **out)
+int yz_unet_create(int device, int nx, int ny, int capacity, unsigned seed, int activation, yz_unet **out)
 {
 	return Guard([&] {
 		if(!out) throw yz::UsageError("yz_unet_create: out is null");
@@ -368,7 +368,8 @@ int yz_unet_create(int device, int nx, int ny, int capacity, unsigned seed, yz_u
 		yz::Check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
 		if(device < 0 || device >= count) throw yz::UsageError("yz_unet_create: no such CUDA device");
 		yz_unet *h = new yz_unet();
-		try { h->u.reset(new yz::Learned(device, nx, ny, capacity, seed)); }
+		if(activation != 0 && activation != 1) throw yz::UsageError("yz_unet_create: activation must be 0 or 1");
+		try { h->u.reset(new yz::Learned(device, nx, ny, capacity, seed, activation)); }
 		catch(...) { delete h; throw; }
 		*out = h;
 		return 0;

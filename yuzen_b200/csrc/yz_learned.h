@@ -4,12 +4,17 @@
 // diagonal, film height) -> AMG-correction pairs the solver generates.
 //
 // The network maps a residual r (a vector over the n = nx*ny rows of the
-// ghost-padded grid) to z ~ M r, where M is the SA-AMG V-cycle the solver
-// would apply: inputs are three maps on the grid -- r / rms(r), the diagonal
-// of the unscaled matrix (log10 |a_ii| / 4) and the film height
-// (log10 h / 2 + 1, or 0 where the caller gives none) -- and the output,
-// scaled back by rms(r), is z.  Architecture (channels per level 16, 32, 64,
-// 64; every convolution 3x3 with bias, ReLU):
+// ghost-padded grid) to z = N(r) ~ M r, where M is the SA-AMG V-cycle the
+// solver would apply.  Its input channels are r / rms(r) and its products with two
+// feature maps of the system -- f1 = log10 |a_ii| / 4 of the unscaled
+// matrix's diagonal, f2 = log10 h / 2 + 1 of the film height (0 where the
+// caller gives none) -- namely r, r f1, r f2, r f1^2, r f2^2, r f1 f2; the
+// output, scaled back by rms(r), is z.  Every input channel is linear in r:
+// with the activation off (the preconditioner's form) the network has no
+// bias and no ReLU and is a linear operator on r whose coefficients vary
+// with f1 and f2, so BiCGStab sees one fixed preconditioner per system; with
+// ReLU on it is the usual nonlinear U-Net.  Architecture (channels per level
+// 16, 32, 64, 64; every convolution 3x3):
 //
 //   F(16: 3 used) -enc0-> E0(16) -pool-> P1 -enc1-> E1(32) -pool-> P2 -enc2->
 //   E2(64) -pool-> P3 -bott-> B3(64) -up, concat E2-> dec2 -> D2(64) -up,
@@ -41,8 +46,9 @@ class Learned
 {
 public:
 	//  capacity: training samples held on the device; seed: the weights'
-	//  initialisation (He-normal from a fixed generator)
-	Learned(int device, int nx, int ny, int capacity, unsigned seed);
+	//  initialisation (He-normal from a fixed generator); act 0: linear (no
+	//  bias, no activation), 1: bias and ReLU
+	Learned(int device, int nx, int ny, int capacity, unsigned seed, int act);
 	~Learned();
 
 	int Nx() const { return _nx; }
@@ -57,12 +63,12 @@ public:
 	//  diagonal (values in storage order, diagonal first in each row) and the
 	//  film height (null: none); queued on st
 	void SetAux(const double *dValues, const int *rowptr, const double *h, cudaStream_t st);
-	//  z = N(r) rms(r) on the device, queued on st; with halt non-null every
+	//  z = N(r) on the device, queued on st; with halt non-null every
 	//  kernel returns at once while *halt != 0 (a finished Krylov run)
 	void Apply(const double *r, double *z, cudaStream_t st, const int *halt);
-	//  a training pair (r, z = M r) with the present features, stored
-	//  normalised by rms(r) in the next slot of the ring (queued on st; the
-	//  slot is marked unused when *halt != 0 at the time)
+	//  a training pair (r, z = M r) with the present features, stored as
+	//  r / rms(r) and z / rms(r) in the next slot of the ring (queued on st;
+	//  the slot is marked unused when *halt != 0 then)
 	void AddSample(const double *r, const double *z, cudaStream_t st, const int *halt);
 	//  the same from host arrays (n each; h may be null)
 	void AddSampleHost(const double *r, const double *z, const double *diag, const double *h, cudaStream_t st);
@@ -78,9 +84,11 @@ public:
 	void GetParams(float *out, cudaStream_t st);
 	void SetParams(const float *in, cudaStream_t st);
 	//  one sample's loss and the gradient of it w.r.t. every parameter
-	//  (features and target as normalised host maps over the n rows)
+	//  (features and target as normalised host maps over the n rows; the
+	//  target in units of the targets' scale)
 	double LossGrad(const float *feat3, const float *target, float *grad, cudaStream_t st);
-	//  the network's output (normalised units) for host feature maps
+	//  the network's output for host feature maps, in the units of z / rms(r)
+	//  (the output layer's value times the targets' scale)
 	void Forward(const float *feat3, float *out, cudaStream_t st);
 
 private:
@@ -95,6 +103,7 @@ private:
 	void Check(cudaStream_t st);
 
 	int _device, _nx, _ny, _n;
+	int _act = 0;
 	Level _lv[4];
 	std::vector<ConvLayer> _conv;   // enc0, enc1, enc2, bott, dec2, dec1, dec0
 	size_t _np = 0, _outW = 0, _outB = 0;
@@ -119,6 +128,11 @@ private:
 	int _cap = 0, _count = 0;
 	bool _trained = false;
 	DBuf<int> _err;
+	//  the training targets' scale (z / rms(r) divided by it is what the
+	//  network learns), set by the first training from its pairs; 1 before
+	DBuf<float> _tsc;
+	float _tscHost = 1.0f;
+	bool _tscSet = false;
 };
 
 } // namespace yz

@@ -901,6 +901,7 @@ void Solver::RunIterations(int kind)
 		_tailDone = false;		// Solve copies the answer after this run
 		int queued = 0;
 		int slot = 0;
+		hook();			// the start residual r = b - A x0
 		EnqueueIteration(kind); ++queued;
 		YZ_LAUNCH(KLoopCount, 1, 1, 0, _st, sc);
 		hook();

@@ -1077,12 +1077,13 @@ void Step::SetLearned(const yz_learned_cfg *cfg)
 		return;
 	}
 	if(cfg->collect_solves < 1 || cfg->samples_per_solve < 1 || cfg->capacity < 2 || cfg->train_iters < 0 ||
-	   cfg->batch < 1 || !(cfg->lr > 0) || cfg->holdout < 0 || !(cfg->cap_factor > 0))
+	   cfg->batch < 1 || !(cfg->lr > 0) || cfg->holdout < 0 || !(cfg->cap_factor > 0) ||
+	   (cfg->activation != 0 && cfg->activation != 1))
 		throw UsageError("set_learned: collect_solves, samples_per_solve, batch >= 1, capacity >= 2, lr and "
 		                 "cap_factor > 0, train_iters and holdout >= 0");
 	_lcfg = *cfg;
 	_solver->SetLearned(nullptr, 0, 0, 0, 1.0);
-	_learned.reset(new Learned(_device, _p.nx, _p.ny, cfg->capacity, cfg->seed));
+	_learned.reset(new Learned(_device, _p.nx, _p.ny, cfg->capacity, cfg->seed, cfg->activation));
 	_solver->SetLearned(_learned.get(), 1, cfg->collect_solves, cfg->samples_per_solve, cfg->cap_factor);
 	_lValErr = -1.0;
 	_lLoss = -1.0;

@@ -104,6 +104,20 @@ __device__ __forceinline__ bool BarWait(uint64_t *bar, uint32_t parity, long lon
 	return true;
 }
 
+//  16 bytes global -> shared without staging through registers (the
+//  copies of a thread stay in flight together); valid false fills zeros
+__device__ __forceinline__ void CpAsync16(void *smem, const void *gmem, bool valid)
+{
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(SmemAddr(smem)), "l"(gmem),
+	             "r"(valid ? 16 : 0)
+	             : "memory");
+}
+__device__ __forceinline__ void CpAsyncWaitAll()
+{
+	asm volatile("cp.async.commit_group;" ::: "memory");
+	asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
 //  TMEM: one whole warp allocates `ncols` columns (a power of two, 32..512)
 //  and writes their address to shared memory; the same warp frees them
 __device__ __forceinline__ void TmemAlloc(uint32_t *slot, uint32_t ncols)

@@ -88,11 +88,12 @@ __global__ void __launch_bounds__(128) KConv3x3(ConvArgs a)
 			const int dyi = idx / per, rem = idx - dyi * per;
 			const int px = rem / chunks, c = rem - px * chunks;
 			const long long q = (long long)p0 + (long long)(dyi - 1) * a.W + (px - 1);
-			uint4 v = make_uint4(0u, 0u, 0u, 0u);
-			if(q >= 0 && q < HW) v = *reinterpret_cast<const uint4 *>(a.x + (size_t)q * a.cin + c * 8);
-			*reinterpret_cast<uint4 *>(As + dyi * aStride + c * (kHalo * 16) + px * 16) = v;
+			const bool in = q >= 0 && q < HW;
+			tc::CpAsync16(As + dyi * aStride + c * (kHalo * 16) + px * 16,
+			              a.x + (in ? (size_t)q * a.cin + c * 8 : (size_t)0), in);
 		}
 	}
+	tc::CpAsyncWaitAll();
 	tc::FenceBeforeSync();
 	__syncthreads();
 	tc::FenceAfterSync();
@@ -105,7 +106,9 @@ __global__ void __launch_bounds__(128) KConv3x3(ConvArgs a)
 	{
 		const int tg = min(a.tpg, 9 - t0);
 		const uint4 *src = reinterpret_cast<const uint4 *>(a.w) + (size_t)t0 * bPerTap;
-		for(int idx = tid; idx < tg * bPerTap; idx += blockDim.x) reinterpret_cast<uint4 *>(Bs)[idx] = src[idx];
+		for(int idx = tid; idx < tg * bPerTap; idx += blockDim.x)
+			tc::CpAsync16(reinterpret_cast<uint4 *>(Bs) + idx, src + idx, true);
+		tc::CpAsyncWaitAll();
 		tc::FenceProxyAsync();
 		__syncthreads();
 		if(tid == 0)
@@ -256,7 +259,7 @@ __global__ void KUp(int C, const bf16 *__restrict__ src, Lv ls, bf16 *__restrict
 //  channels [coff, coff + C) of gU (stride cs, level l), where the forward
 //  activation D (level l+1, after ReLU) is positive
 __global__ void KUpBack(int C, const bf16 *__restrict__ gU, int cs, int coff, Lv lh, const bf16 *__restrict__ D,
-                        Lv ll, bf16 *__restrict__ gD)
+                        Lv ll, bf16 *__restrict__ gD, int act)
 {
 	const int g = C / 8;
 	const long long total = (long long)ll.H * ll.W * g;
@@ -280,7 +283,7 @@ __global__ void KUpBack(int C, const bf16 *__restrict__ gU, int cs, int coff, Lv
 			float d[8];
 			Load8(D + (size_t)q * C + c, d);
 #pragma unroll
-			for(int e = 0; e < 8; ++e) o[e] = d[e] > 0.0f ? s[e] : 0.0f;
+			for(int e = 0; e < 8; ++e) o[e] = (!act || d[e] > 0.0f) ? s[e] : 0.0f;
 		}
 		Store8(gD + (size_t)q * C + c, o);
 	}
@@ -290,7 +293,7 @@ __global__ void KUpBack(int C, const bf16 *__restrict__ gU, int cs, int coff, Lv
 //  level l): its skip part from gU plus a quarter of the pooled gradient gP
 //  (level l+1) of its parent, where E is positive
 __global__ void KSkipBack(int C, const bf16 *__restrict__ gU, const bf16 *__restrict__ U, int cs, Lv lh,
-                          const bf16 *__restrict__ gP, Lv ll, bf16 *__restrict__ gE)
+                          const bf16 *__restrict__ gP, Lv ll, bf16 *__restrict__ gE, int act)
 {
 	const int g = C / 8;
 	const long long total = (long long)lh.H * lh.W * g;
@@ -306,7 +309,7 @@ __global__ void KSkipBack(int C, const bf16 *__restrict__ gU, const bf16 *__rest
 			Load8(gP + ((size_t)(y >> 1) * ll.W + (x >> 1)) * C + c, b);
 			Load8(U + (size_t)p * cs + c, e8);
 #pragma unroll
-			for(int e = 0; e < 8; ++e) o[e] = e8[e] > 0.0f ? a[e] + 0.25f * b[e] : 0.0f;
+			for(int e = 0; e < 8; ++e) o[e] = (!act || e8[e] > 0.0f) ? a[e] + 0.25f * b[e] : 0.0f;
 		}
 		Store8(gE + (size_t)p * C + c, o);
 	}
@@ -351,7 +354,24 @@ __global__ void KAux(int n, const double *__restrict__ vals, const int *__restri
 	}
 }
 
-//  the input image: channel 0 r / rms, 1 and 2 the features, 3..15 zero
+//  The input channels of a pixel: the residual r (normalised) and its
+//  products with the two features and their squares and product -- every
+//  channel linear in r, so that without activations the network is a linear
+//  operator on r whose coefficients vary with the matrix diagonal and the
+//  film height
+__device__ __forceinline__ void InputChannels(float r, float f1, float f2, float (&v)[8])
+{
+	v[0] = r;
+	v[1] = r * f1;
+	v[2] = r * f2;
+	v[3] = (r * f1) * f1;
+	v[4] = (r * f2) * f2;
+	v[5] = (r * f1) * f2;
+	v[6] = 0.0f;
+	v[7] = 0.0f;
+}
+
+//  the input image: channels 0..5 of InputChannels, 6..15 zero
 __global__ void KPackF(int n, int nx, Lv l0, const double *__restrict__ r, const float *__restrict__ inv,
                        const float *__restrict__ aux, bf16 *__restrict__ F, const int *halt)
 {
@@ -365,9 +385,7 @@ __global__ void KPackF(int n, int nx, Lv l0, const double *__restrict__ r, const
 		if(IsReal(l0, p, y, x))
 		{
 			const int i = y * nx + x;
-			v[0] = (float)r[i] * s;
-			v[1] = aux[i];
-			v[2] = aux[n + i];
+			InputChannels((float)r[i] * s, aux[i], aux[n + i], v);
 		}
 		const float zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 		Store8(F + (size_t)p * 16, v);
@@ -375,12 +393,13 @@ __global__ void KPackF(int n, int nx, Lv l0, const double *__restrict__ r, const
 	}
 }
 
-//  z_i = rms (b + sum_c w_c D0[p(i)][c])
+//  z_i = rms s (b + sum_c w_c D0[p(i)][c]), s the training targets' scale
 __global__ void KOut(int n, int nx, Lv l0, const bf16 *__restrict__ D0, const float *__restrict__ w, const float *b,
-                     const double *__restrict__ rms, double *__restrict__ z, const int *halt)
+                     const double *__restrict__ rms, const float *__restrict__ tsc, double *__restrict__ z,
+                     const int *halt)
 {
 	if(halt && *halt != 0) return;
-	const double sc = *rms;
+	const double sc = *rms * (double)*tsc;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
 		const int y = i / nx, x = i - y * nx;
@@ -416,10 +435,11 @@ __global__ void KStoreSample(int n, const double *__restrict__ r, const double *
 }
 
 //  the input image and the target map of a stored pair
-__global__ void KBuildImage(int n, int nx, Lv l0, const float *__restrict__ slot, bf16 *__restrict__ F,
-                            float *__restrict__ T)
+__global__ void KBuildImage(int n, int nx, Lv l0, const float *__restrict__ slot, const float *__restrict__ tsc,
+                            bf16 *__restrict__ F, float *__restrict__ T)
 {
 	const int HW = l0.H * l0.W;
+	const float inv = 1.0f / *tsc;
 	for(int p = blockIdx.x * blockDim.x + threadIdx.x; p < HW; p += gridDim.x * blockDim.x)
 	{
 		int y, x;
@@ -428,10 +448,8 @@ __global__ void KBuildImage(int n, int nx, Lv l0, const float *__restrict__ slot
 		if(IsReal(l0, p, y, x))
 		{
 			const int i = y * nx + x;
-			v[0] = slot[i];
-			v[1] = slot[2 * n + i];
-			v[2] = slot[3 * n + i];
-			t = slot[n + i];
+			InputChannels(slot[i], slot[2 * n + i], slot[3 * n + i], v);
+			t = slot[n + i] * inv;
 		}
 		const float zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 		Store8(F + (size_t)p * 16, v);
@@ -440,13 +458,25 @@ __global__ void KBuildImage(int n, int nx, Lv l0, const float *__restrict__ slot
 	}
 }
 
+//  sum of z^2 over a stored pair's target, per block (the training set's
+//  target scale)
+__global__ void __launch_bounds__(kRT) KSlotSq(int n, const float *__restrict__ z, float *__restrict__ part)
+{
+	__shared__ double sh[kRT];
+	double a[1] = {0.0};
+	const int i = blockIdx.x * kRT + threadIdx.x;
+	if(i < n) a[0] = (double)z[i] * (double)z[i];
+	BlockTree<1>(a, sh);
+	if(threadIdx.x == 0) part[blockIdx.x] = (float)a[0];
+}
+
 //  The loss over the real pixels, L = sum (out - t)^2 / n, and its
 //  gradient: dL/dD0 (where D0 > 0) as bf16, and per block the partials of
 //  L, dL/dw_c (16) and dL/db in a fixed order (BlockTree)
 constexpr int kLossQ = 18;
 __global__ void __launch_bounds__(kRT) KLoss(int n, Lv l0, const bf16 *__restrict__ D0, const float *__restrict__ T,
                                             const float *__restrict__ w, const float *b, bf16 *__restrict__ gD0,
-                                            float *__restrict__ part)
+                                            float *__restrict__ part, int act)
 {
 	__shared__ double sh[kLossQ * kRT];
 	double a[kLossQ];
@@ -478,7 +508,7 @@ __global__ void __launch_bounds__(kRT) KLoss(int n, Lv l0, const bf16 *__restric
 			for(int c = 0; c < 16; ++c)
 			{
 				a[1 + c] = (double)gr * (double)d[c];
-				g[c] = d[c] > 0.0f ? gr * w[c] : 0.0f;
+				g[c] = (!act || d[c] > 0.0f) ? gr * w[c] : 0.0f;
 			}
 			a[17] = (double)gr;
 		}
@@ -498,7 +528,8 @@ __global__ void __launch_bounds__(kRT) KLoss(int n, Lv l0, const bf16 *__restric
 
 //  the loss partials summed in block order; the output layer's gradient
 //  added to grad, the loss to out[0]
-__global__ void KLossReduce(int nb, const float *__restrict__ part, double *out, float *grad, size_t wOff, size_t bOff)
+__global__ void KLossReduce(int nb, const float *__restrict__ part, double *out, float *grad, size_t wOff, size_t bOff,
+                            int bias)
 {
 	const int q = threadIdx.x;
 	if(q >= kLossQ) return;
@@ -506,7 +537,7 @@ __global__ void KLossReduce(int nb, const float *__restrict__ part, double *out,
 	for(int b = 0; b < nb; ++b) s = s + (double)part[(size_t)b * kLossQ + q];
 	if(q == 0) out[0] = out[0] + s;
 	else if(q < 17) grad[wOff + q - 1] = grad[wOff + q - 1] + (float)s;
-	else grad[bOff] = grad[bOff] + (float)s;
+	else if(bias) grad[bOff] = grad[bOff] + (float)s;
 }
 
 //  per-sample relative error parts: |out - t|^2 and |t|^2 over the real pixels
@@ -561,23 +592,26 @@ __global__ void KOutMap(int n, int nx, Lv l0, const bf16 *__restrict__ D0, const
 //  the blocks are summed in block order by KWReduce
 //==========================================================================
 constexpr int kWgJ = 32;
-constexpr int kWgMaxOut = 32;    // outputs per thread (n x cin <= 8192)
+constexpr int kWgTiles = 2;      // 4 x 4 output tiles per thread (n x cin <= 8192)
 
 __global__ void __launch_bounds__(256) KWGrad(int H, int W, int cin, int n, int pb, const bf16 *__restrict__ x,
                                               const bf16 *__restrict__ dy, float *__restrict__ part,
                                               float *__restrict__ partB)
 {
-	__shared__ float sx[kWgJ * 128];
-	__shared__ float sd[kWgJ * 128];
+	__shared__ __align__(16) float sx[kWgJ * 128];
+	__shared__ __align__(16) float sd[kWgJ * 128];
 	const int tap = blockIdx.y;
 	const int ody = tap / 3 - 1, odx = tap % 3 - 1;
 	const int HW = H * W;
 	const int pBeg = blockIdx.x * pb;
 	const int pEnd = min(HW, pBeg + pb);
 	const int outs = n * cin;
-	float acc[kWgMaxOut];
+	const int tcs = cin / 4, tiles = (n / 4) * tcs;
+	float acc[kWgTiles][16];
 #pragma unroll
-	for(int k = 0; k < kWgMaxOut; ++k) acc[k] = 0.0f;
+	for(int k = 0; k < kWgTiles; ++k)
+#pragma unroll
+		for(int e = 0; e < 16; ++e) acc[k][e] = 0.0f;
 	float accB = 0.0f;
 	for(int base = pBeg; base < pEnd; base += kWgJ)
 	{
@@ -596,15 +630,22 @@ __global__ void __launch_bounds__(256) KWGrad(int H, int W, int cin, int n, int 
 		}
 		__syncthreads();
 #pragma unroll
-		for(int k = 0; k < kWgMaxOut; ++k)
+		for(int k = 0; k < kWgTiles; ++k)
 		{
-			const int o = threadIdx.x + k * blockDim.x;
-			if(o < outs)
+			const int t = threadIdx.x + k * blockDim.x;
+			if(t < tiles)
 			{
-				const int nn = o / cin, ci = o - nn * cin;
-				float s = acc[k];
-				for(int j = 0; j < kWgJ; ++j) s = s + sd[j * n + nn] * sx[j * cin + ci];
-				acc[k] = s;
+				const int n0 = (t / tcs) * 4, c0 = (t - (t / tcs) * tcs) * 4;
+				for(int j = 0; j < kWgJ; ++j)
+				{
+					const float4 av = *reinterpret_cast<const float4 *>(&sd[j * n + n0]);
+					const float4 bv = *reinterpret_cast<const float4 *>(&sx[j * cin + c0]);
+					const float ar[4] = {av.x, av.y, av.z, av.w}, br[4] = {bv.x, bv.y, bv.z, bv.w};
+#pragma unroll
+					for(int u = 0; u < 4; ++u)
+#pragma unroll
+						for(int v = 0; v < 4; ++v) acc[k][u * 4 + v] = acc[k][u * 4 + v] + ar[u] * br[v];
+				}
 			}
 		}
 		if(tap == 0 && threadIdx.x < n)
@@ -612,17 +653,25 @@ __global__ void __launch_bounds__(256) KWGrad(int H, int W, int cin, int n, int 
 		__syncthreads();
 	}
 #pragma unroll
-	for(int k = 0; k < kWgMaxOut; ++k)
+	for(int k = 0; k < kWgTiles; ++k)
 	{
-		const int o = threadIdx.x + k * blockDim.x;
-		if(o < outs) part[((size_t)blockIdx.x * 9 + tap) * outs + o] = acc[k];
+		const int t = threadIdx.x + k * blockDim.x;
+		if(t < tiles)
+		{
+			const int n0 = (t / tcs) * 4, c0 = (t - (t / tcs) * tcs) * 4;
+			float *dst = part + ((size_t)blockIdx.x * 9 + tap) * outs;
+#pragma unroll
+			for(int u = 0; u < 4; ++u)
+#pragma unroll
+				for(int v = 0; v < 4; ++v) dst[(n0 + u) * cin + c0 + v] = acc[k][u * 4 + v];
+		}
 	}
 	if(tap == 0 && threadIdx.x < n) partB[(size_t)blockIdx.x * n + threadIdx.x] = accB;
 }
 
 //  grad W[n][tap][ci] += sum_b part[b][tap][n][ci]; grad b[n] += sum_b partB[b][n]
 __global__ void KWReduce(int nb, int cin, int n, const float *__restrict__ part, const float *__restrict__ partB,
-                         float *__restrict__ grad, size_t wOff, size_t bOff)
+                         float *__restrict__ grad, size_t wOff, size_t bOff, int bias)
 {
 	const int outs = n * cin;
 	const int total = 9 * outs + n;
@@ -637,7 +686,7 @@ __global__ void KWReduce(int nb, int cin, int n, const float *__restrict__ part,
 			const size_t g = wOff + ((size_t)nn * 9 + tap) * cin + ci;
 			grad[g] = grad[g] + s;
 		}
-		else
+		else if(bias)
 		{
 			const int nn = k - 9 * outs;
 			float s = 0.0f;
@@ -702,8 +751,8 @@ int Blocks(long long work, int bs = 256)
 //==========================================================================
 //  Learned
 //==========================================================================
-Learned::Learned(int device, int nx, int ny, int capacity, unsigned seed)
-    : _device(device), _nx(nx), _ny(ny), _n(nx * ny), _cap(capacity)
+Learned::Learned(int device, int nx, int ny, int capacity, unsigned seed, int act)
+    : _device(device), _nx(nx), _ny(ny), _n(nx * ny), _act(act ? 1 : 0), _cap(capacity)
 {
 	if(nx < 8 || ny < 8) throw UsageError("learned: the grid needs at least 8 x 8 points");
 	if(capacity < 2) throw UsageError("learned: the sample capacity must be >= 2");
@@ -741,7 +790,8 @@ Learned::Learned(int device, int nx, int ny, int capacity, unsigned seed)
 	std::mt19937 gen(seed);
 	for(const ConvLayer &L : _conv)
 	{
-		std::normal_distribution<float> nd(0.0f, std::sqrt(2.0f / (9.0f * (float)L.cin)));
+		//  He (ReLU) or Glorot-like (linear) scale
+		std::normal_distribution<float> nd(0.0f, std::sqrt((_act ? 2.0f : 1.0f) / (9.0f * (float)L.cin)));
 		for(size_t k = 0; k < (size_t)9 * L.cin * L.cout; ++k) h[L.wOff + k] = nd(gen);
 	}
 	{
@@ -768,6 +818,10 @@ Learned::Learned(int device, int nx, int ny, int capacity, unsigned seed)
 	_cnt.reserve(4);
 	YZ_CUDA(cudaMemsetAsync(_cnt.get(), 0, 4 * sizeof(unsigned int), st));
 	_outSum.reserve(4);
+	{
+		const float one = 1.0f;
+		_tsc.upload(&one, 1, st);
+	}
 	_err.reserve(1);
 	YZ_CUDA(cudaMemsetAsync(_err.get(), 0, sizeof(int), st));
 	_ring.reserve((size_t)_cap * 4 * _n);
@@ -816,19 +870,19 @@ void Learned::ForwardImage(cudaStream_t st, const int *halt)
 	auto px = [&](int l) { return (long long)_lv[l].H * _lv[l].W; };
 	const ConvLayer &enc0 = _conv[0], &enc1 = _conv[1], &enc2 = _conv[2], &bott = _conv[3], &dec2 = _conv[4],
 	                &dec1 = _conv[5], &dec0 = _conv[6];
-	Conv(enc0, false, _F.get(), _U0.get(), 48, 0, true, st, halt);
+	Conv(enc0, false, _F.get(), _U0.get(), 48, 0, _act != 0, st, halt);
 	YZ_LAUNCH(KPool, Blocks(px(1) * 2), 256, 0, st, 16, 48, _U0.get(), L(0), _P1.get(), L(1), halt);
-	Conv(enc1, false, _P1.get(), _U1.get(), 96, 0, true, st, halt);
+	Conv(enc1, false, _P1.get(), _U1.get(), 96, 0, _act != 0, st, halt);
 	YZ_LAUNCH(KPool, Blocks(px(2) * 4), 256, 0, st, 32, 96, _U1.get(), L(1), _P2.get(), L(2), halt);
-	Conv(enc2, false, _P2.get(), _U2.get(), 128, 0, true, st, halt);
+	Conv(enc2, false, _P2.get(), _U2.get(), 128, 0, _act != 0, st, halt);
 	YZ_LAUNCH(KPool, Blocks(px(3) * 8), 256, 0, st, 64, 128, _U2.get(), L(2), _P3.get(), L(3), halt);
-	Conv(bott, false, _P3.get(), _B3.get(), 64, 0, true, st, halt);
+	Conv(bott, false, _P3.get(), _B3.get(), 64, 0, _act != 0, st, halt);
 	YZ_LAUNCH(KUp, Blocks(px(2) * 8), 256, 0, st, 64, _B3.get(), L(3), _U2.get(), 128, 64, L(2), halt);
-	Conv(dec2, false, _U2.get(), _D2.get(), 64, 0, true, st, halt);
+	Conv(dec2, false, _U2.get(), _D2.get(), 64, 0, _act != 0, st, halt);
 	YZ_LAUNCH(KUp, Blocks(px(1) * 8), 256, 0, st, 64, _D2.get(), L(2), _U1.get(), 96, 32, L(1), halt);
-	Conv(dec1, false, _U1.get(), _D1.get(), 32, 0, true, st, halt);
+	Conv(dec1, false, _U1.get(), _D1.get(), 32, 0, _act != 0, st, halt);
 	YZ_LAUNCH(KUp, Blocks(px(0) * 4), 256, 0, st, 32, _D1.get(), L(1), _U0.get(), 48, 16, L(0), halt);
-	Conv(dec0, false, _U0.get(), _D0.get(), 16, 0, true, st, halt);
+	Conv(dec0, false, _U0.get(), _D0.get(), 16, 0, _act != 0, st, halt);
 }
 
 void Learned::WGrad(const ConvLayer &L, const bf16 *x, const bf16 *dy, cudaStream_t st)
@@ -840,12 +894,12 @@ void Learned::WGrad(const ConvLayer &L, const bf16 *x, const bf16 *dy, cudaStrea
 	if(pb < kWgJ) pb = kWgJ;
 	const int nb = (HW + pb - 1) / pb;
 	const size_t outs = (size_t)L.cout * L.cin;
-	if(outs > (size_t)256 * kWgMaxOut || L.cin > 128 || L.cout > 128) throw UsageError("wgrad: layer too wide");
+	if(outs > (size_t)256 * kWgTiles * 16 || L.cin > 128 || L.cout > 128) throw UsageError("wgrad: layer too wide");
 	_part.reserve((size_t)nb * 9 * outs);
 	_partB.reserve((size_t)nb * L.cout);
 	YZ_LAUNCH(KWGrad, dim3(nb, 9), 256, 0, st, lv.H, lv.W, L.cin, L.cout, pb, x, dy, _part.get(), _partB.get());
 	YZ_LAUNCH(KWReduce, Blocks((long long)9 * outs + L.cout), 256, 0, st, nb, L.cin, L.cout, _part.get(), _partB.get(),
-	          _grad.get(), L.wOff, L.bOff);
+	          _grad.get(), L.wOff, L.bOff, _act);
 }
 
 void Learned::BackwardImage(cudaStream_t st)
@@ -860,28 +914,28 @@ void Learned::BackwardImage(cudaStream_t st)
 	//  dec0: gD0 (from the loss) -> gU0; dW
 	Conv(dec0, true, _gD0.get(), _gU0.get(), 48, 0, false, st, nullptr);
 	WGrad(dec0, _U0.get(), _gD0.get(), st);
-	YZ_LAUNCH(KUpBack, Blocks(px(1) * 4), 256, 0, st, 32, _gU0.get(), 48, 16, L(0), _D1.get(), L(1), _gD1.get());
+	YZ_LAUNCH(KUpBack, Blocks(px(1) * 4), 256, 0, st, 32, _gU0.get(), 48, 16, L(0), _D1.get(), L(1), _gD1.get(), _act);
 	//  dec1
 	Conv(dec1, true, _gD1.get(), _gU1.get(), 96, 0, false, st, nullptr);
 	WGrad(dec1, _U1.get(), _gD1.get(), st);
-	YZ_LAUNCH(KUpBack, Blocks(px(2) * 8), 256, 0, st, 64, _gU1.get(), 96, 32, L(1), _D2.get(), L(2), _gD2.get());
+	YZ_LAUNCH(KUpBack, Blocks(px(2) * 8), 256, 0, st, 64, _gU1.get(), 96, 32, L(1), _D2.get(), L(2), _gD2.get(), _act);
 	//  dec2
 	Conv(dec2, true, _gD2.get(), _gU2.get(), 128, 0, false, st, nullptr);
 	WGrad(dec2, _U2.get(), _gD2.get(), st);
-	YZ_LAUNCH(KUpBack, Blocks(px(3) * 8), 256, 0, st, 64, _gU2.get(), 128, 64, L(2), _B3.get(), L(3), _gB3.get());
+	YZ_LAUNCH(KUpBack, Blocks(px(3) * 8), 256, 0, st, 64, _gU2.get(), 128, 64, L(2), _B3.get(), L(3), _gB3.get(), _act);
 	//  bottleneck
 	Conv(bott, true, _gB3.get(), _gP3.get(), 64, 0, false, st, nullptr);
 	WGrad(bott, _P3.get(), _gB3.get(), st);
 	//  enc2
-	YZ_LAUNCH(KSkipBack, Blocks(px(2) * 8), 256, 0, st, 64, _gU2.get(), _U2.get(), 128, L(2), _gP3.get(), L(3), _gE2.get());
+	YZ_LAUNCH(KSkipBack, Blocks(px(2) * 8), 256, 0, st, 64, _gU2.get(), _U2.get(), 128, L(2), _gP3.get(), L(3), _gE2.get(), _act);
 	Conv(enc2, true, _gE2.get(), _gP2.get(), 32, 0, false, st, nullptr);
 	WGrad(enc2, _P2.get(), _gE2.get(), st);
 	//  enc1
-	YZ_LAUNCH(KSkipBack, Blocks(px(1) * 4), 256, 0, st, 32, _gU1.get(), _U1.get(), 96, L(1), _gP2.get(), L(2), _gE1.get());
+	YZ_LAUNCH(KSkipBack, Blocks(px(1) * 4), 256, 0, st, 32, _gU1.get(), _U1.get(), 96, L(1), _gP2.get(), L(2), _gE1.get(), _act);
 	Conv(enc1, true, _gE1.get(), _gP1.get(), 16, 0, false, st, nullptr);
 	WGrad(enc1, _P1.get(), _gE1.get(), st);
 	//  enc0 (no gradient of the input features)
-	YZ_LAUNCH(KSkipBack, Blocks(px(0) * 2), 256, 0, st, 16, _gU0.get(), _U0.get(), 48, L(0), _gP1.get(), L(1), _gE0.get());
+	YZ_LAUNCH(KSkipBack, Blocks(px(0) * 2), 256, 0, st, 16, _gU0.get(), _U0.get(), 48, L(0), _gP1.get(), L(1), _gE0.get(), _act);
 	WGrad(enc0, _F.get(), _gE0.get(), st);
 }
 
@@ -899,7 +953,7 @@ void Learned::Apply(const double *r, double *z, cudaStream_t st, const int *halt
 	YZ_LAUNCH(KPackF, Blocks((long long)l0.H * l0.W), 256, 0, st, _n, _nx, l0, r, _inv.get(), _aux.get(), _F.get(), halt);
 	ForwardImage(st, halt);
 	YZ_LAUNCH(KOut, Blocks(_n), 256, 0, st, _n, _nx, l0, _D0.get(), _param.get() + _outW, _param.get() + _outB,
-	          _rms.get(), z, halt);
+	          _rms.get(), _tsc.get(), z, halt);
 }
 
 void Learned::AddSample(const double *r, const double *z, cudaStream_t st, const int *halt)
@@ -933,7 +987,7 @@ void Learned::BuildImage(int slot, cudaStream_t st)
 {
 	Lv l0; l0.H = _lv[0].H; l0.W = _lv[0].W; l0.realH = _lv[0].realH; l0.realW = _lv[0].realW;
 	YZ_LAUNCH(KBuildImage, Blocks((long long)l0.H * l0.W), 256, 0, st, _n, _nx, l0,
-	          _ring.get() + (size_t)slot * 4 * _n, _F.get(), _T.get());
+	          _ring.get() + (size_t)slot * 4 * _n, _tsc.get(), _F.get(), _T.get());
 }
 
 void Learned::Check(cudaStream_t st)
@@ -958,6 +1012,27 @@ double Learned::Train(int iters, int batch, float lr, int holdout, double *valEr
 	std::vector<int> train(slots.begin(), slots.end() - holdout), held(slots.end() - holdout, slots.end());
 	Lv l0; l0.H = _lv[0].H; l0.W = _lv[0].W; l0.realH = _lv[0].realH; l0.realW = _lv[0].realW;
 	const int lb = (l0.H * l0.W + kRT - 1) / kRT;
+	if(!_tscSet)
+	{
+		//  the targets' scale over the training pairs: the network learns
+		//  z / (rms(r) s), whose size is then about 1 whatever the system's
+		const int nbz = (_n + kRT - 1) / kRT;
+		DBuf<float> part;
+		part.reserve((size_t)nbz * train.size());
+		for(size_t k = 0; k < train.size(); ++k)
+			YZ_LAUNCH(KSlotSq, nbz, kRT, 0, st, _n, _ring.get() + (size_t)train[k] * 4 * _n + _n,
+			          part.get() + k * nbz);
+		std::vector<float> h((size_t)nbz * train.size());
+		part.download(h.data(), h.size(), st);
+		YZ_CUDA(cudaStreamSynchronize(st));
+		double sum = 0.0;
+		for(float v : h) sum += v;
+		const double mean = sum / ((double)_n * (double)train.size());
+		const float sc = mean > 0 ? (float)std::sqrt(mean) : 1.0f;
+		_tsc.upload(&sc, 1, st);
+		_tscHost = sc;
+		_tscSet = true;
+	}
 	_gD0.reserve((size_t)l0.H * l0.W * 16);
 	_lossPart.reserve((size_t)lb * kLossQ);
 	std::mt19937 gen(12345u + (unsigned)_adamT);
@@ -972,8 +1047,8 @@ double Learned::Train(int iters, int batch, float lr, int holdout, double *valEr
 			BuildImage(s, st);
 			ForwardImage(st, nullptr);
 			YZ_LAUNCH(KLoss, lb, kRT, 0, st, _n, l0, _D0.get(), _T.get(), _param.get() + _outW, _param.get() + _outB,
-			          _gD0.get(), _lossPart.get());
-			YZ_LAUNCH(KLossReduce, 1, 32, 0, st, lb, _lossPart.get(), _outSum.get(), _grad.get(), _outW, _outB);
+			          _gD0.get(), _lossPart.get(), _act);
+			YZ_LAUNCH(KLossReduce, 1, 32, 0, st, lb, _lossPart.get(), _outSum.get(), _grad.get(), _outW, _outB, _act);
 			BackwardImage(st);
 		}
 		++_adamT;
@@ -1060,8 +1135,8 @@ double Learned::LossGrad(const float *feat3, const float *target, float *grad, c
 	BuildImage(s, st);
 	ForwardImage(st, nullptr);
 	YZ_LAUNCH(KLoss, lb, kRT, 0, st, _n, l0, _D0.get(), _T.get(), _param.get() + _outW, _param.get() + _outB,
-	          _gD0.get(), _lossPart.get());
-	YZ_LAUNCH(KLossReduce, 1, 32, 0, st, lb, _lossPart.get(), _outSum.get(), _grad.get(), _outW, _outB);
+	          _gD0.get(), _lossPart.get(), _act);
+	YZ_LAUNCH(KLossReduce, 1, 32, 0, st, lb, _lossPart.get(), _outSum.get(), _grad.get(), _outW, _outB, _act);
 	BackwardImage(st);
 	double l = 0;
 	YZ_CUDA(cudaMemcpyAsync(&l, _outSum.get(), sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1092,6 +1167,7 @@ void Learned::Forward(const float *feat3, float *out, cudaStream_t st)
 	          o.get());
 	o.download(out, (size_t)_n, st);
 	YZ_CUDA(cudaStreamSynchronize(st));
+	for(int i = 0; i < _n; ++i) out[i] *= _tscHost;
 	Check(st);
 }
 

@@ -25,12 +25,13 @@ class LearnedConfig(ctypes.Structure):
     """yz_learned_cfg: the step's learned preconditioner."""
     _fields_ = [("collect_solves", ctypes.c_int), ("samples_per_solve", ctypes.c_int), ("capacity", ctypes.c_int),
                 ("train_iters", ctypes.c_int), ("batch", ctypes.c_int), ("lr", ctypes.c_float),
-                ("holdout", ctypes.c_int), ("cap_factor", ctypes.c_double), ("seed", ctypes.c_uint)]
+                ("holdout", ctypes.c_int), ("cap_factor", ctypes.c_double), ("seed", ctypes.c_uint),
+                ("activation", ctypes.c_int)]
 
 
 def default_config(**over) -> LearnedConfig:
     d = {"collect_solves": 6, "samples_per_solve": 8, "capacity": 48, "train_iters": 300, "batch": 4,
-         "lr": 1e-3, "holdout": 4, "cap_factor": 1.0, "seed": 1}
+         "lr": 1e-3, "holdout": 4, "cap_factor": 1.0, "seed": 1, "activation": 0}
     d.update(over)
     return LearnedConfig(**d)
 
@@ -41,7 +42,7 @@ def _bind():
     if _BOUND:
         return L
     vp = ctypes.c_void_p
-    L.yz_unet_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint,
+    L.yz_unet_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_int,
                                  ctypes.POINTER(vp)]
     L.yz_unet_destroy.argtypes = [vp]
     L.yz_unet_param_count.argtypes = [vp]
@@ -71,11 +72,12 @@ def _f32(a) -> np.ndarray:
 class UNet:
     """The device network of one grid (nx x ny points, ghosts included)."""
 
-    def __init__(self, nx: int, ny: int, capacity: int = 64, seed: int = 1, device: int = 0):
+    def __init__(self, nx: int, ny: int, capacity: int = 64, seed: int = 1, activation: int = 0, device: int = 0):
         L = _bind()
         self.nx, self.ny, self.n = nx, ny, nx * ny
+        self.activation = activation
         self._h = ctypes.c_void_p()
-        _check(L.yz_unet_create(device, nx, ny, capacity, seed, ctypes.byref(self._h)), "yz_unet_create")
+        _check(L.yz_unet_create(device, nx, ny, capacity, seed, activation, ctypes.byref(self._h)), "yz_unet_create")
 
     @property
     def handle(self):
@@ -140,9 +142,9 @@ class UNet:
 
 
 def features(r, diag, h=None):
-    """The network's three normalised input maps of a residual (float32,
-    3 x n): r / rms(r), log10 |diag| / 4, log10 h / 2 + 1 (0 without h) --
-    as the device forms them (yz_learned.h)."""
+    """The three normalised maps the network's inputs are formed from
+    (float32, 3 x n): r / rms(r), log10 |diag| / 4, log10 h / 2 + 1 (0
+    without h) -- as the device forms them (yz_learned.h)."""
     r = np.asarray(r, np.float64)
     rms = np.sqrt(np.sum(r * r) / r.size)
     f = np.zeros((3, r.size), np.float32)
