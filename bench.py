@@ -76,11 +76,27 @@ PATHS = {
     "fp32m_reuse": "FP32 V-cycle and FP32 matrix values in the BiCGStab's SpMVs (vectors, dot products and "
                    "recurrences FP64; the Newton residual FP64), each AMG set-up serving several solves, the "
                    "BiCGStab loop replayed as a cached CUDA graph",
+    "learned": "the learned preconditioner: a U-Net (BF16 tcgen05 convolutions, FP32 accumulation) trained on the "
+               "device during the warm-up steps on the (residual, V-cycle) pairs of the first film solves, tried "
+               "first in a flexible BiCGStab on every film solve, SA-AMG (the fp32m_reuse form) as its fallback "
+               "and judge",
 }
 DTYPES = {"fp64": "f64", "fp32_cycle": "f64 (V-cycle f32)", "fp32_reuse": "f64 (V-cycle f32)",
-          "fp32m_reuse": "f64 Newton / f32 matrix and V-cycle in an f64 Krylov"}
-#  arm -> (arithmetic of the solve, AMG hierarchy reuse on)
-ARMS = {"fp64": (0, False), "fp32_cycle": (1, False), "fp32_reuse": (1, True), "fp32m_reuse": (2, True)}
+          "fp32m_reuse": "f64 Newton / f32 matrix and V-cycle in an f64 Krylov",
+          "learned": "f64 Newton / bf16 network (f32 accumulation), f32 matrix and V-cycle fallback in an f64 Krylov"}
+#  arm -> (arithmetic of the solve, AMG hierarchy reuse on, learned preconditioner on)
+ARMS = {"fp64": (0, False, False), "fp32_cycle": (1, False, False), "fp32_reuse": (1, True, False),
+        "fp32m_reuse": (2, True, False), "learned": (2, True, True)}
+
+
+def learned_config():
+    """The learned arm's settings: the first six film solves (two steps)
+    collect up to eight pairs each, the solve after them trains the network
+    (200 Adam steps of four pairs, four held out), and every later film solve
+    tries it first within three times the last SA-AMG solve's iterations."""
+    from yuzen_b200 import learned
+    return learned.default_config(collect_solves=6, samples_per_solve=8, capacity=48, train_iters=200, batch=4,
+                                  holdout=4, cap_factor=3.0, seed=1, activation=0)
 
 
 def spmv_alpha_bytes(n: int, nnz: int) -> int:
@@ -289,23 +305,40 @@ def run_device_arm(a) -> None:
         each timed on the device (CUDA events inside the step) and, around the
         same calls, end to end on the host clock: the film uploaded from
         pinned host memory, the step, the film read back"""
-        precision, reuse = ARMS[name]
+        precision, reuse, learn = ARMS[name]
         st = ys.Step(params, state["field_h0"], state["field_c0"], state["field_s0"], device=local)
         st.set_precision(precision)
         st.set_amg_reuse(a.amg_reuse if reuse else 0)
+        if learn:
+            st.set_learned(learned_config())
         out = {"total_ms": 0.0, "wall_s": 0.0, "newton": 0, "linear": 0, "launches": 0, "conc_solves": 0,
                "conc_iters": 0, "per_step": [], "per_setup": [], "warmup": 0,
-               "parts": {"setup_ms": 0.0, "solve_ms": 0.0, "assemble_ms": 0.0}}
+               "parts": {"setup_ms": 0.0, "solve_ms": 0.0, "assemble_ms": 0.0},
+               "learned": {"solves": 0, "fallbacks": 0, "iterations": 0, "train_ms": 0.0, "val_err": None,
+                           "samples": 0, "warmup_solves": 0, "warmup_fallbacks": 0}}
         done = 0
+        def note_learned(r, timed):
+            L = out["learned"]
+            if timed:
+                L["solves"] += r["learned_solves"]
+                L["fallbacks"] += r["learned_fallbacks"]
+                L["iterations"] += r["learned_iterations"]
+            else:
+                L["warmup_solves"] += r["learned_solves"]
+                L["warmup_fallbacks"] += r["learned_fallbacks"]
+            L["train_ms"] += r["learned_train_ms"]
+            L["val_err"] = r["learned_val_err"]
+            L["samples"] = r["learned_samples"]
         if fx is not None:
             r = st.advance(fx["steps"])
+            note_learned(r, False)
             done = fx["steps"]
             h, c = st.fields()
             out["h_err_vs_oracle"] = rel(h, fx["h"])
             out["c_err_vs_oracle"] = rel(c, fx["c"]) if fx["c"] is not None else None
             out["t_err_vs_oracle"] = abs(r["time"] - fx["t_end"]) / abs(fx["t_end"])
         if a.warmup > done:
-            st.advance(a.warmup - done)
+            note_learned(st.advance(a.warmup - done), False)
             done = a.warmup
         out["warmup"] = done
         st.fields_into(hpin, cpin)
@@ -328,6 +361,7 @@ def run_device_arm(a) -> None:
             out["launches"] += r["launches"]
             out["conc_solves"] += r["conc_solves"]
             out["conc_iters"] += r["conc_iterations"]
+            note_learned(r, True)
             for k in out["parts"]:
                 out["parts"][k] += r[k]
         if dist:
@@ -424,6 +458,7 @@ def run_device_arm(a) -> None:
                 "l2": "flushed between steps (256 MiB write)",
                 "path": PATHS[head_name], "arm": head_name,
                 "amg_reuse": a.amg_reuse if ARMS[head_name][1] else 0,
+                "learned_preconditioner": head_name == "learned",
                 "warmup_steps": head["warmup"]}
     if fx is not None:
         cfg_line.update({
@@ -441,7 +476,17 @@ def run_device_arm(a) -> None:
                             "conc_solves": v["conc_solves"], "conc_iterations": v["conc_iters"],
                             "device_ms": {q: round(w, 3) for q, w in v["parts"].items()},
                             "step_ms": v["per_step"], "setup_ms_per_step": v["per_setup"],
-                            "gpu_launches": v["launches"]} for k, v in arms.items()}
+                            "gpu_launches": v["launches"],
+                            **({"learned": v["learned"]} if ARMS[k][2] else {})} for k, v in arms.items()}
+    if "learned" in arms:
+        L = arms["learned"]
+        cfg_line["learned_steps_per_s"] = L["value"]
+        cfg_line["learned_vs_fp64"] = L["value"] / arms["fp64"]["value"] if "fp64" in arms else None
+        cfg_line["learned_h_err_vs_oracle"] = L.get("h_err_vs_oracle")
+        cfg_line["learned_solves"] = L["learned"]["solves"]
+        cfg_line["learned_fallbacks"] = L["learned"]["fallbacks"]
+        cfg_line["learned_val_err"] = L["learned"]["val_err"]
+        cfg_line["learned_train_ms"] = L["learned"]["train_ms"]
     cfg_line["finite"] = all(v["finite"] for v in arms.values())
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
@@ -495,7 +540,9 @@ def run_ensemble_arm(a) -> None:
     arms = {}
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     for name in [x for x in a.arms.split(",") if x]:
-        prec, reuse = ARMS[name]
+        prec, reuse, learn = ARMS[name]
+        if learn:
+            continue        # the ensemble has no learned arm
         ens = ensemble.Ensemble([batch[k] for k in mine], device=local, precision=prec,
                                 amg_reuse=a.amg_reuse if reuse else 0, workers=a.workers,
                                 graph_loop=None if a.ensemble_graph < 0 else bool(a.ensemble_graph))
@@ -595,9 +642,9 @@ def main() -> None:
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=6, help="steps of the ensemble's end-to-end measurement")
-    ap.add_argument("--arms", default="fp64,fp32_cycle,fp32_reuse,fp32m_reuse",
-                    help="the arms timed, in order (fp64, fp32_cycle, fp32_reuse, fp32m_reuse); headline: the "
-                         "fastest one whose film is within 1e-8 of the FP64 arm's")
+    ap.add_argument("--arms", default="fp64,fp32_cycle,fp32_reuse,fp32m_reuse,learned",
+                    help="the arms timed, in order (fp64, fp32_cycle, fp32_reuse, fp32m_reuse, learned); headline: "
+                         "the fastest one whose film is within 1e-8 of the reference's run")
     ap.add_argument("--amg-reuse", type=int, default=64, help="solves an AMG set-up serves in the fp32_reuse arm")
     ap.add_argument("--roofline-steps", type=int, default=3, help="steps over which the roofline kernel is timed")
     ap.add_argument("--workers", type=int, default=64, help="host threads advancing the ensemble's instances")

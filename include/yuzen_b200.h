@@ -139,6 +139,15 @@ int yz_time_kernel(const char* name);
 /* Device time summed over the timed launches, and their count. */
 int yz_kernel_time(double* total_ms, long long* launches);
 
+/* Fault injection, the test switch of the reference's amgcl backend
+ * (LinearSolverBackend.cpp:630-645, environment YUZEN_FAULT_AMGCL=k:m, which
+ * this library reads too): `count` solves of the process, from the at-th of
+ * those that reach the SA-AMG or Jacobi path on, break down before they
+ * iterate -- return 2, x left as given, unless x already meets the
+ * tolerance -- so that a step cuts dt and retries (or, at a fixed step,
+ * fails with -3).  at = 0 switches it off; the call restarts the count. */
+int yz_fault_inject(long long at, long long count);
+
 /* Building blocks exposed for the parity tests: the deterministic dot
  * product every reduction of the solve uses, and CRS_Matrix::MatVec
  * (CRS_Matrix.cpp:307-329), on host arrays through the device. */
@@ -292,6 +301,18 @@ int yz_step_get_fields(yz_step* st, double* h, double* c);
  * the film the next step starts from, as C_ImplicitSolver::SetX takes it
  * (phi_old = phi_new = h, ImplicitSolver.cpp:94-101). */
 int yz_step_set_fields(yz_step* st, const double* h, const double* c);
+/* The state a later step depends on (the reference's RestartState,
+ * IO/RestartState.h:57): the film and concentration, phi_old, phi_old2,
+ * phi_new, the last Newton correction (the next solve's guess), the clock
+ * and its controller, the Eisenstat-Walker and extrapolation memory, the
+ * solvers' TryBackoff counters and the energy history, as
+ * yz_step_state_size() doubles.  A step given a state with yz_step_set_state
+ * continues as the step it was taken from would have, bit for bit on the
+ * FP64 path (an AMG hierarchy kept for reuse is not part of the state: the
+ * next solve of a reuse form sets one up). */
+long long yz_step_state_size(const yz_step* st);
+int yz_step_get_state(yz_step* st, double* out);
+int yz_step_set_state(yz_step* st, const double* in, long long len);
 /* The fixed CRS pattern of A / I + theta dt J, storage order (diagonal
  * first): rowptr n+1, col nnz, boundary flags n.  nnz is returned. */
 int yz_step_pattern(yz_step* st, int* rowptr, int* col, int* bc);

@@ -52,6 +52,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -686,6 +687,28 @@ struct TryBackoff
 
 } // namespace
 
+//--------------------------------------------------------------------------
+//  Fault injection (LinearSolverBackend.cpp:630-645): YUZEN_FAULT_AMGCL=k:m
+//  makes m solves of the process, from the k-th on, that reach the AMG /
+//  Jacobi path break down before they iterate (m = 1 if left out).  The
+//  count is of the process, over every solver.
+//--------------------------------------------------------------------------
+struct Fault
+{
+	long at = 0, count = 0, solves = 0;
+	Fault()
+	{
+		if(const char *e = std::getenv("YUZEN_FAULT_AMGCL"))
+		{
+			char *end = nullptr;
+			at = std::strtol(e, &end, 10);
+			count = (end && *end == ':') ? std::strtol(end + 1, nullptr, 10) : 1;
+		}
+	}
+	bool Now() { return at > 0 && ++solves >= at && solves < at + count; }
+};
+Fault &TheFault() { static Fault f; return f; }
+
 //==========================================================================
 struct yzo_solver
 {
@@ -813,7 +836,8 @@ int yzo_solve(yzo_solver *S, const yzo_settings *set, int n,
 		}
 	}
 	bool broke = false;
-	if(!done)
+	if(!done && TheFault().Now()) broke = true;
+	else if(!done)
 	{
 		try
 		{
@@ -856,6 +880,12 @@ int yzo_solve(yzo_solver *S, const yzo_settings *set, int n,
 	if(err <= set->epsilon) return 0;
 	if(!(err == err)) return 2;
 	return 1;
+}
+
+void yzo_fault_inject(long at, long count)
+{
+	Fault &f = TheFault();
+	f.at = at; f.count = count; f.solves = 0;
 }
 
 int yzo_memory(const yzo_solver *s, double *out, int cap)

@@ -62,6 +62,12 @@ int yzo_solve(yzo_solver* s, const yzo_settings* set, int n,
               const double* values, const double* rhs, double* x,
               int* iter, double* resid);
 
+/* The fault switch of LinearSolverBackend.cpp:630-645 (also read from
+ * YUZEN_FAULT_AMGCL=k:m at the first solve): solves at .. at+count-1 of the
+ * process that reach the AMG / Jacobi path break down before iterating;
+ * at = 0 switches it off.  Resets the process's solve count. */
+void yzo_fault_inject(long at, long count);
+
 /* TryBackoff counters (ILinearSolverBackend::Memory / SetMemory). */
 int  yzo_memory(const yzo_solver* s, double* out, int cap);
 void yzo_set_memory(yzo_solver* s, const double* m, int len);

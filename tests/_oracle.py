@@ -46,6 +46,7 @@ def lib():
     L.yzo_dot.restype = ctypes.c_double
     L.yzo_dot.argtypes = [ctypes.c_int, _f64p, _f64p]
     L.yzo_spmv.argtypes = [ctypes.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
+    L.yzo_fault_inject.argtypes = [ctypes.c_long, ctypes.c_long]
     _L = L
     return L
 
@@ -126,3 +127,8 @@ def spmv(rowptr, col, val, x):
     y = np.zeros(rowptr.size - 1)
     lib().yzo_spmv(rowptr.size - 1, _ip(rowptr), _ip(col), _fp(val), _fp(x), _fp(y))
     return y
+
+
+def fault_inject(at: int, count: int = 1) -> None:
+    """The oracle's copy of the reference's YUZEN_FAULT_AMGCL switch."""
+    lib().yzo_fault_inject(at, count)

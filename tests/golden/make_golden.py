@@ -268,12 +268,29 @@ def write_case(ref: Path, src: str, over: dict, name: str, work: Path) -> Path:
     return case
 
 
-def make_step_case(ref: Path, name: str, work: Path) -> dict:
+#  Whole-step cases under the reference's fault switch (YUZEN_FAULT_AMGCL,
+#  LinearSolverBackend.cpp:630-645): name: (step case, the switch's k:m for
+#  the reference's run, the same solve counted on the device).  The reference
+#  counts its three set-up solves of the boundary rows before the first Newton
+#  solve; the device step has none, so its count is three less.
+FAULT_STEP_CASES = {
+    # the capillary + disjoining film with the time-step control, its third
+    # Newton solve broken down: the step is cut and retried
+    "fault_adaptive_40": ("step_adaptive_40", "6:1", (3, 1)),
+    # the same with two solves in a row broken down (the cut step's first
+    # solve too)
+    "fault2_adaptive_40": ("step_adaptive_40", "8:2", (5, 2)),
+}
+
+
+def make_step_case(ref: Path, name: str, work: Path, fault: str | None = None) -> dict:
     src, over, steps, first = STEP_CASES[name]
     case = write_case(ref, src, {**over, "Numerics.MaxSteps": steps, "Output.Energy.Enable": True}, name, work)
     dump = work / f"dump_{name}"
     dump.mkdir()
     env = dict(os.environ, YZO_DUMP_DIR=str(dump), YZO_DUMP_MAX="8", OMP_NUM_THREADS="4")
+    if fault:
+        env["YUZEN_FAULT_AMGCL"] = fault
     res = subprocess.run([str(PROBE), case.name, f"{name}.bin"], cwd=work, env=env, capture_output=True,
                          text=True, timeout=900)
     if res.returncode != 0:
@@ -369,6 +386,16 @@ def main() -> None:
             if a.only and name != a.only:
                 continue
             d = make_step_case(Path(a.ref), name, Path(tmp))
+            stateio.save_npz(HERE / f"{name}.npz", d)
+            print(name, d["nx"], d["ny"], "steps", d["steps_done"], "t_end", d["t_end"])
+        for name, (base, fault, dev) in FAULT_STEP_CASES.items():
+            if a.only and name != a.only:
+                continue
+            d = make_step_case(Path(a.ref), base, Path(tmp) / name if (Path(tmp) / name).mkdir() is None else None,
+                               fault=fault)
+            d["case"] = name
+            d["fault_reference"] = fault
+            d["fault_at"], d["fault_count"] = dev
             stateio.save_npz(HERE / f"{name}.npz", d)
             print(name, d["nx"], d["ny"], "steps", d["steps_done"], "t_end", d["t_end"])
         for name in BUILT_STEP_CASES:

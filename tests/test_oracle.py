@@ -135,3 +135,18 @@ def test_reference_unit_tests_pass_with_oracle():
                        env={"OMP_NUM_THREADS": "4", "PATH": "/usr/bin:/bin"})
     assert r.returncode == 0, r.stdout[-3000:]
     assert "Status: SUCCESS" in r.stdout
+
+
+def test_oracle_fault_switch():
+    """The oracle's copy of the reference's YUZEN_FAULT_AMGCL switch: the
+    chosen solve returns 2 before iterating and leaves x as given."""
+    import _systems
+    d = _systems.film_system(40, seed=7)
+    x0 = np.full(d["n"], 0.5)
+    _oracle.fault_inject(1, 1)
+    try:
+        ret, it, res, x = _oracle.OracleSolver().solve(d, x0=x0)
+        assert ret == 2 and it == 0 and np.array_equal(x, x0)
+        assert _oracle.OracleSolver().solve(d, x0=x0)[0] == 0
+    finally:
+        _oracle.fault_inject(0, 0)

@@ -44,7 +44,8 @@ EXPORTED_SYMBOLS = (
     "yz_unet_create", "yz_unet_destroy", "yz_unet_param_count", "yz_unet_get_params", "yz_unet_set_params",
     "yz_unet_forward", "yz_unet_loss_grad", "yz_unet_add_sample", "yz_unet_samples", "yz_unet_train",
     "yz_unet_apply", "yz_solver_set_learned", "yz_solver_set_aux", "yz_solver_learned_stats",
-    "yz_step_set_learned", "yz_conv3x3",
+    "yz_step_set_learned", "yz_conv3x3", "yz_fault_inject", "yz_step_state_size", "yz_step_get_state",
+    "yz_step_set_state",
 )
 
 #: the preconditioner's arithmetic (YZ_PREC_* of include/yuzen_b200.h)
@@ -365,3 +366,12 @@ def dot_noalloc(n: int, x_ptr: int, y_ptr: int, out_ptr: int, stream: int = 0) -
     """yz_dot_noalloc on device pointers (the caller owns every buffer)."""
     _check(lib().yz_dot_noalloc(int(n), ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), ctypes.c_void_p(out_ptr),
                                 ctypes.c_void_p(stream) if stream else None), "yz_dot_noalloc")
+
+
+def fault_inject(at: int, count: int = 1) -> None:
+    """The reference's fault switch (YUZEN_FAULT_AMGCL=at:count): `count`
+    solves of the process from the at-th that reaches the SA-AMG / Jacobi path
+    break down before iterating; at = 0 off (yz_fault_inject)."""
+    L = lib()
+    L.yz_fault_inject.argtypes = [ctypes.c_longlong, ctypes.c_longlong]
+    _check(L.yz_fault_inject(at, count), "yz_fault_inject")

@@ -338,21 +338,28 @@ class Case:
                 "ev_h_ast": self.precursor, "evap_hast_modify": int(self.precursor != 0.0)}
 
     # ------------------------------------------------------------------
+    def write_fields(self, path, h, c) -> None:
+        """h, c (and this case's substrate s) on the whole grid (nx*ny) as an
+        ASCII field file of the reference's restart (columns x y h+s u v c h
+        s, rows of grid points 1..nx-2 x 1..ny-2, iy outer, non-dimensional)."""
+        _, _, s = self.fields()
+        nx, ny = self.Nx + 4, self.Ny + 4
+        lines = ["# x y h+s u v c h s"]
+        for iy in range(1, ny - 1):
+            for ix in range(1, nx - 1):
+                i = iy * nx + ix
+                hi, ci, si = float(h[i]), float(c[i]), float(s[i])
+                lines.append(f"{float(ix)!r} {float(iy)!r} {hi + si!r} 0.0 0.0 {ci!r} {hi!r} {si!r}")
+        Path(path).write_text("\n".join(lines) + "\n")
+
     def write_reference(self, workdir) -> Path:
         """case.toml and the ASCII restart init.dat (columns x y h+s u v c h s,
         rows of grid points 1..nx-2 x 1..ny-2, iy outer; non-dimensional,
         read with coefficient 1 as Output.Dimensioned = false makes it)."""
         w = Path(workdir)
         w.mkdir(parents=True, exist_ok=True)
-        h, c, s = self.fields()
-        nx, ny = self.Nx + 4, self.Ny + 4
-        lines = ["# x y h+s u v c h s (synthetic initial film)"]
-        for iy in range(1, ny - 1):
-            for ix in range(1, nx - 1):
-                i = iy * nx + ix
-                hi, ci, si = float(h[i]), float(c[i]), float(s[i])
-                lines.append(f"{float(ix)!r} {float(iy)!r} {hi + si!r} 0.0 0.0 {ci!r} {hi!r} {si!r}")
-        (w / "init.dat").write_text("\n".join(lines) + "\n")
+        h, c, _ = self.fields()
+        self.write_fields(w / "init.dat", h, c)
         (w / "case.toml").write_text(toml_dumps(self.toml("init.dat")))
         return w / "case.toml"
 

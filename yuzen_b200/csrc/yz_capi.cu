@@ -309,6 +309,26 @@ int yz_step_set_fields(yz_step *st, const double *h, const double *c)
 	});
 }
 
+long long yz_step_state_size(const yz_step *st) { return st ? (long long)st->s->StateSize() : -1; }
+
+int yz_step_get_state(yz_step *st, double *out)
+{
+	return Guard([&] {
+		if(!st || !out) throw yz::UsageError("yz_step_get_state: null argument");
+		st->s->GetState(out);
+		return 0;
+	});
+}
+
+int yz_step_set_state(yz_step *st, const double *in, long long len)
+{
+	return Guard([&] {
+		if(!st || !in || len <= 0) throw yz::UsageError("yz_step_set_state: null argument");
+		st->s->SetState(in, (size_t)len);
+		return 0;
+	});
+}
+
 int yz_step_pattern(yz_step *st, int *rowptr, int *col, int *bc)
 {
 	return Guard([&] {
@@ -494,6 +514,15 @@ int yz_step_set_learned(yz_step *st, const yz_learned_cfg *cfg)
 	return Guard([&] {
 		if(!st) throw yz::UsageError("yz_step_set_learned: null step");
 		st->s->SetLearned(cfg);
+		return 0;
+	});
+}
+
+int yz_fault_inject(long long at, long long count)
+{
+	return Guard([&] {
+		if(at < 0 || count < 0) throw yz::UsageError("yz_fault_inject: at and count must be >= 0");
+		yz::FaultInject((long)at, (long)count);
 		return 0;
 	});
 }

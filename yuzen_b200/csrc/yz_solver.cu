@@ -12,6 +12,7 @@
 #include "yz_solver_impl.h"
 
 #include <map>
+#include <mutex>
 #include <type_traits>
 
 #include <algorithm>
@@ -260,6 +261,49 @@ __global__ void KDot(int n, const double *__restrict__ x, const double *__restri
 }
 
 #undef YZ_CHUNK_LOOP
+
+//==========================================================================
+//  Fault injection: the switch of the reference's amgcl backend
+//  (LinearSolverBackend.cpp:630-645).  YUZEN_FAULT_AMGCL=k:m (read at the
+//  first solve) or FaultInject(k, m) makes m solves of the process, from the
+//  k-th of those that reach the SA-AMG / Jacobi path on, break down before
+//  they iterate -- the reference's "Zero rho in BiCGStab" -- so that the
+//  caller sees the breakdown return (2) and the step its cut-and-retry.
+//==========================================================================
+namespace {
+struct FaultState
+{
+	long at = 0, count = 0, solves = 0;
+	bool read = false;
+};
+std::mutex g_faultMutex;
+FaultState g_fault;
+
+bool FaultNow()
+{
+	std::lock_guard<std::mutex> lk(g_faultMutex);
+	if(!g_fault.read)
+	{
+		g_fault.read = true;
+		if(const char *e = std::getenv("YUZEN_FAULT_AMGCL"))
+		{
+			char *end = nullptr;
+			g_fault.at = std::strtol(e, &end, 10);
+			g_fault.count = (end && *end == ':') ? std::strtol(end + 1, nullptr, 10) : 1;
+		}
+	}
+	return g_fault.at > 0 && ++g_fault.solves >= g_fault.at && g_fault.solves < g_fault.at + g_fault.count;
+}
+} // namespace
+
+void FaultInject(long at, long count)
+{
+	std::lock_guard<std::mutex> lk(g_faultMutex);
+	g_fault.read = true;
+	g_fault.at = at;
+	g_fault.count = count;
+	g_fault.solves = 0;
+}
 
 //==========================================================================
 //  Solver
@@ -1133,7 +1177,8 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 			++_lstats.skipped;
 	}
 	bool broke = false;
-	if(!done)
+	if(!done && FaultNow()) broke = true;
+	else if(!done)
 	{
 		if(set.precondition == 0 || set.precondition == 1)
 		{

@@ -207,5 +207,6 @@ void TimeSelect(const char *name);
 void DotNoAlloc(int n, const double *dx, const double *dy, double *dout, cudaStream_t st);
 long long NoAllocMaxElements();
 void TimeRead(double *ms, long long *count);
+void FaultInject(long at, long count);
 
 } // namespace yz

@@ -1256,6 +1256,61 @@ void Step::SetFields(const double *h, const double *c)
 	}
 }
 
+//  The state of the step between two calls, the counterpart of the
+//  reference's RestartState (IO/RestartState.h:57): the committed film and
+//  concentration, the films of the two steps before (phi_old, phi_old2) and
+//  the last accepted one (phi_new), the last Newton correction (the next
+//  solve's initial guess, LastCorrection), the clock and its controller
+//  (dt, dt of the step before, a pending dt change, the step-keep count),
+//  the Eisenstat-Walker and extrapolation memory, the solvers' TryBackoff
+//  counters and the energy history.  Layout: kStateHead doubles -- a tag,
+//  n, then the scalars in the order written below -- then six fields of n.
+namespace { constexpr size_t kStateHead = 24; constexpr double kStateTag = 20261204.0; }
+
+size_t Step::StateSize() const { return kStateHead + (size_t)6 * _n; }
+
+void Step::GetState(double *out)
+{
+	YZ_CUDA(cudaSetDevice(_device));
+	const size_t n = (size_t)_n;
+	double *o = out;
+	std::fill(o, o + kStateHead, 0.0);
+	o[0] = kStateTag; o[1] = (double)_n;
+	o[2] = _dt; o[3] = _dtOld; o[4] = _time; o[5] = _pendingDt; o[6] = (double)_adjustCount;
+	o[7] = (double)_nkIter; o[8] = _ewEta; o[9] = _ewRhsPrev; o[10] = _extrapMove; o[11] = _lastResid;
+	o[12] = _energyOn ? 1.0 : 0.0; o[13] = _enF; o[14] = _enD; o[15] = _enDiss; o[16] = _enBal;
+	const std::vector<double> mh = _solver->Memory();
+	o[17] = mh.size() > 0 ? mh[0] : 0.0; o[18] = mh.size() > 1 ? mh[1] : 0.0;
+	if(_solverC)
+	{
+		const std::vector<double> mc = _solverC->Memory();
+		o[19] = mc.size() > 0 ? mc[0] : 0.0; o[20] = mc.size() > 1 ? mc[1] : 0.0;
+	}
+	double *f = out + kStateHead;
+	const DBuf<double> *fields[6] = {&_h, &_c, &_hOld, &_hOld2, &_hNew, &_delta};
+	for(int k = 0; k < 6; ++k) fields[k]->download(f + (size_t)k * n, n, _st);
+	YZ_CUDA(cudaStreamSynchronize(_st));
+}
+
+void Step::SetState(const double *in, size_t len)
+{
+	YZ_CUDA(cudaSetDevice(_device));
+	if(len != StateSize() || in[0] != kStateTag || in[1] != (double)_n)
+		throw UsageError("set_state: not a state of this step (wrong size or grid)");
+	const size_t n = (size_t)_n;
+	_dt = in[2]; _dtOld = in[3]; _time = in[4]; _pendingDt = in[5]; _adjustCount = (int)in[6];
+	_nkIter = (int)in[7]; _ewEta = in[8]; _ewRhsPrev = in[9]; _extrapMove = in[10]; _lastResid = in[11];
+	_energyOn = in[12] != 0.0; _enF = in[13]; _enD = in[14]; _enDiss = in[15]; _enBal = in[16];
+	_solver->SetMemory(in + 17, 2);
+	if(_solverC) _solverC->SetMemory(in + 19, 2);
+	const double *f = in + kStateHead;
+	DBuf<double> *fields[6] = {&_h, &_c, &_hOld, &_hOld2, &_hNew, &_delta};
+	for(int k = 0; k < 6; ++k) fields[k]->upload(f + (size_t)k * n, n, _st);
+	YZ_CUDA(cudaMemcpyAsync(_cw.get(), _c.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+	if(_conc) YZ_CUDA(cudaMemcpyAsync(_c0.get(), _c.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+	YZ_CUDA(cudaStreamSynchronize(_st));
+}
+
 void Step::Energy(double &F, double &D)
 {
 	YZ_CUDA(cudaSetDevice(_device));

@@ -24,6 +24,10 @@ public:
 	void Energy(double &F, double &D);
 	void SetEnergy(bool on);
 	void SetFields(const double *h, const double *c);
+	//  the whole state a later step depends on, as a flat array of doubles
+	size_t StateSize() const;
+	void GetState(double *out);
+	void SetState(const double *in, size_t len);
 	int Pattern(int *rowptr, int *col, int *bc) const;
 	void System(const double *hOld, const double *h, double dt, double *ia, double *rhs);
 	int ConcPattern(int *rowptr, int *col) const;

@@ -171,6 +171,31 @@ class Step:
         L = learned._bind()
         _check(L.yz_step_set_learned(self._h, ctypes.byref(cfg) if cfg is not None else None), "yz_step_set_learned")
 
+    def state(self) -> np.ndarray:
+        """The state a later step depends on (yz_step_get_state), a float64
+        array that set_state takes back."""
+        L = lib()
+        L.yz_step_state_size.restype = ctypes.c_longlong
+        L.yz_step_state_size.argtypes = [ctypes.c_void_p]
+        out = np.zeros(int(L.yz_step_state_size(self._h)))
+        _check(L.yz_step_get_state(self._h, _fp(out)), "yz_step_get_state")
+        return out
+
+    def set_state(self, state: np.ndarray) -> None:
+        """Continue from a state taken with state() (yz_step_set_state)."""
+        L = lib()
+        L.yz_step_set_state.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_longlong]
+        a = np.ascontiguousarray(state, np.float64)
+        _check(L.yz_step_set_state(self._h, _fp(a), a.size), "yz_step_set_state")
+
+    def write_field(self, path, case) -> None:
+        """The film as a field file in the reference's ASCII format (columns
+        x y h+s u v c h s over grid points 1..nx-2 x 1..ny-2, non-dimensional;
+        Output.cpp:902-912), which its restart reads back (Restart.h:36-42):
+        `case` is the yuzen_b200.cases.Case the step was built from."""
+        h, c = self.fields()
+        case.write_fields(path, h, c)
+
     def energy(self):
         """(F, D): the free energy of the film the step holds and the flux
         power of the potential (the reference's EnergyEval)."""
