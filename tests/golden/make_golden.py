@@ -270,16 +270,18 @@ def write_case(ref: Path, src: str, over: dict, name: str, work: Path) -> Path:
 
 #  Whole-step cases under the reference's fault switch (YUZEN_FAULT_AMGCL,
 #  LinearSolverBackend.cpp:630-645): name: (step case, the switch's k:m for
-#  the reference's run, the same solve counted on the device).  The reference
-#  counts its three set-up solves of the boundary rows before the first Newton
-#  solve; the device step has none, so its count is three less.
+#  the reference's run, the same solve counted on the device).  The switch
+#  counts the solves of the amgcl backend; the reference's set-up solves of
+#  the boundary rows run on its eigen backend and are not counted, so the
+#  k-th counted solve is the k-th Newton solve of the film on both sides.
 FAULT_STEP_CASES = {
-    # the capillary + disjoining film with the time-step control, its third
-    # Newton solve broken down: the step is cut and retried
-    "fault_adaptive_40": ("step_adaptive_40", "6:1", (3, 1)),
-    # the same with two solves in a row broken down (the cut step's first
-    # solve too)
-    "fault2_adaptive_40": ("step_adaptive_40", "8:2", (5, 2)),
+    # the capillary + disjoining film with the time-step control, the sixth
+    # Newton solve (in the third step) broken down: the attempt fails and is
+    # repeated without the extrapolated start at the same dt
+    "fault_adaptive_40": ("step_adaptive_40", "6:1", (6, 1)),
+    # two solves in a row broken down, the eighth and ninth: the attempt
+    # without the extrapolated start fails too and the step is cut
+    "fault2_adaptive_40": ("step_adaptive_40", "8:2", (8, 2)),
 }
 
 

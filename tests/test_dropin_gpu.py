@@ -42,3 +42,43 @@ def test_reference_run_identical_with_b200_backend(case, tmp_path):
     assert gpu["steps_done"] == cpu["steps_done"] and gpu["t_end"] == cpu["t_end"]
     assert np.array_equal(gpu["field_h1"], cpu["field_h1"])
     assert np.array_equal(gpu["field_c1"], cpu["field_c1"])
+
+
+STEP_B200 = REPO / "oracle" / "_ref" / "yuzen_b200_step"
+
+
+def read_seam2(path: Path) -> dict:
+    """The record yuzen_b200_step writes: magic, nx, ny, steps, Newton passes,
+    the clock, the wall time, linear iterations, then h and c (IL order)."""
+    raw = path.read_bytes()
+    assert raw[:8] == b"YZSEAM21"
+    nx, ny, steps, newton = np.frombuffer(raw, "<i4", 4, 8)
+    t_end, wall, linear = np.frombuffer(raw, "<f8", 3, 24)
+    m = int(nx) * int(ny)
+    h = np.frombuffer(raw, "<f8", m, 48).copy()
+    c = np.frombuffer(raw, "<f8", m, 48 + 8 * m).copy()
+    return {"steps": int(steps), "newton": int(newton), "t_end": float(t_end), "h": h, "c": c}
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c.stem for c in CASES])
+def test_reference_driver_with_the_step_on_the_device(case, tmp_path):
+    """Seam 2: the reference's own set-up of a TOML case (C_Yuzen) with its
+    time loop replaced by the device step (yuzen_b200/host/yz_step_adapter.cpp,
+    the parameters, film and concentration read out of the reference's
+    objects and the result written back into them) against the reference's
+    whole run of the same case: the same steps, the clock to 1e-12, h and c
+    within 1e-10 relative L2."""
+    if not (PROBE.exists() and STEP_B200.exists()):
+        pytest.skip("reference-built binaries not present (make -C oracle ref b200)")
+    cpu = run(PROBE, case, tmp_path / "cpu", {})
+    work = tmp_path / "seam2"
+    work.mkdir()
+    (work / case.name).write_text(case.read_text())
+    r = subprocess.run([str(STEP_B200), case.name, "out.bin"], cwd=work, capture_output=True, text=True, timeout=900,
+                       env=dict(os.environ, OMP_NUM_THREADS="4"))
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    gpu = read_seam2(work / "out.bin")
+    assert gpu["steps"] == cpu["steps_done"]
+    assert abs(gpu["t_end"] - cpu["t_end"]) <= 1e-12 * abs(cpu["t_end"])
+    assert np.linalg.norm(gpu["h"] - cpu["field_h1"]) / np.linalg.norm(cpu["field_h1"]) <= 1e-10
+    assert np.linalg.norm(gpu["c"] - cpu["field_c1"]) / np.linalg.norm(cpu["field_c1"]) <= 1e-10

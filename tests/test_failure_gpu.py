@@ -8,12 +8,12 @@ any fault of the GPU.
 * A NaN in the right-hand side: return 2, x untouched.  An iteration cap of
   one: return 1.
 * The whole step under the switch, against the reference's own run under it
-  (tests/golden/fault_*.npz): a single broken-down Newton solve (its
-  correction thrown away, the pass repeated) and two in a row (the step cut
-  and retried by the time-step control) end on the reference's film and
-  clock.  The reference counts three set-up solves of the boundary rows
-  before its first Newton solve, which the device step does not have, so the
-  device's switch counts three fewer.
+  (tests/golden/fault_*.npz): a single broken-down Newton solve (the attempt
+  fails and is repeated without the extrapolated start) and two in a row
+  (that repeat fails too, and the time-step control cuts the step) end on the
+  reference's film and clock.  The switch counts the film's Newton solves
+  on both sides (the reference's set-up solves of the boundary rows run on
+  its eigen backend, which the switch does not count).
 * At a fixed step a Newton iteration that cannot converge is status -3 with
   the reference's FatalError text (FailedFixedStep, ImplicitSolver.cpp:
   192-201), and the step is usable again after yz_step_set_fields.

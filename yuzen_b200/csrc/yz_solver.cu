@@ -8,6 +8,7 @@
 // by damped Jacobi (None, Jacobi), coarse_enough 500 above 3000 rows (:660-675),
 // a breakdown answered by the residual check of :681-713.
 #include "yz_amg_kernels.cuh"
+#include "yz_coarse.cuh"
 #include "yz_learned.h"
 #include "yz_solver_impl.h"
 
@@ -325,6 +326,10 @@ Solver::Solver(int device, cudaStream_t stream) : _device(device)
 	_counters.reserve(16);
 	YZ_CUDA(cudaMemsetAsync(_counters.get(), 0, 16 * sizeof(unsigned), _st));
 	_flags.reserve(8);
+	_coarseBar.reserve(2);
+	_coarseErr.reserve(1);
+	YZ_CUDA(cudaMemsetAsync(_coarseBar.get(), 0, 2 * sizeof(unsigned), _st));
+	YZ_CUDA(cudaMemsetAsync(_coarseErr.get(), 0, sizeof(int), _st));
 }
 
 Solver::~Solver()
@@ -709,6 +714,17 @@ void Solver::Cycle32(size_t l, const TF *f, TX *x)
 	}
 	const int *so = l == 0 ? _sellOff.get() : nullptr, *col = l == 0 ? _sellCol.get() : L.col.get();
 	const float *val = l == 0 ? _sellVal32.get() : L.val32.get();
+	//  the finest level's smoothing around one persistent launch for all the
+	//  coarser levels (yz_coarse.cuh)
+	if(l == 0 && _nlev > 1 && CoarseCycleOn())
+	{
+		YZ_LAUNCH((KPreSmoothResidual<float, TF, float>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col,
+		          val, L.M32.get(), f, L.x32.get(), L.t32.get());
+		LaunchCoarseCycle();
+		YZ_LAUNCH((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val,
+		          L.M32.get(), f, L.xt32.get(), x);
+		return;
+	}
 	if(l + 1 < _nlev)
 	{
 		Level &C = *_levels[l + 1];
@@ -744,6 +760,64 @@ void Solver::Cycle32(size_t l, const TF *f, TX *x)
 		YZ_LAUNCH((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val, L.M32.get(), f,
 		          L.xt32.get(), x);
 	}
+}
+
+//  The persistent coarse cycle: on while the hierarchy has no more levels than
+//  the launch's plan holds; YZ_COARSE_CYCLE=0 switches it off (the levels
+//  then run as separate kernels)
+bool Solver::CoarseCycleOn() const
+{
+	static const char *env = std::getenv("YZ_COARSE_CYCLE");
+	static const bool off = env && env[0] == '0';
+	return !off && _coarseOn && _nlev - 1 <= (size_t)kMaxCoarse;
+}
+
+void Solver::LaunchCoarseCycle()
+{
+	CoarsePlan P;
+	const Level &F = *_levels[0];
+	P.count = (int)_nlev - 1;
+	P.n0 = F.n;
+	P.p0Lanes = 1;
+	P.t0 = F.t32.get(); P.x0 = F.x32.get(); P.xt0 = F.xt32.get();
+	P.r0ptr = F.rptr.get(); P.r0col = F.rcol.get(); P.r0val = F.rval32.get();
+	P.p0ptr = F.pptr.get(); P.p0col = F.pcol.get(); P.p0val = F.pval32.get();
+	for(size_t l = 1; l < _nlev; ++l)
+	{
+		const Level &L = *_levels[l];
+		CoarseLevel &c = P.lv[l - 1];
+		c.n = L.n;
+		c.direct = L.direct ? 1 : 0;
+		c.last = (!L.direct && l + 1 == _nlev) ? 1 : 0;
+		c.lanes = LanesFor(L.nnz, L.n);
+		c.plLanes = LanesFor(L.pnnz, L.n);
+		c.ptr = L.ptr.get(); c.col = L.col.get(); c.val = L.val32.get(); c.M = L.M32.get(); c.inv = L.inv32.get();
+		c.f = L.f32.get(); c.x = L.x32.get(); c.t = L.t32.get(); c.xt = L.xt32.get();
+		c.rptr = L.rptr.get(); c.rcol = L.rcol.get(); c.rval = L.rval32.get();
+		c.pptr = L.pptr.get(); c.pcol = L.pcol.get(); c.pval = L.pval32.get();
+	}
+	if(_coarseBlocks == 0)
+	{
+		int occ = 0, sms = 0;
+		YZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, KCoarseCycle, 256, 0));
+		YZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, _device));
+		_coarseBlocks = std::max(1, std::min(occ, 2)) * sms;
+	}
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3(_coarseBlocks);
+	cfg.blockDim = dim3(256);
+	cfg.dynamicSmemBytes = 0;
+	cfg.stream = _st;
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeCooperative;
+	attr[0].val.cooperative = 1;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	const bool timed = TimedKernel("KCoarseCycle");
+	if(timed) TimeBegin(_st);
+	YZ_CUDA(cudaLaunchKernelEx(&cfg, KCoarseCycle, Halt(), P, _coarseBar.get(), _coarseErr.get()));
+	if(timed) TimeEnd(_st);
+	CountLaunches(1);
 }
 
 //  lanes a row for a coarse level of the FP32 cycle, by its mean row length
@@ -1244,6 +1318,12 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 	_tailDst = nullptr;
 	if(!_tailDone) YZ_CUDA(cudaEventRecord(_ev2, _st));	// else recorded behind the loop
 	YZ_CUDA(cudaEventSynchronize(_ev2));
+	if(fp32 && CoarseCycleOn())
+	{
+		int e = 0;
+		YZ_CUDA(cudaMemcpy(&e, _coarseErr.get(), sizeof(int), cudaMemcpyDeviceToHost));
+		if(e) throw CudaError("solve: a grid barrier of the coarse V-cycle timed out");
+	}
 	float ms = 0;
 	if(timedSetup)
 	{

@@ -101,6 +101,8 @@ private:
 	void RoundCycle();
 	template<class TF, class TX> void Cycle32(size_t l, const TF *f, TX *x);
 	static int LanesFor(long long nnz, int n);
+	bool CoarseCycleOn() const;
+	void LaunchCoarseCycle();
 	void CoarsePreSmooth(int lanes, int n, const int *ptr, const int *col, const float *val, const float *M,
 	                     const float *f, float *x, float *t);
 	void CoarsePostSmooth(int lanes, int n, const int *ptr, const int *col, const float *val, const float *M,
@@ -196,6 +198,11 @@ private:
 	TryBackoff _offLearned;
 	LearnedStats _lstats;
 	DBuf<double> _zs;               // a collected pair's V-cycle output
+	//  the persistent coarse cycle: its grid, barrier words and error word
+	bool _coarseOn = true;
+	int _coarseBlocks = 0;
+	DBuf<unsigned> _coarseBar;
+	DBuf<int> _coarseErr;
 	double _setupMs = 0, _iterMs = 0;
 	long long _launches = 0;
 };
