@@ -69,7 +69,6 @@ __device__ __forceinline__ void CoarseBarrier(unsigned *count, volatile unsigned
 			while(*gen == g)
 			{
 				if(clock64() - t0 > 2000000000LL) { atomicExch(err, 1); break; }
-				__nanosleep(64);
 			}
 		}
 		__threadfence();

@@ -762,14 +762,24 @@ void Solver::Cycle32(size_t l, const TF *f, TX *x)
 	}
 }
 
-//  The persistent coarse cycle: on while the hierarchy has no more levels than
-//  the launch's plan holds; YZ_COARSE_CYCLE=0 switches it off (the levels
-//  then run as separate kernels)
+//  The persistent coarse cycle, switched on by YZ_COARSE_CYCLE=1 (while the
+//  hierarchy has no more levels than the launch's plan holds).  Off by
+//  default: on the 512^2 film its grid barriers cost more than the separate
+//  launches they replace inside the loop's CUDA graph (65-69 against 80
+//  steps/s with the FP32 V-cycle and reuse)
 bool Solver::CoarseCycleOn() const
 {
 	static const char *env = std::getenv("YZ_COARSE_CYCLE");
-	static const bool off = env && env[0] == '0';
-	return !off && _coarseOn && _nlev - 1 <= (size_t)kMaxCoarse;
+	static const bool on = env && env[0] != '0';
+	return on && _coarseOn && _nlev - 1 <= (size_t)kMaxCoarse;
+}
+
+//  blocks a multiprocessor of the persistent coarse cycle (YZ_COARSE_BLOCKS, default 1)
+int Solver::CoarseBlocksPerSm()
+{
+	static const char *env = std::getenv("YZ_COARSE_BLOCKS");
+	static const int k = env ? std::max(1, std::atoi(env)) : 1;
+	return k;
 }
 
 void Solver::LaunchCoarseCycle()
@@ -801,7 +811,7 @@ void Solver::LaunchCoarseCycle()
 		int occ = 0, sms = 0;
 		YZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, KCoarseCycle, 256, 0));
 		YZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, _device));
-		_coarseBlocks = std::max(1, std::min(occ, 2)) * sms;
+		_coarseBlocks = std::max(1, std::min(occ, CoarseBlocksPerSm())) * sms;
 	}
 	cudaLaunchConfig_t cfg = {};
 	cfg.gridDim = dim3(_coarseBlocks);

@@ -102,6 +102,7 @@ private:
 	template<class TF, class TX> void Cycle32(size_t l, const TF *f, TX *x);
 	static int LanesFor(long long nnz, int n);
 	bool CoarseCycleOn() const;
+	static int CoarseBlocksPerSm();
 	void LaunchCoarseCycle();
 	void CoarsePreSmooth(int lanes, int n, const int *ptr, const int *col, const float *val, const float *M,
 	                     const float *f, float *x, float *t);
