@@ -168,3 +168,26 @@ def conv3x3(x, w, bias, real_w: int, real_h: int, relu: bool) -> np.ndarray:
     _check(L.yz_conv3x3(H, W, cin, n, real_w, real_h, int(bool(relu)), x.ctypes.data_as(_f32p), w.ctypes.data_as(_f32p),
                         b.ctypes.data_as(_f32p) if b is not None else None, y.ctypes.data_as(_f32p)), "yz_conv3x3")
     return y
+
+
+def _main() -> None:
+    """python -m yuzen_b200.learned NX: the network on an NX x NX grid with
+    random inputs -- two forward passes and two loss-and-gradient passes (the
+    launch sequence of one application and of one training sample) -- and
+    their host-clock times."""
+    import sys
+    import time
+    n = int(sys.argv[1]) if len(sys.argv) > 1 else 516
+    net = UNet(n, n, capacity=4, seed=1)
+    rng = np.random.default_rng(0)
+    f = rng.standard_normal((3, n * n)).astype(np.float32)
+    t = rng.standard_normal(n * n).astype(np.float32)
+    for name, fn in (("forward", lambda: net.forward(f)), ("loss and gradient", lambda: net.loss_grad(f, t))):
+        for k in range(2):
+            t0 = time.perf_counter()
+            fn()
+            print(f"{name} {k}: {1e3 * (time.perf_counter() - t0):.2f} ms (host clock, copies included)")
+
+
+if __name__ == "__main__":
+    _main()
