@@ -148,6 +148,21 @@ int yz_kernel_time(double* total_ms, long long* launches);
  * fails with -3).  at = 0 switches it off; the call restarts the count. */
 int yz_fault_inject(long long at, long long count);
 
+/* The reference's profile table (util/Profile.h: YUZEN_PROF scopes, switched
+ * on by the environment variable YUZEN_PROFILE, totals to standard error at
+ * exit as "[profile] name calls seconds").  The device path keeps the names
+ * (step, h.assemble, h.couple, h.linsolve, h.after, c.linsolve, lin.prepare,
+ * lin.precond, lin.iterate, lin.fallback.conc, lin.learned), the switch and
+ * the exit lines; a scope's seconds are the device time of the work it
+ * queued on its stream (CUDA events), and every scope is an NVTX range of
+ * its name whether the switch is on or not.  yz_profile_entry gives the
+ * index-th name's totals so far (returns 1 past the last name, 0 otherwise;
+ * the name stays valid until the next call); yz_profile_reset zeroes them;
+ * yz_profile_enabled is 1 with the switch on. */
+int yz_profile_enabled(void);
+int yz_profile_entry(int index, const char** name, long long* calls, double* seconds);
+int yz_profile_reset(void);
+
 /* Building blocks exposed for the parity tests: the deterministic dot
  * product every reduction of the solve uses, and CRS_Matrix::MatVec
  * (CRS_Matrix.cpp:307-329), on host arrays through the device. */

@@ -45,7 +45,7 @@ EXPORTED_SYMBOLS = (
     "yz_unet_forward", "yz_unet_loss_grad", "yz_unet_add_sample", "yz_unet_samples", "yz_unet_train",
     "yz_unet_apply", "yz_solver_set_learned", "yz_solver_set_aux", "yz_solver_learned_stats",
     "yz_step_set_learned", "yz_conv3x3", "yz_fault_inject", "yz_step_state_size", "yz_step_get_state",
-    "yz_step_set_state",
+    "yz_step_set_state", "yz_profile_enabled", "yz_profile_entry", "yz_profile_reset",
 )
 
 #: the preconditioner's arithmetic (YZ_PREC_* of include/yuzen_b200.h)
@@ -375,3 +375,27 @@ def fault_inject(at: int, count: int = 1) -> None:
     L = lib()
     L.yz_fault_inject.argtypes = [ctypes.c_longlong, ctypes.c_longlong]
     _check(L.yz_fault_inject(at, count), "yz_fault_inject")
+
+
+def profile_table() -> dict:
+    """The profile table (yz_profile_entry): {name: (calls, device seconds)}
+    of every scope run so far; empty unless YUZEN_PROFILE was set when the
+    process first opened one."""
+    L = lib()
+    L.yz_profile_entry.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_longlong),
+                                   ctypes.POINTER(ctypes.c_double)]
+    out = {}
+    i = 0
+    while True:
+        name, calls, sec = ctypes.c_char_p(), ctypes.c_longlong(), ctypes.c_double()
+        r = L.yz_profile_entry(i, ctypes.byref(name), ctypes.byref(calls), ctypes.byref(sec))
+        _check(r, "yz_profile_entry")
+        if r == 1:
+            return out
+        out[name.value.decode()] = (calls.value, sec.value)
+        i += 1
+
+
+def profile_reset() -> None:
+    """Zero the profile table's totals (yz_profile_reset)."""
+    _check(lib().yz_profile_reset(), "yz_profile_reset")

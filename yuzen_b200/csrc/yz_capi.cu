@@ -2,6 +2,7 @@
 // Every call catches what the C++ side throws and turns it into a status.
 #include "yz_solver_impl.h"
 #include "yz_step_impl.h"
+#include "yz_prof.h"
 
 #include <cstring>
 
@@ -523,6 +524,21 @@ int yz_fault_inject(long long at, long long count)
 	return Guard([&] {
 		if(at < 0 || count < 0) throw yz::UsageError("yz_fault_inject: at and count must be >= 0");
 		yz::FaultInject((long)at, (long)count);
+		return 0;
+	});
+}
+
+int yz_profile_enabled(void) { return yz::prof::Enabled() ? 1 : 0; }
+
+int yz_profile_entry(int index, const char **name, long long *calls, double *seconds)
+{
+	return Guard([&] { return yz::prof::Entry(index, name, calls, seconds) ? 0 : 1; });
+}
+
+int yz_profile_reset(void)
+{
+	return Guard([&] {
+		yz::prof::Reset();
 		return 0;
 	});
 }

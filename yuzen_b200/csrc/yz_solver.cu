@@ -11,6 +11,7 @@
 #include "yz_coarse.cuh"
 #include "yz_learned.h"
 #include "yz_solver_impl.h"
+#include "yz_prof.h"
 
 #include <map>
 #include <mutex>
@@ -1195,11 +1196,14 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 		_sellVal32.reserve(_sellSize);
 		if(_sellVal32.get() != was) ++_epoch;
 	}
-	YZ_LAUNCH(KScaleGather, g, kB, 0, _st, n, L0.ptr.get(), _ssrc.get(), dValues, dRhs, set.scaling ? 1 : 0,
-	          L0.val.get(), _b.get(), _sellOff.get(), _sellVal.get(), fp32 ? _sellVal32.get() : nullptr);
-	(void)nnz;
-	YZ_CUDA(cudaMemcpyAsync(_x.get(), dX, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
-	YZ_CUDA(cudaMemcpyAsync(_x0.get(), dX, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+	{
+		YZ_PROF("lin.prepare", _st);
+		YZ_LAUNCH(KScaleGather, g, kB, 0, _st, n, L0.ptr.get(), _ssrc.get(), dValues, dRhs, set.scaling ? 1 : 0,
+		          L0.val.get(), _b.get(), _sellOff.get(), _sellVal.get(), fp32 ? _sellVal32.get() : nullptr);
+		(void)nnz;
+		YZ_CUDA(cudaMemcpyAsync(_x.get(), dX, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+		YZ_CUDA(cudaMemcpyAsync(_x0.get(), dX, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+	}
 	YZ_CUDA(cudaEventRecord(_ev0, _st));
 	//  a run in graph form copies its answer to dX behind the loop (the
 	//  last run's copy is the one that stays)
@@ -1213,6 +1217,7 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 
 	if(set.conc && set.precondition == 2 && _offSpai.Try())
 	{
+		YZ_PROF("lin.fallback.conc", _st);
 		YZ_LAUNCH(KSpai0, g, kB, 0, _st, n, L0.ptr.get(), L0.col.get(), L0.val.get(), _m.get());
 		if(!BiCGStab(kPrecDiag, tryIter, set.epsilon, it, err)) err = 1e300;
 		if(err <= set.epsilon) { done = true; _offSpai.Converged(); }
@@ -1236,6 +1241,7 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 	{
 		if(_offLearned.Try())
 		{
+			YZ_PROF("lin.learned", _st);
 			_learned->SetAux(dValues, L0.ptr.get(), _aux, _st);
 			//  the plain path's count: the last SA-AMG solve's, else the cap
 			const double plain = _amgIters > 0 ? (double)_amgIters : (double)set.max_iteration;
@@ -1266,8 +1272,12 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 	{
 		if(set.precondition == 0 || set.precondition == 1)
 		{
-			YZ_LAUNCH(KDiag, g, kB, 0, _st, n, L0.ptr.get(), L0.col.get(), L0.val.get(), _dia.get());
-			YZ_LAUNCH(KDampedJacobi, g, kB, 0, _st, n, _dia.get(), _m.get());
+			{
+				YZ_PROF("lin.precond", _st);
+				YZ_LAUNCH(KDiag, g, kB, 0, _st, n, L0.ptr.get(), L0.col.get(), L0.val.get(), _dia.get());
+				YZ_LAUNCH(KDampedJacobi, g, kB, 0, _st, n, _dia.get(), _m.get());
+			}
+			YZ_PROF("lin.iterate", _st);
 			broke = !BiCGStab(kPrecDiag, set.max_iteration, set.epsilon, it, err);
 		}
 		else
@@ -1283,32 +1293,38 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 				//  copies (one set up, or rounded, in a float precision)
 				const bool reuse = _amgReuse > 0 && _haveH && !_stale && _sinceBuild < _amgReuse &&
 				                   (!fp32 || _hPrec != YZ_PREC_FP64);
-				if(reuse)
 				{
-					Level &F = *_levels[0];
-					if(!F.direct)
+					YZ_PROF("lin.precond", _st);
+					if(reuse)
 					{
-						YZ_LAUNCH(KSpai0, g, kB, 0, _st, n, F.ptr.get(), F.col.get(), F.val.get(), F.M.get());
-						if(fp32)
+						Level &F = *_levels[0];
+						if(!F.direct)
 						{
-							RoundList one;
-							one.count = 1; one.src[0] = F.M.get(); one.dst[0] = F.M32.get(); one.n[0] = n;
-							YZ_LAUNCH(KRoundToFloat, GridFor(n, kB), kB, 0, _st, one);
+							YZ_LAUNCH(KSpai0, g, kB, 0, _st, n, F.ptr.get(), F.col.get(), F.val.get(), F.M.get());
+							if(fp32)
+							{
+								RoundList one;
+								one.count = 1; one.src[0] = F.M.get(); one.dst[0] = F.M32.get(); one.n[0] = n;
+								YZ_LAUNCH(KRoundToFloat, GridFor(n, kB), kB, 0, _st, one);
+							}
 						}
+						++_sinceBuild;
 					}
-					++_sinceBuild;
-				}
-				else
-				{
-					BuildHierarchy(n > 3000 ? 500 : 3000);
-					if(fp32) RoundCycle();
-					_hPrec = _precision;
-					_sinceBuild = 0;
-					_stale = false;
+					else
+					{
+						BuildHierarchy(n > 3000 ? 500 : 3000);
+						if(fp32) RoundCycle();
+						_hPrec = _precision;
+						_sinceBuild = 0;
+						_stale = false;
+					}
 				}
 				YZ_CUDA(cudaEventRecord(_ev1, _st));
 				timedSetup = true;
-				broke = !BiCGStab(kPrecAmg, set.max_iteration, set.epsilon, it, err);
+				{
+					YZ_PROF("lin.iterate", _st);
+					broke = !BiCGStab(kPrecAmg, set.max_iteration, set.epsilon, it, err);
+				}
 				if(!broke && !set.conc && err <= set.epsilon) _amgIters = it;
 				if(!reuse) { _freshIters = it; break; }
 				if(broke || !(err <= set.epsilon))

@@ -7,6 +7,7 @@
 #include "yz_upwind.cuh"
 #include "yz_conc.cuh"
 #include "yz_step_impl.h"
+#include "yz_prof.h"
 
 #include <algorithm>
 #include <chrono>
@@ -907,6 +908,8 @@ void Step::FaceProps(const double *H, const double *C, bool J)
 
 void Step::Assemble(int mode, const double *hField, const double *cField, double dt)
 {
+	//  one fused pass: the reference's h.assemble, h.jacobian and h.rhs
+	YZ_PROF("h.assemble", _st);
 	FaceProps(hField, cField, mode == 1);
 	UpBuf up;
 	up.base = nullptr; up.stride = _n;
@@ -983,7 +986,11 @@ bool Step::NKLoop(int &iter, double &resid, yz_step_stats &stats)
 		//  concentration, its solve at this film first (a failed one fails
 		//  the pass and with it the attempt).  Solve(): assembly at the film
 		//  and the working field's c.
-		if(_conc && !ConcPass(dt, stats)) { done = false; break; }
+		if(_conc)
+		{
+			YZ_PROF("h.couple", _st);
+			if(!ConcPass(dt, stats)) { done = false; break; }
+		}
 		ZeroMax(kSlotRhs);
 		YZ_CUDA(cudaEventRecord(_e0, _st));
 		Assemble(1, _guess.get(), _cw.get(), dt);
@@ -1021,7 +1028,11 @@ bool Step::NKLoop(int &iter, double &resid, yz_step_stats &stats)
 			if(!_learned->Trained() && _solver->CollectLeft() == 0) TrainLearned(stats);
 		}
 		const int r0 = _solver->Rebuilds();
-		const int ch = _solver->Solve(ls, _ia.get(), _rhs.get(), _delta.get(), it, res);
+		int ch;
+		{
+			YZ_PROF("h.linsolve", _st);
+			ch = _solver->Solve(ls, _ia.get(), _rhs.get(), _delta.get(), it, res);
+		}
 		double su = 0, sit = 0; _solver->Timing(&su, &sit);
 		stats.setup_ms += su; stats.solve_ms += sit;
 		stats.amg_setups += _solver->Rebuilds() - r0;
@@ -1121,6 +1132,7 @@ void Step::Advance(int nsteps, yz_step_stats &stats)
 	YZ_CUDA(cudaEventRecord(_eA, _st));
 	for(int step = 0; step < nsteps; ++step)
 	{
+		YZ_PROF("step", _st);
 		YZ_CUDA(cudaMemcpyAsync(_hOld2.get(), _hOld.get(), bytes, cudaMemcpyDeviceToDevice, _st));
 		YZ_CUDA(cudaMemcpyAsync(_hOld.get(), _hNew.get(), bytes, cudaMemcpyDeviceToDevice, _st));
 		bool timeStepDone = false;
@@ -1195,7 +1207,11 @@ void Step::Advance(int nsteps, yz_step_stats &stats)
 		YZ_CUDA(cudaMemcpyAsync(_hNew.get(), _guess.get(), bytes, cudaMemcpyDeviceToDevice, _st));
 		//  AfterNKLoop: with the concentration, the step of h c completed
 		//  (ConcCommit); the field takes the film
-		if(_conc) ConcCommit(_dt, stats);
+		if(_conc)
+		{
+			YZ_PROF("h.after", _st);
+			ConcCommit(_dt, stats);
+		}
 		YZ_CUDA(cudaMemcpyAsync(_h.get(), _guess.get(), bytes, cudaMemcpyDeviceToDevice, _st));
 		//  the energy budget of the film the step reached, the energy
 		//  dissipated over the step at its Crank-Nicolson weighting, and
@@ -1505,7 +1521,11 @@ int Step::ConcSolve(yz_step_stats &stats)
 {
 	int it = 0; double res = 0;
 	const int r0 = _solverC->Rebuilds();
-	const int ch = _solverC->Solve(_p.lin_conc, _iaC.get(), _rhsC.get(), _dC.get(), it, res);
+	int ch;
+	{
+		YZ_PROF("c.linsolve", _st);
+		ch = _solverC->Solve(_p.lin_conc, _iaC.get(), _rhsC.get(), _dC.get(), it, res);
+	}
 	double su = 0, sit = 0; _solverC->Timing(&su, &sit);
 	stats.setup_ms += su; stats.solve_ms += sit;
 	stats.amg_setups += _solverC->Rebuilds() - r0;
