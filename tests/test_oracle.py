@@ -150,3 +150,32 @@ def test_oracle_fault_switch():
         assert _oracle.OracleSolver().solve(d, x0=x0)[0] == 0
     finally:
         _oracle.fault_inject(0, 0)
+
+
+_THREADS_CHILD = r"""
+import sys
+sys.path[:0] = [sys.argv[1] + "/tests", sys.argv[1] + "/tests/golden"]
+import hashlib
+import numpy as np
+import _oracle, _systems
+p = _systems.film_system(120, seed=5)
+r = _oracle.OracleSolver().solve(p)
+print(r[0], r[1], repr(r[2]), hashlib.sha256(np.ascontiguousarray(r[3]).tobytes()).hexdigest())
+"""
+
+
+def test_oracle_thread_count_invariant():
+    """The oracle's vector loops run on OpenMP threads over the fixed
+    reduction tree, so one thread and eight give the same return code,
+    iteration count, residual and x to the bit (the reference's
+    test_linear_solver.cpp asks a backend for the same)."""
+    import os
+    import sys
+    root = Path(__file__).resolve().parents[1]
+    outs = []
+    for t in ("1", "8"):
+        r = subprocess.run([sys.executable, "-c", _THREADS_CHILD, str(root)], capture_output=True, text=True,
+                           env=dict(os.environ, OMP_NUM_THREADS=t), timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+        outs.append(r.stdout.strip().splitlines()[-1])
+    assert outs[0] == outs[1], outs

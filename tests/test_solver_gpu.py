@@ -351,3 +351,52 @@ def test_fp32_matrix_solves_the_rounded_system(d):
     tg, to = _true_residual(d, g[3]), _true_residual(d, r[3])
     rounding = 4.0 * 2.0 ** -24 * _abs_product(d, g[3])
     assert tg <= max(2.0 * float(d["epsilon"]), 4.0 * to) + rounding, (tg, to, rounding)
+
+
+_FUSE_CHILD = r"""
+import json, sys
+sys.path[:0] = [sys.argv[1], sys.argv[1] + "/tests", sys.argv[1] + "/tests/golden"]
+import numpy as np
+import _systems
+import yuzen_b200 as yz
+import test_solver_gpu as t
+d = _systems.film_system(384, seed=11)
+be = yz.B200Backend()
+be.SetPrecision(int(sys.argv[2]))
+g = t.gpu_solve(d, backend=be)
+print(json.dumps({"ret": g[0], "it": g[1], "res": g[2], "true": t._true_residual(d, g[3]), "levels": len(be.levels()),
+                  "x": float(np.linalg.norm(g[3]))}))
+"""
+
+
+@pytest.mark.parametrize("precision", [yz.PREC_FP32_CYCLE, yz.PREC_FP32_MATRIX])
+def test_fused_coarse_levels_match_the_separate_kernels(precision):
+    """The FP32 cycle's coarse levels with their way down (pre-smoothing,
+    residual, restriction) and way up (prolongation, post-smoothing) each in
+    one launch (YZ_FUSE_FROM=1: every level below the finest; the default
+    fuses from level 2), against the same cycle with every phase a kernel of
+    its own (YZ_FUSE_FROM=0): the same preconditioner up to float
+    rounding, so both solves of a 384^2 film (a hierarchy of several levels)
+    meet the tolerance with true residuals alike and iteration counts within
+    a tenth (float rounding alone moves a count by a few)."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = Path(__file__).resolve().parents[1]
+    out = {}
+    for key, val in (("fused", "1"), ("separate", "0")):
+        env = dict(os.environ)
+        env.pop("YZ_FUSE_FROM", None)
+        if val is not None:
+            env["YZ_FUSE_FROM"] = val
+        r = subprocess.run([sys.executable, "-c", _FUSE_CHILD, str(root), str(precision)], capture_output=True,
+                           text=True, env=env, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[key] = json.loads(r.stdout.strip().splitlines()[-1])
+    a, b = out["fused"], out["separate"]
+    assert a["levels"] == b["levels"] >= 3, (a, b)
+    assert a["ret"] == b["ret"] == 0, (a, b)
+    assert abs(a["it"] - b["it"]) <= max(3, b["it"] // 10), (a, b)
+    assert a["true"] <= 4.0 * max(b["true"], 1e-300) + 1e-14, (a, b)
+    assert abs(a["x"] - b["x"]) <= 1e-6 * b["x"], (a, b)

@@ -997,6 +997,70 @@ __global__ void KProlongL(const int *__restrict__ halt, int n, const int *__rest
 		if(active && q == 0) xout[row] = x[row] + s;
 	}
 }
+
+//--------------------------------------------------------------------------
+//  A coarse level's way down and way up, each in one launch.  Below the
+//  finest level the V-cycle's phases are short (a few thousand rows) and
+//  each costs a kernel boundary more than its work; two of the four per
+//  level go by recomputing what the separate kernels passed through memory:
+//
+//    down:  fc = R (f - A (m .* f))              (pre-smoothing from zero,
+//           the residual and the restriction; t_j recomputed by every R row
+//           that holds j)
+//    up:    x = xt + m .* (f - A xt),  xt = m .* f + P xc
+//           (prolongation and post-smoothing; xt_k recomputed by every row
+//           whose A row holds k)
+//
+//  The same arithmetic as the separate kernels in another order: the FP32
+//  cycle's sums are not the oracle's.  L lanes a row (the down kernel's rows
+//  are the next level's), each lane a fixed share of the row's entries, the
+//  partials folded by shuffles: deterministic.
+//--------------------------------------------------------------------------
+template<int L, class T>
+__global__ void KDownFused(const int *__restrict__ halt, int n, const int *__restrict__ rptr,
+                           const int *__restrict__ rcol, const T *__restrict__ rval, const int *__restrict__ ptr,
+                           const int *__restrict__ col, const T *__restrict__ val, const T *__restrict__ M,
+                           const T *__restrict__ f, T *__restrict__ fc)
+{
+	if(halt && *halt) return;
+	YZ_LANE_LOOP(L)
+	{
+		const long long row = base_ + lane_ / L;
+		const bool active = row < n;
+		const T s = RowSumLanes<L>(rptr, rcol, rval, row, active, q, [&](int j) {
+			T a = T(0);
+			const int st = ptr[j], en = ptr[j + 1];
+			for(int e = st; e < en; ++e)
+			{
+				const int c = col[e];
+				a = a + val[e] * (M[c] * f[c]);
+			}
+			return f[j] - a;
+		});
+		if(active && q == 0) fc[row] = s;
+	}
+}
+
+template<int L, class T>
+__global__ void KUpFused(const int *__restrict__ halt, int n, const int *__restrict__ ptr, const int *__restrict__ col,
+                         const T *__restrict__ val, const T *__restrict__ M, const int *__restrict__ pptr,
+                         const int *__restrict__ pcol, const T *__restrict__ pval, const T *__restrict__ f,
+                         const T *__restrict__ xc, T *__restrict__ x)
+{
+	if(halt && *halt) return;
+	auto xt = [&](int k) {
+		T s = T(0);
+		for(int e = pptr[k], en = pptr[k + 1]; e < en; ++e) s = s + pval[e] * xc[pcol[e]];
+		return M[k] * f[k] + s;
+	};
+	YZ_LANE_LOOP(L)
+	{
+		const long long row = base_ + lane_ / L;
+		const bool active = row < n;
+		const T s = RowSumLanes<L>(ptr, col, val, row, active, q, xt);
+		if(active && q == 0) x[row] = xt((int)row) + M[row] * (f[row] - s);
+	}
+}
 #undef YZ_LANE_LOOP
 
 //  the FP32 copies of the V-cycle's matrices: dst_k[i] = (float)src_k[i] over

@@ -110,6 +110,11 @@ private:
 	                      const float *f, const float *x, float *xout);
 	void CoarseProlong(int lanes, int n, const int *pptr, const int *pcol, const float *pval, const float *xc,
 	                   const float *x, float *xout);
+	//  the first level whose way down and way up run fused (KDownFused,
+	//  KUpFused); past the deepest level: none
+	static int FusedFrom();
+	void CoarseDown(int lanes, int nc, const Level &L, const float *f, float *fc);
+	void CoarseUp(int lanes, const Level &L, const float *f, const float *xc, float *x);
 	const int *Halt() const { return &_sc.get()->state; }
 	void ApplyPrec(int kind, const double *r, double *z);
 	void EnqueueIteration(int kind);
