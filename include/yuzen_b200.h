@@ -245,7 +245,7 @@ typedef struct yz_step_params
 	double t_start;
 	/* the upwinded terms (BodyForceKernel.h, ParallelGravityKernel.h,
 	 * CentrifugalKernel.h, SolutoCapillarityKernel.h) */
-	int    conv_height;           /* YZ_SCHEME_KOREN or YZ_SCHEME_VANLEER */
+	int    conv_height;           /* any YZ_SCHEME_* (Koren is the reference's default) */
 	double Pgx, Pgy;              /* in-plane gravity groups (coefficients Pg/3) */
 	double Sp, rot_x, rot_y;      /* rotation group and the axis (non-dimensional) */
 	double As, Ma;                /* Marangoni coefficient As*Ma/2 */

@@ -134,6 +134,23 @@ STEP_CASES = {
         "Physics.Evaporation.SpatialFunc": "negPow", "Physics.Evaporation.Coef": 1e-6,
         "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-2,
     }, 3, -1),
+    # every height term with the upwinded ones on each unlimited scheme of
+    # Numerics.Convection.Height (the fixed four-point face values,
+    # FiniteDifferences.cpp:22-76, 216-226), c carried unchanged, fixed dt
+    **{f"step_upwind_{s.lower()}_40": ("allphys_2d_reg.toml", {
+        "Physics.ConcField.Model": "None", "Grid.Nx": 40, "Grid.Ny": 36,
+        "Numerics.Convection.Height": s,
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-3,
+    }, 3, 3) for s in ("Upwind1", "Upwind2", "Central2", "UTOPIA", "QUICK", "KK", "Central4")},
+    # the well-mixed concentration solved with Navier slip and the
+    # Kawamura-Kuwahara height scheme (the face fluxes the concentration and
+    # the energy budget take on the unlimited path), QUICK for c
+    "step_wm_kk_slip_40": ("allphys_2d_reg.toml", {
+        "Grid.Nx": 40, "Grid.Ny": 40,
+        "Physics.Slip.Enable": True, "Physics.Slip.Length": 5e-7,
+        "Numerics.Convection.Height": "KK", "Numerics.Convection.Concentration": "QUICK",
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-2,
+    }, 3, -1),
     # capillary + disjoining with the time-step control on
     "step_adaptive_40": ("allphys_2d_reg.toml", {
         **_NO_UPWIND, "Grid.Nx": 40, "Grid.Ny": 40,

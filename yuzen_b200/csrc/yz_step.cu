@@ -783,10 +783,8 @@ void CheckParams(const yz_step_params &p)
 	if((p.bc[0] == YZ_BC_PERIODIC) != (p.bc[1] == YZ_BC_PERIODIC) || (p.bc[2] == YZ_BC_PERIODIC) != (p.bc[3] == YZ_BC_PERIODIC))
 		throw UsageError("step: a Periodic edge needs a Periodic opposite edge");
 	if(!p.on_laplace) throw UsageError("step: the capillary term (Physics.LaplacePressure) must be enabled");
-	if((p.on_pgrav || p.on_marangoni || p.on_centrifugal) && p.conv_height != YZ_SCHEME_KOREN &&
-	   p.conv_height != YZ_SCHEME_VANLEER)
-		throw UsageError("step: the upwinded terms are built on the limited path (Numerics.Convection.Height = "
-		                 "Koren or VanLeer)");
+	if(p.conv_height < YZ_SCHEME_UPWIND1 || p.conv_height > YZ_SCHEME_VANLEER)
+		throw UsageError("step: unknown Numerics.Convection.Height scheme");
 	if(p.conc_field != 0)
 	{
 		if(p.conv_conc < YZ_SCHEME_UPWIND1 || p.conv_conc > YZ_SCHEME_VANLEER)

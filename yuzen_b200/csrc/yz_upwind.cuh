@@ -1,5 +1,6 @@
-// yz_upwind.cuh -- the upwinded terms of the film-height equation on the
-// limited path, one interior row at a time: the in-plane gravity
+// yz_upwind.cuh -- the upwinded terms of the film-height equation, on the
+// limited path (Koren, VanLeer) and on the unlimited one (the fixed
+// four-point schemes, below), one interior row at a time: the in-plane gravity
 // (ParallelGravityKernel.h), the rotation (CentrifugalKernel.h) and the
 // Marangoni stress (SolutoCapillarityKernel.h).
 //
@@ -106,10 +107,81 @@ __device__ __forceinline__ void LimitedFace(const Coef &k, const double *h, doub
 	if(WallFace(k, d, ix, iy)) D = 0;
 }
 
+//--------------------------------------------------------------------------
+//  The unlimited height schemes (Upwind-1st, Central-2nd, Central-4th,
+//  Upwind-2nd, UTOPIA, QUICK, Kawamura-Kuwahara; FiniteDifferences.cpp:22-76):
+//  the face value is the fixed four-point combination with the upwind part
+//  c2 taken by the sign of the drive, and A, the Jacobian and the flux are
+//  BodyForceKernel.h:263-491 and SolutoCapillarityKernel.h:182-373.
+//--------------------------------------------------------------------------
+
+//  CellAvgCoord (GridTraits.h:488-497): the mean of the centres of the two
+//  cells on either side of face d of cell (ix, iy)
+__device__ __forceinline__ double CellAvgCoord(const Coef &k, int d, int ix, int iy)
+{
+	const double cx = k.xmin + ix * k.dx + k.dx2h, cy = k.ymin + iy * k.dy + k.dy2h;
+	switch(d)
+	{
+	case 0:  return 0.5 * ((k.xmin + (ix - 1) * k.dx + k.dx2h) + cx);
+	case 1:  return 0.5 * ((k.xmin + (ix + 1) * k.dx + k.dx2h) + cx);
+	case 2:  return 0.5 * ((k.ymin + (iy - 1) * k.dy + k.dy2h) + cy);
+	default: return 0.5 * ((k.ymin + (iy + 1) * k.dy + k.dy2h) + cy);
+	}
+}
+
+//  Drive: the direction the face value of the unlimited path is upwinded by
+//  (in-plane gravity: the sign of Pg; the rotation: the distance of the
+//  cells' mean centre from the axis, CentrifugalKernel.h:87-92).  A's and
+//  the Jacobian's coefficients take DriveFace's sign instead; the two agree
+//  but at a face on the axis.
+template<int T>
+__device__ __forceinline__ double DriveCells(const Coef &k, int d, int ix, int iy)
+{
+	if(T == kPG) return k.pgSign[d / 2];
+	return CellAvgCoord(k, d, ix, iy) - k.cnt[d / 2];
+}
+
+//  C(j) + Sign(dv) C2(j) of a body force, the coefficients divided by the
+//  mesh spacing one by one (UpwindKernelBase SetUpwindCoef(true))
+__device__ __forceinline__ void UnlimitedWeights(const Coef &k, double dv, double hs, double wt[4])
+{
+#pragma unroll
+	for(int q = 0; q < 4; ++q) wt[q] = k.hI.c1[q] / hs + MSign(dv) * (k.hI.c2[q] / hs);
+}
+
+//  NonlinearTerm's face value (BodyForceKernel.h:263-302): sum_q h_q (c1 + Sign(pp) c2)
+__device__ __forceinline__ double UnlimitedFaceValue(const Coef &k, const double f[4], double pp)
+{
+	double hh = 0;
+#pragma unroll
+	for(int q = 0; q < 4; ++q) hh += f[q] * (k.hI.c1[q] + MSign(pp) * k.hI.c2[q]);
+	return hh;
+}
+
+//  BodyForceKernel::FaceFlux, unlimited (BodyForceKernel.h:129-147)
+template<int T>
+__device__ __forceinline__ double BodyForceFluxU(const Coef &k, const double *h, double vis, int d, int ix, int iy)
+{
+	if(WallFace(k, d, ix, iy)) return 0.0;
+	const double w = Weight<T>(k, d, ix, iy);
+	const double hsp = (d < 2) ? k.dxx : k.dyy;
+	double f[4], wt[4];
+#pragma unroll
+	for(int q = 0; q < 4; ++q) f[q] = h[FS(d, q)];
+	const double hh = UnlimitedFaceValue(k, f, DriveCells<T>(k, d, ix, iy));
+	const double D = (k.slip ? MobDperH(k, hh) : hh * hh) / vis;
+	UnlimitedWeights(k, DriveFace<T>(k, d, ix, iy), hsp, wt);
+	double hs = 0;
+#pragma unroll
+	for(int q = 0; q < 4; ++q) hs += wt[q] * f[q];
+	return Mag<T>(k, d / 2) * (w * hs * D);
+}
+
 //  BodyForceKernel::FaceFlux, limited: Mag w (sum_q wt_q h_q) D through face d
 template<int T>
 __device__ __forceinline__ double BodyForceFlux(const Coef &k, const double *h, double vis, int d, int ix, int iy)
 {
+	if(!k.hI.limited) return BodyForceFluxU<T>(k, h, vis, d, ix, iy);
 	const double w = Weight<T>(k, d, ix, iy);
 	double hf, D, wt[4];
 	LimitedFace<T, false>(k, h, vis, d, ix, iy, hf, D, wt, nullptr);
@@ -189,6 +261,34 @@ __device__ __forceinline__ void BodyForceFace(const Coef &k, const double f[4], 
 	const double hs = (d < 2) ? k.dxx : k.dyy;
 	const double w = Weight<T>(k, d, ix, iy);
 	const int term = (T == kPG) ? 0 : 1;
+	if(!k.hI.limited)
+	{
+		//  SetMatrixA / SetJacobiMatrix (BodyForceKernel.h:343-491): A's
+		//  w (C + Sign(dv) C2)_q D; the Jacobian adds g_q acc, g_q = dD/dh_q
+		//  (NonlinearJacobi: 2 h_f c_q / mu, slip dUpwind(h_f) c_q / mu) and
+		//  acc = sum_s w (C + Sign(dv) C2)_s h_s the face's A applied to h
+		const double pp = DriveCells<T>(k, d, ix, iy);
+		const double hh = UnlimitedFaceValue(k, f, pp);
+		const double D = wall ? 0.0 : (k.slip ? MobDperH(k, hh) : hh * hh) / vis;
+		double wt[4];
+		UnlimitedWeights(k, dv, hs, wt);
+#pragma unroll
+		for(int q = 0; q < 4; ++q) up.at(0, a, term, q)[j] = w * wt[q] * D;
+		if(J)
+		{
+			double acc = 0;
+#pragma unroll
+			for(int q = 0; q < 4; ++q) acc += w * wt[q] * f[q];
+			const double dd = k.slip ? (hh < 0 ? -(2.0 * (-hh) + k.a3) : 2.0 * hh + k.a3) : 2.0 * hh;
+#pragma unroll
+			for(int q = 0; q < 4; ++q)
+			{
+				const double g = wall ? 0.0 : dd * (k.hI.c1[q] + MSign(pp) * k.hI.c2[q]) / vis;
+				up.at(1, a, term, q)[j] = g * acc;
+			}
+		}
+		return;
+	}
 	double hf, D, wt[4], g[4];
 	LimitedFaceF<false>(k, f, vis, dv, hs, wall, hf, D, wt, nullptr);
 #pragma unroll
@@ -224,7 +324,23 @@ __device__ __forceinline__ void MarangoniFace(const Coef &k, const double f[4], 
 #pragma unroll
 		for(int q = 0; q < 4; ++q) up.at(0, a, kUpSC, q)[j] = wt[q] * S / hsp;
 	}
-	if(J)
+	if(J && !k.hI.limited)
+	{
+		//  SetJacobiMatrix, unlimited (SolutoCapillarityKernel.h:322-373):
+		//  g_q a with g_q = dc / mu (C + Up C2)_q and a = sum_s (C + Up C2)_s h_s / h
+		double wt[4];
+		FaceWeights(k.hI, f, upw, -1, wt);
+		double av = 0;
+#pragma unroll
+		for(int q = 0; q < 4; ++q) av += wt[q] * f[q] / hsp;
+#pragma unroll
+		for(int q = 0; q < 4; ++q)
+		{
+			const double g = wall ? 0.0 : dc / vis * wt[q];
+			up.at(1, a, kUpSC, q)[j] = g * av;
+		}
+	}
+	else if(J)
 	{
 		double wt[4], gd[4];
 		const double hf = FaceDerivative(k.hI, f, upw, gd);
