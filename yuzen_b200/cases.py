@@ -31,7 +31,7 @@ GG = 9.80665
 PI = 4.0 * math.atan(1.0)   # Math::pi(), MyMath.h:110
 
 #  BoundaryCondition::tBoundaryCondition
-BC = {"Symmetry": 0, "Periodic": 1}
+BC = {"Symmetry": 0, "Periodic": 1, "Pinning": 2, "FreshInlet": 3, "Outlet": 4}
 #  C_Interpolation_base4::t_Scheme by its Numerics.Convection key (FiniteDifferences.cpp:216-226)
 SCHEMES = {"Upwind1": 0, "Upwind2": 1, "Central2": 2, "UTOPIA": 3, "QUICK": 4, "KK": 5, "Central4": 6,
            "Koren": 7, "VanLeer": 8}
