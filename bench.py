@@ -65,6 +65,10 @@ ROOFLINE_KERNEL = "KSpmvAlpha"
 #  capture reports null.
 NCU_TRAFFIC = {
     ("KSpmvAlpha", "allphys_512"): 33880064,
+    # a Newton pass's assembly: KAssemble (180,615,424 B) + KUpwindFaces
+    # (50,359,808 B); the pass's two smaller kernels (KFaceProps, KCellPi) were
+    # not captured
+    ("assembly", "allphys_512"): 180615424 + 50359808,
 }
 
 

@@ -203,14 +203,18 @@ long long yz_dot_noalloc_max(void);
  */
 typedef struct yz_step yz_step;
 
-/* BoundaryCondition::tBoundaryCondition (BoundaryCondition.h:56-63); the
- * step supports Symmetry and Periodic edges. */
-enum { YZ_BC_SYMMETRY = 0, YZ_BC_PERIODIC = 1 };
+/* BoundaryCondition::tBoundaryCondition (BoundaryCondition.h:56-63).  The
+ * film takes every kind (ghost rows as BoundaryCondition2D::Apply writes
+ * them, BoundaryCondition.cpp:104-187, 376-517; a Pinning corner next to a
+ * FreshInlet or an Outlet edge, and two Pinning edges meeting, are refused
+ * as the reference refuses or leaves them); the concentration equation
+ * (conc_field) takes Symmetry and Periodic edges. */
+enum { YZ_BC_SYMMETRY = 0, YZ_BC_PERIODIC = 1, YZ_BC_PINNING = 2, YZ_BC_FRESHINLET = 3, YZ_BC_OUTLET = 4 };
 
 /* C_Interpolation_base4::t_Scheme (FiniteDifferences.h:42-53), the face
- * interpolation of Numerics.Convection.Height / .Concentration.  The
- * upwinded height terms take the limited ones (Koren, the default, and
- * VanLeer); the concentration takes every scheme. */
+ * interpolation of Numerics.Convection.Height / .Concentration: the
+ * limited ones (Koren, the height's default, and VanLeer) and the fixed
+ * four-point ones, for both. */
 enum { YZ_SCHEME_UPWIND1 = 0, YZ_SCHEME_UPWIND2 = 1, YZ_SCHEME_CENTRAL2 = 2, YZ_SCHEME_UTOPIA = 3,
        YZ_SCHEME_QUICK = 4, YZ_SCHEME_KK = 5, YZ_SCHEME_CENTRAL4 = 6, YZ_SCHEME_KOREN = 7,
        YZ_SCHEME_VANLEER = 8 };

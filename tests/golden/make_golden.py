@@ -151,6 +151,49 @@ STEP_CASES = {
         "Numerics.Convection.Height": "KK", "Numerics.Convection.Concentration": "QUICK",
         "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-2,
     }, 3, -1),
+    # open edges (BoundaryCondition.cpp:104-187): an Outlet at Xmin, a
+    # FreshInlet at Xmax, mirror edges in y (their corners mirror in y), every
+    # height term, c carried unchanged, fixed dt
+    "step_outlet_inlet_40": ("allphys_2d_reg.toml", {
+        "Physics.ConcField.Model": "None", "Grid.Nx": 40, "Grid.Ny": 36,
+        "Boundary.XminBC.Type": "Outlet", "Boundary.XmaxBC.Type": "FreshInlet",
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-3,
+    }, 3, 3),
+    # open edges on all four sides: every corner stencil of the reference
+    # (Inlet-Outlet, Inlet-Inlet, Outlet-Outlet, Outlet-Inlet; :556-597)
+    "step_open_corners_40": ("allphys_2d_reg.toml", {
+        "Physics.ConcField.Model": "None", "Grid.Nx": 40, "Grid.Ny": 40,
+        "Boundary.XminBC.Type": "FreshInlet", "Boundary.XmaxBC.Type": "Outlet",
+        "Boundary.YminBC.Type": "Outlet", "Boundary.YmaxBC.Type": "FreshInlet",
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-3,
+    }, 3, 3),
+    # a Pinning edge at Xmin with the film shaped down to it (an EdgeBump,
+    # as the reference's property tests build one), mirror edges elsewhere,
+    # every height term, c carried unchanged
+    "step_pinning_40": ("allphys_2d_reg.toml", {
+        "Physics.ConcField.Model": "None", "Grid.Nx": 40, "Grid.Ny": 36,
+        "Boundary.XminBC.Type": "Pinning",
+        "Initial.SurfaceShape.PrecursorRatio": 0.02,
+        "Initial.SurfaceShape.EllipseBump.Height": 0.0,
+        "Initial.SurfaceShape.EdgeBump": {"Order": 1, "CreateType": "add", "Base": 0.5, "Height": 1.0,
+                                          "Location": "Xmin", "Alpha": 1.0, "InnerLength": 0.05e-3,
+                                          "OuterLength": 0.15e-3},
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-4,
+    }, 3, 3),
+    # a Pinning edge at Ymax with periodic x edges (the Pinning-Periodic
+    # corners), capillary + gravity + evaporation, adaptive dt
+    "step_pinning_periodic_40": ("allphys_2d_reg.toml", {
+        **_NO_UPWIND, "Grid.Nx": 40, "Grid.Ny": 40,
+        "Boundary.XminBC.Type": "Periodic", "Boundary.XmaxBC.Type": "Periodic",
+        "Boundary.YmaxBC.Type": "Pinning",
+        "Initial.SurfaceShape.PrecursorRatio": 0.02,
+        "Initial.SurfaceShape.EllipseBump.Height": 0.0,
+        "Initial.SurfaceShape.EdgeBump": {"Order": 1, "CreateType": "add", "Base": 0.5, "Height": 1.0,
+                                          "Location": "Ymax", "Alpha": 1.0, "InnerLength": 0.05e-3,
+                                          "OuterLength": 0.15e-3},
+        "Numerics.TimeStepControl.Enable": True, "Numerics.TimeStepControl.KeepSteps": 2,
+        "Numerics.TimeStepControl.ChangeFactor": 0.75, "Numerics.InitialDt": 1e-4,
+    }, 4, 3),
     # capillary + disjoining with the time-step control on
     "step_adaptive_40": ("allphys_2d_reg.toml", {
         **_NO_UPWIND, "Grid.Nx": 40, "Grid.Ny": 40,

@@ -10,7 +10,8 @@ import pytest
 import stateio
 from yuzen_b200 import step as ys
 
-STEPS = sorted(Path(__file__).parent.joinpath("golden").glob("step_*.npz"))
+GOLDEN = Path(__file__).parent.joinpath("golden")
+STEPS = sorted(GOLDEN.glob("step_*.npz"))
 
 
 @pytest.mark.parametrize("f", STEPS, ids=[f.stem for f in STEPS])
@@ -31,8 +32,25 @@ def test_params_from_state(f):
     assert p.lin.epsilon == d["lin_eps"]
 
 
-def test_unsupported_edges_are_refused():
-    d = stateio.load_npz(STEPS[0])
+@pytest.mark.parametrize("bc,why", [
+    ((2, 0, 4, 0), "Pinning next to an Outlet"),        # BC: Pinning-Outlet, not implemented in the reference
+    ((3, 0, 2, 0), "FreshInlet next to a Pinning"),     # BC: Inlet-Pinning
+    ((2, 0, 2, 0), "two Pinning edges meeting"),        # three corner rows left without a condition
+    ((7, 0, 0, 0), "an unknown kind"),
+])
+def test_refused_edges(bc, why):
+    d = stateio.load_npz(GOLDEN / "step_upwind_48.npz")
+    p = ys.params_from_state(d)
+    for e in range(4):
+        p.bc[e] = bc[e]
+    with pytest.raises(Exception):
+        ys.pattern_2d(p)
+
+
+def test_concentration_needs_closed_edges():
+    """The concentration equation is built for Symmetry and Periodic edges;
+    an open edge with conc_field on is refused."""
+    d = stateio.load_npz(GOLDEN / "step_wm_allphys_48.npz")
     p = ys.params_from_state(d)
     p.bc[0] = 4  # Outlet
     with pytest.raises(Exception):

@@ -92,6 +92,7 @@ struct Coef
 	//  SolutoCapillarityKernel.h:411-516)
 	int onPG, onSC, onCF;
 	int wall[4];                // IsWall of the Xmin, Xmax, Ymin, Ymax edges (Symmetry, Pinning)
+	int pinned[4];              // Pinning edges: no capillary flux through their wall face
 	Interp hI;                  // Numerics.Convection.Height (a limited scheme)
 	double pgMag[2], pgSign[2]; // Pg/3 per axis and Math::Sign(Pg)
 	double cfMag, cnt[2];       // Sp/3 and the rotation axis

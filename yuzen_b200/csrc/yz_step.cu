@@ -68,16 +68,19 @@ __global__ void KFaceProps(Coef k, const double *__restrict__ H, const double *_
 	{
 		int lo, hi;
 		FaceSet f;
+		bool pinned;
 		if(t < nxF)
 		{
 			const int ix = 1 + t % (nx - 3), iy = 2 + t / (nx - 3);
 			lo = iy * nx + ix; hi = lo + 1; f = fb.x;
+			pinned = (ix == 1 && k.pinned[0]) || (ix == nx - 3 && k.pinned[1]);
 		}
 		else
 		{
 			const int u = t - nxF;
 			const int ix = 2 + u % (nx - 4), iy = 1 + u / (nx - 4);
 			lo = iy * nx + ix; hi = lo + nx; f = fb.y;
+			pinned = (iy == 1 && k.pinned[2]) || (iy == ny - 3 && k.pinned[3]);
 		}
 		const double hl = H[lo], hh = H[hi];
 		const double cfc = 0.5 * (C[lo] + C[hi]);
@@ -85,7 +88,9 @@ __global__ void KFaceProps(Coef k, const double *__restrict__ H, const double *_
 		const double FM = Face(k, hl, hh);
 		const double val = k.slip ? FM : 2.0 * (hl * hl) * (hh * hh) / (hl + hh);
 		f.vis[lo] = vis; f.sig[lo] = sig; f.FM[lo] = FM;
-		f.DL[lo] = val * sig / vis;
+		//  LaplacePressure_WM2D::PinnedFace (LaplacePressure_2D.cpp:21-30): the
+		//  capillary term's mobility and its derivatives zero on a pinned face
+		f.DL[lo] = pinned ? 0.0 : val * sig / vis;
 		if(!J) continue;
 		const double dLH = (k.onV || k.onD || k.slip) ? Face_d1(k, hl, hh) : 0.0;
 		const double dHL = (k.onV || k.onD || k.slip) ? Face_d1(k, hh, hl) : 0.0;
@@ -97,8 +102,8 @@ __global__ void KFaceProps(Coef k, const double *__restrict__ H, const double *_
 			const double vLH = k.slip ? dLH : 2.0 * (hl * hh * hh) * (hl + hh + hh) / den;
 			const double den2 = (hh + hl) * (hh + hl);
 			const double vHL = k.slip ? dHL : 2.0 * (hh * hl * hl) * (hh + hl + hl) / den2;
-			f.gLH[lo] = vLH * sig / vis;
-			f.gHL[lo] = vHL * sig / vis;
+			f.gLH[lo] = pinned ? 0.0 : vLH * sig / vis;
+			f.gHL[lo] = pinned ? 0.0 : vHL * sig / vis;
 		}
 	}
 }
@@ -648,15 +653,58 @@ __global__ void KLte(int n, const double *__restrict__ hp, const double *__restr
 	WarpMaxAbs(out, m);
 }
 
-__global__ void KSetGhostRows(int nGhost, const int *__restrict__ ghost, const int *__restrict__ rowptr,
-                              double *__restrict__ ia, double *__restrict__ rhs)
+//  the Newton matrix's ghost rows and their right-hand side, once (yz_bc.h)
+__global__ void KSetGhostRows(int nVal, const int *__restrict__ pos, const double *__restrict__ val, int nGhost,
+                              const int *__restrict__ ghost, const double *__restrict__ grhs, double *__restrict__ ia,
+                              double *__restrict__ rhs)
 {
-	for(int g = blockIdx.x * blockDim.x + threadIdx.x; g < nGhost; g += gridDim.x * blockDim.x)
+	for(int t = blockIdx.x * blockDim.x + threadIdx.x; t < nVal; t += gridDim.x * blockDim.x) ia[pos[t]] = val[t];
+	for(int g = blockIdx.x * blockDim.x + threadIdx.x; g < nGhost; g += gridDim.x * blockDim.x) rhs[ghost[g]] = grhs[g];
+}
+
+//  CRS_Matrix::SatisfyBCRows (CRS_Matrix.cpp:198-302) on x with the plan of
+//  yz_bc.h, one thread a set of coupled ghost rows: each row's right-hand
+//  side less its other terms (in the plan's order), the elimination of the
+//  right-hand side with the plan's pivots and multipliers, and the back
+//  substitution on the eliminated matrix
+struct BcSets
+{
+	int n;
+	const int *m, *rowOff, *matOff, *row, *termOff, *termCol, *piv;
+	const double *rhs, *termVal, *fac, *U;
+};
+
+__global__ void KSatisfyBC(BcSets S, double *__restrict__ x)
+{
+	for(int c = blockIdx.x * blockDim.x + threadIdx.x; c < S.n; c += gridDim.x * blockDim.x)
 	{
-		const int i = ghost[g];
-		ia[rowptr[i]] = 1.0;
-		ia[rowptr[i] + 1] = -1.0;
-		rhs[i] = 0.0;
+		const int m = S.m[c];
+		if(m <= 0 || m > kMaxBcSet) continue;
+		const int r0 = S.rowOff[c], m0 = S.matOff[c];
+		double b[kMaxBcSet];
+		for(int p = 0; p < m; ++p)
+		{
+			double s = 0;
+			for(int t = S.termOff[r0 + p]; t < S.termOff[r0 + p + 1]; ++t) s += S.termVal[t] * x[S.termCol[t]];
+			b[p] = S.rhs[r0 + p] - s;
+		}
+		for(int col = 0; col < m; ++col)
+		{
+			const int pv = S.piv[r0 + col];
+			if(pv != col) { const double t = b[pv]; b[pv] = b[col]; b[col] = t; }
+			for(int p = col + 1; p < m; ++p)
+			{
+				const double f = S.fac[m0 + p * m + col];
+				if(f == 0.0) continue;
+				b[p] -= f * b[col];
+			}
+		}
+		for(int p = m - 1; p >= 0; --p)
+		{
+			double s = b[p];
+			for(int q = p + 1; q < m; ++q) s -= S.U[m0 + p * m + q] * x[S.row[r0 + q]];
+			x[S.row[r0 + p]] = s / S.U[m0 + p * m + p];
+		}
 	}
 }
 
@@ -719,8 +767,8 @@ Step::Step(int device, const yz_step_params &p, const double *h, const double *c
 		for(int q = 0; q < 19; ++q) *slots[q] = m + (size_t)q * n;
 	}
 	_dt = p.dt; _dtOld = p.dt; _time = p.t_start;
-	YZ_LAUNCH(KSetGhostRows, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
-	          _dRowptr.get(), _ia.get(), _rhs.get());
+	YZ_LAUNCH(KSetGhostRows, GridFor((long long)_nBcVal, 256), 256, 0, _st, _nBcVal, _dBcPos.get(),
+	          _dBcVal.get(), (int)_ghost.size(), _dGhost.get(), _dBcRhs.get(), _ia.get(), _rhs.get());
 	_cw.reserve(n);
 	YZ_CUDA(cudaMemcpyAsync(_cw.get(), _c.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
 	_conc = (p.conc_field != 0);
@@ -736,18 +784,22 @@ Step::~Step()
 }
 
 //  The pattern the reference fixes in C_ImplicitSolver::Alloc
-//  (ImplicitSolver.cpp:60-81): ghost rows [diag, partner] (EqualVal,
-//  BoundaryCondition.cpp:81-86), interior rows the capillary term's 13 points
-//  in FullIdx order with the diagonal first.
+//  (ImplicitSolver.cpp:60-81): the ghost rows as BoundaryCondition2D::Apply
+//  writes them (yz_bc.h), interior rows the capillary term's 13 points in
+//  FullIdx order with the diagonal first.  ghost and partner: the ghost rows
+//  and, where a ghost row copies one cell, that cell (else -1).
 void BuildPattern2D(const yz_step_params &p, std::vector<int> &rowptr, std::vector<int> &col,
-                    std::vector<int> &isbc, std::vector<int> &ghost, std::vector<int> &partner)
+                    std::vector<int> &isbc, std::vector<int> &ghost, std::vector<int> &partner, BcPlan *planOut)
 {
 	const int nx = p.nx, ny = p.ny, n = nx * ny;
+	BcPlan plan = BuildBcPlan(p);
 	rowptr.assign((size_t)n + 1, 0);
 	col.clear(); isbc.assign((size_t)n, 0);
-	ghost.clear(); partner.clear();
+	ghost = plan.ghost;
+	partner = plan.partner;
 	static const int off[13][2] = {{0, -2}, {-1, -1}, {0, -1}, {1, -1}, {-2, 0}, {-1, 0}, {0, 0}, {1, 0}, {2, 0},
 	                               {-1, 1}, {0, 1}, {1, 1}, {0, 2}};
+	size_t g = 0;
 	for(int iy = 0; iy < ny; ++iy)
 		for(int ix = 0; ix < nx; ++ix)
 		{
@@ -762,24 +814,19 @@ void BuildPattern2D(const yz_step_params &p, std::vector<int> &rowptr, std::vect
 			else
 			{
 				isbc[(size_t)i] = 1;
-				const int px = PartnerOf(ix, nx, p.bc[0], p.bc[1]);
-				const int py = PartnerOf(iy, ny, p.bc[2], p.bc[3]);
-				const int j = py * nx + px;
-				col.push_back(i);
-				col.push_back(j);
-				ghost.push_back(i);
-				partner.push_back(j);
+				const std::vector<int> &c = plan.cols[g++];
+				col.insert(col.end(), c.begin(), c.end());
 			}
 			rowptr[(size_t)i + 1] = (int)col.size();
 		}
+	if(planOut) *planOut = std::move(plan);
 }
 
 void CheckParams(const yz_step_params &p)
 {
 	if(p.nx < 8 || p.ny < 8) throw UsageError("step: the grid needs at least 4 x 4 cells");
 	for(int e = 0; e < 4; ++e)
-		if(p.bc[e] != YZ_BC_SYMMETRY && p.bc[e] != YZ_BC_PERIODIC)
-			throw UsageError("step: only Symmetry and Periodic edges are supported");
+		if(p.bc[e] < YZ_BC_SYMMETRY || p.bc[e] > YZ_BC_OUTLET) throw UsageError("step: unknown edge kind");
 	if((p.bc[0] == YZ_BC_PERIODIC) != (p.bc[1] == YZ_BC_PERIODIC) || (p.bc[2] == YZ_BC_PERIODIC) != (p.bc[3] == YZ_BC_PERIODIC))
 		throw UsageError("step: a Periodic edge needs a Periodic opposite edge");
 	if(!p.on_laplace) throw UsageError("step: the capillary term (Physics.LaplacePressure) must be enabled");
@@ -787,6 +834,9 @@ void CheckParams(const yz_step_params &p)
 		throw UsageError("step: unknown Numerics.Convection.Height scheme");
 	if(p.conc_field != 0)
 	{
+		for(int e = 0; e < 4; ++e)
+			if(p.bc[e] != YZ_BC_SYMMETRY && p.bc[e] != YZ_BC_PERIODIC)
+				throw UsageError("step: the concentration equation is built for Symmetry and Periodic edges only");
 		if(p.conv_conc < YZ_SCHEME_UPWIND1 || p.conv_conc > YZ_SCHEME_VANLEER)
 			throw UsageError("step: unknown Numerics.Convection.Concentration scheme");
 		if(!(p.theta_c > 0.0)) throw UsageError("step: theta_c must be > 0");
@@ -795,7 +845,7 @@ void CheckParams(const yz_step_params &p)
 
 void Step::BuildPattern()
 {
-	BuildPattern2D(_p, _rowptr, _col, _isbc, _ghost, _partner);
+	BuildPattern2D(_p, _rowptr, _col, _isbc, _ghost, _partner, &_bc);
 	_nnz = (int)_col.size();
 	//  the sorted mirror (CRS_Matrix::BuildSortPermutation, CRS_Matrix.cpp:360-384)
 	std::vector<int> scol((size_t)_nnz), ssrc((size_t)_nnz);
@@ -814,6 +864,35 @@ void Step::BuildPattern()
 	_dIsbc.upload(bc8.data(), bc8.size(), _st);
 	_dGhost.upload(_ghost.data(), _ghost.size(), _st);
 	_dPartner.upload(_partner.data(), _partner.size(), _st);
+	//  the Newton matrix's ghost rows (their values in storage order) and
+	//  right-hand side, and the SatisfyBCRows programme
+	std::vector<int> pos;
+	std::vector<double> val;
+	for(size_t g = 0; g < _bc.ghost.size(); ++g)
+		for(size_t k = 0; k < _bc.vals[g].size(); ++k)
+		{
+			pos.push_back(_rowptr[(size_t)_bc.ghost[g]] + (int)k);
+			val.push_back(_bc.vals[g][k]);
+		}
+	_nBcVal = (int)pos.size();
+	_dBcPos.upload(pos.data(), pos.size(), _st);
+	_dBcVal.upload(val.data(), val.size(), _st);
+	_dBcRhs.upload(_bc.rhs.data(), _bc.rhs.size(), _st);
+	_nBcSets = (int)_bc.setM.size();
+	if(!_bc.simple)
+	{
+		_dSetM.upload(_bc.setM.data(), _bc.setM.size(), _st);
+		_dSetRowOff.upload(_bc.setRowOff.data(), _bc.setRowOff.size(), _st);
+		_dSetMatOff.upload(_bc.setMatOff.data(), _bc.setMatOff.size(), _st);
+		_dSetRow.upload(_bc.row.data(), _bc.row.size(), _st);
+		_dSetRhs.upload(_bc.rowRhs.data(), _bc.rowRhs.size(), _st);
+		_dTermOff.upload(_bc.termOff.data(), _bc.termOff.size(), _st);
+		_dTermCol.upload(_bc.termCol.data(), _bc.termCol.size(), _st);
+		_dTermVal.upload(_bc.termVal.data(), _bc.termVal.size(), _st);
+		_dPiv.upload(_bc.piv.data(), _bc.piv.size(), _st);
+		_dFac.upload(_bc.fac.data(), _bc.fac.size(), _st);
+		_dU.upload(_bc.U.data(), _bc.U.size(), _st);
+	}
 }
 
 //  The coefficient tables, computed as the reference's SetLinearCoef does
@@ -866,7 +945,11 @@ void Step::BuildCoef()
 	k.xmin = p.xmin; k.ymin = p.ymin; k.dx = dx; k.dy = dy; k.dx2h = dx * 0.5; k.dy2h = dy * 0.5;
 	//  the upwinded terms
 	k.onPG = p.on_pgrav; k.onSC = p.on_marangoni; k.onCF = p.on_centrifugal;
-	for(int e = 0; e < 4; ++e) k.wall[e] = (p.bc[e] == YZ_BC_SYMMETRY);   // BoundaryCondition::IsWall
+	for(int e = 0; e < 4; ++e)
+	{
+		k.wall[e] = (p.bc[e] == YZ_BC_SYMMETRY || p.bc[e] == YZ_BC_PINNING);   // BoundaryCondition::IsWall
+		k.pinned[e] = (p.bc[e] == YZ_BC_PINNING);
+	}
 	k.hI = MakeInterp(p.conv_height);
 	const double pg[2] = {p.Pgx, p.Pgy};
 	for(int a = 0; a < 2; ++a) { k.pgMag[a] = pg[a] / 3.0; k.pgSign[a] = pg[a] >= 0 ? 1.0 : -1.0; }
@@ -926,6 +1009,24 @@ void Step::Assemble(int mode, const double *hField, const double *cField, double
 	const int nIn = (_p.nx - 4) * (_p.ny - 4);
 	YZ_LAUNCH(KAssemble, GridFor(nIn, 128, 148 * 32), 128, 0, _st, _k, mode, dt, _dRowptr.get(), hField, cField,
 	          _s.get(), o, _fb, up);
+}
+
+//  the ghost rows of x satisfied exactly (SatisfyBCRows with the Newton
+//  system's right-hand side on them)
+void Step::SatisfyGhosts(double *x)
+{
+	if(_bc.simple)
+	{
+		YZ_LAUNCH(KGhostCopy, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
+		          _dPartner.get(), x);
+		return;
+	}
+	BcSets S;
+	S.n = _nBcSets;
+	S.m = _dSetM.get(); S.rowOff = _dSetRowOff.get(); S.matOff = _dSetMatOff.get(); S.row = _dSetRow.get();
+	S.termOff = _dTermOff.get(); S.termCol = _dTermCol.get(); S.piv = _dPiv.get();
+	S.rhs = _dSetRhs.get(); S.termVal = _dTermVal.get(); S.fac = _dFac.get(); S.U = _dU.get();
+	YZ_LAUNCH(KSatisfyBC, GridFor((long long)_nBcSets, 128), 128, 0, _st, S, x);
 }
 
 //  one Newton-Kantorovich attempt at the present dt (NKLoop)
@@ -1036,11 +1137,7 @@ bool Step::NKLoop(int &iter, double &resid, yz_step_stats &stats)
 		stats.amg_setups += _solver->Rebuilds() - r0;
 		stats.linear_iterations += it;
 		ZeroMax(kSlotDelta);
-		if(ch == 0)
-		{
-			YZ_LAUNCH(KGhostCopy, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
-			          _dPartner.get(), _delta.get());
-		}
+		if(ch == 0) SatisfyGhosts(_delta.get());
 		else YZ_CUDA(cudaMemsetAsync(_delta.get(), 0, (size_t)n * sizeof(double), _st));
 		YZ_LAUNCH(KAbsMax, g, 256, 0, _st, n, _delta.get(), _red.get() + kSlotDelta);
 		double residEq = ReadMax(kSlotDelta);

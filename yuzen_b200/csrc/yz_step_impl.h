@@ -1,6 +1,8 @@
 // yz_step_impl.h -- the device step context behind yz_step_* (C ABI).
 #pragma once
 
+#include "yz_bc.h"
+
 #include "yz_learned.h"
 #include "yz_physics.cuh"
 #include "yz_solver_impl.h"
@@ -11,7 +13,8 @@
 namespace yz {
 
 void BuildPattern2D(const yz_step_params &p, std::vector<int> &rowptr, std::vector<int> &col,
-                    std::vector<int> &isbc, std::vector<int> &ghost, std::vector<int> &partner);
+                    std::vector<int> &isbc, std::vector<int> &ghost, std::vector<int> &partner,
+                    BcPlan *plan = nullptr);
 void CheckParams(const yz_step_params &p);
 
 class Step
@@ -63,6 +66,7 @@ private:
 	void BuildPattern();
 	void BuildCoef();
 	void FaceProps(const double *H, const double *C, bool J);
+	void SatisfyGhosts(double *x);
 	void Assemble(int mode, const double *hField, const double *cField, double dt);
 	bool NKLoop(int &iter, double &resid, yz_step_stats &stats);
 	//  the concentration equation
@@ -88,6 +92,15 @@ private:
 	std::vector<int> _rowptr, _col, _isbc, _ghost, _partner;
 	DBuf<int> _dRowptr, _dGhost, _dPartner;
 	DBuf<unsigned char> _dIsbc;
+	//  the ghost rows (yz_bc.h): the Newton matrix's values on them and their
+	//  right-hand side, and the SatisfyBCRows programme (used unless every
+	//  ghost row copies one cell)
+	BcPlan _bc;
+	DBuf<int> _dBcPos;
+	DBuf<double> _dBcVal, _dBcRhs;
+	int _nBcSets = 0, _nBcVal = 0;
+	DBuf<int> _dSetM, _dSetRowOff, _dSetMatOff, _dSetRow, _dTermOff, _dTermCol, _dPiv;
+	DBuf<double> _dSetRhs, _dTermVal, _dFac, _dU;
 	//  fields: the committed film h (field), c, s; phi_old, phi_old2, phi_new,
 	//  phi_guess; A h at phi_old and at the guess; the system
 	DBuf<double> _h, _c, _s, _hOld, _hOld2, _hNew, _guess, _axOld, _axGuess, _rhs, _delta, _evapOld, _evapB, _ia;
