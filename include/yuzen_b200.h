@@ -260,6 +260,17 @@ typedef struct yz_step_params
 	double theta_c;               /* 0.5 (Crank-Nicolson) */
 	double Df, diff_c0, diff_base, diff_exp;   /* Df and the diffusivity law D(c) = base exp(exp (c - c0)) */
 	yz_settings lin_conc;         /* its linear solve (conc = 1: the SPAI0-first role) */
+	/* the liquid supply of a nozzle (Physics.Source; SourceBase.cpp,
+	 * WM2D/Source.cpp): flow rate src_rate (1 - exp(-t / src_tau)) into the
+	 * cells' area fractions within src_radius of the nozzle, sampled on
+	 * src_subregions^2 points a cell; the nozzle at the tip of an arm of
+	 * length src_arm about (src_arm_x, src_arm_y) turning at src_omega from
+	 * src_angle0, its angular speed ramped up over src_ramp, held over
+	 * src_plateau and ramped down, from src_t0; evaluated at the middle of
+	 * each step.  Not with conc_field. */
+	int    on_source, src_subregions;
+	double src_radius, src_rate, src_tau, src_arm, src_arm_x, src_arm_y, src_omega, src_angle0, src_ramp,
+	       src_plateau, src_t0;
 } yz_step_params;
 
 typedef struct yz_step_stats

@@ -154,6 +154,12 @@ int main(int argc, char **argv)
 		put(D, G->X(G->HalfXm(z0))); put(D, G->Y(G->HalfYm(z0)));
 		put(D, he._Centrifugal._Cnt[0]); put(D, he._Centrifugal._Cnt[1]);
 		put(D, ce._bcg._set.epsilon); put(D, ce._theta);
+		//  the nozzle (SourceBase)
+		const auto &src = he._Source;
+		put(I, src._numSubRegion);
+		put(D, src._Radius); put(D, src._flowRate); put(D, src._timeConstant); put(D, src._armLength);
+		put(D, src._armX); put(D, src._armY); put(D, src._rotationRate); put(D, src._startAngle);
+		put(D, src._slopeTime); put(D, src._mainTime); put(D, m->_timeStep.StartTime());
 	}
 
 	std::vector<double> h0, c0, s0;

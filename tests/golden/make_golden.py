@@ -194,6 +194,29 @@ STEP_CASES = {
         "Numerics.TimeStepControl.Enable": True, "Numerics.TimeStepControl.KeepSteps": 2,
         "Numerics.TimeStepControl.ChangeFactor": 0.75, "Numerics.InitialDt": 1e-4,
     }, 4, 3),
+    # the nozzle (Physics.Source): a supply at the tip of a turning arm, its
+    # angular speed ramped up, its flow rate rising with a time constant;
+    # capillary + gravity + evaporation, mirror edges, fixed dt
+    "step_nozzle_40": ("allphys_2d_reg.toml", {
+        **_NO_UPWIND, "Grid.Nx": 40, "Grid.Ny": 40,
+        "Physics.Source": {"Enable": True, "Radius": 0.1e-3, "InletRate": 2e-3, "Conc": 0.2,
+                           "TimeConstant": 1e-4, "ArmLength": 0.25e-3, "ArmCenter": [0.0, 0.0],
+                           "RotationRate": 2000.0, "StartAngle": 0.3, "RampTime": 1e-4, "PlateauTime": 1e-3,
+                           "SubRegions": 6},
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-4,
+    }, 4, 3),
+    # the same nozzle with an Outlet edge at Xmax and the time-step control
+    # on (the nozzle is evaluated at the middle of each attempt's step)
+    "step_nozzle_outlet_adaptive_40": ("allphys_2d_reg.toml", {
+        **_NO_UPWIND, "Grid.Nx": 40, "Grid.Ny": 36,
+        "Boundary.XmaxBC.Type": "Outlet",
+        "Physics.Source": {"Enable": True, "Radius": 0.12e-3, "InletRate": 4e-3, "Conc": 0.2,
+                           "TimeConstant": 0.0, "ArmLength": 0.2e-3, "ArmCenter": [0.1e-3, 0.0],
+                           "RotationRate": 3000.0, "StartAngle": 1.0, "RampTime": 0.0, "PlateauTime": 1e-3,
+                           "SubRegions": 4},
+        "Numerics.TimeStepControl.Enable": True, "Numerics.TimeStepControl.KeepSteps": 2,
+        "Numerics.TimeStepControl.ChangeFactor": 0.75, "Numerics.InitialDt": 1e-4,
+    }, 6, 3),
     # capillary + disjoining with the time-step control on
     "step_adaptive_40": ("allphys_2d_reg.toml", {
         **_NO_UPWIND, "Grid.Nx": 40, "Grid.Ny": 40,

@@ -14,6 +14,8 @@ INT_KEYS = (
     "max_steps", "on_source",
     "conv_height", "conv_conc", "conc_conv", "conc_diff", "lin_c_precond", "lin_c_scaling", "lin_c_maxit",
     "lin_c_conc",
+    # the nozzle (SourceBase)
+    "src_subregions",
     # appended after the run
     "steps_done", "diverged",
 )
@@ -26,6 +28,10 @@ REAL_KEYS = (
     "nk_eps", "nk_eps_rel", "lin_eps", "dt_change_factor", "dt_criterion", "dt_scale_floor",
     "x0", "y0", "t_start",
     "xmin", "ymin", "rot_x", "rot_y", "lin_c_eps", "theta_c",
+    # the nozzle (SourceBase): radius, flow rate, time constant, arm length and
+    # centre, rotation rate, start angle, ramp and plateau times, start time
+    "src_radius", "src_rate", "src_tau", "src_arm", "src_arm_x", "src_arm_y", "src_omega", "src_angle0",
+    "src_ramp", "src_plateau", "src_t0",
     # appended after the run
     "run_seconds", "t_end",
     # the energy budget (EnergyEval) of the start and the end film

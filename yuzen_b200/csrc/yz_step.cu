@@ -181,6 +181,7 @@ struct RowOut
 	double *rhs;       // mode 1
 	const double *hOld, *axOld;
 	unsigned long long *rhsMax;
+	const double *src;   // mode 1: the nozzle's supply of the step, or null
 };
 
 //  three blocks of 128 a SM (168 registers a thread, a few spills) ran the
@@ -500,7 +501,7 @@ KAssemble(Coef k, int mode, double dt, const int *__restrict__ rowptr,
 		double evp = 0.0;
 		if(k.onEvap) evp = (1.0 - k.theta) * o.evapOld[i] + k.theta * EvapAt(k, hoo, coo, xx, yy, dt);
 		o.evapB[i] = evp;
-		const double B = evp - 0.0;
+		const double B = evp - (o.src ? o.src[i] : 0.0);
 		const double r = o.hOld[i] - hoo - (dt * k.theta * y) - (dt * (1.0 - k.theta) * o.axOld[i]) - dt * B;
 		o.rhs[i] = r;
 		rmax = fmax(rmax, fabs(r));
@@ -651,6 +652,41 @@ __global__ void KLte(int n, const double *__restrict__ hp, const double *__restr
 		m = fmax(m, fabs(e));
 	}
 	WarpMaxAbs(out, m);
+}
+
+//  The nozzle's supply of every real cell (Source_WM2D::updateFraction and
+//  operator(), WM2D/Source.cpp:40-110): the flow rate times the fraction of
+//  the cell's sub^2 sample points within the nozzle's radius, for the cells
+//  whose centre lies within the radius and a cell diagonal of the nozzle
+__global__ void KSource(Coef k, double xn, double yn, double radius, int sub, double flow, double *__restrict__ src)
+{
+	const int nx = k.nx, n = nx * k.ny;
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		const int ix = i % nx, iy = i / nx;
+		const double xc = k.xmin + ix * k.dx + k.dx2h, yc = k.ymin + iy * k.dy + k.dy2h;
+		const double ex = xc - xn, ey = yc - yn;
+		const double rr = sqrt(ex * ex + ey * ey);
+		double alpha = 0.0;
+		if(rr < radius + sqrt(k.dx * k.dx + k.dy * k.dy))
+		{
+			const double dxs = k.dx / (double)sub, dys = k.dy / (double)sub;
+			const double xL = xc - 0.5 * k.dx, yB = yc - 0.5 * k.dy;
+			for(int a = 0; a < sub; ++a)
+			{
+				const double xx = xL + ((double)a + 0.5) * dxs;
+				for(int b = 0; b < sub; ++b)
+				{
+					const double yy = yB + ((double)b + 0.5) * dys;
+					const double fx = xx - xn, fy = yy - yn;
+					const double r2 = sqrt(fx * fx + fy * fy);
+					alpha += (r2 <= radius ? 1.0 : 0.0);
+				}
+			}
+			alpha /= (double)(sub * sub);
+		}
+		src[i] = flow * alpha;
+	}
 }
 
 //  the Newton matrix's ghost rows and their right-hand side, once (yz_bc.h)
@@ -832,6 +868,12 @@ void CheckParams(const yz_step_params &p)
 	if(!p.on_laplace) throw UsageError("step: the capillary term (Physics.LaplacePressure) must be enabled");
 	if(p.conv_height < YZ_SCHEME_UPWIND1 || p.conv_height > YZ_SCHEME_VANLEER)
 		throw UsageError("step: unknown Numerics.Convection.Height scheme");
+	if(p.on_source)
+	{
+		if(p.conc_field != 0)
+			throw UsageError("step: the nozzle (Physics.Source) is built for the film without the concentration equation");
+		if(p.src_subregions < 1) throw UsageError("step: Physics.Source.SubRegions must be 1 or larger");
+	}
 	if(p.conc_field != 0)
 	{
 		for(int e = 0; e < 4; ++e)
@@ -1006,6 +1048,7 @@ void Step::Assemble(int mode, const double *hField, const double *cField, double
 	o.ia = _ia.get(); o.ax = mode == 0 ? _axOld.get() : _axGuess.get();
 	o.evapOld = _evapOld.get(); o.evapB = _evapB.get(); o.rhs = _rhs.get();
 	o.hOld = _hOld.get(); o.axOld = _axOld.get(); o.rhsMax = _red.get() + kSlotRhs;
+	o.src = _p.on_source ? _src.get() : nullptr;
 	const int nIn = (_p.nx - 4) * (_p.ny - 4);
 	YZ_LAUNCH(KAssemble, GridFor(nIn, 128, 148 * 32), 128, 0, _st, _k, mode, dt, _dRowptr.get(), hField, cField,
 	          _s.get(), o, _fb, up);
@@ -1029,6 +1072,36 @@ void Step::SatisfyGhosts(double *x)
 	YZ_LAUNCH(KSatisfyBC, GridFor((long long)_nBcSets, 128), 128, 0, _st, S, x);
 }
 
+//  The nozzle at the middle of the step (SourceBase::SetEvalTime in
+//  BeforeNKLoop, HeightEquationBase.h:1339): its position on the arm
+//  (SourceBase::NozzlePos: the arm's angle is the start angle plus the rate
+//  times the integral of a trapezoid ramp) and the flow rate
+//  (FlowRateNow: 1 - exp(-t / tau) of the rate), then every cell's supply
+void Step::UpdateSource(double dt)
+{
+	const yz_step_params &p = _p;
+	const double tt = _time + 0.5 * dt;
+	const double Ts = p.src_ramp, Tm = p.src_plateau;
+	const double t = std::max(0.0, tt - p.src_t0);
+	double swept;
+	if(t <= Ts) swept = (Ts > 0) ? 0.5 * t * t / Ts : 0.0;
+	else if(t <= Ts + Tm) swept = 0.5 * Ts + (t - Ts);
+	else if(t <= 2.0 * Ts + Tm)
+	{
+		const double tau = t - Ts - Tm;
+		swept = 0.5 * Ts + Tm + tau - 0.5 * tau * tau / Ts;
+	}
+	else swept = Ts + Tm;
+	const double theta = p.src_angle0 + p.src_omega * swept;
+	const double xn = p.src_arm_x + p.src_arm * std::cos(theta);
+	const double yn = p.src_arm_y + p.src_arm * std::sin(theta);
+	double coef = 1.0;
+	if(!(std::fabs(p.src_tau) <= std::numeric_limits<double>::epsilon())) coef = 1.0 - std::exp(-tt / p.src_tau);
+	const double flow = p.src_rate * coef;
+	_src.reserve((size_t)_n);
+	YZ_LAUNCH(KSource, GridFor(_n, 256), 256, 0, _st, _k, xn, yn, p.src_radius, p.src_subregions, flow, _src.get());
+}
+
 //  one Newton-Kantorovich attempt at the present dt (NKLoop)
 bool Step::NKLoop(int &iter, double &resid, yz_step_stats &stats)
 {
@@ -1038,6 +1111,7 @@ bool Step::NKLoop(int &iter, double &resid, yz_step_stats &stats)
 	YZ_CUDA(cudaMemcpyAsync(_guess.get(), _hOld.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
 	//  opt extrap
 	_extrapMove = 0;
+	if(_p.on_source) UpdateSource(dt);
 	if(!_extrapBlocked)
 	{
 		const double r = (_dtOld > 0) ? dt / _dtOld : 0.0;

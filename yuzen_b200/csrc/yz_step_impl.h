@@ -67,6 +67,7 @@ private:
 	void BuildCoef();
 	void FaceProps(const double *H, const double *C, bool J);
 	void SatisfyGhosts(double *x);
+	void UpdateSource(double dt);
 	void Assemble(int mode, const double *hField, const double *cField, double dt);
 	bool NKLoop(int &iter, double &resid, yz_step_stats &stats);
 	//  the concentration equation
@@ -101,6 +102,7 @@ private:
 	int _nBcSets = 0, _nBcVal = 0;
 	DBuf<int> _dSetM, _dSetRowOff, _dSetMatOff, _dSetRow, _dTermOff, _dTermCol, _dPiv;
 	DBuf<double> _dSetRhs, _dTermVal, _dFac, _dU;
+	DBuf<double> _src;                       // the nozzle's supply of the step (Physics.Source)
 	//  fields: the committed film h (field), c, s; phi_old, phi_old2, phi_new,
 	//  phi_guess; A h at phi_old and at the guess; the system
 	DBuf<double> _h, _c, _s, _hOld, _hOld2, _hNew, _guess, _axOld, _axGuess, _rhs, _delta, _evapOld, _evapB, _ia;

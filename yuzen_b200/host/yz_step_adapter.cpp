@@ -124,6 +124,14 @@ void FillParams(Model2D *m, yz_step_params &p)
 	p.lin_conc.precondition = (int)ce._bcg._set.precondition; p.lin_conc.scaling = ce._bcg._set.scaling ? 1 : 0;
 	p.lin_conc.max_iteration = ce._bcg._set.maxIteration; p.lin_conc.epsilon = ce._bcg._set.epsilon;
 	p.lin_conc.conc = ce._bcg._set.conc ? 1 : 0;
+	//  the nozzle (SourceBase.cpp:20-38)
+	const auto &src = he._Source;
+	p.on_source = src.Enabled() ? 1 : 0;
+	p.src_subregions = src._numSubRegion;
+	p.src_radius = src._Radius; p.src_rate = src._flowRate; p.src_tau = src._timeConstant;
+	p.src_arm = src._armLength; p.src_arm_x = src._armX; p.src_arm_y = src._armY;
+	p.src_omega = src._rotationRate; p.src_angle0 = src._startAngle;
+	p.src_ramp = src._slopeTime; p.src_plateau = src._mainTime; p.src_t0 = m->_timeStep.StartTime();
 }
 
 //  the model's fields in the device's row order IL(ix, iy) = iy nx + ix

@@ -45,6 +45,11 @@ class StepParams(ctypes.Structure):
         ("Df", ctypes.c_double), ("diff_c0", ctypes.c_double), ("diff_base", ctypes.c_double),
         ("diff_exp", ctypes.c_double),
         ("lin_conc", _Settings),
+        ("on_source", ctypes.c_int), ("src_subregions", ctypes.c_int),
+        ("src_radius", ctypes.c_double), ("src_rate", ctypes.c_double), ("src_tau", ctypes.c_double),
+        ("src_arm", ctypes.c_double), ("src_arm_x", ctypes.c_double), ("src_arm_y", ctypes.c_double),
+        ("src_omega", ctypes.c_double), ("src_angle0", ctypes.c_double), ("src_ramp", ctypes.c_double),
+        ("src_plateau", ctypes.c_double), ("src_t0", ctypes.c_double),
     ]
 
 
@@ -100,6 +105,11 @@ def params_from_state(d: dict) -> StepParams:
     p.theta_c = d["theta_c"]
     p.Df, p.diff_c0, p.diff_base, p.diff_exp = d["Df"], d["diff_c0"], d["diff_base"], d["diff_exp"]
     p.lin_conc = _Settings(d["lin_c_precond"], d["lin_c_scaling"], d["lin_c_maxit"], d["lin_c_eps"], d["lin_c_conc"])
+    # the nozzle (fixtures written before the probe dumped it have none)
+    p.on_source = int(d.get("on_source", 0))
+    p.src_subregions = int(d.get("src_subregions", 1))
+    for k in ("radius", "rate", "tau", "arm", "arm_x", "arm_y", "omega", "angle0", "ramp", "plateau", "t0"):
+        setattr(p, "src_" + k, float(d.get("src_" + k, 0.0)))
     return p
 
 
