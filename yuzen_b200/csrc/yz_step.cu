@@ -1554,6 +1554,7 @@ void Step::System(const double *hOld, const double *h, double dt, double *ia, do
 	const size_t bytes = (size_t)_n * sizeof(double);
 	YZ_CUDA(cudaMemcpyAsync(_hOld.get(), hOld, bytes, cudaMemcpyHostToDevice, _st));
 	YZ_CUDA(cudaMemcpyAsync(_guess.get(), h, bytes, cudaMemcpyHostToDevice, _st));
+	if(_p.on_source) UpdateSource(dt);
 	Assemble(0, _hOld.get(), _c.get(), dt);
 	ZeroMax(kSlotRhs);
 	Assemble(1, _guess.get(), _c.get(), dt);
