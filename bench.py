@@ -512,13 +512,14 @@ def run_device_arm(a) -> None:
         dist.destroy_process_group()
 
 
-ENSEMBLE_METRIC = "instance-steps/s of the 256-instance dewetting ensemble (64²-256², periodic)"
+ENSEMBLE_METRIC = "instance-steps/s of the 256-instance dewetting and levelling ensemble (64²-256²)"
 ENSEMBLE_UNIT = "instance-steps/s"
 
 
 def run_ensemble_arm(a) -> None:
-    """The batched ensemble (yuzen_b200.ensemble): 256 seeded dewetting
-    instances partitioned over the ranks by cost, each rank advancing its
+    """The batched ensemble (yuzen_b200.ensemble): 256 seeded dewetting and
+    levelling instances, the FP32 arms' coarse launch shapes tuned per size
+    (yuzen_b200.autotune, before the timed steps), partitioned over the ranks by cost, each rank advancing its
     instances concurrently on its GPU; a step is one step of every instance.
     Timed with CUDA events between device-wide synchronisations (the
     instances run on streams of their own), the maximum over ranks."""
@@ -543,13 +544,22 @@ def run_ensemble_arm(a) -> None:
     mine = parts[rank]
     arms = {}
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    tunings = {}
     for name in [x for x in a.arms.split(",") if x]:
         prec, reuse, learn = ARMS[name]
         if learn:
             continue        # the ensemble has no learned arm
+        #  the coarse levels' launch shapes per instance size, measured on one
+        #  instance of each size (untimed; the FP64 cycle has none)
+        tuning = {}
+        if not a.no_autotune:
+            from yuzen_b200 import autotune
+            tuning = autotune.tune([batch[k] for k in mine], prec, amg_reuse=a.amg_reuse if reuse else 0,
+                                   device=local)
+            tunings[name] = autotune.summary(tuning)
         ens = ensemble.Ensemble([batch[k] for k in mine], device=local, precision=prec,
                                 amg_reuse=a.amg_reuse if reuse else 0, workers=a.workers,
-                                graph_loop=None if a.ensemble_graph < 0 else bool(a.ensemble_graph))
+                                graph_loop=None if a.ensemble_graph < 0 else bool(a.ensemble_graph), tuning=tuning)
         if a.warmup > 0:
             ens.advance(a.warmup)
         if dist:
@@ -621,7 +631,10 @@ def run_ensemble_arm(a) -> None:
                        "graph_loop": "with hierarchy reuse" if a.ensemble_graph < 0 else bool(a.ensemble_graph),
                        "arms": {k: {"instance_steps_per_s": v["value"], "ms_per_step": v["max_ms"] / a.steps,
                                     "gpu_launches": v["launches"]} for k, v in arms.items()},
-                       "checksum_rel_diff_vs_fp64": diff},
+                       "checksum_rel_diff_vs_fp64": diff,
+                       "autotune": tunings.get(head_name) if tunings else "off",
+                       "kinds": {"dewetting": sum(1 for c in batch if c.name.startswith("dewetting")),
+                                 "levelling": sum(1 for c in batch if c.name.startswith("levelling"))}},
             "e2e": {"value": len(batch) * e2e_steps / float(et.item()) if e2e_steps else None, "unit": ENSEMBLE_UNIT,
                     "h2d_bytes_per_step": bytes_step, "d2h_bytes_per_step": bytes_step, "steps": e2e_steps},
             "gpu_launches": head["launches"],
@@ -652,6 +665,7 @@ def main() -> None:
     ap.add_argument("--amg-reuse", type=int, default=64, help="solves an AMG set-up serves in the fp32_reuse arm")
     ap.add_argument("--roofline-steps", type=int, default=3, help="steps over which the roofline kernel is timed")
     ap.add_argument("--workers", type=int, default=64, help="host threads advancing the ensemble's instances")
+    ap.add_argument("--no-autotune", action="store_true", help="the ensemble's default launch shapes, untuned")
     ap.add_argument("--ref-instances", type=int, default=3, help="ensemble instances the reference arm samples")
     ap.add_argument("--ensemble-graph", type=int, default=-1,
                     help="the ensemble's BiCGStab loops as CUDA graphs (1) or from the streams (0); -1: graphs "

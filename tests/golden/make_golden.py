@@ -235,6 +235,9 @@ STEP_CASES = {
 BUILT_STEP_CASES = {
     # the all-physics film of the 512^2 workload on 64^2 cells, 3 steps
     "step_allphys_64": ("allphys", {"N": 64, "steps": 3}),
+    # one instance of each kind of the batched ensemble (yuzen_b200.cases.batch)
+    "step_batch_dewetting_64": ("dewetting", {"N": 64, "theta_e": 12.0, "amp": 3e-3, "seed": 11, "steps": 5}),
+    "step_batch_levelling_64": ("levelling", {"N": 64, "amp": 0.05, "waves": 3, "seed": 7, "steps": 5}),
 }
 
 

@@ -15,15 +15,39 @@ from yuzen_b200 import cases, ensemble
 
 def test_batch_is_seeded_and_in_range():
     a, b = cases.batch(64), cases.batch(64)
-    assert [(c.Nx, c.disjoining, float(c.h_init[3, 5])) for c in a] == \
-           [(c.Nx, c.disjoining, float(c.h_init[3, 5])) for c in b]
+    key = lambda c: (c.name, c.Nx, c.disjoining, float(c.h_init[3, 5]))
+    assert [key(c) for c in a] == [key(c) for c in b]
     assert {c.Nx for c in a} <= {64, 96, 128, 192, 256}
+    kinds = {"dewetting": 0, "levelling": 0}
     for c in a:
-        assert c.Nx == c.Ny and c.bc == ("Periodic",) * 4 and c.dt_control
-        assert 5.0 <= c.disjoining[0] <= 20.0
-        amp = np.max(np.abs(c.h_init - 1.0))
-        assert amp <= 1e-2 and amp > 1e-4 * 0.5
+        assert c.Nx == c.Ny and c.dt_control
+        if c.name.startswith("dewetting"):
+            kinds["dewetting"] += 1
+            assert c.bc == ("Periodic",) * 4 and 5.0 <= c.disjoining[0] <= 20.0
+            amp = np.max(np.abs(c.h_init - 1.0))
+            assert amp <= 1e-2 and amp > 1e-4 * 0.5
+        else:
+            kinds["levelling"] += 1
+            assert c.name.startswith("levelling") and c.bc == ("Symmetry",) * 4
+            assert c.disjoining is None and c.vgrav is not None
+            amp = np.max(np.abs(c.h_init - 1.0))
+            assert 1e-2 * 0.5 < amp <= 1.1e-1
+    assert kinds["dewetting"] > 16 and kinds["levelling"] > 16
     assert len({c.Nx for c in cases.batch(256)}) == 5
+
+
+def test_autotune_classes_and_summary():
+    from yuzen_b200 import PREC_FP64, autotune
+    batch = cases.batch(32)
+    cls = autotune.size_classes(batch)
+    assert set(cls) == {(c.Nx, c.Ny) for c in batch}
+    assert all(batch[k].Nx == s[0] for s, k in cls.items())
+    assert all(min(j for j, c in enumerate(batch) if (c.Nx, c.Ny) == s) == k for s, k in cls.items())
+    assert autotune.tune(batch, PREC_FP64) == {}          # nothing to tune on the FP64 cycle
+    t = {(64, 64): {"fuse_from": 2, "coarse_lanes": 4, "ms_per_step": 1.0, "default_ms_per_step": 1.5,
+                    "trials": {"-1,0": 1.5, "2,4": 1.0}}}
+    assert autotune.summary(t) == {"64x64": {"fuse_from": 2, "coarse_lanes": 4, "ms_per_step": 1.0,
+                                             "default_ms_per_step": 1.5}}
 
 
 @pytest.mark.parametrize("world", [1, 2, 3, 8])

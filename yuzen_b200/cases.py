@@ -391,15 +391,43 @@ def dewetting(N: int, theta_e: float, amp: float, seed: int, steps: int = 12, en
                 dt_control=True, disjoining=(theta_e, 3.0, 2.0), h_init=h, conc0=0.5)
 
 
+def levelling(N: int, amp: float, waves: int, seed: int, steps: int = 12, end_time: float = 0.8) -> Case:
+    """A levelling instance of the batched ensemble: a film of mean height 1
+    corrugated by amp cos(pi waves (i + 1/2) / N) cos(pi waves (j + 1/2) / N)
+    (a mode the mirror edges keep) with seeded noise of amp / 10, on N x N
+    cells of the dewetting instances' size with Symmetry edges; capillary
+    pressure and vertical gravity (the reference's leveling cases), adaptive
+    dt."""
+    rng = np.random.default_rng(seed)
+    i = (np.arange(N) + 0.5) / N
+    mode = np.outer(np.cos(math.pi * waves * i), np.cos(math.pi * waves * i))
+    h = 1.0 + amp * mode + 0.1 * amp * rng.uniform(-1.0, 1.0, size=(N, N))
+    side = 0.64e-3 * N / 224.0
+    return Case(name=f"levelling_{N}_{seed}", Nx=N, Ny=N, xlim=(-side / 2, side / 2), ylim=(-side / 2, side / 2),
+                h0=1e-6, precursor=0.01, bc=("Symmetry",) * 4, dt=1e-4, steps=steps, end_time=end_time,
+                dt_control=True, vgrav=9.8, h_init=h, conc0=0.5)
+
+
 def batch(count: int = 256, seed: int = 20261204, sizes=(64, 96, 128, 192, 256), steps: int = 12) -> list:
-    """The batched ensemble: count seeded dewetting instances, N uniform in
-    sizes, theta_e uniform in [5, 20] deg, noise amplitude log-uniform in
-    [1e-4, 1e-2], periodic edges; instance k is seeded by (seed, k)."""
+    """The batched ensemble: count seeded instances, N uniform in sizes, half
+    of them (by a seeded draw) dewetting films -- theta_e uniform in [5, 20]
+    deg, noise amplitude log-uniform in [1e-4, 1e-2], periodic edges -- and
+    half levelling films -- corrugation amplitude log-uniform in [1e-2, 1e-1],
+    one to four half-waves, mirror edges; instance k is seeded by (seed, k)."""
     rng = np.random.default_rng(seed)
     Ns = rng.choice(np.asarray(sizes), size=count)
     th = rng.uniform(5.0, 20.0, size=count)
     amp = 10.0 ** rng.uniform(-4.0, -2.0, size=count)
-    return [dewetting(int(Ns[k]), float(th[k]), float(amp[k]), seed=seed * 1000 + k, steps=steps) for k in range(count)]
+    kind = rng.random(size=count) < 0.5
+    lamp = 10.0 ** rng.uniform(-2.0, -1.0, size=count)
+    waves = rng.integers(1, 5, size=count)
+    out = []
+    for k in range(count):
+        if kind[k]:
+            out.append(levelling(int(Ns[k]), float(lamp[k]), int(waves[k]), seed=seed * 1000 + k, steps=steps))
+        else:
+            out.append(dewetting(int(Ns[k]), float(th[k]), float(amp[k]), seed=seed * 1000 + k, steps=steps))
+    return out
 
 
 def allphys(N: int = 512, steps: int = 12, dt: float = 1e-5) -> Case:

@@ -262,6 +262,24 @@ int yz_step_set_graph_loop(yz_step *st, int on)
 	});
 }
 
+int yz_solver_set_tuning(yz_solver *s, int fuse_from, int coarse_lanes)
+{
+	return Guard([&] {
+		if(!s) throw yz::UsageError("yz_solver_set_tuning: null solver");
+		s->s->SetTuning(fuse_from, coarse_lanes);
+		return 0;
+	});
+}
+
+int yz_step_set_tuning(yz_step *st, int fuse_from, int coarse_lanes)
+{
+	return Guard([&] {
+		if(!st) throw yz::UsageError("yz_step_set_tuning: null step");
+		st->s->SetTuning(fuse_from, coarse_lanes);
+		return 0;
+	});
+}
+
 int yz_step_set_energy(yz_step *st, int on)
 {
 	return Guard([&] {

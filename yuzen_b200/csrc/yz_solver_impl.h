@@ -77,6 +77,7 @@ public:
 	int Precision() const { return _precision; }
 	void SetAmgReuse(int maxSolves);
 	void SetGraphLoop(bool on) { _graphLoop = on; }
+	void SetTuning(int fuseFrom, int coarseLanes);
 	int Rebuilds() const { return _rebuilds; }
 	//  the learned preconditioner (not owned): mode 0 off, 1 collect (the
 	//  next `collectSolves` AMG solves feed the network's sample ring with up
@@ -100,7 +101,7 @@ private:
 	Sten StenOf(size_t l) const;
 	void RoundCycle();
 	template<class TF, class TX> void Cycle32(size_t l, const TF *f, TX *x);
-	static int LanesFor(long long nnz, int n);
+	int LanesFor(long long nnz, int n) const;
 	bool CoarseCycleOn() const;
 	static int CoarseBlocksPerSm();
 	void LaunchCoarseCycle();
@@ -112,7 +113,7 @@ private:
 	                   const float *x, float *xout);
 	//  the first level whose way down and way up run fused (KDownFused,
 	//  KUpFused); past the deepest level: none
-	static int FusedFrom();
+	int FusedFrom() const;
 	void CoarseDown(int lanes, int nc, const Level &L, const float *f, float *fc);
 	void CoarseUp(int lanes, const Level &L, const float *f, const float *xc, float *x);
 	const int *Halt() const { return &_sc.get()->state; }
@@ -188,6 +189,10 @@ private:
 	//  bumped whenever a pointer or size a loop graph holds may change: the
 	//  pattern, precision or buffers (_epoch), the hierarchy (_epochH)
 	unsigned _epoch = 0, _epochH = 0;
+	//  launch shapes of the FP32 cycle's coarse levels (SetTuning): the first
+	//  fused level (-1: YZ_FUSE_FROM or 2; 0: none) and the lanes a row (0:
+	//  by the level's mean row length)
+	int _fuseFrom = -1, _coarseLanes = 0;
 	LoopGraph _loop[3];
 	bool _graphLoop = true;       // the loop as a CUDA graph (else from the stream)
 	//  Solve's tail, queued behind a graph run: x into the caller's dX

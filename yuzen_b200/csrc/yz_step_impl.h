@@ -48,6 +48,11 @@ public:
 		if(_solverC) _solverC->SetGraphLoop(on);
 		_graphLoop = on;
 	}
+	void SetTuning(int fuseFrom, int coarseLanes)
+	{
+		_solver->SetTuning(fuseFrom, coarseLanes);
+		if(_solverC) _solverC->SetTuning(fuseFrom, coarseLanes);
+	}
 	void SetAmgReuse(int maxSolves)
 	{
 		_solver->SetAmgReuse(maxSolves);

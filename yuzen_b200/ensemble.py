@@ -46,11 +46,13 @@ def partition(costs, world: int) -> list:
 
 
 class Ensemble:
-    """Ensemble(cases, device, precision, amg_reuse, workers): one Step per
-    case; advance(n) advances every instance n steps concurrently."""
+    """Ensemble(cases, device, precision, amg_reuse, workers, graph_loop,
+    tuning): one Step per case, each with the launch shapes tuning (from
+    yuzen_b200.autotune.tune) gives its size; advance(n) advances every
+    instance n steps concurrently."""
 
     def __init__(self, cases, device: int = 0, precision: int = PREC_FP64, amg_reuse: int = 0,
-                 workers: int | None = None, graph_loop: bool | None = None):
+                 workers: int | None = None, graph_loop: bool | None = None, tuning: dict | None = None):
         self.cases = list(cases)
         self.steps = []
         #  the loop graphs pay when a hierarchy serves several solves (a
@@ -66,6 +68,10 @@ class Ensemble:
             #  each context captures its loop graph from its own thread in
             #  thread-local mode; graph_loop False launches from the stream
             st.set_graph_loop(bool(graph_loop))
+            #  the launch shapes the autotuner chose for the instance's size
+            t = (tuning or {}).get((c.Nx, c.Ny))
+            if t is not None:
+                st.set_tuning(t["fuse_from"], t["coarse_lanes"])
             self.steps.append(st)
         self.workers = workers or min(len(self.steps), max(1, 2 * (os.cpu_count() or 1)))
         self._pool = concurrent.futures.ThreadPoolExecutor(max_workers=self.workers) if self.steps else None
