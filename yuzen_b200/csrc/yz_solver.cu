@@ -82,9 +82,17 @@ __global__ void KPUpdate(int n, const double *__restrict__ r, const double *__re
 		p[i] = r[i] + beta * (p[i] - omega * v[i]);
 }
 
+//  the BiCGStab SpMVs: blocks of kRT a multiprocessor (RowSumStenAll) and
+//  the film's stencil length
+#ifndef YZ_SPMV_BLOCKS
+#define YZ_SPMV_BLOCKS 4
+#endif
+constexpr int kSpmvBlocks = YZ_SPMV_BLOCKS;
+constexpr int kStenK = 13;
+
 //  v = A ph; alpha = rho / (rh . v)
 template<class V>
-__global__ void __launch_bounds__(kRT, 8) KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, Sten sn,
+__global__ void __launch_bounds__(kRT, kSpmvBlocks) KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, Sten sn,
                            const int *__restrict__ col, const V *__restrict__ val, const double *__restrict__ ph,
                            const double *__restrict__ rh, double *__restrict__ v, RedScratch rs, Scal *sc)
 {
@@ -96,7 +104,7 @@ __global__ void __launch_bounds__(kRT, 8) KSpmvAlpha(int n, const int *__restric
 		if(i >= n) break;
 		int st, len, sd;
 		RowRange(ptr, sellOff, i, st, len, sd);
-		const double s = RowSumSten(sn, i, st, len, sd, col, val, [&](int c) { return ph[c]; });
+		const double s = RowSumStenAll<kStenK>(sn, i, st, len, sd, col, val, [&](int c) { return ph[c]; });
 		v[i] = s;
 		a[0] = a[0] + rh[i] * s;
 	}
@@ -132,7 +140,7 @@ __global__ void KSUpdate(int n, const double *__restrict__ r, const double *__re
 
 //  t = A sh; omega = (t . s) / (t . t)
 template<class V>
-__global__ void __launch_bounds__(kRT, 8) KSpmvOmega(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, Sten sn,
+__global__ void __launch_bounds__(kRT, kSpmvBlocks) KSpmvOmega(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, Sten sn,
                            const int *__restrict__ col, const V *__restrict__ val, const double *__restrict__ sh_,
                            const double *__restrict__ s, double *__restrict__ t, RedScratch rs, Scal *sc)
 {
@@ -144,7 +152,7 @@ __global__ void __launch_bounds__(kRT, 8) KSpmvOmega(int n, const int *__restric
 		if(i >= n) break;
 		int st, len, sd;
 		RowRange(ptr, sellOff, i, st, len, sd);
-		const double u = RowSumSten(sn, i, st, len, sd, col, val, [&](int c) { return sh_[c]; });
+		const double u = RowSumStenAll<kStenK>(sn, i, st, len, sd, col, val, [&](int c) { return sh_[c]; });
 		t[i] = u;
 		a[0] = a[0] + u * u;
 		a[1] = a[1] + u * s[i];
@@ -847,16 +855,29 @@ void Solver::LaunchCoarseCycle()
 //  266,256 / ~30,000 / ~3,500 / ~400 rows): from level 1 the recomputation
 //  costs what the launches save (the same solve time with a quarter fewer
 //  launches), from level 2 the solve is 3 % faster than with no fusion.
-int Solver::FusedFrom()
+//  SetTuning overrides it for one context.
+int Solver::FusedFrom() const
 {
 	static const char *env = std::getenv("YZ_FUSE_FROM");
 	static const int k = env ? (std::atoi(env) > 0 ? std::atoi(env) : 1 << 30) : 2;
-	return k;
+	if(_fuseFrom == 0) return 1 << 30;
+	return _fuseFrom > 0 ? _fuseFrom : k;
+}
+
+void Solver::SetTuning(int fuseFrom, int coarseLanes)
+{
+	if(fuseFrom < -1) throw UsageError("set_tuning: fuse_from must be -1 (default), 0 (off) or a level >= 1");
+	if(coarseLanes != 0 && coarseLanes != 1 && coarseLanes != 2 && coarseLanes != 4 && coarseLanes != 8)
+		throw UsageError("set_tuning: coarse_lanes must be 0 (by row length), 1, 2, 4 or 8");
+	if(fuseFrom != _fuseFrom || coarseLanes != _coarseLanes) ++_epoch;   // the loop graph holds the old shapes
+	_fuseFrom = fuseFrom;
+	_coarseLanes = coarseLanes;
 }
 
 //  lanes a row for a coarse level of the FP32 cycle, by its mean row length
-int Solver::LanesFor(long long nnz, int n)
+int Solver::LanesFor(long long nnz, int n) const
 {
+	if(_coarseLanes > 0) return _coarseLanes;
 	const long long avg = n > 0 ? nnz / n : 0;
 	return avg >= 24 ? 8 : avg >= 10 ? 4 : avg >= 4 ? 2 : 1;
 }
