@@ -98,30 +98,6 @@ __device__ __forceinline__ auto RowSumSten(const Sten &sn, int i, int st, int le
 	return RowSum(st, len, sd, col, val, xf);
 }
 
-//  The BiCGStab SpMV's row: as RowSumSten, but a stencil row of K entries
-//  (the film's thirteen) has all its loads issued before the first product
-//  is added -- one round of memory latency instead of four; the sum is the
-//  same sequential one, so the result is the same to the bit.  Its kernels
-//  run four blocks of 256 a multiprocessor (64 registers a thread) to hold
-//  the loads.
-template<int K, class V, class XF>
-__device__ __forceinline__ auto RowSumStenAll(const Sten &sn, int i, int st, int len, int sd, const int *__restrict__ col,
-                                              const V *__restrict__ val, XF xf) -> decltype(xf(0))
-{
-	using T = decltype(xf(0));
-	if(len == K && sn.slice && sn.slice[i >> 5])
-	{
-		T v[K], xv[K];
-#pragma unroll
-		for(int j = 0; j < K; ++j) { v[j] = (T)val[st + j * sd]; xv[j] = xf(i + sn.off[j]); }
-		T s = T(0);
-#pragma unroll
-		for(int j = 0; j < K; ++j) s = s + v[j] * xv[j];
-		return s;
-	}
-	return RowSumSten(sn, i, st, len, sd, col, val, xf);
-}
-
 //--------------------------------------------------------------------------
 //  ScaleRows + gather into the sorted mirror (LinearSolverBackend.cpp:227-252),
 //  into both layouts of the finest level

@@ -82,17 +82,9 @@ __global__ void KPUpdate(int n, const double *__restrict__ r, const double *__re
 		p[i] = r[i] + beta * (p[i] - omega * v[i]);
 }
 
-//  the BiCGStab SpMVs: blocks of kRT a multiprocessor (RowSumStenAll) and
-//  the film's stencil length
-#ifndef YZ_SPMV_BLOCKS
-#define YZ_SPMV_BLOCKS 4
-#endif
-constexpr int kSpmvBlocks = YZ_SPMV_BLOCKS;
-constexpr int kStenK = 13;
-
 //  v = A ph; alpha = rho / (rh . v)
 template<class V>
-__global__ void __launch_bounds__(kRT, kSpmvBlocks) KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, Sten sn,
+__global__ void __launch_bounds__(kRT, 8) KSpmvAlpha(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, Sten sn,
                            const int *__restrict__ col, const V *__restrict__ val, const double *__restrict__ ph,
                            const double *__restrict__ rh, double *__restrict__ v, RedScratch rs, Scal *sc)
 {
@@ -104,7 +96,7 @@ __global__ void __launch_bounds__(kRT, kSpmvBlocks) KSpmvAlpha(int n, const int 
 		if(i >= n) break;
 		int st, len, sd;
 		RowRange(ptr, sellOff, i, st, len, sd);
-		const double s = RowSumStenAll<kStenK>(sn, i, st, len, sd, col, val, [&](int c) { return ph[c]; });
+		const double s = RowSumSten(sn, i, st, len, sd, col, val, [&](int c) { return ph[c]; });
 		v[i] = s;
 		a[0] = a[0] + rh[i] * s;
 	}
@@ -140,7 +132,7 @@ __global__ void KSUpdate(int n, const double *__restrict__ r, const double *__re
 
 //  t = A sh; omega = (t . s) / (t . t)
 template<class V>
-__global__ void __launch_bounds__(kRT, kSpmvBlocks) KSpmvOmega(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, Sten sn,
+__global__ void __launch_bounds__(kRT, 8) KSpmvOmega(int n, const int *__restrict__ ptr, const int *__restrict__ sellOff, Sten sn,
                            const int *__restrict__ col, const V *__restrict__ val, const double *__restrict__ sh_,
                            const double *__restrict__ s, double *__restrict__ t, RedScratch rs, Scal *sc)
 {
@@ -152,7 +144,7 @@ __global__ void __launch_bounds__(kRT, kSpmvBlocks) KSpmvOmega(int n, const int 
 		if(i >= n) break;
 		int st, len, sd;
 		RowRange(ptr, sellOff, i, st, len, sd);
-		const double u = RowSumStenAll<kStenK>(sn, i, st, len, sd, col, val, [&](int c) { return sh_[c]; });
+		const double u = RowSumSten(sn, i, st, len, sd, col, val, [&](int c) { return sh_[c]; });
 		t[i] = u;
 		a[0] = a[0] + u * u;
 		a[1] = a[1] + u * s[i];
