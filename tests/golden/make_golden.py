@@ -194,6 +194,32 @@ STEP_CASES = {
         "Numerics.TimeStepControl.Enable": True, "Numerics.TimeStepControl.KeepSteps": 2,
         "Numerics.TimeStepControl.ChangeFactor": 0.75, "Numerics.InitialDt": 1e-4,
     }, 4, 3),
+    # the well-mixed concentration solved with open edges (its own ghost rows:
+    # the FreshInlet holds the start concentration, BoundaryCondition.cpp:
+    # 156-163), every term, fixed dt
+    "step_wm_outlet_inlet_40": ("allphys_2d_reg.toml", {
+        "Grid.Nx": 40, "Grid.Ny": 36,
+        "Boundary.XminBC.Type": "Outlet", "Boundary.XmaxBC.Type": "FreshInlet",
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-2,
+    }, 3, -1),
+    # open edges on all four sides with the concentration (its corner stencils)
+    "step_wm_open_corners_40": ("allphys_2d_reg.toml", {
+        "Grid.Nx": 40, "Grid.Ny": 40,
+        "Boundary.XminBC.Type": "FreshInlet", "Boundary.XmaxBC.Type": "Outlet",
+        "Boundary.YminBC.Type": "Outlet", "Boundary.YmaxBC.Type": "FreshInlet",
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-2,
+    }, 3, -1),
+    # a Pinning edge with the concentration (copied outwards there)
+    "step_wm_pinning_40": ("allphys_2d_reg.toml", {
+        "Grid.Nx": 40, "Grid.Ny": 36,
+        "Boundary.XminBC.Type": "Pinning",
+        "Initial.SurfaceShape.PrecursorRatio": 0.02,
+        "Initial.SurfaceShape.EllipseBump.Height": 0.0,
+        "Initial.SurfaceShape.EdgeBump": {"Order": 1, "CreateType": "add", "Base": 0.5, "Height": 1.0,
+                                          "Location": "Xmin", "Alpha": 1.0, "InnerLength": 0.05e-3,
+                                          "OuterLength": 0.15e-3},
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-3,
+    }, 3, -1),
     # the nozzle (Physics.Source): a supply at the tip of a turning arm, its
     # angular speed ramped up, its flow rate rising with a time constant;
     # capillary + gravity + evaporation, mirror edges, fixed dt

@@ -11,7 +11,6 @@
 namespace yz {
 namespace {
 
-enum Field { kHeight, kHeightJacobi };
 
 //  a CRS row as the reference's CRS_Matrix keeps it: a diagonal slot first,
 //  then the other columns in the order they were first written
@@ -79,9 +78,10 @@ void EqualVal(Rows &w, int i, int j)
 struct Slot
 {
 	int L[4], opp[4], cs, st;
+	double cb;      // the concentration the FreshInlet holds (the start field's, next to the edge)
 };
 
-void ApplyEdge(Rows &w, Field tf, int tbc, const Slot &e)
+void ApplyEdge(Rows &w, int tf, int tbc, const Slot &e)
 {
 	const int *L = e.L;
 	switch(tbc)
@@ -96,16 +96,29 @@ void ApplyEdge(Rows &w, Field tf, int tbc, const Slot &e)
 		EqualVal(w, L[1], e.opp[2]);
 		break;
 	case kBcPinning:
+		if(tf == kBcFieldConc)
+		{
+			//  the concentration copied outwards (the 2-D form)
+			EqualVal(w, L[1], L[2]);
+			EqualVal(w, L[0], L[1]);
+			break;
+		}
 		//  the film on the wall face zero, no normal velocity
 		w.Diag(L[1], 0.5); w.Set(L[1], L[2], 0.5);
 		w.Diag(L[0], 1.0); w.Set(L[0], L[1], -3.0); w.Set(L[0], L[2], +3.0); w.Set(L[0], L[3], -1.0);
 		break;
 	case kBcFreshInlet:
+		if(tf == kBcFieldConc)
+		{
+			//  the start concentration at the edge held, zero second difference
+			Dirichlet(w, L[1], e.cs, e.st, e.cb);
+			w.Diag(L[0], 1.0); w.Set(L[0], L[1], -2.0); w.Set(L[0], L[2], +1.0);
+			break;
+		}
 		//  the film's start value held (its right-hand side does not enter
 		//  the pattern; the correction's is zero)
 		Dirichlet(w, L[1], e.cs, e.st, 0.0);
 		Derive3(w, L[0], e.cs, e.st);
-		(void)tf;
 		break;
 	case kBcOutlet:
 		Derive2(w, L[0], e.cs, e.st);
@@ -156,6 +169,10 @@ const CornerRow kInletInletH[4] = {{-1.0, +4.0, -18.0, -18.0, +81.0, -(16.0 - 72
                                    {-3.0, +2.0, -9.0, -12.0, +54.0, -(8.0 - 48.0 + 8.0)},
                                    {-3.0, +2.0, -12.0, -9.0, +54.0, -(16.0 - 72.0 + 24.0)},
                                    {-9.0, +1.0, -6.0, -6.0, +36.0, -(8.0 - 48.0 + 24.0)}};
+const CornerRow kInletInletC[4] = {{-49.0, +4.0, -54.0, -54.0, +729.0, -(64.0 - 864.0 + 224.0)},
+                                   {-49.0, +2.0, -27.0, -20.0, +270.0, -(32.0 - 320.0 + 112.0)},
+                                   {-49.0, +2.0, -20.0, -27.0, +270.0, -(32.0 - 432.0 + 224.0)},
+                                   {-49.0, +1.0, -10.0, -10.0, +100.0, -(16.0 - 160.0 + 112.0)}};
 const CornerRow kInletOutlet[4] = {{-1.0, -4.0, +6.0, +18.0, -27.0, -8.0},
                                    {-3.0, -2.0, +3.0, +12.0, -18.0, -8.0},
                                    {-1.0, -2.0, +4.0, +9.0, -18.0, -8.0},
@@ -195,13 +212,14 @@ const char *BcName(int t)
 	}
 }
 
-//  ApplyCorners (BoundaryCondition.cpp:612-743) with the film's corner value
-//  zero (the correction's); the combinations the reference does not
-//  implement are refused as it refuses them
-void ApplyCorner(Rows &w, int tx, int ty, const Corner &ci, const Corner &ciRO, const Corner &ciOR,
-                 const Corner &ciRR)
+//  ApplyCorners (BoundaryCondition.cpp:612-743) with the corner value val
+//  (the correction's zero for the film; the start concentration's mean near
+//  the corner for the concentration); the combinations the reference does
+//  not implement are refused as it refuses them
+void ApplyCorner(Rows &w, int tf, int tx, int ty, const Corner &ci, const Corner &ciRO, const Corner &ciOR,
+                 const Corner &ciRR, double val)
 {
-	const double val = 0.0;
+	const bool conc = (tf == kBcFieldConc);
 	auto refuse = [&]() {
 		throw UsageError(std::string("step: a corner of a ") + BcName(tx) + " and a " + BcName(ty) +
 		                 " edge is not implemented (BC: " + BcName(tx) + "-" + BcName(ty) + ")");
@@ -220,7 +238,8 @@ void ApplyCorner(Rows &w, int tx, int ty, const Corner &ci, const Corner &ciRO, 
 		else MirrorX(w, ci, ciRO);
 		break;
 	case kBcPinning:
-		if(ty == kBcSymmetry)
+		if(ty == kBcSymmetry && conc) MirrorXY(w, ci, ci);
+		else if(ty == kBcSymmetry)
 		{
 			w.Diag(ci.OOii, 0.5); w.Set(ci.OOii, ci.IIoo, 0.5);
 			w.Diag(ci.OOio, 0.5); w.Set(ci.OOio, ci.IIoi, 0.5);
@@ -228,6 +247,7 @@ void ApplyCorner(Rows &w, int tx, int ty, const Corner &ci, const Corner &ciRO, 
 			w.Diag(ci.OOoo, 1.0); w.Set(ci.OOoo, ci.OIoi, -1.0);
 		}
 		else if(ty == kBcPeriodic) MirrorY(w, ci, ciOR);
+		else if(ty == kBcPinning && conc) CopyCorner(w, ci, ci.IIoo, ci.OOii, ci.OOii, ci.OOii);
 		else if(ty == kBcPinning)
 			throw UsageError("step: two Pinning edges meeting at a corner leave three of the corner's ghost "
 			                 "rows without a condition in the reference (BoundaryCondition.cpp:678-689)");
@@ -236,7 +256,7 @@ void ApplyCorner(Rows &w, int tx, int ty, const Corner &ci, const Corner &ciRO, 
 	case kBcFreshInlet:
 		if(ty == kBcSymmetry) MirrorY(w, ci, ci);
 		else if(ty == kBcPeriodic) MirrorY(w, ci, ciOR);
-		else if(ty == kBcFreshInlet) CornerStencil(w, ci, kInletInletH, val, true);
+		else if(ty == kBcFreshInlet) CornerStencil(w, ci, conc ? kInletInletC : kInletInletH, val, true);
 		else if(ty == kBcOutlet) CornerStencil(w, ci, kInletOutlet, val, true);
 		else refuse();
 		break;
@@ -250,10 +270,12 @@ void ApplyCorner(Rows &w, int tx, int ty, const Corner &ci, const Corner &ciRO, 
 	}
 }
 
-void ApplyAll(Rows &w, const yz_step_params &p)
+void ApplyAll(Rows &w, const yz_step_params &p, int tf, const double *c)
 {
 	const int nx = p.nx, ny = p.ny;
 	auto il = [nx](int ix, int iy) { return iy * nx + ix; };
+	//  the start concentration (zero for the film's rows, which take none)
+	auto cc = [&](int ix, int iy) { return c ? c[(size_t)il(ix, iy)] : 0.0; };
 	for(int jy = 2; jy < ny - 2; ++jy)
 	{
 		Slot m, q;
@@ -264,8 +286,10 @@ void ApplyAll(Rows &w, const yz_step_params &p)
 		}
 		m.cs = m.L[0]; m.st = 1;
 		q.cs = q.L[3]; q.st = 1;
-		ApplyEdge(w, kHeightJacobi, p.bc[0], m);
-		ApplyEdge(w, kHeightJacobi, p.bc[1], q);
+		m.cb = 0.5 * (cc(1, jy) + cc(2, jy));
+		q.cb = 0.5 * (cc(nx - 2, jy) + cc(nx - 3, jy));
+		ApplyEdge(w, tf, p.bc[0], m);
+		ApplyEdge(w, tf, p.bc[1], q);
 	}
 	for(int ix = 2; ix < nx - 2; ++ix)
 	{
@@ -277,28 +301,39 @@ void ApplyAll(Rows &w, const yz_step_params &p)
 		}
 		m.cs = m.L[0]; m.st = nx;
 		q.cs = q.L[3]; q.st = nx;
-		ApplyEdge(w, kHeightJacobi, p.bc[2], m);
-		ApplyEdge(w, kHeightJacobi, p.bc[3], q);
+		m.cb = 0.5 * (cc(ix, 1) + cc(ix, 2));
+		q.cb = 0.5 * (cc(ix, ny - 2) + cc(ix, ny - 3));
+		ApplyEdge(w, tf, p.bc[2], m);
+		ApplyEdge(w, tf, p.bc[3], q);
 	}
 	const int xm[4] = {0, 1, 2, 3}, xp[4] = {nx - 1, nx - 2, nx - 3, nx - 4};
 	const int ym[4] = {0, 1, 2, 3}, yp[4] = {ny - 1, ny - 2, ny - 3, ny - 4};
 	const Corner mm = MakeCorner(nx, xm, ym), mp = MakeCorner(nx, xm, yp), pm = MakeCorner(nx, xp, ym),
 	             pp = MakeCorner(nx, xp, yp);
-	ApplyCorner(w, p.bc[0], p.bc[2], mm, pm, mp, pp);
-	ApplyCorner(w, p.bc[0], p.bc[3], mp, pp, mm, pm);
-	ApplyCorner(w, p.bc[1], p.bc[2], pm, mm, pp, mp);
-	ApplyCorner(w, p.bc[1], p.bc[3], pp, mp, pm, mm);
+	//  ApplyCornersAll (BoundaryCondition.cpp:486-524): the corner values
+	double vMM = 0, vMP = 0, vPM = 0, vPP = 0;
+	if(tf == kBcFieldConc)
+	{
+		vMM = 0.25 * (cc(1, 1) + cc(2, 1) + cc(1, 2) + cc(2, 2));
+		vPM = 0.25 * (cc(nx - 2, 1) + cc(nx - 3, 1) + cc(nx - 2, 2) + cc(nx - 3, 2));
+		vMP = 0.25 * (cc(1, ny - 2) + cc(2, ny - 2) + cc(1, ny - 3) + cc(2, ny - 3));
+		vPP = 0.25 * (cc(nx - 2, ny - 2) + cc(nx - 3, ny - 2) + cc(nx - 2, ny - 3) + cc(nx - 3, ny - 3));
+	}
+	ApplyCorner(w, tf, p.bc[0], p.bc[2], mm, pm, mp, pp, vMM);
+	ApplyCorner(w, tf, p.bc[0], p.bc[3], mp, pp, mm, pm, vMP);
+	ApplyCorner(w, tf, p.bc[1], p.bc[2], pm, mm, pp, mp, vPM);
+	ApplyCorner(w, tf, p.bc[1], p.bc[3], pp, mp, pm, mm, vPP);
 }
 
 } // namespace
 
-BcPlan BuildBcPlan(const yz_step_params &p)
+BcPlan BuildBcPlan(const yz_step_params &p, int field, const double *c)
 {
 	const int nx = p.nx, ny = p.ny, n = nx * ny;
 	for(int e = 0; e < 4; ++e)
 		if(p.bc[e] < kBcSymmetry || p.bc[e] > kBcOutlet) throw UsageError("step: unknown edge kind");
 	Rows w(n);
-	ApplyAll(w, p);
+	ApplyAll(w, p, field, c);
 	BcPlan P;
 	std::vector<int> loc((size_t)n, -1);
 	for(int iy = 0; iy < ny; ++iy)
@@ -315,12 +350,18 @@ BcPlan BuildBcPlan(const yz_step_params &p)
 			c.insert(c.end(), r.col.begin(), r.col.end());
 			v.insert(v.end(), r.val.begin(), r.val.end());
 			const bool copy = v.size() == 2 && v[0] == 1.0 && v[1] == -1.0 && r.rhs == 0.0 && !std::signbit(r.rhs);
-			if(!copy) P.simple = false;
 			P.partner.push_back(copy ? c[1] : -1);
 			P.cols.push_back(c);
 			P.vals.push_back(v);
 			P.rhs.push_back(r.rhs);
 		}
+	//  a copy whose cell is itself a ghost is coupled to that ghost's row
+	//  (solved with it), not a copy of a solved value
+	for(size_t g = 0; g < P.ghost.size(); ++g)
+	{
+		if(P.partner[g] >= 0 && loc[(size_t)P.partner[g]] >= 0) P.partner[g] = -1;
+		if(P.partner[g] < 0) P.simple = false;
+	}
 	//  SatisfyBCRows (CRS_Matrix.cpp:198-302): the sets by union-find over
 	//  the rows' nonzero entries in other ghost rows
 	const int nr = (int)P.ghost.size();

@@ -64,8 +64,24 @@ struct BcPlan
 
 constexpr int kMaxBcSet = 8;
 
+//  a plan on the device, as the SatisfyBCRows kernel reads it; rhsVec
+//  non-null: the right-hand side of row i is rhsVec[i] instead of the plan's
+struct BcSets
+{
+	int n;
+	const int *m, *rowOff, *matOff, *row, *termOff, *termCol, *piv;
+	const double *rhs, *termVal, *fac, *U;
+	const double *rhsVec;
+};
+
+//  the rows of the film's Newton matrix (the correction's, HeightJacobi) or
+//  of the concentration equation (Conc: its values, and its right-hand side
+//  from the start concentration c next to the edges and corners)
+enum { kBcFieldHeight = 0, kBcFieldConc = 1 };
+
 //  the plan of a grid with the edges of p (throws UsageError for a corner
-//  the reference does not implement or leaves open)
-BcPlan BuildBcPlan(const yz_step_params &p);
+//  the reference does not implement or leaves open); c: the start
+//  concentration (n values) for the Conc field, else null
+BcPlan BuildBcPlan(const yz_step_params &p, int field = kBcFieldHeight, const double *c = nullptr);
 
 } // namespace yz

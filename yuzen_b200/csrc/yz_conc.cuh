@@ -252,7 +252,9 @@ __global__ void KConcGhostRhs(int nGhost, const int *__restrict__ ghost, const i
 //  field's c = min(c1, 1) and the largest move of it since the last pass;
 //  mode 1 (the solves that complete the step): the largest move of c1 from
 //  the limiter state it was solved with.
-__global__ void KConcUpdate(int n, int mode, const int *__restrict__ partnerAll, const double *__restrict__ c0,
+//  useCx: c1 and its ghosts are in cx already (the ghost rows solved
+//  another way); the kernel then does the bookkeeping only
+__global__ void KConcUpdate(int n, int mode, int useCx, const int *__restrict__ partnerAll, const double *__restrict__ c0,
                             double *__restrict__ d, const double *__restrict__ rhsD, double *__restrict__ cx,
                             double *__restrict__ cLim, double *__restrict__ cw, double *__restrict__ cPrev,
                             unsigned long long *maxOut)
@@ -262,7 +264,8 @@ __global__ void KConcUpdate(int n, int mode, const int *__restrict__ partnerAll,
 	{
 		const int p = partnerAll[i];
 		double x;
-		if(p == i) x = c0[i] + d[i];
+		if(useCx) x = cx[i];
+		else if(p == i) x = c0[i] + d[i];
 		else
 		{
 			const double dp = d[p];

@@ -689,6 +689,28 @@ __global__ void KSource(Coef k, double xn, double yn, double radius, int sub, do
 	}
 }
 
+//  the right-hand side of the concentration's correction d on the ghost rows:
+//  the row's b less its product with c0, summed in storage order
+//  (ConcEquationBase.h:283-294)
+__global__ void KBcRhs(int nGhost, const int *__restrict__ ghost, const int *__restrict__ rowptr,
+                       const int *__restrict__ col, const double *__restrict__ val, const double *__restrict__ b,
+                       const double *__restrict__ c0, double *__restrict__ rhs)
+{
+	for(int g = blockIdx.x * blockDim.x + threadIdx.x; g < nGhost; g += gridDim.x * blockDim.x)
+	{
+		const int i = ghost[g];
+		double v = 0;
+		for(int k = rowptr[i]; k < rowptr[i + 1]; ++k) v += val[k] * c0[col[k]];
+		rhs[i] = b[g] - v;
+	}
+}
+
+//  y = a + d
+__global__ void KAddTo(int n, const double *__restrict__ a, const double *__restrict__ d, double *__restrict__ y)
+{
+	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = a[i] + d[i];
+}
+
 //  the Newton matrix's ghost rows and their right-hand side, once (yz_bc.h)
 __global__ void KSetGhostRows(int nVal, const int *__restrict__ pos, const double *__restrict__ val, int nGhost,
                               const int *__restrict__ ghost, const double *__restrict__ grhs, double *__restrict__ ia,
@@ -703,13 +725,6 @@ __global__ void KSetGhostRows(int nVal, const int *__restrict__ pos, const doubl
 //  side less its other terms (in the plan's order), the elimination of the
 //  right-hand side with the plan's pivots and multipliers, and the back
 //  substitution on the eliminated matrix
-struct BcSets
-{
-	int n;
-	const int *m, *rowOff, *matOff, *row, *termOff, *termCol, *piv;
-	const double *rhs, *termVal, *fac, *U;
-};
-
 __global__ void KSatisfyBC(BcSets S, double *__restrict__ x)
 {
 	for(int c = blockIdx.x * blockDim.x + threadIdx.x; c < S.n; c += gridDim.x * blockDim.x)
@@ -722,7 +737,7 @@ __global__ void KSatisfyBC(BcSets S, double *__restrict__ x)
 		{
 			double s = 0;
 			for(int t = S.termOff[r0 + p]; t < S.termOff[r0 + p + 1]; ++t) s += S.termVal[t] * x[S.termCol[t]];
-			b[p] = S.rhs[r0 + p] - s;
+			b[p] = (S.rhsVec ? S.rhsVec[S.row[r0 + p]] : S.rhs[r0 + p]) - s;
 		}
 		for(int col = 0; col < m; ++col)
 		{
@@ -808,7 +823,7 @@ Step::Step(int device, const yz_step_params &p, const double *h, const double *c
 	_cw.reserve(n);
 	YZ_CUDA(cudaMemcpyAsync(_cw.get(), _c.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
 	_conc = (p.conc_field != 0);
-	if(_conc) BuildConc();
+	if(_conc) BuildConc(c);
 	YZ_CUDA(cudaStreamSynchronize(_st));
 }
 
@@ -876,9 +891,6 @@ void CheckParams(const yz_step_params &p)
 	}
 	if(p.conc_field != 0)
 	{
-		for(int e = 0; e < 4; ++e)
-			if(p.bc[e] != YZ_BC_SYMMETRY && p.bc[e] != YZ_BC_PERIODIC)
-				throw UsageError("step: the concentration equation is built for Symmetry and Periodic edges only");
 		if(p.conv_conc < YZ_SCHEME_UPWIND1 || p.conv_conc > YZ_SCHEME_VANLEER)
 			throw UsageError("step: unknown Numerics.Convection.Concentration scheme");
 		if(!(p.theta_c > 0.0)) throw UsageError("step: theta_c must be > 0");
@@ -920,21 +932,7 @@ void Step::BuildPattern()
 	_dBcPos.upload(pos.data(), pos.size(), _st);
 	_dBcVal.upload(val.data(), val.size(), _st);
 	_dBcRhs.upload(_bc.rhs.data(), _bc.rhs.size(), _st);
-	_nBcSets = (int)_bc.setM.size();
-	if(!_bc.simple)
-	{
-		_dSetM.upload(_bc.setM.data(), _bc.setM.size(), _st);
-		_dSetRowOff.upload(_bc.setRowOff.data(), _bc.setRowOff.size(), _st);
-		_dSetMatOff.upload(_bc.setMatOff.data(), _bc.setMatOff.size(), _st);
-		_dSetRow.upload(_bc.row.data(), _bc.row.size(), _st);
-		_dSetRhs.upload(_bc.rowRhs.data(), _bc.rowRhs.size(), _st);
-		_dTermOff.upload(_bc.termOff.data(), _bc.termOff.size(), _st);
-		_dTermCol.upload(_bc.termCol.data(), _bc.termCol.size(), _st);
-		_dTermVal.upload(_bc.termVal.data(), _bc.termVal.size(), _st);
-		_dPiv.upload(_bc.piv.data(), _bc.piv.size(), _st);
-		_dFac.upload(_bc.fac.data(), _bc.fac.size(), _st);
-		_dU.upload(_bc.U.data(), _bc.U.size(), _st);
-	}
+	_dBc.Upload(_bc, _st);
 }
 
 //  The coefficient tables, computed as the reference's SetLinearCoef does
@@ -1064,12 +1062,20 @@ void Step::SatisfyGhosts(double *x)
 		          _dPartner.get(), x);
 		return;
 	}
-	BcSets S;
-	S.n = _nBcSets;
-	S.m = _dSetM.get(); S.rowOff = _dSetRowOff.get(); S.matOff = _dSetMatOff.get(); S.row = _dSetRow.get();
-	S.termOff = _dTermOff.get(); S.termCol = _dTermCol.get(); S.piv = _dPiv.get();
-	S.rhs = _dSetRhs.get(); S.termVal = _dTermVal.get(); S.fac = _dFac.get(); S.U = _dU.get();
-	YZ_LAUNCH(KSatisfyBC, GridFor((long long)_nBcSets, 128), 128, 0, _st, S, x);
+	YZ_LAUNCH(KSatisfyBC, GridFor((long long)_dBc.nSets, 128), 128, 0, _st, _dBc.Sets(nullptr), x);
+}
+
+void Step::SatisfyConcGhosts(double *x, const double *rhsVec)
+{
+	if(_bcC.simple)
+	{
+		//  every ghost copies one cell: with the equation's right-hand side
+		//  (zero) the copy; the d system's is done by KConcUpdate
+		YZ_LAUNCH(KGhostCopy, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
+		          _dPartner.get(), x);
+		return;
+	}
+	YZ_LAUNCH(KSatisfyBC, GridFor((long long)_dBcC.nSets, 128), 128, 0, _st, _dBcC.Sets(rhsVec), x);
 }
 
 //  The nozzle at the middle of the step (SourceBase::SetEvalTime in
@@ -1571,12 +1577,13 @@ void Step::System(const double *hOld, const double *h, double dt, double *ia, do
 //  Apply for the concentration (EqualVal [diag, partner] on Symmetry and
 //  Periodic edges, as for the film), interior rows the diagonal and the wide
 //  set in WideIdx order.
-void BuildConcPattern2D(const yz_step_params &p, std::vector<int> &rowptr, std::vector<int> &col)
+void BuildConcPattern2D(const yz_step_params &p, std::vector<int> &rowptr, std::vector<int> &col, const BcPlan &plan)
 {
 	const int nx = p.nx, ny = p.ny, n = nx * ny;
 	rowptr.assign((size_t)n + 1, 0);
 	col.clear();
 	static const int wide[8][2] = {{0, -2}, {0, -1}, {-2, 0}, {-1, 0}, {1, 0}, {2, 0}, {0, 1}, {0, 2}};
+	size_t g = 0;
 	for(int iy = 0; iy < ny; ++iy)
 		for(int ix = 0; ix < nx; ++ix)
 		{
@@ -1587,18 +1594,20 @@ void BuildConcPattern2D(const yz_step_params &p, std::vector<int> &rowptr, std::
 				for(int q = 0; q < 8; ++q) col.push_back((iy + wide[q][1]) * nx + ix + wide[q][0]);
 			else
 			{
-				const int px = PartnerOf(ix, nx, p.bc[0], p.bc[1]);
-				const int py = PartnerOf(iy, ny, p.bc[2], p.bc[3]);
-				col.push_back(py * nx + px);
+				//  the ghost row as BoundaryCondition2D::Apply writes the
+				//  concentration's (its diagonal is the one pushed above)
+				const std::vector<int> &c = plan.cols[g++];
+				col.insert(col.end(), c.begin() + 1, c.end());
 			}
 			rowptr[(size_t)i + 1] = (int)col.size();
 		}
 }
 
-void Step::BuildConc()
+void Step::BuildConc(const double *cHost)
 {
 	const size_t n = (size_t)_n;
-	BuildConcPattern2D(_p, _rowptrC, _colC);
+	_bcC = BuildBcPlan(_p, kBcFieldConc, cHost);
+	BuildConcPattern2D(_p, _rowptrC, _colC, _bcC);
 	_nnzC = (int)_colC.size();
 	std::vector<int> scol((size_t)_nnzC), ssrc((size_t)_nnzC);
 	std::vector<std::pair<int, int>> tmp;
@@ -1618,7 +1627,8 @@ void Step::BuildConc()
 	_dRowptrC.upload(_rowptrC.data(), _rowptrC.size(), _st);
 	std::vector<int> pall(n);
 	for(int i = 0; i < _n; ++i) pall[(size_t)i] = i;
-	for(size_t g = 0; g < _ghost.size(); ++g) pall[(size_t)_ghost[g]] = _partner[g];
+	for(size_t g = 0; g < _ghost.size(); ++g)
+		if(_partner[g] >= 0) pall[(size_t)_ghost[g]] = _partner[g];
 	_dPartnerAll.upload(pall.data(), n, _st);
 	for(DBuf<double> *v : {&_c0, &_cLim, &_cPrev, &_cx, &_cxLast, &_dC, &_rhsC, &_F0x, &_F0y, &_F1x, &_F1y, &_evpStep,
 	                       &_rho, &_room, &_give})
@@ -1636,15 +1646,21 @@ void Step::BuildConc()
 	_cntStep.reserve(4);
 	YZ_CUDA(cudaMemsetAsync(_cntStep.get(), 0, 4 * sizeof(unsigned int), _st));
 	_iflags.reserve(4);
-	//  the matrix: the boundary rows [1, -1] once, the interior rows every solve
+	//  the matrix: the boundary rows once (the concentration's, yz_bc.h),
+	//  the interior rows every solve
 	std::vector<double> vals((size_t)_nnzC, 0.0);
-	for(size_t g = 0; g < _ghost.size(); ++g)
+	for(size_t g = 0; g < _bcC.ghost.size(); ++g)
 	{
-		const int i = _ghost[g];
-		vals[(size_t)_rowptrC[(size_t)i]] = 1.0;
-		vals[(size_t)_rowptrC[(size_t)i] + 1] = -1.0;
+		const int i = _bcC.ghost[g];
+		for(size_t k = 0; k < _bcC.vals[g].size(); ++k) vals[(size_t)_rowptrC[(size_t)i] + k] = _bcC.vals[g][k];
 	}
 	_iaC.upload(vals.data(), vals.size(), _st);
+	//  the copy form of the ghosts reads the film's ghost and partner lists:
+	//  only where the two plans copy alike
+	_bcC.simple = _bcC.simple && _bc.simple && _bcC.ghost == _bc.ghost && _bcC.partner == _bc.partner;
+	_dBcC.Upload(_bcC, _st);
+	_dBcCRhs.upload(_bcC.rhs.data(), _bcC.rhs.size(), _st);
+	_dColC.upload(_colC.data(), _colC.size(), _st);
 	//  C_ImplicitSolver::SetX: c0 = c
 	YZ_CUDA(cudaMemcpyAsync(_c0.get(), _c.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
 }
@@ -1682,8 +1698,31 @@ void Step::ConcAssemble(double dt)
 	in.F0x = _F0x.get(); in.F0y = _F0y.get(); in.F1x = _F1x.get(); in.F1y = _F1y.get(); in.evp = _evpStep.get();
 	YZ_LAUNCH(KConcAssemble, GridFor(nIn, 128, 148 * 32), 128, 0, _st, _kc, dt, in, _dRowptrC.get(), _iaC.get(),
 	          _rhsC.get());
-	YZ_LAUNCH(KConcGhostRhs, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
-	          _dPartner.get(), _c0.get(), _rhsC.get());
+	if(_bcC.simple)
+		YZ_LAUNCH(KConcGhostRhs, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
+		          _dPartner.get(), _c0.get(), _rhsC.get());
+	else
+		YZ_LAUNCH(KBcRhs, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
+		          _dRowptrC.get(), _dColC.get(), _iaC.get(), _dBcCRhs.get(), _c0.get(), _rhsC.get());
+}
+
+//  after a converged concentration solve: the ghosts of d by the boundary
+//  rows with the d system's right-hand side, c1 = c0 + d, c1's ghosts by
+//  the rows with the equation's, then the pass's bookkeeping (KConcUpdate)
+void Step::ConcUpdate(int mode)
+{
+	const int n = _n, g = GridFor(n, 256);
+	if(_bcC.simple)
+	{
+		YZ_LAUNCH(KConcUpdate, g, 256, 0, _st, n, mode, 0, _dPartnerAll.get(), _c0.get(), _dC.get(), _rhsC.get(),
+		          _cx.get(), _cLim.get(), _cw.get(), _cPrev.get(), _red.get() + kSlotCorr);
+		return;
+	}
+	SatisfyConcGhosts(_dC.get(), _rhsC.get());
+	YZ_LAUNCH(KAddTo, g, 256, 0, _st, n, _c0.get(), _dC.get(), _cx.get());
+	SatisfyConcGhosts(_cx.get(), nullptr);
+	YZ_LAUNCH(KConcUpdate, g, 256, 0, _st, n, mode, 1, _dPartnerAll.get(), _c0.get(), _dC.get(), _rhsC.get(), _cx.get(),
+	          _cLim.get(), _cw.get(), _cPrev.get(), _red.get() + kSlotCorr);
 }
 
 //  _bcg.Solve of the concentration (ConcEquationBase.h:371): d in/out
@@ -1715,8 +1754,7 @@ bool Step::ConcPass(double dt, yz_step_stats &stats)
 	const int ch = ConcSolve(stats);
 	if(ch != 0) return false;
 	ZeroMax(kSlotCorr);
-	YZ_LAUNCH(KConcUpdate, g, 256, 0, _st, n, 0, _dPartnerAll.get(), _c0.get(), _dC.get(), _rhsC.get(), _cx.get(),
-	          _cLim.get(), _cw.get(), _cPrev.get(), _red.get() + kSlotCorr);
+	ConcUpdate(0);
 	_coupled = ReadMax(kSlotCorr);
 	return true;
 }
@@ -1752,8 +1790,7 @@ void Step::ConcCommit(double dt, yz_step_stats &stats)
 		ConcAssemble(dt);
 		if(ConcSolve(stats) != 0) { solved = false; break; }
 		ZeroMax(kSlotCorr);
-		YZ_LAUNCH(KConcUpdate, g, 256, 0, _st, n, 1, _dPartnerAll.get(), _c0.get(), _dC.get(), _rhsC.get(), _cx.get(),
-		          _cLim.get(), _cw.get(), _cPrev.get(), _red.get() + kSlotCorr);
+		ConcUpdate(1);
 		if(!limited) break;
 		if(ReadMax(kSlotCorr) <= 1e-12) break;
 	}
@@ -1778,9 +1815,7 @@ void Step::Redistribute()
 	const bool over = (f & 1) != 0, under = (f & 2) != 0;
 	if(over) MoveExcess(false);
 	if(under) MoveExcess(true);
-	if(over || under)
-		YZ_LAUNCH(KGhostCopy, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
-		          _dPartner.get(), _cx.get());
+	if(over || under) SatisfyConcGhosts(_cx.get(), nullptr);
 	YZ_LAUNCH(KBoundRows, g, 256, 0, _st, n, under ? 1 : 0, _cx.get());
 }
 

@@ -17,6 +17,42 @@ void BuildPattern2D(const yz_step_params &p, std::vector<int> &rowptr, std::vect
                     BcPlan *plan = nullptr);
 void CheckParams(const yz_step_params &p);
 
+//  a SatisfyBCRows plan (yz_bc.h) on the device
+struct DevBcPlan
+{
+	int nSets = 0;
+	bool simple = true;
+	DBuf<int> m, rowOff, matOff, row, termOff, termCol, piv;
+	DBuf<double> rhs, termVal, fac, U;
+	void Upload(const BcPlan &P, cudaStream_t st)
+	{
+		nSets = (int)P.setM.size();
+		simple = P.simple;
+		if(simple) return;
+		m.upload(P.setM.data(), P.setM.size(), st);
+		rowOff.upload(P.setRowOff.data(), P.setRowOff.size(), st);
+		matOff.upload(P.setMatOff.data(), P.setMatOff.size(), st);
+		row.upload(P.row.data(), P.row.size(), st);
+		rhs.upload(P.rowRhs.data(), P.rowRhs.size(), st);
+		termOff.upload(P.termOff.data(), P.termOff.size(), st);
+		termCol.upload(P.termCol.data(), P.termCol.size(), st);
+		termVal.upload(P.termVal.data(), P.termVal.size(), st);
+		piv.upload(P.piv.data(), P.piv.size(), st);
+		fac.upload(P.fac.data(), P.fac.size(), st);
+		U.upload(P.U.data(), P.U.size(), st);
+	}
+	BcSets Sets(const double *rhsVec) const
+	{
+		BcSets S;
+		S.n = nSets;
+		S.m = m.get(); S.rowOff = rowOff.get(); S.matOff = matOff.get(); S.row = row.get();
+		S.termOff = termOff.get(); S.termCol = termCol.get(); S.piv = piv.get();
+		S.rhs = rhs.get(); S.termVal = termVal.get(); S.fac = fac.get(); S.U = U.get();
+		S.rhsVec = rhsVec;
+		return S;
+	}
+};
+
 class Step
 {
 public:
@@ -72,11 +108,15 @@ private:
 	void BuildCoef();
 	void FaceProps(const double *H, const double *C, bool J);
 	void SatisfyGhosts(double *x);
+	//  the concentration's ghost rows of x exactly, with the right-hand side
+	//  rhsVec (a vector over the rows) or the equation's own (null)
+	void SatisfyConcGhosts(double *x, const double *rhsVec);
+	void ConcUpdate(int mode);
 	void UpdateSource(double dt);
 	void Assemble(int mode, const double *hField, const double *cField, double dt);
 	bool NKLoop(int &iter, double &resid, yz_step_stats &stats);
 	//  the concentration equation
-	void BuildConc();
+	void BuildConc(const double *cHost);
 	int FaceFluxes(const double *H, const double *C, double *Fx, double *Fy, double dt, bool withEvap);
 	void ConcAssemble(double dt);
 	int ConcSolve(yz_step_stats &stats);
@@ -104,9 +144,14 @@ private:
 	BcPlan _bc;
 	DBuf<int> _dBcPos;
 	DBuf<double> _dBcVal, _dBcRhs;
-	int _nBcSets = 0, _nBcVal = 0;
-	DBuf<int> _dSetM, _dSetRowOff, _dSetMatOff, _dSetRow, _dTermOff, _dTermCol, _dPiv;
-	DBuf<double> _dSetRhs, _dTermVal, _dFac, _dU;
+	int _nBcVal = 0;
+	DevBcPlan _dBc;
+	//  the concentration equation's ghost rows (its own plan; b: their
+	//  right-hand side, from the start concentration)
+	BcPlan _bcC;
+	DevBcPlan _dBcC;
+	DBuf<double> _dBcCRhs;
+	DBuf<int> _dColC;
 	DBuf<double> _src;                       // the nozzle's supply of the step (Physics.Source)
 	//  fields: the committed film h (field), c, s; phi_old, phi_old2, phi_new,
 	//  phi_guess; A h at phi_old and at the guess; the system
