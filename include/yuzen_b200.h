@@ -267,10 +267,13 @@ typedef struct yz_step_params
 	 * length src_arm about (src_arm_x, src_arm_y) turning at src_omega from
 	 * src_angle0, its angular speed ramped up over src_ramp, held over
 	 * src_plateau and ramped down, from src_t0; evaluated at the middle of
-	 * each step.  Not with conc_field. */
+	 * each step.  With conc_field the supplied liquid arrives at src_conc
+	 * (src_supplied = 1, ConcType "supplied") or at the local c (0). */
 	int    on_source, src_subregions;
 	double src_radius, src_rate, src_tau, src_arm, src_arm_x, src_arm_y, src_omega, src_angle0, src_ramp,
 	       src_plateau, src_t0;
+	int    src_supplied;
+	double src_conc;
 } yz_step_params;
 
 typedef struct yz_step_stats

@@ -156,10 +156,10 @@ int main(int argc, char **argv)
 		put(D, ce._bcg._set.epsilon); put(D, ce._theta);
 		//  the nozzle (SourceBase)
 		const auto &src = he._Source;
-		put(I, src._numSubRegion);
+		put(I, src._numSubRegion); put(I, src._concSupplied ? 1 : 0);
 		put(D, src._Radius); put(D, src._flowRate); put(D, src._timeConstant); put(D, src._armLength);
 		put(D, src._armX); put(D, src._armY); put(D, src._rotationRate); put(D, src._startAngle);
-		put(D, src._slopeTime); put(D, src._mainTime); put(D, m->_timeStep.StartTime());
+		put(D, src._slopeTime); put(D, src._mainTime); put(D, m->_timeStep.StartTime()); put(D, src._Conc);
 	}
 
 	std::vector<double> h0, c0, s0;

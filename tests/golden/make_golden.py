@@ -243,6 +243,16 @@ STEP_CASES = {
         "Numerics.TimeStepControl.Enable": True, "Numerics.TimeStepControl.KeepSteps": 2,
         "Numerics.TimeStepControl.ChangeFactor": 0.75, "Numerics.InitialDt": 1e-4,
     }, 6, 3),
+    # the nozzle with the well-mixed concentration: the supplied liquid at
+    # the local concentration, and at the nozzle's (ConcType "supplied")
+    **{f"step_wm_nozzle_{kind}_40": ("allphys_2d_reg.toml", {
+        "Grid.Nx": 40, "Grid.Ny": 40,
+        "Physics.Source": {"Enable": True, "Radius": 0.1e-3, "InletRate": 2e-3, "Conc": 0.2, "ConcType": kind,
+                           "TimeConstant": 1e-4, "ArmLength": 0.25e-3, "ArmCenter": [0.0, 0.0],
+                           "RotationRate": 2000.0, "StartAngle": 0.3, "RampTime": 1e-4, "PlateauTime": 1e-3,
+                           "SubRegions": 6},
+        "Numerics.TimeStepControl.Enable": False, "Numerics.InitialDt": 1e-3,
+    }, 3, -1) for kind in ("local", "supplied")},
     # capillary + disjoining with the time-step control on
     "step_adaptive_40": ("allphys_2d_reg.toml", {
         **_NO_UPWIND, "Grid.Nx": 40, "Grid.Ny": 40,

@@ -15,7 +15,7 @@ INT_KEYS = (
     "conv_height", "conv_conc", "conc_conv", "conc_diff", "lin_c_precond", "lin_c_scaling", "lin_c_maxit",
     "lin_c_conc",
     # the nozzle (SourceBase)
-    "src_subregions",
+    "src_subregions", "src_supplied",
     # appended after the run
     "steps_done", "diverged",
 )
@@ -31,7 +31,7 @@ REAL_KEYS = (
     # the nozzle (SourceBase): radius, flow rate, time constant, arm length and
     # centre, rotation rate, start angle, ramp and plateau times, start time
     "src_radius", "src_rate", "src_tau", "src_arm", "src_arm_x", "src_arm_y", "src_omega", "src_angle0",
-    "src_ramp", "src_plateau", "src_t0",
+    "src_ramp", "src_plateau", "src_t0", "src_conc",
     # appended after the run
     "run_seconds", "t_end",
     # the energy budget (EnergyEval) of the start and the end film

@@ -45,14 +45,3 @@ def test_refused_edges(bc, why):
         p.bc[e] = bc[e]
     with pytest.raises(Exception):
         ys.pattern_2d(p)
-
-
-def test_concentration_takes_no_nozzle():
-    """The film takes the nozzle; the concentration equation with one (its
-    supplied solute) is not built, and is refused."""
-    d = stateio.load_npz(GOLDEN / "step_wm_allphys_48.npz")
-    p = ys.params_from_state(d)
-    p.on_source = 1
-    p.src_subregions = 2
-    with pytest.raises(Exception):
-        ys.pattern_2d(p)

@@ -151,6 +151,11 @@ __global__ void KFaceFlux(Coef k, const double *__restrict__ H, const double *__
 struct ConcIn
 {
 	const double *c0, *cLim, *h0, *h1, *cw, *F0x, *F0y, *F1x, *F1y, *evp;
+	//  the nozzle's supply of the step (null: none) and whether its liquid
+	//  arrives at srcConc (ConcType "supplied") or at the local c
+	const double *src;
+	int srcSupplied;
+	double srcConc;
 };
 
 __global__ void KConcAssemble(ConcCoef q, double dt, ConcIn in, const int *__restrict__ rowptr, double *__restrict__ val,
@@ -174,8 +179,12 @@ __global__ void KConcAssemble(ConcCoef q, double dt, ConcIn in, const int *__res
 		const double c0i = c0w[oo];
 		const double h1 = in.h1[i];
 		//  no supply and no sideways outflow in 2-D: theta dt (r1 - S) is 0
-		double diag = h1 + th * dt * (0.0 - 0.0);
+		//  the supply (ConcEquationBase.h:310-319): at the local c, theta d
+		//  of it is the new level's; at the nozzle's c, all of it is known
+		const double S = in.src ? in.src[i] : 0.0;
+		double diag = h1 + th * dt * (0.0 - (in.srcSupplied ? 0.0 : S));
 		double R = dt * in.evp[i] * c0i;
+		if(in.srcSupplied) R += dt * S * (in.srcConc - c0i);
 #pragma unroll
 		for(int d = 0; d < 4; ++d)
 		{
@@ -305,7 +314,7 @@ __global__ void KConcUpdate(int n, int mode, int useCx, const int *__restrict__ 
 __global__ void KRho(int nx, int ny, double theta, double dt, const double *__restrict__ hOld,
                      const double *__restrict__ h1, const double *__restrict__ F1x, const double *__restrict__ F1y,
                      const double *__restrict__ F0x, const double *__restrict__ F0y, const double *__restrict__ evp,
-                     double *__restrict__ rho, RedScratch rs, double *sumOut)
+                     const double *__restrict__ src, double *__restrict__ rho, RedScratch rs, double *sumOut)
 {
 	__shared__ double sh[kRT];
 	const int nIn = (nx - 4) * (ny - 4);
@@ -320,8 +329,9 @@ __global__ void KRho(int nx, int ny, double theta, double dt, const double *__re
 		div0 += F0x[i] - F0x[i - 1];
 		div1 += F1y[i] - F1y[i - nx];
 		div0 += F0y[i] - F0y[i - nx];
-		//  no sideways outflow (r = 0) and no supply in 2-D
-		const double r = (hOld[i] - h1[i]) / dt - (theta * (div1 + 0.0) + (1.0 - theta) * (div0 + 0.0) + (evp[i] - 0.0));
+		//  no sideways outflow in 2-D (r = 0); the nozzle's supply, if any
+		const double r = (hOld[i] - h1[i]) / dt -
+		                 (theta * (div1 + 0.0) + (1.0 - theta) * (div0 + 0.0) + (evp[i] - (src ? src[i] : 0.0)));
 		rho[i] = r;
 		a[0] = r;
 	}

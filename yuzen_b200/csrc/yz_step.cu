@@ -883,12 +883,7 @@ void CheckParams(const yz_step_params &p)
 	if(!p.on_laplace) throw UsageError("step: the capillary term (Physics.LaplacePressure) must be enabled");
 	if(p.conv_height < YZ_SCHEME_UPWIND1 || p.conv_height > YZ_SCHEME_VANLEER)
 		throw UsageError("step: unknown Numerics.Convection.Height scheme");
-	if(p.on_source)
-	{
-		if(p.conc_field != 0)
-			throw UsageError("step: the nozzle (Physics.Source) is built for the film without the concentration equation");
-		if(p.src_subregions < 1) throw UsageError("step: Physics.Source.SubRegions must be 1 or larger");
-	}
+	if(p.on_source && p.src_subregions < 1) throw UsageError("step: Physics.Source.SubRegions must be 1 or larger");
 	if(p.conc_field != 0)
 	{
 		if(p.conv_conc < YZ_SCHEME_UPWIND1 || p.conv_conc > YZ_SCHEME_VANLEER)
@@ -1696,6 +1691,9 @@ void Step::ConcAssemble(double dt)
 	ConcIn in;
 	in.c0 = _c0.get(); in.cLim = _cLim.get(); in.h0 = _hOld.get(); in.h1 = _guess.get(); in.cw = _cw.get();
 	in.F0x = _F0x.get(); in.F0y = _F0y.get(); in.F1x = _F1x.get(); in.F1y = _F1y.get(); in.evp = _evpStep.get();
+	in.src = _p.on_source ? _src.get() : nullptr;
+	in.srcSupplied = _p.src_supplied;
+	in.srcConc = _p.src_conc;
 	YZ_LAUNCH(KConcAssemble, GridFor(nIn, 128, 148 * 32), 128, 0, _st, _kc, dt, in, _dRowptrC.get(), _iaC.get(),
 	          _rhsC.get());
 	if(_bcC.simple)
@@ -1774,7 +1772,8 @@ void Step::ConcCommit(double dt, yz_step_stats &stats)
 		const int nIn = (nx - 4) * (ny - 4);
 		const double w = 1.0 / _p.theta;
 		YZ_LAUNCH(KRho, RedBlocks(nIn), kRT, 0, _st, nx, ny, _p.theta, dt, _hOld.get(), _guess.get(), _F1x.get(),
-		          _F1y.get(), _F0x.get(), _F0y.get(), _evpStep.get(), _rho.get(), StepRed(0), _sums.get());
+		          _F1y.get(), _F0x.get(), _F0y.get(), _evpStep.get(), _p.on_source ? _src.get() : nullptr, _rho.get(),
+		          StepRed(0), _sums.get());
 		YZ_LAUNCH(KRowPass, GridFor(ny - 4, 64), 64, 0, _st, nx, ny, w, _rho.get(), _sums.get(), _rowSum.get(),
 		          _F1x.get());
 		YZ_LAUNCH(KAccY, 1, 32, 0, _st, nx, ny, _rowSum.get(), _accY.get());
@@ -1870,6 +1869,7 @@ void Step::ConcSystem(const double *h, const double *c, double dt, double *val, 
 	YZ_CUDA(cudaMemcpyAsync(_c0.get(), c, bytes, cudaMemcpyHostToDevice, _st));
 	YZ_CUDA(cudaMemcpyAsync(_cw.get(), c, bytes, cudaMemcpyHostToDevice, _st));
 	YZ_CUDA(cudaMemcpyAsync(_cLim.get(), c, bytes, cudaMemcpyHostToDevice, _st));
+	if(_p.on_source) UpdateSource(dt);
 	//  evapOld at h (mode 0 of the assembly), then the pass's fluxes and sources
 	Assemble(0, _hOld.get(), _cw.get(), dt);
 	FaceFluxes(_hOld.get(), _cw.get(), _F0x.get(), _F0y.get(), dt, false);

@@ -132,6 +132,7 @@ void FillParams(Model2D *m, yz_step_params &p)
 	p.src_arm = src._armLength; p.src_arm_x = src._armX; p.src_arm_y = src._armY;
 	p.src_omega = src._rotationRate; p.src_angle0 = src._startAngle;
 	p.src_ramp = src._slopeTime; p.src_plateau = src._mainTime; p.src_t0 = m->_timeStep.StartTime();
+	p.src_supplied = src._concSupplied ? 1 : 0; p.src_conc = src._Conc;
 }
 
 //  the model's fields in the device's row order IL(ix, iy) = iy nx + ix

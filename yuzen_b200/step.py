@@ -50,6 +50,7 @@ class StepParams(ctypes.Structure):
         ("src_arm", ctypes.c_double), ("src_arm_x", ctypes.c_double), ("src_arm_y", ctypes.c_double),
         ("src_omega", ctypes.c_double), ("src_angle0", ctypes.c_double), ("src_ramp", ctypes.c_double),
         ("src_plateau", ctypes.c_double), ("src_t0", ctypes.c_double),
+        ("src_supplied", ctypes.c_int), ("src_conc", ctypes.c_double),
     ]
 
 
@@ -110,6 +111,8 @@ def params_from_state(d: dict) -> StepParams:
     p.src_subregions = int(d.get("src_subregions", 1))
     for k in ("radius", "rate", "tau", "arm", "arm_x", "arm_y", "omega", "angle0", "ramp", "plateau", "t0"):
         setattr(p, "src_" + k, float(d.get("src_" + k, 0.0)))
+    p.src_supplied = int(d.get("src_supplied", 0))
+    p.src_conc = float(d.get("src_conc", 0.0))
     return p
 
 
