@@ -308,6 +308,89 @@ __global__ void KConcUpdate(int n, int mode, int useCx, const int *__restrict__ 
 }
 
 //--------------------------------------------------------------------------
+//  Reconstruct (ConcEquationBase.h:428-518): after a committed solve with the
+//  advection, c1 of every real cell with liquid is formed once more from the
+//  theta-weighted solute fluxes of its faces (SoluteFlux: the volume flux
+//  times the scheme's face value of c1 and of c0, less the diffusive flux),
+//  so that the sum of h c changes by the edge fluxes and the sources alone,
+//  to rounding, whatever the solve's tolerance.
+//--------------------------------------------------------------------------
+//  the solute flux through face d of the real cell i (c1 the solve's answer
+//  with its ghosts, K1 at the working field's h and c)
+__device__ __forceinline__ double SoluteFluxC(const ConcCoef &q, const ConcIn &in, const double *__restrict__ c1, int i,
+                                              int d)
+{
+	const int nx = q.nx;
+	const int a = d / 2;
+	const bool high = (d % 2 == 1);
+	const int ia = i + OffsetOf(AdjIdx(d), nx);
+	const int lo = high ? i : ia, hi = high ? ia : i;
+	const double F1 = (a == 0) ? in.F1x[lo] : in.F1y[lo];
+	const double F0 = (a == 0) ? in.F0x[lo] : in.F0y[lo];
+	double f1[4], f0[4];
+#pragma unroll
+	for(int qq = 0; qq < 4; ++qq)
+	{
+		const int j = i + OffsetOf(FS(d, qq), nx);
+		f1[qq] = c1[j];
+		f0[qq] = in.c0[j];
+	}
+	double G1 = F1 * FaceValue(q.cI, f1, F1);
+	double G0 = F0 * FaceValue(q.cI, f0, F0);
+	if(q.diff)
+	{
+		const double dn = (a == 0) ? q.dxx : q.dyy;
+		const double K1 = KFace(q, in.h1[lo], in.h1[hi], in.cw[lo], in.cw[hi], dn);
+		const double K0 = KFace(q, in.h0[lo], in.h0[hi], in.c0[lo], in.c0[hi], dn);
+		G1 -= K1 * (c1[hi] - c1[lo]);
+		G0 -= K0 * (in.c0[hi] - in.c0[lo]);
+	}
+	return q.th * G1 + (1.0 - q.th) * G0;
+}
+
+//  every face once: the high faces of the real cells, and the low face of a
+//  real cell whose neighbour there is a ghost (indexed by the face's low cell)
+__global__ void KSoluteFaces(ConcCoef q, ConcIn in, const double *__restrict__ c1, double *__restrict__ G2x,
+                             double *__restrict__ G2y)
+{
+	const int nx = q.nx, ny = q.ny;
+	const int nIn = (nx - 4) * (ny - 4);
+	for(int t = blockIdx.x * blockDim.x + threadIdx.x; t < nIn; t += gridDim.x * blockDim.x)
+	{
+		const int ix = 2 + t % (nx - 4), iy = 2 + t / (nx - 4);
+		const int i = iy * nx + ix;
+		G2x[i] = SoluteFluxC(q, in, c1, i, 1);
+		G2y[i] = SoluteFluxC(q, in, c1, i, 3);
+		if(ix == 2) G2x[i - 1] = SoluteFluxC(q, in, c1, i, 0);
+		if(iy == 2) G2y[i - nx] = SoluteFluxC(q, in, c1, i, 2);
+	}
+}
+
+//  c1 of every real cell with liquid from the faces' fluxes (c1pre: the
+//  solve's answer, read; cx: written)
+__global__ void KReconstruct(ConcCoef q, double dt, ConcIn in, const double *__restrict__ c1pre,
+                             const double *__restrict__ G2x, const double *__restrict__ G2y, double *__restrict__ cx)
+{
+	const int nx = q.nx, ny = q.ny;
+	const int nIn = (nx - 4) * (ny - 4);
+	const double th = q.th;
+	for(int t = blockIdx.x * blockDim.x + threadIdx.x; t < nIn; t += gridDim.x * blockDim.x)
+	{
+		const int ix = 2 + t % (nx - 4), iy = 2 + t / (nx - 4);
+		const int i = iy * nx + ix;
+		const double h1 = in.h1[i], h0 = in.h0[i];
+		if(!(h1 > 0.0)) continue;
+		double div = 0;
+		div += G2x[i] - G2x[i - 1];
+		div += G2y[i] - G2y[i - nx];
+		const double c0 = in.c0[i];
+		double qq = h0 * c0 - dt * div;
+		if(in.src) qq += dt * in.src[i] * (in.srcSupplied ? in.srcConc : th * c1pre[i] + (1.0 - th) * c0);
+		cx[i] = qq / h1;
+	}
+}
+
+//--------------------------------------------------------------------------
 //  ConsistentFluxes (HeightEquationBase.h:985-1060)
 //--------------------------------------------------------------------------
 //  rho of every interior cell and their sum (the library's reduction tree)

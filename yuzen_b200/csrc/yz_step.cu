@@ -705,6 +705,18 @@ __global__ void KBcRhs(int nGhost, const int *__restrict__ ghost, const int *__r
 	}
 }
 
+//  the ghosts of the concentration's d where every ghost copies one cell
+//  (SatisfyBCRows of rows [1, -1] with the d system's right-hand side)
+__global__ void KGhostD(int nGhost, const int *__restrict__ ghost, const int *__restrict__ partner,
+                        const double *__restrict__ rhsD, double *__restrict__ d)
+{
+	for(int g = blockIdx.x * blockDim.x + threadIdx.x; g < nGhost; g += gridDim.x * blockDim.x)
+	{
+		const int i = ghost[g];
+		d[i] = (rhsD[i] - (-1.0 * d[partner[g]])) / 1.0;
+	}
+}
+
 //  y = a + d
 __global__ void KAddTo(int n, const double *__restrict__ a, const double *__restrict__ d, double *__restrict__ y)
 {
@@ -1626,7 +1638,7 @@ void Step::BuildConc(const double *cHost)
 		if(_partner[g] >= 0) pall[(size_t)_ghost[g]] = _partner[g];
 	_dPartnerAll.upload(pall.data(), n, _st);
 	for(DBuf<double> *v : {&_c0, &_cLim, &_cPrev, &_cx, &_cxLast, &_dC, &_rhsC, &_F0x, &_F0y, &_F1x, &_F1y, &_evpStep,
-	                       &_rho, &_room, &_give})
+	                       &_rho, &_room, &_give, &_cPre, &_G2x, &_G2y})
 	{
 		v->reserve(n);
 		YZ_CUDA(cudaMemsetAsync(v->get(), 0, n * sizeof(double), _st));
@@ -1685,15 +1697,20 @@ int Step::FaceFluxes(const double *H, const double *C, double *Fx, double *Fy, d
 	return h;
 }
 
-void Step::ConcAssemble(double dt)
+void Step::ConcInputs(ConcIn &in) const
 {
-	const int nIn = (_p.nx - 4) * (_p.ny - 4);
-	ConcIn in;
 	in.c0 = _c0.get(); in.cLim = _cLim.get(); in.h0 = _hOld.get(); in.h1 = _guess.get(); in.cw = _cw.get();
 	in.F0x = _F0x.get(); in.F0y = _F0y.get(); in.F1x = _F1x.get(); in.F1y = _F1y.get(); in.evp = _evpStep.get();
 	in.src = _p.on_source ? _src.get() : nullptr;
 	in.srcSupplied = _p.src_supplied;
 	in.srcConc = _p.src_conc;
+}
+
+void Step::ConcAssemble(double dt)
+{
+	const int nIn = (_p.nx - 4) * (_p.ny - 4);
+	ConcIn in;
+	ConcInputs(in);
 	YZ_LAUNCH(KConcAssemble, GridFor(nIn, 128, 148 * 32), 128, 0, _st, _kc, dt, in, _dRowptrC.get(), _iaC.get(),
 	          _rhsC.get());
 	if(_bcC.simple)
@@ -1705,11 +1722,32 @@ void Step::ConcAssemble(double dt)
 }
 
 //  after a converged concentration solve: the ghosts of d by the boundary
-//  rows with the d system's right-hand side, c1 = c0 + d, c1's ghosts by
-//  the rows with the equation's, then the pass's bookkeeping (KConcUpdate)
-void Step::ConcUpdate(int mode)
+//  rows with the d system's right-hand side, c1 = c0 + d, on a committed
+//  solve with the advection c1 formed once more from the face fluxes
+//  (Reconstruct), c1's ghosts by the rows with the equation's, then the
+//  pass's bookkeeping (KConcUpdate)
+void Step::ConcUpdate(int mode, double dt)
 {
 	const int n = _n, g = GridFor(n, 256);
+	if(mode == 1 && _kc.conv)
+	{
+		if(_bcC.simple)
+			YZ_LAUNCH(KGhostD, GridFor((long long)_ghost.size(), 256), 256, 0, _st, (int)_ghost.size(), _dGhost.get(),
+			          _dPartner.get(), _rhsC.get(), _dC.get());
+		else SatisfyConcGhosts(_dC.get(), _rhsC.get());
+		YZ_LAUNCH(KAddTo, g, 256, 0, _st, n, _c0.get(), _dC.get(), _cx.get());
+		YZ_CUDA(cudaMemcpyAsync(_cPre.get(), _cx.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
+		ConcIn in;
+		ConcInputs(in);
+		const int nIn = (_p.nx - 4) * (_p.ny - 4);
+		YZ_LAUNCH(KSoluteFaces, GridFor(nIn, 128), 128, 0, _st, _kc, in, _cPre.get(), _G2x.get(), _G2y.get());
+		YZ_LAUNCH(KReconstruct, GridFor(nIn, 256), 256, 0, _st, _kc, dt, in, _cPre.get(), _G2x.get(), _G2y.get(),
+		          _cx.get());
+		SatisfyConcGhosts(_cx.get(), nullptr);
+		YZ_LAUNCH(KConcUpdate, g, 256, 0, _st, n, mode, 1, _dPartnerAll.get(), _c0.get(), _dC.get(), _rhsC.get(),
+		          _cx.get(), _cLim.get(), _cw.get(), _cPrev.get(), _red.get() + kSlotCorr);
+		return;
+	}
 	if(_bcC.simple)
 	{
 		YZ_LAUNCH(KConcUpdate, g, 256, 0, _st, n, mode, 0, _dPartnerAll.get(), _c0.get(), _dC.get(), _rhsC.get(),
@@ -1752,7 +1790,7 @@ bool Step::ConcPass(double dt, yz_step_stats &stats)
 	const int ch = ConcSolve(stats);
 	if(ch != 0) return false;
 	ZeroMax(kSlotCorr);
-	ConcUpdate(0);
+	ConcUpdate(0, dt);
 	_coupled = ReadMax(kSlotCorr);
 	return true;
 }
@@ -1789,7 +1827,7 @@ void Step::ConcCommit(double dt, yz_step_stats &stats)
 		ConcAssemble(dt);
 		if(ConcSolve(stats) != 0) { solved = false; break; }
 		ZeroMax(kSlotCorr);
-		ConcUpdate(1);
+		ConcUpdate(1, dt);
 		if(!limited) break;
 		if(ReadMax(kSlotCorr) <= 1e-12) break;
 	}

@@ -11,6 +11,12 @@
 #include <vector>
 
 namespace yz {
+namespace phys {
+struct ConcIn;
+} // namespace phys
+} // namespace yz
+
+namespace yz {
 
 void BuildPattern2D(const yz_step_params &p, std::vector<int> &rowptr, std::vector<int> &col,
                     std::vector<int> &isbc, std::vector<int> &ghost, std::vector<int> &partner,
@@ -111,7 +117,8 @@ private:
 	//  the concentration's ghost rows of x exactly, with the right-hand side
 	//  rhsVec (a vector over the rows) or the equation's own (null)
 	void SatisfyConcGhosts(double *x, const double *rhsVec);
-	void ConcUpdate(int mode);
+	void ConcUpdate(int mode, double dt);
+	void ConcInputs(phys::ConcIn &in) const;
 	void UpdateSource(double dt);
 	void Assemble(int mode, const double *hField, const double *cField, double dt);
 	bool NKLoop(int &iter, double &resid, yz_step_stats &stats);
@@ -152,6 +159,7 @@ private:
 	DevBcPlan _dBcC;
 	DBuf<double> _dBcCRhs;
 	DBuf<int> _dColC;
+	DBuf<double> _cPre, _G2x, _G2y;          // Reconstruct: c1 as solved, the faces' solute fluxes
 	DBuf<double> _src;                       // the nozzle's supply of the step (Physics.Source)
 	//  fields: the committed film h (field), c, s; phi_old, phi_old2, phi_new,
 	//  phi_guess; A h at phi_old and at the guess; the system
