@@ -207,8 +207,8 @@ typedef struct yz_step yz_step;
  * film takes every kind (ghost rows as BoundaryCondition2D::Apply writes
  * them, BoundaryCondition.cpp:104-187, 376-517; a Pinning corner next to a
  * FreshInlet or an Outlet edge, and two Pinning edges meeting, are refused
- * as the reference refuses or leaves them); the concentration equation
- * (conc_field) takes Symmetry and Periodic edges. */
+ * as the reference refuses or leaves them), for the film and for the
+ * concentration equation (conc_field) alike. */
 enum { YZ_BC_SYMMETRY = 0, YZ_BC_PERIODIC = 1, YZ_BC_PINNING = 2, YZ_BC_FRESHINLET = 3, YZ_BC_OUTLET = 4 };
 
 /* C_Interpolation_base4::t_Scheme (FiniteDifferences.h:42-53), the face
