@@ -322,15 +322,17 @@ int yz_step_set_amg_reuse(yz_step* st, int max_solves);
 /* The graph form of the step's BiCGStab loops (yz_solver_set_graph_loop). */
 int yz_step_set_graph_loop(yz_step* st, int on);
 
-/* Launch shapes of the FP32 V-cycle's coarse levels, for one context (both
- * of a step's solvers): fuse_from the first level whose way down and way up
- * run as one launch each (-1: the library's default, level 2 or
- * YZ_FUSE_FROM; 0: none), coarse_lanes the lanes a row of the coarse
- * levels' kernels (0: by the level's mean row length; 1, 2, 4 or 8).  The
- * preconditioner is the same up to float rounding; the FP64 cycle is not
+/* The FP32 V-cycle's shape, for one context (both of a step's solvers):
+ * fuse_from the first level whose way down and way up run as one launch
+ * each (-1: the library's default, level 2 or YZ_FUSE_FROM; 0: none),
+ * coarse_lanes the lanes a row of the coarse levels' kernels (0: by the
+ * level's mean row length; 1, 2, 4 or 8), fine_sweeps the post-smoothing
+ * sweeps at the finest level (0: the default, 5 or YZ_FINE_SWEEPS; 1 to 8).
+ * The launch shapes change the preconditioner by float rounding only, the
+ * sweeps change it (a better one); the FP64 cycle, the reference's, is not
  * affected.  yuzen_b200.autotune picks them per instance size. */
-int yz_solver_set_tuning(yz_solver* s, int fuse_from, int coarse_lanes);
-int yz_step_set_tuning(yz_step* st, int fuse_from, int coarse_lanes);
+int yz_solver_set_tuning(yz_solver* s, int fuse_from, int coarse_lanes, int fine_sweeps);
+int yz_step_set_tuning(yz_step* st, int fuse_from, int coarse_lanes, int fine_sweeps);
 /* The energy budget of the film the step holds (WellMixed_ModelBase::EnergyEval,
  * WellMixedModelBase.h:883-893, after EnergyBudget.h): the free energy F and
  * the flux power D (HeightEquationBase::FluxPower), both times the cell

@@ -44,10 +44,11 @@ def test_autotune_classes_and_summary():
     assert all(batch[k].Nx == s[0] for s, k in cls.items())
     assert all(min(j for j, c in enumerate(batch) if (c.Nx, c.Ny) == s) == k for s, k in cls.items())
     assert autotune.tune(batch, PREC_FP64) == {}          # nothing to tune on the FP64 cycle
-    t = {(64, 64): {"fuse_from": 2, "coarse_lanes": 4, "ms_per_step": 1.0, "default_ms_per_step": 1.5,
-                    "trials": {"-1,0": 1.5, "2,4": 1.0}}}
-    assert autotune.summary(t) == {"64x64": {"fuse_from": 2, "coarse_lanes": 4, "ms_per_step": 1.0,
+    t = {(64, 64): {"fuse_from": 2, "coarse_lanes": 4, "fine_sweeps": 3, "ms_per_step": 1.0,
+                    "default_ms_per_step": 1.5, "trials": {"-1,0,0": 1.5, "2,4,3": 1.0}}}
+    assert autotune.summary(t) == {"64x64": {"fuse_from": 2, "coarse_lanes": 4, "fine_sweeps": 3, "ms_per_step": 1.0,
                                              "default_ms_per_step": 1.5}}
+    assert all(len(c) == 3 for c in autotune.CANDIDATES) and autotune.CANDIDATES[0] == (-1, 0, 0)
 
 
 @pytest.mark.parametrize("world", [1, 2, 3, 8])

@@ -262,20 +262,20 @@ int yz_step_set_graph_loop(yz_step *st, int on)
 	});
 }
 
-int yz_solver_set_tuning(yz_solver *s, int fuse_from, int coarse_lanes)
+int yz_solver_set_tuning(yz_solver *s, int fuse_from, int coarse_lanes, int fine_sweeps)
 {
 	return Guard([&] {
 		if(!s) throw yz::UsageError("yz_solver_set_tuning: null solver");
-		s->s->SetTuning(fuse_from, coarse_lanes);
+		s->s->SetTuning(fuse_from, coarse_lanes, fine_sweeps);
 		return 0;
 	});
 }
 
-int yz_step_set_tuning(yz_step *st, int fuse_from, int coarse_lanes)
+int yz_step_set_tuning(yz_step *st, int fuse_from, int coarse_lanes, int fine_sweeps)
 {
 	return Guard([&] {
 		if(!st) throw yz::UsageError("yz_step_set_tuning: null step");
-		st->s->SetTuning(fuse_from, coarse_lanes);
+		st->s->SetTuning(fuse_from, coarse_lanes, fine_sweeps);
 		return 0;
 	});
 }

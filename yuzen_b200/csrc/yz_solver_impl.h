@@ -77,7 +77,7 @@ public:
 	int Precision() const { return _precision; }
 	void SetAmgReuse(int maxSolves);
 	void SetGraphLoop(bool on) { _graphLoop = on; }
-	void SetTuning(int fuseFrom, int coarseLanes);
+	void SetTuning(int fuseFrom, int coarseLanes, int fineSweeps);
 	int Rebuilds() const { return _rebuilds; }
 	//  the learned preconditioner (not owned): mode 0 off, 1 collect (the
 	//  next `collectSolves` AMG solves feed the network's sample ring with up
@@ -114,6 +114,7 @@ private:
 	//  the first level whose way down and way up run fused (KDownFused,
 	//  KUpFused); past the deepest level: none
 	int FusedFrom() const;
+	int FineSweeps() const;
 	void CoarseDown(int lanes, int nc, const Level &L, const float *f, float *fc);
 	void CoarseUp(int lanes, const Level &L, const float *f, const float *xc, float *x);
 	const int *Halt() const { return &_sc.get()->state; }
@@ -192,7 +193,7 @@ private:
 	//  launch shapes of the FP32 cycle's coarse levels (SetTuning): the first
 	//  fused level (-1: YZ_FUSE_FROM or 2; 0: none) and the lanes a row (0:
 	//  by the level's mean row length)
-	int _fuseFrom = -1, _coarseLanes = 0;
+	int _fuseFrom = -1, _coarseLanes = 0, _fineSweeps = 0;
 	LoopGraph _loop[3];
 	bool _graphLoop = true;       // the loop as a CUDA graph (else from the stream)
 	//  Solve's tail, queued behind a graph run: x into the caller's dX

@@ -90,10 +90,10 @@ public:
 		if(_solverC) _solverC->SetGraphLoop(on);
 		_graphLoop = on;
 	}
-	void SetTuning(int fuseFrom, int coarseLanes)
+	void SetTuning(int fuseFrom, int coarseLanes, int fineSweeps)
 	{
-		_solver->SetTuning(fuseFrom, coarseLanes);
-		if(_solverC) _solverC->SetTuning(fuseFrom, coarseLanes);
+		_solver->SetTuning(fuseFrom, coarseLanes, fineSweeps);
+		if(_solverC) _solverC->SetTuning(fuseFrom, coarseLanes, fineSweeps);
 	}
 	void SetAmgReuse(int maxSolves)
 	{

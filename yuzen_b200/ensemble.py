@@ -71,7 +71,7 @@ class Ensemble:
             #  the launch shapes the autotuner chose for the instance's size
             t = (tuning or {}).get((c.Nx, c.Ny))
             if t is not None:
-                st.set_tuning(t["fuse_from"], t["coarse_lanes"])
+                st.set_tuning(t["fuse_from"], t["coarse_lanes"], t.get("fine_sweeps", 0))
             self.steps.append(st)
         self.workers = workers or min(len(self.steps), max(1, 2 * (os.cpu_count() or 1)))
         self._pool = concurrent.futures.ThreadPoolExecutor(max_workers=self.workers) if self.steps else None

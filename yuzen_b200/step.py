@@ -131,7 +131,7 @@ def _bind():
     L.yz_step_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_step_set_amg_reuse.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_step_set_graph_loop.argtypes = [ctypes.c_void_p, ctypes.c_int]
-    L.yz_step_set_tuning.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    L.yz_step_set_tuning.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.yz_step_energy.argtypes = [ctypes.c_void_p, _f64p, _f64p]
     L.yz_step_set_energy.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_step_get_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
@@ -178,11 +178,12 @@ class Step:
         from the stream (yz_step_set_graph_loop)."""
         _check(lib().yz_step_set_graph_loop(self._h, int(bool(on))), "yz_step_set_graph_loop")
 
-    def set_tuning(self, fuse_from: int = -1, coarse_lanes: int = 0) -> None:
-        """Launch shapes of the FP32 V-cycle's coarse levels (yz_step_set_tuning):
-        the first fused level (-1 default, 0 none) and the lanes a row (0: by
-        row length)."""
-        _check(lib().yz_step_set_tuning(self._h, int(fuse_from), int(coarse_lanes)), "yz_step_set_tuning")
+    def set_tuning(self, fuse_from: int = -1, coarse_lanes: int = 0, fine_sweeps: int = 0) -> None:
+        """The FP32 V-cycle's shape (yz_step_set_tuning): the first fused level
+        (-1 default, 0 none), the coarse levels' lanes a row (0: by row
+        length) and the finest level's post-smoothing sweeps (0: default)."""
+        _check(lib().yz_step_set_tuning(self._h, int(fuse_from), int(coarse_lanes), int(fine_sweeps)),
+               "yz_step_set_tuning")
 
     def set_learned(self, cfg=None) -> None:
         """The learned preconditioner of the film's solves
