@@ -400,3 +400,24 @@ def test_fused_coarse_levels_match_the_separate_kernels(precision):
     assert abs(a["it"] - b["it"]) <= max(3, b["it"] // 10), (a, b)
     assert a["true"] <= 4.0 * max(b["true"], 1e-300) + 1e-14, (a, b)
     assert abs(a["x"] - b["x"]) <= 1e-6 * b["x"], (a, b)
+
+
+def test_tuning_shapes_and_sweeps():
+    """yz_solver_set_tuning: out-of-range shapes are usage errors; every shape
+    solves the 384^2 film to the tolerance in the FP32 cycle, and the finest
+    level's five default sweeps take fewer iterations than the reference's
+    one."""
+    d = _systems.film_system(384, seed=11)
+    be = yz.B200Backend()
+    for bad in ((-2, 0, 0), (2, 3, 0), (2, 0, 9)):
+        with pytest.raises(yz.YzError):
+            be.SetTuning(*bad)
+    its = {}
+    for shape in ((-1, 0, 1), (-1, 0, 0), (0, 8, 0), (1, 4, 3)):
+        be = yz.B200Backend()
+        be.SetPrecision(yz.PREC_FP32_CYCLE)
+        be.SetTuning(*shape)
+        g = gpu_solve(d, backend=be)
+        assert g[0] == 0 and g[2] <= float(d["epsilon"]), (shape, g[:3])
+        its[shape] = g[1]
+    assert its[(-1, 0, 0)] < its[(-1, 0, 1)], its

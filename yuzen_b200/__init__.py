@@ -103,6 +103,7 @@ def lib():
     L.yz_solver_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_solver_set_amg_reuse.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_solver_set_graph_loop.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.yz_solver_set_tuning.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.yz_solver_memory.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_int]
     L.yz_solver_set_memory.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_int]
     L.yz_solver_levels.argtypes = [ctypes.c_void_p]
@@ -246,6 +247,13 @@ class B200Backend:
         """The BiCGStab loop as one CUDA graph launch (default) or from the
         stream (yz_solver_set_graph_loop)."""
         _check(lib().yz_solver_set_graph_loop(self._h, int(bool(on))), "yz_solver_set_graph_loop")
+
+    def SetTuning(self, fuse_from: int = -1, coarse_lanes: int = 0, fine_sweeps: int = 0) -> None:
+        """The FP32 V-cycle's shape (yz_solver_set_tuning): the first fused
+        coarse level (-1 default, 0 none), the coarse levels' lanes a row (0:
+        by row length), the finest level's post-smoothing sweeps (0: default)."""
+        _check(lib().yz_solver_set_tuning(self._h, int(fuse_from), int(coarse_lanes), int(fine_sweeps)),
+               "yz_solver_set_tuning")
 
     def Memory(self) -> list:
         buf = np.zeros(8, dtype=np.float64)
