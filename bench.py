@@ -83,7 +83,7 @@ PATHS = {
     "learned": "the learned preconditioner: a U-Net (BF16 tcgen05 convolutions, FP32 accumulation) trained on the "
                "device during the warm-up steps on the (residual, V-cycle) pairs of the first film solves, tried "
                "first in a flexible BiCGStab on every film solve, SA-AMG (the fp32m_reuse form) as its fallback "
-               "and judge",
+               "and yardstick",
 }
 DTYPES = {"fp64": "f64", "fp32_cycle": "f64 (V-cycle f32)", "fp32_reuse": "f64 (V-cycle f32)",
           "fp32m_reuse": "f64 Newton / f32 matrix and V-cycle in an f64 Krylov",

@@ -400,7 +400,7 @@ int yz_pattern_2d(const yz_step_params* p, int* rowptr, int* col, int* bc);
  * (r, V r) pairs the solver collects from its own AMG-preconditioned solves,
  * and used in a flexible BiCGStab (the right-preconditioned iteration with a
  * preconditioner that may change between applications).  SA-AMG stays the
- * judge and the fallback: a learned solve that needs more than cap_factor
+ * yardstick and the fallback: a learned solve that needs more than cap_factor
  * times the iterations of the last SA-AMG solve is repeated on the AMG path,
  * and the network then sits out a growing number of solves.
  * ---------------------------------------------------------------------

@@ -177,7 +177,7 @@ def _solve(backend, d, rhs, s):
 def test_learned_preconditioner_in_the_solver():
     """The network trained on the (residual, V-cycle) pairs the solver
     collects from its own SA-AMG solves of twelve film systems.  SA-AMG is
-    the judge: on the held-out pairs the trained network's error against the
+    the yardstick: on the held-out pairs the trained network's error against the
     V-cycle is well below the untrained network's (the same weights before
     training, on the same pairs) -- what the training gains.  As the
     preconditioner of a flexible BiCGStab on held-out systems every solve

@@ -75,7 +75,7 @@ public:
 	//  Adam on the samples held (the last `holdout` of them kept out):
 	//  iters steps of `batch` samples each; returns the mean loss of the last
 	//  step and, in *valErr, the relative error ||N(r) - M r|| / ||M r|| over
-	//  the held-out samples (the AMG as the judge of the network)
+	//  the held-out samples (the AMG as the yardstick of the network)
 	double Train(int iters, int batch, float lr, int holdout, double *valErr, cudaStream_t st);
 	//  relative error over held-out samples [first, first + count)
 	double Validate(int first, int count, cudaStream_t st);
