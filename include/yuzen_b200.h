@@ -482,6 +482,94 @@ int yz_step_set_learned(yz_step* st, const yz_learned_cfg* cfg);
 int yz_conv3x3(int H, int W, int cin, int n, int real_w, int real_h, int relu, const float* x,
                const float* w, const float* bias, float* y);
 
+/* ---------------------------------------------------------------------
+ * Seam 3: the time step of the ConcZ model (a 2-D film with its
+ * concentration resolved through the thickness on a zeta grid).  Replaces
+ * _heightEq.TimeAdvance in ConcZ_Model_2D::Run (ConcZ_Model_2D.cpp:782):
+ * CZ_HeightEquation_2D::TimeAdvance (CZ_HeightEquation_2D.cpp:1965-1974)
+ * over C_SemiImplicitEquation::TimeAdvance / TimeStepTrial
+ * (SemiImplicit.cpp:100-150) -- the semi-implicit film in two stages
+ * (Solve, SolveStage: :1949-2020), its conservative update, the velocity
+ * through the film (CalVelocity), the concentration equation on the moving
+ * zeta grid (CZ_ConcEquation_2D.cpp) advanced by the same step, the
+ * Aitken-relaxed coupling passes of the Marangoni film
+ * (AfterTimeStepTrial, :207-386), RedistributeExcess / Deficit and the
+ * LTE time-step control -- all on the device, both linear solves on this
+ * library's SA-AMG BiCGStab.
+ * ------------------------------------------------------------------- */
+typedef struct yz_cz yz_cz;
+
+typedef struct yz_cz_params
+{
+	int    nx, ny, nz;            /* grid sizes with the two ghost layers at each end (ny > 1) */
+	int    bc[4];                 /* Xmin, Xmax, Ymin, Ymax: 0 Symmetry or 1 Periodic, in pairs (the
+	                                 kinds the reference's CZ model implements:
+	                                 CheckParameters.cpp:340-353 refuses the rest) */
+	int    on_lap, on_sc, on_vg, on_hg, on_cf, on_evap;   /* Physics.* switches */
+	int    ev_conc, ev_spatial, ev_hast;                 /* Raoult 0 / PowerN 1; uniform 0 / negPow 1; h* cap */
+	int    dt_control, dt_keep_steps;                    /* Numerics.TimeStepControl */
+	int    c_scheme;              /* Numerics.Convection.Concentration, YZ_SCHEME_* */
+	yz_settings h_lin, c_lin;     /* the film's and the concentration's linear solver */
+	double dx, dy, dzeta;         /* non-dimensional spacings; dzeta = 1 / (nz - 4) */
+	double theta_h, theta_c;      /* Crank-Nicolson weights (0.5) */
+	double dt, dt_old, dt_max, dt_min, time;
+	double dt_change_factor, dt_criterion, dt_scale_floor;
+	double As, Ma, Bo, Pgx, Pgy, Sp, Df, Ev;             /* non-dimensional numbers */
+	double rot_center[2];
+	double visc_c0, visc_base, visc_exp;  /* base * exp(exp (c - c0)), non-dimensional */
+	double sig_c0, sig_base, sig_coef;    /* base + coef (c - c0) */
+	double diff_c0, diff_base, diff_exp;
+	double ev_mr, ev_ms, ev_pown, ev_concr, ev_negexp, ev_negrmax, ev_hast_h, ev_dr;
+	double coupling_floor;        /* max(1e-10, 10 c_lin.epsilon) */
+} yz_cz_params;
+
+typedef struct yz_cz_stats
+{
+	int    steps;                 /* steps taken by this call */
+	int    linear_iterations;     /* the film's BiCGStab iterations of the accepted trials (the
+	                                 reference's BCGIterTotal) */
+	int    conc_iterations;       /* the concentration's BiCGStab iterations, every solve */
+	int    coupling_passes;       /* CouplingPasses() summed (CouplingPassTotal) */
+	int    retries;               /* trials cut and repeated (dt control) */
+	int    solves;                /* linear solves of either equation */
+	double time, dt;              /* the clock and DT().now after the call */
+	double device_ms;             /* the call on the model's stream (CUDA events) */
+	long long launches;           /* kernels the call launched */
+} yz_cz_stats;
+
+/* Build the model: the coordinates of the cell centres (xc, yc) and of the
+ * faces below them (xf: the face between ix-1 and ix, yf likewise), and the
+ * film h, substrate s (nx*ny, row jy*nx + ix) and concentration c (nx*ny*nz,
+ * kz*nx*ny + jy*nx + ix) with their ghosts, as the reference's Build leaves
+ * them; host arrays. */
+int yz_cz_create(int device, const yz_cz_params* p, const double* xc, const double* xf, const double* yc,
+                 const double* yf, const double* h, const double* s, const double* c, yz_cz** out);
+int yz_cz_destroy(yz_cz* z);
+/* nsteps time steps (TimeAdvance, then the clock's ++). */
+int yz_cz_advance(yz_cz* z, int nsteps, yz_cz_stats* stats);
+/* The film (nx*ny) and the concentration (nx*ny*nz) the model holds. */
+int yz_cz_get_fields(yz_cz* z, double* h, double* c);
+/* Preconditioner arithmetic (YZ_PREC_*) and AMG hierarchy reuse of both
+ * equations' solves, from the next solve on (FP64, no reuse: the reference's). */
+int yz_cz_set_precision(yz_cz* z, int precision);
+int yz_cz_set_amg_reuse(yz_cz* z, int max_solves);
+/* The pieces of one step on the present state, as the reference forms them
+ * (its parity test): the film's assembly at the step's dt, its conservative
+ * update with the film unchanged, the velocity and the concentration's
+ * assembly with those fluxes.  Afterwards yz_cz_read copies a named array
+ * ("h_A", "h_B", "h_colsrc", "h_qcapx", "h_qexpx", "h_qcapy", "h_qexpy",
+ * "h_IA", "h_qx", "h_qy", "h_end", "h_dtdh", "ux", "uy", "c_A", "c_B",
+ * "c_rhs", "c_react", "c_qx", "c_qy", "c_w") of up to cap values and
+ * returns its length.  The model's state is not changed by the pieces. */
+int yz_cz_parts(yz_cz* z);
+long long yz_cz_read(yz_cz* z, const char* name, double* out, long long cap);
+/* The patterns of the film's and the concentration's matrices in storage
+ * order (the diagonal first), with the ghost-row flags; rowptr of n+1. */
+int yz_cz_pattern(yz_cz* z, int which, int* rowptr, int* col, int* bc);
+/* The same from the parameters alone (no device): which 0 the film, 1 the
+ * concentration; returns the number of entries (arrays may be null to ask). */
+int yz_cz_build_pattern(const yz_cz_params* p, int which, int* rowptr, int* col, int* bc);
+
 #ifdef __cplusplus
 }
 #endif

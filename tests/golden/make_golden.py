@@ -303,6 +303,66 @@ REF_CASES = {
 }
 
 
+#  The ConcZ model (oracle/probe/yz_probe_cz): name: (reference case,
+#  overrides, whether the pieces of the first step are kept too).  Each runs
+#  the reference's time loop to Numerics.MaxSteps; EndTime is far.
+PROBE_CZ = REPO / "oracle" / "_ref" / "yz_probe_cz"
+CZ_PARTS = ("h_A", "h_B", "h_colsrc", "h_qcapx", "h_qexpx", "h_qcapy", "h_qexpy", "h_IA", "h_qx", "h_qy", "h_end",
+            "h_dtdh", "ux", "uy", "c_A", "c_B", "c_rhs", "c_react", "c_qx", "c_qy", "c_w")
+CZ_CASES = {
+    # the reference's 2-D case: capillary + Marangoni (the coupling passes)
+    # + evaporation, Symmetry walls, the LTE control cutting a long first step
+    "cz_sym_16": ("concz_2d.toml", {
+        "Grid.Nx": 16, "Grid.Ny": 16, "Grid.Nz": 8, "Numerics.MaxSteps": 6,
+        "Numerics.InitialDt": 1000.0, "Numerics.EndTime": 1e6,
+    }, True),
+    # periodic film, no Marangoni (the concentration's own two stages), both
+    # gravities, the limited Koren scheme (SettleLimiter) and the negPow
+    # evaporation
+    "cz_per_koren_16": ("concz_2d.toml", {
+        "Grid.Nx": 16, "Grid.Ny": 20, "Grid.Nz": 8, "Numerics.MaxSteps": 5,
+        "Numerics.InitialDt": 1.0, "Numerics.EndTime": 1e6,
+        "Boundary.XminBC.Type": "Periodic", "Boundary.XmaxBC.Type": "Periodic",
+        "Boundary.YminBC.Type": "Periodic", "Boundary.YmaxBC.Type": "Periodic",
+        "Physics.SolutoCapillarity.Enable": False, "Physics.VerticalGravity.Enable": True,
+        "Physics.HorizontalGravity.Enable": True, "Numerics.Convection.Concentration": "Koren",
+        "Physics.Evaporation.SpatialFunc": "negPow", "Physics.Evaporation.NegPowRmax": 0.8e-3,
+    }, True),
+    # the centrifugal term about an off-centre axis at a fixed step
+    "cz_spin_fixed_18": ("concz_2d.toml", {
+        "Grid.Nx": 18, "Grid.Ny": 16, "Grid.Nz": 9, "Numerics.MaxSteps": 4,
+        "Numerics.InitialDt": 0.2, "Numerics.EndTime": 1e6, "Numerics.TimeStepControl.Enable": False,
+        "Physics.Centrifugal.Enable": True, "Physics.Centrifugal.RotationAxis": [0.1e-3, -0.2e-3],
+    }, True),
+    # 64^2 x 16 levels: more than one AMG level in both solves
+    "cz_sym_64": ("concz_2d.toml", {
+        "Grid.Nx": 64, "Grid.Ny": 64, "Grid.Nz": 16, "Numerics.MaxSteps": 4,
+        "Numerics.InitialDt": 10.0, "Numerics.EndTime": 1e6,
+    }, False),
+}
+
+
+def make_cz_case(ref: Path, name: str, work: Path) -> dict:
+    src, over, parts = CZ_CASES[name]
+    case = write_case(ref, src, over, name, work)
+    env = dict(os.environ, OMP_NUM_THREADS="4")
+    res = subprocess.run([str(PROBE_CZ), case.name, f"{name}.bin"], cwd=work, env=env, capture_output=True, text=True,
+                         timeout=900)
+    if res.returncode != 0:
+        raise RuntimeError(f"{name}: probe failed\n{res.stdout[-2000:]}\n{res.stderr[-2000:]}")
+    d = stateio.read_records(work / f"{name}.bin")
+    if parts:
+        res = subprocess.run([str(PROBE_CZ), case.name, f"{name}_parts.bin", "parts"], cwd=work, env=env,
+                             capture_output=True, text=True, timeout=900)
+        if res.returncode != 0:
+            raise RuntimeError(f"{name}: probe (parts) failed\n{res.stdout[-2000:]}\n{res.stderr[-2000:]}")
+        p = stateio.read_records(work / f"{name}_parts.bin")
+        for k in CZ_PARTS:
+            d["parts_" + k] = p[k]
+    d["case"] = name
+    return d
+
+
 def make_ref_case(ref: Path, name: str, work: Path, threads: int) -> dict:
     src, builder, kw = REF_CASES[name]
     doc = tomllib.loads((ref / "cases" / src).read_text())
@@ -542,6 +602,12 @@ def main() -> None:
             d = make_big_step_case(name, Path(tmp), a.threads)
             stateio.save_npz(HERE / f"big_{name}.npz", d)
             print(name, d["nx"], d["ny"], "steps", d["steps_done"], "t_end", d["t_end"])
+        for name in CZ_CASES:
+            if a.only and name != a.only:
+                continue
+            d = make_cz_case(Path(a.ref), name, Path(tmp))
+            stateio.save_npz(HERE / f"{name}.npz", d)
+            print(name, d["nx"], d["ny"], d["nz"], "steps", d["steps_done"], "t_end", d["t_end"])
         for name in CASES:
             if a.only and name != a.only:
                 continue

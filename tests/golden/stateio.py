@@ -78,3 +78,26 @@ def save_npz(path, d: dict) -> None:
 def load_npz(path) -> dict:
     z = np.load(path)
     return {k: (z[k].item() if z[k].ndim == 0 else z[k]) for k in z.files}
+
+
+def read_records(path) -> dict:
+    """The named records oracle/probe/yz_probe_cz.cpp writes: magic
+    "YZCZREC1", then per record the name's length and bytes, its kind (0
+    int32, 1 float64), its count and its values.  Single values come back as
+    Python scalars, the rest as arrays."""
+    raw = Path(path).read_bytes()
+    assert raw[:8] == b"YZCZREC1", "not a record file"
+    out, o = {}, 8
+    while o < len(raw):
+        ln = int(np.frombuffer(raw, "<i4", 1, o)[0]); o += 4
+        name = raw[o:o + ln].decode(); o += ln
+        kind = int(np.frombuffer(raw, "<i4", 1, o)[0]); o += 4
+        cnt = int(np.frombuffer(raw, "<i8", 1, o)[0]); o += 8
+        dt, sz = ("<i4", 4) if kind == 0 else ("<f8", 8)
+        v = np.frombuffer(raw, dt, cnt, o).copy(); o += sz * cnt
+        out[name] = (int(v[0]) if kind == 0 else float(v[0])) if cnt == 1 and name not in ARRAY_RECORDS else v
+    return out
+
+
+#  records that stay arrays even when they hold one value
+ARRAY_RECORDS = {"rot_center", "bc", "h_lin", "c_lin", "visc", "sigma", "diff", "evap"}

@@ -1,0 +1,91 @@
+"""The ConcZ model's step on the device (yz_cz_*) against the reference's own
+runs of its CZ model (tests/golden/cz_*.npz, made by oracle/probe/yz_probe_cz
+through tests/golden/make_golden.py):
+
+  * the pieces of one step on the start state -- the film's matrix and
+    right-hand side, its face fluxes and conservative update, the velocity
+    through the film, the concentration's matrix, right-hand side and volume
+    fluxes -- each within 1e-12 of the reference's largest value of it;
+  * the whole run (MaxSteps steps with the reference's dt control, coupling
+    passes and both linear solves): the same steps and clock, the same
+    linear iteration and coupling pass counts, h and c within 1e-10
+    relative L2;
+  * the solute of the closed film conserved on the device as in the
+    reference, and two runs bit-identical."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import stateio
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+CASES = ["cz_sym_16", "cz_per_koren_16", "cz_spin_fixed_18", "cz_sym_64"]
+PARTS_CASES = ["cz_sym_16", "cz_per_koren_16", "cz_spin_fixed_18"]
+
+
+def load(name):
+    return stateio.load_npz(GOLD / f"{name}.npz")
+
+
+def model(d):
+    from yuzen_b200 import cz
+    p = cz.params_from_record(d)
+    return cz.CzModel(p, d["xc"], d["xf"], d["yc"], d["yf"], d["h0"], d["s"], d["c0"])
+
+
+@pytest.mark.parametrize("name", PARTS_CASES)
+def test_pieces_of_a_step_match_the_reference(name):
+    d = load(name)
+    m = model(d)
+    got = m.parts()
+    m.close()
+    bc = d["c_bc"].astype(bool)
+    bad = []
+    for k, v in got.items():
+        ref = d["parts_" + k]
+        if k == "c_rhs":
+            # only the ghost rows' right-hand sides are the step's
+            v, ref = v[bc], ref[bc]
+        assert v.shape == ref.shape, k
+        scale = max(np.abs(ref).max(), 1e-300)
+        err = np.abs(v - ref).max() / scale
+        if not err <= 1e-12:
+            bad.append((k, err))
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_whole_run_matches_the_reference(name):
+    d = load(name)
+    m = model(d)
+    st = m.advance(int(d["steps_done"]))
+    h, c = m.fields()
+    m.close()
+    assert st["steps"] == d["steps_done"]
+    assert abs(st["time"] - d["t_end"]) <= 1e-12 * abs(d["t_end"])
+    assert abs(st["dt"] - d["dt_end"]) <= 1e-12 * abs(d["dt_end"])
+    assert st["linear_iterations"] == d["linear_iterations"]
+    assert st["coupling_passes"] == d["coupling_passes"]
+    eh = np.linalg.norm(h - d["h1"]) / np.linalg.norm(d["h1"])
+    ec = np.linalg.norm(c - d["c1"]) / np.linalg.norm(d["c1"])
+    assert eh <= 1e-10 and ec <= 1e-10, (eh, ec)
+
+
+def test_solute_conserved_and_runs_repeat():
+    d = load("cz_sym_16")
+    out = []
+    for _ in range(2):
+        m = model(d)
+        m.advance(int(d["steps_done"]))
+        out.append(m.fields())
+        m.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    nx, ny, nz = d["nx"], d["ny"], d["nz"]
+
+    def solute(h, c):
+        return float((h.reshape(ny, nx)[2:-2, 2:-2] * c.reshape(nz, ny, nx)[2:-2, 2:-2, 2:-2].mean(axis=0)).sum())
+
+    s0, s1 = solute(d["h0"], d["c0"]), solute(*out[0])
+    assert abs(s1 - s0) <= 1e-11 * abs(s0)

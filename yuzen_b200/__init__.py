@@ -47,6 +47,9 @@ EXPORTED_SYMBOLS = (
     "yz_step_set_learned", "yz_conv3x3", "yz_fault_inject", "yz_step_state_size", "yz_step_get_state",
     "yz_step_set_state", "yz_profile_enabled", "yz_profile_entry", "yz_profile_reset", "yz_solver_set_tuning",
     "yz_step_set_tuning",
+    # the ConcZ model (seam 3)
+    "yz_cz_create", "yz_cz_destroy", "yz_cz_advance", "yz_cz_get_fields", "yz_cz_set_precision",
+    "yz_cz_set_amg_reuse", "yz_cz_parts", "yz_cz_read", "yz_cz_pattern", "yz_cz_build_pattern",
 )
 
 #: the preconditioner's arithmetic (YZ_PREC_* of include/yuzen_b200.h)

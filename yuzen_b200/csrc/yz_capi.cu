@@ -2,6 +2,7 @@
 // Every call catches what the C++ side throws and turns it into a status.
 #include "yz_solver_impl.h"
 #include "yz_step_impl.h"
+#include "yz_cz.h"
 #include "yz_prof.h"
 
 #include <cstring>
@@ -14,6 +15,11 @@ struct yz_solver
 struct yz_step
 {
 	std::unique_ptr<yz::Step> s;
+};
+
+struct yz_cz
+{
+	std::unique_ptr<yz::CzStep> z;
 };
 
 struct yz_unet
@@ -572,3 +578,108 @@ int yz_conv3x3(int H, int W, int cin, int n, int real_w, int real_h, int relu, c
 }
 
 } // extern "C"
+
+//--------------------------------------------------------------------------
+//  seam 3: the ConcZ model's step
+//--------------------------------------------------------------------------
+int yz_cz_create(int device, const yz_cz_params *p, const double *xc, const double *xf, const double *yc,
+                 const double *yf, const double *h, const double *s, const double *c, yz_cz **out)
+{
+	return Guard([&] {
+		if(!p || !xc || !xf || !yc || !yf || !h || !s || !c || !out) throw yz::UsageError("yz_cz_create: null argument");
+		yz::CheckCzParams(*p);
+		int count = 0;
+		yz::Check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+		if(device < 0 || device >= count) throw yz::UsageError("yz_cz_create: no such CUDA device");
+		yz_cz *z = new yz_cz();
+		try { z->z.reset(new yz::CzStep(device, *p, xc, xf, yc, yf, h, s, c)); }
+		catch(...) { delete z; throw; }
+		*out = z;
+		return 0;
+	});
+}
+
+int yz_cz_destroy(yz_cz *z)
+{
+	return Guard([&] { delete z; return 0; });
+}
+
+int yz_cz_advance(yz_cz *z, int nsteps, yz_cz_stats *stats)
+{
+	return Guard([&] {
+		if(!z || !stats) throw yz::UsageError("yz_cz_advance: null argument");
+		if(nsteps < 0) throw yz::UsageError("yz_cz_advance: nsteps must be >= 0");
+		z->z->Advance(nsteps, *stats);
+		return 0;
+	});
+}
+
+int yz_cz_get_fields(yz_cz *z, double *h, double *c)
+{
+	return Guard([&] {
+		if(!z) throw yz::UsageError("yz_cz_get_fields: null model");
+		z->z->GetFields(h, c);
+		return 0;
+	});
+}
+
+int yz_cz_set_precision(yz_cz *z, int precision)
+{
+	return Guard([&] {
+		if(!z) throw yz::UsageError("yz_cz_set_precision: null model");
+		z->z->SetPrecision(precision);
+		return 0;
+	});
+}
+
+int yz_cz_set_amg_reuse(yz_cz *z, int max_solves)
+{
+	return Guard([&] {
+		if(!z) throw yz::UsageError("yz_cz_set_amg_reuse: null model");
+		z->z->SetAmgReuse(max_solves);
+		return 0;
+	});
+}
+
+int yz_cz_parts(yz_cz *z)
+{
+	return Guard([&] {
+		if(!z) throw yz::UsageError("yz_cz_parts: null model");
+		z->z->Parts();
+		return 0;
+	});
+}
+
+long long yz_cz_read(yz_cz *z, const char *name, double *out, long long cap)
+{
+	long long n = -1;
+	const int r = Guard([&] {
+		if(!z || !name) throw yz::UsageError("yz_cz_read: null argument");
+		n = z->z->Read(name, out, cap);
+		return 0;
+	});
+	return r != 0 ? r : n;
+}
+
+int yz_cz_pattern(yz_cz *z, int which, int *rowptr, int *col, int *bc)
+{
+	return Guard([&] {
+		if(!z) throw yz::UsageError("yz_cz_pattern: null model");
+		return z->z->Pattern(which, rowptr, col, bc);
+	});
+}
+
+int yz_cz_build_pattern(const yz_cz_params *p, int which, int *rowptr, int *col, int *bc)
+{
+	return Guard([&] {
+		if(!p) throw yz::UsageError("yz_cz_build_pattern: null params");
+		yz::CheckCzParams(*p);
+		std::vector<int> rh, ch, bh, rc, cc, bcc;
+		yz::BuildCzPatterns(*p, rh, ch, bh, rc, cc, bcc);
+		const std::vector<int> &R = which ? rc : rh, &C = which ? cc : ch, &B = which ? bcc : bh;
+		if(rowptr) std::memcpy(rowptr, R.data(), R.size() * sizeof(int));
+		if(col) std::memcpy(col, C.data(), C.size() * sizeof(int));
+		if(bc) std::memcpy(bc, B.data(), B.size() * sizeof(int));
+		return (int)C.size();
+	});
+}
