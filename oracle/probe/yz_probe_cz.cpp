@@ -14,6 +14,13 @@
  *                                          (ConcZ_Model_2D::Run) to
  *                                          Numerics.MaxSteps and writes the
  *                                          state it ends on;
+ *   yz_probe_cz case.toml out.bin ... init=h.bin
+ *                                          first replaces the film the case
+ *                                          built by the nx*ny doubles of
+ *                                          h.bin (row jy nx + ix, ghosts
+ *                                          included): the field, its copy at
+ *                                          the start of the step and the
+ *                                          height equation's unknowns;
  *   yz_probe_cz case.toml out.bin parts    takes the pieces of one step on the
  *                                          start state instead, each written
  *                                          as the reference forms it: the
@@ -188,8 +195,14 @@ std::vector<double> Vec(const Vector<double> &x)
 
 int main(int argc, char **argv)
 {
-	if(argc < 3) { std::fprintf(stderr, "usage: yz_probe_cz case.toml out.bin [parts]\n"); return 2; }
-	const bool parts = argc > 3 && std::strcmp(argv[3], "parts") == 0;
+	if(argc < 3) { std::fprintf(stderr, "usage: yz_probe_cz case.toml out.bin [parts] [init=h.bin]\n"); return 2; }
+	bool parts = false;
+	const char *init = nullptr;
+	for(int a = 3; a < argc; ++a)
+	{
+		if(std::strcmp(argv[a], "parts") == 0) parts = true;
+		else if(std::strncmp(argv[a], "init=", 5) == 0) init = argv[a] + 5;
+	}
 	C_Yuzen solver;
 	if(!solver.ReadInputFile(argv[1])) return 1;
 	if(!solver.Initialize()) return 1;
@@ -217,6 +230,27 @@ int main(int argc, char **argv)
 	auto &he = m->_heightEq;
 	auto &ce = m->_concEq;
 	const BoundaryCondition2D &bc = m->_boundary;
+	if(init)
+	{
+		std::vector<double> h((size_t)P.nx * P.ny);
+		FILE *f = std::fopen(init, "rb");
+		if(!f || std::fread(h.data(), sizeof(double), h.size(), f) != h.size())
+		{
+			std::fprintf(stderr, "yz_probe_cz: cannot read %zu doubles from %s\n", h.size(), init);
+			return 5;
+		}
+		std::fclose(f);
+		for(int j = 0; j < P.ny; ++j)
+			for(int i = 0; i < P.nx; ++i)
+			{
+				const double v = h[(size_t)j * P.nx + i];
+				m->_field.HH(P.G2->At<Zface>(i, j)) = v;
+				he._phi_old2[j * P.nx + i] = v;
+				he._phi_old[j * P.nx + i] = v;
+				he._phi_new[j * P.nx + i] = v;
+			}
+		he.TakeFieldAsStart();
+	}
 
 	PutI("nx", P.nx); PutI("ny", P.ny); PutI("nz", P.nz);
 	PutI("bc", std::vector<int>{(int)bc._tXmin, (int)bc._tXmax, (int)bc._tYmin, (int)bc._tYmax});

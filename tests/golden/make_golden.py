@@ -342,6 +342,12 @@ CZ_CASES = {
 }
 
 
+#  the CZ cases written as TOML for the drop-in test of seam 3
+#  (tests/test_dropin_gpu.py: the reference's driver with its CZ loop on the
+#  device against the reference's own run)
+CZ_DROPIN_CASES = ("cz_sym_16", "cz_per_koren_16")
+
+
 def make_cz_case(ref: Path, name: str, work: Path) -> dict:
     src, over, parts = CZ_CASES[name]
     case = write_case(ref, src, over, name, work)
@@ -566,6 +572,10 @@ def main() -> None:
         for name, (src, over) in DROPIN_CASES.items():
             write_case(Path(a.ref), src, over, name, cases_dir)
             print("case", name)
+        for name in CZ_DROPIN_CASES:
+            src, over, _ = CZ_CASES[name]
+            write_case(Path(a.ref), src, over, "czdropin_" + name, cases_dir)
+            print("case", "czdropin_" + name)
         for name in STEP_CASES:
             if a.only and name != a.only:
                 continue

@@ -82,3 +82,54 @@ def test_reference_driver_with_the_step_on_the_device(case, tmp_path):
     assert abs(gpu["t_end"] - cpu["t_end"]) <= 1e-12 * abs(cpu["t_end"])
     assert np.linalg.norm(gpu["h"] - cpu["field_h1"]) / np.linalg.norm(cpu["field_h1"]) <= 1e-10
     assert np.linalg.norm(gpu["c"] - cpu["field_c1"]) / np.linalg.norm(cpu["field_c1"]) <= 1e-10
+
+
+PROBE_CZ = REPO / "oracle" / "_ref" / "yz_probe_cz"
+CZ_B200 = REPO / "oracle" / "_ref" / "yuzen_b200_cz"
+CZ_CASES = sorted((REPO / "tests" / "golden" / "cases").glob("czdropin_*.toml"))
+
+
+def read_seam3(path: Path) -> dict:
+    """The record yuzen_b200_cz writes: magic, nx, ny, nz, steps, linear
+    iterations, coupling passes, the clock, dt, the wall time, then h
+    (nx*ny) and c (nx*ny*nz)."""
+    raw = path.read_bytes()
+    assert raw[:8] == b"YZSEAM31"
+    nx, ny, nz, steps, linear, coupling = (int(v) for v in np.frombuffer(raw, "<i4", 6, 8))
+    t_end, dt, wall = np.frombuffer(raw, "<f8", 3, 32)
+    m2, m3 = nx * ny, nx * ny * nz
+    h = np.frombuffer(raw, "<f8", m2, 56).copy()
+    c = np.frombuffer(raw, "<f8", m3, 56 + 8 * m2).copy()
+    return {"steps": steps, "linear": linear, "coupling": coupling, "t_end": float(t_end), "dt": float(dt),
+            "h": h, "c": c}
+
+
+@pytest.mark.parametrize("case", CZ_CASES, ids=[c.stem for c in CZ_CASES])
+def test_reference_driver_with_the_cz_step_on_the_device(case, tmp_path):
+    """Seam 3: the reference's own set-up of a ConcZ case (C_Yuzen) with its
+    time loop replaced by the device step (yuzen_b200/host/yz_cz_adapter.cpp)
+    against the reference's whole run of the same case (yz_probe_cz): the
+    same steps, linear iterations and coupling passes, the clock to 1e-12,
+    h and c within 1e-10 relative L2."""
+    if not (PROBE_CZ.exists() and CZ_B200.exists()):
+        pytest.skip("reference-built binaries not present (make -C oracle ref b200)")
+    work = tmp_path / "ref"
+    work.mkdir()
+    (work / case.name).write_text(case.read_text())
+    r = subprocess.run([str(PROBE_CZ), case.name, "out.bin"], cwd=work, capture_output=True, text=True, timeout=900,
+                       env=dict(os.environ, OMP_NUM_THREADS="4"))
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    ref = stateio.read_records(work / "out.bin")
+    work = tmp_path / "seam3"
+    work.mkdir()
+    (work / case.name).write_text(case.read_text())
+    r = subprocess.run([str(CZ_B200), case.name, "out.bin"], cwd=work, capture_output=True, text=True, timeout=900,
+                       env=dict(os.environ, OMP_NUM_THREADS="4"))
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    gpu = read_seam3(work / "out.bin")
+    assert gpu["steps"] == ref["steps_done"]
+    assert gpu["linear"] == ref["linear_iterations"] and gpu["coupling"] == ref["coupling_passes"]
+    assert abs(gpu["t_end"] - ref["t_end"]) <= 1e-12 * abs(ref["t_end"])
+    eh = np.linalg.norm(gpu["h"] - ref["h1"]) / np.linalg.norm(ref["h1"])
+    ec = np.linalg.norm(gpu["c"] - ref["c1"]) / np.linalg.norm(ref["c1"])
+    assert eh <= 1e-10 and ec <= 1e-10, (eh, ec)
