@@ -549,6 +549,9 @@ int yz_cz_destroy(yz_cz* z);
 int yz_cz_advance(yz_cz* z, int nsteps, yz_cz_stats* stats);
 /* The film (nx*ny) and the concentration (nx*ny*nz) the model holds. */
 int yz_cz_get_fields(yz_cz* z, double* h, double* c);
+/* Replace them (host arrays; either may be null): the state the next step
+ * starts from. */
+int yz_cz_set_fields(yz_cz* z, const double* h, const double* c);
 /* Preconditioner arithmetic (YZ_PREC_*) and AMG hierarchy reuse of both
  * equations' solves, from the next solve on (FP64, no reuse: the reference's). */
 int yz_cz_set_precision(yz_cz* z, int precision);

@@ -348,6 +348,41 @@ CZ_CASES = {
 CZ_DROPIN_CASES = ("cz_sym_16", "cz_per_koren_16")
 
 
+#  the ConcZ workload at its bench size (yuzen_b200.cases.cz_bumps), run by
+#  the reference from the builder's seeded film: compact, the end state as
+#  the film, the column sums of c over the real levels and every 61st c
+BIG_CZ_CASES = {"cz_256": {"N": 256, "Nz": 16, "steps": 3}}
+
+
+def make_big_cz_case(name: str, work: Path, threads: int) -> dict:
+    sys.path.insert(0, str(REPO))
+    from yuzen_b200 import cases
+    kw = BIG_CZ_CASES[name]
+    case = cases.cz_bumps(**kw)
+    w = work / name
+    case.write_reference(w)
+    env = dict(os.environ, OMP_NUM_THREADS=str(min(threads, 8)))
+    res = subprocess.run([str(PROBE_CZ), "case.toml", "out.bin", "init=init.bin"], cwd=w, env=env,
+                         capture_output=True, text=True, timeout=3600)
+    if res.returncode != 0:
+        raise RuntimeError(f"{name}: probe failed\n{res.stdout[-2000:]}\n{res.stderr[-2000:]}")
+    d = stateio.read_records(w / "out.bin")
+    rec = case.record()
+    for k, v in rec.items():
+        if not np.array_equal(np.asarray(v), np.asarray(d[k])):
+            raise RuntimeError(f"{name}: the builder's {k} differs from the reference's")
+    nx, ny, nz = d["nx"], d["ny"], d["nz"]
+    c1 = d["c1"]
+    out = {k: d[k] for k in ("nx", "ny", "nz", "steps_done", "t_end", "dt_end", "linear_iterations",
+                             "coupling_passes", "h1", "wall")}
+    out["c1_colsum"] = c1.reshape(nz, ny, nx)[2:-2].sum(axis=0).ravel()
+    out["c1_sample"] = c1[::61].copy()
+    out["h0"] = d["h0"]
+    out["builder"] = name
+    out["threads"] = min(threads, 8)
+    return out
+
+
 def make_cz_case(ref: Path, name: str, work: Path) -> dict:
     src, over, parts = CZ_CASES[name]
     case = write_case(ref, src, over, name, work)
@@ -612,6 +647,14 @@ def main() -> None:
             d = make_big_step_case(name, Path(tmp), a.threads)
             stateio.save_npz(HERE / f"big_{name}.npz", d)
             print(name, d["nx"], d["ny"], "steps", d["steps_done"], "t_end", d["t_end"])
+        for name in BIG_CZ_CASES:
+            if a.only and name != a.only:
+                continue
+            if not a.big and a.only != name:
+                continue
+            d = make_big_cz_case(name, Path(tmp), a.threads)
+            stateio.save_npz(HERE / f"czbig_{name.split('_')[-1]}.npz", d)
+            print(name, d["nx"], d["ny"], d["nz"], "steps", d["steps_done"], "t_end", d["t_end"])
         for name in CZ_CASES:
             if a.only and name != a.only:
                 continue

@@ -82,3 +82,14 @@ def test_fixture_covers_the_paths():
     assert b["on_sc"] == 0 and b["c_scheme"] == 7 and b["bc"][0] == 1 and b["on_vg"] == 1 and b["on_hg"] == 1
     assert c["dt_control"] == 0 and c["on_cf"] == 1
     assert (big["nx"] - 4) * (big["ny"] - 4) > 3000
+
+
+def test_bench_size_builder_matches_the_fixture():
+    """The seeded 256^2 x 16 film of yuzen_b200.cases.cz_bumps is the one the
+    reference ran for tests/golden/czbig_256.npz (make_golden checked every
+    parameter against the reference's set-up when it was made)."""
+    from yuzen_b200 import cases
+    ref = stateio.load_npz(GOLD / "czbig_256.npz")
+    rec = cases.cz_bumps(N=256, Nz=16, steps=3).record()
+    assert np.array_equal(rec["h0"], ref["h0"])
+    assert (rec["nx"], rec["ny"], rec["nz"]) == (ref["nx"], ref["ny"], ref["nz"])

@@ -89,3 +89,27 @@ def test_solute_conserved_and_runs_repeat():
 
     s0, s1 = solute(d["h0"], d["c0"]), solute(*out[0])
     assert abs(s1 - s0) <= 1e-11 * abs(s0)
+
+
+def test_bench_size_run_matches_the_reference():
+    """The ConcZ workload at its bench size, 256^2 x 16 levels
+    (yuzen_b200.cases.cz_bumps), built from the seed: three steps against the
+    reference's run of the same film (tests/golden/czbig_256.npz): the film
+    within 1e-10 relative L2, the column sums of c and a sample of c within
+    1e-10, the same steps, clock and iteration counts."""
+    from yuzen_b200 import cases, cz
+    ref = stateio.load_npz(GOLD / "czbig_256.npz")
+    rec = cases.cz_bumps(N=256, Nz=16, steps=3).record()
+    m = cz.CzModel(cz.params_from_record(rec), rec["xc"], rec["xf"], rec["yc"], rec["yf"], rec["h0"], rec["s"],
+                   rec["c0"])
+    st = m.advance(int(ref["steps_done"]))
+    h, c = m.fields()
+    m.close()
+    nx, ny, nz = ref["nx"], ref["ny"], ref["nz"]
+    assert st["steps"] == ref["steps_done"] and abs(st["time"] - ref["t_end"]) <= 1e-12 * ref["t_end"]
+    assert st["linear_iterations"] == ref["linear_iterations"] and st["coupling_passes"] == ref["coupling_passes"]
+    eh = np.linalg.norm(h - ref["h1"]) / np.linalg.norm(ref["h1"])
+    cs = c.reshape(nz, ny, nx)[2:-2].sum(axis=0).ravel()
+    ecs = np.linalg.norm(cs - ref["c1_colsum"]) / np.linalg.norm(ref["c1_colsum"])
+    esm = np.linalg.norm(c[::61] - ref["c1_sample"]) / np.linalg.norm(ref["c1_sample"])
+    assert eh <= 1e-10 and ecs <= 1e-10 and esm <= 1e-10, (eh, ecs, esm)

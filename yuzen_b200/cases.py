@@ -517,3 +517,139 @@ def bench2d_512(N: int = 512, steps: int = 12) -> Case:
 
 
 CONFIGS = {"spinodal_224": spinodal_224, "allphys_512": allphys, "bench2d_512": bench2d_512}
+
+
+# ----------------------------------------------------------------------
+#  the ConcZ model (the film with its concentration through the thickness)
+# ----------------------------------------------------------------------
+@dataclass
+class CzCase:
+    """A 2-D ConcZ case: the film of a well-mixed Case (its fluid, physics,
+    grid and non-dimensional groups, NonDimensionalNumbers::Build) with Nz
+    levels through the film and the concentration equation of the CZ model.
+    The seeded film replaces the one the case builds (the reference's CZ
+    model reads no 2-D restart: oracle/probe/yz_probe_cz takes it as init=)."""
+    base: Case
+    Nz: int
+    conc_linear: dict = field(default_factory=lambda: {"maxit": 5000, "eps": 1e-13, "precond": "ILU",
+                                                       "scaling": True})
+
+    def toml(self) -> dict:
+        b = self.base
+        doc = b.toml()
+        doc["Grid"]["Nz"] = self.Nz
+        doc["Physics"]["ConcField"]["Model"] = "CZ"
+        doc["Restart"] = {"Enable": False}
+        #  the CZ film has no upwinded term (CheckParameters refuses the key)
+        del doc["Numerics"]["Convection"]["Height"]
+        cl = self.conc_linear
+        doc["Numerics"]["ConcEquation"]["LinearSolver"] = {
+            "Backend": "amgcl", "MaxIterations": cl["maxit"], "Epsilon": cl["eps"], "RowScaling": cl["scaling"],
+            "PreconditionType": cl["precond"]}
+        return doc
+
+    def zeta(self) -> float:
+        """C_Grid3D::Build (Grids.cpp:150-183) with RectGrid::SetExtentZ: the
+        spacing of the zeta levels with two ghost levels at each end."""
+        d0 = (1.0 - 0.0) / float(self.Nz)
+        zmin, zmax = 0.0 - 2 * d0, 1.0 + 2 * d0
+        return (zmax - zmin) / (self.Nz + 4)
+
+    def record(self) -> dict:
+        """The model's state as the reference's Build leaves it, in the keys of
+        oracle/probe/yz_probe_cz (yuzen_b200.cz.params_from_record)."""
+        b = self.base
+        sc = b.scales()
+        g = b.grid(sc["L0"])
+        ev = b.evaporation or {}
+        f = b.fluid
+        nx, ny, nz = g["nx"], g["ny"], self.Nz + 4
+        dt = b.dt / sc["T0"]
+        #  C_TimeSteps::Build's range (TimeSteps.cpp:38-60), capped by the
+        #  output intervals in ConcZ_Model_2D::Run (:714-735)
+        dt_max = 1e10
+        cap = 1e30 / sc["T0"]
+        if cap < dt_max:
+            dt_max = cap
+        if dt_max < dt:
+            dt = dt_max
+        h, c, s = b.fields()
+        evp = b._evap_params(sc)
+        xc = [g["xmin"] + ix * g["dx"] + g["dx"] * 0.5 for ix in range(nx)]
+        xf = [g["xmin"] + ix * g["dx"] + 0.0 for ix in range(nx)]
+        yc = [g["ymin"] + iy * g["dy"] + g["dy"] * 0.5 for iy in range(ny)]
+        yf = [g["ymin"] + iy * g["dy"] + 0.0 for iy in range(ny)]
+        lin, cl = b.linear, self.conc_linear
+        pre = {"None": 0, "Jacobi": 1, "ILU": 2}
+        #  without the control the solver keeps C_ImplicitSolver's defaults
+        dtc = b.dtc if b.dt_control else {"KeepSteps": 50, "ChangeFactor": 0.5, "Criterion": 1e-3, "ScaleFloor": 0.0}
+        rec = {
+            "nx": nx, "ny": ny, "nz": nz, "bc": np.array([BC[x] for x in b.bc], np.int32),
+            "on_lap": int(b.laplace), "on_sc": int(b.marangoni), "on_vg": int(b.vgrav is not None),
+            "on_hg": int(b.hgrav is not None), "on_cf": int(b.centrifugal is not None),
+            "on_evap": int(b.evaporation is not None), "on_mms": 0,
+            "ev_conc": 1 if ev.get("ConcFunc") == "PowerN" else 0,
+            "ev_spatial": 1 if ev.get("SpatialFunc") == "negPow" else 0,
+            "ev_hast": evp["evap_hast_modify"], "dt_control": int(b.dt_control), "dt_keep_steps": dtc["KeepSteps"],
+            "max_steps": b.steps,
+            "h_lin": np.array([pre[lin["precond"]], int(lin["scaling"]), lin["maxit"], 0], np.int32),
+            "c_lin": np.array([pre[cl["precond"]], int(cl["scaling"]), cl["maxit"], 1], np.int32),
+            "c_scheme": SCHEMES[b.conv_conc],
+            "dx": g["dx"], "dy": g["dy"], "dzeta": self.zeta(), "theta_h": 0.5, "theta_c": 0.5,
+            "dt": dt, "dt_old": dt, "dt_max": dt_max, "dt_min": 1e-15, "time": 0.0,
+            "dt_change_factor": dtc["ChangeFactor"], "dt_criterion": dtc["Criterion"],
+            "dt_scale_floor": dtc["ScaleFloor"],
+            "As": sc["As"], "Ma": sc["Ma"], "Bo": sc["Bo"], "Pgx": sc["Pgx"], "Pgy": sc["Pgy"], "Sp": sc["Sp"],
+            "Df": sc["Df"], "Ev": sc["Ev"],
+            "rot_center": np.array([(b.centrifugal[1][0] if b.centrifugal else 0.0) / sc["L0"],
+                                    (b.centrifugal[1][1] if b.centrifugal else 0.0) / sc["L0"]]),
+            "visc": np.array([f["mu_c0"], 1.0, f["mu_exp"]]), "sigma": np.array([f["sigma_c0"], 1.0, sc["Ma"]]),
+            "diff": np.array([f["D_c0"], 1.0, f["D_exp"]]),
+            "evap": np.array([evp["ev_m_resin"], evp["ev_m_solvent"], evp["ev_e0"], evp["ev_power_n"],
+                              evp["ev_negpow_exp"], evp["ev_negpow_rmax"], evp["ev_conc_r"], evp["ev_h_ast"],
+                              min(g["dx"], g["dy"])]),
+            "h_eps": lin["eps"], "c_eps": cl["eps"], "coupling_floor": max(1e-10, 10.0 * cl["eps"]),
+            "xc": np.array(xc), "xf": np.array(xf), "yc": np.array(yc), "yf": np.array(yf),
+            "h0": h, "s": s, "c0": np.full(nx * ny * nz, float(b.conc0)),
+        }
+        return rec
+
+    def write_reference(self, workdir) -> Path:
+        """case.toml and init.bin (the film, nx*ny doubles, row iy*nx + ix,
+        ghosts included) for oracle/probe/yz_probe_cz ... init=init.bin."""
+        w = Path(workdir)
+        w.mkdir(parents=True, exist_ok=True)
+        h, _, _ = self.base.fields()
+        np.asarray(h, "<f8").tofile(w / "init.bin")
+        (w / "case.toml").write_text(toml_dumps(self.toml()))
+        return w / "case.toml"
+
+
+def cz_bumps(N: int = 256, Nz: int = 16, seed: int = 20261205, steps: int = 6, dt: float = 0.01,
+             bumps: int = 8, sigma_cells: float = 10.0, amp: float = 0.05, Ev: float = 2e-3, Df: float = 1.0,
+             conc0: float = 0.3, side: float = 1.0e-3) -> CzCase:
+    """The evaporating film through the thickness at N^2 x Nz: h = 1 +
+    amp * the sum of `bumps` Gaussians of sigma_cells cells at seeded
+    centres, c = conc0, capillary + Marangoni + evaporation, mu(c), sigma(c)
+    and D(c) of the reference's resist (concz_2d.toml), Symmetry edges, a
+    fixed dt [s]; the evaporation coefficient and the diffusivity chosen so
+    that Ev and Df come out as given (T0 = mu L0^4 / (sigma h0^3))."""
+    rng = np.random.default_rng(seed)
+    cx, cy = rng.uniform(0, N, bumps), rng.uniform(0, N, bumps)
+    ii = np.arange(N) + 0.5
+    X, Y = np.meshgrid(ii, ii)
+    h = np.ones((N, N))
+    for k in range(bumps):
+        h += amp * np.exp(-((X - cx[k]) ** 2 + (Y - cy[k]) ** 2) / (2.0 * sigma_cells ** 2))
+    fluid = {"rho": 1000.0, "sigma": 30.0e-3, "sigma_c0": 0.5, "sigma_coef": 10e-3,
+             "mu": 100.0e-3, "mu_c0": 0.5, "mu_exp": 10.0, "D": 1.0e-9, "D_c0": 0.5, "D_exp": -7.0,
+             "M_solvent": 100.0, "M_resin": 2000.0}
+    h0 = 10e-6
+    L0 = math.sqrt(fluid["sigma"] / (fluid["rho"] * GG))
+    T0 = fluid["mu"] * math.pow(L0, 4.0) / (fluid["sigma"] * math.pow(h0, 3.0))
+    fluid["D"] = Df * math.pow(L0, 2.0) / T0
+    base = Case(name=f"cz_bumps_{N}", Nx=N, Ny=N, xlim=(-0.5 * side, 0.5 * side), ylim=(-0.5 * side, 0.5 * side),
+                h0=h0, precursor=0.5, bc=("Symmetry",) * 4, dt=dt, steps=steps, fluid=fluid, marangoni=True,
+                evaporation={"Coef": Ev * h0 / T0, "ConcFunc": "Raoult", "SpatialFunc": "uniform"},
+                conc_model="CZ", conc0=conc0, h_init=h)
+    return CzCase(base=base, Nz=Nz)

@@ -623,6 +623,15 @@ int yz_cz_get_fields(yz_cz *z, double *h, double *c)
 	});
 }
 
+int yz_cz_set_fields(yz_cz *z, const double *h, const double *c)
+{
+	return Guard([&] {
+		if(!z) throw yz::UsageError("yz_cz_set_fields: null model");
+		z->z->SetFields(h, c);
+		return 0;
+	});
+}
+
 int yz_cz_set_precision(yz_cz *z, int precision)
 {
 	return Guard([&] {

@@ -2076,6 +2076,25 @@ void CzStep::GetFields(double *h, double *c)
 	YZ_CUDA(cudaStreamSynchronize(_st));
 }
 
+//  the state a step starts from: the film and the concentration the model
+//  holds (and the field and its copy at the start of the step)
+void CzStep::SetFields(const double *h, const double *c)
+{
+	YZ_CUDA(cudaSetDevice(_device));
+	if(h)
+	{
+		_hNew.upload(h, (size_t)_n2, _st);
+		Copy(_fH.get(), _hNew.get(), (size_t)_n2);
+		Copy(_tH.get(), _hNew.get(), (size_t)_n2);
+	}
+	if(c)
+	{
+		_cNew.upload(c, (size_t)_n3, _st);
+		Copy(_fC.get(), _cNew.get(), (size_t)_n3);
+		Copy(_tC.get(), _cNew.get(), (size_t)_n3);
+	}
+}
+
 void CzStep::SetPrecision(int precision)
 {
 	_solverH->SetPrecision(precision);

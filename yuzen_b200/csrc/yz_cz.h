@@ -75,6 +75,7 @@ public:
 	~CzStep();
 	void Advance(int nsteps, yz_cz_stats &stats);
 	void GetFields(double *h, double *c);
+	void SetFields(const double *h, const double *c);
 	void SetPrecision(int precision);
 	void SetAmgReuse(int maxSolves);
 	void Parts();

@@ -68,6 +68,7 @@ def _bind():
     L.yz_cz_destroy.argtypes = [ctypes.c_void_p]
     L.yz_cz_advance.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(CzStats)]
     L.yz_cz_get_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
+    L.yz_cz_set_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
     L.yz_cz_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_cz_set_amg_reuse.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_cz_parts.argtypes = [ctypes.c_void_p]
@@ -160,6 +161,13 @@ class CzModel:
         h, c = np.zeros(self.n2), np.zeros(self.n3)
         _check(lib().yz_cz_get_fields(self._h, _fp(h), _fp(c)), "yz_cz_get_fields")
         return h, c
+
+    def fields_into(self, h: np.ndarray, c: np.ndarray) -> None:
+        """The fields into caller arrays (pinned host memory, say)."""
+        _check(lib().yz_cz_get_fields(self._h, _fp(h), _fp(c)), "yz_cz_get_fields")
+
+    def set_fields(self, h: np.ndarray, c: np.ndarray) -> None:
+        _check(lib().yz_cz_set_fields(self._h, _fp(h), _fp(c)), "yz_cz_set_fields")
 
     def set_precision(self, precision: int) -> None:
         _check(lib().yz_cz_set_precision(self._h, int(precision)), "yz_cz_set_precision")
