@@ -783,10 +783,17 @@ def run_cz_arm(a) -> None:
         out["model"] = m
         return out
 
-    arms = {}
+    arms, failed = {}, {}
     with Clocks(local) as clk:
         for x in names:
-            arms[x] = timed_arm(x)
+            try:
+                arms[x] = timed_arm(x)
+            except yz.StepFailedError as e:
+                #  an arm whose solve does not converge at the fixed step
+                #  (the FP32 matrix on the concentration's stiff zeta
+                #  diffusion) is reported, not timed
+                failed[x] = str(e)[:200]
+    names = [x for x in names if x in arms]
 
     def qualifies(x) -> bool:
         v = arms[x]
@@ -830,7 +837,7 @@ def run_cz_arm(a) -> None:
             "data": "synthetic (seeded: yuzen_b200.cases.cz_bumps)",
             "config": {"workload": "cz_256", "grid": [256, 256, 16], "arm": head_name, "l2": "flushed (256 MiB)",
                        "arms": {x: {k: v for k, v in arms[x].items() if k != "model"} | {"steps_per_s": arms[x]["value"]}
-                                for x in names}},
+                                for x in names}, "arms_failed": failed},
             "e2e": {"value": head["e2e"], "unit": UNIT, "h2d_bytes_per_step": 8 * (n2 + n3),
                     "d2h_bytes_per_step": 8 * (n2 + n3)},
             "gpu_launches": head["launches"], "clocks": clk.summary(), "roofline": roof, "cpu_baseline": cpu,
