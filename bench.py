@@ -69,6 +69,8 @@ NCU_TRAFFIC = {
     # (50,359,808 B); the pass's two smaller kernels (KFaceProps, KCellPi) were
     # not captured
     ("assembly", "allphys_512"): 180615424 + 50359808,
+    # the ConcZ concentration assembly (profiles/KCzAssembleC_cz_256.md)
+    ("KCzAssembleC", "cz_256"): 41707776 + 136976896,
 }
 
 
@@ -820,7 +822,8 @@ def run_cz_arm(a) -> None:
         per = kern_ms / kern_n
         ach = cz_assembly_bytes(nr) / (per * 1e-3) / 1e9
         roof = {"kernel": CZ_ROOFLINE_KERNEL, "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"],
-                "unit": "GB/s", "frac": ach / peaks["hbm_gbs"], "traffic": None, "launches_timed": kern_n,
+                "unit": "GB/s", "frac": ach / peaks["hbm_gbs"],
+                "traffic": NCU_TRAFFIC.get((CZ_ROOFLINE_KERNEL, "cz_256")), "launches_timed": kern_n,
                 "avg_launch_us": per * 1e3, "algorithmic_bytes_per_launch": cz_assembly_bytes(nr),
                 "peak_source": peaks["source"]}
     cpu = None
