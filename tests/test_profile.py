@@ -98,3 +98,37 @@ def test_profile_off_prints_nothing():
     out, err = _run(None)
     assert out["enabled"] == 0 and out["table"] == {}
     assert "[profile]" not in err
+
+
+_CHILD_CZ = r"""
+import json, sys
+sys.path[:0] = [sys.argv[1], sys.argv[1] + "/tests", sys.argv[1] + "/tests/golden"]
+import stateio
+import yuzen_b200 as yz
+from yuzen_b200 import cz
+d = stateio.load_npz(sys.argv[1] + "/tests/golden/cz_sym_16.npz")
+m = cz.CzModel(cz.params_from_record(d), d["xc"], d["xf"], d["yc"], d["yf"], d["h0"], d["s"], d["c0"])
+r = m.advance(int(d["steps_done"]))
+m.close()
+print(json.dumps({"table": yz.profile_table(), "steps": r["steps"], "solves": r["solves"]}))
+"""
+
+
+@pytest.mark.gpu
+def test_profile_table_of_the_concz_step():
+    """The ConcZ step's scopes carry the reference's CZ labels (YUZEN_PROF in
+    CZ_HeightEquation_2D.cpp and CZ_ConcEquation_2D.cpp): the film's
+    assembly, right-hand side and solve, the velocity, the concentration's
+    step and its solves."""
+    env = dict(os.environ, YUZEN_PROFILE="1")
+    res = subprocess.run([sys.executable, "-c", _CHILD_CZ, str(ROOT)], capture_output=True, text=True, env=env,
+                         timeout=600)
+    assert res.returncode == 0, res.stderr[-3000:]
+    import json
+    out = json.loads(res.stdout.strip().splitlines()[-1])
+    t = out["table"]
+    for name in ("step", "h.assemble", "h.rhs", "h.linsolve", "velocity", "c.solve", "c.linsolve", "lin.iterate"):
+        assert name in t and t[name][0] > 0 and t[name][1] > 0.0, (name, t)
+    assert t["step"][0] == out["steps"]
+    assert t["h.linsolve"][0] + t["c.linsolve"][0] == out["solves"]
+    assert t["h.linsolve"][1] <= t["step"][1] + 1e-4

@@ -1540,14 +1540,24 @@ void CzStep::SetMatrixAH(const double *fH, const double *fC, double dt)
 //  SolveStage (CZ_HeightEquation_2D.cpp:1949-1963)
 void CzStep::SolveStageH(const double *fH, const double *fC, double dt, int &iter, double &resid, int &ch)
 {
-	SetMatrixAH(fH, fC, dt);
+	{
+		YZ_PROF("h.assemble", _st);
+		SetMatrixAH(fH, fC, dt);
+	}
 	const int g = GridFor(_n2, kB);
-	YZ_LAUNCH(KCzMatVec, g, kB, 0, _st, _n2, _dRowptrH.get(), _dColH.get(), _A.get(), _hOld.get(), _Ax.get());
-	YZ_LAUNCH(KCzMakeIA, g, kB, 0, _st, _n2, _dRowptrH.get(), _dBcH.get(), _A.get(), _IA.get(), _p.theta_h, dt);
-	YZ_LAUNCH(KCzMakeRhsH, g, kB, 0, _st, _n2, _dBcH.get(), _hOld.get(), _Ax.get(), _B.get(), _p.theta_h, dt, _rhs.get());
+	{
+		YZ_PROF("h.rhs", _st);
+		YZ_LAUNCH(KCzMatVec, g, kB, 0, _st, _n2, _dRowptrH.get(), _dColH.get(), _A.get(), _hOld.get(), _Ax.get());
+		YZ_LAUNCH(KCzMakeIA, g, kB, 0, _st, _n2, _dRowptrH.get(), _dBcH.get(), _A.get(), _IA.get(), _p.theta_h, dt);
+		YZ_LAUNCH(KCzMakeRhsH, g, kB, 0, _st, _n2, _dBcH.get(), _hOld.get(), _Ax.get(), _B.get(), _p.theta_h, dt,
+		          _rhs.get());
+	}
 	iter = 0;
 	resid = 0;
-	ch = _solverH->Solve(_p.h_lin, _IA.get(), _rhs.get(), _hNew.get(), iter, resid);
+	{
+		YZ_PROF("h.linsolve", _st);
+		ch = _solverH->Solve(_p.h_lin, _IA.get(), _rhs.get(), _hNew.get(), iter, resid);
+	}
 	++_solves;
 }
 
@@ -1598,6 +1608,7 @@ void CzStep::CalDtDh(double dt)
 
 void CzStep::CalVelocity(const double *fH, const double *fC)
 {
+	YZ_PROF("velocity", _st);
 	YZ_LAUNCH(KCzVel<1>, GridFor((_p.nx - 3) * _p.ny, kB), kB, 0, _st, _k, fH, _s.get(), fC, _Ux.get());
 	YZ_LAUNCH(KCzVel<0>, GridFor(_p.nx * (_p.ny - 3), kB), kB, 0, _st, _k, fH, _s.get(), fC, _Uy.get());
 	YZ_LAUNCH(KCzVelGhost<1>, GridFor(_p.ny * _p.nz, kB), kB, 0, _st, _k, _Ux.get());
@@ -1683,6 +1694,7 @@ int CzStep::SolveStageC(const double *fH, const double *fC, double dt, int &iter
 	resid = 0;
 	if(any)
 	{
+		YZ_PROF("c.linsolve", _st);
 		ch = _solverC->Solve(_p.c_lin, _IAc.get(), _rhsc.get(), _d.get(), iter, resid);
 		++_solves;
 		_concIters += iter;
@@ -1923,6 +1935,7 @@ bool CzStep::AfterTrial(double dt, yz_cz_stats &stats)
 		Copy(_fC.get(), _c0.get(), (size_t)n3);
 		int itc = 0;
 		double rc = 0;
+		YZ_PROF("c.solve", _st);
 		if(pass > 0) ch = SolveAtMidpointC(_fH.get(), _cm.get(), dt, itc, rc);
 		else
 		{
