@@ -556,6 +556,9 @@ int yz_cz_set_fields(yz_cz* z, const double* h, const double* c);
  * equations' solves, from the next solve on (FP64, no reuse: the reference's). */
 int yz_cz_set_precision(yz_cz* z, int precision);
 int yz_cz_set_amg_reuse(yz_cz* z, int max_solves);
+/* The FP32 V-cycle's launch shape of both equations' solves
+ * (yz_solver_set_tuning). */
+int yz_cz_set_tuning(yz_cz* z, int fuse_from, int coarse_lanes, int fine_sweeps);
 /* The pieces of one step on the present state, as the reference forms them
  * (its parity test): the film's assembly at the step's dt, its conservative
  * update with the film unchanged, the velocity and the concentration's

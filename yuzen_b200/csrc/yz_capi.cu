@@ -641,6 +641,15 @@ int yz_cz_set_precision(yz_cz *z, int precision)
 	});
 }
 
+int yz_cz_set_tuning(yz_cz *z, int fuse_from, int coarse_lanes, int fine_sweeps)
+{
+	return Guard([&] {
+		if(!z) throw yz::UsageError("yz_cz_set_tuning: null model");
+		z->z->SetTuning(fuse_from, coarse_lanes, fine_sweeps);
+		return 0;
+	});
+}
+
 int yz_cz_set_amg_reuse(yz_cz *z, int max_solves)
 {
 	return Guard([&] {

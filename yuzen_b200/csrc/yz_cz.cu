@@ -2114,6 +2114,12 @@ void CzStep::SetPrecision(int precision)
 	_solverC->SetPrecision(precision);
 }
 
+void CzStep::SetTuning(int fuseFrom, int coarseLanes, int fineSweeps)
+{
+	_solverH->SetTuning(fuseFrom, coarseLanes, fineSweeps);
+	_solverC->SetTuning(fuseFrom, coarseLanes, fineSweeps);
+}
+
 void CzStep::SetAmgReuse(int maxSolves)
 {
 	_solverH->SetAmgReuse(maxSolves);

@@ -78,6 +78,7 @@ public:
 	void SetFields(const double *h, const double *c);
 	void SetPrecision(int precision);
 	void SetAmgReuse(int maxSolves);
+	void SetTuning(int fuseFrom, int coarseLanes, int fineSweeps);
 	void Parts();
 	long long Read(const std::string &name, double *out, long long cap);
 	int Pattern(int which, int *rowptr, int *col, int *bc) const;

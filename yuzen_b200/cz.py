@@ -71,6 +71,7 @@ def _bind():
     L.yz_cz_set_fields.argtypes = [ctypes.c_void_p, _f64p, _f64p]
     L.yz_cz_set_precision.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.yz_cz_set_amg_reuse.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.yz_cz_set_tuning.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.yz_cz_parts.argtypes = [ctypes.c_void_p]
     L.yz_cz_read.argtypes = [ctypes.c_void_p, ctypes.c_char_p, _f64p, ctypes.c_longlong]
     L.yz_cz_read.restype = ctypes.c_longlong
@@ -174,6 +175,10 @@ class CzModel:
 
     def set_amg_reuse(self, max_solves: int) -> None:
         _check(lib().yz_cz_set_amg_reuse(self._h, int(max_solves)), "yz_cz_set_amg_reuse")
+
+    def set_tuning(self, fuse_from: int, coarse_lanes: int, fine_sweeps: int) -> None:
+        _check(lib().yz_cz_set_tuning(self._h, int(fuse_from), int(coarse_lanes), int(fine_sweeps)),
+               "yz_cz_set_tuning")
 
     def parts(self) -> dict:
         """The pieces of one step on the present state (yz_cz_parts), by the
