@@ -575,6 +575,9 @@ int yz_cz_pattern(yz_cz* z, int which, int* rowptr, int* col, int* bc);
 /* The same from the parameters alone (no device): which 0 the film, 1 the
  * concentration; returns the number of entries (arrays may be null to ask). */
 int yz_cz_build_pattern(const yz_cz_params* p, int which, int* rowptr, int* col, int* bc);
+/* The correctly rounded exp the ConcZ step's property laws use, on the
+ * current device for n host values (its parity test against the host's). */
+int yz_exp_cr(long long n, const double* x, double* y);
 
 #ifdef __cplusplus
 }

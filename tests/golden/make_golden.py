@@ -367,6 +367,12 @@ def make_big_cz_case(name: str, work: Path, threads: int) -> dict:
     if res.returncode != 0:
         raise RuntimeError(f"{name}: probe failed\n{res.stdout[-2000:]}\n{res.stderr[-2000:]}")
     d = stateio.read_records(w / "out.bin")
+    #  the same run with the libm's exp (the reference exactly as it builds)
+    res = subprocess.run([str(PROBE_CZ) + "_libm", "case.toml", "out_libm.bin", "init=init.bin"], cwd=w, env=env,
+                         capture_output=True, text=True, timeout=3600)
+    if res.returncode != 0:
+        raise RuntimeError(f"{name}: probe (libm) failed\n{res.stdout[-2000:]}\n{res.stderr[-2000:]}")
+    dl = stateio.read_records(w / "out_libm.bin")
     rec = case.record()
     for k, v in rec.items():
         if not np.array_equal(np.asarray(v), np.asarray(d[k])):
@@ -377,6 +383,9 @@ def make_big_cz_case(name: str, work: Path, threads: int) -> dict:
                              "coupling_passes", "h1", "wall")}
     out["c1_colsum"] = c1.reshape(nz, ny, nx)[2:-2].sum(axis=0).ravel()
     out["c1_sample"] = c1[::61].copy()
+    out["h1_libm"] = dl["h1"]
+    out["c1_colsum_libm"] = dl["c1"].reshape(nz, ny, nx)[2:-2].sum(axis=0).ravel()
+    out["linear_iterations_libm"] = dl["linear_iterations"]
     out["h0"] = d["h0"]
     out["builder"] = name
     out["threads"] = min(threads, 8)

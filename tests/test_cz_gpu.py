@@ -94,12 +94,14 @@ def test_solute_conserved_and_runs_repeat():
 def test_bench_size_run_matches_the_reference():
     """The ConcZ workload at its bench size, 256^2 x 16 levels
     (yuzen_b200.cases.cz_bumps), built from the seed: three steps against the
-    reference's run of the same film (tests/golden/czbig_256.npz): the film
-    within 1e-10 relative L2, the column sums of c and a sample of c within
-    1e-10, the same steps, clock and coupling passes.  At this size a
-    last-bit difference of the device's exp from the host's in the property
-    laws can move a film solve's iteration count by one or two (2,077 against
-    the reference's 2,079 over the three steps): within 1 %."""
+    reference's run of the same film (tests/golden/czbig_256.npz, the
+    reference's sources with the correctly rounded exp the device uses): the
+    same steps, clock, iteration and coupling-pass counts, the film within
+    1e-10 relative L2, the column sums of c and a sample of c within 1e-10.
+    Against the reference built with the libm's exp (which misrounds about
+    one argument in 1,300) the film is within 1e-8: the reference's own two
+    builds differ by 1.0e-9 at this size (the conditioning of the film's
+    capillary system), and by 2,079 against 2,172 film iterations."""
     from yuzen_b200 import cases, cz
     ref = stateio.load_npz(GOLD / "czbig_256.npz")
     rec = cases.cz_bumps(N=256, Nz=16, steps=3).record()
@@ -110,10 +112,11 @@ def test_bench_size_run_matches_the_reference():
     m.close()
     nx, ny, nz = ref["nx"], ref["ny"], ref["nz"]
     assert st["steps"] == ref["steps_done"] and abs(st["time"] - ref["t_end"]) <= 1e-12 * ref["t_end"]
-    assert abs(st["linear_iterations"] - ref["linear_iterations"]) <= 0.01 * ref["linear_iterations"]
-    assert st["coupling_passes"] == ref["coupling_passes"]
+    assert st["linear_iterations"] == ref["linear_iterations"] and st["coupling_passes"] == ref["coupling_passes"]
     eh = np.linalg.norm(h - ref["h1"]) / np.linalg.norm(ref["h1"])
     cs = c.reshape(nz, ny, nx)[2:-2].sum(axis=0).ravel()
     ecs = np.linalg.norm(cs - ref["c1_colsum"]) / np.linalg.norm(ref["c1_colsum"])
     esm = np.linalg.norm(c[::61] - ref["c1_sample"]) / np.linalg.norm(ref["c1_sample"])
     assert eh <= 1e-10 and ecs <= 1e-10 and esm <= 1e-10, (eh, ecs, esm)
+    el = np.linalg.norm(h - ref["h1_libm"]) / np.linalg.norm(ref["h1_libm"])
+    assert el <= 1e-8, el

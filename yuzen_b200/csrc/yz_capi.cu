@@ -701,3 +701,12 @@ int yz_cz_build_pattern(const yz_cz_params *p, int which, int *rowptr, int *col,
 		return (int)C.size();
 	});
 }
+
+int yz_exp_cr(long long n, const double *x, double *y)
+{
+	return Guard([&] {
+		if(n < 0 || (n > 0 && (!x || !y))) throw yz::UsageError("yz_exp_cr: bad argument");
+		yz::ExpCrHost(n, x, y);
+		return 0;
+	});
+}

@@ -1,5 +1,6 @@
 // yz_cz.cu -- the ConcZ model's time step on the device (see yz_cz.h).
 #include "yz_cz.h"
+#include "yz_exp.h"
 #include "yz_prof.h"
 
 #include <algorithm>
@@ -18,7 +19,16 @@ enum { kBcSym = 0, kBcPer = 1, kBcPin = 2 };
 __host__ __device__ __forceinline__ int I2(const CzCoef &k, int ix, int jy) { return jy * k.nx + ix; }
 __host__ __device__ __forceinline__ int I3(const CzCoef &k, int ix, int jy, int kz) { return (kz * k.ny + jy) * k.nx + ix; }
 
-__device__ __forceinline__ double Diff(const CzCoef &k, double c) { return k.diffBase * exp(k.diffExp * (c - k.diffC0)); }
+//  the property laws (FluidProperty.h:176-180) with the correctly rounded exp
+//  (yz_exp.h), the one the ConcZ oracle links too
+__device__ __forceinline__ double Diff(const CzCoef &k, double c)
+{
+	return k.diffBase * crexp::Exp(k.diffExp * (c - k.diffC0));
+}
+__device__ __forceinline__ double ViscCz(const CzCoef &k, double c)
+{
+	return k.ev.viscBase * crexp::Exp(k.ev.viscExp * (c - k.ev.viscC0));
+}
 
 //  |v| into a running maximum (non-negative doubles order as their bits);
 //  every lane of the warp takes part
@@ -47,7 +57,7 @@ __device__ double FaceInvVisc(const CzCoef &k, const double *C, int ix, int jy, 
 		const double c = 0.5 * (C[I3(k, ix - ax, jy - ay, kz)] + C[I3(k, ix, jy, kz)]);
 		const double r = 1.0 - k.dzeta * (-1.5 + (double)kz);
 		const double w = (power == 2) ? r * r : r;
-		num += w / Viscosity(k.ev, c);
+		num += w / ViscCz(k, c);
 		den += w;
 	}
 	return num / den;
@@ -496,7 +506,7 @@ __global__ void KCzVel(CzCoef k, const double *__restrict__ H, const double *__r
 
 		double Cooo = Cc(ix, jy, 2), Cmoo = Cc(ix - ax, jy - ay, 2);
 		double Coom = Cc(ix, jy, 1), Cmom = Cc(ix - ax, jy - ay, 1);
-		const double muB = Viscosity(k.ev, 0.25 * (Cooo + Coom + Cmoo + Cmom));
+		const double muB = ViscCz(k, 0.25 * (Cooo + Coom + Cmoo + Cmom));
 		double fB1 = 1.0 / muB;
 		double fB2 = sL / muB;
 		const double dz = k.dzeta * hL;
@@ -532,9 +542,9 @@ __global__ void KCzVel(CzCoef k, const double *__restrict__ H, const double *__r
 				Cooo = Cc(ix, jy, kz);
 				Cmoo = Cc(ix - ax, jy - ay, kz);
 			}
-			const double muM = (kz == 2) ? Viscosity(k.ev, 0.375 * (Cooo + Cmoo) + 0.125 * (Coom + Cmom))
-			                             : Viscosity(k.ev, 0.25 * (Cooo + Coom + Cmoo + Cmom));
-			const double muT = Viscosity(k.ev, 0.50 * (Cooo + Cmoo));
+			const double muM = (kz == 2) ? ViscCz(k, 0.375 * (Cooo + Cmoo) + 0.125 * (Coom + Cmom))
+			                             : ViscCz(k, 0.25 * (Cooo + Coom + Cmoo + Cmom));
+			const double muT = ViscCz(k, 0.50 * (Cooo + Cmoo));
 			const double fT1 = 1.0 / muT;
 			const double fT2 = zT / muT;
 			const double fM1 = 1.0 / muM;
@@ -1251,6 +1261,13 @@ __global__ void KCzDeficitCol(CzCoef k, double *c, int *flag)
 }
 
 } // namespace
+
+//  the correctly rounded exp of yz_exp.h, element by element (its test)
+__global__ void KCrExp(long long n, const double *__restrict__ x, double *y)
+{
+	for(long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+		y[i] = crexp::Exp(x[i]);
+}
 
 //==========================================================================
 //  Host side
@@ -2185,6 +2202,18 @@ int CzStep::Pattern(int which, int *rowptr, int *col, int *bc) const
 	if(col) std::memcpy(col, cl.data(), cl.size() * sizeof(int));
 	if(bc) std::memcpy(bc, b.data(), b.size() * sizeof(int));
 	return (int)cl.size();
+}
+
+//  yz_exp_cr: the device's correctly rounded exp on host arrays
+void ExpCrHost(long long n, const double *x, double *y)
+{
+	if(n <= 0) return;
+	DBuf<double> dx, dy;
+	dx.upload(x, (size_t)n, nullptr);
+	dy.reserve((size_t)n);
+	YZ_LAUNCH(KCrExp, GridFor(n, kB), kB, 0, nullptr, n, dx.get(), dy.get());
+	dy.download(y, (size_t)n, nullptr);
+	YZ_CUDA(cudaStreamSynchronize(nullptr));
 }
 
 } // namespace yz

@@ -44,6 +44,9 @@
 
 namespace yz {
 
+//  the correctly rounded exp (yz_exp.h) of n host values on the current device
+void ExpCrHost(long long n, const double *x, double *y);
+
 //  the parameters this path takes (UsageError otherwise)
 void CheckCzParams(const yz_cz_params &p);
 
