@@ -681,7 +681,8 @@ def cz_assembly_bytes(nr: int) -> int:
 
 
 def cz_reference_run(steps: int, threads: int) -> dict:
-    exe = REPO / "oracle" / "_ref" / "yz_probe_cz"
+    #  the reference exactly as it builds (the libm's exp), for its timing
+    exe = REPO / "oracle" / "_ref" / "yz_probe_cz_libm"
     if not exe.exists():
         return {"unavailable": f"{exe.relative_to(REPO)} is not built (make -C oracle ref)"}
     from yuzen_b200 import cases
