@@ -332,14 +332,6 @@ int yz_step_set_graph_loop(yz_step* st, int on);
  * sweeps change it (a better one); the FP64 cycle, the reference's, is not
  * affected.  yuzen_b200.autotune picks them per instance size. */
 int yz_solver_set_tuning(yz_solver* s, int fuse_from, int coarse_lanes, int fine_sweeps);
-/* The finest level's post-smoothing sweeps of the FP32 cycle in one
- * temporally blocked launch (1, the default) or one launch a sweep (0).  The
- * blocked form is taken only where the finest level is a 2-D grid of the
- * 13-point stencil whose every column lies within 3 cells of its row (walls,
- * not periodic seams), and only for 2 to 5 sweeps; its result is the
- * separate sweeps' to the bit. */
-int yz_solver_set_sweep_tiles(yz_solver* s, int on);
-int yz_step_set_sweep_tiles(yz_step* st, int on);
 int yz_step_set_tuning(yz_step* st, int fuse_from, int coarse_lanes, int fine_sweeps);
 /* The energy budget of the film the step holds (WellMixed_ModelBase::EnergyEval,
  * WellMixedModelBase.h:883-893, after EnergyBudget.h): the free energy F and

@@ -15,8 +15,6 @@ import _systems
 import dumpio
 import yuzen_b200 as yz
 
-ROOT = Path(__file__).resolve().parents[1]
-
 pytestmark = pytest.mark.gpu
 GOLDEN = sorted(Path(__file__).parent.joinpath("golden").glob("solve_*.npz"))
 
@@ -423,41 +421,3 @@ def test_tuning_shapes_and_sweeps():
         assert g[0] == 0 and g[2] <= float(d["epsilon"]), (shape, g[:3])
         its[shape] = g[1]
     assert its[(-1, 0, 0)] < its[(-1, 0, 1)], its
-
-
-@pytest.mark.parametrize("N,sweeps", [(384, 0), (384, 2), (61, 3), (200, 5)])
-def test_tiled_post_smoothing_is_the_separate_sweeps(N, sweeps):
-    """yz_solver_set_sweep_tiles: the finest level's post-smoothing sweeps of
-    the FP32 cycle in one temporally blocked launch (KPostSmoothTiled) give
-    the separate launches' solve to the bit: answer, iterations, residual.
-    Grids whose sides are not multiples of the tile (61 + 4, 200 + 4) put
-    partial tiles at the far edges."""
-    d = _systems.film_system(N, seed=3)
-    out = {}
-    for on in (True, False):
-        be = yz.B200Backend()
-        be.SetPrecision(yz.PREC_FP32_CYCLE)
-        be.SetTuning(-1, 0, sweeps)
-        be.SetSweepTiles(on)
-        out[on] = gpu_solve(d, backend=be)
-    assert out[True][0] == 0
-    assert_same(out[True], out[False])
-
-
-def test_tiled_post_smoothing_in_the_step():
-    """The whole 64^2 all-physics step with the FP32 matrix and reused
-    hierarchy: the blocked sweeps and the separate ones end on the same film
-    and concentration to the bit."""
-    import stateio
-    from yuzen_b200 import step as ys
-    f = stateio.load_npz(ROOT / "tests" / "golden" / "step_allphys_64.npz")
-    res = {}
-    for on in (True, False):
-        st = ys.Step(ys.params_from_state(f), f["field_h0"], f["field_c0"], f["field_s0"])
-        st.set_precision(yz.PREC_FP32_MATRIX)
-        st.set_amg_reuse(64)
-        st.set_sweep_tiles(on)
-        st.advance(int(f["steps_done"]))
-        res[on] = st.fields()
-        st.close()
-    assert np.array_equal(res[True][0], res[False][0]) and np.array_equal(res[True][1], res[False][1])

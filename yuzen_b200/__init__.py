@@ -49,7 +49,7 @@ EXPORTED_SYMBOLS = (
     "yz_step_set_tuning",
     # the ConcZ model (seam 3)
     "yz_cz_create", "yz_cz_destroy", "yz_cz_advance", "yz_cz_get_fields", "yz_cz_set_fields", "yz_cz_set_precision",
-    "yz_cz_set_amg_reuse", "yz_cz_set_tuning", "yz_cz_parts", "yz_cz_read", "yz_cz_pattern", "yz_cz_build_pattern", "yz_exp_cr", "yz_solver_set_sweep_tiles", "yz_step_set_sweep_tiles",
+    "yz_cz_set_amg_reuse", "yz_cz_set_tuning", "yz_cz_parts", "yz_cz_read", "yz_cz_pattern", "yz_cz_build_pattern", "yz_exp_cr",
 )
 
 #: the preconditioner's arithmetic (YZ_PREC_* of include/yuzen_b200.h)
@@ -250,12 +250,6 @@ class B200Backend:
         """The BiCGStab loop as one CUDA graph launch (default) or from the
         stream (yz_solver_set_graph_loop)."""
         _check(lib().yz_solver_set_graph_loop(self._h, int(bool(on))), "yz_solver_set_graph_loop")
-
-    def SetSweepTiles(self, on: bool) -> None:
-        """The finest level's post-smoothing sweeps in one launch (yz_solver_set_sweep_tiles)."""
-        L = lib()
-        L.yz_solver_set_sweep_tiles.argtypes = [ctypes.c_void_p, ctypes.c_int]
-        _check(L.yz_solver_set_sweep_tiles(self._h, 1 if on else 0), "yz_solver_set_sweep_tiles")
 
     def SetTuning(self, fuse_from: int = -1, coarse_lanes: int = 0, fine_sweeps: int = 0) -> None:
         """The FP32 V-cycle's shape (yz_solver_set_tuning): the first fused

@@ -896,93 +896,6 @@ __global__ void KPostSmooth(const int *__restrict__ halt, int n, const int *__re
 	}
 }
 
-//--------------------------------------------------------------------------
-//  K post-smoothing sweeps of the finest level in one launch (K <= 5), by
-//  temporal blocking on the 2-D grid the level's rows lie on (row i = y nx +
-//  x): a block takes a tile of TX x TY rows and the halo of 3 K cells around
-//  it (clipped at the domain), loads x there into shared memory once, and
-//  applies sweep s = 1 .. K to the tile grown by 3 (K - s) cells, from one
-//  shared buffer into the other; the last sweep, on the tile itself, writes
-//  xout.  Every column of every row lies within 3 cells of it (the solver
-//  checks this before choosing the kernel), so a sweep reads only rows the
-//  sweep before it wrote.  Each row's sum is KPostSmooth's, in the same
-//  order, so the result is the K launches' to the bit.  lo: the stencil's
-//  offsets in the shared tile (dy * kTileEW + dx).
-//--------------------------------------------------------------------------
-constexpr int kTileX = 64, kTileY = 16, kTileMaxK = 5;
-constexpr int kTileEW = kTileX + 6 * kTileMaxK, kTileEH = kTileY + 6 * kTileMaxK;
-
-struct TileOff
-{
-	int lo[16];
-};
-
-template<class TF, class TX>
-__global__ void __launch_bounds__(256) KPostSmoothTiled(const int *__restrict__ halt, int nx, int ny, int K,
-                                                        const int *__restrict__ ptr, const int *__restrict__ sellOff,
-                                                        Sten sn, TileOff to, const int *__restrict__ col,
-                                                        const float *__restrict__ val, const float *__restrict__ M,
-                                                        const TF *__restrict__ f, const float *__restrict__ xin,
-                                                        TX *__restrict__ xout)
-{
-	if(halt && *halt) return;
-	__shared__ float buf[2][kTileEW * kTileEH];
-	const int ntx = (nx + kTileX - 1) / kTileX, nty = (ny + kTileY - 1) / kTileY;
-	const int H = 3 * K;
-	for(int tile = blockIdx.x; tile < ntx * nty; tile += gridDim.x)
-	{
-		const int x0 = (tile % ntx) * kTileX, y0 = (tile / ntx) * kTileY;
-		const int x1 = min(nx, x0 + kTileX), y1 = min(ny, y0 + kTileY);
-		const int ex0 = max(0, x0 - H), ey0 = max(0, y0 - H);
-		const int ew = min(nx, x1 + H) - ex0, eh = min(ny, y1 + H) - ey0;
-		for(int q = threadIdx.x; q < ew * eh; q += blockDim.x)
-		{
-			const int ly = q / ew, lx = q - ly * ew;
-			buf[0][ly * kTileEW + lx] = xin[(size_t)(ey0 + ly) * nx + ex0 + lx];
-		}
-		__syncthreads();
-		int cur = 0;
-		for(int sw = 1; sw <= K; ++sw)
-		{
-			const int h = 3 * (K - sw);
-			const int rx0 = max(0, x0 - h), ry0 = max(0, y0 - h);
-			const int rw = min(nx, x1 + h) - rx0, rh = min(ny, y1 + h) - ry0;
-			const float *xp = buf[cur];
-			float *xn = buf[cur ^ 1];
-			for(int q = threadIdx.x; q < rw * rh; q += blockDim.x)
-			{
-				const int gy = ry0 + q / rw, gx = rx0 + q % rw;
-				const int i = gy * nx + gx;
-				const int li = (gy - ey0) * kTileEW + (gx - ex0);
-				int st, len, sd;
-				RowRange(ptr, sellOff, i, st, len, sd);
-				float s = 0.0f;
-				if(sn.slice && sn.slice[i >> 5])
-				{
-#pragma unroll
-					for(int k = 0; k < 16; ++k)
-						if(k < len) s = s + val[st + k * sd] * xp[li + to.lo[k]];
-				}
-				else
-				{
-					for(int k = 0, e = st; k < len; ++k, e += sd)
-					{
-						const int c = col[e];
-						const int cy = c / nx, cx = c - cy * nx;
-						s = s + val[e] * xp[(cy - ey0) * kTileEW + (cx - ex0)];
-					}
-				}
-				const float t = (float)f[i] - s;
-				const float v = xp[li] + M[i] * t;
-				if(sw == K) xout[i] = (TX)v;
-				else xn[li] = v;
-			}
-			__syncthreads();
-			cur ^= 1;
-		}
-	}
-}
-
 //  x = inv f, inv row-major: one warp per row, lane l sums j = l, l+32, ...
 //  from 0.0 (coalesced reads of the row), then a pairwise shuffle fold
 template<class T, class TF, class TX>

@@ -277,24 +277,6 @@ int yz_solver_set_tuning(yz_solver *s, int fuse_from, int coarse_lanes, int fine
 	});
 }
 
-int yz_solver_set_sweep_tiles(yz_solver *s, int on)
-{
-	return Guard([&] {
-		if(!s) throw yz::UsageError("yz_solver_set_sweep_tiles: null solver");
-		s->s->SetSweepTiles(on != 0);
-		return 0;
-	});
-}
-
-int yz_step_set_sweep_tiles(yz_step *st, int on)
-{
-	return Guard([&] {
-		if(!st) throw yz::UsageError("yz_step_set_sweep_tiles: null step");
-		st->s->SetSweepTiles(on != 0);
-		return 0;
-	});
-}
-
 int yz_step_set_tuning(yz_step *st, int fuse_from, int coarse_lanes, int fine_sweeps)
 {
 	return Guard([&] {

@@ -428,37 +428,6 @@ void Solver::SetPattern(int n, int nnz, const int *rowptr, const int *scol, cons
 			_sten.len = (int)best.size();
 			for(size_t k = 0; k < best.size(); ++k) _sten.off[k] = best[k];
 		}
-		//  the temporally blocked post-smoothing (KPostSmoothTiled) needs the
-		//  rows on a 2-D grid: the stencil the 13-point one of a row length
-		//  nx (its sorted offsets), and every column of every row within 3
-		//  cells of the row in both directions
-		_tileNx = _tileNy = 0;
-		if(flagged > 0 && best.size() == 13 && best[12] % 2 == 0)
-		{
-			const int g = best[12] / 2;
-			const int want[13] = {-2 * g, -g - 1, -g, -g + 1, -2, -1, 0, 1, 2, g - 1, g, g + 1, 2 * g};
-			bool ok = g >= 8 && n % g == 0;
-			for(int k = 0; k < 13 && ok; ++k) ok = best[(size_t)k] == want[k];
-			for(int i = 0; i < n && ok; ++i)
-			{
-				const int ix = i % g, iy = i / g;
-				for(int k = _hptr[(size_t)i]; k < _hptr[(size_t)i + 1] && ok; ++k)
-				{
-					const int c = scol[k], cx = c % g, cy = c / g;
-					ok = std::abs(cx - ix) <= 3 && std::abs(cy - iy) <= 3;
-				}
-			}
-			if(ok)
-			{
-				_tileNx = g;
-				_tileNy = n / g;
-				for(int k = 0; k < 13; ++k)
-				{
-					const int dy = (int)std::lround((double)best[(size_t)k] / g), dx = best[(size_t)k] - dy * g;
-					_tileLo[k] = dy * kTileEW + dx;
-				}
-			}
-		}
 	}
 	_levels.clear();
 	_levels.emplace_back(new Level());
@@ -792,16 +761,7 @@ void Solver::Cycle32(size_t l, const TF *f, TX *x)
 		{
 			if(la > 1) CoarsePostSmooth(la, n, L.ptr.get(), col, val, L.M32.get(), f, L.xt32.get(), x);
 		}
-		if(la == 1 && l == 0 && SweepTiles() && FineSweeps() >= 2 && FineSweeps() <= kTileMaxK)
-		{
-			//  the finest level's FineSweeps() sweeps in one launch
-			TileOff to;
-			for(int k = 0; k < 16; ++k) to.lo[k] = _tileLo[k];
-			const int tiles = ((_tileNx + kTileX - 1) / kTileX) * ((_tileNy + kTileY - 1) / kTileY);
-			YZ_LAUNCH((KPostSmoothTiled<TF, TX>), std::min(tiles, 148 * 8), 256, 0, _st, Halt(), _tileNx, _tileNy,
-			          FineSweeps(), L.ptr.get(), so, StenOf(l), to, col, val, L.M32.get(), f, L.xt32.get(), x);
-		}
-		else if(la == 1)
+		if(la == 1)
 		{
 			//  FineSweeps() - 1 more SPAI0 sweeps at the finest level before
 			//  the last, float to float (x32 and xt32 in turn)
@@ -920,12 +880,6 @@ int Solver::FineSweeps() const
 	static const char *env = std::getenv("YZ_FINE_SWEEPS");
 	static const int k = env ? std::max(1, std::min(8, std::atoi(env))) : 5;
 	return _fineSweeps > 0 ? _fineSweeps : k;
-}
-
-void Solver::SetSweepTiles(bool on)
-{
-	if(on != _sweepTiles) ++_epoch;   // the loop graph holds the old launches
-	_sweepTiles = on;
 }
 
 void Solver::SetTuning(int fuseFrom, int coarseLanes, int fineSweeps)

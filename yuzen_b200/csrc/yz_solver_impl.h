@@ -78,10 +78,6 @@ public:
 	void SetAmgReuse(int maxSolves);
 	void SetGraphLoop(bool on) { _graphLoop = on; }
 	void SetTuning(int fuseFrom, int coarseLanes, int fineSweeps);
-	//  the finest level's post-smoothing sweeps in one launch where the level
-	//  allows (on by default); off: one launch a sweep
-	void SetSweepTiles(bool on);
-	bool SweepTiles() const { return _tileNx > 0 && _sweepTiles; }
 	int Rebuilds() const { return _rebuilds; }
 	//  the learned preconditioner (not owned): mode 0 off, 1 collect (the
 	//  next `collectSolves` AMG solves feed the network's sample ring with up
@@ -198,11 +194,6 @@ private:
 	//  fused level (-1: YZ_FUSE_FROM or 2; 0: none) and the lanes a row (0:
 	//  by the level's mean row length)
 	int _fuseFrom = -1, _coarseLanes = 0, _fineSweeps = 0;
-	//  the finest level's post-smoothing sweeps in one temporally blocked
-	//  launch (KPostSmoothTiled): the 2-D grid the rows lie on (0: the level
-	//  is not such a grid) and the stencil's offsets in the shared tile
-	int _tileNx = 0, _tileNy = 0, _tileLo[16] = {};
-	bool _sweepTiles = true;
 	LoopGraph _loop[3];
 	bool _graphLoop = true;       // the loop as a CUDA graph (else from the stream)
 	//  Solve's tail, queued behind a graph run: x into the caller's dX

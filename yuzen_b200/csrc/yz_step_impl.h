@@ -90,11 +90,6 @@ public:
 		if(_solverC) _solverC->SetGraphLoop(on);
 		_graphLoop = on;
 	}
-	void SetSweepTiles(bool on)
-	{
-		_solver->SetSweepTiles(on);
-		if(_solverC) _solverC->SetSweepTiles(on);
-	}
 	void SetTuning(int fuseFrom, int coarseLanes, int fineSweeps)
 	{
 		_solver->SetTuning(fuseFrom, coarseLanes, fineSweeps);

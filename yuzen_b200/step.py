@@ -178,12 +178,6 @@ class Step:
         from the stream (yz_step_set_graph_loop)."""
         _check(lib().yz_step_set_graph_loop(self._h, int(bool(on))), "yz_step_set_graph_loop")
 
-    def set_sweep_tiles(self, on: bool) -> None:
-        """The finest level's post-smoothing sweeps in one launch (yz_step_set_sweep_tiles)."""
-        L = lib()
-        L.yz_step_set_sweep_tiles.argtypes = [ctypes.c_void_p, ctypes.c_int]
-        _check(L.yz_step_set_sweep_tiles(self._h, 1 if on else 0), "yz_step_set_sweep_tiles")
-
     def set_tuning(self, fuse_from: int = -1, coarse_lanes: int = 0, fine_sweeps: int = 0) -> None:
         """The FP32 V-cycle's shape (yz_step_set_tuning): the first fused level
         (-1 default, 0 none), the coarse levels' lanes a row (0: by row
