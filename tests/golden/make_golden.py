@@ -334,6 +334,21 @@ CZ_CASES = {
         "Numerics.InitialDt": 0.2, "Numerics.EndTime": 1e6, "Numerics.TimeStepControl.Enable": False,
         "Physics.Centrifugal.Enable": True, "Physics.Centrifugal.RotationAxis": [0.1e-3, -0.2e-3],
     }, True),
+    # the smallest grid the model takes (4 x 4 cells, 3 levels), the VanLeer
+    # limiter and the PowerN evaporation
+    "cz_min_4": ("concz_2d.toml", {
+        "Grid.Nx": 4, "Grid.Ny": 4, "Grid.Nz": 3, "Numerics.MaxSteps": 4,
+        "Numerics.InitialDt": 1.0, "Numerics.EndTime": 1e6,
+        "Numerics.Convection.Concentration": "VanLeer", "Physics.Evaporation.ConcFunc": "PowerN",
+    }, True),
+    # the VanLeer limiter with the Marangoni coupling passes on a periodic
+    # film that is not square, the LTE control on
+    "cz_vanleer_per_20": ("concz_2d.toml", {
+        "Grid.Nx": 20, "Grid.Ny": 12, "Grid.Nz": 6, "Numerics.MaxSteps": 5,
+        "Numerics.InitialDt": 10.0, "Numerics.EndTime": 1e6,
+        "Boundary.XminBC.Type": "Periodic", "Boundary.XmaxBC.Type": "Periodic",
+        "Numerics.Convection.Concentration": "VanLeer", "Physics.VerticalGravity.Enable": True,
+    }, True),
     # 64^2 x 16 levels: more than one AMG level in both solves
     "cz_sym_64": ("concz_2d.toml", {
         "Grid.Nx": 64, "Grid.Ny": 64, "Grid.Nz": 16, "Numerics.MaxSteps": 4,

@@ -12,7 +12,7 @@ import pytest
 import stateio
 
 GOLD = Path(__file__).resolve().parent / "golden"
-CASES = ["cz_sym_16", "cz_per_koren_16", "cz_spin_fixed_18", "cz_sym_64"]
+CASES = ["cz_sym_16", "cz_per_koren_16", "cz_spin_fixed_18", "cz_sym_64", "cz_min_4", "cz_vanleer_per_20"]
 
 
 def load(name):
@@ -77,7 +77,7 @@ def test_fixture_covers_the_paths():
     """What the fixtures exercise: the coupling passes (Marangoni), the
     concentration's own two stages with the limited scheme, the LTE control's
     cuts, a fixed step, more than one AMG level."""
-    a, b, c, big = (load(n) for n in CASES)
+    a, b, c, big = (load(n) for n in CASES[:4])
     assert a["on_sc"] == 1 and a["coupling_passes"] > 0 and a["dt_control"] == 1 and a["dt_end"] < a["dt"]
     assert b["on_sc"] == 0 and b["c_scheme"] == 7 and b["bc"][0] == 1 and b["on_vg"] == 1 and b["on_hg"] == 1
     assert c["dt_control"] == 0 and c["on_cf"] == 1

@@ -21,8 +21,8 @@ import stateio
 
 pytestmark = pytest.mark.gpu
 GOLD = Path(__file__).resolve().parent / "golden"
-CASES = ["cz_sym_16", "cz_per_koren_16", "cz_spin_fixed_18", "cz_sym_64"]
-PARTS_CASES = ["cz_sym_16", "cz_per_koren_16", "cz_spin_fixed_18"]
+CASES = ["cz_sym_16", "cz_per_koren_16", "cz_spin_fixed_18", "cz_sym_64", "cz_min_4", "cz_vanleer_per_20"]
+PARTS_CASES = ["cz_sym_16", "cz_per_koren_16", "cz_spin_fixed_18", "cz_min_4", "cz_vanleer_per_20"]
 
 
 def load(name):
