@@ -69,7 +69,7 @@ NCU_TRAFFIC = {
     # (50,359,808 B); the pass's two smaller kernels (KFaceProps, KCellPi) were
     # not captured
     ("assembly", "allphys_512"): 180615424 + 50359808,
-    # the ConcZ concentration assembly (profiles/KCzAssembleC_cz_256.md)
+    # the ConcZ concentration assembly (one capture of its fourth launch on cz_256)
     ("KCzAssembleC", "cz_256"): 41707776 + 136976896,
 }
 
