@@ -105,6 +105,18 @@ def learned_config():
                                   holdout=4, cap_factor=3.0, seed=1, activation=0)
 
 
+def cz_learned_config():
+    """The ConcZ learned arm's settings: the first four film solves (the
+    predictor and corrector of two steps) collect up to eight pairs each, the
+    film solve after them (the third step's predictor, inside the steps
+    checked against the reference) trains the network (200 Adam steps of four
+    pairs, four held out), and every later film solve tries it first within
+    three times the last SA-AMG solve's iterations."""
+    from yuzen_b200 import learned
+    return learned.default_config(collect_solves=4, samples_per_solve=8, capacity=32, train_iters=200, batch=4,
+                                  holdout=4, cap_factor=3.0, seed=1, activation=0)
+
+
 def spmv_alpha_bytes(n: int, nnz: int) -> int:
     return 12 * nnz + 4 * (n + 1) + 3 * 8 * n
 
@@ -728,7 +740,9 @@ def run_cz_arm(a) -> None:
     fx = dict(np.load(fxp)) if fxp.exists() else None
     hpin = torch.empty(n2, dtype=torch.float64, pin_memory=True).numpy()
     cpin = torch.empty(n3, dtype=torch.float64, pin_memory=True).numpy()
-    arms_cz = {"fp64": (0, 0), "fp32_reuse": (1, 64), "fp32m_reuse": (2, 64)}
+    #  arm -> (arithmetic of the solves, AMG hierarchy reuse); the learned
+    #  arm is fp32_reuse with the network tried first on the film's solves
+    arms_cz = {"fp64": (0, 0), "fp32_reuse": (1, 64), "fp32m_reuse": (2, 64), "learned": (1, 64)}
     names = [x for x in a.arms.split(",") if x in arms_cz] or ["fp64", "fp32_reuse"]
 
     def rel(x, y) -> float:
@@ -740,11 +754,27 @@ def run_cz_arm(a) -> None:
                        device=local)
         m.set_precision(prec)
         m.set_amg_reuse(reuse)
+        if name == "learned":
+            m.set_learned(cz_learned_config())
         out = {"total_ms": 0.0, "wall_s": 0.0, "linear": 0, "conc_iters": 0, "coupling": 0, "launches": 0,
                "per_step": []}
+        L = {"solves": 0, "fallbacks": 0, "iterations": 0, "train_ms": 0.0, "warmup_solves": 0,
+             "warmup_fallbacks": 0}
+
+        def note_learned(r, timed):
+            if name != "learned":
+                return
+            pre = "" if timed else "warmup_"
+            L[pre + "solves"] += r["learned_solves"]
+            L[pre + "fallbacks"] += r["learned_fallbacks"]
+            if timed:
+                L["iterations"] += r["learned_iterations"]
+            L["train_ms"] += r["learned_train_ms"]
+            L["val_err"], L["samples"] = r["learned_val_err"], r["learned_samples"]
         done = 0
         if fx is not None:
             r = m.advance(int(fx["steps_done"]))
+            note_learned(r, False)
             done = int(fx["steps_done"])
             h, c = m.fields()
             nx, ny, nz = params.nx, params.ny, params.nz
@@ -752,7 +782,7 @@ def run_cz_arm(a) -> None:
             out["c_colsum_err_vs_oracle"] = rel(c.reshape(nz, ny, nx)[2:-2].sum(axis=0).ravel(), fx["c1_colsum"])
             out["t_err_vs_oracle"] = abs(r["time"] - float(fx["t_end"])) / float(fx["t_end"])
         if a.warmup > done:
-            m.advance(a.warmup - done)
+            note_learned(m.advance(a.warmup - done), False)
             done = a.warmup
         out["warmup"] = done
         m.fields_into(hpin, cpin)
@@ -773,6 +803,9 @@ def run_cz_arm(a) -> None:
             out["conc_iters"] += r["conc_iterations"]
             out["coupling"] += r["coupling_passes"]
             out["launches"] += r["launches"]
+            note_learned(r, True)
+        if name == "learned":
+            out["learned"] = L
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -837,7 +870,8 @@ def run_cz_arm(a) -> None:
         line = {
             "metric": CZ_METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": head["max_ms"] / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if head_name == "fp64" else "f64 (V-cycle f32)",
+            "vs_baseline": None, "dtype": {"fp64": "f64", "learned": "f64 (V-cycle f32, bf16 network with f32 "
+                                                               "accumulation)"}.get(head_name, "f64 (V-cycle f32)"),
             "data": "synthetic (seeded: yuzen_b200.cases.cz_bumps)",
             "config": {"workload": "cz_256", "grid": [256, 256, 16], "arm": head_name, "l2": "flushed (256 MiB)",
                        "arms": {x: {k: v for k, v in arms[x].items() if k != "model"} | {"steps_per_s": arms[x]["value"]}

@@ -535,6 +535,13 @@ typedef struct yz_cz_stats
 	double time, dt;              /* the clock and DT().now after the call */
 	double device_ms;             /* the call on the model's stream (CUDA events) */
 	long long launches;           /* kernels the call launched */
+	/* the learned preconditioner of the film's solves (yz_cz_set_learned),
+	 * for this call: film solves it converged, fallbacks to SA-AMG, its
+	 * iterations, the training pairs held, the training's device time, the
+	 * held-out error against the V-cycle and the last training loss (-1:
+	 * not trained) */
+	int    learned_solves, learned_fallbacks, learned_iterations, learned_samples;
+	double learned_train_ms, learned_val_err, learned_loss;
 } yz_cz_stats;
 
 /* Build the model: the coordinates of the cell centres (xc, yc) and of the
@@ -559,6 +566,13 @@ int yz_cz_set_amg_reuse(yz_cz* z, int max_solves);
 /* The FP32 V-cycle's launch shape of both equations' solves
  * (yz_solver_set_tuning). */
 int yz_cz_set_tuning(yz_cz* z, int fuse_from, int coarse_lanes, int fine_sweeps);
+/* The film's solves with a learned preconditioner of their own, as
+ * yz_step_set_learned gives the well-mixed film's: the first collect_solves
+ * SA-AMG film solves collect training pairs, the film solve after them
+ * trains the network, and every later film solve tries it first within
+ * cap_factor x the last SA-AMG solve's iterations.  The concentration's
+ * solves keep SA-AMG.  Null: off. */
+int yz_cz_set_learned(yz_cz* z, const yz_learned_cfg* cfg);
 /* The pieces of one step on the present state, as the reference forms them
  * (its parity test): the film's assembly at the step's dt, its conservative
  * update with the film unchanged, the velocity and the concentration's

@@ -120,3 +120,32 @@ def test_bench_size_run_matches_the_reference():
     assert eh <= 1e-10 and ecs <= 1e-10 and esm <= 1e-10, (eh, ecs, esm)
     el = np.linalg.norm(h - ref["h1_libm"]) / np.linalg.norm(ref["h1_libm"])
     assert el <= 1e-8, el
+
+
+def test_learned_film_solves_meet_the_bar():
+    """The film's solves with the learned preconditioner (yz_cz_set_learned)
+    on the 64^2 x 16 film with the LTE control: the first four SA-AMG film
+    solves collect up to eight (residual, V-cycle) pairs each, the film solve
+    after them trains the network, and the later film solves try it first
+    with SA-AMG as the fallback.  The run keeps the reference's steps, its
+    clock to 1e-8 and h and c within 1e-8 of the reference's run; the stats
+    show the collection, the training and the network's solves or fallbacks;
+    the concentration's solves are untouched (their SPAI0 / SA-AMG path)."""
+    from yuzen_b200 import learned as yl
+    d = load("cz_sym_64")
+    m = model(d)
+    m.set_learned(yl.default_config(collect_solves=4, samples_per_solve=8, capacity=32, train_iters=150, batch=4,
+                                    holdout=4, cap_factor=3.0))
+    st = m.advance(int(d["steps_done"]))
+    h, c = m.fields()
+    m.close()
+    assert st["steps"] == d["steps_done"]
+    assert abs(st["time"] - d["t_end"]) <= 1e-8 * abs(d["t_end"])
+    eh = np.linalg.norm(h - d["h1"]) / np.linalg.norm(d["h1"])
+    ec = np.linalg.norm(c - d["c1"]) / np.linalg.norm(d["c1"])
+    assert eh <= 1e-8 and ec <= 1e-8, (eh, ec)
+    assert st["learned_samples"] >= 8
+    assert st["learned_train_ms"] > 0 and st["learned_loss"] >= 0
+    assert st["learned_solves"] + st["learned_fallbacks"] >= 1, st
+    print("learned film solves:", {k: st[k] for k in st if k.startswith("learned")},
+          "film iterations", st["linear_iterations"], "reference", d["linear_iterations"])

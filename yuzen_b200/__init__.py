@@ -49,7 +49,7 @@ EXPORTED_SYMBOLS = (
     "yz_step_set_tuning",
     # the ConcZ model (seam 3)
     "yz_cz_create", "yz_cz_destroy", "yz_cz_advance", "yz_cz_get_fields", "yz_cz_set_fields", "yz_cz_set_precision",
-    "yz_cz_set_amg_reuse", "yz_cz_set_tuning", "yz_cz_parts", "yz_cz_read", "yz_cz_pattern", "yz_cz_build_pattern", "yz_exp_cr",
+    "yz_cz_set_amg_reuse", "yz_cz_set_tuning", "yz_cz_set_learned", "yz_cz_parts", "yz_cz_read", "yz_cz_pattern", "yz_cz_build_pattern", "yz_exp_cr",
 )
 
 #: the preconditioner's arithmetic (YZ_PREC_* of include/yuzen_b200.h)

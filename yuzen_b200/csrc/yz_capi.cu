@@ -650,6 +650,15 @@ int yz_cz_set_tuning(yz_cz *z, int fuse_from, int coarse_lanes, int fine_sweeps)
 	});
 }
 
+int yz_cz_set_learned(yz_cz *z, const yz_learned_cfg *cfg)
+{
+	return Guard([&] {
+		if(!z) throw yz::UsageError("yz_cz_set_learned: null model");
+		z->z->SetLearned(cfg);
+		return 0;
+	});
+}
+
 int yz_cz_set_amg_reuse(yz_cz *z, int max_solves)
 {
 	return Guard([&] {

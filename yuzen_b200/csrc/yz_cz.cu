@@ -1510,6 +1510,7 @@ CzStep::~CzStep()
 	if(_st) cudaStreamSynchronize(_st);
 	_solverH.reset();
 	_solverC.reset();
+	_learned.reset();
 	if(_st) cudaStreamDestroy(_st);
 }
 
@@ -1571,6 +1572,13 @@ void CzStep::SolveStageH(const double *fH, const double *fC, double dt, int &ite
 	}
 	iter = 0;
 	resid = 0;
+	//  the learned preconditioner reads the stage's film as a feature, and is
+	//  trained once the solves that collect its pairs are done
+	if(_learned)
+	{
+		_solverH->SetAux(fH);
+		if(!_learned->Trained() && _solverH->CollectLeft() == 0) TrainLearned();
+	}
 	{
 		YZ_PROF("h.linsolve", _st);
 		ch = _solverH->Solve(_p.h_lin, _IA.get(), _rhs.get(), _hNew.get(), iter, resid);
@@ -2016,6 +2024,8 @@ void CzStep::Advance(int nsteps, yz_cz_stats &stats)
 	YZ_CUDA(cudaSetDevice(_device));
 	std::memset(&stats, 0, sizeof(stats));
 	const long long l0 = t_launches, s0 = _solves, c0 = _concIters;
+	const Solver::LearnedStats ls0 = _solverH->LStats();
+	_lTrainMs = 0.0;
 	cudaEvent_t eA, eB;
 	YZ_CUDA(cudaEventCreate(&eA));
 	YZ_CUDA(cudaEventCreate(&eB));
@@ -2096,6 +2106,14 @@ void CzStep::Advance(int nsteps, yz_cz_stats &stats)
 	stats.conc_iterations = (int)(_concIters - c0);
 	stats.launches = t_launches - l0;
 	_launches += stats.launches;
+	const Solver::LearnedStats &ls1 = _solverH->LStats();
+	stats.learned_solves = ls1.solves - ls0.solves;
+	stats.learned_fallbacks = ls1.fallbacks - ls0.fallbacks;
+	stats.learned_iterations = ls1.iterations - ls0.iterations;
+	stats.learned_samples = _learned ? _learned->Samples() : 0;
+	stats.learned_train_ms = _lTrainMs;
+	stats.learned_val_err = _lValErr;
+	stats.learned_loss = _lLoss;
 }
 
 void CzStep::GetFields(double *h, double *c)
@@ -2123,6 +2141,46 @@ void CzStep::SetFields(const double *h, const double *c)
 		Copy(_fC.get(), _cNew.get(), (size_t)_n3);
 		Copy(_tC.get(), _cNew.get(), (size_t)_n3);
 	}
+}
+
+void CzStep::SetLearned(const yz_learned_cfg *cfg)
+{
+	YZ_CUDA(cudaSetDevice(_device));
+	_solverH->SetLearned(nullptr, 0, 0, 0, 1.0);
+	_learned.reset();
+	_lValErr = -1.0;
+	_lLoss = -1.0;
+	if(!cfg) return;
+	if(cfg->collect_solves < 1 || cfg->samples_per_solve < 1 || cfg->capacity < 2 || cfg->train_iters < 0 ||
+	   cfg->batch < 1 || !(cfg->lr > 0) || cfg->holdout < 0 || !(cfg->cap_factor > 0) ||
+	   (cfg->activation != 0 && cfg->activation != 1))
+		throw UsageError("set_learned: collect_solves, samples_per_solve, batch >= 1, capacity >= 2, lr and "
+		                 "cap_factor > 0, train_iters and holdout >= 0");
+	_lcfg = *cfg;
+	_learned.reset(new Learned(_device, _p.nx, _p.ny, cfg->capacity, cfg->seed, cfg->activation));
+	_solverH->SetLearned(_learned.get(), 1, cfg->collect_solves, cfg->samples_per_solve, cfg->cap_factor);
+}
+
+//  Adam on the pairs the film's solves collected; then the film's solves try
+//  the network first
+void CzStep::TrainLearned()
+{
+	cudaEvent_t e0, e1;
+	YZ_CUDA(cudaEventCreate(&e0));
+	YZ_CUDA(cudaEventCreate(&e1));
+	YZ_CUDA(cudaEventRecord(e0, _st));
+	const int hold = std::min(_lcfg.holdout, std::max(0, _learned->Samples() - 1));
+	double val = -1.0;
+	_lLoss = _learned->Train(_lcfg.train_iters, _lcfg.batch, _lcfg.lr, hold, &val, _st);
+	_lValErr = val;
+	YZ_CUDA(cudaEventRecord(e1, _st));
+	YZ_CUDA(cudaEventSynchronize(e1));
+	float ms = 0;
+	YZ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	_lTrainMs += ms;
+	_solverH->SetLearned(_learned.get(), 2, 0, 0, _lcfg.cap_factor);
 }
 
 void CzStep::SetPrecision(int precision)

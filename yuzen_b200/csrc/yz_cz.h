@@ -36,6 +36,7 @@
 #include "yz_common.cuh"
 #include "yz_physics.cuh"
 #include "yz_solver_impl.h"
+#include "yz_learned.h"
 
 #include <map>
 #include <memory>
@@ -82,6 +83,7 @@ public:
 	void SetPrecision(int precision);
 	void SetAmgReuse(int maxSolves);
 	void SetTuning(int fuseFrom, int coarseLanes, int fineSweeps);
+	void SetLearned(const yz_learned_cfg *cfg);
 	void Parts();
 	long long Read(const std::string &name, double *out, long long cap);
 	int Pattern(int which, int *rowptr, int *col, int *bc) const;
@@ -107,6 +109,7 @@ private:
 	int SolveAtMidpointC(const double *fH, const double *cmid, double dt, int &iter, double &resid);
 	int SettleLimiterC(const double *fH, double dt, int &iter, double &resid);
 	bool AfterTrial(double dt, yz_cz_stats &stats);
+	void TrainLearned();
 	void RedistributeExcess();
 	void RedistributeDeficit();
 	double Lte(double dt);
@@ -124,6 +127,10 @@ private:
 	std::vector<int> _rowptrH, _colH, _bcH, _rowptrC, _colC, _bcC;
 	std::unique_ptr<Solver> _solverH, _solverC;
 	long long _launches = 0;
+	//  the learned preconditioner of the film's solves
+	std::unique_ptr<Learned> _learned;
+	yz_learned_cfg _lcfg = {};
+	double _lValErr = -1.0, _lLoss = -1.0, _lTrainMs = 0.0;
 
 	DBuf<double> _xc, _xf, _yc, _yf;
 	DBuf<int> _dRowptrH, _dColH, _dRowptrC, _dColC;

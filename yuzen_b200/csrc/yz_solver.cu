@@ -1087,7 +1087,7 @@ void Solver::RunIterations(int kind)
 	Scal *sc = _sc.get();
 	//  an AMG run that feeds the network's sample ring: after each of its
 	//  first iterations, the residual r and the V-cycle's answer to it
-	const bool collect = kind == kPrecAmg && _learned && _collectLeft > 0 && _perSolve > 0;
+	const bool collect = kind == kPrecAmg && _learned && _filmSolve && _collectLeft > 0 && _perSolve > 0;
 	int hooks = 0;
 	auto hook = [&]() {
 		if(!collect || hooks >= _perSolve) return;
@@ -1284,6 +1284,11 @@ int Solver::Solve(const yz_settings &set, const double *dValues, const double *d
 		YZ_CUDA(cudaMemcpyAsync(_x.get(), dX, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
 		YZ_CUDA(cudaMemcpyAsync(_x0.get(), dX, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, _st));
 	}
+	//  a film solve that collects training pairs stores them with the
+	//  features of its own system (the matrix diagonal and the film height),
+	//  those the network reads when it is applied to such a system
+	_filmSolve = !set.conc && set.precondition == 2;
+	if(_learned && _filmSolve && _collectLeft > 0 && _perSolve > 0) _learned->SetAux(dValues, L0.ptr.get(), _aux, _st);
 	YZ_CUDA(cudaEventRecord(_ev0, _st));
 	//  a run in graph form copies its answer to dX behind the loop (the
 	//  last run's copy is the one that stays)

@@ -204,6 +204,7 @@ private:
 	//  the learned preconditioner
 	Learned *_learned = nullptr;
 	int _learnedMode = 0, _collectLeft = 0, _perSolve = 0, _collected = 0;
+	bool _filmSolve = false;        // the present solve is one the network serves (a film's, SA-AMG)
 	double _capFactor = 1.0;
 	const double *_aux = nullptr;
 	int _amgIters = 0;              // iterations of the last SA-AMG solve (the plain path's count)

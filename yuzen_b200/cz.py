@@ -57,6 +57,9 @@ class CzStats(ctypes.Structure):
         ("coupling_passes", ctypes.c_int), ("retries", ctypes.c_int), ("solves", ctypes.c_int),
         ("time", ctypes.c_double), ("dt", ctypes.c_double), ("device_ms", ctypes.c_double),
         ("launches", ctypes.c_longlong),
+        ("learned_solves", ctypes.c_int), ("learned_fallbacks", ctypes.c_int), ("learned_iterations", ctypes.c_int),
+        ("learned_samples", ctypes.c_int), ("learned_train_ms", ctypes.c_double), ("learned_val_err", ctypes.c_double),
+        ("learned_loss", ctypes.c_double),
     ]
 
 
@@ -179,6 +182,13 @@ class CzModel:
     def set_tuning(self, fuse_from: int, coarse_lanes: int, fine_sweeps: int) -> None:
         _check(lib().yz_cz_set_tuning(self._h, int(fuse_from), int(coarse_lanes), int(fine_sweeps)),
                "yz_cz_set_tuning")
+
+    def set_learned(self, cfg=None) -> None:
+        """The learned preconditioner of the film's solves
+        (yuzen_b200.learned.LearnedConfig, or default_config(); None: off)."""
+        from . import learned
+        L = learned._bind()
+        _check(L.yz_cz_set_learned(self._h, ctypes.byref(cfg) if cfg is not None else None), "yz_cz_set_learned")
 
     def parts(self) -> dict:
         """The pieces of one step on the present state (yz_cz_parts), by the

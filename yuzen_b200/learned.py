@@ -60,6 +60,7 @@ def _bind():
     L.yz_solver_set_aux.argtypes = [vp, vp]
     L.yz_solver_learned_stats.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 4
     L.yz_step_set_learned.argtypes = [vp, ctypes.POINTER(LearnedConfig)]
+    L.yz_cz_set_learned.argtypes = [vp, ctypes.POINTER(LearnedConfig)]
     L.yz_conv3x3.argtypes = [ctypes.c_int] * 7 + [_f32p, _f32p, _f32p, _f32p]
     _BOUND = True
     return L
