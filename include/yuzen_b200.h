@@ -426,6 +426,11 @@ int yz_unet_loss_grad(yz_unet* u, const float* feat3, const float* target, doubl
  * the matrix diagonal and the film height (null: none), n each. */
 int yz_unet_add_sample(yz_unet* u, const double* r, const double* z, const double* diag, const double* h);
 int yz_unet_samples(const yz_unet* u);
+/* Slot k (0 <= k < yz_unet_samples) of the pair ring, 4 x n floats: r/rms(r),
+ * z/rms(r) and the two feature maps the pair was stored with (the diagonal's
+ * log10|a_ii| / 4 and the film's log10 h / 2 + 1, 0 without a film); *valid 0
+ * for a slot marked unused. */
+int yz_unet_get_sample(yz_unet* u, int k, float* out, int* valid);
 /* Adam over the pairs held, the last `holdout` kept out: iters steps of
  * `batch` pairs at learning rate lr; the last step's mean loss, and the
  * held-out relative error ||N r - V r|| / ||V r|| (-1 without held-out pairs). */

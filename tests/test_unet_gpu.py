@@ -154,6 +154,34 @@ def _collect(net, films, s, per_solve):
 S = yz.LinearSolverSettings(2, True, 3000, 1e-10, False)
 
 
+def test_collected_pairs_carry_their_systems_features():
+    """A pair the solver collects from its own SA-AMG solve holds the feature
+    maps of that solve's system -- f1 = log10|a_ii| / 4 of the unscaled
+    matrix's diagonal (the first entry of each row in storage order) and
+    f2 = log10 h / 2 + 1 of the film given -- the maps the network reads when
+    it is applied to such a system."""
+    import torch
+    d = _step_films(64, (1.0,), (0,))[0]
+    net = yl.UNet(68, 68, capacity=4, seed=1)
+    be = yz.B200Backend()
+    hd = torch.tensor(d["h"], dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    be.SetAux(hd.data_ptr())
+    be.SetLearned(net, 1, collect_solves=1, per_solve=2)
+    x = np.zeros(d["n"])
+    ret, _, _ = be.Solve(S, _pattern(d), d["values"], d["rhs"], x)
+    assert ret == 0 and net.samples() >= 1
+    diag = np.abs(d["values"][d["rowptr"][:-1]])
+    f1 = (np.log10(np.maximum(diag, 1e-30)) * 0.25).astype(np.float32)
+    f2 = (np.log10(np.maximum(d["h"], 1e-30)) * 0.5 + 1.0).astype(np.float32)
+    s = net.sample(0)
+    assert s["valid"]
+    assert np.abs(f1).max() > 1e-3 and np.abs(f2).max() > 0.5
+    np.testing.assert_allclose(s["f1"], f1, rtol=1e-6, atol=1e-6)
+    np.testing.assert_allclose(s["f2"], f2, rtol=1e-6, atol=1e-6)
+    del hd
+
+
 def test_training_lowers_the_loss():
     """Pairs the solver collects from its SA-AMG solves of twelve film
     systems of the 64^2 all-physics film; 300 Adam steps on the device lower

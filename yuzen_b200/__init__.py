@@ -42,7 +42,7 @@ EXPORTED_SYMBOLS = (
     "yz_step_set_energy",
     # the learned preconditioner
     "yz_unet_create", "yz_unet_destroy", "yz_unet_param_count", "yz_unet_get_params", "yz_unet_set_params",
-    "yz_unet_forward", "yz_unet_loss_grad", "yz_unet_add_sample", "yz_unet_samples", "yz_unet_train",
+    "yz_unet_forward", "yz_unet_loss_grad", "yz_unet_add_sample", "yz_unet_samples", "yz_unet_get_sample", "yz_unet_train",
     "yz_unet_apply", "yz_solver_set_learned", "yz_solver_set_aux", "yz_solver_learned_stats",
     "yz_step_set_learned", "yz_conv3x3", "yz_fault_inject", "yz_step_state_size", "yz_step_get_state",
     "yz_step_set_state", "yz_profile_enabled", "yz_profile_entry", "yz_profile_reset", "yz_solver_set_tuning",

@@ -476,6 +476,16 @@ int yz_unet_add_sample(yz_unet *u, const double *r, const double *z, const doubl
 
 int yz_unet_samples(const yz_unet *u) { return u ? u->u->Samples() : -1; }
 
+int yz_unet_get_sample(yz_unet *u, int k, float *out, int *valid)
+{
+	return Guard([&] {
+		if(!u || !out) throw yz::UsageError("yz_unet_get_sample: null argument");
+		const bool v = u->u->GetSample(k, out, 0);
+		if(valid) *valid = v ? 1 : 0;
+		return 0;
+	});
+}
+
 int yz_unet_train(yz_unet *u, int iters, int batch, float lr, int holdout, double *loss, double *val_err)
 {
 	return Guard([&] {

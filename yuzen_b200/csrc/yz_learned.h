@@ -83,6 +83,10 @@ public:
 	//  parameters (FP32 master copy, ParamCount values)
 	void GetParams(float *out, cudaStream_t st);
 	void SetParams(const float *in, cudaStream_t st);
+	//  slot k of the sample ring (0 <= k < Samples()): r / rms(r), z / rms(r)
+	//  and the two feature maps, n floats each; returns whether the slot holds
+	//  a pair (a pair queued after its run had ended is marked unused)
+	bool GetSample(int k, float *out, cudaStream_t st);
 	//  one sample's loss and the gradient of it w.r.t. every parameter
 	//  (features and target as normalised host maps over the n rows; the
 	//  target in units of the targets' scale)

@@ -1104,6 +1104,17 @@ void Learned::GetParams(float *out, cudaStream_t st)
 	YZ_CUDA(cudaStreamSynchronize(st));
 }
 
+bool Learned::GetSample(int k, float *out, cudaStream_t st)
+{
+	if(k < 0 || k >= Samples()) throw UsageError("unet: no sample in that slot");
+	int valid = 0;
+	YZ_CUDA(cudaMemcpyAsync(out, _ring.get() + (size_t)k * 4 * _n, (size_t)4 * _n * sizeof(float),
+	                        cudaMemcpyDeviceToHost, st));
+	YZ_CUDA(cudaMemcpyAsync(&valid, _valid.get() + k, sizeof(int), cudaMemcpyDeviceToHost, st));
+	YZ_CUDA(cudaStreamSynchronize(st));
+	return valid != 0;
+}
+
 void Learned::SetParams(const float *in, cudaStream_t st)
 {
 	_param.upload(in, _np, st);

@@ -53,6 +53,7 @@ def _bind():
     L.yz_unet_loss_grad.argtypes = [vp, _f32p, _f32p, ctypes.POINTER(ctypes.c_double), _f32p]
     L.yz_unet_add_sample.argtypes = [vp] + [ctypes.POINTER(ctypes.c_double)] * 4
     L.yz_unet_samples.argtypes = [vp]
+    L.yz_unet_get_sample.argtypes = [vp, ctypes.c_int, _f32p, ctypes.POINTER(ctypes.c_int)]
     L.yz_unet_train.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     L.yz_unet_apply.argtypes = [vp, vp, vp, vp, vp, vp, vp]
@@ -123,6 +124,16 @@ class UNet:
 
     def samples(self) -> int:
         return int(lib().yz_unet_samples(self._h))
+
+    def sample(self, k: int) -> dict:
+        """Slot k of the pair ring: r and z scaled by 1/rms(r), the two
+        feature maps it was stored with, and whether the slot holds a pair."""
+        out = np.zeros(4 * self.n, np.float32)
+        valid = ctypes.c_int()
+        _check(lib().yz_unet_get_sample(self._h, int(k), out.ctypes.data_as(_f32p), ctypes.byref(valid)),
+               "yz_unet_get_sample")
+        r, z, f1, f2 = out.reshape(4, self.n)
+        return {"r": r, "z": z, "f1": f1, "f2": f2, "valid": bool(valid.value)}
 
     def train(self, iters: int, batch: int = 4, lr: float = 1e-3, holdout: int = 0):
         loss, val = ctypes.c_double(), ctypes.c_double()
