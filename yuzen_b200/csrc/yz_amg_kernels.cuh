@@ -807,6 +807,7 @@ __global__ void KPreSmoothResidual(const int *__restrict__ halt, int n, const in
                                    const T *__restrict__ val, const T *__restrict__ M, const TF *__restrict__ f,
                                    TX *__restrict__ x, T *__restrict__ t)
 {
+	PdlEntry();
 	if(halt && *halt) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
@@ -823,6 +824,7 @@ template<class T, class TF, class TX>
 __global__ void KPreSmooth(const int *__restrict__ halt, int n, const T *__restrict__ M, const TF *__restrict__ f,
                            TX *__restrict__ x)
 {
+	PdlEntry();
 	if(halt && *halt) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = (TX)(M[i] * (T)f[i]);
 }
@@ -845,6 +847,7 @@ template<class T>
 __global__ void KRestrict(const int *__restrict__ halt, int n, const int *__restrict__ ptr, const int *__restrict__ col,
                           const T *__restrict__ val, const T *__restrict__ t, T *__restrict__ y)
 {
+	PdlEntry();
 	if(halt && *halt) return;
 	const int lane = threadIdx.x & 31, q = lane & 3;
 	const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -870,6 +873,7 @@ __global__ void KProlong(const int *__restrict__ halt, int n, const int *__restr
                          const T *__restrict__ pval, const T *__restrict__ xc, const T *__restrict__ x,
                          T *__restrict__ xout)
 {
+	PdlEntry();
 	if(halt && *halt) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
@@ -885,6 +889,7 @@ __global__ void KPostSmooth(const int *__restrict__ halt, int n, const int *__re
                             const T *__restrict__ val, const T *__restrict__ M, const TF *__restrict__ f,
                             const T *__restrict__ x, TX *__restrict__ xout)
 {
+	PdlEntry();
 	if(halt && *halt) return;
 	for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
@@ -902,6 +907,7 @@ template<class T, class TF, class TX>
 __global__ void KDenseMV(const int *__restrict__ halt, int n, const T *__restrict__ inv, const TF *__restrict__ f,
                          TX *__restrict__ x)
 {
+	PdlEntry();
 	if(halt && *halt) return;
 	const int lane = threadIdx.x & 31;
 	const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -951,6 +957,7 @@ __global__ void KPreSmoothResidualL(const int *__restrict__ halt, int n, const i
                                     const int *__restrict__ col, const T *__restrict__ val, const T *__restrict__ M,
                                     const T *__restrict__ f, T *__restrict__ x, T *__restrict__ t)
 {
+	PdlEntry();
 	if(halt && *halt) return;
 	YZ_LANE_LOOP(L)
 	{
@@ -972,6 +979,7 @@ __global__ void KPostSmoothL(const int *__restrict__ halt, int n, const int *__r
                              const int *__restrict__ col, const T *__restrict__ val, const T *__restrict__ M,
                              const T *__restrict__ f, const T *__restrict__ x, T *__restrict__ xout)
 {
+	PdlEntry();
 	if(halt && *halt) return;
 	YZ_LANE_LOOP(L)
 	{
@@ -988,6 +996,7 @@ __global__ void KProlongL(const int *__restrict__ halt, int n, const int *__rest
                           const T *__restrict__ pval, const T *__restrict__ xc, const T *__restrict__ x,
                           T *__restrict__ xout)
 {
+	PdlEntry();
 	if(halt && *halt) return;
 	YZ_LANE_LOOP(L)
 	{
@@ -1022,6 +1031,7 @@ __global__ void KDownFused(const int *__restrict__ halt, int n, const int *__res
                            const int *__restrict__ col, const T *__restrict__ val, const T *__restrict__ M,
                            const T *__restrict__ f, T *__restrict__ fc)
 {
+	PdlEntry();
 	if(halt && *halt) return;
 	YZ_LANE_LOOP(L)
 	{
@@ -1047,6 +1057,7 @@ __global__ void KUpFused(const int *__restrict__ halt, int n, const int *__restr
                          const int *__restrict__ pcol, const T *__restrict__ pval, const T *__restrict__ f,
                          const T *__restrict__ xc, T *__restrict__ x)
 {
+	PdlEntry();
 	if(halt && *halt) return;
 	auto xt = [&](int k) {
 		T s = T(0);

@@ -1,6 +1,8 @@
 // yz_common.cu -- launch accounting, the last-error string and the integer scan.
 #include "yz_common.cuh"
 
+#include <cstdlib>
+
 #include <mutex>
 
 namespace yz {
@@ -24,6 +26,13 @@ bool TimedKernel(const char *name)
 	if(!g_timeOn.load(std::memory_order_acquire)) return false;
 	std::lock_guard<std::mutex> lk(g_timeMutex);
 	return !g_timeName.empty() && g_timeName == name;
+}
+
+bool PdlOn()
+{
+	static const char *env = std::getenv("YZ_PDL");
+	static const bool on = env && env[0] == '1';
+	return on;
 }
 
 bool TimingActive() { return g_timeOn.load(std::memory_order_acquire); }

@@ -74,6 +74,47 @@ void TimeDropLast(long long k);   // forget the last k of them
 		::yz::Check(cudaGetLastError(), #kernel);                                 \
 	} while(0)
 
+//  Programmatic dependent launch for the chains of short kernels in the
+//  BiCGStab loop and the V-cycle: a kernel launched by YZ_LAUNCH_PDL may be
+//  scheduled while the kernel before it on the stream drains.  Such a kernel
+//  begins with PdlEntry(): griddepcontrol.wait holds every thread until the
+//  kernels it depends on have completed and their memory is visible (so its
+//  reads and writes are those of a plain launch), then launch_dependents lets
+//  the next kernel be scheduled.  Without the launch attribute both are no-ops.
+//  YZ_PDL=0 in the environment launches these kernels plainly.
+bool PdlOn();
+__device__ __forceinline__ void PdlEntry()
+{
+#if defined(__CUDA_ARCH__)
+	asm volatile("griddepcontrol.wait;" ::: "memory");
+	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+#define YZ_LAUNCH_PDL(kernel, grid, block, smem, strm, ...)                     \
+	do {                                                                          \
+		const bool yzTimed_ = ::yz::TimedKernel(#kernel);                         \
+		if(yzTimed_) ::yz::TimeBegin(strm);                                     \
+		if(::yz::PdlOn())                                                         \
+		{                                                                         \
+			cudaLaunchConfig_t yzCfg_ = {};                                       \
+			yzCfg_.gridDim = dim3(grid);                                          \
+			yzCfg_.blockDim = dim3(block);                                        \
+			yzCfg_.dynamicSmemBytes = (smem);                                     \
+			yzCfg_.stream = (strm);                                             \
+			cudaLaunchAttribute yzAttr_[1];                                       \
+			yzAttr_[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;   \
+			yzAttr_[0].val.programmaticStreamSerializationAllowed = 1;            \
+			yzCfg_.attrs = yzAttr_;                                               \
+			yzCfg_.numAttrs = 1;                                                  \
+			::yz::Check(cudaLaunchKernelEx(&yzCfg_, kernel, __VA_ARGS__), #kernel); \
+		}                                                                         \
+		else                                                                      \
+			kernel<<<(grid), (block), (smem), (strm)>>>(__VA_ARGS__);           \
+		if(yzTimed_) ::yz::TimeEnd(strm);                                       \
+		::yz::CountLaunches(1);                                                   \
+		::yz::Check(cudaGetLastError(), #kernel);                                 \
+	} while(0)
+
 void SetLastError(const std::string &m);
 
 //--------------------------------------------------------------------------

@@ -66,6 +66,7 @@ __global__ void __launch_bounds__(kRT, 8) KBInit(int n, const int *__restrict__ 
 __global__ void KPUpdate(int n, const double *__restrict__ r, const double *__restrict__ v,
                          double *__restrict__ p, Scal *sc)
 {
+	PdlEntry();
 	if(sc->state != kRun) return;
 	const bool lead = (blockIdx.x == 0 && threadIdx.x == 0);
 	if(sc->it >= sc->maxIter) { if(lead) sc->state = kCap; return; }
@@ -88,6 +89,7 @@ __global__ void __launch_bounds__(kRT, 8) KSpmvAlpha(int n, const int *__restric
                            const int *__restrict__ col, const V *__restrict__ val, const double *__restrict__ ph,
                            const double *__restrict__ rh, double *__restrict__ v, RedScratch rs, Scal *sc)
 {
+	PdlEntry();
 	if(sc->state != kRun) return;
 	__shared__ double sh[kRT];
 	double a[1] = {0.0};
@@ -108,6 +110,7 @@ __global__ void __launch_bounds__(kRT, 8) KSpmvAlpha(int n, const int *__restric
 __global__ void KSUpdate(int n, const double *__restrict__ r, const double *__restrict__ v,
                          double *__restrict__ s, RedScratch rs, Scal *sc)
 {
+	PdlEntry();
 	if(sc->state != kRun) return;
 	__shared__ double sh[kRT];
 	const double alpha = sc->alpha;
@@ -136,6 +139,7 @@ __global__ void __launch_bounds__(kRT, 8) KSpmvOmega(int n, const int *__restric
                            const int *__restrict__ col, const V *__restrict__ val, const double *__restrict__ sh_,
                            const double *__restrict__ s, double *__restrict__ t, RedScratch rs, Scal *sc)
 {
+	PdlEntry();
 	if(sc->state != kRun) return;
 	__shared__ double sh[2 * kRT];
 	double a[2] = {0.0, 0.0};
@@ -162,6 +166,7 @@ __global__ void KXRUpdate(int n, const double *__restrict__ ph, const double *__
                           const double *__restrict__ rh, double *__restrict__ x, double *__restrict__ r,
                           RedScratch rs, Scal *sc)
 {
+	PdlEntry();
 	const int state = sc->state;
 	if(state == kConvHalf)
 	{
@@ -710,7 +715,7 @@ void Solver::Cycle32(size_t l, const TF *f, TX *x)
 	const int n = L.n, g = GridFor(n, kB);
 	if(L.direct)
 	{
-		YZ_LAUNCH((KDenseMV<float, TF, TX>), GridFor((long long)n * 32, kB), kB, 0, _st, Halt(), n, L.inv32.get(), f, x);
+		YZ_LAUNCH_PDL((KDenseMV<float, TF, TX>), GridFor((long long)n * 32, kB), kB, 0, _st, Halt(), n, L.inv32.get(), f, x);
 		return;
 	}
 	const int *so = l == 0 ? _sellOff.get() : nullptr, *col = l == 0 ? _sellCol.get() : L.col.get();
@@ -719,10 +724,10 @@ void Solver::Cycle32(size_t l, const TF *f, TX *x)
 	//  coarser levels (yz_coarse.cuh)
 	if(l == 0 && _nlev > 1 && CoarseCycleOn())
 	{
-		YZ_LAUNCH((KPreSmoothResidual<float, TF, float>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col,
+		YZ_LAUNCH_PDL((KPreSmoothResidual<float, TF, float>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col,
 		          val, L.M32.get(), f, L.x32.get(), L.t32.get());
 		LaunchCoarseCycle();
-		YZ_LAUNCH((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val,
+		YZ_LAUNCH_PDL((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val,
 		          L.M32.get(), f, L.xt32.get(), x);
 		return;
 	}
@@ -747,15 +752,15 @@ void Solver::Cycle32(size_t l, const TF *f, TX *x)
 			if(la > 1) CoarsePreSmooth(la, n, L.ptr.get(), col, val, L.M32.get(), f, L.x32.get(), L.t32.get());
 		}
 		if(la == 1)
-			YZ_LAUNCH((KPreSmoothResidual<float, TF, float>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col,
+			YZ_LAUNCH_PDL((KPreSmoothResidual<float, TF, float>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col,
 			          val, L.M32.get(), f, L.x32.get(), L.t32.get());
-		YZ_LAUNCH(KRestrict<float>, GridFor((long long)C.n * 4, kB), kB, 0, _st, Halt(), C.n, L.rptr.get(), L.rcol.get(),
+		YZ_LAUNCH_PDL(KRestrict<float>, GridFor((long long)C.n * 4, kB), kB, 0, _st, Halt(), C.n, L.rptr.get(), L.rcol.get(),
 		          L.rval32.get(), L.t32.get(), C.f32.get());
 		Cycle32<float, float>(l + 1, C.f32.get(), C.x32.get());
 		if(lp > 1)
 			CoarseProlong(lp, n, L.pptr.get(), L.pcol.get(), L.pval32.get(), C.x32.get(), L.x32.get(), L.xt32.get());
 		else
-			YZ_LAUNCH(KProlong<float>, g, kB, 0, _st, Halt(), n, L.pptr.get(), L.pcol.get(), L.pval32.get(), C.x32.get(),
+			YZ_LAUNCH_PDL(KProlong<float>, g, kB, 0, _st, Halt(), n, L.pptr.get(), L.pcol.get(), L.pval32.get(), C.x32.get(),
 			          L.x32.get(), L.xt32.get());
 		if constexpr(coarse)
 		{
@@ -770,18 +775,18 @@ void Solver::Cycle32(size_t l, const TF *f, TX *x)
 				for(int k = 1; k < FineSweeps(); ++k)
 				{
 					float *xo = (xin == L.xt32.get()) ? L.x32.get() : L.xt32.get();
-					YZ_LAUNCH((KPostSmooth<float, TF, float>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col,
+					YZ_LAUNCH_PDL((KPostSmooth<float, TF, float>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col,
 					          val, L.M32.get(), f, xin, xo);
 					xin = xo;
 				}
-			YZ_LAUNCH((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val,
+			YZ_LAUNCH_PDL((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val,
 			          L.M32.get(), f, xin, x);
 		}
 	}
 	else
 	{
-		YZ_LAUNCH((KPreSmooth<float, TF, float>), g, kB, 0, _st, Halt(), n, L.M32.get(), f, L.xt32.get());
-		YZ_LAUNCH((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val, L.M32.get(), f,
+		YZ_LAUNCH_PDL((KPreSmooth<float, TF, float>), g, kB, 0, _st, Halt(), n, L.M32.get(), f, L.xt32.get());
+		YZ_LAUNCH_PDL((KPostSmooth<float, TF, TX>), g, kB, 0, _st, Halt(), n, L.ptr.get(), so, StenOf(l), col, val, L.M32.get(), f,
 		          L.xt32.get(), x);
 	}
 }
@@ -907,9 +912,9 @@ int Solver::LanesFor(long long nnz, int n) const
 	do {                                                                                                \
 		switch(lanes)                                                                                   \
 		{                                                                                               \
-		case 8:  YZ_LAUNCH((K<8, float>), GridFor((long long)(n) * 8, kB), kB, 0, _st, __VA_ARGS__); break;  \
-		case 4:  YZ_LAUNCH((K<4, float>), GridFor((long long)(n) * 4, kB), kB, 0, _st, __VA_ARGS__); break;  \
-		default: YZ_LAUNCH((K<2, float>), GridFor((long long)(n) * 2, kB), kB, 0, _st, __VA_ARGS__); break;  \
+		case 8:  YZ_LAUNCH_PDL((K<8, float>), GridFor((long long)(n) * 8, kB), kB, 0, _st, __VA_ARGS__); break;  \
+		case 4:  YZ_LAUNCH_PDL((K<4, float>), GridFor((long long)(n) * 4, kB), kB, 0, _st, __VA_ARGS__); break;  \
+		default: YZ_LAUNCH_PDL((K<2, float>), GridFor((long long)(n) * 2, kB), kB, 0, _st, __VA_ARGS__); break;  \
 		}                                                                                               \
 	} while(0)
 
@@ -933,7 +938,7 @@ void Solver::CoarseProlong(int lanes, int n, const int *pptr, const int *pcol, c
 void Solver::CoarseDown(int lanes, int nc, const Level &L, const float *f, float *fc)
 {
 	if(lanes == 32)
-		YZ_LAUNCH((KDownFused<32, float>), GridFor((long long)nc * 32, kB), kB, 0, _st, Halt(), nc, L.rptr.get(),
+		YZ_LAUNCH_PDL((KDownFused<32, float>), GridFor((long long)nc * 32, kB), kB, 0, _st, Halt(), nc, L.rptr.get(),
 		          L.rcol.get(), L.rval32.get(), L.ptr.get(), L.col.get(), L.val32.get(), L.M32.get(), f, fc);
 	else
 		YZ_BY_LANES(lanes, KDownFused, nc, Halt(), nc, L.rptr.get(), L.rcol.get(), L.rval32.get(), L.ptr.get(),
@@ -1049,19 +1054,19 @@ void Solver::EnqueueIteration(int kind)
 	const float *val32 = _precision == YZ_PREC_FP32_MATRIX ? _sellVal32.get() : nullptr;
 	Scal *sc = _sc.get();
 	double *x = _x.get();
-	YZ_LAUNCH(KPUpdate, g, kB, 0, _st, n, _r.get(), _v.get(), _p.get(), sc);
+	YZ_LAUNCH_PDL(KPUpdate, g, kB, 0, _st, n, _r.get(), _v.get(), _p.get(), sc);
 	ApplyPrec(kind, _p.get(), _ph.get());
 	if(val32)
-		YZ_LAUNCH(KSpmvAlpha, nb, kRT, 0, _st, n, ptr, so, _sten, col, val32, _ph.get(), _rh.get(), _v.get(), Red(1), sc);
+		YZ_LAUNCH_PDL(KSpmvAlpha<float>, nb, kRT, 0, _st, n, ptr, so, _sten, col, val32, _ph.get(), _rh.get(), _v.get(), Red(1), sc);
 	else
-		YZ_LAUNCH(KSpmvAlpha, nb, kRT, 0, _st, n, ptr, so, _sten, col, val, _ph.get(), _rh.get(), _v.get(), Red(1), sc);
-	YZ_LAUNCH(KSUpdate, nb, kRT, 0, _st, n, _r.get(), _v.get(), _s.get(), Red(2), sc);
+		YZ_LAUNCH_PDL(KSpmvAlpha<double>, nb, kRT, 0, _st, n, ptr, so, _sten, col, val, _ph.get(), _rh.get(), _v.get(), Red(1), sc);
+	YZ_LAUNCH_PDL(KSUpdate, nb, kRT, 0, _st, n, _r.get(), _v.get(), _s.get(), Red(2), sc);
 	ApplyPrec(kind, _s.get(), _sh.get());
 	if(val32)
-		YZ_LAUNCH(KSpmvOmega, nb, kRT, 0, _st, n, ptr, so, _sten, col, val32, _sh.get(), _s.get(), _t.get(), Red(3), sc);
+		YZ_LAUNCH_PDL(KSpmvOmega<float>, nb, kRT, 0, _st, n, ptr, so, _sten, col, val32, _sh.get(), _s.get(), _t.get(), Red(3), sc);
 	else
-		YZ_LAUNCH(KSpmvOmega, nb, kRT, 0, _st, n, ptr, so, _sten, col, val, _sh.get(), _s.get(), _t.get(), Red(3), sc);
-	YZ_LAUNCH(KXRUpdate, nb, kRT, 0, _st, n, _ph.get(), _sh.get(), _s.get(), _t.get(), _rh.get(), x, _r.get(),
+		YZ_LAUNCH_PDL(KSpmvOmega<double>, nb, kRT, 0, _st, n, ptr, so, _sten, col, val, _sh.get(), _s.get(), _t.get(), Red(3), sc);
+	YZ_LAUNCH_PDL(KXRUpdate, nb, kRT, 0, _st, n, _ph.get(), _sh.get(), _s.get(), _t.get(), _rh.get(), x, _r.get(),
 	          Red(4), sc);
 }
 
