@@ -11,7 +11,9 @@ through tests/golden/make_golden.py):
     linear iteration and coupling pass counts, h and c within 1e-10
     relative L2;
   * the solute of the closed film conserved on the device as in the
-    reference, and two runs bit-identical."""
+    reference, and two runs bit-identical;
+  * the film's solves with the learned preconditioner within 1e-8 of the
+    reference's run."""
 from pathlib import Path
 
 import numpy as np
